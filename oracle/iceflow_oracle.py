@@ -1,0 +1,657 @@
+"""CPU oracle for IGM's iceflow + thk hot path.
+
+TEST INFRASTRUCTURE ONLY.  Nothing in the product (``igm_b200``) imports this
+module; it is imported by ``tests/``, by ``__graft_entry__.smoke()`` as the
+checker, and by ``bench.py``'s CPU-baseline leg.
+
+It restates, op by op and in the same evaluation order, the reference's
+TensorFlow code for the path (all paths relative to the reference project):
+
+* Blatter-Pattyn energy, staggered grid, Lagrange vertical basis
+  - ``igm/processes/iceflow/energy/cost_shear.py:55-209``
+  - ``igm/processes/iceflow/energy/cost_gravity.py:24-69``
+  - ``igm/processes/iceflow/energy/cost_sliding_weertman.py:23-43``
+  - ``igm/processes/iceflow/energy/utils.py:11-25`` (stag2, stag2v, stag4h)
+  - ``igm/utils/gradient/compute_gradient.py:3-16`` (staggered branch)
+  - the per-term ``reduce_mean`` + ``add_n`` of ``igm/processes/iceflow/solve/solve.py:57-59``
+* vertical discretisation ``igm/processes/iceflow/vert_disc.py:10-47``
+* velbase / velsurf / velbar ``igm/processes/iceflow/utils.py:21-51``
+* EarlyStopping ``igm/processes/iceflow/utils.py:80-110``
+* the plain solver loop ``igm/processes/iceflow/solve/solve.py:22-119``
+* Keras legacy Adam (TF 2.15.1, third party, not vendored): the published
+  Adam update of Kingma & Ba (2015, Algorithm 1 with the "epsilon hat"
+  variant), in the form ``m += (g-m)(1-b1); v += (g^2-v)(1-b2);
+  x -= lr*sqrt(1-b2^t)/(1-b1^t) * m/(sqrt(v)+eps)``, with optional
+  per-variable clip-by-norm ``g*c/max(|g|,c)``.
+* slope-limited upwind transport
+  ``igm/utils/gradient/compute_divflux_slope_limiter.py:3-65`` and the thk
+  update ``igm/processes/thk/thk.py:11-54``
+* CFL time step ``igm/processes/time/time.py:28-65``
+* ELA mass balance ``igm/processes/smb_simple/smb_simple.py:24-50``
+* the CNN emulator ``igm/processes/iceflow/emulate/neural_network.py:9-66``
+  (Conv2D 3x3 "same" + bias + LeakyReLU(0.01), 1x1 head), with the NHWC
+  layout conversions of ``igm/processes/iceflow/utils.py:133-158``.
+
+All functions take and return ``torch`` CPU tensors; the dtype of the inputs
+(float32 or float64) is the arithmetic precision.  Gradients of the energy are
+obtained with torch autograd of this restatement, the stand-in for the
+reference's ``tf.GradientTape`` (``solve.py:77``).
+
+Parity pin: ``tests/golden/make_golden.py`` executes the reference's own
+source files for these functions (under a TF-API shim over torch, because
+TensorFlow cannot be installed here) and stores the results as fixtures;
+``tests/test_oracle_golden.py`` checks this module against them.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+# --------------------------------------------------------------------------
+# physical parameters (defaults of igm/conf/processes/iceflow.yaml:4-21)
+# --------------------------------------------------------------------------
+
+
+@dataclass
+class Physics:
+    exp_glen: float = 3.0
+    exp_weertman: float = 3.0
+    regu_glen: float = 1.0e-5
+    regu_weertman: float = 1.0e-10
+    thr_ice_thk: float = 0.1
+    min_sr: float = 1.0e-20
+    max_sr: float = 1.0e20
+    ice_density: float = 910.0
+    gravity_cst: float = 9.81
+    force_negative_gravitational_energy: bool = False
+
+
+def _t(x, dtype=None):
+    if isinstance(x, torch.Tensor):
+        return x if dtype is None else x.to(dtype)
+    return torch.as_tensor(np.asarray(x), dtype=dtype)
+
+
+# --------------------------------------------------------------------------
+# vertical discretisation  (vert_disc.py:10-13, 27-35, 43-47)
+# --------------------------------------------------------------------------
+
+
+def compute_levels(Nz: int, vert_spacing: float, dtype=torch.float32):
+    """vert_disc.py:10-13: zeta_k = k/(Nz-1), level = zeta/s * (1 + (s-1) zeta)."""
+    zeta = (torch.arange(Nz, dtype=torch.float64) / (Nz - 1)).to(dtype) if Nz > 1 else torch.zeros(1, dtype=dtype)
+    return (zeta / vert_spacing) * (1.0 + (vert_spacing - 1.0) * zeta)
+
+
+def compute_zeta_dzeta(levels):
+    """vert_disc.py:27-35: midpoints and differences of the levels."""
+    if levels.shape[0] > 1:
+        return (levels[1:] + levels[:-1]) / 2, levels[1:] - levels[:-1]
+    return 0.5 * torch.ones(1, dtype=levels.dtype), torch.ones(1, dtype=levels.dtype)
+
+
+def define_vertical_weight(Nz: int, vert_spacing: float, dtype=torch.float32):
+    """vert_disc.py:43-47: weights from Nz+1 equispaced points through the same map."""
+    zeta = (torch.arange(Nz + 1, dtype=torch.float64) / Nz).to(dtype)
+    w = (zeta / vert_spacing) * (1.0 + (vert_spacing - 1.0) * zeta)
+    return (w[1:] - w[:-1])[:, None, None]
+
+
+# --------------------------------------------------------------------------
+# staggered-grid primitives  (energy/utils.py:11-25, compute_gradient.py:3-16)
+# --------------------------------------------------------------------------
+
+
+def stag2v(B):
+    if B.shape[-3] > 1:
+        B = (B[..., :-1, :, :] + B[..., 1:, :, :]) / 2
+    return B
+
+
+def stag4h(B):
+    return (B[..., 1:, 1:] + B[..., 1:, :-1] + B[..., :-1, 1:] + B[..., :-1, :-1]) / 4
+
+
+def compute_gradient_stag(s, dx):
+    """compute_gradient.py:3-16 with a uniform dX field equal to ``dx``."""
+    E = 2.0 * (s[..., :, 1:] - s[..., :, :-1]) / (dx + dx)
+    diffx = 0.5 * (E[..., 1:, :] + E[..., :-1, :])
+    EE = 2.0 * (s[..., 1:, :] - s[..., :-1, :]) / (dx + dx)
+    diffy = 0.5 * (EE[..., :, 1:] + EE[..., :, :-1])
+    return diffx, diffy
+
+
+# --------------------------------------------------------------------------
+# energy  (cost_shear.py, cost_gravity.py, cost_sliding_weertman.py)
+# U, V : [B, Nz, Ny, Nx]   thk, usurf, arrhenius, slidingco : [B, Ny, Nx]
+# --------------------------------------------------------------------------
+
+
+def _horizontal_derivatives(U, V, dx):
+    """cost_shear.py:25-38 (staggered branch)."""
+    dUdx = (U[..., :, :, 1:] - U[..., :, :, :-1]) / dx
+    dVdx = (V[..., :, :, 1:] - V[..., :, :, :-1]) / dx
+    dUdy = (U[..., :, 1:, :] - U[..., :, :-1, :]) / dx
+    dVdy = (V[..., :, 1:, :] - V[..., :, :-1, :]) / dx
+    dUdx = (dUdx[..., :, :-1, :] + dUdx[..., :, 1:, :]) / 2
+    dVdx = (dVdx[..., :, :-1, :] + dVdx[..., :, 1:, :]) / 2
+    dUdy = (dUdy[..., :, :, :-1] + dUdy[..., :, :, 1:]) / 2
+    dVdy = (dVdy[..., :, :, :-1] + dVdy[..., :, :, 1:]) / 2
+    return dUdx, dVdx, dUdy, dVdy
+
+
+def cost_shear(U, V, thk, usurf, arrhenius, slidingco, dx, dzeta, ph: Physics):
+    """cost_shear.py:103-179, Lagrange basis, staggered grid."""
+    B = 2.0 * arrhenius ** (-1.0 / ph.exp_glen)
+    B = B[:, None, :, :]
+    p = 1.0 + 1.0 / ph.exp_glen
+    dUdx, dVdx, dUdy, dVdy = _horizontal_derivatives(U, V, dx)
+    sloptopgx, sloptopgy = compute_gradient_stag(usurf - thk, dx)
+    U = stag4h(U)
+    V = stag4h(V)
+    slidingco = stag4h(slidingco)
+    thk = stag4h(thk)
+    B = stag4h(B)
+    dUdx = stag2v(dUdx)
+    dVdx = stag2v(dVdx)
+    dUdy = stag2v(dUdy)
+    dVdy = stag2v(dVdy)
+    B = stag2v(B)
+    if U.shape[-3] > 1:
+        h = torch.clamp(thk, min=ph.thr_ice_thk)[:, None]
+        dUdz = (U[:, 1:] - U[:, :-1]) / (dzeta[None, :, None, None] * h)
+        dVdz = (V[:, 1:] - V[:, :-1]) / (dzeta[None, :, None, None] * h)
+    else:
+        dUdz = torch.zeros_like(U)
+        dVdz = torch.zeros_like(V)
+    fl = slidingco[:, None] > 0
+    dUdz = torch.where(fl, dUdz, 0.01 * dUdz)
+    dVdz = torch.where(fl, dVdz, 0.01 * dVdz)
+    sx = sloptopgx[:, None]
+    sy = sloptopgy[:, None]
+    dUdx = dUdx - dUdz * sx
+    dUdy = dUdy - dUdz * sy
+    dVdx = dVdx - dVdz * sx
+    dVdy = dVdy - dVdz * sy
+    Exx = dUdx
+    Eyy = dVdy
+    Ezz = -dUdx - dVdy
+    Exy = 0.5 * dVdx + 0.5 * dUdy
+    srxy2 = 0.5 * (Exx**2 + Exy**2 + Exy**2 + Eyy**2 + Ezz**2)
+    Exz = 0.5 * dUdz
+    Eyz = 0.5 * dVdz
+    srz2 = 0.5 * (Exz**2 + Eyz**2 + Exz**2 + Eyz**2)
+    sr2 = srxy2 + srz2
+    # TF converts the clip bounds to the tensor's dtype: in float32, 1e40 -> +inf
+    npdt = np.float32 if sr2.dtype == torch.float32 else np.float64
+    with np.errstate(over="ignore"):
+        lo = torch.as_tensor(npdt(ph.min_sr**2), dtype=sr2.dtype)
+        hi = torch.as_tensor(npdt(ph.max_sr**2), dtype=sr2.dtype)
+    sr2capped = torch.clamp(sr2, lo, hi)
+    p_term = ((sr2capped + ph.regu_glen**2) ** ((p - 2) / 2)) * sr2 / p
+    return thk * torch.sum(B * dzeta[None, :, None, None] * p_term, dim=1)
+
+
+def cost_gravity(U, V, thk, usurf, dx, dzeta, ph: Physics):
+    """cost_gravity.py:24-69, Lagrange basis, staggered grid."""
+    slopsurfx, slopsurfy = compute_gradient_stag(usurf, dx)
+    U = stag4h(U)
+    V = stag4h(V)
+    thk = stag4h(thk)
+    U = stag2v(U)
+    V = stag2v(V)
+    uds = U * slopsurfx[:, None] + V * slopsurfy[:, None]
+    if ph.force_negative_gravitational_energy:
+        uds = torch.clamp(uds, max=0.0)
+    return ph.ice_density * ph.gravity_cst * 10 ** (-6) * thk * torch.sum(dzeta[None, :, None, None] * uds, dim=1)
+
+
+def cost_sliding_weertman(U, V, thk, usurf, slidingco, dx, ph: Physics):
+    """cost_sliding_weertman.py:23-43, staggered grid."""
+    C = 1.0 * slidingco
+    s = 1.0 + 1.0 / ph.exp_weertman
+    sloptopgx, sloptopgy = compute_gradient_stag(usurf - thk, dx)
+    U = stag4h(U)
+    V = stag4h(V)
+    C = stag4h(C)
+    ub = U[:, 0]
+    vb = V[:, 0]
+    N = (ub**2 + vb**2) + ph.regu_weertman**2 + (ub * sloptopgx + vb * sloptopgy) ** 2
+    return C * N ** (s / 2) / s
+
+
+def energy_terms(U, V, thk, usurf, arrhenius, slidingco, dx, dzeta, ph: Physics | None = None):
+    """Per-cell energy densities [shear, sliding, gravity], each [B, Ny-1, Nx-1].
+
+    Order follows ``energy_components: [shear, sliding_weertman, gravity]``
+    (iceflow.yaml:5) as dispatched by energy.py:12-22.  4-D U/V expected
+    (batch first, as solve.py:51 passes ``U[None]``); 3-D inputs get a batch
+    dimension added.
+    """
+    ph = ph or Physics()
+    if U.dim() == 3:
+        U, V = U[None], V[None]
+        thk, usurf, arrhenius, slidingco = thk[None], usurf[None], arrhenius[None], slidingco[None]
+    return [
+        cost_shear(U, V, thk, usurf, arrhenius, slidingco, dx, dzeta, ph),
+        cost_sliding_weertman(U, V, thk, usurf, slidingco, dx, ph),
+        cost_gravity(U, V, thk, usurf, dx, dzeta, ph),
+    ]
+
+
+def energy(U, V, thk, usurf, arrhenius, slidingco, dx, dzeta, ph: Physics | None = None):
+    """COST = sum of reduce_mean of each term (solve.py:57-59).  Returns (cost, [means])."""
+    terms = energy_terms(U, V, thk, usurf, arrhenius, slidingco, dx, dzeta, ph)
+    means = [t.mean() for t in terms]
+    return means[0] + means[1] + means[2], means
+
+
+def energy_and_grad(U, V, thk, usurf, arrhenius, slidingco, dx, dzeta, ph: Physics | None = None):
+    """COST and dCOST/dU, dCOST/dV by autograd (stand-in for tape.gradient, solve.py:77)."""
+    U = U.detach().clone().requires_grad_(True)
+    V = V.detach().clone().requires_grad_(True)
+    cost, means = energy(U, V, thk, usurf, arrhenius, slidingco, dx, dzeta, ph)
+    gU, gV = torch.autograd.grad(cost, [U, V])
+    return cost.detach(), [m.detach() for m in means], gU, gV
+
+
+# --------------------------------------------------------------------------
+# optimiser, early stopping, solver
+# --------------------------------------------------------------------------
+
+
+class KerasLegacyAdam:
+    """Adam as Keras' legacy optimizer applies it (see module docstring).
+
+    ``iterations`` is global to the optimizer object and survives across
+    solves, exactly as ``state.optimizer`` does in the reference
+    (solve.py:11-20, 84); moment slots are per variable object.
+    """
+
+    def __init__(self, lr=1.0, beta_1=0.9, beta_2=0.999, epsilon=1e-7, clipnorm=None):
+        self.lr, self.b1, self.b2, self.eps, self.clipnorm = lr, beta_1, beta_2, epsilon, clipnorm
+        self.iterations = 0
+        self.slots: dict[int, tuple[torch.Tensor, torch.Tensor]] = {}
+
+    def apply_gradients(self, grads_and_vars):
+        t = self.iterations + 1
+        dt = None
+        for g, x in grads_and_vars:
+            dt = x.dtype
+            if self.clipnorm is not None:
+                n = torch.sqrt(torch.sum(g.to(torch.float64) ** 2)).to(g.dtype)
+                g = g * self.clipnorm / torch.maximum(n, torch.tensor(self.clipnorm, dtype=g.dtype))
+            key = id(x)
+            if key not in self.slots:
+                self.slots[key] = (torch.zeros_like(x), torch.zeros_like(x))
+            m, v = self.slots[key]
+            one = torch.tensor(1.0, dtype=dt)
+            b1p = torch.tensor(self.b1, dtype=dt) ** t
+            b2p = torch.tensor(self.b2, dtype=dt) ** t
+            alpha = self.lr * torch.sqrt(one - b2p) / (one - b1p)
+            m += (g - m) * (1 - self.b1)
+            v += (g * g - v) * (1 - self.b2)
+            x -= (m * alpha) / (torch.sqrt(v) + self.eps)
+        self.iterations += 1
+
+
+class EarlyStopping:
+    """utils.py:80-110."""
+
+    def __init__(self, relative_min_delta=1e-3, patience=10):
+        self.relative_min_delta = relative_min_delta
+        self.patience = patience
+        self.wait = 0
+        self.best_loss = None
+
+    def should_stop(self, current_loss):
+        if self.best_loss is None:
+            self.best_loss = current_loss
+            return False
+        rel = (self.best_loss - current_loss) / abs(self.best_loss)
+        if rel > self.relative_min_delta:
+            self.best_loss = current_loss
+            self.wait = 0
+            return False
+        self.wait += 1
+        return self.wait >= self.patience
+
+
+def solve_iceflow(U, V, thk, usurf, arrhenius, slidingco, dx, dzeta, optimizer: KerasLegacyAdam,
+                  nbitmax=100, ph: Physics | None = None, early_stopping=True,
+                  relative_min_delta=0.0002, patience=10):
+    """solve.py:22-119 (Adam branch, no sliding_law, no plotting).
+
+    U, V [Nz, Ny, Nx] are copied (the reference wraps them in new
+    tf.Variables, so the optimizer creates fresh moment slots).  Returns
+    (U, V, cost_history) with U, V masked to zero where thk == 0.
+    """
+    U = U.detach().clone()
+    V = V.detach().clone()
+    es = EarlyStopping(relative_min_delta=relative_min_delta, patience=patience)
+    costs = []
+    for _ in range(nbitmax):
+        cost, _, gU, gV = energy_and_grad(U, V, thk, usurf, arrhenius, slidingco, dx, dzeta, ph)
+        costs.append(float(cost))
+        optimizer.apply_gradients([(gU, U), (gV, V)])
+        if early_stopping and es.should_stop(np.float32(cost) if U.dtype == torch.float32 else float(cost)):
+            break
+    mask = (thk > 0)[None]
+    U = torch.where(mask, U, torch.zeros_like(U))
+    V = torch.where(mask, V, torch.zeros_like(V))
+    return U, V, costs
+
+
+def get_velbase(U, V):
+    return U[..., 0, :, :], V[..., 0, :, :]
+
+
+def get_velsurf(U, V):
+    return U[..., -1, :, :], V[..., -1, :, :]
+
+
+def get_velbar(U, V, vert_weight):
+    return torch.sum(U * vert_weight, dim=-3), torch.sum(V * vert_weight, dim=-3)
+
+
+# --------------------------------------------------------------------------
+# transport, time step, mass balance
+# --------------------------------------------------------------------------
+
+
+def _minmod(a, b):
+    z = torch.zeros_like(a)
+    return torch.where((a.abs() < b.abs()) & (a * b > 0.0), a,
+                       torch.where((a.abs() > b.abs()) & (a * b > 0.0), b, z))
+
+
+def _maxmod(a, b):
+    z = torch.zeros_like(a)
+    return torch.where((a.abs() < b.abs()) & (a * b > 0.0), b,
+                       torch.where((a.abs() > b.abs()) & (a * b > 0.0), a, z))
+
+
+def compute_divflux_slope_limiter(u, v, h, dx, dy, dt, slope_type="superbee"):
+    """compute_divflux_slope_limiter.py:11-65.  u, v, h : [Ny, Nx]."""
+    u = torch.cat([u[:, 0:1], 0.5 * (u[:, :-1] + u[:, 1:]), u[:, -1:]], 1)
+    v = torch.cat([v[0:1, :], 0.5 * (v[:-1, :] + v[1:, :]), v[-1:, :]], 0)
+    Hx = torch.nn.functional.pad(h, (2, 2, 0, 0))
+    Hy = torch.nn.functional.pad(h, (0, 0, 2, 2))
+    sigpx = (Hx[:, 2:] - Hx[:, 1:-1]) / dx
+    sigmx = (Hx[:, 1:-1] - Hx[:, :-2]) / dx
+    sigpy = (Hy[2:, :] - Hy[1:-1, :]) / dy
+    sigmy = (Hy[1:-1, :] - Hy[:-2, :]) / dy
+    if slope_type == "godunov":
+        slopex = torch.zeros_like(sigpx)
+        slopey = torch.zeros_like(sigpy)
+    elif slope_type == "minmod":
+        slopex = _minmod(sigmx, sigpx)
+        slopey = _minmod(sigmy, sigpy)
+    elif slope_type == "superbee":
+        slopex = _maxmod(_minmod(sigpx, 2.0 * sigmx), _minmod(sigmx, 2.0 * sigpx))
+        slopey = _maxmod(_minmod(sigpy, 2.0 * sigmy), _minmod(sigmy, 2.0 * sigpy))
+    else:
+        raise ValueError(f"unknown slope_type {slope_type}")
+    w = Hx[:, 1:-2] + 0.5 * dx * (1.0 - u * dt / dx) * slopex[:, :-1]
+    e = Hx[:, 2:-1] - 0.5 * dx * (1.0 + u * dt / dx) * slopex[:, 1:]
+    s = Hy[1:-2, :] + 0.5 * dy * (1.0 - v * dt / dy) * slopey[:-1, :]
+    n = Hy[2:-1, :] - 0.5 * dy * (1.0 + v * dt / dy) * slopey[1:, :]
+    Qx = u * torch.where(u > 0, w, e)
+    Qy = v * torch.where(v > 0, s, n)
+    return (Qx[:, 1:] - Qx[:, :-1]) / dx + (Qy[1:, :] - Qy[:-1, :]) / dy
+
+
+def thk_update(thk, topg, ubar, vbar, smb, dx, dt, slope_type="superbee",
+               ratio_density=0.910, sealevel=0.0):
+    """thk.py:27-54.  Returns (thk, lsurf, usurf, divflux)."""
+    divflux = compute_divflux_slope_limiter(ubar, vbar, thk, dx, dx, dt, slope_type)
+    thk = torch.clamp(thk + dt * (smb - divflux), min=0)
+    lsurf = torch.maximum(topg, -ratio_density * thk + sealevel)
+    usurf = lsurf + thk
+    return thk, lsurf, usurf, divflux
+
+
+def thk_surfaces(thk, topg, ratio_density=0.910, sealevel=0.0):
+    """thk.py:11-24 (initialize)."""
+    lsurf = torch.maximum(topg, -ratio_density * thk + sealevel)
+    return lsurf, lsurf + thk
+
+
+def cfl_dt(ubar, vbar, dx, cfl=0.3, step_max=1.0):
+    """time.py:36-50 (without the save-time snapping, done by the caller)."""
+    velomax = float(torch.maximum(ubar.abs().max(), vbar.abs().max()))
+    if cfl > 0 and velomax > 0:
+        return min(cfl * dx / velomax, step_max), velomax
+    return step_max, velomax
+
+
+def smb_simple(usurf, gradabl, gradacc, ela, maxacc):
+    """smb_simple.py:39-41."""
+    smb = usurf - ela
+    smb = smb * torch.where(smb < 0, torch.tensor(gradabl, dtype=smb.dtype), torch.tensor(gradacc, dtype=smb.dtype))
+    return torch.clamp(smb, -100, maxacc)
+
+
+def interp1d(xs, ys, x):
+    """interp1d_tf.py: piecewise-linear, clamped to the table's range."""
+    return float(np.interp(np.clip(x, np.min(xs), np.max(xs)), xs, ys))
+
+
+# --------------------------------------------------------------------------
+# CNN emulator (neural_network.py:9-66) and layout helpers (utils.py:133-158)
+# --------------------------------------------------------------------------
+
+
+def cnn_forward(X, weights, biases, alpha=0.01, bf16=False, return_acts=False):
+    """Stack of Conv2D(3x3, same) + LeakyReLU, then a 1x1 Conv2D head.
+
+    X : [B, H, W, Cin] (NHWC, as fieldin_to_X builds it);
+    weights[l] : [3, 3, Cin_l, Cout_l] (Keras kernel layout), biases[l] : [Cout_l].
+    The last entry is the 1x1 head ([1, 1, 32, 2Nz]).  With ``bf16`` the
+    inputs of every 3x3 conv and their weights are rounded to bfloat16 and the
+    products accumulated in float32 (the emulator kernels' arithmetic); the
+    head and everything else stay float32.
+    Returns Y : [B, H, W, 2Nz].
+    """
+    x = X.permute(0, 3, 1, 2)
+    acts = []
+    nl = len(weights) - 1
+    for l in range(nl):
+        w = weights[l].permute(3, 2, 0, 1)
+        if bf16:
+            xin = x.to(torch.bfloat16).to(torch.float32)
+            w = w.to(torch.bfloat16).to(torch.float32)
+        else:
+            xin = x
+        x = torch.nn.functional.conv2d(xin, w, biases[l], padding=1)
+        x = torch.nn.functional.leaky_relu(x, alpha)
+        if bf16:
+            x = x.to(torch.bfloat16).to(torch.float32)
+        acts.append(x)
+    w = weights[-1].permute(3, 2, 0, 1)
+    y = torch.nn.functional.conv2d(x, w, biases[-1])
+    y = y.permute(0, 2, 3, 1)
+    return (y, acts) if return_acts else y
+
+
+def Y_to_UV(Y, Nz):
+    """utils.py:133-139: channels [0,Nz) are U levels, [Nz,2Nz) V levels."""
+    return Y[..., :Nz].movedim(-1, 1), Y[..., Nz:].movedim(-1, 1)
+
+
+def fieldin_to_X(fields):
+    """utils.py:147-158 for 2-D fields: stack on a trailing channel axis, add batch."""
+    return torch.stack(fields, dim=-1)[None]
+
+
+def split_into_patches(X, nbmax):
+    """emulate.py:283-308 ("sequential"): X [1, ny, nx, C] -> [P, 1, ly, lx, C]."""
+    ny, nx = X.shape[1], X.shape[2]
+    sy = ny // nbmax + 1
+    sx = nx // nbmax + 1
+    ly = int(ny / sy)
+    lx = int(nx / sx)
+    XX = []
+    for i in range(sx):
+        for j in range(sy):
+            XX.append(X[:, j * ly:(j + 1) * ly, i * lx:(i + 1) * lx, :])
+    return torch.stack(XX, dim=0)
+
+
+# --------------------------------------------------------------------------
+# synthetic glaciers (the shapes and distributions of the benchmark configs)
+# --------------------------------------------------------------------------
+
+
+def box_filter(a: np.ndarray, k: int = 5) -> np.ndarray:
+    """k x k moving average with edge replication."""
+    r = k // 2
+    p = np.pad(a, r, mode="edge")
+    c = np.cumsum(np.cumsum(p, 0), 1)
+    c = np.pad(c, ((1, 0), (1, 0)))
+    return (c[k:, k:] - c[:-k, k:] - c[k:, :-k] + c[:-k, :-k]) / (k * k)
+
+
+def valley_glacier(ny=100, nx=100, dx=100.0, seed=0, noise_sigma=5.0, varying_coeffs=False):
+    """Synthetic valley glacier.
+
+    The 10 km x 10 km valley of the 100x100 / dx=100 m case; larger grids map
+    their domain onto the same shape (coordinates scaled to 10 km), and the
+    bed noise is scaled with dx/100 m so its slope stays the same.
+    Bed: 3000 - 0.1 X + 0.002 (Y-5000)^2 + N(0, sigma^2);
+    thk = max(0, 300 (1-((Y-5000)/2500)^2) (1-X/10000)); usurf = topg + thk.
+    A = 78, c = 0.045 uniform, or (``varying_coeffs``) log-uniform per cell
+    in [20,150] and [0.01,0.1], smoothed with a 5-cell box filter.
+    Returns float32 numpy arrays.
+    """
+    rng = np.random.default_rng(seed)
+    Lx, Ly = nx * dx, ny * dx
+    x = np.arange(nx) * dx * (10000.0 / Lx)
+    y = np.arange(ny) * dx * (10000.0 / Ly)
+    X, Y = np.meshgrid(x, y)
+    sigma = noise_sigma * (dx / 100.0) if (nx, ny) != (100, 100) else noise_sigma
+    topg = 3000.0 - 0.1 * X + 0.002 * (Y - 5000.0) ** 2 + rng.normal(0.0, sigma, size=(ny, nx))
+    thk = np.maximum(0.0, 300.0 * (1.0 - ((Y - 5000.0) / 2500.0) ** 2) * (1.0 - X / 10000.0))
+    usurf = topg + thk
+    if varying_coeffs:
+        A = np.exp(rng.uniform(np.log(20.0), np.log(150.0), size=(ny, nx)))
+        c = np.exp(rng.uniform(np.log(0.01), np.log(0.1), size=(ny, nx)))
+        A = box_filter(A, 5)
+        c = box_filter(c, 5)
+    else:
+        A = np.full((ny, nx), 78.0)
+        c = np.full((ny, nx), 0.045)
+    f = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+    return dict(topg=f(topg), thk=f(thk), usurf=f(usurf), arrhenius=f(A), slidingco=f(c), dx=float(dx))
+
+
+def ridge_glacier(n=4096, dx=25.0, seed=0, n_ridges=12):
+    """Multi-valley bed: a 0.05-slope plane plus seeded Gaussian ridges
+    (height 500-1500 m, sigma 2-8 km).  thk starts at zero (the caller spins
+    it up).  A, c log-uniform per cell as in ``valley_glacier``."""
+    rng = np.random.default_rng(seed)
+    x = np.arange(n) * dx
+    X, Y = np.meshgrid(x, x)
+    topg = 3500.0 - 0.05 * X
+    for _ in range(n_ridges):
+        cx, cy = rng.uniform(0, n * dx, size=2)
+        h = rng.uniform(500.0, 1500.0)
+        s = rng.uniform(2000.0, 8000.0)
+        topg = topg + h * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * s * s))
+    A = box_filter(np.exp(rng.uniform(np.log(20.0), np.log(150.0), size=(n, n))), 5)
+    c = box_filter(np.exp(rng.uniform(np.log(0.01), np.log(0.1), size=(n, n))), 5)
+    thk = np.zeros((n, n))
+    f = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+    return dict(topg=f(topg), thk=f(thk), usurf=f(topg), arrhenius=f(A), slidingco=f(c), dx=float(dx))
+
+
+# --------------------------------------------------------------------------
+# emulator retraining loop (emulate.py:155-281) and the clock (time.py:11-65)
+# --------------------------------------------------------------------------
+
+
+@dataclass
+class EmulatorTraining:
+    retrain_freq: int = 10
+    lr: float = 2.0e-5
+    lr_init: float = 1.0e-4
+    lr_decay: float = 0.95
+    warm_up_it: float = -1e10
+    nbit_init: int = 1
+    nbit: int = 1
+    framesizemax: int = 750
+
+
+def emulator_retrain(weights, biases, optimizer: KerasLegacyAdam, X, it, tr: EmulatorTraining,
+                     Nz, dzeta, ph: Physics | None = None, bf16=False):
+    """emulate.py:155-281 ("sequential" patches, no perturbation, no borders).
+
+    ``weights``/``biases`` are leaf tensors updated in place; X is
+    [1, ny, nx, 5] (thk, usurf, arrhenius, slidingco, dX).  Returns the list
+    of per-epoch summed costs, or None when this iteration does not retrain.
+    """
+    run_it = tr.retrain_freq > 0 and (it % tr.retrain_freq == 0)
+    warm_up = int(it <= tr.warm_up_it)
+    if not (warm_up or run_it):
+        return None
+    Xp = split_into_patches(X, tr.framesizemax)
+    nbit, lr = (tr.nbit_init, tr.lr_init) if warm_up else (tr.nbit, tr.lr)
+    optimizer.lr = lr
+    params = []
+    for w, b in zip(weights, biases):
+        params += [w, b]
+    costs = []
+    for _ in range(nbit):
+        total = 0.0
+        for i in range(Xp.shape[0]):
+            if tr.lr_decay < 1:
+                optimizer.lr = lr * (tr.lr_decay ** (i / 1000))
+            Xi = Xp[i]
+            ps = [p.detach().clone().requires_grad_(True) for p in params]
+            Y = cnn_forward(Xi, ps[0::2], ps[1::2], bf16=bf16)
+            U, V = Y_to_UV(Y, Nz)
+            cost, _ = energy(U, V, Xi[..., 0], Xi[..., 1], Xi[..., 2], Xi[..., 3], Xi[0, 0, 0, 4], dzeta, ph)
+            grads = torch.autograd.grad(cost, ps)
+            with torch.no_grad():
+                optimizer.apply_gradients(list(zip(grads, params)))
+            total = total + float(cost.detach())
+        costs.append(total)
+    return costs
+
+
+class Clock:
+    """time.py:11-65: CFL time step snapped to the save times."""
+
+    def __init__(self, start=2000.0, end=2100.0, save=10.0, cfl=0.3, step_max=1.0):
+        self.t = np.float32(start)
+        self.end, self.cfl, self.step_max = end, cfl, step_max
+        self.itsave = -1
+        ts = list(np.arange(start, end, save)) + [end]
+        self.time_save = np.asarray(ts, dtype=np.float32)
+        self.dt = np.float32(step_max)
+        self.saveresult = False
+        self.continue_run = True
+
+    def update(self, ubar, vbar, dx, it):
+        if self.cfl > 0:
+            velomax = np.float32(max(float(ubar.abs().max()), float(vbar.abs().max())))
+            if velomax > 0:
+                dt = np.float32(min(np.float32(self.cfl * dx) / velomax, self.step_max))
+            else:
+                dt = np.float32(self.step_max)
+        else:
+            dt = np.float32(self.step_max)
+        self.dt = dt
+        if self.time_save[self.itsave + 1] <= self.t + self.dt:
+            self.dt = np.float32(self.time_save[self.itsave + 1] - self.t)
+            self.saveresult = True
+            self.itsave += 1
+        else:
+            self.saveresult = False
+        if it >= 0:
+            self.t = np.float32(self.t + self.dt)
+        self.continue_run = bool(self.t < self.end)

@@ -1,0 +1,318 @@
+"""Generate the golden vectors in this directory by executing the reference's
+own source files (IGM 3.0.0) for the iceflow + thk path.
+
+TensorFlow is not installable here, so ``tf_shim`` stands in for it (every
+``tf.*`` call maps to the torch op with the same semantics; GradientTape is
+torch autograd).  The reference package's ``__init__`` files import Hydra,
+xarray, OGGM and the rest of the model, so the packages on the path are
+registered as bare namespace stubs and only the hot-path modules are loaded
+from their files.
+
+Run from the repository root:  python tests/golden/make_golden.py [REF_ROOT]
+(REF_ROOT defaults to /root/reference).  Writes ``*.npz`` next to this file.
+The generated inputs are seeded; re-running reproduces the files bit for bit.
+"""
+
+from __future__ import annotations
+
+import importlib
+import os
+import sys
+import types
+
+import numpy as np
+import torch
+import yaml
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import tf_shim  # noqa: E402
+
+tf_shim.install()
+import tensorflow as tf  # noqa: E402  (the shim)
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+IGM = os.path.join(REF, "igm")
+
+
+def _stub(name, path):
+    m = types.ModuleType(name)
+    m.__path__ = [path]
+    sys.modules[name] = m
+    parent, _, child = name.rpartition(".")
+    if parent:
+        setattr(sys.modules[parent], child, m)
+    return m
+
+
+for pkg in ["", "processes", "processes/iceflow", "processes/iceflow/energy",
+            "processes/iceflow/energy/sliding_laws", "processes/iceflow/emulate",
+            "processes/iceflow/emulate/emulators", "processes/iceflow/solve",
+            "processes/iceflow/diagnostic", "processes/thk", "processes/time",
+            "utils", "utils/gradient", "utils/math"]:
+    _stub("igm" + ("." + pkg.replace("/", ".") if pkg else ""), os.path.join(IGM, pkg))
+
+energy_pkg = sys.modules["igm.processes.iceflow.energy"]
+for comp in ["cost_shear", "cost_gravity", "cost_sliding_weertman"]:
+    mod = importlib.import_module(f"igm.processes.iceflow.energy.{comp}")
+    setattr(energy_pkg, comp, getattr(mod, comp))
+
+vert_disc = importlib.import_module("igm.processes.iceflow.vert_disc")
+ice_utils = importlib.import_module("igm.processes.iceflow.utils")
+energy_mod = importlib.import_module("igm.processes.iceflow.energy.energy")
+solve_mod = importlib.import_module("igm.processes.iceflow.solve.solve")
+emulate_mod = importlib.import_module("igm.processes.iceflow.emulate.emulate")
+divflux_mod = importlib.import_module("igm.utils.gradient.compute_divflux_slope_limiter")
+thk_mod = importlib.import_module("igm.processes.thk.thk")
+time_mod = importlib.import_module("igm.processes.time.time")
+
+
+def ns(d):
+    if isinstance(d, dict):
+        return types.SimpleNamespace(**{k: ns(v) for k, v in d.items()})
+    return d
+
+
+def load_cfg(**over):
+    procs = {}
+    for p in ["iceflow", "thk", "time"]:
+        with open(os.path.join(IGM, "conf", "processes", f"{p}.yaml")) as f:
+            procs.update(yaml.safe_load(f))
+    for path, val in over.items():
+        d = procs
+        keys = path.split(".")
+        for k in keys[:-1]:
+            d = d[k]
+        d[keys[-1]] = val
+    return ns({"processes": procs})
+
+
+def glacier(ny, nx, dx, seed, dtype, c_neg=False):
+    """Seeded small valley-glacier state with varying A, c and some ice-free cells."""
+    rng = np.random.default_rng(seed)
+    y, x = np.meshgrid(np.arange(ny) * dx, np.arange(nx) * dx, indexing="ij")
+    Ly, Lx = ny * dx, nx * dx
+    topg = 2500 - 0.08 * x + 4e-4 * (y - Ly / 2) ** 2 / (Ly / 2000) + rng.normal(0, 3, (ny, nx))
+    thk = np.maximum(0, 150 * (1 - ((y - Ly / 2) / (0.4 * Ly)) ** 2) * (1 - x / (1.1 * Lx)))
+    thk = thk + rng.uniform(0, 5, (ny, nx)) * (thk > 0)
+    usurf = topg + thk
+    A = np.exp(rng.uniform(np.log(20), np.log(150), (ny, nx)))
+    c = np.exp(rng.uniform(np.log(0.01), np.log(0.1), (ny, nx)))
+    if c_neg:
+        c[rng.uniform(size=(ny, nx)) < 0.1] = 0.0
+    f = lambda a: torch.as_tensor(a, dtype=dtype)
+    return dict(topg=f(topg), thk=f(thk), usurf=f(usurf), arrhenius=f(A), slidingco=f(c),
+                dX=f(np.full((ny, nx), dx)), dx=dx)
+
+
+def vel(nz, ny, nx, seed, dtype, scale=40.0):
+    rng = np.random.default_rng(seed + 1000)
+    base = rng.normal(0, scale, (2, nz, ny, nx))
+    prof = np.linspace(0.3, 1.0, nz)[:, None, None]
+    return (torch.as_tensor(base[0] * prof + 30, dtype=dtype),
+            torch.as_tensor(base[1] * prof - 5, dtype=dtype))
+
+
+def energy_case(name, ny, nx, nz, dx, seed, dtype, spacing=4.0, c_neg=False):
+    cfg = load_cfg(**{"iceflow.numerics.Nz": nz, "iceflow.numerics.vert_spacing": spacing})
+    g = glacier(ny, nx, dx, seed, dtype, c_neg)
+    U, V = vel(nz, ny, nx, seed, dtype)
+    levels = vert_disc.compute_levels(nz, spacing).to(dtype)
+    zeta, dzeta = vert_disc.compute_zeta_dzeta(levels)
+    fieldin = [g[f][None] for f in cfg.processes.iceflow.emulator.fieldin]
+    Uv = U.clone().requires_grad_(True)
+    Vv = V.clone().requires_grad_(True)
+    with tf.GradientTape(persistent=True) as t:
+        terms = energy_mod.iceflow_energy(cfg, Uv[None], Vv[None], fieldin, [zeta, dzeta, None, None])
+        means = [tf.reduce_mean(e) for e in terms]
+        COST = tf.add_n(means)
+    gU, gV = t.gradient(COST, [Uv, Vv])
+    out = dict(U=U, V=V, thk=g["thk"], usurf=g["usurf"], arrhenius=g["arrhenius"], slidingco=g["slidingco"],
+               dx=np.array(dx), levels=levels, dzeta=dzeta, cost=COST.detach(),
+               shear=terms[0][0].detach(), sliding=terms[1][0].detach(), gravity=terms[2][0].detach(),
+               means=torch.stack([m.detach() for m in means]), gradU=gU, gradV=gV)
+    save(f"energy_{name}", out)
+
+
+def vert_cases():
+    out = {}
+    for nz in [2, 3, 5, 10, 16, 30]:
+        for sp in [1.0, 2.0, 4.0]:
+            lv = vert_disc.compute_levels(nz, sp)
+            z, dz = vert_disc.compute_zeta_dzeta(lv)
+            w = vert_disc.define_vertical_weight(nz, sp)
+            key = f"nz{nz}_s{int(sp)}"
+            out[key + "_levels"] = lv
+            out[key + "_zeta"] = z
+            out[key + "_dzeta"] = dz
+            out[key + "_weight"] = w[:, 0, 0]
+    save("vert_disc", out)
+
+
+def solver_case(name, ny, nx, nz, dx, seed, dtype, nbitmax, n_solves):
+    cfg = load_cfg(**{"iceflow.numerics.Nz": nz, "iceflow.solver.nbitmax": nbitmax,
+                      "iceflow.method": "solved"})
+    g = glacier(ny, nx, dx, seed, dtype)
+    state = types.SimpleNamespace(**{k: g[k] for k in ["thk", "usurf", "arrhenius", "slidingco", "dX", "topg"]})
+    state.it = 5
+    state.U = torch.zeros((nz, ny, nx), dtype=dtype)
+    state.V = torch.zeros((nz, ny, nx), dtype=dtype)
+    state.levels = vert_disc.compute_levels(nz, 4.0).to(dtype)
+    state.zeta, state.dzeta = vert_disc.compute_zeta_dzeta(state.levels)
+    state.Leg_P = state.Leg_dPdz = None
+    state.vert_weight = vert_disc.define_vertical_weight(nz, 4.0).to(dtype)
+    solve_mod.initialize_iceflow_solver(cfg, state)
+    out = dict(thk=g["thk"], usurf=g["usurf"], arrhenius=g["arrhenius"], slidingco=g["slidingco"],
+               dx=np.array(dx), nbitmax=np.array(nbitmax))
+    for s in range(n_solves):
+        U0 = state.U.detach().clone()
+        Uf, Vf, costs = solve_mod.solve_iceflow(cfg, state, state.U, state.V)
+        solve_mod.update_iceflow_solved(cfg, state) if False else None
+        state.U, state.V = Uf.detach(), Vf.detach()
+        state.COST_Glen = costs[-1].numpy()
+        ub, vb = ice_utils.get_velbar(state.U, state.V, state.vert_weight, "Lagrange")
+        out[f"s{s}_U"] = state.U
+        out[f"s{s}_V"] = state.V
+        out[f"s{s}_ubar"] = ub
+        out[f"s{s}_vbar"] = vb
+        out[f"s{s}_costs"] = torch.stack([c.detach() for c in costs])
+        out[f"s{s}_iterations_after"] = np.array(state.optimizer.iterations)
+    save(f"solver_{name}", out)
+
+
+def transport_cases():
+    rng = np.random.default_rng(7)
+    out = {}
+    ny, nx = 17, 13
+    h = np.maximum(0, rng.normal(50, 60, (ny, nx)))
+    h[:, :2] = 0
+    u = rng.normal(5, 30, (ny, nx))
+    v = rng.normal(-3, 30, (ny, nx))
+    for dtype, tag in [(torch.float32, "f32"), (torch.float64, "f64")]:
+        H, Uu, Vv = (torch.as_tensor(a, dtype=dtype) for a in (h, u, v))
+        out[f"{tag}_h"], out[f"{tag}_u"], out[f"{tag}_v"] = H, Uu, Vv
+        for st in ["godunov", "minmod", "superbee"]:
+            out[f"{tag}_{st}"] = divflux_mod.compute_divflux_slope_limiter(Uu, Vv, H, 50.0, 50.0, 0.7, slope_type=st)
+    # thk.update through the reference process (superbee, smb present)
+    cfg = load_cfg()
+    topg = torch.as_tensor(rng.normal(100, 150, (ny, nx)), dtype=torch.float32)
+    smb = torch.as_tensor(rng.normal(0, 2, (ny, nx)), dtype=torch.float32)
+    state = types.SimpleNamespace(topg=topg, thk=torch.as_tensor(h, dtype=torch.float32), it=3,
+                                  ubar=torch.as_tensor(u, dtype=torch.float32),
+                                  vbar=torch.as_tensor(v, dtype=torch.float32),
+                                  dx=50.0, dt=torch.tensor(0.7), smb=smb)
+    thk_mod.initialize(cfg, state)
+    out["thk_init_usurf"] = state.usurf
+    out["thk_topg"], out["thk_smb"], out["thk_h"] = topg, smb, state.thk
+    thk_mod.update(cfg, state)
+    out["thk_new"], out["thk_usurf"], out["thk_lsurf"], out["thk_divflux"] = state.thk, state.usurf, state.lsurf, state.divflux
+    save("transport", out)
+
+
+def time_case():
+    cfg = load_cfg(**{"time.start": 0.0, "time.end": 3.0, "time.save": 1.0})
+    state = types.SimpleNamespace(dx=100.0, it=0)
+    time_mod.initialize(cfg, state)
+    rng = np.random.default_rng(3)
+    ts, dts = [], []
+    for k in range(12):
+        sc = [80.0, 120.0, 15.0, 300.0][k % 4]
+        state.ubar = torch.as_tensor(rng.normal(0, sc, (6, 5)), dtype=torch.float32)
+        state.vbar = torch.as_tensor(rng.normal(0, sc, (6, 5)), dtype=torch.float32)
+        time_mod.update(cfg, state)
+        ts.append(float(state.t))
+        dts.append(float(state.dt))
+        state.it += 1
+        if not bool(state.continue_run):
+            break
+    save("time", dict(t=np.array(ts, np.float32), dt=np.array(dts, np.float32)))
+
+
+class TinyCNN:
+    """Stand-in for the Keras model object: callable on NHWC input, with
+    ``trainable_variables`` ordered as Keras orders them (kernel, bias per layer)."""
+
+    def __init__(self, cin, nfilt, nlayers, nout, seed, dtype):
+        rng = np.random.default_rng(seed)
+        self.w, self.b = [], []
+        c = cin
+        for _ in range(nlayers):
+            self.w.append(torch.as_tensor(rng.normal(0, np.sqrt(2 / (9 * c)), (3, 3, c, nfilt)), dtype=dtype).requires_grad_(True))
+            self.b.append(torch.as_tensor(rng.normal(0, 0.01, (nfilt,)), dtype=dtype).requires_grad_(True))
+            c = nfilt
+        self.w.append(torch.as_tensor(rng.normal(0, np.sqrt(1 / c), (1, 1, c, nout)) * 20, dtype=dtype).requires_grad_(True))
+        self.b.append(torch.as_tensor(rng.normal(0, 0.01, (nout,)), dtype=dtype).requires_grad_(True))
+
+    @property
+    def trainable_variables(self):
+        out = []
+        for w, b in zip(self.w, self.b):
+            out += [w, b]
+        return out
+
+    def __call__(self, X):
+        x = X.permute(0, 3, 1, 2)
+        for w, b in zip(self.w[:-1], self.b[:-1]):
+            x = torch.nn.functional.leaky_relu(torch.nn.functional.conv2d(x, w.permute(3, 2, 0, 1), b, padding=1), 0.01)
+        return torch.nn.functional.conv2d(x, self.w[-1].permute(3, 2, 0, 1), self.b[-1]).permute(0, 2, 3, 1)
+
+
+def emulator_case():
+    """update_iceflow_emulator (emulate.py:155-281) + update_iceflow_emulated (:116-152)."""
+    nz, ny, nx, dx = 4, 22, 19, 100.0
+    dtype = torch.float64
+    cfg = load_cfg(**{"iceflow.numerics.Nz": nz, "iceflow.emulator.framesizemax": 9,
+                      "iceflow.emulator.nbit": 2, "iceflow.emulator.nbit_init": 3,
+                      "iceflow.emulator.lr": 1e-3, "iceflow.emulator.lr_init": 3e-3,
+                      "iceflow.emulator.warm_up_it": 0, "iceflow.emulator.retrain_freq": 2})
+    g = glacier(ny, nx, dx, 11, dtype)
+    state = types.SimpleNamespace(**{k: g[k] for k in ["thk", "usurf", "arrhenius", "slidingco", "dX", "topg"]})
+    state.levels = vert_disc.compute_levels(nz, 4.0).to(dtype)
+    state.zeta, state.dzeta = vert_disc.compute_zeta_dzeta(state.levels)
+    state.Leg_P = state.Leg_dPdz = None
+    state.vert_weight = vert_disc.define_vertical_weight(nz, 4.0).to(dtype)
+    state.iceflow_model = TinyCNN(5, 6, 2, 2 * nz, 5, dtype)
+    state.opti_retrain = tf.keras.optimizers.legacy.Adam(
+        learning_rate=cfg.processes.iceflow.emulator.lr,
+        epsilon=cfg.processes.iceflow.emulator.optimizer_epsilon,
+        clipnorm=cfg.processes.iceflow.emulator.optimizer_clipnorm)
+    out = dict(thk=g["thk"], usurf=g["usurf"], arrhenius=g["arrhenius"], slidingco=g["slidingco"], dx=np.array(dx))
+    for i, v in enumerate(state.iceflow_model.trainable_variables):
+        out[f"w0_{i}"] = v.detach().clone()
+    for step, it in enumerate([0, 1, 2]):
+        emulate_mod.update_iceflow_emulator(cfg, state, it)
+        for i, v in enumerate(state.iceflow_model.trainable_variables):
+            out[f"w{step + 1}_{i}"] = v.detach().clone()
+        if hasattr(state, "COST_EMULATOR"):
+            out[f"cost{step + 1}"] = torch.stack([torch.as_tensor(c).detach() for c in state.COST_EMULATOR])
+    emulate_mod.update_iceflow_emulated(cfg, state)
+    out["U"], out["V"], out["ubar"], out["vbar"] = state.U, state.V, state.ubar, state.vbar
+    out["opt_iterations"] = np.array(state.opti_retrain.iterations)
+    save("emulator", out)
+
+
+def save(name, d):
+    arrs = {}
+    for k, v in d.items():
+        if isinstance(v, torch.Tensor):
+            v = v.detach().cpu().numpy()
+        arrs[k] = np.asarray(v)
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **arrs)
+    print(f"wrote {path} ({os.path.getsize(path)} B)")
+
+
+if __name__ == "__main__":
+    torch.set_num_threads(1)
+    vert_cases()
+    energy_case("small_f64", 13, 11, 4, 100.0, 1, torch.float64, c_neg=True)
+    energy_case("small_f32", 13, 11, 4, 100.0, 1, torch.float32, c_neg=True)
+    energy_case("nz2_f64", 9, 12, 2, 50.0, 2, torch.float64)
+    energy_case("mid_f32", 40, 30, 10, 100.0, 3, torch.float32)
+    energy_case("mid_f64", 40, 30, 10, 100.0, 3, torch.float64, spacing=1.0)
+    energy_case("nz16_f64", 21, 35, 16, 25.0, 4, torch.float64)
+    solver_case("f64", 20, 16, 5, 100.0, 5, torch.float64, nbitmax=40, n_solves=3)
+    solver_case("f32", 20, 16, 5, 100.0, 5, torch.float32, nbitmax=40, n_solves=2)
+    transport_cases()
+    time_case()
+    emulator_case()

@@ -1,0 +1,130 @@
+"""The oracle against golden vectors produced by the reference's own source
+(tests/golden/make_golden.py).  CPU only."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import iceflow_oracle as O
+
+
+def T(a):
+    return torch.as_tensor(a)
+
+
+def test_vert_disc(golden):
+    g = golden("vert_disc")
+    for nz in [2, 3, 5, 10, 16, 30]:
+        for sp in [1.0, 2.0, 4.0]:
+            k = f"nz{nz}_s{int(sp)}"
+            lv = O.compute_levels(nz, sp)
+            z, dz = O.compute_zeta_dzeta(lv)
+            w = O.define_vertical_weight(nz, sp)[:, 0, 0]
+            np.testing.assert_array_equal(lv.numpy(), g[k + "_levels"])
+            np.testing.assert_array_equal(z.numpy(), g[k + "_zeta"])
+            np.testing.assert_array_equal(dz.numpy(), g[k + "_dzeta"])
+            np.testing.assert_array_equal(w.numpy(), g[k + "_weight"])
+
+
+@pytest.mark.parametrize("case", ["small_f64", "small_f32", "nz2_f64", "mid_f32", "mid_f64", "nz16_f64"])
+def test_energy_and_autodiff_gradient(golden, case):
+    g = golden(f"energy_{case}")
+    f64 = g["U"].dtype == np.float64
+    rtol = 1e-12 if f64 else 2e-6
+    args = [T(g[k]) for k in ["U", "V", "thk", "usurf", "arrhenius", "slidingco"]]
+    dx = float(g["dx"])
+    terms = O.energy_terms(*args, dx, T(g["dzeta"]))
+    for name, t in zip(["shear", "sliding", "gravity"], terms):
+        np.testing.assert_allclose(t[0].numpy(), g[name], rtol=rtol, atol=rtol * np.abs(g[name]).max())
+    cost, means, gU, gV = O.energy_and_grad(*args, dx, T(g["dzeta"]))
+    np.testing.assert_allclose(float(cost), float(g["cost"]), rtol=rtol)
+    for a, b in [(gU, g["gradU"]), (gV, g["gradV"])]:
+        np.testing.assert_allclose(a.numpy(), b, rtol=rtol * 10, atol=rtol * 10 * np.abs(b).max())
+
+
+@pytest.mark.parametrize("case,nsolve", [("f64", 3), ("f32", 2)])
+def test_solver_sequence(golden, case, nsolve):
+    """solve_iceflow called repeatedly on one optimizer: the Adam iteration
+    counter carries over between solves while the moment slots restart."""
+    g = golden(f"solver_{case}")
+    f64 = case == "f64"
+    dt = torch.float64 if f64 else torch.float32
+    thk, usurf, A, c = (T(g[k]) for k in ["thk", "usurf", "arrhenius", "slidingco"])
+    nz = g["s0_U"].shape[0]
+    dzeta = O.compute_zeta_dzeta(O.compute_levels(nz, 4.0).to(dt))[1]
+    vw = O.define_vertical_weight(nz, 4.0).to(dt)
+    opt = O.KerasLegacyAdam(lr=1.0)
+    U = torch.zeros((nz,) + thk.shape, dtype=dt)
+    V = torch.zeros_like(U)
+    for s in range(nsolve):
+        U, V, costs = O.solve_iceflow(U, V, thk, usurf, A, c, float(g["dx"]), dzeta, opt, nbitmax=int(g["nbitmax"]))
+        assert len(costs) == len(g[f"s{s}_costs"])
+        assert opt.iterations == int(g[f"s{s}_iterations_after"])
+        tol = 1e-9 if f64 else 2e-3
+        np.testing.assert_allclose(costs, g[f"s{s}_costs"], rtol=tol)
+        scale = np.abs(g[f"s{s}_U"]).max()
+        np.testing.assert_allclose(U.numpy(), g[f"s{s}_U"], rtol=tol, atol=tol * scale)
+        np.testing.assert_allclose(V.numpy(), g[f"s{s}_V"], rtol=tol, atol=tol * scale)
+        ub, vb = O.get_velbar(U, V, vw)
+        np.testing.assert_allclose(ub.numpy(), g[f"s{s}_ubar"], rtol=tol, atol=tol * scale)
+
+
+def test_divflux_all_limiters(golden):
+    g = golden("transport")
+    for tag in ["f32", "f64"]:
+        h, u, v = T(g[f"{tag}_h"]), T(g[f"{tag}_u"]), T(g[f"{tag}_v"])
+        for st in ["godunov", "minmod", "superbee"]:
+            out = O.compute_divflux_slope_limiter(u, v, h, 50.0, 50.0, 0.7, st)
+            np.testing.assert_array_equal(out.numpy(), g[f"{tag}_{st}"])
+
+
+def test_thk_update(golden):
+    g = golden("transport")
+    lsurf, usurf = O.thk_surfaces(T(g["thk_h"]), T(g["thk_topg"]))
+    np.testing.assert_array_equal(usurf.numpy(), g["thk_init_usurf"])
+    thk, lsurf, usurf, div = O.thk_update(T(g["thk_h"]), T(g["thk_topg"]), T(g["f32_u"]), T(g["f32_v"]),
+                                          T(g["thk_smb"]), 50.0, torch.tensor(0.7))
+    for a, k in [(thk, "thk_new"), (lsurf, "thk_lsurf"), (usurf, "thk_usurf"), (div, "thk_divflux")]:
+        np.testing.assert_array_equal(a.numpy(), g[k])
+
+
+def test_clock(golden):
+    g = golden("time")
+    rng = np.random.default_rng(3)
+    clk = O.Clock(start=0.0, end=3.0, save=1.0)
+    ts, dts = [], []
+    for k in range(12):
+        sc = [80.0, 120.0, 15.0, 300.0][k % 4]
+        ub = T(rng.normal(0, sc, (6, 5)).astype(np.float32))
+        vb = T(rng.normal(0, sc, (6, 5)).astype(np.float32))
+        clk.update(ub, vb, 100.0, k)
+        ts.append(clk.t)
+        dts.append(clk.dt)
+        if not clk.continue_run:
+            break
+    np.testing.assert_allclose(ts, g["t"], rtol=1e-6)
+    np.testing.assert_allclose(dts, g["dt"], rtol=1e-5)
+
+
+def test_emulator_retrain_loop(golden):
+    """Patch split, lr schedule, clipnorm and iteration gating of the
+    emulator retraining (emulate.py:155-281), in float64."""
+    g = golden("emulator")
+    nz = g["U"].shape[0]
+    thk, usurf, A, c = (T(g[k]) for k in ["thk", "usurf", "arrhenius", "slidingco"])
+    X = O.fieldin_to_X([thk, usurf, A, c, torch.full_like(thk, float(g["dx"]))])
+    params = [T(g[f"w0_{i}"]).clone() for i in range(6)]
+    ws, bs = params[0::2], params[1::2]
+    dzeta = O.compute_zeta_dzeta(O.compute_levels(nz, 4.0).to(torch.float64))[1]
+    opt = O.KerasLegacyAdam(lr=1e-3, epsilon=1e-7, clipnorm=1.0)
+    tr = O.EmulatorTraining(retrain_freq=2, lr=1e-3, lr_init=3e-3, warm_up_it=0, nbit_init=3, nbit=2, framesizemax=9)
+    for step, it in enumerate([0, 1, 2]):
+        O.emulator_retrain(ws, bs, opt, X, it, tr, nz, dzeta)
+        for i, p in enumerate(params):
+            np.testing.assert_allclose(p.numpy(), g[f"w{step + 1}_{i}"], rtol=1e-9, atol=1e-12)
+    assert opt.iterations == int(g["opt_iterations"])
+    Y = O.cnn_forward(X, ws, bs)
+    U, V = O.Y_to_UV(Y, nz)
+    mask = (thk > 0)[None]
+    U = torch.where(mask, U[0], 0.0)
+    np.testing.assert_allclose(U.numpy(), g["U"], rtol=1e-9, atol=1e-9 * np.abs(g["U"]).max())
