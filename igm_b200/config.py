@@ -1,0 +1,129 @@
+"""Default parameters under the reference's key names.
+
+The processes read ``cfg.processes.<name>.<key>`` by attribute access, so an
+OmegaConf DictConfig composed by the reference's Hydra setup works as is;
+``default_cfg()`` builds an equivalent plain object for callers without
+Hydra.  Keys and defaults follow igm/conf/processes/iceflow.yaml,
+thk.yaml, time.yaml and smb_simple.yaml.  Keys this implementation adds are
+marked "(igm_b200)".
+"""
+
+from __future__ import annotations
+
+import copy
+from types import SimpleNamespace
+
+DEFAULTS = {
+    "iceflow": {
+        "method": "emulated",
+        "force_max_velbar": 0.0,
+        "physics": {
+            "energy_components": ["shear", "sliding_weertman", "gravity"],
+            "sliding_law": "",
+            "gravity_cst": 9.81,
+            "ice_density": 910.0,
+            "init_slidingco": 0.0464,
+            "init_arrhenius": 78.0,
+            "enhancement_factor": 1.0,
+            "exp_glen": 3.0,
+            "exp_weertman": 3.0,
+            "regu_glen": 1.0e-5,
+            "regu_weertman": 1.0e-10,
+            "dim_arrhenius": 2,
+            "thr_ice_thk": 0.1,
+            "min_sr": 1.0e-20,
+            "max_sr": 1.0e20,
+            "force_negative_gravitational_energy": False,
+            "cf_eswn": [],
+        },
+        "numerics": {"Nz": 10, "vert_spacing": 4.0, "staggered_grid": 1, "vert_basis": "Lagrange"},
+        "solver": {"step_size": 1.0, "nbitmax": 100, "stop_if_no_decrease": True, "optimizer": "Adam",
+                   "lbfgs": False, "save_cost": "", "plot_sol": False},
+        "emulator": {
+            "fieldin": ["thk", "usurf", "arrhenius", "slidingco", "dX"],
+            "retrain_freq": 10,
+            "lr": 2.0e-5,
+            "lr_init": 1.0e-4,
+            "lr_decay": 0.95,
+            "warm_up_it": -10000000000.0,
+            "nbit_init": 1,
+            "nbit": 1,
+            "framesizemax": 750,
+            "split_patch_method": "sequential",
+            "pretrained": True,
+            "name": "",
+            "save_model": False,
+            "exclude_borders": 0,
+            "optimizer": "Adam",
+            "optimizer_clipnorm": 1.0,
+            "optimizer_epsilon": 1.0e-7,
+            "save_cost": "",
+            "output_directory": "",
+            "plot_sol": False,
+            "pertubate": False,
+            # (igm_b200) fixed input scales per fieldin channel (1.0 = raw, as the reference)
+            "input_scales": [1.0, 1.0, 1.0, 1.0, 1.0],
+            # (igm_b200) weight seed for networks built from scratch
+            "seed": 0,
+            "network": {
+                "architecture": "cnn",
+                "multiple_window_size": 0,
+                "activation": "LeakyReLU",
+                "nb_layers": 16,
+                "nb_blocks": 4,
+                "nb_out_filter": 32,
+                "conv_ker_size": 3,
+                "dropout_rate": 0,
+                "weight_initialization": "glorot_uniform",
+                "cnn3d_for_vertical": False,
+            },
+        },
+        # (igm_b200) emulator fallback / judge: every `every` updates the plain
+        # solver is run from the emulated velocities; when the emulated energy
+        # exceeds the solved one by more than `margin` (relative), the solved
+        # velocities replace the emulated ones.  every <= 0 disables it.
+        "fallback": {"every": 0, "margin": 0.02, "nbitmax": 100},
+    },
+    "thk": {"slope_type": "superbee", "ratio_density": 0.910, "default_sealevel": 0.0},
+    "time": {"start": 2000.0, "end": 2100.0, "save": 10.0, "cfl": 0.3, "step_max": 1.0},
+    "smb_simple": {"update_freq": 1.0, "file": "param.txt", "array": []},
+}
+
+
+class Cfg(SimpleNamespace):
+    """Attribute-access config node (the subset of OmegaConf's interface the
+    processes use)."""
+
+    def get(self, key, default=None):
+        return getattr(self, key, default)
+
+    def __contains__(self, key):
+        return hasattr(self, key)
+
+
+def to_cfg(d):
+    if isinstance(d, dict):
+        return Cfg(**{k: to_cfg(v) for k, v in d.items()})
+    return d
+
+
+def _merge(base: dict, over: dict):
+    for k, v in over.items():
+        if isinstance(v, dict) and isinstance(base.get(k), dict):
+            _merge(base[k], v)
+        else:
+            base[k] = v
+
+
+def default_cfg(overrides: dict | None = None, **dotted):
+    """``default_cfg({"iceflow": {"method": "solved"}}, **{"iceflow.numerics.Nz": 5})``"""
+    d = copy.deepcopy(DEFAULTS)
+    if overrides:
+        _merge(d, overrides)
+    for path, val in dotted.items():
+        node = d
+        keys = path.split(".")
+        for k in keys[:-1]:
+            node = node[k]
+        node[keys[-1]] = val
+    return to_cfg({"processes": d})

@@ -1,0 +1,483 @@
+// CUDA-core kernels around the tensor-core convolutions of the CNN emulator:
+// input windows, the 1x1 output head (forward and backward), weight packing
+// for the UMMA B operands, deterministic partial-sum reductions, the mapping
+// of the weight-gradient accumulators to the Keras kernel layout, and the
+// Keras-legacy Adam update with per-variable clip-by-norm.
+//
+// Reference: igm/processes/iceflow/emulate/neural_network.py:9-66 (network),
+// igm/processes/iceflow/utils.py:133-158 (fieldin_to_X / Y_to_UV layouts),
+// emulate.py:116-152 (inference + mask), emulate.py:22-35 and :267 (Adam,
+// epsilon, clipnorm), emulate.py:283-308 (patches).
+//
+// Parameter vector (fp32, Keras order): for each 3x3 layer l: kernel
+// [3][3][cin_l][32] then bias [32]; then the head kernel [1][1][32][nout] and
+// bias [nout].  cin_0 = the number of input fields (5), cin_l = 32 after.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace igm {
+
+constexpr int kF = 32;  // filters
+
+__device__ __forceinline__ float bf_lo(uint32_t w) {
+  return __low2float(*reinterpret_cast<const __nv_bfloat162*>(&w));
+}
+__device__ __forceinline__ float bf_hi(uint32_t w) {
+  return __high2float(*reinterpret_cast<const __nv_bfloat162*>(&w));
+}
+__device__ __forceinline__ uint32_t bf_pack(float lo, float hi) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+
+// offsets (in floats) of the parameters of layer l (0-based; l == L is the head)
+__host__ __device__ inline size_t w_offset(int l, int cin0, int nout) {
+  (void)nout;
+  if (l == 0) return 0;
+  const size_t l0 = (size_t)9 * cin0 * kF + kF;
+  const size_t li = (size_t)9 * kF * kF + kF;
+  return l0 + (size_t)(l - 1) * li;
+}
+__host__ __device__ inline size_t b_offset(int l, int cin0, int nout, int L) {
+  if (l < L) return w_offset(l, cin0, nout) + (size_t)9 * (l == 0 ? cin0 : kF) * kF;
+  return w_offset(L, cin0, nout) + (size_t)kF * nout;
+}
+__host__ __device__ inline size_t param_count(int L, int cin0, int nout) {
+  return w_offset(L, cin0, nout) + (size_t)kF * nout + nout;
+}
+
+// ---------------------------------------------------------------------------
+// weight packing: fp32 Keras layout -> bf16 UMMA B operands
+//  forward  layer l: [tap][k-chunk (ci)][co][8]   (layer 0: 2 k-chunks, zero above cin0)
+//  dgrad    layer l>=1: [tap'][k-chunk (co)][ci][8] with tap' = 8 - tap (flipped)
+// ---------------------------------------------------------------------------
+__global__ void pack_kernel(const float* params, int L, int cin0, int nout, __nv_bfloat16* wf, __nv_bfloat16* wb) {
+  const size_t n0 = (size_t)9 * 2 * kF * 8;   // layer 0, forward
+  const size_t ni = (size_t)9 * 4 * kF * 8;   // other layers, per pack
+  const size_t total_f = n0 + (size_t)(L - 1) * ni;
+  const size_t total = total_f + (size_t)(L - 1) * ni;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    if (i < total_f) {
+      int l, rem;
+      int c8;
+      if (i < n0) { l = 0; rem = (int)i; c8 = 2; }
+      else { l = 1 + (int)((i - n0) / ni); rem = (int)((i - n0) % ni); c8 = 4; }
+      const int e = rem % 8, co = (rem / 8) % kF, kc = (rem / (8 * kF)) % c8, tap = rem / (8 * kF * c8);
+      const int ci = kc * 8 + e;
+      const int cin = l == 0 ? cin0 : kF;
+      const int kh = tap / 3, kw = tap % 3;
+      float v = 0.f;
+      if (ci < cin) v = params[w_offset(l, cin0, nout) + (((size_t)kh * 3 + kw) * cin + ci) * kF + co];
+      wf[i] = __float2bfloat16_rn(v);
+    } else {
+      const size_t j = i - total_f;
+      const int l = 1 + (int)(j / ni);
+      const int rem = (int)(j % ni);
+      const int e = rem % 8, ci = (rem / 8) % kF, kc = (rem / (8 * kF)) % 4, tapp = rem / (8 * kF * 4);
+      const int co = kc * 8 + e;
+      const int tap = 8 - tapp;
+      const int kh = tap / 3, kw = tap % 3;
+      const float v = params[w_offset(l, cin0, nout) + (((size_t)kh * 3 + kw) * kF + ci) * kF + co];
+      wb[j] = __float2bfloat16_rn(v);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// input windows: fields [Ny][Nx] -> X bf16 [B][h][2][w][8] (channels thk, usurf,
+// arrhenius, slidingco, dX, scaled; zero above) and optional fp32 copies of
+// the windowed fields [B][h][w] for the energy
+// ---------------------------------------------------------------------------
+struct InputArgs {
+  int B, h, w, Ny, Nx;
+  const float* f[4];
+  float dx;
+  float scale[5];
+  int y0[IGM_MAX_WINDOWS], x0[IGM_MAX_WINDOWS];
+  __nv_bfloat16* X;
+  float* out[4];
+};
+
+__global__ void input_kernel(const InputArgs a) {
+  const size_t plane = (size_t)a.h * a.w;
+  const size_t total = plane * a.B;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(i / plane);
+    const int rem = (int)(i - (size_t)b * plane);
+    const int y = rem / a.w, x = rem - (rem / a.w) * a.w;
+    const size_t src = (size_t)(a.y0[b] + y) * a.Nx + (a.x0[b] + x);
+    float v[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      v[c] = a.f[c][src];
+      if (a.out[c]) a.out[c][i] = v[c];
+    }
+    uint4 c0, c1;
+    c0.x = bf_pack(v[0] * a.scale[0], v[1] * a.scale[1]);
+    c0.y = bf_pack(v[2] * a.scale[2], v[3] * a.scale[3]);
+    c0.z = bf_pack(a.dx * a.scale[4], 0.f);
+    c0.w = 0u;
+    c1.x = c1.y = c1.z = c1.w = 0u;
+    uint4* X = reinterpret_cast<uint4*>(a.X);
+    const size_t row = ((size_t)b * a.h + y) * 2;
+    X[(row + 0) * a.w + x] = c0;
+    X[(row + 1) * a.w + x] = c1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// head forward: Y = A16 Wh + bh, written as planar U [B][Nz][H][W], V [B][Nz][H][W]
+// (Y_to_UV: channels [0,Nz) are U, [Nz, 2Nz) are V), masked where thk <= 0
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) head_fwd_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act,
+                                                       const float* wh, const float* bh, float* U, float* V,
+                                                       const float* thk_mask) {
+  extern __shared__ float sw[];  // [32][2nz] then bias [2nz]
+  const int nout = 2 * nz;
+  for (int i = threadIdx.x; i < kF * nout; i += blockDim.x) sw[i] = wh[i];
+  for (int i = threadIdx.x; i < nout; i += blockDim.x) sw[kF * nout + i] = bh[i];
+  __syncthreads();
+  const size_t plane = (size_t)H * W;
+  const size_t total = plane * B;
+  const uint4* A = reinterpret_cast<const uint4*>(act);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(i / plane);
+    const size_t rem = i - (size_t)b * plane;
+    const int y = (int)(rem / W), x = (int)(rem - (size_t)y * W);
+    float av[kF];
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+      const uint4 u = A[(((size_t)b * H + y) * 4 + ch) * W + x];
+      const uint32_t wv[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        av[ch * 8 + 2 * e] = bf_lo(wv[e]);
+        av[ch * 8 + 2 * e + 1] = bf_hi(wv[e]);
+      }
+    }
+    const bool keep = thk_mask == nullptr || thk_mask[i] > 0.f;
+    for (int j = 0; j < nout; ++j) {
+      float s = 0.f;
+#pragma unroll
+      for (int ci = 0; ci < kF; ++ci) s = fmaf(av[ci], sw[ci * nout + j], s);
+      s += sw[kF * nout + j];
+      if (!keep) s = 0.f;
+      float* dst = j < nz ? U : V;
+      const int k = j < nz ? j : j - nz;
+      dst[((size_t)b * nz + k) * plane + rem] = s;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// head backward: from dU, dV (planar) and A16:
+//   dPre16 = (dY Wh^T) * LeakyReLU'(A16)  (bf16, row-chunked),
+//   partials per block of dWh [32][nout], dbh [nout] and db16 [32].
+// ---------------------------------------------------------------------------
+constexpr int kHB = 128;  // pixels per chunk
+__global__ void __launch_bounds__(256) head_bwd_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act,
+                                                       const float* wh, const float* dU, const float* dV,
+                                                       float alpha, __nv_bfloat16* dpre, float* partial) {
+  extern __shared__ float sm[];
+  const int nout = 2 * nz;
+  float* sw = sm;                          // [32][nout]
+  float* sA = sw + kF * nout;              // [kHB][33]
+  float* sD = sA + kHB * 33;               // [kHB][nout + 1]
+  float* sP = sD + kHB * (nout + 1);       // [kHB][33]
+  for (int i = threadIdx.x; i < kF * nout; i += blockDim.x) sw[i] = wh[i];
+  const size_t plane = (size_t)H * W;
+  const size_t total = plane * B;
+  const size_t nchunks = (total + kHB - 1) / kHB;
+  const int npairs = kF * nout;
+  float accw[((kF * 2 * IGM_MAX_NZ) + 255) / 256];
+  const int npt = (npairs + 255) / 256;
+  for (int r = 0; r < npt; ++r) accw[r] = 0.f;
+  float accb = 0.f, accd = 0.f;
+  __syncthreads();
+  const uint4* A = reinterpret_cast<const uint4*>(act);
+  uint4* DP = reinterpret_cast<uint4*>(dpre);
+  for (size_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+    const int t = threadIdx.x;
+    if (t < kHB) {
+      const size_t i = chunk * kHB + t;
+      if (i < total) {
+        const int b = (int)(i / plane);
+        const size_t rem = i - (size_t)b * plane;
+        const int y = (int)(rem / W), x = (int)(rem - (size_t)y * W);
+        float av[kF];
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch) {
+          const uint4 u = A[(((size_t)b * H + y) * 4 + ch) * W + x];
+          const uint32_t wv[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            av[ch * 8 + 2 * e] = bf_lo(wv[e]);
+            av[ch * 8 + 2 * e + 1] = bf_hi(wv[e]);
+          }
+        }
+        float da[kF];
+#pragma unroll
+        for (int ci = 0; ci < kF; ++ci) da[ci] = 0.f;
+        for (int j = 0; j < nout; ++j) {
+          const float* src = j < nz ? dU : dV;
+          const int k = j < nz ? j : j - nz;
+          const float g = src[((size_t)b * nz + k) * plane + rem];
+          sD[t * (nout + 1) + j] = g;
+#pragma unroll
+          for (int ci = 0; ci < kF; ++ci) da[ci] = fmaf(g, sw[ci * nout + j], da[ci]);
+        }
+#pragma unroll
+        for (int ci = 0; ci < kF; ++ci) {
+          sA[t * 33 + ci] = av[ci];
+          da[ci] *= av[ci] > 0.f ? 1.f : alpha;
+          sP[t * 33 + ci] = da[ci];
+        }
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch) {
+          uint4 o;
+          o.x = bf_pack(da[ch * 8 + 0], da[ch * 8 + 1]);
+          o.y = bf_pack(da[ch * 8 + 2], da[ch * 8 + 3]);
+          o.z = bf_pack(da[ch * 8 + 4], da[ch * 8 + 5]);
+          o.w = bf_pack(da[ch * 8 + 6], da[ch * 8 + 7]);
+          DP[(((size_t)b * H + y) * 4 + ch) * W + x] = o;
+        }
+      } else {
+        for (int j = 0; j < nout; ++j) sD[t * (nout + 1) + j] = 0.f;
+        for (int ci = 0; ci < kF; ++ci) {
+          sA[t * 33 + ci] = 0.f;
+          sP[t * 33 + ci] = 0.f;
+        }
+      }
+    }
+    __syncthreads();
+    for (int r = 0; r < npt; ++r) {
+      const int pr = threadIdx.x + r * 256;
+      if (pr < npairs) {
+        const int ci = pr / nout, j = pr - ci * nout;
+        float s = 0.f;
+        for (int p = 0; p < kHB; ++p) s = fmaf(sA[p * 33 + ci], sD[p * (nout + 1) + j], s);
+        accw[r] += s;
+      }
+    }
+    if (threadIdx.x < nout) {
+      float s = 0.f;
+      for (int p = 0; p < kHB; ++p) s += sD[p * (nout + 1) + threadIdx.x];
+      accb += s;
+    }
+    if (threadIdx.x >= 128 && threadIdx.x < 128 + kF) {
+      const int ci = threadIdx.x - 128;
+      float s = 0.f;
+      for (int p = 0; p < kHB; ++p) s += sP[p * 33 + ci];
+      accd += s;
+    }
+    __syncthreads();
+  }
+  // partial layout per block: [dWh (32*nout)] [dbh (nout)] [db16 (32)]
+  float* out = partial + (size_t)blockIdx.x * (npairs + nout + kF);
+  for (int r = 0; r < npt; ++r) {
+    const int pr = threadIdx.x + r * 256;
+    if (pr < npairs) out[pr] = accw[r];
+  }
+  if (threadIdx.x < nout) out[npairs + threadIdx.x] = accb;
+  if (threadIdx.x >= 128 && threadIdx.x < 128 + kF) out[npairs + nout + threadIdx.x - 128] = accd;
+}
+
+// ---------------------------------------------------------------------------
+// reductions of per-block partials (fixed order -> deterministic)
+// ---------------------------------------------------------------------------
+__global__ void reduce_partials_kernel(const float* part, int n_parts, int len, int stride, float* out,
+                                       int accumulate) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int p = 0; p < n_parts; ++p) s += part[(size_t)p * stride + i];
+    out[i] = accumulate ? out[i] + s : s;
+  }
+}
+
+// wgrad raw partials [n_parts][dx][128][32] -> Keras kernel gradient [kh][kw][cin][32]
+// where accumulator row m = (kh) * cw + ci, cw = 8 * C/8 of the layer's input tensor.
+__global__ void wgrad_finish_kernel(const float* part, int n_parts, int cin, int cw, float* out) {
+  const int total = 9 * cin * kF;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const int co = i % kF, ci = (i / kF) % cin, tap = i / (kF * cin);
+    const int kh = tap / 3, kw = tap % 3;
+    const int m = kh * cw + ci;
+    float s = 0.f;
+    for (int p = 0; p < n_parts; ++p) s += part[(((size_t)p * 3 + kw) * 128 + m) * kF + co];
+    out[i] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Adam (Keras legacy): per-variable clip_by_norm, then
+//   m += (g - m)(1 - b1); v += (g^2 - v)(1 - b2); x -= lr_t m / (sqrt(v) + eps)
+// ---------------------------------------------------------------------------
+struct AdamVars {
+  int n;
+  size_t off[IGM_MAX_VARS + 1];
+};
+
+__global__ void __launch_bounds__(256) grad_norms_kernel(const float* g, const AdamVars vars, double* norms) {
+  __shared__ double sh[8];
+  const int v = blockIdx.x;
+  double s = 0.0;
+  for (size_t i = vars.off[v] + threadIdx.x; i < vars.off[v + 1]; i += blockDim.x) s += (double)g[i] * g[i];
+  s = block_sum<256>(s, sh, threadIdx.x);
+  if (threadIdx.x == 0) norms[v] = sqrt(s);
+}
+
+__global__ void adam_kernel(float* x, const float* g, float* m, float* v, const AdamVars vars, const double* norms,
+                            float lr_t, float b1, float b2, float eps, float clipnorm) {
+  const size_t total = vars.off[vars.n];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    int k = 0;
+    while (k + 1 < vars.n && i >= vars.off[k + 1]) ++k;
+    float gi = g[i];
+    if (clipnorm > 0.f) {
+      const float nrm = (float)norms[k];
+      gi = gi * clipnorm / (nrm > clipnorm ? nrm : clipnorm);
+    }
+    float mi = m[i], vi = v[i];
+    mi += (gi - mi) * (1.f - b1);
+    vi += (gi * gi - vi) * (1.f - b2);
+    m[i] = mi;
+    v[i] = vi;
+    x[i] -= (mi * lr_t) / (sqrtf(vi) + eps);
+  }
+}
+
+static int grid_for(size_t n, int per = 256) {
+  size_t b = (n + per - 1) / per;
+  if (b > 148 * 8) b = 148 * 8;
+  return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace igm
+
+using namespace igm;
+
+extern "C" size_t igm_cnn_param_count(int nb_layers, int cin, int nout) {
+  if (nb_layers < 1 || cin < 1 || cin > 8 || nout < 1 || nout > 2 * IGM_MAX_NZ) return 0;
+  return param_count(nb_layers, cin, nout);
+}
+
+extern "C" size_t igm_cnn_param_offset(int nb_layers, int cin, int nout, int layer, int bias) {
+  if (layer < 0 || layer > nb_layers) return (size_t)-1;
+  return bias ? b_offset(layer, cin, nout, nb_layers) : w_offset(layer, cin, nout);
+}
+
+extern "C" int igm_cnn_pack_weights(int nb_layers, int cin, int nout, const float* params, void* wpack_fwd,
+                                    void* wpack_bwd, void* stream) {
+  IGM_CHECK_ARG(nb_layers >= 1 && cin >= 1 && cin <= 8 && nout >= 1, IGM_ERR_BAD_SHAPE,
+                "igm_cnn_pack_weights: bad network shape");
+  IGM_CHECK_ARG(params && wpack_fwd && (wpack_bwd || nb_layers == 1), IGM_ERR_BAD_ARGUMENT,
+                "igm_cnn_pack_weights: NULL argument");
+  const size_t total = (size_t)9 * 2 * kF * 8 + (size_t)(nb_layers - 1) * 9 * 4 * kF * 8 * 2;
+  pack_kernel<<<grid_for(total), 256, 0, as_stream(stream)>>>(params, nb_layers, cin, nout,
+                                                              (__nv_bfloat16*)wpack_fwd, (__nv_bfloat16*)wpack_bwd);
+  return launch_status("pack_kernel");
+}
+
+extern "C" int igm_cnn_input(int batch, int h, int w, int ny, int nx, const float* thk, const float* usurf,
+                             const float* arrhenius, const float* slidingco, double dx, const float* scales,
+                             const int* win_y0, const int* win_x0, void* X, float* thk_out, float* usurf_out,
+                             float* arrhenius_out, float* slidingco_out, void* stream) {
+  IGM_CHECK_ARG(batch >= 1 && batch <= IGM_MAX_WINDOWS && h >= 1 && w >= 1, IGM_ERR_BAD_SHAPE,
+                "igm_cnn_input: bad shape (batch must be <= %d)", IGM_MAX_WINDOWS);
+  IGM_CHECK_ARG(thk && usurf && arrhenius && slidingco && scales && win_y0 && win_x0 && X, IGM_ERR_BAD_ARGUMENT,
+                "igm_cnn_input: NULL argument");
+  InputArgs a{};
+  a.B = batch; a.h = h; a.w = w; a.Ny = ny; a.Nx = nx;
+  a.f[0] = thk; a.f[1] = usurf; a.f[2] = arrhenius; a.f[3] = slidingco;
+  a.dx = (float)dx;
+  for (int c = 0; c < 5; ++c) a.scale[c] = scales[c];
+  for (int b = 0; b < batch; ++b) {
+    IGM_CHECK_ARG(win_y0[b] >= 0 && win_x0[b] >= 0 && win_y0[b] + h <= ny && win_x0[b] + w <= nx,
+                  IGM_ERR_BAD_SHAPE, "igm_cnn_input: window %d outside the domain", b);
+    a.y0[b] = win_y0[b];
+    a.x0[b] = win_x0[b];
+  }
+  a.X = (__nv_bfloat16*)X;
+  a.out[0] = thk_out; a.out[1] = usurf_out; a.out[2] = arrhenius_out; a.out[3] = slidingco_out;
+  input_kernel<<<grid_for((size_t)batch * h * w), 256, 0, as_stream(stream)>>>(a);
+  return launch_status("input_kernel");
+}
+
+extern "C" int igm_cnn_head_forward(int batch, int h, int w, int nz, const void* act, const float* head_w,
+                                    const float* head_b, float* U, float* V, const float* thk_mask, void* stream) {
+  IGM_CHECK_ARG(batch >= 1 && h >= 1 && w >= 1 && nz >= 1 && nz <= IGM_MAX_NZ, IGM_ERR_BAD_SHAPE,
+                "igm_cnn_head_forward: bad shape");
+  IGM_CHECK_ARG(act && head_w && head_b && U && V, IGM_ERR_BAD_ARGUMENT, "igm_cnn_head_forward: NULL argument");
+  const size_t smem = (size_t)(kF * 2 * nz + 2 * nz) * sizeof(float);
+  head_fwd_kernel<<<grid_for((size_t)batch * h * w), 256, smem, as_stream(stream)>>>(
+      batch, h, w, nz, (const __nv_bfloat16*)act, head_w, head_b, U, V, thk_mask);
+  return launch_status("head_fwd_kernel");
+}
+
+extern "C" size_t igm_cnn_head_partial_len(int nz) { return (size_t)kF * 2 * nz + 2 * nz + kF; }
+
+extern "C" int igm_cnn_head_backward(int batch, int h, int w, int nz, const void* act, const float* head_w,
+                                     const float* dU, const float* dV, float alpha, void* dpre, float* partials,
+                                     int n_parts, void* stream) {
+  IGM_CHECK_ARG(batch >= 1 && h >= 1 && w >= 1 && nz >= 1 && nz <= IGM_MAX_NZ && n_parts >= 1, IGM_ERR_BAD_SHAPE,
+                "igm_cnn_head_backward: bad shape");
+  IGM_CHECK_ARG(act && head_w && dU && dV && dpre && partials, IGM_ERR_BAD_ARGUMENT,
+                "igm_cnn_head_backward: NULL argument");
+  const int nout = 2 * nz;
+  const size_t smem = (size_t)(kF * nout + kHB * 33 + kHB * (nout + 1) + kHB * 33) * sizeof(float);
+  static size_t configured = 0;
+  if (smem > 48 * 1024 && configured < smem) {
+    cudaError_t e = cudaFuncSetAttribute(head_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+      set_error("head_bwd smem attribute: %s", cudaGetErrorString(e));
+      return IGM_ERR_CUDA;
+    }
+    configured = smem;
+  }
+  head_bwd_kernel<<<n_parts, 256, smem, as_stream(stream)>>>(batch, h, w, nz, (const __nv_bfloat16*)act, head_w, dU,
+                                                            dV, alpha, (__nv_bfloat16*)dpre, partials);
+  return launch_status("head_bwd_kernel");
+}
+
+extern "C" int igm_reduce_partials(const float* partials, int n_parts, int len, int stride, float* out,
+                                   int accumulate, void* stream) {
+  IGM_CHECK_ARG(partials && out && n_parts >= 1 && len >= 0 && stride >= len, IGM_ERR_BAD_ARGUMENT,
+                "igm_reduce_partials: bad argument");
+  if (len == 0) return IGM_OK;
+  reduce_partials_kernel<<<grid_for(len), 256, 0, as_stream(stream)>>>(partials, n_parts, len, stride, out,
+                                                                      accumulate);
+  return launch_status("reduce_partials_kernel");
+}
+
+extern "C" int igm_cnn_wgrad_finish(const float* partials, int n_parts, int cin, int cin_tensor, float* out,
+                                    void* stream) {
+  IGM_CHECK_ARG(partials && out && n_parts >= 1, IGM_ERR_BAD_ARGUMENT, "igm_cnn_wgrad_finish: bad argument");
+  IGM_CHECK_ARG((cin_tensor == 16 || cin_tensor == 32) && cin >= 1 && cin <= cin_tensor, IGM_ERR_BAD_SHAPE,
+                "igm_cnn_wgrad_finish: bad channel counts");
+  wgrad_finish_kernel<<<grid_for((size_t)9 * cin * kF), 256, 0, as_stream(stream)>>>(partials, n_parts, cin,
+                                                                                     cin_tensor, out);
+  return launch_status("wgrad_finish_kernel");
+}
+
+extern "C" int igm_adam_clipnorm(int n_vars, const size_t* var_offsets, float* params, const float* grads,
+                                 float* m, float* v, double* norms, double lr, double beta_1, double beta_2,
+                                 double epsilon, double clipnorm, int64_t iteration, void* stream) {
+  IGM_CHECK_ARG(n_vars >= 1 && n_vars <= IGM_MAX_VARS, IGM_ERR_BAD_ARGUMENT, "igm_adam_clipnorm: 1..%d variables",
+                IGM_MAX_VARS);
+  IGM_CHECK_ARG(var_offsets && params && grads && m && v && norms, IGM_ERR_BAD_ARGUMENT,
+                "igm_adam_clipnorm: NULL argument");
+  AdamVars vars{};
+  vars.n = n_vars;
+  for (int i = 0; i <= n_vars; ++i) vars.off[i] = var_offsets[i];
+  const double t = (double)iteration;
+  const float b1p = powf((float)beta_1, (float)t), b2p = powf((float)beta_2, (float)t);
+  const float lr_t = (float)lr * sqrtf(1.f - b2p) / (1.f - b1p);
+  cudaStream_t st = as_stream(stream);
+  grad_norms_kernel<<<n_vars, 256, 0, st>>>(grads, vars, norms);
+  int rc = launch_status("grad_norms_kernel");
+  if (rc) return rc;
+  adam_kernel<<<grid_for(vars.off[n_vars]), 256, 0, st>>>(params, grads, m, v, vars, norms, lr_t, (float)beta_1,
+                                                         (float)beta_2, (float)epsilon, (float)clipnorm);
+  return launch_status("adam_kernel");
+}

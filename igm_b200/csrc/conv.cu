@@ -1,0 +1,561 @@
+// 3x3 "same" convolutions of the CNN emulator on the 5th-generation tensor
+// cores (tcgen05.mma kind::f16, BF16 operands, FP32 accumulation in TMEM).
+//
+// Reference: igm/processes/iceflow/emulate/neural_network.py:9-66 (Keras
+// Conv2D(3x3, padding="same") + LeakyReLU(0.01)); the backward passes are the
+// data and weight gradients Keras' GradientTape computes for it
+// (emulate.py:252).
+//
+// Activation layout ("row-chunked"): bf16 [B][H][C/8][W][8].  One TMA box
+// {8, 130, C/8, R+2, 1} at (0, x0-1, 0, y0-1, b) lands in shared memory as
+// [row][chunk][pixel][8], which IS the canonical no-swizzle K-major UMMA
+// layout for "pixels x channels" (8-pixel core matrices of 16-byte rows).
+// Out-of-bounds rows/columns are zero-filled by TMA, which implements the
+// zero "same" padding.  Each of the nine taps is then just a shifted
+// descriptor start address: (row + dy) * row_stride + (dx) * 16 bytes.
+//
+// Forward / dgrad kernel (persistent, one CTA per SM, 6 warps):
+//   warp 0  TMA producer (and TMEM allocator),
+//   warp 1  MMA issuer: per tile R rows x 9 taps x C/16 MMAs of M=128 (pixels),
+//           N=32 (output channels), K=16 into R TMEM accumulators,
+//   warps 2-5 epilogue: TMEM -> registers (one pixel per thread), bias +
+//           LeakyReLU (forward) or the LeakyReLU derivative mask of the previous
+//           activation (dgrad, plus the bias-gradient partial sums), bf16 store.
+//   Two input stages and two accumulator sets overlap load, MMA and epilogue.
+// Weight-gradient kernel: D[(input row, ci)][co] += X^T G over the pixels of
+// one output row, with both operands MN-major: M = 128 spans 128/(C/8*8)
+// consecutive input rows x C input channels (row stride = C/8 chunk strides,
+// so the M groups are uniformly strided), one accumulator per horizontal tap.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "tc.cuh"
+
+namespace igm {
+
+constexpr int kTW = 128;        // pixels per tile row (the UMMA M)
+constexpr int kBoxW = kTW + 2;  // with the 1-pixel halo on each side
+constexpr int kCout = 32;       // output channels (the UMMA N)
+constexpr int kConvThreads = 192;
+
+enum ConvEpi { kEpiFwdLeaky = 0, kEpiDgrad = 1 };
+
+struct ConvArgs {
+  int B, H, W;
+  int tiles_w, tiles_h, n_tiles;
+  const __nv_bfloat16* wpack;  // [9][C8_IN][32][8]
+  const float* bias;           // [32] (forward)
+  const __nv_bfloat16* amask;  // dgrad: previous activation [B][H][4][W][8]
+  __nv_bfloat16* out;          // [B][H][4][W][8]
+  float* db_partial;           // dgrad: [gridDim.x][32] or NULL
+  float alpha;
+  int* err;
+};
+
+template <int C8_IN, int R>
+struct ConvGeom {
+  static constexpr uint32_t P = kBoxW * 16;                   // chunk plane stride (bytes)
+  static constexpr uint32_t RS = C8_IN * P;                   // row stride
+  static constexpr uint32_t STAGE = (R + 2) * RS;             // one input stage
+  static constexpr uint32_t WBYTES = 9 * C8_IN * kCout * 16;  // packed weights
+  static constexpr uint32_t OFF_W = 2 * STAGE;
+  static constexpr uint32_t OFF_BAR = OFF_W + WBYTES;
+  static constexpr uint32_t TMEM_COLS = 2 * R * kCout;  // two accumulator sets
+  static constexpr uint32_t SMEM = OFF_BAR + 8 * 8 + 16 + 32 * 4 + 1024;
+};
+
+__device__ __forceinline__ void set_err(int* err, int code) {
+  if (err) atomicExch(err, code);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+
+template <int C8_IN, int R, int EPI>
+__global__ void __launch_bounds__(kConvThreads, 1)
+    conv3x3_kernel(const __grid_constant__ CUtensorMap tmap_in, const ConvArgs a) {
+  using G = ConvGeom<C8_IN, R>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
+  uint64_t* full = bars;         // [2] TMA -> MMA
+  uint64_t* empty = bars + 2;    // [2] MMA -> TMA
+  uint64_t* tfull = bars + 4;    // [2] MMA -> epilogue
+  uint64_t* tempty = bars + 6;   // [2] epilogue -> MMA
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + G::OFF_BAR + 64);
+  float* sbias = reinterpret_cast<float*>(smem + G::OFF_BAR + 80);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  // packed weights -> shared memory, bias, barriers
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(a.wpack);
+    uint4* dst = reinterpret_cast<uint4*>(smem + G::OFF_W);
+    for (int i = threadIdx.x; i < (int)(G::WBYTES / 16); i += kConvThreads) dst[i] = src[i];
+    if (threadIdx.x < kCout) sbias[threadIdx.x] = (EPI == kEpiFwdLeaky && a.bias) ? a.bias[threadIdx.x] : 0.f;
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 2; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+      tc::mbar_init(&tfull[s], 1);
+      tc::mbar_init(&tempty[s], 128);
+    }
+    tc::fence_mbar_init();
+    tc::prefetch_tmap(&tmap_in);
+  }
+  tc::fence_proxy_async_smem();
+  if (warp == 0) {
+    tc::tmem_alloc(tmem_slot, G::TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t sbase = tc::smem_u32(smem);
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
+        const int s = it & 1, use = it >> 1;
+        if (!tc::mbar_wait(&empty[s], (use & 1) ^ 1)) {
+          set_err(a.err, 1);
+          break;
+        }
+        const int txi = t % a.tiles_w, rest = t / a.tiles_w;
+        const int tyi = rest % a.tiles_h, b = rest / a.tiles_h;
+        tc::mbar_expect_tx(&full[s], G::STAGE);
+        tc::tma_load_5d(smem + s * G::STAGE, &tmap_in, 0, txi * kTW - 1, 0, tyi * R - 1, b, &full[s]);
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      constexpr uint32_t idesc = tc::make_idesc_bf16(128, kCout, false, false);
+      for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
+        const int s = it & 1, use = it >> 1, acc = it & 1;
+        if (!tc::mbar_wait(&tempty[acc], (use & 1) ^ 1) || !tc::mbar_wait(&full[s], use & 1)) {
+          set_err(a.err, 2);
+          break;
+        }
+        tc::tc_fence_after();
+        const uint32_t in0 = sbase + s * G::STAGE;
+        const uint32_t w0 = sbase + G::OFF_W;
+#pragma unroll 1
+        for (int r = 0; r < R; ++r) {
+          const uint32_t d = tmem + (uint32_t)((acc * R + r) * kCout);
+#pragma unroll
+          for (int tap = 0; tap < 9; ++tap) {
+            const int dy = tap / 3, dx = tap % 3;
+#pragma unroll
+            for (int ks = 0; ks < C8_IN / 2; ++ks) {
+              const uint32_t aaddr = in0 + (r + dy) * G::RS + dx * 16 + ks * 2 * G::P;
+              const uint32_t baddr = w0 + (tap * C8_IN + ks * 2) * (kCout * 16);
+              tc::mma_bf16(d, tc::make_desc(aaddr, G::P, 128), tc::make_desc(baddr, kCout * 16, 128), idesc,
+                           (tap | ks) != 0);
+            }
+          }
+        }
+        tc::mma_commit(&empty[s]);
+        tc::mma_commit(&tfull[acc]);
+      }
+    }
+  } else {
+    // ---------------- epilogue (warps 2..5) ----------------
+    const int q = warp & 3;           // TMEM lane quarter this warp may access
+    const int p = q * 32 + lane;      // pixel within the tile = TMEM lane
+    float dbacc[kCout];
+#pragma unroll
+    for (int c = 0; c < kCout; ++c) dbacc[c] = 0.f;
+    for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
+      const int use = it >> 1, acc = it & 1;
+      if (!tc::mbar_wait(&tfull[acc], use & 1)) {
+        set_err(a.err, 3);
+        break;
+      }
+      tc::tc_fence_after();
+      const int txi = t % a.tiles_w, rest = t / a.tiles_w;
+      const int tyi = rest % a.tiles_h, b = rest / a.tiles_h;
+      const int x = txi * kTW + p;
+#pragma unroll 1
+      for (int r = 0; r < R; ++r) {
+        uint32_t v[32];
+        tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((acc * R + r) * kCout), v);
+        tc::tmem_wait_ld();
+        const int y = tyi * R + r;
+        if (y < a.H && x < a.W) {
+          const size_t pix = (((size_t)b * a.H + y) * 4) * a.W + x;  // chunk 0 of this pixel, in 8-element units
+          float f[kCout];
+#pragma unroll
+          for (int c = 0; c < kCout; ++c) f[c] = __uint_as_float(v[c]);
+          if (EPI == kEpiFwdLeaky) {
+#pragma unroll
+            for (int c = 0; c < kCout; ++c) {
+              const float z = f[c] + sbias[c];
+              f[c] = z > 0.f ? z : a.alpha * z;
+            }
+          } else {
+            const uint4* am = reinterpret_cast<const uint4*>(a.amask);
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch) {
+              const uint4 mv = am[pix + (size_t)ch * a.W];
+              const uint32_t mw[4] = {mv.x, mv.y, mv.z, mv.w};
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&mw[e]);
+                const float lo = __low2float(h), hi = __high2float(h);
+                const int c = ch * 8 + e * 2;
+                f[c] *= lo > 0.f ? 1.f : a.alpha;
+                f[c + 1] *= hi > 0.f ? 1.f : a.alpha;
+              }
+            }
+#pragma unroll
+            for (int c = 0; c < kCout; ++c) dbacc[c] += f[c];
+          }
+          uint4* o = reinterpret_cast<uint4*>(a.out);
+#pragma unroll
+          for (int ch = 0; ch < 4; ++ch) {
+            uint4 w;
+            w.x = pack_bf16x2(f[ch * 8 + 0], f[ch * 8 + 1]);
+            w.y = pack_bf16x2(f[ch * 8 + 2], f[ch * 8 + 3]);
+            w.z = pack_bf16x2(f[ch * 8 + 4], f[ch * 8 + 5]);
+            w.w = pack_bf16x2(f[ch * 8 + 6], f[ch * 8 + 7]);
+            o[pix + (size_t)ch * a.W] = w;
+          }
+        }
+      }
+      tc::tc_fence_before();
+      tc::mbar_arrive(&tempty[acc]);
+    }
+    if (EPI == kEpiDgrad && a.db_partial) {
+      // deterministic CTA reduction of the bias-gradient partial sums
+#pragma unroll
+      for (int c = 0; c < kCout; ++c) {
+        float v = dbacc[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        dbacc[c] = v;
+      }
+      float* red = reinterpret_cast<float*>(smem + G::OFF_W);  // weights no longer needed after the last MMA
+      // wait until every MMA of this CTA completed before reusing the weight area
+      if (lane == 0) {
+#pragma unroll
+        for (int c = 0; c < kCout; ++c) red[(warp - 2) * kCout + c] = dbacc[c];
+      }
+    }
+  }
+  __syncthreads();
+  if (EPI == kEpiDgrad && a.db_partial && threadIdx.x < kCout) {
+    const float* red = reinterpret_cast<const float*>(smem + G::OFF_W);
+    a.db_partial[(size_t)blockIdx.x * kCout + threadIdx.x] =
+        ((red[0 * kCout + threadIdx.x] + red[1 * kCout + threadIdx.x]) + red[2 * kCout + threadIdx.x]) +
+        red[3 * kCout + threadIdx.x];
+  }
+  if (warp == 0) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem, G::TMEM_COLS);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// weight gradient
+// ---------------------------------------------------------------------------
+struct WgradArgs {
+  int B, H, W;
+  int segs_w, n_items;
+  float* partial;  // [gridDim.x][3][128][32]
+  int* err;
+};
+
+template <int C8_IN>
+struct WgradGeom {
+  static constexpr int NROW = 128 / (C8_IN * 8);         // input rows covered by M = 128
+  static constexpr uint32_t P = kBoxW * 16;              // X chunk plane stride
+  static constexpr uint32_t XBYTES = NROW * C8_IN * P;   // X stage
+  static constexpr uint32_t GP = kTW * 16;               // G chunk plane stride
+  static constexpr uint32_t GBYTES = 4 * GP;             // G stage (32 channels)
+  static constexpr uint32_t STAGE = XBYTES + GBYTES;
+  static constexpr int NST = 3;
+  static constexpr uint32_t OFF_BAR = NST * STAGE;
+  static constexpr uint32_t TMEM_COLS = 128;
+  static constexpr uint32_t SMEM = OFF_BAR + 8 * 8 + 16 + 1024;
+};
+
+template <int C8_IN>
+__global__ void __launch_bounds__(kConvThreads, 1)
+    conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmap_x, const __grid_constant__ CUtensorMap tmap_g,
+                         const WgradArgs a) {
+  using G = WgradGeom<C8_IN>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
+  uint64_t* full = bars;          // [3]
+  uint64_t* empty = bars + 3;     // [3]
+  uint64_t* done = bars + 6;      // [1]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + G::OFF_BAR + 64);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < G::NST; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    tc::mbar_init(done, 1);
+    tc::fence_mbar_init();
+    tc::prefetch_tmap(&tmap_x);
+    tc::prefetch_tmap(&tmap_g);
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tmem_slot, G::TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t sbase = tc::smem_u32(smem);
+  const int my_items = blockIdx.x < a.n_items ? (a.n_items - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int it = 0, t = blockIdx.x; t < a.n_items; t += gridDim.x, ++it) {
+        const int s = it % G::NST, use = it / G::NST;
+        if (!tc::mbar_wait(&empty[s], (use & 1) ^ 1)) {
+          set_err(a.err, 11);
+          break;
+        }
+        const int sx = t % a.segs_w, rest = t / a.segs_w;
+        const int y = rest % a.H, b = rest / a.H;
+        tc::mbar_expect_tx(&full[s], G::STAGE);
+        tc::tma_load_5d(smem + s * G::STAGE, &tmap_x, 0, sx * kTW - 1, 0, y - 1, b, &full[s]);
+        tc::tma_load_5d(smem + s * G::STAGE + G::XBYTES, &tmap_g, 0, sx * kTW, 0, y, b, &full[s]);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = tc::make_idesc_bf16(128, kCout, true, true);
+      for (int it = 0, t = blockIdx.x; t < a.n_items; t += gridDim.x, ++it) {
+        const int s = it % G::NST, use = it / G::NST;
+        if (!tc::mbar_wait(&full[s], use & 1)) {
+          set_err(a.err, 12);
+          break;
+        }
+        tc::tc_fence_after();
+        const uint32_t x0 = sbase + s * G::STAGE;
+        const uint32_t g0 = x0 + G::XBYTES;
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx) {
+#pragma unroll
+          for (int ks = 0; ks < kTW / 16; ++ks) {
+            // A: M = (input row, ci) groups of 8 channels every P bytes; K = pixels, 8-pixel groups 128 B apart
+            const uint64_t ad = tc::make_desc(x0 + dx * 16 + ks * 256, 128, G::P);
+            // B: N = co groups of 8 every GP bytes; K = pixels
+            const uint64_t bd = tc::make_desc(g0 + ks * 256, 128, G::GP);
+            tc::mma_bf16(tmem + dx * kCout, ad, bd, idesc, (it > 0 || ks > 0) ? 1u : 0u);
+          }
+        }
+        tc::mma_commit(&empty[s]);
+      }
+      tc::mma_commit(done);
+    }
+  } else {
+    const int q = warp & 3;
+    const int m = q * 32 + lane;  // accumulator row: (input row slot, ci)
+    bool ok = true;
+    if (my_items > 0) {
+      ok = tc::mbar_wait(done, 0);
+      if (!ok) set_err(a.err, 13);
+      tc::tc_fence_after();
+    }
+#pragma unroll 1
+    for (int dx = 0; dx < 3; ++dx) {
+      uint32_t v[32];
+      tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(dx * kCout), v);
+      tc::tmem_wait_ld();
+      float4* dst = reinterpret_cast<float4*>(a.partial + (((size_t)blockIdx.x * 3 + dx) * 128 + m) * kCout);
+#pragma unroll
+      for (int c = 0; c < kCout; c += 4) {
+        float4 f;
+        const bool z = my_items == 0 || !ok;
+        f.x = z ? 0.f : __uint_as_float(v[c + 0]);
+        f.y = z ? 0.f : __uint_as_float(v[c + 1]);
+        f.z = z ? 0.f : __uint_as_float(v[c + 2]);
+        f.w = z ? 0.f : __uint_as_float(v[c + 3]);
+        dst[c / 4] = f;
+      }
+    }
+    tc::tc_fence_before();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem, G::TMEM_COLS);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+static int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+// cuTensorMapEncodeTiled is resolved through the runtime at first use, so the
+// library does not link the driver library directly (it loads on hosts
+// without a GPU driver; only calls that launch kernels need one).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// bf16 [B][H][c8][W][8] tensor map with box {8, box_w, c8, box_h, 1}.
+static int act_tmap(CUtensorMap* m, const void* base, int B, int H, int W, int c8, int box_w, int box_h) {
+  if (((uintptr_t)base & 15) != 0) {
+    set_error("activation base address must be 16-byte aligned");
+    return IGM_ERR_BAD_ARGUMENT;
+  }
+  cuuint64_t dims[5] = {8, (cuuint64_t)W, (cuuint64_t)c8, (cuuint64_t)H, (cuuint64_t)B};
+  cuuint64_t strides[4] = {16, (cuuint64_t)W * 16, (cuuint64_t)c8 * W * 16, (cuuint64_t)H * c8 * W * 16};
+  cuuint32_t box[5] = {8, (cuuint32_t)box_w, (cuuint32_t)c8, (cuuint32_t)box_h, 1};
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is not available from the CUDA driver");
+    return IGM_ERR_CUDA;
+  }
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(base), dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (CUresult %d)", (int)r);
+    return IGM_ERR_CUDA;
+  }
+  return IGM_OK;
+}
+
+template <typename K>
+static int set_smem(K kernel, uint32_t bytes, bool* done) {
+  if (!*done) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) {
+      set_error("conv smem attribute: %s", cudaGetErrorString(e));
+      return IGM_ERR_CUDA;
+    }
+    *done = true;
+  }
+  return IGM_OK;
+}
+
+constexpr int kRows = 4;
+
+template <int C8_IN, int EPI>
+static int conv_launch(int B, int H, int W, const void* x, const void* wpack, const float* bias, const void* amask,
+                       void* y, float* db_partial, int db_slots, float alpha, int* err, cudaStream_t st) {
+  using G = ConvGeom<C8_IN, kRows>;
+  static bool configured = false;
+  int rc = set_smem(conv3x3_kernel<C8_IN, kRows, EPI>, G::SMEM, &configured);
+  if (rc) return rc;
+  CUtensorMap tm;
+  rc = act_tmap(&tm, x, B, H, W, C8_IN, kBoxW, kRows + 2);
+  if (rc) return rc;
+  ConvArgs a{};
+  a.B = B; a.H = H; a.W = W;
+  a.tiles_w = (W + kTW - 1) / kTW;
+  a.tiles_h = (H + kRows - 1) / kRows;
+  a.n_tiles = B * a.tiles_w * a.tiles_h;
+  a.wpack = (const __nv_bfloat16*)wpack;
+  a.bias = bias;
+  a.amask = (const __nv_bfloat16*)amask;
+  a.out = (__nv_bfloat16*)y;
+  a.alpha = alpha;
+  a.err = err;
+  int grid = a.n_tiles < sm_count() ? a.n_tiles : sm_count();
+  if (db_partial) {
+    if (db_slots < grid) grid = db_slots;
+    a.db_partial = db_partial;
+  }
+  if (grid < 1) grid = 1;
+  conv3x3_kernel<C8_IN, kRows, EPI><<<grid, kConvThreads, G::SMEM, st>>>(tm, a);
+  return launch_status("conv3x3_kernel");
+}
+
+template <int C8_IN>
+static int wgrad_launch(int B, int H, int W, const void* x, const void* g, float* partial, int n_parts, int* err,
+                        cudaStream_t st) {
+  using G = WgradGeom<C8_IN>;
+  static bool configured = false;
+  int rc = set_smem(conv3x3_wgrad_kernel<C8_IN>, G::SMEM, &configured);
+  if (rc) return rc;
+  CUtensorMap tx, tg;
+  rc = act_tmap(&tx, x, B, H, W, C8_IN, kBoxW, G::NROW);
+  if (rc) return rc;
+  rc = act_tmap(&tg, g, B, H, W, 4, kTW, 1);
+  if (rc) return rc;
+  WgradArgs a{};
+  a.B = B; a.H = H; a.W = W;
+  a.segs_w = (W + kTW - 1) / kTW;
+  a.n_items = B * H * a.segs_w;
+  a.partial = partial;
+  a.err = err;
+  conv3x3_wgrad_kernel<C8_IN><<<n_parts, kConvThreads, G::SMEM, st>>>(tx, tg, a);
+  return launch_status("conv3x3_wgrad_kernel");
+}
+
+}  // namespace igm
+
+using namespace igm;
+
+extern "C" int igm_conv3x3(int mode, int batch, int height, int width, int cin, const void* x, const void* wpack,
+                           const float* bias, const void* act_mask, void* y, float* db_partials, int db_slots,
+                           float alpha, int* err, void* stream) {
+  IGM_CHECK_ARG(batch >= 1 && height >= 1 && width >= 1 && batch <= 65535, IGM_ERR_BAD_SHAPE,
+                "igm_conv3x3: bad shape %dx%dx%d", batch, height, width);
+  IGM_CHECK_ARG(cin == 16 || cin == 32, IGM_ERR_UNSUPPORTED, "igm_conv3x3: cin must be 16 or 32 (got %d)", cin);
+  IGM_CHECK_ARG(x && wpack && y, IGM_ERR_BAD_ARGUMENT, "igm_conv3x3: NULL argument");
+  IGM_CHECK_ARG(mode == IGM_CONV_FWD_LEAKY || mode == IGM_CONV_DGRAD, IGM_ERR_BAD_ARGUMENT,
+                "igm_conv3x3: unknown mode %d", mode);
+  IGM_CHECK_ARG(mode != IGM_CONV_DGRAD || act_mask, IGM_ERR_BAD_ARGUMENT, "igm_conv3x3: dgrad needs act_mask");
+  IGM_CHECK_ARG(mode != IGM_CONV_FWD_LEAKY || bias, IGM_ERR_BAD_ARGUMENT, "igm_conv3x3: forward needs bias");
+  cudaStream_t st = as_stream(stream);
+  if (mode == IGM_CONV_FWD_LEAKY) {
+    if (cin == 16)
+      return conv_launch<2, kEpiFwdLeaky>(batch, height, width, x, wpack, bias, nullptr, y, nullptr, 0, alpha, err, st);
+    return conv_launch<4, kEpiFwdLeaky>(batch, height, width, x, wpack, bias, nullptr, y, nullptr, 0, alpha, err, st);
+  }
+  IGM_CHECK_ARG(cin == 32, IGM_ERR_UNSUPPORTED, "igm_conv3x3: dgrad needs cin == 32");
+  return conv_launch<4, kEpiDgrad>(batch, height, width, x, wpack, nullptr, act_mask, y, db_partials, db_slots, alpha,
+                                   err, st);
+}
+
+extern "C" int igm_conv3x3_wgrad(int batch, int height, int width, int cin, const void* x, const void* g,
+                                 float* partials, int n_parts, int* err, void* stream) {
+  IGM_CHECK_ARG(batch >= 1 && height >= 1 && width >= 1, IGM_ERR_BAD_SHAPE, "igm_conv3x3_wgrad: bad shape");
+  IGM_CHECK_ARG(cin == 16 || cin == 32, IGM_ERR_UNSUPPORTED, "igm_conv3x3_wgrad: cin must be 16 or 32");
+  IGM_CHECK_ARG(x && g && partials && n_parts >= 1, IGM_ERR_BAD_ARGUMENT, "igm_conv3x3_wgrad: bad argument");
+  cudaStream_t st = as_stream(stream);
+  if (cin == 16) return wgrad_launch<2>(batch, height, width, x, g, partials, n_parts, err, st);
+  return wgrad_launch<4>(batch, height, width, x, g, partials, n_parts, err, st);
+}
+
+extern "C" int igm_conv_sm_count(void) { return sm_count(); }

@@ -1,0 +1,346 @@
+// 2-D field kernels of the path: velocity reduction (+ mask + CFL max),
+// slope-limited upwind thickness transport, surfaces, ELA mass balance and
+// the CFL time step.  All are HBM-bound elementwise/stencil passes.
+#include "common.cuh"
+
+namespace igm {
+
+// ---------------------------------------------------------------------------
+// velbase / velsurf / velbar (iceflow/utils.py:21-51), optional mask
+// where(thk > 0, U, 0) (solve.py:116-117), and max(|ubar|, |vbar|) (time.py:36-39)
+// ---------------------------------------------------------------------------
+template <typename T>
+struct VelArgs {
+  int batch, nz, ny, nx, mask;
+  T* U;
+  T* V;
+  const T* thk;
+  T w[IGM_MAX_NZ];
+  T* ubar;
+  T* vbar;
+  T* ub0;
+  T* vb0;
+  T* us0;
+  T* vs0;
+  float* velomax;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) velocity_reduce_kernel(const VelArgs<T> a) {
+  const size_t plane = (size_t)a.ny * a.nx;
+  const size_t total = plane * a.batch;
+  float vmax = 0.f;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    const size_t b = idx / plane, p = idx - b * plane;
+    const size_t base = b * a.nz * plane + p;
+    const bool keep = !a.mask || a.thk[idx] > T(0);
+    T su = 0, sv = 0, u0 = 0, v0 = 0, u1 = 0, v1 = 0;
+    for (int k = 0; k < a.nz; ++k) {
+      T u = a.U[base + k * plane], v = a.V[base + k * plane];
+      if (!keep) {
+        u = T(0);
+        v = T(0);
+        a.U[base + k * plane] = u;
+        a.V[base + k * plane] = v;
+      }
+      su += u * a.w[k];
+      sv += v * a.w[k];
+      if (k == 0) { u0 = u; v0 = v; }
+      if (k == a.nz - 1) { u1 = u; v1 = v; }
+    }
+    if (a.ubar) a.ubar[idx] = su;
+    if (a.vbar) a.vbar[idx] = sv;
+    if (a.ub0) a.ub0[idx] = u0;
+    if (a.vb0) a.vb0[idx] = v0;
+    if (a.us0) a.us0[idx] = u1;
+    if (a.vs0) a.vs0[idx] = v1;
+    const float m = fmaxf(fabsf((float)su), fabsf((float)sv));
+    vmax = fmaxf(vmax, m);
+  }
+  if (a.velomax) {
+    for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_down_sync(0xffffffffu, vmax, o));
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(a.velomax, vmax);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// transport (compute_divflux_slope_limiter.py:11-65 + thk.py:36-54)
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T minmod(T a, T b) {
+  const bool pos = a * b > T(0);
+  const T fa = fabs(a), fb = fabs(b);
+  return (fa < fb && pos) ? a : ((fa > fb && pos) ? b : T(0));
+}
+template <typename T>
+__device__ __forceinline__ T maxmod(T a, T b) {
+  const bool pos = a * b > T(0);
+  const T fa = fabs(a), fb = fabs(b);
+  return (fa < fb && pos) ? b : ((fa > fb && pos) ? a : T(0));
+}
+
+template <typename T>
+struct TransportArgs {
+  int ny, nx, slope;
+  T dx, half_dx, dt_host, ratio, sealevel;
+  const float* dt_dev;
+  const T* u;
+  const T* v;
+  const T* h;
+  T* h_out;
+  const T* topg;
+  const T* smb;
+  T* usurf;
+  T* lsurf;
+  T* divflux;
+};
+
+template <typename T>
+__device__ __forceinline__ T limited_slope(T hm, T h0, T hp, T dx, int slope) {
+  // slope of the cell holding h0 from its neighbours hm (left) and hp (right)
+  const T sigp = (hp - h0) / dx, sigm = (h0 - hm) / dx;
+  if (slope == IGM_GODUNOV) return T(0);
+  if (slope == IGM_MINMOD) return minmod(sigm, sigp);
+  return maxmod(minmod(sigp, T(2) * sigm), minmod(sigm, T(2) * sigp));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) transport_kernel(const TransportArgs<T> a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nx = a.nx, ny = a.ny;
+  if (i >= nx || j >= ny) return;
+  const T dt = a.dt_dev ? (T)(*a.dt_dev) : a.dt_host;
+  const T dx = a.dx;
+  auto H = [&](int jj, int ii) -> T {
+    return (jj >= 0 && jj < ny && ii >= 0 && ii < nx) ? a.h[(size_t)jj * nx + ii] : T(0);
+  };
+  // x faces i (west) and i+1 (east) of this node
+  T q[2];
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const int f = i + s;
+    const T uf = f == 0 ? a.u[(size_t)j * nx] : (f == nx ? a.u[(size_t)j * nx + nx - 1]
+                                                         : T(0.5) * (a.u[(size_t)j * nx + f - 1] + a.u[(size_t)j * nx + f]));
+    const T hl = H(j, f - 1), hr = H(j, f);
+    const T sl = limited_slope(H(j, f - 2), hl, hr, dx, a.slope);
+    const T sr = limited_slope(hl, hr, H(j, f + 1), dx, a.slope);
+    const T w = hl + a.half_dx * (T(1) - uf * dt / dx) * sl;
+    const T e = hr - a.half_dx * (T(1) + uf * dt / dx) * sr;
+    q[s] = uf * (uf > T(0) ? w : e);
+  }
+  T r[2];
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const int f = j + s;
+    const T vf = f == 0 ? a.v[i] : (f == ny ? a.v[(size_t)(ny - 1) * nx + i]
+                                            : T(0.5) * (a.v[(size_t)(f - 1) * nx + i] + a.v[(size_t)f * nx + i]));
+    const T hl = H(f - 1, i), hr = H(f, i);
+    const T sl = limited_slope(H(f - 2, i), hl, hr, dx, a.slope);
+    const T sr = limited_slope(hl, hr, H(f + 1, i), dx, a.slope);
+    const T s_ = hl + a.half_dx * (T(1) - vf * dt / dx) * sl;
+    const T n_ = hr - a.half_dx * (T(1) + vf * dt / dx) * sr;
+    r[s] = vf * (vf > T(0) ? s_ : n_);
+  }
+  const T div = (q[1] - q[0]) / dx + (r[1] - r[0]) / dx;
+  const size_t o = (size_t)j * nx + i;
+  const T sm = a.smb ? a.smb[o] : T(0);
+  T hn = a.h[o] + dt * (sm - div);
+  hn = hn > T(0) ? hn : T(0);
+  const T tg = a.topg[o];
+  const T fl = -a.ratio * hn + a.sealevel;
+  const T ls = tg > fl ? tg : fl;
+  a.h_out[o] = hn;
+  a.usurf[o] = ls + hn;
+  if (a.lsurf) a.lsurf[o] = ls;
+  if (a.divflux) a.divflux[o] = div;
+}
+
+template <typename T>
+__global__ void surfaces_kernel(int n, const T* thk, const T* topg, T* lsurf, T* usurf, T ratio, T sealevel) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+    const T h = thk[idx], tg = topg[idx];
+    const T fl = -ratio * h + sealevel;
+    const T ls = tg > fl ? tg : fl;
+    if (lsurf) lsurf[idx] = ls;
+    usurf[idx] = ls + h;
+  }
+}
+
+template <typename T>
+__global__ void smb_kernel(int n, const T* usurf, const T* icemask, T* smb, T gabl, T gacc, T ela, T maxacc) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+    T s = usurf[idx] - ela;
+    s *= s < T(0) ? gabl : gacc;
+    s = s < T(-100) ? T(-100) : (s > maxacc ? maxacc : s);
+    if (icemask && !(s < T(0) || icemask[idx] > T(0.5))) s = T(-10);
+    smb[idx] = s;
+  }
+}
+
+template <typename T>
+__global__ void absmax2_kernel(int n, const T* a, const T* b, float* out) {
+  float m = 0.f;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x)
+    m = fmaxf(m, fmaxf(fabsf((float)a[idx]), fabsf((float)b[idx])));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, m);
+}
+
+__global__ void cfl_dt_kernel(const float* velomax, float* dt, float cfl_dx, float step_max) {
+  const float vm = *velomax;
+  float d = step_max;
+  if (vm > 0.f) {
+    const float c = cfl_dx / vm;
+    d = c < step_max ? c : step_max;
+  }
+  *dt = d;
+}
+
+static int grid1d(size_t n) {
+  size_t b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  return (int)(b < 1 ? 1 : b);
+}
+
+template <typename T>
+static int velocity_t(int batch, int nz, int ny, int nx, void* U, void* V, const void* thk, int mask,
+                      const double* w, void* ubar, void* vbar, void* ub0, void* vb0, void* us0, void* vs0,
+                      float* velomax, cudaStream_t st) {
+  VelArgs<T> a{};
+  a.batch = batch; a.nz = nz; a.ny = ny; a.nx = nx; a.mask = mask;
+  a.U = (T*)U; a.V = (T*)V; a.thk = (const T*)thk;
+  for (int k = 0; k < nz; ++k) a.w[k] = (T)w[k];
+  a.ubar = (T*)ubar; a.vbar = (T*)vbar; a.ub0 = (T*)ub0; a.vb0 = (T*)vb0; a.us0 = (T*)us0; a.vs0 = (T*)vs0;
+  a.velomax = velomax;
+  if (velomax) {
+    cudaError_t e = cudaMemsetAsync(velomax, 0, sizeof(float), st);
+    if (e != cudaSuccess) {
+      set_error("igm_velocity_reduce: %s", cudaGetErrorString(e));
+      return IGM_ERR_CUDA;
+    }
+  }
+  velocity_reduce_kernel<T><<<grid1d((size_t)batch * ny * nx), 256, 0, st>>>(a);
+  return launch_status("velocity_reduce_kernel");
+}
+
+template <typename T>
+static int transport_t(int ny, int nx, double dx, const void* u, const void* v, const void* h, void* h_out,
+                       const void* topg, const void* smb, void* usurf, void* lsurf, void* divflux, double dt,
+                       const float* dt_dev, int slope, double ratio, double sealevel, cudaStream_t st) {
+  TransportArgs<T> a{};
+  a.ny = ny; a.nx = nx; a.slope = slope;
+  a.dx = (T)dx; a.half_dx = (T)(0.5 * dx); a.dt_host = (T)dt; a.ratio = (T)ratio; a.sealevel = (T)sealevel;
+  a.dt_dev = dt_dev;
+  a.u = (const T*)u; a.v = (const T*)v; a.h = (const T*)h; a.h_out = (T*)h_out; a.topg = (const T*)topg;
+  a.smb = (const T*)smb; a.usurf = (T*)usurf; a.lsurf = (T*)lsurf; a.divflux = (T*)divflux;
+  dim3 blk(32, 8), grd((nx + 31) / 32, (ny + 7) / 8);
+  transport_kernel<T><<<grd, blk, 0, st>>>(a);
+  return launch_status("transport_kernel");
+}
+
+}  // namespace igm
+
+using namespace igm;
+
+extern "C" int igm_velocity_reduce(int dtype, int batch, int nz, int ny, int nx, void* U, void* V, const void* thk,
+                                   int mask, const double* vert_weight, void* ubar, void* vbar, void* uvelbase,
+                                   void* vvelbase, void* uvelsurf, void* vvelsurf, float* velomax, void* stream) {
+  IGM_CHECK_ARG(batch >= 1 && nz >= 1 && nz <= IGM_MAX_NZ && ny >= 1 && nx >= 1, IGM_ERR_BAD_SHAPE,
+                "igm_velocity_reduce: bad shape");
+  IGM_CHECK_ARG(U && V && vert_weight && (thk || !mask), IGM_ERR_BAD_ARGUMENT, "igm_velocity_reduce: NULL argument");
+  cudaStream_t st = as_stream(stream);
+  if (dtype == IGM_F32)
+    return velocity_t<float>(batch, nz, ny, nx, U, V, thk, mask, vert_weight, ubar, vbar, uvelbase, vvelbase,
+                             uvelsurf, vvelsurf, velomax, st);
+  if (dtype == IGM_F64)
+    return velocity_t<double>(batch, nz, ny, nx, U, V, thk, mask, vert_weight, ubar, vbar, uvelbase, vvelbase,
+                              uvelsurf, vvelsurf, velomax, st);
+  set_error("igm_velocity_reduce: unknown dtype %d", dtype);
+  return IGM_ERR_BAD_ARGUMENT;
+}
+
+extern "C" int igm_transport_step(int dtype, int ny, int nx, double dx, const void* ubar, const void* vbar,
+                                  const void* thk_in, void* thk_out, const void* topg, const void* smb,
+                                  void* usurf_out, void* lsurf_out, void* divflux_out, double dt,
+                                  const float* dt_device, int slope_type, double ratio_density, double sealevel,
+                                  void* stream) {
+  IGM_CHECK_ARG(ny >= 1 && nx >= 1, IGM_ERR_BAD_SHAPE, "igm_transport_step: bad shape %dx%d", ny, nx);
+  IGM_CHECK_ARG(ubar && vbar && thk_in && thk_out && topg && usurf_out, IGM_ERR_BAD_ARGUMENT,
+                "igm_transport_step: NULL argument");
+  IGM_CHECK_ARG(thk_in != thk_out, IGM_ERR_BAD_ARGUMENT, "igm_transport_step: thk_out must not alias thk_in");
+  IGM_CHECK_ARG(slope_type >= IGM_GODUNOV && slope_type <= IGM_SUPERBEE, IGM_ERR_BAD_ARGUMENT,
+                "igm_transport_step: unknown slope_type %d", slope_type);
+  IGM_CHECK_ARG(dx > 0, IGM_ERR_BAD_ARGUMENT, "igm_transport_step: dx must be positive");
+  cudaStream_t st = as_stream(stream);
+  if (dtype == IGM_F32)
+    return transport_t<float>(ny, nx, dx, ubar, vbar, thk_in, thk_out, topg, smb, usurf_out, lsurf_out, divflux_out,
+                              dt, dt_device, slope_type, ratio_density, sealevel, st);
+  if (dtype == IGM_F64)
+    return transport_t<double>(ny, nx, dx, ubar, vbar, thk_in, thk_out, topg, smb, usurf_out, lsurf_out, divflux_out,
+                               dt, dt_device, slope_type, ratio_density, sealevel, st);
+  set_error("igm_transport_step: unknown dtype %d", dtype);
+  return IGM_ERR_BAD_ARGUMENT;
+}
+
+extern "C" int igm_thk_surfaces(int dtype, int n, const void* thk, const void* topg, void* lsurf, void* usurf,
+                                double ratio_density, double sealevel, void* stream) {
+  IGM_CHECK_ARG(n >= 0 && thk && topg && usurf, IGM_ERR_BAD_ARGUMENT, "igm_thk_surfaces: bad argument");
+  cudaStream_t st = as_stream(stream);
+  if (n == 0) return IGM_OK;
+  if (dtype == IGM_F32)
+    surfaces_kernel<float><<<grid1d(n), 256, 0, st>>>(n, (const float*)thk, (const float*)topg, (float*)lsurf,
+                                                     (float*)usurf, (float)ratio_density, (float)sealevel);
+  else if (dtype == IGM_F64)
+    surfaces_kernel<double><<<grid1d(n), 256, 0, st>>>(n, (const double*)thk, (const double*)topg, (double*)lsurf,
+                                                       (double*)usurf, ratio_density, sealevel);
+  else {
+    set_error("igm_thk_surfaces: unknown dtype %d", dtype);
+    return IGM_ERR_BAD_ARGUMENT;
+  }
+  return launch_status("surfaces_kernel");
+}
+
+extern "C" int igm_smb_simple(int dtype, int n, const void* usurf, const void* icemask, void* smb, double gradabl,
+                              double gradacc, double ela, double maxacc, void* stream) {
+  IGM_CHECK_ARG(n >= 0 && usurf && smb, IGM_ERR_BAD_ARGUMENT, "igm_smb_simple: bad argument");
+  cudaStream_t st = as_stream(stream);
+  if (n == 0) return IGM_OK;
+  if (dtype == IGM_F32)
+    smb_kernel<float><<<grid1d(n), 256, 0, st>>>(n, (const float*)usurf, (const float*)icemask, (float*)smb,
+                                                 (float)gradabl, (float)gradacc, (float)ela, (float)maxacc);
+  else if (dtype == IGM_F64)
+    smb_kernel<double><<<grid1d(n), 256, 0, st>>>(n, (const double*)usurf, (const double*)icemask, (double*)smb,
+                                                  gradabl, gradacc, ela, maxacc);
+  else {
+    set_error("igm_smb_simple: unknown dtype %d", dtype);
+    return IGM_ERR_BAD_ARGUMENT;
+  }
+  return launch_status("smb_kernel");
+}
+
+extern "C" int igm_cfl_dt(const float* velomax, float* dt_out, double cfl, double dx, double step_max, void* stream) {
+  IGM_CHECK_ARG(velomax && dt_out, IGM_ERR_BAD_ARGUMENT, "igm_cfl_dt: NULL argument");
+  cfl_dt_kernel<<<1, 1, 0, as_stream(stream)>>>(velomax, dt_out, (float)(cfl * dx), (float)step_max);
+  return launch_status("cfl_dt_kernel");
+}
+
+extern "C" int igm_absmax2(int dtype, int n, const void* a, const void* b, float* out, void* stream) {
+  IGM_CHECK_ARG(n >= 0 && a && b && out, IGM_ERR_BAD_ARGUMENT, "igm_absmax2: bad argument");
+  cudaStream_t st = as_stream(stream);
+  cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float), st);
+  if (e != cudaSuccess) {
+    set_error("igm_absmax2: %s", cudaGetErrorString(e));
+    return IGM_ERR_CUDA;
+  }
+  if (n == 0) return IGM_OK;
+  if (dtype == IGM_F32)
+    absmax2_kernel<float><<<grid1d(n), 256, 0, st>>>(n, (const float*)a, (const float*)b, out);
+  else if (dtype == IGM_F64)
+    absmax2_kernel<double><<<grid1d(n), 256, 0, st>>>(n, (const double*)a, (const double*)b, out);
+  else {
+    set_error("igm_absmax2: unknown dtype %d", dtype);
+    return IGM_ERR_BAD_ARGUMENT;
+  }
+  return launch_status("absmax2_kernel");
+}

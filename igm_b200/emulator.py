@@ -1,0 +1,254 @@
+"""Emulator side of the iceflow process (igm/processes/iceflow/emulate/emulate.py
+and diagnostic/diagnostic.py), on the device.
+
+* ``update_iceflow_emulated``: one forward pass of the CNN over the whole
+  domain, masked where thk == 0, then velbase / velsurf / velbar
+  (emulate.py:116-152).
+* ``update_iceflow_emulator``: physics-informed retraining by minimising the
+  Blatter-Pattyn energy of the emulated velocities, one Adam step per patch
+  (split_into_patches, emulate.py:155-308), gated by retrain_freq / warm_up_it.
+* ``update_iceflow_diagnostic``: every 10 model years the plain solver is run
+  from the emulated velocities and the L1/L2 velbar misfit is logged
+  (diagnostic.py:34-84).
+* ``update_iceflow_fallback`` (this implementation's addition): every
+  ``fallback.every`` updates the solver judges the emulator; when the emulated
+  energy exceeds the solved one by more than ``fallback.margin`` (relative)
+  the solved velocities replace the emulated ones.
+* ``save_iceflow_model`` / ``load_iceflow_model``: weights, Adam moments and
+  iteration count as ``model.npz`` next to the reference's ``fieldin.dat`` and
+  ``vert_grid.dat`` text files (emulate.py:331-359).  Keras ``.h5`` files are
+  not read (no HDF5 reader in this environment).
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+
+import numpy as np
+import torch
+
+from . import kernels as K
+from . import state as S
+from .cnn import CNN
+from .processes import iceflow as P
+
+
+def _patch_windows(ny, nx, nbmax):
+    """split_into_patches (emulate.py:283-308): sy = ny//nbmax + 1 patches of
+    int(ny/sy) rows, column-major patch order."""
+    sy, sx = ny // nbmax + 1, nx // nbmax + 1
+    ly, lx = int(ny / sy), int(nx / sx)
+    wins = []
+    for i in range(sx):
+        for j in range(sy):
+            wins.append((j * ly, i * lx))
+    return wins, ly, lx
+
+
+class EmulatorOptimizer:
+    """State of ``state.opti_retrain``: the Keras legacy Adam hyper-parameters;
+    the moments and the global iteration count live with the network."""
+
+    def __init__(self, lr, epsilon, clipnorm):
+        self.lr, self.epsilon, self.clipnorm = float(lr), float(epsilon), float(clipnorm)
+
+
+def initialize_iceflow_emulator(cfg, state):
+    """emulate.py:22-114."""
+    ic = cfg.processes.iceflow
+    e = ic.emulator
+    state.opti_retrain = EmulatorOptimizer(e.lr, e.optimizer_epsilon, e.optimizer_clipnorm)
+    net = e.network
+    nb_inputs = len(e.fieldin)
+    if nb_inputs != 5 or list(e.fieldin) != ["thk", "usurf", "arrhenius", "slidingco", "dX"]:
+        raise NotImplementedError(f"emulator fieldin {list(e.fieldin)}: only the default five fields are supported")
+    if net.activation != "LeakyReLU" or net.conv_ker_size != 3 or net.dropout_rate > 0 or net.cnn3d_for_vertical:
+        raise NotImplementedError("only LeakyReLU 3x3 CNNs without dropout are supported")
+    thk = S.get(state, "thk")
+    state.iceflow_model = CNN(nb_layers=int(net.nb_layers), cin=nb_inputs, nout=2 * int(ic.numerics.Nz),
+                              init=net.weight_initialization, seed=int(e.get("seed", 0)),
+                              scales=list(e.get("input_scales", [1.0] * 5)), device=thk.device,
+                              nb_out_filter=int(net.nb_out_filter))
+    loaded = False
+    if e.pretrained and e.name:
+        path = os.path.join(getattr(state, "original_cwd", os.getcwd()), e.name)
+        if os.path.exists(os.path.join(path, "model.npz")):
+            load_iceflow_model(state, path, cfg)
+            loaded = True
+            print("Found pretrained emulator: " + e.name)
+    if not loaded:
+        print("No pretrained emulator, start from scratch.")
+    state.COST_EMULATOR = []
+    state.GRAD_EMULATOR = []
+
+
+def _fields(state):
+    return [S.get(state, f) for f in ("thk", "usurf", "arrhenius", "slidingco")]
+
+
+def update_iceflow_emulated(cfg, state):
+    """emulate.py:116-152."""
+    model: CNN = state.iceflow_model
+    f = _fields(state)
+    ny, nx = f[0].shape
+    buf = model.buffers(1, ny, nx, train=False)
+    model.prepare_input(f, P._dx(state), [(0, 0)], ny, nx, buf)
+    U, V = model.forward(buf, 1, ny, nx, thk_mask=f[0])
+    state.U, state.V = U[0], V[0]
+    if cfg.processes.iceflow.force_max_velbar > 0:
+        raise NotImplementedError("force_max_velbar > 0 is not supported")
+    P.set_derived_velocities(cfg, state, mask=False)
+    S.sync_host(state)
+
+
+def train_step(model: CNN, fields_full, dx, windows, h, w, dzeta, phys, lr, opt: EmulatorOptimizer):
+    """One physics-informed Adam step on a batch of windows: forward, energy
+    and adjoint on the windowed fields, backward, Adam.  Returns the device
+    energy sums [3] (divide by B (h-1)(w-1) for COST)."""
+    B = len(windows)
+    buf = model.buffers(B, h, w, train=True)
+    model.prepare_input(fields_full, dx, windows, h, w, buf)
+    U, V = model.forward(buf, B, h, w, keep_acts=True)
+    count = B * (h - 1) * (w - 1)
+    terms, dU, dV = K.energy(U, V, *buf["fields"], dx, dzeta, phys, grad=True, grad_scale=1.0 / count)
+    model.backward(buf, B, h, w, dU, dV)
+    model.adam_step(lr, epsilon=opt.epsilon, clipnorm=opt.clipnorm)
+    return terms
+
+
+def update_iceflow_emulator(cfg, state, it, pertubate=False):
+    """emulate.py:155-281."""
+    e = cfg.processes.iceflow.emulator
+    run_it = e.retrain_freq > 0 and (it % e.retrain_freq == 0)
+    warm_up = int(it <= e.warm_up_it)
+    if not (warm_up or run_it):
+        return
+    if pertubate:
+        raise NotImplementedError("emulator.pertubate is not supported")
+    model: CNN = state.iceflow_model
+    f = _fields(state)
+    ny, nx = f[0].shape
+    wins, ly, lx = _patch_windows(ny, nx, int(e.framesizemax))
+    nbit, lr = (int(e.nbit_init), float(e.lr_init)) if warm_up else (int(e.nbit), float(e.lr))
+    phys = P.physics(cfg)
+    dx = P._dx(state)
+    state.COST_EMULATOR = []
+    state.GRAD_EMULATOR = []
+    parallel = e.split_patch_method == "parrallel"
+    for _ in range(nbit):
+        sums = []
+        if parallel:
+            sums.append(train_step(model, f, dx, wins, ly, lx, state.dzeta, phys, lr, state.opti_retrain))
+        else:
+            for i, win in enumerate(wins):
+                lr_i = lr * (e.lr_decay ** (i / 1000)) if e.lr_decay < 1 else lr
+                sums.append(train_step(model, f, dx, [win], ly, lx, state.dzeta, phys, lr_i, state.opti_retrain))
+        count = (ly - 1) * (lx - 1) * (len(wins) if parallel else 1)
+        state.COST_EMULATOR.append(float(torch.stack(sums).sum(1).sum().item()) / count)
+    model.check_errors()
+    if len(e.save_cost) > 0:
+        np.savetxt(e.save_cost + "-" + str(it) + ".dat", np.array(state.COST_EMULATOR), fmt="%5.10f")
+
+
+def initialize_iceflow_diagnostic(cfg, state):
+    """diagnostic.py:16-31."""
+    initialize_iceflow_emulator(cfg, state)
+    P.initialize_iceflow_solver(cfg, state)
+    state.diagno = []
+    state.tlast_diagno = -(10 ** 10)
+
+
+def _velbar_misfit(state, dU, dV, thk):
+    """computemisfit (diagnostic.py:74-84): L1 and L2 of the velbar difference where thk > 1."""
+    w = np.asarray(state.vert_weight, np.float64)
+    ub = (dU.double().cpu().numpy() * w).sum(0)
+    vb = (dV.double().cpu().numpy() * w).sum(0)
+    vel = np.stack([ub, vb])
+    ma = np.broadcast_to((thk.cpu().numpy() > 1)[None], vel.shape).astype(np.float64)
+    n = ma.sum()
+    if n == 0:
+        return 0.0, 0.0
+    return float((ma * np.abs(vel)).sum() / n), float(np.sqrt((ma * vel ** 2).sum() / n))
+
+
+def update_iceflow_diagnostic(cfg, state):
+    """diagnostic.py:34-71."""
+    t = float(state.t)
+    if (t - state.tlast_diagno) >= 10:
+        import time as _t
+        t0 = _t.time()
+        U, V, costs = P.solve_iceflow(cfg, state, state.U, state.V)
+        l1, l2 = _velbar_misfit(state, state.U - U, state.V - V, S.get(state, "thk"))
+        vol = float(S.get(state, "thk").double().sum().item()) * (P._dx(state) ** 2) / 1e9
+        cost_em = state.COST_EMULATOR[-1] if state.COST_EMULATOR else float("nan")
+        state.diagno.append([t, l1, l2, float(costs[-1]), cost_em, len(costs), len(state.COST_EMULATOR), vol])
+        np.savetxt("errors_diagno.txt", np.stack(state.diagno), delimiter=",", fmt="%10.3f",
+                   header="time,l1,l2,COST_Glen,COST_Emulator,nb_it_solve,nb_it_emul,vol", comments="")
+        state.tlast_diagno = t
+        state.diagno_time_solve = _t.time() - t0
+
+
+def update_iceflow_fallback(cfg, state):
+    """Solver as judge and fallback of the emulator (see module docstring)."""
+    fb = cfg.processes.iceflow.fallback
+    n = state.__dict__.setdefault("_igm_fallback_counter", 0)
+    state._igm_fallback_counter = n + 1
+    if n % int(fb.every) != 0:
+        return
+    f = _fields(state)
+    dx = P._dx(state)
+    phys = P.physics(cfg)
+    e_em = float(K.energy(state.U, state.V, *f, dx, state.dzeta, phys)[0].sum().item())
+    U, V, costs = state.iceflow_solver.solve(state.U, state.V, *f, dx, state.dzeta, nbitmax=int(fb.nbitmax),
+                                             phys=phys, relative_min_delta=0.0002, patience=10)
+    e_sv = float(K.energy(U, V, *f, dx, state.dzeta, phys)[0].sum().item())
+    ny, nx = f[0].shape
+    ns = (ny - 1) * (nx - 1)
+    e_em, e_sv = e_em / ns, e_sv / ns
+    du = torch.cat([(state.U - U).reshape(-1), (state.V - V).reshape(-1)])
+    ref = torch.cat([U.reshape(-1), V.reshape(-1)])
+    rel = float(torch.linalg.vector_norm(du.double()) / torch.linalg.vector_norm(ref.double()).clamp_min(1e-30))
+    fallback = e_em > e_sv + float(fb.margin) * abs(e_sv)
+    log = state.__dict__.setdefault("fallback_log", [])
+    log.append(dict(t=float(state.t), it=int(state.it), e_emulated=e_em, e_solved=e_sv, vel_rel_l2=rel,
+                    fallback=bool(fallback), solver_iterations=len(costs)))
+    if fallback:
+        state.U, state.V = U, V
+        P.set_derived_velocities(cfg, state, mask=False)
+        S.sync_host(state)
+
+
+def save_iceflow_model(cfg, state, directory="iceflow-model"):
+    """emulate.py:331-359, with model.npz in place of model.h5."""
+    if os.path.exists(directory):
+        shutil.rmtree(directory)
+    os.mkdir(directory)
+    m: CNN = state.iceflow_model
+    np.savez(os.path.join(directory, "model.npz"), params=m.params.cpu().numpy(), adam_m=m.m.cpu().numpy(),
+             adam_v=m.v.cpu().numpy(), iterations=np.array(m.opt_iterations), nb_layers=np.array(m.L),
+             nout=np.array(m.nout), cin=np.array(m.cin), scales=m.scales)
+    with open(os.path.join(directory, "fieldin.dat"), "w") as fid:
+        for key in cfg.processes.iceflow.emulator.fieldin:
+            fid.write("%s \n" % key)
+    with open(os.path.join(directory, "vert_grid.dat"), "w") as fid:
+        fid.write("%4.0f  %s \n" % (cfg.processes.iceflow.numerics.Nz, "# number of vertical grid point (Nz)"))
+        fid.write("%2.2f  %s \n" % (cfg.processes.iceflow.numerics.vert_spacing,
+                                    "# param for vertical spacing (vert_spacing)"))
+
+
+def load_iceflow_model(state, directory, cfg=None):
+    d = np.load(os.path.join(directory, "model.npz"))
+    m: CNN = state.iceflow_model
+    if int(d["nb_layers"]) != m.L or int(d["nout"]) != m.nout or int(d["cin"]) != m.cin:
+        raise ValueError("saved emulator has a different architecture")
+    m.set_params(d["params"])
+    m.m.copy_(torch.as_tensor(d["adam_m"]))
+    m.v.copy_(torch.as_tensor(d["adam_v"]))
+    m.opt_iterations = int(d["iterations"])
+    m.scales = np.asarray(d["scales"], np.float32)
+    fin = os.path.join(directory, "fieldin.dat")
+    if cfg is not None and os.path.exists(fin):
+        with open(fin) as f:
+            names = [ln.split()[0] for ln in f if ln.strip()]
+        assert list(cfg.processes.iceflow.emulator.fieldin) == names

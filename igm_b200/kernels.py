@@ -1,0 +1,137 @@
+"""Typed host wrappers over the C ABI.  Torch tensors are device buffers only:
+every computation below is a libigmb200 kernel."""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+class Workspace:
+    """Zero-filled scratch for the reducing kernels (they leave it zeroed).
+
+    One per device/stream; grown on demand.  Calls that share it must be
+    ordered on one stream."""
+
+    def __init__(self):
+        self.buf = None
+
+    def get(self, grid: L.Grid, device) -> tuple[int, int]:
+        need = int(L.lib().igm_workspace_size(C.byref(grid)))
+        if need == 0:
+            L.check(1, f"igm_workspace_size rejected grid {grid.batch}x{grid.nz}x{grid.ny}x{grid.nx}: "
+                       + L.lib().igm_last_error().decode())
+        if self.buf is None or self.buf.numel() < need or self.buf.device != torch.device(device):
+            self.buf = torch.zeros(max(need, 1 << 16), dtype=torch.uint8, device=device)
+        return self.buf.data_ptr(), self.buf.numel()
+
+
+_WS: dict = {}
+
+
+def workspace(device) -> Workspace:
+    key = str(torch.device(device))
+    if key not in _WS:
+        _WS[key] = Workspace()
+    return _WS[key]
+
+
+def fields_struct(thk, usurf, arrhenius, slidingco) -> L.Fields:
+    f = L.Fields()
+    f.thk, f.usurf, f.arrhenius, f.slidingco = (L.ptr(t) for t in (thk, usurf, arrhenius, slidingco))
+    return f
+
+
+def energy(U, V, thk, usurf, arrhenius, slidingco, dx, dzeta, phys=None, grad=False, grad_scale=1.0,
+           terms_out=None):
+    """Energy sums (device float64 [3]: shear, sliding, gravity) and optionally
+    grad_scale * d(sum)/d(U,V).  U, V: [B, Nz, Ny, Nx] or [Nz, Ny, Nx]."""
+    squeeze = U.dim() == 3
+    if squeeze:
+        U, V = U[None], V[None]
+        thk, usurf, arrhenius, slidingco = (t[None] for t in (thk, usurf, arrhenius, slidingco))
+    B, nz, ny, nx = U.shape
+    g = L.make_grid(B, nz, ny, nx, dx, dzeta)
+    ph = phys if isinstance(phys, L.Physics) else L.make_physics(phys)
+    terms = terms_out if terms_out is not None else torch.empty(3, dtype=torch.float64, device=U.device)
+    dU = torch.empty_like(U) if grad else None
+    dV = torch.empty_like(V) if grad else None
+    wp, wn = workspace(U.device).get(g, U.device)
+    f = fields_struct(thk, usurf, arrhenius, slidingco)
+    rc = L.lib().igm_energy(L.dtype_code(U.dtype), C.byref(g), C.byref(ph), C.byref(f), L.ptr(U), L.ptr(V),
+                            L.ptr(dU), L.ptr(dV), float(grad_scale), L.ptr(terms), wp, wn, L.stream_ptr())
+    L.check(rc, "igm_energy")
+    if squeeze and grad:
+        dU, dV = dU[0], dV[0]
+    return terms, dU, dV
+
+
+def velocity_reduce(U, V, thk, vert_weight, mask=True, want_velomax=True):
+    """Masks U, V in place (where thk <= 0) and returns
+    (ubar, vbar, uvelbase, vvelbase, uvelsurf, vvelsurf, velomax[1] float32)."""
+    squeeze = U.dim() == 3
+    if squeeze:
+        U4, V4, th = U[None], V[None], thk[None]
+    else:
+        U4, V4, th = U, V, thk
+    B, nz, ny, nx = U4.shape
+    outs = [torch.empty((B, ny, nx), dtype=U.dtype, device=U.device) for _ in range(6)]
+    vm = torch.empty(1, dtype=torch.float32, device=U.device) if want_velomax else None
+    w = (C.c_double * nz)(*[float(x) for x in np.asarray(vert_weight, dtype=np.float64).reshape(-1)[:nz]])
+    rc = L.lib().igm_velocity_reduce(L.dtype_code(U.dtype), B, nz, ny, nx, L.ptr(U4), L.ptr(V4), L.ptr(th),
+                                     int(bool(mask)), w, *[L.ptr(o) for o in outs], L.ptr(vm), L.stream_ptr())
+    L.check(rc, "igm_velocity_reduce")
+    if squeeze:
+        outs = [o[0] for o in outs]
+    return (*outs, vm)
+
+
+def transport_step(ubar, vbar, thk, topg, smb, dx, dt, slope_type="superbee", ratio_density=0.910, sealevel=0.0,
+                   want_lsurf=True, want_divflux=True, dt_device=None):
+    """Returns (thk_new, usurf, lsurf, divflux) (the last two may be None)."""
+    ny, nx = thk.shape
+    thk_new = torch.empty_like(thk)
+    usurf = torch.empty_like(thk)
+    lsurf = torch.empty_like(thk) if want_lsurf else None
+    div = torch.empty_like(thk) if want_divflux else None
+    rc = L.lib().igm_transport_step(L.dtype_code(thk.dtype), ny, nx, float(dx), L.ptr(ubar), L.ptr(vbar), L.ptr(thk),
+                                    L.ptr(thk_new), L.ptr(topg), L.ptr(smb), L.ptr(usurf), L.ptr(lsurf), L.ptr(div),
+                                    float(dt), L.ptr(dt_device), L.SLOPE[slope_type], float(ratio_density),
+                                    float(sealevel), L.stream_ptr())
+    L.check(rc, "igm_transport_step")
+    return thk_new, usurf, lsurf, div
+
+
+def surfaces(thk, topg, ratio_density=0.910, sealevel=0.0):
+    lsurf = torch.empty_like(thk)
+    usurf = torch.empty_like(thk)
+    rc = L.lib().igm_thk_surfaces(L.dtype_code(thk.dtype), thk.numel(), L.ptr(thk), L.ptr(topg), L.ptr(lsurf),
+                                  L.ptr(usurf), float(ratio_density), float(sealevel), L.stream_ptr())
+    L.check(rc, "igm_thk_surfaces")
+    return lsurf, usurf
+
+
+def smb_simple(usurf, gradabl, gradacc, ela, maxacc, icemask=None, out=None):
+    smb = out if out is not None else torch.empty_like(usurf)
+    rc = L.lib().igm_smb_simple(L.dtype_code(usurf.dtype), usurf.numel(), L.ptr(usurf), L.ptr(icemask), L.ptr(smb),
+                                float(gradabl), float(gradacc), float(ela), float(maxacc), L.stream_ptr())
+    L.check(rc, "igm_smb_simple")
+    return smb
+
+
+def cfl_dt(velomax, cfl, dx, step_max, out=None):
+    dt = out if out is not None else torch.empty(1, dtype=torch.float32, device=velomax.device)
+    rc = L.lib().igm_cfl_dt(L.ptr(velomax), L.ptr(dt), float(cfl), float(dx), float(step_max), L.stream_ptr())
+    L.check(rc, "igm_cfl_dt")
+    return dt
+
+
+def absmax2(a, b, out=None):
+    vm = out if out is not None else torch.empty(1, dtype=torch.float32, device=a.device)
+    rc = L.lib().igm_absmax2(L.dtype_code(a.dtype), a.numel(), L.ptr(a), L.ptr(b), L.ptr(vm), L.stream_ptr())
+    L.check(rc, "igm_absmax2")
+    return vm

@@ -1,0 +1,85 @@
+"""The shared state bag and its residency.
+
+``State`` mirrors igm.common.State (igm/common/core/src.py:19-20): a plain
+attribute bag.  The processes accept two residencies:
+
+* device-resident (the fast path): 2-D/3-D fields are torch CUDA tensors;
+  processes rebind attributes to new tensors, as the reference rebinds TF
+  tensors;
+* host-resident: ``state.thk`` is a numpy array.  Each process then copies
+  the fields it reads to the device (through pinned staging buffers) and
+  writes the fields it produces back into pinned numpy arrays on the state.
+  This is what a host-side caller of the plugin pays per step.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+
+class State:
+    pass
+
+
+def is_host(state) -> bool:
+    return isinstance(getattr(state, "thk", None), np.ndarray)
+
+
+def device(state):
+    d = getattr(state, "device", None)
+    if d is not None:
+        return torch.device(d)
+    t = getattr(state, "thk", None)
+    if isinstance(t, torch.Tensor) and t.is_cuda:
+        return t.device
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _pinned(state, name, shape, dtype):
+    cache = state.__dict__.setdefault("_igm_pinned", {})
+    key = (name, tuple(shape), dtype)
+    buf = cache.get(key)
+    if buf is None:
+        buf = torch.empty(shape, dtype=dtype, pin_memory=True)
+        cache[key] = buf
+    return buf
+
+
+def get(state, name, dtype=torch.float32):
+    """Field ``name`` as a device tensor of ``dtype``."""
+    v = getattr(state, name)
+    dev = device(state)
+    if isinstance(v, torch.Tensor):
+        if v.is_cuda:
+            return v if v.dtype == dtype else v.to(dtype)
+        src = v
+    else:
+        src = None
+        arr = np.asarray(v)
+        pins = state.__dict__.get("_igm_pinned_views", {})
+        t = pins.get(id(v))
+        if t is not None and t.numpy() is not None and t.data_ptr() == arr.__array_interface__["data"][0]:
+            src = t
+        if src is None:
+            src = _pinned(state, "in:" + name, arr.shape, torch.from_numpy(np.empty(0, arr.dtype)).dtype)
+            src.numpy()[...] = arr
+    return src.to(dev, non_blocking=True).to(dtype)
+
+
+def put(state, name, tensor):
+    """Bind ``tensor`` (device) to ``state.name`` in the state's residency."""
+    if not is_host(state):
+        setattr(state, name, tensor)
+        return
+    host = _pinned(state, "out:" + name, tensor.shape, tensor.dtype)
+    host.copy_(tensor, non_blocking=True)
+    arr = host.numpy()
+    state.__dict__.setdefault("_igm_pinned_views", {})[id(arr)] = host
+    setattr(state, name, arr)
+
+
+def sync_host(state):
+    """Completes the device->host copies of a host-resident state."""
+    if is_host(state):
+        torch.cuda.current_stream().synchronize()

@@ -1,0 +1,314 @@
+/*
+ * igm_b200.h - C ABI of libigmb200.so, the B200 (sm_100a) implementation of
+ * IGM's iceflow process and the thk transport step it drives.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (igm_status); 0 is success.
+ *    igm_status_string() names a code, igm_last_error() returns the detail
+ *    of the most recent failure on the calling thread.
+ *  - All array arguments are DEVICE pointers (cudaMalloc'd or torch CUDA
+ *    storage) unless the comment says "host".  `stream` is a cudaStream_t
+ *    passed as void* (NULL = legacy default stream).  Every call is
+ *    asynchronous with respect to the host.
+ *  - dtype selects the arithmetic: IGM_F32 (the product path) or IGM_F64
+ *    (the double-precision judge used to measure the FP32 error).
+ *  - 2-D fields are [batch][ny][nx], 3-D velocity fields are
+ *    [batch][nz][ny][nx], C order (x fastest), as the reference stores
+ *    state.U (igm/processes/iceflow/utils.py:31-32).
+ *  - Scratch: calls that reduce over the grid take a caller-owned
+ *    workspace of igm_workspace_size() bytes.  It must be zero-filled once
+ *    before its first use; every kernel leaves it zeroed again.  Calls that
+ *    share one workspace must be ordered (same stream).
+ *
+ * Reference paths below are relative to the IGM 3.0.0 source tree.
+ */
+#ifndef IGM_B200_H
+#define IGM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define IGM_API __attribute__((visibility("default")))
+#else
+#define IGM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IGM_MAX_NZ 64
+#define IGM_MAX_WINDOWS 64 /* patches per emulator batch */
+#define IGM_MAX_VARS 80    /* trainable tensors handled by one Adam call */
+
+typedef enum igm_status {
+  IGM_OK = 0,
+  IGM_ERR_BAD_SHAPE = 1,
+  IGM_ERR_BAD_ARGUMENT = 2,
+  IGM_ERR_NAN_DETECTED = 3,
+  IGM_ERR_NOT_CONVERGED = 4,
+  IGM_ERR_CUDA = 5,
+  IGM_ERR_UNSUPPORTED = 6,
+  IGM_ERR_WORKSPACE = 7
+} igm_status;
+
+typedef enum igm_dtype { IGM_F32 = 0, IGM_F64 = 1 } igm_dtype;
+
+typedef enum igm_slope_type { IGM_GODUNOV = 0, IGM_MINMOD = 1, IGM_SUPERBEE = 2 } igm_slope_type;
+
+typedef enum igm_conv_mode {
+  IGM_CONV_FWD_LEAKY = 0, /* y = LeakyReLU(conv3x3(x) + bias) */
+  IGM_CONV_DGRAD = 1      /* y = conv3x3_flipped(x) * LeakyReLU'(act_mask) (+ bias-gradient partials) */
+} igm_conv_mode;
+
+/* cfg.processes.iceflow.physics.* (igm/conf/processes/iceflow.yaml:4-21) */
+typedef struct igm_physics {
+  double exp_glen;       /* n */
+  double exp_weertman;   /* m */
+  double regu_glen;
+  double regu_weertman;
+  double thr_ice_thk;
+  double min_sr;
+  double max_sr;
+  double ice_density;
+  double gravity_cst;
+  int32_t force_negative_gravitational_energy;
+  int32_t reserved;
+} igm_physics;
+
+/* Grid and vertical discretisation.  dzeta[0..nz-2] are the layer weights of
+ * compute_zeta_dzeta (igm/processes/iceflow/vert_disc.py:27-35); with nz == 1
+ * dzeta[0] = 1.  dx is the uniform spacing dX (m). */
+typedef struct igm_grid {
+  int32_t batch;
+  int32_t nz;
+  int32_t ny;
+  int32_t nx;
+  double dx;
+  double dzeta[IGM_MAX_NZ];
+} igm_grid;
+
+/* The 2-D inputs of the energy (cfg.processes.iceflow.emulator.fieldin minus
+ * dX), each [batch][ny][nx] of the call's dtype. */
+typedef struct igm_fields {
+  const void* thk;
+  const void* usurf;
+  const void* arrhenius;
+  const void* slidingco;
+} igm_fields;
+
+/* Keras legacy Adam hyper-parameters (solve.py:11-20 uses the defaults with
+ * learning_rate = solver.step_size). */
+typedef struct igm_adam {
+  double lr;
+  double beta_1;
+  double beta_2;
+  double epsilon;
+} igm_adam;
+
+/* EarlyStopping(relative_min_delta, patience) (iceflow/utils.py:80-110). */
+typedef struct igm_early_stop {
+  double relative_min_delta;
+  int32_t patience;
+  int32_t enabled;
+} igm_early_stop;
+
+/* Device-resident control block of one solve (caller allocates
+ * sizeof(igm_solver_ctl) bytes of device memory).  Written by the kernels;
+ * read back by the host once per solve. */
+typedef struct igm_solver_ctl {
+  int32_t iter;       /* iterations completed in this solve */
+  int32_t stopped;    /* early stopping fired (or an error stopped the solve) */
+  int32_t status;     /* IGM_OK or IGM_ERR_NAN_DETECTED */
+  int32_t wait;       /* EarlyStopping.wait */
+  int64_t adam_t0;    /* optimizer.iterations before this solve */
+  double best;        /* EarlyStopping.best_loss */
+  double last_cost;   /* COST of the last completed iteration */
+  double terms[3];    /* its shear, sliding, gravity means */
+} igm_solver_ctl;
+
+IGM_API const char* igm_status_string(int status);
+IGM_API const char* igm_last_error(void);
+IGM_API int igm_version(void);
+
+/* Bytes of scratch the energy / solver / reduction calls need for this grid. */
+IGM_API size_t igm_workspace_size(const igm_grid* grid);
+
+/* ---------------------------------------------------------------------------
+ * Blatter-Pattyn energy and its adjoint.
+ * Replaces iceflow_energy (igm/processes/iceflow/energy/energy.py:12-22 with
+ * cost_shear.py:55-209, cost_sliding_weertman.py:23-43, cost_gravity.py:24-69,
+ * staggered grid, Lagrange basis) followed by the per-term reduce_mean of
+ * solve.py:57-59, and its tf.GradientTape gradient (solve.py:77,
+ * emulate.py:252).
+ *   terms (device double[3]): sums over all staggered cells of all batch
+ *     entries of the shear, sliding and gravity densities (MPa m/a); the
+ *     reference's COST is (terms[0]+terms[1]+terms[2]) / (batch*(ny-1)*(nx-1)).
+ *   dU, dV: NULL for the energy only; otherwise they receive
+ *     grad_scale * d(sum of all densities)/d(U,V), same layout as U, V.
+ * ------------------------------------------------------------------------- */
+IGM_API int igm_energy(int dtype, const igm_grid* grid, const igm_physics* phys, const igm_fields* fields,
+               const void* U, const void* V, void* dU, void* dV, double grad_scale, double* terms,
+               void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Plain solver: n_iterations fused iterations of
+ *   COST, grad = energy_and_gradient(U, V); Adam.apply_gradients;
+ *   EarlyStopping.should_stop(COST)
+ * (igm/processes/iceflow/solve/solve.py:45-114), each ONE kernel: stencil
+ * energy + adjoint + Adam + the FP64 reduction + the early-stopping update
+ * on the device, no host synchronisation.  Iteration i reads (U0,V0) when
+ * ctl->iter is even and (U1,V1) when odd, and writes the other pair; after
+ * the solve the result is in pair (ctl->iter % 2).  Iterations after early
+ * stopping (or after max_iter) return at once.  mU..vV are the Adam moments
+ * (zero-filled by the caller at the start of a solve, as the reference's
+ * fresh tf.Variables get fresh slots).  costs (device double[max_iter])
+ * receives the COST history.
+ * igm_solver_begin resets ctl for a new solve whose optimizer has already
+ * taken adam_iterations steps (Keras' global optimizer.iterations).
+ * ------------------------------------------------------------------------- */
+IGM_API int igm_solver_begin(igm_solver_ctl* ctl, int64_t adam_iterations, void* stream);
+IGM_API int igm_solver_iterate(int dtype, const igm_grid* grid, const igm_physics* phys, const igm_fields* fields,
+                       void* U0, void* V0, void* U1, void* V1, void* mU, void* mV, void* vU, void* vV,
+                       const igm_adam* adam, const igm_early_stop* early_stop, int n_iterations, int max_iter,
+                       igm_solver_ctl* ctl, double* costs, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Velocity post-processing: optional mask U,V = where(thk > 0, U, 0)
+ * (solve.py:116-117, emulate.py:143-144), then velbase = U[0],
+ * velsurf = U[nz-1], velbar = sum_k U[k] * vert_weight[k]
+ * (igm/processes/iceflow/utils.py:21-51) and, fused, the CFL maximum
+ * max(max|ubar|, max|vbar|) of time.update (igm/processes/time/time.py:36-39).
+ * vert_weight: host double[nz] (define_vertical_weight, vert_disc.py:43-47).
+ * Any of the 2-D outputs and velomax (device float, overwritten) may be NULL.
+ * ------------------------------------------------------------------------- */
+IGM_API int igm_velocity_reduce(int dtype, int batch, int nz, int ny, int nx, void* U, void* V, const void* thk,
+                        int mask, const double* vert_weight, void* ubar, void* vbar, void* uvelbase,
+                        void* vvelbase, void* uvelsurf, void* vvelsurf, float* velomax, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Thickness transport step (igm/processes/thk/thk.py:27-54 with
+ * compute_divflux_slope_limiter, igm/utils/gradient/
+ * compute_divflux_slope_limiter.py:11-65):
+ *   divflux = div(q) slope-limited upwind; thk_out = max(thk + dt (smb - divflux), 0);
+ *   lsurf = max(topg, -ratio_density thk_out + sealevel); usurf = lsurf + thk_out.
+ * smb may be NULL (zero, thk.py:41-42).  lsurf_out and divflux_out may be NULL.
+ * dt is taken from dt_device (device float) when it is not NULL, else from dt.
+ * thk_out must not alias thk_in.
+ * ------------------------------------------------------------------------- */
+IGM_API int igm_transport_step(int dtype, int ny, int nx, double dx, const void* ubar, const void* vbar,
+                       const void* thk_in, void* thk_out, const void* topg, const void* smb, void* usurf_out,
+                       void* lsurf_out, void* divflux_out, double dt, const float* dt_device, int slope_type,
+                       double ratio_density, double sealevel, void* stream);
+
+/* Surfaces from thickness (thk.py:11-24): lsurf = max(topg, -r thk + sealevel),
+ * usurf = lsurf + thk.  lsurf may be NULL. */
+IGM_API int igm_thk_surfaces(int dtype, int n, const void* thk, const void* topg, void* lsurf, void* usurf,
+                     double ratio_density, double sealevel, void* stream);
+
+/* ELA mass balance (igm/processes/smb_simple/smb_simple.py:39-46):
+ * smb = clip((usurf - ela) * (usurf < ela ? gradabl : gradacc), -100, maxacc),
+ * then, when icemask is not NULL, smb = (smb < 0 || icemask > 0.5) ? smb : -10. */
+IGM_API int igm_smb_simple(int dtype, int n, const void* usurf, const void* icemask, void* smb, double gradabl,
+                   double gradacc, double ela, double maxacc, void* stream);
+
+/* max(max|a|, max|b|) over n elements into the device float *out
+ * (time.py:36-39 when ubar/vbar did not come from igm_velocity_reduce). */
+IGM_API int igm_absmax2(int dtype, int n, const void* a, const void* b, float* out, void* stream);
+
+/* CFL step on the device (time.py:36-50, without the save-time snapping):
+ * dt_out = velomax > 0 ? min(cfl dx / velomax, step_max) : step_max. */
+IGM_API int igm_cfl_dt(const float* velomax, float* dt_out, double cfl, double dx, double step_max, void* stream);
+
+/* ===========================================================================
+ * CNN emulator (igm/processes/iceflow/emulate/neural_network.py:9-66:
+ * nb_layers x [Conv2D 3x3 "same", 32 filters, bias, LeakyReLU(alpha)] and a
+ * 1x1 Conv2D head to 2 Nz outputs), BF16 tensor-core convolutions with FP32
+ * accumulation.
+ *
+ * Activations use the row-chunked layout bf16 [batch][H][C/8][W][8]
+ * ("channels in groups of 8, innermost"); the input tensor has C = 16 (the
+ * fieldin channels, zero-padded), hidden activations C = 32.
+ * Parameters are one fp32 vector in Keras order: per 3x3 layer the kernel
+ * [3][3][cin][32] then the bias [32]; then the head kernel [32][nout] and bias
+ * [nout] (igm_cnn_param_offset gives each offset).
+ * ========================================================================= */
+
+/* 3x3 convolution on the tensor cores.  cin = 16 or 32 (C of x); 32 outputs.
+ *  IGM_CONV_FWD_LEAKY: y = LeakyReLU_alpha(conv(x, wpack) + bias).
+ *  IGM_CONV_DGRAD: x is the gradient w.r.t. a layer's pre-activation, wpack the
+ *    layer's dgrad pack; y = (dL/d input of the layer) * (act_mask > 0 ? 1 : alpha),
+ *    i.e. the gradient w.r.t. the previous layer's pre-activation.  When
+ *    db_partials is not NULL it receives per-CTA sums of y over the pixels
+ *    ([db_slots][32]; slots beyond the CTAs used are left untouched).
+ * err (device int, may be NULL) is set non-zero if a pipeline wait timed out. */
+IGM_API int igm_conv3x3(int mode, int batch, int height, int width, int cin, const void* x, const void* wpack,
+                        const float* bias, const void* act_mask, void* y, float* db_partials, int db_slots,
+                        float alpha, int* err, void* stream);
+
+/* Weight gradient of a 3x3 convolution: per-CTA partial sums
+ * partials[n_parts][3 (kw)][128 (kh * cin + ci)][32 (co)] of X^T G over all
+ * pixels (G = gradient w.r.t. the pre-activation, 32 channels).  Reduce them
+ * with igm_cnn_wgrad_finish. */
+IGM_API int igm_conv3x3_wgrad(int batch, int height, int width, int cin, const void* x, const void* g,
+                              float* partials, int n_parts, int* err, void* stream);
+IGM_API int igm_conv_sm_count(void);
+
+IGM_API size_t igm_cnn_param_count(int nb_layers, int cin, int nout);
+IGM_API size_t igm_cnn_param_offset(int nb_layers, int cin, int nout, int layer, int bias);
+
+/* fp32 parameters -> bf16 UMMA operand packs: wpack_fwd (layer 0: 9*2*32*8,
+ * layers >= 1: 9*4*32*8 elements each) and wpack_bwd (layers >= 1, flipped
+ * and transposed for dgrad, 9*4*32*8 each). */
+IGM_API int igm_cnn_pack_weights(int nb_layers, int cin, int nout, const float* params, void* wpack_fwd,
+                                 void* wpack_bwd, void* stream);
+
+/* Emulator input (fieldin_to_X, iceflow/utils.py:147-158, with split_into_patches
+ * windows, emulate.py:283-308): X[b] = scaled (thk, usurf, arrhenius, slidingco, dx)
+ * of the window at host (win_y0[b], win_x0[b]) of size h x w of the [ny][nx]
+ * fields; optional fp32 copies of the windowed fields ([batch][h][w]).
+ * scales: host float[5]. */
+IGM_API int igm_cnn_input(int batch, int h, int w, int ny, int nx, const float* thk, const float* usurf,
+                          const float* arrhenius, const float* slidingco, double dx, const float* scales,
+                          const int* win_y0, const int* win_x0, void* X, float* thk_out, float* usurf_out,
+                          float* arrhenius_out, float* slidingco_out, void* stream);
+
+/* 1x1 head: U[b][k] = Y[..., k], V[b][k] = Y[..., nz + k] (Y_to_UV,
+ * iceflow/utils.py:133-139), planar fp32 [batch][nz][h][w]; zero where
+ * thk_mask <= 0 when thk_mask is not NULL (emulate.py:143-144). */
+IGM_API int igm_cnn_head_forward(int batch, int h, int w, int nz, const void* act, const float* head_w,
+                                 const float* head_b, float* U, float* V, const float* thk_mask, void* stream);
+
+/* Backward of the head and of the last LeakyReLU: dpre (bf16 row-chunked) and
+ * per-block partials [n_parts][igm_cnn_head_partial_len(nz)] = dWh [32][2nz],
+ * dbh [2nz], db_last [32]. */
+IGM_API size_t igm_cnn_head_partial_len(int nz);
+IGM_API int igm_cnn_head_backward(int batch, int h, int w, int nz, const void* act, const float* head_w,
+                                  const float* dU, const float* dV, float alpha, void* dpre, float* partials,
+                                  int n_parts, void* stream);
+
+/* out[i] (+)= sum_p partials[p * stride + i], i < len, fixed summation order. */
+IGM_API int igm_reduce_partials(const float* partials, int n_parts, int len, int stride, float* out,
+                                int accumulate, void* stream);
+
+/* igm_conv3x3_wgrad partials -> kernel gradient [3][3][cin][32]; cin_tensor is
+ * the C of the layer's input tensor (16 or 32). */
+IGM_API int igm_cnn_wgrad_finish(const float* partials, int n_parts, int cin, int cin_tensor, float* out,
+                                 void* stream);
+
+/* Keras legacy Adam with per-variable clip_by_norm (emulate.py:22-35, :267):
+ * for each variable v (elements [var_offsets[v], var_offsets[v+1]) of the
+ * vectors): g = g * c / max(|g|, c) when clipnorm c > 0, then the Adam update
+ * at step `iteration` (1-based).  var_offsets: host size_t[n_vars + 1];
+ * norms: device double[n_vars] scratch. */
+IGM_API int igm_adam_clipnorm(int n_vars, const size_t* var_offsets, float* params, const float* grads, float* m,
+                              float* v, double* norms, double lr, double beta_1, double beta_2, double epsilon,
+                              double clipnorm, int64_t iteration, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IGM_B200_H */

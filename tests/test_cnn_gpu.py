@@ -1,0 +1,109 @@
+"""The emulator network end to end through the C ABI against the oracle
+(torch-CPU float32 with the same bf16 rounding of conv inputs and weights):
+forward (U, V), the physics-informed gradient (energy adjoint -> head ->
+dgrad/wgrad chain) and one Adam step with per-variable clipnorm.
+
+Tolerances: bf16 activations make single roundings differ where the two
+sides accumulate in different orders, so fields are compared in relative L2:
+forward <= 1e-2, parameter gradients <= 5e-2, one Adam update <= 5e-2."""
+
+import numpy as np
+import pytest
+import torch
+
+from igm_b200 import kernels as K
+from igm_b200.cnn import CNN
+from igm_b200.emulator import EmulatorOptimizer, train_step
+from oracle import iceflow_oracle as O
+from tests.gpu_util import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+SCALES = [1 / 300.0, 1 / 3000.0, 1 / 100.0, 10.0, 1 / 100.0]
+
+
+def setup(nl=3, nz=4, ny=40, nx=70, seed=0):
+    st = O.valley_glacier(ny, nx, 100.0, seed=seed, varying_coeffs=True)
+    net = CNN(nb_layers=nl, cin=5, nout=2 * nz, init="he_normal", seed=seed, scales=SCALES)
+    # non-zero biases so that every bias path is exercised
+    host = net.params.cpu().numpy()
+    rng = np.random.default_rng(seed + 1)
+    for i, s in enumerate(net.shapes):
+        if len(s) == 1:
+            host[net.offsets[i]:net.offsets[i + 1]] = rng.normal(0, 0.05, s)
+    net.set_params(host)
+    f = [torch.as_tensor(st[k]).cuda() for k in ["thk", "usurf", "arrhenius", "slidingco"]]
+    return st, net, f
+
+
+def oracle_X(st, dx):
+    fl = [torch.as_tensor(st[k]) for k in ["thk", "usurf", "arrhenius", "slidingco"]]
+    fl.append(torch.full_like(fl[0], dx))
+    X = O.fieldin_to_X(fl)
+    return X * torch.tensor(SCALES, dtype=torch.float32)
+
+
+def oracle_params(net):
+    v = [torch.as_tensor(a.copy()) for a in net.get_variables()]
+    return v[0::2], v[1::2]
+
+
+@pytest.mark.parametrize("nl,nz,ny,nx", [(3, 4, 40, 70), (2, 10, 33, 129), (4, 5, 64, 64)])
+def test_forward_matches_oracle(nl, nz, ny, nx):
+    st, net, f = setup(nl, nz, ny, nx)
+    buf = net.buffers(1, ny, nx, train=False)
+    net.prepare_input(f, 100.0, [(0, 0)], ny, nx, buf)
+    U, V = net.forward(buf, 1, ny, nx)
+    ws, bs = oracle_params(net)
+    Y = O.cnn_forward(oracle_X(st, 100.0), ws, bs, bf16=True)
+    Uo, Vo = O.Y_to_UV(Y, nz)
+    assert rel_l2(U.cpu().numpy(), Uo.numpy()) < 1e-2
+    assert rel_l2(V.cpu().numpy(), Vo.numpy()) < 1e-2
+    net.check_errors()
+
+
+def test_masked_inference():
+    st, net, f = setup(2, 3, 30, 40)
+    buf = net.buffers(1, 30, 40, train=False)
+    net.prepare_input(f, 100.0, [(0, 0)], 30, 40, buf)
+    U, V = net.forward(buf, 1, 30, 40, thk_mask=f[0])
+    m = (st["thk"] > 0)[None]
+    assert np.all(U.cpu().numpy()[0][np.broadcast_to(~m, U.shape[1:])] == 0)
+
+
+def test_physics_gradient_and_adam_step_match_oracle():
+    nl, nz, ny, nx, dx = 3, 4, 40, 70, 100.0
+    st, net, f = setup(nl, nz, ny, nx, seed=3)
+    ws, bs = oracle_params(net)
+    params = []
+    for w, b in zip(ws, bs):
+        params += [w.clone().requires_grad_(True), b.clone().requires_grad_(True)]
+    dz = O.compute_zeta_dzeta(O.compute_levels(nz, 4.0))[1]
+    X = oracle_X(st, dx)
+    Y = O.cnn_forward(X, params[0::2], params[1::2], bf16=True)
+    Uo, Vo = O.Y_to_UV(Y, nz)
+    fl = [torch.as_tensor(st[k])[None] for k in ["thk", "usurf", "arrhenius", "slidingco"]]
+    cost, _ = O.energy(Uo, Vo, *fl, dx, dz)
+    grads = torch.autograd.grad(cost, params)
+    # device: one physics-informed training step
+    opt = EmulatorOptimizer(lr=1e-3, epsilon=1e-7, clipnorm=1.0)
+    p0 = net.params.clone()
+    terms = train_step(net, f, dx, [(0, 0)], ny, nx, dz.numpy(), None, 1e-3, opt)
+    net.check_errors()
+    np.testing.assert_allclose(float(terms.sum()) / ((ny - 1) * (nx - 1)), float(cost), rtol=2e-2)
+    g = net.grads.cpu().numpy()
+    for i, (s, gr) in enumerate(zip(net.shapes, grads)):
+        gd = g[net.offsets[i]:net.offsets[i + 1]].reshape(s)
+        e = rel_l2(gd, gr.numpy())
+        assert e < 5e-2, (i, s, e)
+    # the Adam update with per-variable clipnorm, against the oracle's Keras Adam
+    opt_o = O.KerasLegacyAdam(lr=1e-3, epsilon=1e-7, clipnorm=1.0)
+    xs = [p.detach().clone() for p in params]
+    gs = [torch.as_tensor(g[net.offsets[i]:net.offsets[i + 1]].reshape(s)) for i, s in enumerate(net.shapes)]
+    opt_o.apply_gradients(list(zip(gs, xs)))
+    new = net.params.cpu().numpy()
+    old = p0.cpu().numpy()
+    for i, s in enumerate(net.shapes):
+        dn = new[net.offsets[i]:net.offsets[i + 1]] - old[net.offsets[i]:net.offsets[i + 1]]
+        do = (xs[i] - params[i].detach()).numpy().ravel()
+        assert rel_l2(dn, do) < 1e-4, (i, rel_l2(dn, do))

@@ -1,0 +1,127 @@
+"""Tensor-core 3x3 convolutions (forward, data gradient, weight gradient)
+through the C ABI against torch-CPU float32 convolutions of the same
+bf16-rounded operands.  Outputs are bf16 (forward, dgrad): tolerance 1 bf16
+ulp relative plus a small absolute term; wgrad is fp32: 1e-4 relative to the
+gradient's scale."""
+
+import numpy as np
+import pytest
+import torch
+import torch.nn.functional as Fn
+
+from igm_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+
+def to_rc(x_nchw):
+    """[B, C, H, W] -> row-chunked [B, H, C/8, W, 8]"""
+    B, Cc, H, W = x_nchw.shape
+    return x_nchw.reshape(B, Cc // 8, 8, H, W).permute(0, 3, 1, 4, 2).contiguous()
+
+
+def from_rc(x):
+    B, H, C8, W, E = x.shape
+    return x.permute(0, 2, 4, 1, 3).reshape(B, C8 * E, H, W)
+
+
+def bf(t):
+    return t.to(torch.bfloat16).to(torch.float32)
+
+
+def pack_fwd(w_kkio, cin_t):
+    """Keras kernel [3,3,cin,32] -> [9][cin_t/8][32][8] bf16."""
+    kh, kw, cin, co = w_kkio.shape
+    out = torch.zeros(9, cin_t // 8, co, 8)
+    for t in range(9):
+        for ci in range(cin):
+            out[t, ci // 8, :, ci % 8] = w_kkio[t // 3, t % 3, ci, :]
+    return out.to(torch.bfloat16).contiguous()
+
+
+def pack_bwd(w_kkio):
+    out = torch.zeros(9, 4, 32, 8)
+    for tp in range(9):
+        t = 8 - tp
+        for co in range(32):
+            out[tp, co // 8, :, co % 8] = w_kkio[t // 3, t % 3, :, co]
+    return out.to(torch.bfloat16).contiguous()
+
+
+def keras_to_torch(w):
+    return w.permute(3, 2, 0, 1)  # [co, ci, kh, kw]
+
+
+SHAPES = [(1, 4, 128, 32), (1, 9, 200, 32), (2, 7, 37, 32), (1, 13, 1000, 32), (1, 1, 5, 32), (3, 6, 129, 16),
+          (1, 33, 300, 16)]
+
+
+@pytest.mark.parametrize("B,H,W,cin", SHAPES)
+def test_conv_forward(B, H, W, cin):
+    g = torch.Generator().manual_seed(H * 1000 + W)
+    x = bf(torch.randn(B, cin, H, W, generator=g))
+    cin_real = cin if cin == 32 else 5
+    if cin == 16:
+        x[:, 5:] = 0
+    w = torch.randn(3, 3, cin_real, 32, generator=g) * (1.0 / np.sqrt(9 * cin_real))
+    b = torch.randn(32, generator=g) * 0.1
+    ref = Fn.leaky_relu(Fn.conv2d(x[:, :cin_real], bf(keras_to_torch(w)), b, padding=1), 0.01)
+    xd = to_rc(x).to(torch.bfloat16).cuda()
+    wp = pack_fwd(w, cin).cuda()
+    y = torch.empty((B, H, 4, W, 8), dtype=torch.bfloat16, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    bd = b.cuda()
+    rc = L.lib().igm_conv3x3(0, B, H, W, cin, xd.data_ptr(), wp.data_ptr(), bd.data_ptr(), None,
+                             y.data_ptr(), None, 0, 0.01, err.data_ptr(), L.stream_ptr())
+    L.check(rc)
+    out = from_rc(y.float().cpu())
+    assert int(err.item()) == 0
+    np.testing.assert_allclose(out.numpy(), ref.numpy(), rtol=8e-3, atol=2e-3 * float(ref.abs().max()))
+
+
+@pytest.mark.parametrize("B,H,W", [(1, 8, 128), (2, 11, 173), (1, 5, 1000)])
+def test_conv_dgrad(B, H, W):
+    g = torch.Generator().manual_seed(B * 100 + H)
+    gout = bf(torch.randn(B, 32, H, W, generator=g))
+    aprev = bf(torch.randn(B, 32, H, W, generator=g))
+    w = torch.randn(3, 3, 32, 32, generator=g) * (1.0 / np.sqrt(288))
+    dx = torch.nn.grad.conv2d_input((B, 32, H, W), bf(keras_to_torch(w)), gout, padding=1)
+    ref = dx * torch.where(aprev > 0, 1.0, 0.01)
+    y = torch.empty((B, H, 4, W, 8), dtype=torch.bfloat16, device="cuda")
+    dbp = torch.zeros((148, 32), device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    gd = to_rc(gout).to(torch.bfloat16).cuda()
+    wd = pack_bwd(w).cuda()
+    ad = to_rc(aprev).to(torch.bfloat16).cuda()
+    rc = L.lib().igm_conv3x3(1, B, H, W, 32, gd.data_ptr(), wd.data_ptr(), None, ad.data_ptr(),
+                             y.data_ptr(), dbp.data_ptr(), 148, 0.01, err.data_ptr(), L.stream_ptr())
+    L.check(rc)
+    out = from_rc(y.float().cpu())
+    assert int(err.item()) == 0
+    np.testing.assert_allclose(out.numpy(), ref.numpy(), rtol=8e-3, atol=2e-3 * float(ref.abs().max()))
+    db = dbp.sum(0).cpu().numpy()
+    np.testing.assert_allclose(db, ref.sum((0, 2, 3)).numpy(), rtol=1e-3, atol=1e-3 * float(ref.abs().sum((0, 2, 3)).max()))
+
+
+@pytest.mark.parametrize("B,H,W,cin", [(1, 8, 128, 32), (2, 9, 150, 32), (1, 6, 1000, 32), (2, 10, 77, 16)])
+def test_conv_wgrad(B, H, W, cin):
+    g = torch.Generator().manual_seed(H * 7 + W)
+    x = bf(torch.randn(B, cin, H, W, generator=g))
+    cin_real = 32 if cin == 32 else 5
+    if cin == 16:
+        x[:, 5:] = 0
+    gout = bf(torch.randn(B, 32, H, W, generator=g))
+    ref = torch.nn.grad.conv2d_weight(x[:, :cin_real], (32, cin_real, 3, 3), gout, padding=1)  # [co, ci, kh, kw]
+    ref_k = ref.permute(2, 3, 1, 0).contiguous()  # Keras [kh, kw, ci, co]
+    npart = 37
+    part = torch.empty((npart, 3, 128, 32), device="cuda")
+    out = torch.empty((3, 3, cin_real, 32), device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    xd = to_rc(x).to(torch.bfloat16).cuda()
+    gd = to_rc(gout).to(torch.bfloat16).cuda()
+    rc = L.lib().igm_conv3x3_wgrad(B, H, W, cin, xd.data_ptr(), gd.data_ptr(), part.data_ptr(), npart,
+                                   err.data_ptr(), L.stream_ptr())
+    L.check(rc)
+    L.check(L.lib().igm_cnn_wgrad_finish(part.data_ptr(), npart, cin_real, cin, out.data_ptr(), L.stream_ptr()))
+    assert int(err.item()) == 0
+    np.testing.assert_allclose(out.cpu().numpy(), ref_k.numpy(), rtol=1e-4, atol=1e-4 * float(ref_k.abs().max()))

@@ -1,0 +1,121 @@
+"""The fused device solver against the reference's solve_iceflow (golden
+vectors made from the reference source) and against the oracle."""
+
+import numpy as np
+import pytest
+import torch
+
+from igm_b200 import _lib as L
+from igm_b200.solver import DeviceAdamSolver
+from oracle import iceflow_oracle as O
+from tests.gpu_util import dev, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case,nsolve", [("f64", 3), ("f32", 2)])
+def test_solver_sequence_matches_reference(golden, case, nsolve):
+    """Three solves on one optimizer: iteration counts (early stopping), the
+    global Adam step counter, the COST history and U, V after each solve."""
+    g = golden(f"solver_{case}")
+    f64 = case == "f64"
+    dt = torch.float64 if f64 else torch.float32
+    thk, usurf, A, c = (dev(g[k], dt) for k in ["thk", "usurf", "arrhenius", "slidingco"])
+    nz = g["s0_U"].shape[0]
+    dz = O.compute_zeta_dzeta(O.compute_levels(nz, 4.0).to(dt))[1].numpy()
+    solver = DeviceAdamSolver(lr=1.0)
+    U = torch.zeros((nz,) + tuple(thk.shape), dtype=dt, device="cuda")
+    V = torch.zeros_like(U)
+    for s in range(nsolve):
+        U, V, costs = solver.solve(U, V, thk, usurf, A, c, float(g["dx"]), dz, nbitmax=int(g["nbitmax"]))
+        ref_costs = g[f"s{s}_costs"]
+        assert len(costs) == len(ref_costs), (len(costs), len(ref_costs))
+        assert solver.iterations == int(g[f"s{s}_iterations_after"])
+        # FP32: the trajectory's sensitivity (see test_fp32_solver_error_against_fp64)
+        np.testing.assert_allclose(costs, ref_costs, rtol=1e-9 if f64 else 1e-4,
+                                   atol=(1e-9 if f64 else 1e-4) * np.abs(ref_costs).max())
+        e = max(rel_l2(U.cpu().numpy(), g[f"s{s}_U"]), rel_l2(V.cpu().numpy(), g[f"s{s}_V"]))
+        assert e < (1e-9 if f64 else 1e-2), e
+
+
+def _oracle_solve(st, nz, dt, n):
+    f = [torch.as_tensor(st[k]).to(dt) for k in ["thk", "usurf", "arrhenius", "slidingco"]]
+    dz = O.compute_zeta_dzeta(O.compute_levels(nz, 4.0).to(dt))[1]
+    Z = torch.zeros((nz,) + tuple(f[0].shape), dtype=dt)
+    U, V, c = O.solve_iceflow(Z, Z, *f, 100.0, dz, O.KerasLegacyAdam(lr=1.0), nbitmax=n, early_stopping=False)
+    return np.concatenate([U.double().numpy().ravel(), V.double().numpy().ravel()]), c
+
+
+def _device_solve(st, nz, dt, n):
+    f = [dev(st[k], dt) for k in ["thk", "usurf", "arrhenius", "slidingco"]]
+    dz = O.compute_zeta_dzeta(O.compute_levels(nz, 4.0).to(dt))[1].numpy()
+    Z = torch.zeros((nz,) + tuple(f[0].shape), dtype=dt, device="cuda")
+    U, V, c = DeviceAdamSolver().solve(Z, Z, *f, 100.0, dz, nbitmax=n, early_stopping=False)
+    return np.concatenate([U.double().cpu().numpy().ravel(), V.double().cpu().numpy().ravel()]), c
+
+
+@pytest.mark.parametrize("n", [1, 10, 30])
+def test_fp64_solver_matches_fp64_oracle(n):
+    st = O.valley_glacier(40, 36, 100.0, seed=2)
+    ref, cref = _oracle_solve(st, 10, torch.float64, n)
+    got, c = _device_solve(st, 10, torch.float64, n)
+    assert rel_l2(got, ref) < 1e-8, rel_l2(got, ref)
+    np.testing.assert_allclose(c, cref, rtol=1e-10)
+
+
+def test_fp64_solver_100_iterations_within_sensitivity():
+    """After 100 iterations a 1e-15 relative perturbation of the inputs moves
+    the FP64 oracle solution by ~3e-4 (the trajectory amplifies round-off), so
+    the device FP64 solve is bounded by that sensitivity."""
+    st = O.valley_glacier(40, 36, 100.0, seed=2)
+    ref, cref = _oracle_solve(st, 10, torch.float64, 100)
+    rng = np.random.default_rng(0)
+    pert = {k: (v * (1 + 1e-15 * rng.standard_normal(v.shape))) if k in ("thk", "usurf", "arrhenius", "slidingco") else v
+            for k, v in {k: np.asarray(st[k], np.float64) for k in ("thk", "usurf", "arrhenius", "slidingco")}.items()}
+    refp, cpert = _oracle_solve(pert, 10, torch.float64, 100)
+    sens = rel_l2(refp, ref)
+    got, c = _device_solve(st, 10, torch.float64, 100)
+    e = rel_l2(got, ref)
+    print(f"device FP64 vs oracle FP64 after 100 iterations: {e:.3e}; oracle sensitivity to 1e-15 input noise: {sens:.3e}")
+    assert e <= 10 * sens + 1e-9, (e, sens)
+    spread = max(abs(cpert[-1] - cref[-1]), 1e-9 * abs(cref[-1]))
+    print(f"final COST: device {c[-1]:.6f}, oracle {cref[-1]:.6f}, perturbed oracle {cpert[-1]:.6f}")
+    assert abs(c[-1] - cref[-1]) <= 10 * spread + 1e-3 * abs(cref[-1])
+
+
+@pytest.mark.parametrize("n", [1, 10, 100])
+def test_fp32_solver_error_against_fp64(n):
+    """Adam at lr = 1 amplifies rounding (a 1e-7 relative perturbation of the
+    inputs moves the FP64 solution by ~3e-3 after 100 iterations), so the FP32
+    result is judged against the FP64 oracle relative to the reference
+    algorithm's own FP32 error: |U32 - U64| <= 3 |U32_oracle - U64_oracle| + 1e-6."""
+    st = O.valley_glacier(40, 36, 100.0, seed=2)
+    ref64, c64 = _oracle_solve(st, 10, torch.float64, n)
+    ref32, _ = _oracle_solve(st, 10, torch.float32, n)
+    got, c = _device_solve(st, 10, torch.float32, n)
+    e_dev, e_ref = rel_l2(got, ref64), rel_l2(ref32, ref64)
+    print(f"n={n}: device FP32 vs FP64 {e_dev:.3e}; reference algorithm FP32 vs FP64 {e_ref:.3e}")
+    assert e_dev <= 3 * e_ref + 1e-6, (e_dev, e_ref)
+    _, c32 = _oracle_solve(st, 10, torch.float32, n)
+    assert abs(c[-1] - c64[-1]) <= 3 * abs(c32[-1] - c64[-1]) + 1e-5 * abs(c64[-1])
+
+
+def test_nan_input_stops_with_status():
+    st = O.valley_glacier(20, 20, 100.0, seed=1)
+    st["thk"][5, 5] = np.nan
+    dz = O.compute_zeta_dzeta(O.compute_levels(5, 4.0))[1].numpy()
+    Z = torch.zeros((5, 20, 20), device="cuda")
+    with pytest.raises(L.IgmError) as ei:
+        DeviceAdamSolver().solve(Z, Z, *[dev(st[k]) for k in ["thk", "usurf", "arrhenius", "slidingco"]], 100.0, dz,
+                                 nbitmax=20)
+    assert ei.value.status == 3
+
+
+def test_max_iter_caps_and_no_early_stop():
+    st = O.valley_glacier(20, 24, 100.0, seed=1)
+    dz = O.compute_zeta_dzeta(O.compute_levels(5, 4.0))[1].numpy()
+    Z = torch.zeros((5, 20, 24), device="cuda")
+    s = DeviceAdamSolver()
+    _, _, c = s.solve(Z, Z, *[dev(st[k]) for k in ["thk", "usurf", "arrhenius", "slidingco"]], 100.0, dz,
+                      nbitmax=7, early_stopping=False)
+    assert len(c) == 7 and s.iterations == 7
