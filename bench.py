@@ -1,0 +1,469 @@
+"""Benchmark: model years per second of the transient glacier run at
+1000 x 1000 x Nz=10 on one B200, emulator-driven vs the plain solver.
+
+Workload (the transient emulator-driven run): the synthetic valley glacier
+mapped to a 50 km domain (1000 x 1000 cells at dx = 50 m, Nz = 10; A and c
+log-uniform per cell, smoothed), an ELA mass balance (ELA 2900 m, gradient
+0.009 /a, cap 2 m/a) and CFL 0.3 adaptive time steps.  One step is one model
+time step of the reference's process loop: smb_simple -> iceflow -> time ->
+thk.  The emulated run retrains the CNN (16 x 3x3 conv, 32 filters, 1x1 head
+to 20 channels) 5 Adam steps every 10 time steps and lets the plain solver
+judge it every 50 steps (fallback margin 2 %); before timing, the emulator is
+trained on 64 x 64 windows of the initial state (batch 8, Adam lr 1e-4).
+The plain run uses method "solved" (Adam lr 1, up to 100 iterations, early
+stopping) on the same state.
+
+value       emulator-driven model years/s (all ranks; inputs resident in HBM)
+e2e         the same run through the process API with a host-resident state:
+            each step copies its 2-D inputs host->device and its 2-D results
+            device->host (pinned buffers)
+extra keys  plain-solver years/s, the emulator/plain speed-up, the emulator's
+            relative L2 velocity error against an FP64 solve, the fallback log.
+--impl reference   times the CPU restatement of the reference (torch-CPU, all
+            host threads) on a bounded sample of the same workload.
+Multi-GPU: replicas only (each rank simulates its own glacier, no exchange).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ELA_TABLE = [["time", "gradabl", "gradacc", "ela", "accmax"],
+             [0.0, 0.009, 0.009, 2900.0, 2.0], [249.99, 0.009, 0.009, 2900.0, 2.0],
+             [250.0, 0.009, 0.009, 3000.0, 2.0], [1e6, 0.009, 0.009, 3000.0, 2.0]]
+SCALES = [1 / 300.0, 1 / 3000.0, 1 / 100.0, 10.0, 1 / 50.0]
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=1000)
+    ap.add_argument("--nz", type=int, default=10)
+    ap.add_argument("--pretrain", type=int, default=2000)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(args):
+    return {"workload": f"transient emulator-driven glacier run {args.size}x{args.size}xNz{args.nz}",
+            "dx_m": 50.0, "nz": args.nz, "retrain": "5 Adam steps every 10 time steps",
+            "fallback_check_every": 50, "fallback_margin": 0.02, "cfl": 0.3,
+            "l2": "working set larger than L2 (16 x 64 MB activations, 80 MB U/V)"}
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index, self.rows, self.proc = index, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[0]) for r in self.rows if len(r) >= 7 and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) >= 7 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 7 for i in range(4)
+                          if r[3 + i].strip().lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def make_state(args, host=False):
+    import torch
+    from igm_b200.state import State
+    from oracle.iceflow_oracle import valley_glacier  # synthetic input generator only
+    g = valley_glacier(args.size, args.size, 50.0, seed=0, varying_coeffs=True)
+    st = State()
+    for k in ["topg", "thk", "arrhenius", "slidingco"]:
+        setattr(st, k, np.ascontiguousarray(g[k]) if host else torch.as_tensor(g[k]).cuda())
+    st.dx = 50.0
+    st.dX = 50.0
+    st.it = -1
+    if host:
+        st.device = "cuda"
+    return st
+
+
+def make_cfg(args, method):
+    from igm_b200.config import default_cfg
+    return default_cfg({
+        "iceflow": {"method": method,
+                    "numerics": {"Nz": args.nz},
+                    "emulator": {"retrain_freq": 10, "nbit": 5, "lr": 1e-4, "lr_init": 1e-4, "framesizemax": 1024,
+                                 "pretrained": False, "input_scales": SCALES, "seed": 0,
+                                 "network": {"weight_initialization": "he_normal"}},
+                    "fallback": {"every": 50 if method == "emulated" else 0, "margin": 0.02, "nbitmax": 100}},
+        "time": {"start": 0.0, "end": 500.0, "save": 1000.0, "cfl": 0.3, "step_max": 1.0},
+        "smb_simple": {"array": ELA_TABLE},
+    })
+
+
+def processes():
+    from igm_b200.processes import iceflow, smb_simple, thk
+    from igm_b200.processes import time as tproc
+    return [smb_simple, iceflow, tproc, thk]
+
+
+def init_run(cfg, st, pretrain=None):
+    mods = processes()
+    from igm_b200.processes import thk as thk_mod
+    thk_mod.initialize(cfg, st)  # usurf from topg + thk before the emulator sees it
+    for m in mods:
+        if m.__name__.endswith("iceflow") and pretrain is not None:
+            pretrain(cfg, st)
+        m.initialize(cfg, st)
+    st.it = 0
+    return mods
+
+
+def step(cfg, st, mods):
+    for m in mods:
+        m.update(cfg, st)
+    st.it += 1
+
+
+def pretrain_emulator(args, nsteps):
+    """Trains the emulator on 64 x 64 windows of the initial state, batch 8,
+    Adam lr 1e-4 (untimed), before the iceflow process initialises."""
+    def run(cfg, st):
+        import torch
+        from igm_b200 import state as S
+        from igm_b200.cnn import CNN
+        from igm_b200.emulator import EmulatorOptimizer, train_step
+        from igm_b200.processes.iceflow import physics
+        from igm_b200.vertical import compute_levels, compute_zeta_dzeta
+        e = cfg.processes.iceflow.emulator
+        net = CNN(nb_layers=16, cin=5, nout=2 * args.nz, init="he_normal", seed=0, scales=SCALES)
+        f = [S.get(st, k) for k in ("thk", "usurf", "arrhenius", "slidingco")]
+        dz = compute_zeta_dzeta(compute_levels(args.nz, 4.0))[1]
+        opt = EmulatorOptimizer(1e-4, e.optimizer_epsilon, e.optimizer_clipnorm)
+        rng = np.random.default_rng(0)
+        ny, nx = f[0].shape
+        thk = f[0].cpu().numpy()
+        iy, ix = np.nonzero(thk > 0)
+        for i in range(nsteps):
+            k = rng.integers(0, len(iy), size=8)
+            wins = [(int(np.clip(iy[j] - 32, 0, ny - 64)), int(np.clip(ix[j] - 32, 0, nx - 64))) for j in k]
+            train_step(net, f, 50.0, wins, 64, 64, dz, physics(cfg), 1e-4, opt)
+        net.check_errors()
+        torch.cuda.synchronize()
+        path = os.path.join(ROOT, "_bench_emulator")
+        os.makedirs(path, exist_ok=True)
+        np.savez(os.path.join(path, "model.npz"), params=net.params.cpu().numpy(), adam_m=net.m.cpu().numpy(),
+                 adam_v=net.v.cpu().numpy(), iterations=np.array(net.opt_iterations), nb_layers=np.array(16),
+                 nout=np.array(2 * args.nz), cin=np.array(5), scales=np.asarray(SCALES, np.float32))
+        e.pretrained = True
+        e.name = path
+    return run
+
+
+def timed(fn, K, sync):
+    import torch
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sync()
+    s.record()
+    out = fn(K)
+    e.record()
+    sync()
+    return s.elapsed_time(e) / 1e3, out
+
+
+def velocity_error_fp64(cfg, st):
+    """Relative L2 of the emulated velocities against a long FP64 solve from them."""
+    import torch
+    from igm_b200 import state as S
+    from igm_b200.processes.iceflow import physics
+    from igm_b200.solver import DeviceAdamSolver
+    f = [S.get(st, k).double() for k in ("thk", "usurf", "arrhenius", "slidingco")]
+    U0, V0 = st.U.double(), st.V.double()
+    s = DeviceAdamSolver(lr=1.0)
+    U, V, c = s.solve(U0, V0, *f, 50.0, np.asarray(st.dzeta, np.float64), nbitmax=500, phys=physics(cfg),
+                      early_stopping=False)
+    m = (f[0] > 0)[None]
+    num = torch.sqrt(((U0 - U)[m.expand_as(U)] ** 2).sum() + ((V0 - V)[m.expand_as(V)] ** 2).sum())
+    den = torch.sqrt((U[m.expand_as(U)] ** 2).sum() + (V[m.expand_as(V)] ** 2).sum())
+    return float(num / den), float(c[-1])
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    from igm_b200 import _lib as L
+    from igm_b200.build import build
+    build()
+    lib = L.lib()
+    dev = torch.cuda.current_device()
+
+    def sync():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    res = {}
+    # ---- emulator-driven run ---------------------------------------------------
+    cfg_e = make_cfg(args, "emulated")
+    st = make_state(args)
+    t0 = time.time()
+    mods = init_run(cfg_e, st, pretrain=pretrain_emulator(args, args.pretrain))
+    res["setup_s"] = time.time() - t0
+    for _ in range(args.warmup):
+        step(cfg_e, st, mods)
+    conv_ev = []
+    st.iceflow_model.event_hook = conv_ev
+    t_start = float(st.t)
+    l0 = lib.igm_launch_count()
+    clk = ClockSampler(dev)
+    clk.start()
+
+    def run_em(K):
+        for _ in range(K):
+            step(cfg_e, st, mods)
+    el_e, _ = timed(run_em, args.steps, sync)
+    clocks = clk.stop()
+    launches = lib.igm_launch_count() - l0
+    st.iceflow_model.event_hook = None
+    years_e = float(st.t) - t_start
+    el_e = max_over_ranks(el_e)
+    res["emulated"] = dict(years=years_e, seconds=el_e, years_per_s=years_e / el_e)
+    conv_ms = [a.elapsed_time(b) for a, b in conv_ev]
+    # velocity error of the emulator against a long FP64 solve of the current state
+    try:
+        res["vel_rel_l2_vs_fp64"], _ = velocity_error_fp64(cfg_e, st)
+    except Exception as exc:  # reported, not fatal
+        res["vel_rel_l2_vs_fp64"] = f"failed: {exc}"
+    res["fallback_log"] = getattr(st, "fallback_log", [])
+    del st, mods
+    torch.cuda.empty_cache()
+
+    # ---- plain-solver run ---------------------------------------------------------
+    cfg_s = make_cfg(args, "solved")
+    st = make_state(args)
+    mods = init_run(cfg_s, st)
+    for _ in range(args.warmup):
+        step(cfg_s, st, mods)
+    t_start = float(st.t)
+    it0 = st.iceflow_solver.iterations
+    el_s, _ = timed(lambda K: [step(cfg_s, st, mods) for _ in range(K)], args.steps, sync)
+    years_s = float(st.t) - t_start
+    el_s = max_over_ranks(el_s)
+    res["solved"] = dict(years=years_s, seconds=el_s, years_per_s=years_s / el_s,
+                         solver_iterations_per_step=(st.iceflow_solver.iterations - it0) / args.steps)
+    del st, mods
+    torch.cuda.empty_cache()
+
+    # ---- e2e: host-resident state through the process API ----------------------
+    e2e = None
+    if not args.no_e2e:
+        st = make_state(args, host=True)
+        mods = init_run(cfg_e, st)
+        for _ in range(args.warmup):
+            step(cfg_e, st, mods)
+        t_start = float(st.t)
+        nbytes = args.size * args.size * 4
+        el_h, _ = timed(lambda K: [step(cfg_e, st, mods) for _ in range(K)], args.steps, sync)
+        el_h = max_over_ranks(el_h)
+        yrs = float(st.t) - t_start
+        # per step: smb reads usurf; iceflow reads thk, usurf, arrhenius, slidingco; time reads nothing new
+        # (fused max); thk reads ubar, vbar, thk, topg, smb.  Writes: smb; ubar, vbar, velbase x2,
+        # velsurf x2; thk, lsurf, usurf, divflux.
+        e2e = {"value": world * yrs / el_h, "unit": "model years/s", "h2d_bytes_per_step": 10 * nbytes,
+               "d2h_bytes_per_step": 11 * nbytes}
+        del st, mods
+    return res, conv_ms, clocks, launches, e2e
+
+
+def roofline_conv(conv_ms, size, peaks):
+    """Forward 3x3 conv (cin = 32): algorithmic bytes per launch = one read of
+    the input activation and one write of the output, 2 x 64 B per pixel."""
+    if not conv_ms:
+        return None
+    t = float(np.mean(conv_ms)) / 1e3
+    byts = 2 * 64 * size * size
+    achieved = byts / t / 1e9
+    peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "conv3x3_fwd_1000x1000.txt")
+    if os.path.exists(prof):
+        for line in open(prof):
+            if line.startswith("dram_bytes_per_launch:"):
+                traffic = float(line.split(":")[1])
+    return {"kernel": "conv3x3_kernel<4,4,fwd> (tcgen05, cin 32)", "bound": "hbm", "achieved": round(achieved, 1),
+            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+            "algorithmic_bytes": byts, "avg_launch_us": round(t * 1e6, 2), "launches": len(conv_ms),
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback"}
+
+
+def cpu_sample(args, nthreads, steps=1):
+    """CPU restatement of the reference (torch-CPU FP32) on a bounded sample of
+    the workload: per model time step one CNN forward over the whole domain,
+    two training steps on 500 x 500 patches (5 steps x 4 patches every 10 time
+    steps), and the transport; the model time per step is the CFL step of the
+    physical velocity field from a coarse (200 x 200) CPU solve of the same glacier."""
+    import torch
+    from oracle import iceflow_oracle as O
+    torch.set_num_threads(nthreads)
+    nz = args.nz
+    g = O.valley_glacier(args.size, args.size, 50.0, seed=0, varying_coeffs=True)
+    f = {k: torch.as_tensor(g[k]) for k in ["thk", "usurf", "arrhenius", "slidingco", "topg"]}
+    # physical CFL step from a coarse solve
+    gc = O.valley_glacier(200, 200, 250.0, seed=0, varying_coeffs=True)
+    fc = [torch.as_tensor(gc[k]) for k in ["thk", "usurf", "arrhenius", "slidingco"]]
+    dzc = O.compute_zeta_dzeta(O.compute_levels(nz, 4.0))[1]
+    Z = torch.zeros((nz, 200, 200))
+    Uc, Vc, _ = O.solve_iceflow(Z, Z, *fc, 250.0, dzc, O.KerasLegacyAdam(lr=1.0), nbitmax=300)
+    w = O.define_vertical_weight(nz, 4.0)
+    ub, vb = O.get_velbar(Uc, Vc, w)
+    dt, _ = O.cfl_dt(ub, vb, 50.0)
+    rng = np.random.default_rng(0)
+    ws, bs, c = [], [], 5
+    for _ in range(16):
+        ws.append(torch.as_tensor(rng.normal(0, np.sqrt(2 / (9 * c)), (3, 3, c, 32)).astype(np.float32)))
+        bs.append(torch.zeros(32))
+        c = 32
+    ws.append(torch.as_tensor(rng.normal(0, np.sqrt(1 / 32), (1, 1, 32, 2 * nz)).astype(np.float32)))
+    bs.append(torch.zeros(2 * nz))
+    X = O.fieldin_to_X([f["thk"], f["usurf"], f["arrhenius"], f["slidingco"], torch.full_like(f["thk"], 50.0)])
+    dz = O.compute_zeta_dzeta(O.compute_levels(nz, 4.0))[1]
+    times = []
+    for _ in range(steps):
+        t0 = time.time()
+        with torch.no_grad():
+            Y = O.cnn_forward(X, ws, bs)
+        t1 = time.time()
+        Xp = X[:, :500, :500]
+        ps = [p.clone().requires_grad_(True) for p in ws + bs]
+        Yp = O.cnn_forward(Xp, ps[:17], ps[17:])
+        Up, Vp = O.Y_to_UV(Yp, nz)
+        cost, _ = O.energy(Up, Vp, Xp[..., 0], Xp[..., 1], Xp[..., 2], Xp[..., 3], 50.0, dz)
+        torch.autograd.grad(cost, ps)
+        t2 = time.time()
+        Ue, Ve = O.Y_to_UV(Y, nz)
+        ubar, vbar = O.get_velbar(Ue[0], Ve[0], w)
+        O.thk_update(f["thk"], f["topg"], ubar, vbar, torch.zeros_like(f["thk"]), 50.0, torch.tensor(dt))
+        t3 = time.time()
+        times.append((t1 - t0) + 2 * (t2 - t1) + (t3 - t2))
+    step_s = float(np.median(times))
+    return {"value": dt / step_s, "unit": "model years/s", "cores": nthreads, "kind": "port",
+            "sample": f"{steps} model time step(s) at {args.size}^2 x Nz{args.nz}: 1 CNN forward (1000^2) + "
+                      f"2 training steps on 500^2 patches + transport, torch-CPU FP32; dt = {dt:.4f} a from "
+                      "the CFL step of a 200^2 CPU solve of the same glacier",
+            "seconds_per_step": step_s}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        n = os.cpu_count() or 1
+        cpu_sample(args, n, steps=1)  # warm-up of the CPU path
+        t0 = time.time()
+        vals = []
+        for _ in range(max(1, args.steps // 10)):
+            vals.append(cpu_sample(args, n, steps=1))
+        v = float(np.median([x["value"] for x in vals]))
+        cb = dict(vals[-1])
+        cb["value"] = v
+        line = {"impl": "reference", "metric": "model years/s", "value": v, "unit": "model years/s",
+                "n_gpus": args.gpus, "steps": len(vals), "warmup": 1, "ms_per_step": 1e3 * cb["seconds_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": workload_config(args), "cpu_baseline": cb,
+                "e2e": {"value": v, "unit": "model years/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "wall_s": time.time() - t0}
+        print(json.dumps(line))
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as D
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        import datetime
+        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = D
+    res, conv_ms, clocks, launches, e2e = run_ours(args, rank, world, dist)
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    em, sv = res["emulated"], res["solved"]
+    value = world * em["years_per_s"]
+    line = {"metric": "model years/s at 1000^2xNz10: emulator vs plain solver, one B200, <=1% vel err",
+            "value": value, "unit": "model years/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * em["seconds"] / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 conv / f32 energy", "data": "synthetic",
+            "config": workload_config(args),
+            "plain_solver_years_per_s": world * sv["years_per_s"],
+            "plain_solver_ms_per_step": 1e3 * sv["seconds"] / args.steps,
+            "plain_solver_iterations_per_step": sv["solver_iterations_per_step"],
+            "speedup_vs_plain": em["years_per_s"] / sv["years_per_s"],
+            "vel_rel_l2_vs_fp64": res["vel_rel_l2_vs_fp64"],
+            "fallback_checks": len(res["fallback_log"]),
+            "fallbacks": sum(1 for x in res["fallback_log"] if x["fallback"]),
+            "roofline": roofline_conv(conv_ms, args.size, peaks),
+            "clocks": clocks, "gpu_launches": int(launches), "e2e": e2e, "setup_s": res["setup_s"]}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_sample(args, os.cpu_count() or 1, steps=1)
+        except Exception as exc:
+            line["cpu_baseline"] = {"value": None, "error": str(exc)}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -70,6 +70,7 @@ SIGNATURES = {
     "igm_status_string": (C.c_char_p, [I]),
     "igm_last_error": (C.c_char_p, []),
     "igm_version": (I, []),
+    "igm_launch_count": (C.c_longlong, []),
     "igm_workspace_size": (C.c_size_t, [C.POINTER(Grid)]),
     "igm_energy": (I, [I, C.POINTER(Grid), C.POINTER(Physics), C.POINTER(Fields), P, P, P, P, D, P, P,
                        C.c_size_t, P]),

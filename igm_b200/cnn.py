@@ -60,6 +60,7 @@ class CNN:
         self.wpack_b = torch.zeros(max(self.L - 1, 1) * 9 * 4 * F * 8, dtype=torch.bfloat16, device=self.device)
         self.init_weights(init, seed)
         self._bufs = {}
+        self.event_hook = None  # list: (start, end) CUDA events of each 32-channel forward conv launch
         self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.n_sm = int(lib.igm_conv_sm_count())
 
@@ -154,11 +155,18 @@ class CNN:
         acts = buf["acts"]
         x = buf["X"]
         cin_t = 16
+        hook = self.event_hook if (self.event_hook is not None and not keep_acts) else None
         for l in range(self.L):
             y = acts[l] if keep_acts else acts[l % 2]
+            if hook is not None and l > 0:
+                ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                ev[0].record()
             rc = lib.igm_conv3x3(0, B, h, w, cin_t, _p(x), self._wf(l), self._b(l), None, _p(y), None, 0,
                                  self.alpha, _p(self.err), st)
             L.check(rc, f"igm_conv3x3 layer {l}")
+            if hook is not None and l > 0:
+                ev[1].record()
+                hook.append(ev)
             x, cin_t = y, F
         hw = self.params.data_ptr() + 4 * self.offsets[2 * self.L]
         hb = self.params.data_ptr() + 4 * self.offsets[2 * self.L + 1]

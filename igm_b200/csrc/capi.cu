@@ -1,6 +1,8 @@
 // Status strings, error text and version of the C ABI.
 #include <stdarg.h>
 
+#include <atomic>
+
 #include "common.cuh"
 
 namespace igm {
@@ -14,7 +16,12 @@ void set_error(const char* fmt, ...) {
   va_end(ap);
 }
 
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 }  // namespace igm
+
+extern "C" long long igm_launch_count(void) { return igm::g_launches.load(std::memory_order_relaxed); }
 
 extern "C" const char* igm_status_string(int status) {
   switch (status) {

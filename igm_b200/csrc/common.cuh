@@ -20,8 +20,11 @@ void set_error(const char* fmt, ...);
     }                                       \
   } while (0)
 
-// Returns IGM_ERR_CUDA with the error text when the last launch failed.
+// Counts kernel launches (igm_launch_count) and returns IGM_ERR_CUDA with the
+// error text when the last launch failed.  Called after every launch.
+void note_launch();
 inline int launch_status(const char* what) {
+  note_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_error("%s: %s", what, cudaGetErrorString(e));

@@ -131,6 +131,8 @@ typedef struct igm_solver_ctl {
 IGM_API const char* igm_status_string(int status);
 IGM_API const char* igm_last_error(void);
 IGM_API int igm_version(void);
+/* Number of kernels this library has launched in the process (all threads). */
+IGM_API long long igm_launch_count(void);
 
 /* Bytes of scratch the energy / solver / reduction calls need for this grid. */
 IGM_API size_t igm_workspace_size(const igm_grid* grid);
