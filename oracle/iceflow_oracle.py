@@ -275,7 +275,7 @@ class KerasLegacyAdam:
     def __init__(self, lr=1.0, beta_1=0.9, beta_2=0.999, epsilon=1e-7, clipnorm=None):
         self.lr, self.b1, self.b2, self.eps, self.clipnorm = lr, beta_1, beta_2, epsilon, clipnorm
         self.iterations = 0
-        self.slots: dict[int, tuple[torch.Tensor, torch.Tensor]] = {}
+        self.slots: dict[int, tuple[torch.Tensor, torch.Tensor, torch.Tensor]] = {}
 
     def apply_gradients(self, grads_and_vars):
         t = self.iterations + 1
@@ -285,10 +285,13 @@ class KerasLegacyAdam:
             if self.clipnorm is not None:
                 n = torch.sqrt(torch.sum(g.to(torch.float64) ** 2)).to(g.dtype)
                 g = g * self.clipnorm / torch.maximum(n, torch.tensor(self.clipnorm, dtype=g.dtype))
+            # slots are keyed by the variable object; holding the variable in its
+            # slot keeps its id from being reused by a later variable (TF variables
+            # have unique handles, so a new variable always gets fresh slots)
             key = id(x)
-            if key not in self.slots:
-                self.slots[key] = (torch.zeros_like(x), torch.zeros_like(x))
-            m, v = self.slots[key]
+            if key not in self.slots or self.slots[key][0] is not x:
+                self.slots[key] = (x, torch.zeros_like(x), torch.zeros_like(x))
+            _, m, v = self.slots[key]
             one = torch.tensor(1.0, dtype=dt)
             b1p = torch.tensor(self.b1, dtype=dt) ** t
             b2p = torch.tensor(self.b2, dtype=dt) ** t

@@ -247,9 +247,10 @@ class _LegacyAdam:
                 if self.clipnorm is not None:
                     n = torch.sqrt(torch.sum(g.to(torch.float64) ** 2)).to(dt)
                     g = g * self.clipnorm / torch.maximum(n, torch.tensor(self.clipnorm, dtype=dt))
-                if id(x) not in self._slots:
-                    self._slots[id(x)] = (torch.zeros_like(x), torch.zeros_like(x))
-                m, v = self._slots[id(x)]
+                # keyed by the variable object (held in the slot so its id is never reused)
+                if id(x) not in self._slots or self._slots[id(x)][0] is not x:
+                    self._slots[id(x)] = (x, torch.zeros_like(x), torch.zeros_like(x))
+                _, m, v = self._slots[id(x)]
                 one = torch.tensor(1.0, dtype=dt)
                 alpha = float(self.lr) * torch.sqrt(one - torch.tensor(self.beta_2, dtype=dt) ** t) / (
                     one - torch.tensor(self.beta_1, dtype=dt) ** t)
