@@ -74,6 +74,7 @@ SIGNATURES = {
     "igm_workspace_size": (C.c_size_t, [C.POINTER(Grid)]),
     "igm_energy": (I, [I, C.POINTER(Grid), C.POINTER(Physics), C.POINTER(Fields), P, P, P, P, D, P, P,
                        C.c_size_t, P]),
+    "igm_energy_noalloc": (I, [I, C.POINTER(Grid), C.POINTER(Physics), C.POINTER(Fields), P, P, P, P, D, P, P]),
     "igm_solver_begin": (I, [P, C.c_int64, P]),
     "igm_solver_iterate": (I, [I, C.POINTER(Grid), C.POINTER(Physics), C.POINTER(Fields), P, P, P, P, P, P, P, P,
                                C.POINTER(Adam), C.POINTER(EarlyStop), I, I, P, P, P, C.c_size_t, P]),

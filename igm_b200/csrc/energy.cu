@@ -30,6 +30,8 @@
 // order (deterministic) and, in solver mode, runs EarlyStopping on the device.
 #include <stdarg.h>
 
+#include <mutex>
+
 #include "common.cuh"
 
 namespace igm {
@@ -647,9 +649,79 @@ __global__ void solver_begin_kernel(igm_solver_ctl* ctl, long long t0) {
   ctl->terms[0] = ctl->terms[1] = ctl->terms[2] = 0.0;
 }
 
+// ---------------------------------------------------------------------------
+// Reduction scratch of igm_energy_noalloc: a fixed array inside the library.
+// The first 256 bytes hold the CTA counter, the rest the per-CTA FP64
+// partial sums.  Every device that loads the library keeps this array until
+// the process exits.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = (size_t)2 << 20;  // 2 MiB
+static __device__ __align__(256) unsigned char g_energy_scratch[kNoAllocScratchBytes];
+
+// Device address of g_energy_scratch for the current device.  In host code the
+// array's name only stands in for the symbol; the address is looked up once per
+// device (with that device current) and cached.
+static int noalloc_scratch(void** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    set_error("igm_energy_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+    return IGM_ERR_CUDA;
+  }
+  constexpr int kMaxDevices = 128;
+  static std::mutex mu;
+  static void* addr[kMaxDevices] = {};
+  IGM_CHECK_ARG(dev >= 0 && dev < kMaxDevices, IGM_ERR_CUDA, "igm_energy_noalloc: device index %d out of range", dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (addr[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_energy_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      set_error("igm_energy_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+      return IGM_ERR_CUDA;
+    }
+    addr[dev] = p;
+  }
+  *out = addr[dev];
+  return IGM_OK;
+}
+
 }  // namespace igm
 
 using namespace igm;
+
+extern "C" int igm_energy_noalloc(int dtype, const igm_grid* grid, const igm_physics* phys, const igm_fields* fields,
+                                  const void* U, const void* V, void* dU, void* dV, double grad_scale, double* terms,
+                                  void* stream) {
+  int rc = check_grid(grid);
+  if (rc) return rc;
+  IGM_CHECK_ARG(phys && fields && U && V && terms, IGM_ERR_BAD_ARGUMENT, "igm_energy_noalloc: NULL argument");
+  IGM_CHECK_ARG((dU == nullptr) == (dV == nullptr), IGM_ERR_BAD_ARGUMENT,
+                "igm_energy_noalloc: dU and dV must both be set or both NULL");
+  IGM_CHECK_ARG(fields->thk && fields->usurf && fields->arrhenius && fields->slidingco, IGM_ERR_BAD_ARGUMENT,
+                "igm_energy_noalloc: NULL field");
+  IGM_CHECK_ARG(dtype == IGM_F32 || dtype == IGM_F64, IGM_ERR_BAD_ARGUMENT, "igm_energy_noalloc: unknown dtype %d",
+                dtype);
+  const size_t need = workspace_bytes_for(grid);
+  IGM_CHECK_ARG(need <= kNoAllocScratchBytes, IGM_ERR_WORKSPACE,
+                "igm_energy_noalloc: this grid (batch %d x %d x %d) needs %zu bytes of reduction scratch, more than "
+                "the library's fixed %zu-byte array; call igm_energy with a workspace instead",
+                grid->batch, grid->ny, grid->nx, need, kNoAllocScratchBytes);
+  void* ws = nullptr;
+  rc = noalloc_scratch(&ws);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  // The CTA counter must start at zero.  Kernels leave it at zero, but a call
+  // that failed part-way could not; clearing it costs one 256-byte memset.
+  cudaError_t e = cudaMemsetAsync(ws, 0, 256, st);
+  if (e != cudaSuccess) {
+    set_error("igm_energy_noalloc: clearing the counter: %s", cudaGetErrorString(e));
+    return IGM_ERR_CUDA;
+  }
+  if (dtype == IGM_F32)
+    return energy_t<float>(grid, phys, fields, U, V, dU, dV, grad_scale, terms, ws, kNoAllocScratchBytes, st);
+  return energy_t<double>(grid, phys, fields, U, V, dU, dV, grad_scale, terms, ws, kNoAllocScratchBytes, st);
+}
 
 extern "C" size_t igm_workspace_size(const igm_grid* grid) {
   if (check_grid(grid) != IGM_OK) return 0;

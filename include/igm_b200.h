@@ -154,6 +154,27 @@ IGM_API int igm_energy(int dtype, const igm_grid* grid, const igm_physics* phys,
                const void* U, const void* V, void* dU, void* dV, double grad_scale, double* terms,
                void* workspace, size_t workspace_bytes, void* stream);
 
+/* Same computation and results as igm_energy, for callers that cannot
+ * allocate device memory: a host model that has already handed all device
+ * memory to its own pool, or code that must not call cudaMalloc/cudaFree
+ * because those calls may synchronise the device.  No counterpart in the
+ * reference (its TensorFlow ops allocate their temporaries).
+ *  - No workspace argument and no allocation: the reduction scratch is a fixed
+ *    2 MiB array compiled into the library, held by every device that loads
+ *    the library until the process exits.  A grid needing more scratch than
+ *    that (roughly more than 87,000 CTAs of 31 x 7 nodes, e.g. 4096 x 4096 with
+ *    batch 2) is rejected with IGM_ERR_WORKSPACE and no launch.
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) with that device current; make that first call
+ *    before any stream capture.
+ *  - All calls share the one array, which keeps the last call's contents;
+ *    each call clears the counter it needs at zero on its stream.  Calls that
+ *    overlap on the GPU (other streams, other host threads) race on the array:
+ *    order them on one stream. */
+IGM_API int igm_energy_noalloc(int dtype, const igm_grid* grid, const igm_physics* phys, const igm_fields* fields,
+                               const void* U, const void* V, void* dU, void* dV, double grad_scale, double* terms,
+                               void* stream);
+
 /* ---------------------------------------------------------------------------
  * Plain solver: n_iterations fused iterations of
  *   COST, grad = energy_and_gradient(U, V); Adam.apply_gradients;
