@@ -91,9 +91,11 @@ SIGNATURES = {
     "igm_cnn_param_offset": (C.c_size_t, [I, I, I, I, I]),
     "igm_cnn_pack_weights": (I, [I, I, I, P, P, P, P]),
     "igm_cnn_input": (I, [I, I, I, I, I, P, P, P, P, D, P, P, P, P, P, P, P, P, P]),
-    "igm_cnn_head_forward": (I, [I, I, I, I, P, P, P, P, P, P, P]),
+    "igm_cnn_layer1_forward": (I, [I, I, I, I, P, P, P, P, D, P, P, P, C.c_float, P, P]),
+    "igm_cnn_layer1_wgrad": (I, [I, I, I, I, P, P, P, P, D, P, P, P, I, P]),
+    "igm_cnn_head_forward": (I, [I, I, I, I, P, P, P, C.c_float, P, P, P, P]),
     "igm_cnn_head_partial_len": (C.c_size_t, [I]),
-    "igm_cnn_head_backward": (I, [I, I, I, I, P, P, P, P, C.c_float, P, P, I, P]),
+    "igm_cnn_head_backward": (I, [I, I, I, I, P, P, P, P, C.c_float, C.c_float, P, P, I, P]),
     "igm_reduce_partials": (I, [P, I, I, I, P, I, P]),
     "igm_cnn_wgrad_finish": (I, [P, I, I, I, P, P]),
     "igm_adam_clipnorm": (I, [I, P, P, P, P, P, P, D, D, D, D, D, C.c_int64, P]),

@@ -29,12 +29,13 @@ class CNN:
     [32] per layer; head kernel [1,1,32,nout], bias [nout])."""
 
     def __init__(self, nb_layers=16, cin=5, nout=20, alpha=0.01, init="glorot_uniform", seed=0,
-                 scales=(1.0, 1.0, 1.0, 1.0, 1.0), device="cuda", nb_out_filter=32):
+                 scales=(1.0, 1.0, 1.0, 1.0, 1.0), device="cuda", nb_out_filter=32, out_scale=1.0):
         if nb_out_filter != F:
             raise NotImplementedError(f"nb_out_filter={nb_out_filter}: only 32 filters are supported")
         if cin > 8:
             raise NotImplementedError("at most 8 input fields")
         self.L, self.cin, self.nout, self.alpha = int(nb_layers), int(cin), int(nout), float(alpha)
+        self.out_scale = float(out_scale)  # the head's outputs are multiplied by this fixed factor
         self.nz = self.nout // 2
         self.device = torch.device(device)
         self.scales = np.asarray(list(scales) + [1.0] * (5 - len(scales)), dtype=np.float32)[:5]
@@ -65,9 +66,10 @@ class CNN:
         self.n_sm = int(lib.igm_conv_sm_count())
 
     # ---- parameters ------------------------------------------------------
-    def init_weights(self, init="glorot_uniform", seed=0):
+    def init_weights(self, init="glorot_uniform", seed=0, head_gain=1.0):
         """Keras initialisers: glorot_uniform (the reference default,
-        iceflow.yaml weight_initialization) or he_normal / he_uniform; biases zero."""
+        iceflow.yaml weight_initialization) or he_normal / he_uniform; biases
+        zero.  ``head_gain`` multiplies the head kernel's initial values."""
         rng = np.random.default_rng(seed)
         host = np.zeros(self.n_params, dtype=np.float32)
         for i, s in enumerate(self.shapes):
@@ -86,6 +88,8 @@ class CNN:
                 w = rng.uniform(-lim, lim, size=s)
             else:
                 raise NotImplementedError(f"weight_initialization={init!r}")
+            if i == len(self.shapes) - 2:
+                w = w * head_gain
             host[self.offsets[i]:self.offsets[i + 1]] = w.astype(np.float32).ravel()
         self.set_params(host)
 
@@ -122,7 +126,7 @@ class CNN:
         if b is None:
             d = self.device
             act = lambda c: torch.empty((B, h, c // 8, w, 8), dtype=torch.bfloat16, device=d)
-            b = {"X": act(16), "acts": [act(F) for _ in range(self.L if train else 2)]}
+            b = {"acts": [act(F) for _ in range(self.L if train else 2)]}
             b["U"] = torch.empty((B, self.nz, h, w), dtype=torch.float32, device=d)
             b["V"] = torch.empty_like(b["U"])
             b["fields"] = [torch.empty((B, h, w), dtype=torch.float32, device=d) for _ in range(4)]
@@ -146,17 +150,25 @@ class CNN:
         x0 = (C.c_int * B)(*[int(b) for _, b in windows])
         sc = (C.c_float * 5)(*[float(s) for s in self.scales])
         rc = L.lib().igm_cnn_input(B, h, w, ny, nx, *[_p(f) for f in fields_full], float(dx), sc, y0, x0,
-                                   _p(buf["X"]), *[_p(f) for f in buf["fields"]], L.stream_ptr())
+                                   None, *[_p(f) for f in buf["fields"]], L.stream_ptr())
         L.check(rc, "igm_cnn_input")
+        buf["dx"] = float(dx)
+
+    def _scales(self):
+        return (C.c_float * 5)(*[float(s) for s in self.scales])
 
     def forward(self, buf, B, h, w, thk_mask=None, keep_acts=False):
-        """Runs the conv stack and the head on buf["X"]; U, V into buf."""
+        """Runs the network on the windowed fields of ``buf`` (prepare_input):
+        the FP32 first layer, the tensor-core layers, the head; U, V into buf."""
         lib, st = L.lib(), L.stream_ptr()
         acts = buf["acts"]
-        x = buf["X"]
-        cin_t = 16
+        rc = lib.igm_cnn_layer1_forward(B, h, w, self.cin, *[_p(f) for f in buf["fields"]], buf["dx"], self._scales(),
+                                        self.params.data_ptr(), self._b(0), self.alpha, _p(acts[0]), st)
+        L.check(rc, "igm_cnn_layer1_forward")
+        x = acts[0]
+        cin_t = F
         hook = self.event_hook if (self.event_hook is not None and not keep_acts) else None
-        for l in range(self.L):
+        for l in range(1, self.L):
             y = acts[l] if keep_acts else acts[l % 2]
             if hook is not None and l > 0:
                 ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -170,7 +182,8 @@ class CNN:
             x, cin_t = y, F
         hw = self.params.data_ptr() + 4 * self.offsets[2 * self.L]
         hb = self.params.data_ptr() + 4 * self.offsets[2 * self.L + 1]
-        rc = lib.igm_cnn_head_forward(B, h, w, self.nz, _p(x), hw, hb, _p(buf["U"]), _p(buf["V"]), _p(thk_mask), st)
+        rc = lib.igm_cnn_head_forward(B, h, w, self.nz, _p(x), hw, hb, self.out_scale, _p(buf["U"]), _p(buf["V"]),
+                                      _p(thk_mask), st)
         L.check(rc, "igm_cnn_head_forward")
         return buf["U"], buf["V"]
 
@@ -184,8 +197,8 @@ class CNN:
         hw = self.params.data_ptr() + 4 * self.offsets[2 * self.L]
         hl = buf["hpart"].shape[1]
         g = buf["g"]
-        rc = lib.igm_cnn_head_backward(B, h, w, self.nz, _p(acts[self.L - 1]), hw, _p(dU), _p(dV), self.alpha,
-                                       _p(g[0]), _p(buf["hpart"]), npart, st)
+        rc = lib.igm_cnn_head_backward(B, h, w, self.nz, _p(acts[self.L - 1]), hw, _p(dU), _p(dV), self.out_scale,
+                                       self.alpha, _p(g[0]), _p(buf["hpart"]), npart, st)
         L.check(rc, "igm_cnn_head_backward")
         gp = self.grads.data_ptr()
         nh = F * self.nout
@@ -197,13 +210,19 @@ class CNN:
         cur = 0
         for l in range(self.L - 1, -1, -1):
             gl = g[cur]
-            xin = acts[l - 1] if l > 0 else buf["X"]
-            cin_t = F if l > 0 else 16
-            rc = lib.igm_conv3x3_wgrad(B, h, w, cin_t, _p(xin), _p(gl), _p(buf["wpart"]), npart, _p(self.err), st)
-            L.check(rc, f"igm_conv3x3_wgrad layer {l}")
-            rc = lib.igm_cnn_wgrad_finish(_p(buf["wpart"]), npart, self.cin if l == 0 else F, cin_t,
-                                          gp + 4 * self.offsets[2 * l], st)
-            L.check(rc, "igm_cnn_wgrad_finish")
+            if l > 0:
+                rc = lib.igm_conv3x3_wgrad(B, h, w, F, _p(acts[l - 1]), _p(gl), _p(buf["wpart"]), npart,
+                                           _p(self.err), st)
+                L.check(rc, f"igm_conv3x3_wgrad layer {l}")
+                rc = lib.igm_cnn_wgrad_finish(_p(buf["wpart"]), npart, F, F, gp + 4 * self.offsets[2 * l], st)
+                L.check(rc, "igm_cnn_wgrad_finish")
+            else:
+                n1 = 9 * self.cin * F
+                rc = lib.igm_cnn_layer1_wgrad(B, h, w, self.cin, *[_p(f) for f in buf["fields"]], buf["dx"],
+                                              self._scales(), _p(gl), _p(buf["wpart"]), npart, st)
+                L.check(rc, "igm_cnn_layer1_wgrad")
+                L.check(lib.igm_reduce_partials(_p(buf["wpart"]), npart, n1, n1, gp + 4 * self.offsets[0], 0, st),
+                        "reduce layer-1 wgrad")
             if l > 0:
                 nxt = g[1 - cur]
                 buf["dbpart"].zero_()

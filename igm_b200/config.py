@@ -65,6 +65,8 @@ DEFAULTS = {
             "input_scales": [1.0, 1.0, 1.0, 1.0, 1.0],
             # (igm_b200) weight seed for networks built from scratch
             "seed": 0,
+            # (igm_b200) fixed factor multiplying the head's output (m/a); 1.0 = raw, as the reference
+            "output_scale": 1.0,
             "network": {
                 "architecture": "cnn",
                 "multiple_window_size": 0,

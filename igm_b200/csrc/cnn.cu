@@ -113,16 +113,18 @@ __global__ void input_kernel(const InputArgs a) {
       v[c] = a.f[c][src];
       if (a.out[c]) a.out[c][i] = v[c];
     }
-    uint4 c0, c1;
-    c0.x = bf_pack(v[0] * a.scale[0], v[1] * a.scale[1]);
-    c0.y = bf_pack(v[2] * a.scale[2], v[3] * a.scale[3]);
-    c0.z = bf_pack(a.dx * a.scale[4], 0.f);
-    c0.w = 0u;
-    c1.x = c1.y = c1.z = c1.w = 0u;
-    uint4* X = reinterpret_cast<uint4*>(a.X);
-    const size_t row = ((size_t)b * a.h + y) * 2;
-    X[(row + 0) * a.w + x] = c0;
-    X[(row + 1) * a.w + x] = c1;
+    if (a.X) {
+      uint4 c0, c1;
+      c0.x = bf_pack(v[0] * a.scale[0], v[1] * a.scale[1]);
+      c0.y = bf_pack(v[2] * a.scale[2], v[3] * a.scale[3]);
+      c0.z = bf_pack(a.dx * a.scale[4], 0.f);
+      c0.w = 0u;
+      c1.x = c1.y = c1.z = c1.w = 0u;
+      uint4* X = reinterpret_cast<uint4*>(a.X);
+      const size_t row = ((size_t)b * a.h + y) * 2;
+      X[(row + 0) * a.w + x] = c0;
+      X[(row + 1) * a.w + x] = c1;
+    }
   }
 }
 
@@ -131,8 +133,8 @@ __global__ void input_kernel(const InputArgs a) {
 // (Y_to_UV: channels [0,Nz) are U, [Nz, 2Nz) are V), masked where thk <= 0
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) head_fwd_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act,
-                                                       const float* wh, const float* bh, float* U, float* V,
-                                                       const float* thk_mask) {
+                                                       const float* wh, const float* bh, float out_scale, float* U,
+                                                       float* V, const float* thk_mask) {
   extern __shared__ float sw[];  // [32][2nz] then bias [2nz]
   const int nout = 2 * nz;
   for (int i = threadIdx.x; i < kF * nout; i += blockDim.x) sw[i] = wh[i];
@@ -161,7 +163,7 @@ __global__ void __launch_bounds__(256) head_fwd_kernel(int B, int H, int W, int 
       float s = 0.f;
 #pragma unroll
       for (int ci = 0; ci < kF; ++ci) s = fmaf(av[ci], sw[ci * nout + j], s);
-      s += sw[kF * nout + j];
+      s = (s + sw[kF * nout + j]) * out_scale;
       if (!keep) s = 0.f;
       float* dst = j < nz ? U : V;
       const int k = j < nz ? j : j - nz;
@@ -178,7 +180,8 @@ __global__ void __launch_bounds__(256) head_fwd_kernel(int B, int H, int W, int 
 constexpr int kHB = 128;  // pixels per chunk
 __global__ void __launch_bounds__(256) head_bwd_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act,
                                                        const float* wh, const float* dU, const float* dV,
-                                                       float alpha, __nv_bfloat16* dpre, float* partial) {
+                                                       float out_scale, float alpha, __nv_bfloat16* dpre,
+                                                       float* partial) {
   extern __shared__ float sm[];
   const int nout = 2 * nz;
   float* sw = sm;                          // [32][nout]
@@ -222,7 +225,7 @@ __global__ void __launch_bounds__(256) head_bwd_kernel(int B, int H, int W, int 
         for (int j = 0; j < nout; ++j) {
           const float* src = j < nz ? dU : dV;
           const int k = j < nz ? j : j - nz;
-          const float g = src[((size_t)b * nz + k) * plane + rem];
+          const float g = src[((size_t)b * nz + k) * plane + rem] * out_scale;
           sD[t * (nout + 1) + j] = g;
 #pragma unroll
           for (int ci = 0; ci < kF; ++ci) da[ci] = fmaf(g, sw[ci * nout + j], da[ci]);
@@ -281,6 +284,143 @@ __global__ void __launch_bounds__(256) head_bwd_kernel(int B, int H, int W, int 
   }
   if (threadIdx.x < nout) out[npairs + threadIdx.x] = accb;
   if (threadIdx.x >= 128 && threadIdx.x < 128 + kF) out[npairs + nout + threadIdx.x - 128] = accd;
+}
+
+// ---------------------------------------------------------------------------
+// First layer in FP32 on CUDA cores: the raw fields (surface elevation of
+// ~3000 m varying by a few metres per cell) cannot be rounded to BF16 without
+// losing the surface slope that drives the flow, so the 5 -> 32 layer reads
+// the FP32 fields and writes BF16 activations.  Input channels in fieldin
+// order: thk, usurf, arrhenius, slidingco (windowed copies [B][H][W]) and the
+// constant dX channel; zero outside the window ("same" padding of X).
+// ---------------------------------------------------------------------------
+struct L1Args {
+  int B, H, W, cin;
+  const float* f[4];
+  float dxs;        // dx * scale of the dX channel
+  float scale[4];   // fixed input scales
+  const float* w;   // [3][3][cin][32]
+  const float* b;   // [32]
+  float alpha;
+  __nv_bfloat16* out;  // [B][H][4][W][8]
+};
+
+__device__ __forceinline__ void l1_inputs(const L1Args& a, int b, int y, int x, float (&in)[9][5]) {
+#pragma unroll
+  for (int t = 0; t < 9; ++t) {
+    const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
+    const bool ok = yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
+    const size_t o = ((size_t)b * a.H + (ok ? yy : 0)) * a.W + (ok ? xx : 0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) in[t][c] = ok ? a.f[c][o] * a.scale[c] : 0.f;
+    in[t][4] = ok ? a.dxs : 0.f;
+  }
+}
+
+__global__ void __launch_bounds__(256) layer1_fwd_kernel(const L1Args a) {
+  __shared__ float sw[9 * 5 * kF + kF];
+  for (int i = threadIdx.x; i < 9 * a.cin * kF; i += blockDim.x) sw[i] = a.w[i];
+  if (threadIdx.x < kF) sw[9 * 5 * kF + threadIdx.x] = a.b[threadIdx.x];
+  __syncthreads();
+  const size_t plane = (size_t)a.H * a.W;
+  const size_t total = plane * a.B;
+  uint4* O = reinterpret_cast<uint4*>(a.out);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(i / plane);
+    const size_t rem = i - (size_t)b * plane;
+    const int y = (int)(rem / a.W), x = (int)(rem - (size_t)y * a.W);
+    float in[9][5];
+    l1_inputs(a, b, y, x, in);
+    float acc[kF];
+#pragma unroll
+    for (int co = 0; co < kF; ++co) acc[co] = sw[9 * 5 * kF + co];
+#pragma unroll
+    for (int t = 0; t < 9; ++t)
+      for (int c = 0; c < a.cin; ++c) {
+        const float v = in[t][c];
+        const float* wr = &sw[(t * a.cin + c) * kF];
+#pragma unroll
+        for (int co = 0; co < kF; ++co) acc[co] = fmaf(v, wr[co], acc[co]);
+      }
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+      float z[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const float v = acc[ch * 8 + e];
+        z[e] = v > 0.f ? v : a.alpha * v;
+      }
+      uint4 o;
+      o.x = bf_pack(z[0], z[1]);
+      o.y = bf_pack(z[2], z[3]);
+      o.z = bf_pack(z[4], z[5]);
+      o.w = bf_pack(z[6], z[7]);
+      O[(((size_t)b * a.H + y) * 4 + ch) * a.W + x] = o;
+    }
+  }
+}
+
+// dW1[t][c][co] = sum_p X[p + off(t)][c] * G[p][co], per-block partials [9*cin*32]
+constexpr int kL1P = 64;  // pixels per chunk
+__global__ void __launch_bounds__(256) layer1_wgrad_kernel(const L1Args a, const __nv_bfloat16* g, float* partial) {
+  __shared__ float sX[kL1P][46];
+  __shared__ float sG[kL1P][kF + 1];
+  const int nw = 9 * a.cin * kF;
+  constexpr int kPer = (9 * 5 * kF + 255) / 256;
+  float acc[kPer];
+#pragma unroll
+  for (int r = 0; r < kPer; ++r) acc[r] = 0.f;
+  const size_t plane = (size_t)a.H * a.W;
+  const size_t total = plane * a.B;
+  const size_t nchunks = (total + kL1P - 1) / kL1P;
+  const uint4* G = reinterpret_cast<const uint4*>(g);
+  for (size_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+    const int t = threadIdx.x;
+    if (t < kL1P) {
+      const size_t i = chunk * kL1P + t;
+      if (i < total) {
+        const int b = (int)(i / plane);
+        const size_t rem = i - (size_t)b * plane;
+        const int y = (int)(rem / a.W), x = (int)(rem - (size_t)y * a.W);
+        float in[9][5];
+        l1_inputs(a, b, y, x, in);
+#pragma unroll
+        for (int tp = 0; tp < 9; ++tp)
+#pragma unroll
+          for (int c = 0; c < 5; ++c) sX[t][tp * 5 + c] = in[tp][c];
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch) {
+          const uint4 u = G[(((size_t)b * a.H + y) * 4 + ch) * a.W + x];
+          const uint32_t wv[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            sG[t][ch * 8 + 2 * e] = bf_lo(wv[e]);
+            sG[t][ch * 8 + 2 * e + 1] = bf_hi(wv[e]);
+          }
+        }
+      } else {
+        for (int k = 0; k < 45; ++k) sX[t][k] = 0.f;
+        for (int k = 0; k < kF; ++k) sG[t][k] = 0.f;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kPer; ++r) {
+      const int o = threadIdx.x + r * 256;
+      if (o < nw) {
+        const int co = o % kF, c = (o / kF) % a.cin, tp = o / (kF * a.cin);
+        float sacc = 0.f;
+        for (int p = 0; p < kL1P; ++p) sacc = fmaf(sX[p][tp * 5 + c], sG[p][co], sacc);
+        acc[r] += sacc;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < kPer; ++r) {
+    const int o = threadIdx.x + r * 256;
+    if (o < nw) partial[(size_t)blockIdx.x * nw + o] = acc[r];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -385,7 +525,7 @@ extern "C" int igm_cnn_input(int batch, int h, int w, int ny, int nx, const floa
                              float* arrhenius_out, float* slidingco_out, void* stream) {
   IGM_CHECK_ARG(batch >= 1 && batch <= IGM_MAX_WINDOWS && h >= 1 && w >= 1, IGM_ERR_BAD_SHAPE,
                 "igm_cnn_input: bad shape (batch must be <= %d)", IGM_MAX_WINDOWS);
-  IGM_CHECK_ARG(thk && usurf && arrhenius && slidingco && scales && win_y0 && win_x0 && X, IGM_ERR_BAD_ARGUMENT,
+  IGM_CHECK_ARG(thk && usurf && arrhenius && slidingco && scales && win_y0 && win_x0, IGM_ERR_BAD_ARGUMENT,
                 "igm_cnn_input: NULL argument");
   InputArgs a{};
   a.B = batch; a.h = h; a.w = w; a.Ny = ny; a.Nx = nx;
@@ -404,22 +544,64 @@ extern "C" int igm_cnn_input(int batch, int h, int w, int ny, int nx, const floa
   return launch_status("input_kernel");
 }
 
+static int l1_args(L1Args* a, int batch, int h, int w, int cin, const float* thk, const float* usurf,
+                   const float* arrhenius, const float* slidingco, double dx, const float* scales, const float* w1,
+                   const float* b1, float alpha) {
+  IGM_CHECK_ARG(batch >= 1 && h >= 1 && w >= 1 && cin >= 1 && cin <= 5, IGM_ERR_BAD_SHAPE,
+                "igm_cnn_layer1: bad shape (cin must be 1..5)");
+  IGM_CHECK_ARG(thk && usurf && arrhenius && slidingco && scales && w1, IGM_ERR_BAD_ARGUMENT,
+                "igm_cnn_layer1: NULL argument");
+  a->B = batch; a->H = h; a->W = w; a->cin = cin;
+  a->f[0] = thk; a->f[1] = usurf; a->f[2] = arrhenius; a->f[3] = slidingco;
+  for (int c = 0; c < 4; ++c) a->scale[c] = scales[c];
+  a->dxs = (float)dx * scales[4];
+  a->w = w1;
+  a->b = b1;
+  a->alpha = alpha;
+  return IGM_OK;
+}
+
+extern "C" int igm_cnn_layer1_forward(int batch, int h, int w, int cin, const float* thk, const float* usurf,
+                                      const float* arrhenius, const float* slidingco, double dx, const float* scales,
+                                      const float* w1, const float* b1, float alpha, void* act, void* stream) {
+  L1Args a{};
+  int rc = l1_args(&a, batch, h, w, cin, thk, usurf, arrhenius, slidingco, dx, scales, w1, b1, alpha);
+  if (rc) return rc;
+  IGM_CHECK_ARG(b1 && act, IGM_ERR_BAD_ARGUMENT, "igm_cnn_layer1_forward: NULL argument");
+  a.out = (__nv_bfloat16*)act;
+  layer1_fwd_kernel<<<grid_for((size_t)batch * h * w), 256, 0, as_stream(stream)>>>(a);
+  return launch_status("layer1_fwd_kernel");
+}
+
+extern "C" int igm_cnn_layer1_wgrad(int batch, int h, int w, int cin, const float* thk, const float* usurf,
+                                    const float* arrhenius, const float* slidingco, double dx, const float* scales,
+                                    const void* g, float* partials, int n_parts, void* stream) {
+  L1Args a{};
+  const float dummy = 0.f;
+  int rc = l1_args(&a, batch, h, w, cin, thk, usurf, arrhenius, slidingco, dx, scales, &dummy, nullptr, 0.f);
+  if (rc) return rc;
+  IGM_CHECK_ARG(g && partials && n_parts >= 1, IGM_ERR_BAD_ARGUMENT, "igm_cnn_layer1_wgrad: bad argument");
+  layer1_wgrad_kernel<<<n_parts, 256, 0, as_stream(stream)>>>(a, (const __nv_bfloat16*)g, partials);
+  return launch_status("layer1_wgrad_kernel");
+}
+
 extern "C" int igm_cnn_head_forward(int batch, int h, int w, int nz, const void* act, const float* head_w,
-                                    const float* head_b, float* U, float* V, const float* thk_mask, void* stream) {
+                                    const float* head_b, float out_scale, float* U, float* V, const float* thk_mask,
+                                    void* stream) {
   IGM_CHECK_ARG(batch >= 1 && h >= 1 && w >= 1 && nz >= 1 && nz <= IGM_MAX_NZ, IGM_ERR_BAD_SHAPE,
                 "igm_cnn_head_forward: bad shape");
   IGM_CHECK_ARG(act && head_w && head_b && U && V, IGM_ERR_BAD_ARGUMENT, "igm_cnn_head_forward: NULL argument");
   const size_t smem = (size_t)(kF * 2 * nz + 2 * nz) * sizeof(float);
   head_fwd_kernel<<<grid_for((size_t)batch * h * w), 256, smem, as_stream(stream)>>>(
-      batch, h, w, nz, (const __nv_bfloat16*)act, head_w, head_b, U, V, thk_mask);
+      batch, h, w, nz, (const __nv_bfloat16*)act, head_w, head_b, out_scale, U, V, thk_mask);
   return launch_status("head_fwd_kernel");
 }
 
 extern "C" size_t igm_cnn_head_partial_len(int nz) { return (size_t)kF * 2 * nz + 2 * nz + kF; }
 
 extern "C" int igm_cnn_head_backward(int batch, int h, int w, int nz, const void* act, const float* head_w,
-                                     const float* dU, const float* dV, float alpha, void* dpre, float* partials,
-                                     int n_parts, void* stream) {
+                                     const float* dU, const float* dV, float out_scale, float alpha, void* dpre,
+                                     float* partials, int n_parts, void* stream) {
   IGM_CHECK_ARG(batch >= 1 && h >= 1 && w >= 1 && nz >= 1 && nz <= IGM_MAX_NZ && n_parts >= 1, IGM_ERR_BAD_SHAPE,
                 "igm_cnn_head_backward: bad shape");
   IGM_CHECK_ARG(act && head_w && dU && dV && dpre && partials, IGM_ERR_BAD_ARGUMENT,
@@ -436,7 +618,7 @@ extern "C" int igm_cnn_head_backward(int batch, int h, int w, int nz, const void
     configured = smem;
   }
   head_bwd_kernel<<<n_parts, 256, smem, as_stream(stream)>>>(batch, h, w, nz, (const __nv_bfloat16*)act, head_w, dU,
-                                                            dV, alpha, (__nv_bfloat16*)dpre, partials);
+                                                            dV, out_scale, alpha, (__nv_bfloat16*)dpre, partials);
   return launch_status("head_bwd_kernel");
 }
 

@@ -69,7 +69,7 @@ def initialize_iceflow_emulator(cfg, state):
     state.iceflow_model = CNN(nb_layers=int(net.nb_layers), cin=nb_inputs, nout=2 * int(ic.numerics.Nz),
                               init=net.weight_initialization, seed=int(e.get("seed", 0)),
                               scales=list(e.get("input_scales", [1.0] * 5)), device=thk.device,
-                              nb_out_filter=int(net.nb_out_filter))
+                              nb_out_filter=int(net.nb_out_filter), out_scale=float(e.get("output_scale", 1.0)))
     loaded = False
     if e.pretrained and e.name:
         path = os.path.join(getattr(state, "original_cwd", os.getcwd()), e.name)
@@ -227,7 +227,7 @@ def save_iceflow_model(cfg, state, directory="iceflow-model"):
     m: CNN = state.iceflow_model
     np.savez(os.path.join(directory, "model.npz"), params=m.params.cpu().numpy(), adam_m=m.m.cpu().numpy(),
              adam_v=m.v.cpu().numpy(), iterations=np.array(m.opt_iterations), nb_layers=np.array(m.L),
-             nout=np.array(m.nout), cin=np.array(m.cin), scales=m.scales)
+             nout=np.array(m.nout), cin=np.array(m.cin), scales=m.scales, out_scale=np.array(m.out_scale))
     with open(os.path.join(directory, "fieldin.dat"), "w") as fid:
         for key in cfg.processes.iceflow.emulator.fieldin:
             fid.write("%s \n" % key)
@@ -247,6 +247,8 @@ def load_iceflow_model(state, directory, cfg=None):
     m.v.copy_(torch.as_tensor(d["adam_v"]))
     m.opt_iterations = int(d["iterations"])
     m.scales = np.asarray(d["scales"], np.float32)
+    if "out_scale" in d.files:
+        m.out_scale = float(d["out_scale"])
     fin = os.path.join(directory, "fieldin.dat")
     if cfg is not None and os.path.exists(fin):
         with open(fin) as f:

@@ -291,26 +291,42 @@ IGM_API int igm_cnn_pack_weights(int nb_layers, int cin, int nout, const float* 
 /* Emulator input (fieldin_to_X, iceflow/utils.py:147-158, with split_into_patches
  * windows, emulate.py:283-308): X[b] = scaled (thk, usurf, arrhenius, slidingco, dx)
  * of the window at host (win_y0[b], win_x0[b]) of size h x w of the [ny][nx]
- * fields; optional fp32 copies of the windowed fields ([batch][h][w]).
- * scales: host float[5]. */
+ * fields (bf16, may be NULL) and fp32 copies of the windowed fields
+ * ([batch][h][w], each may be NULL).  scales: host float[5]. */
 IGM_API int igm_cnn_input(int batch, int h, int w, int ny, int nx, const float* thk, const float* usurf,
                           const float* arrhenius, const float* slidingco, double dx, const float* scales,
                           const int* win_y0, const int* win_x0, void* X, float* thk_out, float* usurf_out,
                           float* arrhenius_out, float* slidingco_out, void* stream);
 
-/* 1x1 head: U[b][k] = Y[..., k], V[b][k] = Y[..., nz + k] (Y_to_UV,
- * iceflow/utils.py:133-139), planar fp32 [batch][nz][h][w]; zero where
- * thk_mask <= 0 when thk_mask is not NULL (emulate.py:143-144). */
+/* First 3x3 layer in FP32 on CUDA cores, from the windowed FP32 fields
+ * (thk, usurf, arrhenius, slidingco [batch][h][w]) and the constant dX
+ * channel, scaled by host scales[5]: act = LeakyReLU(conv(X, w1) + b1), bf16
+ * row-chunked with 32 channels.  w1 is the Keras kernel [3][3][cin][32].
+ * BF16 inputs would lose the surface slope (metres on a ~3000 m surface). */
+IGM_API int igm_cnn_layer1_forward(int batch, int h, int w, int cin, const float* thk, const float* usurf,
+                                   const float* arrhenius, const float* slidingco, double dx, const float* scales,
+                                   const float* w1, const float* b1, float alpha, void* act, void* stream);
+/* Its weight gradient: per-block partials [n_parts][9 * cin * 32] of
+ * X^T G (G = gradient w.r.t. the layer's pre-activation, bf16 row-chunked). */
+IGM_API int igm_cnn_layer1_wgrad(int batch, int h, int w, int cin, const float* thk, const float* usurf,
+                                 const float* arrhenius, const float* slidingco, double dx, const float* scales,
+                                 const void* g, float* partials, int n_parts, void* stream);
+
+/* 1x1 head: Y = out_scale (A Wh + bh); U[b][k] = Y[..., k], V[b][k] =
+ * Y[..., nz + k] (Y_to_UV, iceflow/utils.py:133-139), planar fp32
+ * [batch][nz][h][w]; zero where thk_mask <= 0 when thk_mask is not NULL
+ * (emulate.py:143-144).  out_scale = 1 is the reference network. */
 IGM_API int igm_cnn_head_forward(int batch, int h, int w, int nz, const void* act, const float* head_w,
-                                 const float* head_b, float* U, float* V, const float* thk_mask, void* stream);
+                                 const float* head_b, float out_scale, float* U, float* V, const float* thk_mask,
+                                 void* stream);
 
 /* Backward of the head and of the last LeakyReLU: dpre (bf16 row-chunked) and
  * per-block partials [n_parts][igm_cnn_head_partial_len(nz)] = dWh [32][2nz],
  * dbh [2nz], db_last [32]. */
 IGM_API size_t igm_cnn_head_partial_len(int nz);
 IGM_API int igm_cnn_head_backward(int batch, int h, int w, int nz, const void* act, const float* head_w,
-                                  const float* dU, const float* dV, float alpha, void* dpre, float* partials,
-                                  int n_parts, void* stream);
+                                  const float* dU, const float* dV, float out_scale, float alpha, void* dpre,
+                                  float* partials, int n_parts, void* stream);
 
 /* out[i] (+)= sum_p partials[p * stride + i], i < len, fixed summation order. */
 IGM_API int igm_reduce_partials(const float* partials, int n_parts, int len, int stride, float* out,

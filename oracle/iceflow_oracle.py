@@ -449,7 +449,7 @@ def interp1d(xs, ys, x):
 # --------------------------------------------------------------------------
 
 
-def cnn_forward(X, weights, biases, alpha=0.01, bf16=False, return_acts=False):
+def cnn_forward(X, weights, biases, alpha=0.01, bf16=False, return_acts=False, bf16_first=True, out_scale=1.0):
     """Stack of Conv2D(3x3, same) + LeakyReLU, then a 1x1 Conv2D head.
 
     X : [B, H, W, Cin] (NHWC, as fieldin_to_X builds it);
@@ -465,7 +465,7 @@ def cnn_forward(X, weights, biases, alpha=0.01, bf16=False, return_acts=False):
     nl = len(weights) - 1
     for l in range(nl):
         w = weights[l].permute(3, 2, 0, 1)
-        if bf16:
+        if bf16 and (l > 0 or bf16_first):
             xin = x.to(torch.bfloat16).to(torch.float32)
             w = w.to(torch.bfloat16).to(torch.float32)
         else:
@@ -476,7 +476,7 @@ def cnn_forward(X, weights, biases, alpha=0.01, bf16=False, return_acts=False):
             x = x.to(torch.bfloat16).to(torch.float32)
         acts.append(x)
     w = weights[-1].permute(3, 2, 0, 1)
-    y = torch.nn.functional.conv2d(x, w, biases[-1])
+    y = torch.nn.functional.conv2d(x, w, biases[-1]) * out_scale
     y = y.permute(0, 2, 3, 1)
     return (y, acts) if return_acts else y
 

@@ -22,9 +22,12 @@ pytestmark = pytest.mark.gpu
 SCALES = [1 / 300.0, 1 / 3000.0, 1 / 100.0, 10.0, 1 / 100.0]
 
 
+OUT = 50.0
+
+
 def setup(nl=3, nz=4, ny=40, nx=70, seed=0):
     st = O.valley_glacier(ny, nx, 100.0, seed=seed, varying_coeffs=True)
-    net = CNN(nb_layers=nl, cin=5, nout=2 * nz, init="he_normal", seed=seed, scales=SCALES)
+    net = CNN(nb_layers=nl, cin=5, nout=2 * nz, init="he_normal", seed=seed, scales=SCALES, out_scale=OUT)
     # non-zero biases so that every bias path is exercised
     host = net.params.cpu().numpy()
     rng = np.random.default_rng(seed + 1)
@@ -55,7 +58,7 @@ def test_forward_matches_oracle(nl, nz, ny, nx):
     net.prepare_input(f, 100.0, [(0, 0)], ny, nx, buf)
     U, V = net.forward(buf, 1, ny, nx)
     ws, bs = oracle_params(net)
-    Y = O.cnn_forward(oracle_X(st, 100.0), ws, bs, bf16=True)
+    Y = O.cnn_forward(oracle_X(st, 100.0), ws, bs, bf16=True, bf16_first=False, out_scale=OUT)
     Uo, Vo = O.Y_to_UV(Y, nz)
     assert rel_l2(U.cpu().numpy(), Uo.numpy()) < 1e-2
     assert rel_l2(V.cpu().numpy(), Vo.numpy()) < 1e-2
@@ -80,7 +83,7 @@ def test_physics_gradient_and_adam_step_match_oracle():
         params += [w.clone().requires_grad_(True), b.clone().requires_grad_(True)]
     dz = O.compute_zeta_dzeta(O.compute_levels(nz, 4.0))[1]
     X = oracle_X(st, dx)
-    Y = O.cnn_forward(X, params[0::2], params[1::2], bf16=True)
+    Y = O.cnn_forward(X, params[0::2], params[1::2], bf16=True, bf16_first=False, out_scale=OUT)
     Uo, Vo = O.Y_to_UV(Y, nz)
     fl = [torch.as_tensor(st[k])[None] for k in ["thk", "usurf", "arrhenius", "slidingco"]]
     cost, _ = O.energy(Uo, Vo, *fl, dx, dz)
