@@ -6,26 +6,28 @@
 // data and weight gradients Keras' GradientTape computes for it
 // (emulate.py:252).
 //
-// Activation layout ("row-chunked"): bf16 [B][H][C/8][W][8].  One TMA box
-// {8, 130, C/8, R+2, 1} at (0, x0-1, 0, y0-1, b) lands in shared memory as
-// [row][chunk][pixel][8], which IS the canonical no-swizzle K-major UMMA
-// layout for "pixels x channels" (8-pixel core matrices of 16-byte rows).
-// Out-of-bounds rows/columns are zero-filled by TMA, which implements the
-// zero "same" padding.  Each of the nine taps is then just a shifted
-// descriptor start address: (row + dy) * row_stride + (dx) * 16 bytes.
+// Activation layout ("row-chunked"): bf16 [B][H][C/8][W][8].  A haloed input
+// tile (R+2 rows, 130 pixels) lands in shared memory as [row][chunk][pixel][8]
+// -- one ~2 KB bulk copy per (row, chunk), because each is contiguous in
+// global memory -- which IS the canonical no-swizzle K-major UMMA layout for
+// "pixels x channels" (8-pixel core matrices of 16-byte rows).  Rows/pixels
+// outside the domain are zero-filled (the zero "same" padding).  Each of the
+// nine taps is then just a shifted descriptor start address:
+// (row + dy) * row_stride + (dx) * 16 bytes.
 //
 // Forward / dgrad kernel (persistent, one CTA per SM, 6 warps):
-//   warp 0  TMA producer (and TMEM allocator),
+//   warp 0  producer: bulk copies of the input tile (and TMEM allocator),
 //   warp 1  MMA issuer: per tile R rows x 9 taps x C/16 MMAs of M=128 (pixels),
 //           N=32 (output channels), K=16 into R TMEM accumulators,
 //   warps 2-5 epilogue: TMEM -> registers (one pixel per thread), bias +
 //           LeakyReLU (forward) or the LeakyReLU derivative mask of the previous
 //           activation (dgrad, plus the bias-gradient partial sums), bf16 store.
-//   Two input stages and two accumulator sets overlap load, MMA and epilogue.
+//   Three input stages and two accumulator sets overlap load, MMA and epilogue.
 // Weight-gradient kernel: D[(input row, ci)][co] += X^T G over the pixels of
-// one output row, with both operands MN-major: M = 128 spans 128/(C/8*8)
-// consecutive input rows x C input channels (row stride = C/8 chunk strides,
-// so the M groups are uniformly strided), one accumulator per horizontal tap.
+// four output rows per work item, with both operands MN-major: M = 128 spans
+// 128/(C/8*8) consecutive input rows x C input channels (row stride = C/8
+// chunk strides, so the M groups are uniformly strided), one accumulator per
+// horizontal tap; the four output rows share one input tile of 3 + 4 rows.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -43,6 +45,7 @@ enum ConvEpi { kEpiFwdLeaky = 0, kEpiDgrad = 1 };
 struct ConvArgs {
   int B, H, W;
   int tiles_w, tiles_h, n_tiles;
+  const __nv_bfloat16* x;      // input activation [B][H][C8_IN][W][8]
   const __nv_bfloat16* wpack;  // [9][C8_IN][32][8]
   const float* bias;           // [32] (forward)
   const __nv_bfloat16* amask;  // dgrad: previous activation [B][H][4][W][8]
@@ -54,18 +57,62 @@ struct ConvArgs {
 
 template <int C8_IN, int R>
 struct ConvGeom {
+  static constexpr int NST = 3;                               // input stages
   static constexpr uint32_t P = kBoxW * 16;                   // chunk plane stride (bytes)
   static constexpr uint32_t RS = C8_IN * P;                   // row stride
   static constexpr uint32_t STAGE = (R + 2) * RS;             // one input stage
   static constexpr uint32_t WBYTES = 9 * C8_IN * kCout * 16;  // packed weights
-  static constexpr uint32_t OFF_W = 2 * STAGE;
+  static constexpr uint32_t OFF_W = NST * STAGE;
   static constexpr uint32_t OFF_BAR = OFF_W + WBYTES;
   static constexpr uint32_t TMEM_COLS = 2 * R * kCout;  // two accumulator sets
-  static constexpr uint32_t SMEM = OFF_BAR + 8 * 8 + 16 + 32 * 4 + 1024;
+  static constexpr uint32_t SMEM = OFF_BAR + 16 * 8 + 16 + 32 * 4 + 1024;
 };
 
 __device__ __forceinline__ void set_err(int* err, int code) {
   if (err) atomicExch(err, code);
+}
+
+// Loads, with one full warp, the tile of a row-chunked activation (bf16
+// [B][H][c8][W][8]) covering rows gy0 .. gy0+rows-1 and pixels gx0 .. gx0+npx-1
+// into shared memory as [row][chunk][pixel][8] (plane stride npx * 16 bytes).
+// Every (row, chunk) plane is one contiguous run in global memory: one lane
+// issues one bulk copy for its in-domain part; pixels and rows outside the
+// domain are zero-filled with shared-memory stores ("same" zero padding),
+// made visible to the tensor cores by a proxy fence before the arrival.
+// Lane 0 arrives on `bar` with the number of bytes the copies will deliver.
+__device__ __forceinline__ void load_tile(const __nv_bfloat16* act, int H, int W, int c8, int b, int gy0, int rows,
+                                          int gx0, int npx, unsigned char* dst, uint64_t* bar, int lane) {
+  const int nplanes = rows * c8;
+  const uint32_t P = (uint32_t)npx * 16;
+  const int xa = gx0 < 0 ? 0 : gx0;                // first in-domain pixel
+  const int xb = gx0 + npx > W ? W : gx0 + npx;     // one past the last
+  const uint32_t run = xb > xa ? (uint32_t)(xb - xa) * 16 : 0;
+  uint32_t mine = 0;
+  for (int p = lane; p < nplanes; p += 32) {
+    const int gy = gy0 + p / c8;
+    uint4* plane = reinterpret_cast<uint4*>(dst + (size_t)p * P);
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    if (gy < 0 || gy >= H || run == 0) {
+      for (int q = 0; q < npx; ++q) plane[q] = z;
+    } else {
+      for (int q = 0; q < xa - gx0; ++q) plane[q] = z;
+      for (int q = xb - gx0; q < npx; ++q) plane[q] = z;
+      mine += run;
+    }
+  }
+  uint32_t total = mine;
+  for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+  tc::fence_proxy_async_smem();
+  __syncwarp();
+  if (lane == 0) tc::mbar_expect_tx(bar, total);
+  __syncwarp();
+  for (int p = lane; p < nplanes; p += 32) {
+    const int gy = gy0 + p / c8, c = p % c8;
+    if (gy >= 0 && gy < H && run > 0) {
+      const __nv_bfloat16* src = act + ((((size_t)b * H + gy) * c8 + c) * W + xa) * 8;
+      tc::bulk_load(dst + (size_t)p * P + (size_t)(xa - gx0) * 16, src, run, bar);
+    }
+  }
 }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
@@ -74,18 +121,18 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
 }
 
 template <int C8_IN, int R, int EPI>
-__global__ void __launch_bounds__(kConvThreads, 1)
-    conv3x3_kernel(const __grid_constant__ CUtensorMap tmap_in, const ConvArgs a) {
+__global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs a) {
   using G = ConvGeom<C8_IN, R>;
+  constexpr int NST = G::NST;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
-  uint64_t* full = bars;         // [2] TMA -> MMA
-  uint64_t* empty = bars + 2;    // [2] MMA -> TMA
-  uint64_t* tfull = bars + 4;    // [2] MMA -> epilogue
-  uint64_t* tempty = bars + 6;   // [2] epilogue -> MMA
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + G::OFF_BAR + 64);
-  float* sbias = reinterpret_cast<float*>(smem + G::OFF_BAR + 80);
+  uint64_t* full = bars;               // [NST] loads -> MMA
+  uint64_t* empty = bars + NST;        // [NST] MMA -> loads
+  uint64_t* tfull = bars + 2 * NST;    // [2] MMA -> epilogue
+  uint64_t* tempty = bars + 2 * NST + 2;  // [2] epilogue -> MMA
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + G::OFF_BAR + 128);
+  float* sbias = reinterpret_cast<float*>(smem + G::OFF_BAR + 144);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -97,14 +144,15 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     if (threadIdx.x < kCout) sbias[threadIdx.x] = (EPI == kEpiFwdLeaky && a.bias) ? a.bias[threadIdx.x] : 0.f;
   }
   if (threadIdx.x == 0) {
-    for (int s = 0; s < 2; ++s) {
+    for (int s = 0; s < NST; ++s) {
       tc::mbar_init(&full[s], 1);
       tc::mbar_init(&empty[s], 1);
+    }
+    for (int s = 0; s < 2; ++s) {
       tc::mbar_init(&tfull[s], 1);
       tc::mbar_init(&tempty[s], 128);
     }
     tc::fence_mbar_init();
-    tc::prefetch_tmap(&tmap_in);
   }
   tc::fence_proxy_async_smem();
   if (warp == 0) {
@@ -118,27 +166,25 @@ __global__ void __launch_bounds__(kConvThreads, 1)
   const uint32_t sbase = tc::smem_u32(smem);
 
   if (warp == 0) {
-    // ---------------- TMA producer ----------------
-    if (lane == 0) {
-      for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
-        const int s = it & 1, use = it >> 1;
-        if (!tc::mbar_wait(&empty[s], (use & 1) ^ 1)) {
-          set_err(a.err, 1);
-          break;
-        }
-        const int txi = t % a.tiles_w, rest = t / a.tiles_w;
-        const int tyi = rest % a.tiles_h, b = rest / a.tiles_h;
-        tc::mbar_expect_tx(&full[s], G::STAGE);
-        tc::tma_load_5d(smem + s * G::STAGE, &tmap_in, 0, txi * kTW - 1, 0, tyi * R - 1, b, &full[s]);
+    // ---------------- producer: bulk copies of the haloed input tile ----------------
+    for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
+      const int s = it % NST, use = it / NST;
+      if (!tc::mbar_wait(&empty[s], (use & 1) ^ 1)) {
+        if (lane == 0) set_err(a.err, 1);
+        break;
       }
+      const int txi = t % a.tiles_w, rest = t / a.tiles_w;
+      const int tyi = rest % a.tiles_h, b = rest / a.tiles_h;
+      load_tile(a.x, a.H, a.W, C8_IN, b, tyi * R - 1, R + 2, txi * kTW - 1, kBoxW, smem + s * G::STAGE, &full[s],
+                lane);
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
       constexpr uint32_t idesc = tc::make_idesc_bf16(128, kCout, false, false);
       for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
-        const int s = it & 1, use = it >> 1, acc = it & 1;
-        if (!tc::mbar_wait(&tempty[acc], (use & 1) ^ 1) || !tc::mbar_wait(&full[s], use & 1)) {
+        const int s = it % NST, use = it / NST, acc = it & 1, ause = it >> 1;
+        if (!tc::mbar_wait(&tempty[acc], (ause & 1) ^ 1) || !tc::mbar_wait(&full[s], use & 1)) {
           set_err(a.err, 2);
           break;
         }
@@ -265,29 +311,33 @@ __global__ void __launch_bounds__(kConvThreads, 1)
 // ---------------------------------------------------------------------------
 struct WgradArgs {
   int B, H, W;
-  int segs_w, n_items;
+  int segs_w, yblocks, n_items;
+  const __nv_bfloat16* x;  // layer input [B][H][C8_IN][W][8]
+  const __nv_bfloat16* g;  // gradient w.r.t. the pre-activation [B][H][4][W][8]
   float* partial;  // [gridDim.x][3][128][32]
   int* err;
 };
 
+constexpr int kWRows = 4;  // output rows per work item
+
 template <int C8_IN>
 struct WgradGeom {
   static constexpr int NROW = 128 / (C8_IN * 8);         // input rows covered by M = 128
+  static constexpr int XROWS = NROW + kWRows - 1;        // input rows of one item
   static constexpr uint32_t P = kBoxW * 16;              // X chunk plane stride
-  static constexpr uint32_t XBYTES = NROW * C8_IN * P;   // X stage
+  static constexpr uint32_t RS = C8_IN * P;              // X row stride
+  static constexpr uint32_t XBYTES = XROWS * RS;         // X stage
   static constexpr uint32_t GP = kTW * 16;               // G chunk plane stride
-  static constexpr uint32_t GBYTES = 4 * GP;             // G stage (32 channels)
+  static constexpr uint32_t GBYTES = kWRows * 4 * GP;    // G stage (32 channels, kWRows rows)
   static constexpr uint32_t STAGE = XBYTES + GBYTES;
-  static constexpr int NST = 3;
+  static constexpr int NST = 2;
   static constexpr uint32_t OFF_BAR = NST * STAGE;
   static constexpr uint32_t TMEM_COLS = 128;
   static constexpr uint32_t SMEM = OFF_BAR + 8 * 8 + 16 + 1024;
 };
 
 template <int C8_IN>
-__global__ void __launch_bounds__(kConvThreads, 1)
-    conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmap_x, const __grid_constant__ CUtensorMap tmap_g,
-                         const WgradArgs a) {
+__global__ void __launch_bounds__(kConvThreads, 1) conv3x3_wgrad_kernel(const WgradArgs a) {
   using G = WgradGeom<C8_IN>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -300,13 +350,11 @@ __global__ void __launch_bounds__(kConvThreads, 1)
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < G::NST; ++s) {
-      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&full[s], 2);  // the X and the G tile loads each arrive once
       tc::mbar_init(&empty[s], 1);
     }
     tc::mbar_init(done, 1);
     tc::fence_mbar_init();
-    tc::prefetch_tmap(&tmap_x);
-    tc::prefetch_tmap(&tmap_g);
   }
   if (warp == 0) {
     tc::tmem_alloc(tmem_slot, G::TMEM_COLS);
@@ -320,19 +368,16 @@ __global__ void __launch_bounds__(kConvThreads, 1)
   const int my_items = blockIdx.x < a.n_items ? (a.n_items - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
   if (warp == 0) {
-    if (lane == 0) {
-      for (int it = 0, t = blockIdx.x; t < a.n_items; t += gridDim.x, ++it) {
-        const int s = it % G::NST, use = it / G::NST;
-        if (!tc::mbar_wait(&empty[s], (use & 1) ^ 1)) {
-          set_err(a.err, 11);
-          break;
-        }
-        const int sx = t % a.segs_w, rest = t / a.segs_w;
-        const int y = rest % a.H, b = rest / a.H;
-        tc::mbar_expect_tx(&full[s], G::STAGE);
-        tc::tma_load_5d(smem + s * G::STAGE, &tmap_x, 0, sx * kTW - 1, 0, y - 1, b, &full[s]);
-        tc::tma_load_5d(smem + s * G::STAGE + G::XBYTES, &tmap_g, 0, sx * kTW, 0, y, b, &full[s]);
+    for (int it = 0, t = blockIdx.x; t < a.n_items; t += gridDim.x, ++it) {
+      const int s = it % G::NST, use = it / G::NST;
+      if (!tc::mbar_wait(&empty[s], (use & 1) ^ 1)) {
+        if (lane == 0) set_err(a.err, 11);
+        break;
       }
+      const int sx = t % a.segs_w, rest = t / a.segs_w;
+      const int y0 = (rest % a.yblocks) * kWRows, b = rest / a.yblocks;
+      load_tile(a.x, a.H, a.W, C8_IN, b, y0 - 1, G::XROWS, sx * kTW - 1, kBoxW, smem + s * G::STAGE, &full[s], lane);
+      load_tile(a.g, a.H, a.W, 4, b, y0, kWRows, sx * kTW, kTW, smem + s * G::STAGE + G::XBYTES, &full[s], lane);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -346,15 +391,18 @@ __global__ void __launch_bounds__(kConvThreads, 1)
         tc::tc_fence_after();
         const uint32_t x0 = sbase + s * G::STAGE;
         const uint32_t g0 = x0 + G::XBYTES;
+#pragma unroll 1
+        for (int j = 0; j < kWRows; ++j) {  // output row y0 + j uses input rows y0 + j - 1 ...
 #pragma unroll
-        for (int dx = 0; dx < 3; ++dx) {
+          for (int dx = 0; dx < 3; ++dx) {
 #pragma unroll
-          for (int ks = 0; ks < kTW / 16; ++ks) {
-            // A: M = (input row, ci) groups of 8 channels every P bytes; K = pixels, 8-pixel groups 128 B apart
-            const uint64_t ad = tc::make_desc(x0 + dx * 16 + ks * 256, 128, G::P);
-            // B: N = co groups of 8 every GP bytes; K = pixels
-            const uint64_t bd = tc::make_desc(g0 + ks * 256, 128, G::GP);
-            tc::mma_bf16(tmem + dx * kCout, ad, bd, idesc, (it > 0 || ks > 0) ? 1u : 0u);
+            for (int ks = 0; ks < kTW / 16; ++ks) {
+              // A: M = (input row, ci) groups of 8 channels every P bytes; K = pixels, 8-pixel groups 128 B apart
+              const uint64_t ad = tc::make_desc(x0 + j * G::RS + dx * 16 + ks * 256, 128, G::P);
+              // B: N = co groups of 8 every GP bytes; K = pixels
+              const uint64_t bd = tc::make_desc(g0 + j * 4 * G::GP + ks * 256, 128, G::GP);
+              tc::mma_bf16(tmem + dx * kCout, ad, bd, idesc, (it > 0 || j > 0 || ks > 0) ? 1u : 0u);
+            }
           }
         }
         tc::mma_commit(&empty[s]);
@@ -411,49 +459,6 @@ static int sm_count() {
   return n;
 }
 
-// cuTensorMapEncodeTiled is resolved through the runtime at first use, so the
-// library does not link the driver library directly (it loads on hosts
-// without a GPU driver; only calls that launch kernels need one).
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-static EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
-  return fn;
-}
-
-// bf16 [B][H][c8][W][8] tensor map with box {8, box_w, c8, box_h, 1}.
-static int act_tmap(CUtensorMap* m, const void* base, int B, int H, int W, int c8, int box_w, int box_h) {
-  if (((uintptr_t)base & 15) != 0) {
-    set_error("activation base address must be 16-byte aligned");
-    return IGM_ERR_BAD_ARGUMENT;
-  }
-  cuuint64_t dims[5] = {8, (cuuint64_t)W, (cuuint64_t)c8, (cuuint64_t)H, (cuuint64_t)B};
-  cuuint64_t strides[4] = {16, (cuuint64_t)W * 16, (cuuint64_t)c8 * W * 16, (cuuint64_t)H * c8 * W * 16};
-  cuuint32_t box[5] = {8, (cuuint32_t)box_w, (cuuint32_t)c8, (cuuint32_t)box_h, 1};
-  cuuint32_t es[5] = {1, 1, 1, 1, 1};
-  EncodeTiledFn enc = encode_fn();
-  if (!enc) {
-    set_error("cuTensorMapEncodeTiled is not available from the CUDA driver");
-    return IGM_ERR_CUDA;
-  }
-  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(base), dims, strides, box, es,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    set_error("cuTensorMapEncodeTiled failed (CUresult %d)", (int)r);
-    return IGM_ERR_CUDA;
-  }
-  return IGM_OK;
-}
-
 template <typename K>
 static int set_smem(K kernel, uint32_t bytes, bool* done) {
   if (!*done) {
@@ -476,11 +481,11 @@ static int conv_launch(int B, int H, int W, const void* x, const void* wpack, co
   static bool configured = false;
   int rc = set_smem(conv3x3_kernel<C8_IN, kRows, EPI>, G::SMEM, &configured);
   if (rc) return rc;
-  CUtensorMap tm;
-  rc = act_tmap(&tm, x, B, H, W, C8_IN, kBoxW, kRows + 2);
-  if (rc) return rc;
+  IGM_CHECK_ARG(((uintptr_t)x & 15) == 0 && ((uintptr_t)y & 15) == 0, IGM_ERR_BAD_ARGUMENT,
+                "igm_conv3x3: activations must be 16-byte aligned");
   ConvArgs a{};
   a.B = B; a.H = H; a.W = W;
+  a.x = (const __nv_bfloat16*)x;
   a.tiles_w = (W + kTW - 1) / kTW;
   a.tiles_h = (H + kRows - 1) / kRows;
   a.n_tiles = B * a.tiles_w * a.tiles_h;
@@ -496,7 +501,7 @@ static int conv_launch(int B, int H, int W, const void* x, const void* wpack, co
     a.db_partial = db_partial;
   }
   if (grid < 1) grid = 1;
-  conv3x3_kernel<C8_IN, kRows, EPI><<<grid, kConvThreads, G::SMEM, st>>>(tm, a);
+  conv3x3_kernel<C8_IN, kRows, EPI><<<grid, kConvThreads, G::SMEM, st>>>(a);
   return launch_status("conv3x3_kernel");
 }
 
@@ -507,18 +512,18 @@ static int wgrad_launch(int B, int H, int W, const void* x, const void* g, float
   static bool configured = false;
   int rc = set_smem(conv3x3_wgrad_kernel<C8_IN>, G::SMEM, &configured);
   if (rc) return rc;
-  CUtensorMap tx, tg;
-  rc = act_tmap(&tx, x, B, H, W, C8_IN, kBoxW, G::NROW);
-  if (rc) return rc;
-  rc = act_tmap(&tg, g, B, H, W, 4, kTW, 1);
-  if (rc) return rc;
+  IGM_CHECK_ARG(((uintptr_t)x & 15) == 0 && ((uintptr_t)g & 15) == 0, IGM_ERR_BAD_ARGUMENT,
+                "igm_conv3x3_wgrad: activations must be 16-byte aligned");
   WgradArgs a{};
   a.B = B; a.H = H; a.W = W;
   a.segs_w = (W + kTW - 1) / kTW;
-  a.n_items = B * H * a.segs_w;
+  a.yblocks = (H + kWRows - 1) / kWRows;
+  a.n_items = B * a.yblocks * a.segs_w;
+  a.x = (const __nv_bfloat16*)x;
+  a.g = (const __nv_bfloat16*)g;
   a.partial = partial;
   a.err = err;
-  conv3x3_wgrad_kernel<C8_IN><<<n_parts, kConvThreads, G::SMEM, st>>>(tx, tg, a);
+  conv3x3_wgrad_kernel<C8_IN><<<n_parts, kConvThreads, G::SMEM, st>>>(a);
   return launch_status("conv3x3_wgrad_kernel");
 }
 

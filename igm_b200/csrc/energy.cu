@@ -13,35 +13,42 @@
 // layer l (between levels l and l+1) the stag2v averages and the vertical
 // derivative (Us[l+1]-Us[l]) / (dzeta[l] max(thk_s, thr)).
 //
-// Kernel shape.  A CTA is one warp wide (32 cells in x) and TYC warps tall.
-// Its cells are [j0-1, j0-1+TYC) x [i0-1, i0+31), which covers every cell that
-// touches its (TYC-1) x 31 output nodes, so the adjoint (a scatter from
-// cells to their 4 corners) becomes a gather inside the CTA with no atomics.
-// The kernel streams through the Nz levels: each level's node tile of U and V
-// is staged in shared memory (double-buffered, next level prefetched into
-// registers), each thread evaluates its cell's layer l = k-1 energy and
-// adjoint, and as soon as level k-1's adjoint is complete its per-cell
-// partials (S = dUs/4, P = dDx/(2dx), Q = dDy/(2dx)) are gathered into the
-// node gradient and written (or fed to Adam) for that level.  Shared memory
-// therefore holds two levels at a time, independent of Nz.
+// Kernel shape.  A tile is 32 cells in x (one per lane) and TYC cell rows;
+// each thread evaluates TWO vertically adjacent cells, whose values travel as
+// a pair: for float the pair arithmetic runs on sm_100's packed FP32x2 pipe
+// (one instruction for both cells), which halves the instruction count of the
+// per-cell math that bounds this kernel; a warp reads whole tile rows, free of
+// shared-memory bank conflicts.  A tile's cells [j0-1, j0-1+TYC) x
+// [i0-1, i0+31) cover every cell touching its (TYC-1) x 31 output nodes, so
+// the adjoint (a scatter from cells to their 4 corners) becomes a gather
+// inside the CTA with no atomics: the horizontal half by warp shuffles, the
+// vertical half through one shared-memory row per warp.
+// CTAs are persistent (as many as fit on the device) and walk their tiles
+// level by level as one sequence: each level's node tile of U and V (and, in
+// solver mode, the Adam moments) arrives by TMA (or cp.async when the row pitch
+// is not a multiple of 16 bytes) into a ring of stages kept several levels
+// ahead of the one being computed -- across tile boundaries -- and a tile's
+// 2-D fields arrive while the previous tile is computed.  Each level's node
+// outputs (gradient, or the Adam update) are finished two levels later, when
+// all of the layers touching them are done.
 //
-// Energy reduction: per-cell FP32 densities, FP64 block sums, per-CTA
-// partials in the workspace, and the last CTA to finish sums them in a fixed
-// order (deterministic) and, in solver mode, runs EarlyStopping on the device.
+// Energy reduction: per-cell FP32 densities, FP64 per-thread sums over its
+// tiles, FP64 block sums, per-CTA partials in the workspace, and the last CTA
+// to finish sums them in a fixed order (deterministic for a given device) and,
+// in solver mode, runs EarlyStopping on the device.
 #include <stdarg.h>
 
+#include <string.h>
+
+#include <initializer_list>
 #include <mutex>
 
 #include "common.cuh"
+#include "tc.cuh"
 
 namespace igm {
 
-constexpr int kTX = 32;
-// Levels of U, V (and Adam moments) kept in flight ahead of the one being
-// computed.  The ring has kStages = kAhead + 2 slots: the extra slot keeps
-// the level whose moments are read by the gather one iteration later.
-constexpr int kAhead = 3;
-constexpr int kStages = kAhead + 2;
+constexpr int kCW = 32;  // cells per CTA row (one per lane)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -58,7 +65,87 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// Node tiles are loaded as boxes of (TYC + 1) rows x BW columns starting at
+// the 16-byte aligned column xs <= i0 - 1; the tile's column 0 (node i0 - 1)
+// sits at box column ox = i0 - 1 - xs.  Out-of-domain nodes read as zero.
+template <typename T> struct Box {
+  static constexpr int AL = 16 / (int)sizeof(T);                   // elements per 16 bytes
+  static constexpr int BW = ((kCW + 1 + AL - 1 + AL - 1) / AL) * AL;  // >= 33 + (AL - 1), multiple of AL
+};
+
+// ---- cell pairs --------------------------------------------------------------
+// Two values of adjacent cells.  float: packed FP32x2 instructions (add, mul,
+// fma; a - b as fma(b, -1, a), exact); double: two scalar operations.
+template <typename T> struct Two { T x, y; };
+template <typename T> __device__ __forceinline__ Two<T> two(T s) { return {s, s}; }
+template <typename T> __device__ __forceinline__ Two<T> operator+(Two<T> a, Two<T> b) { return {a.x + b.x, a.y + b.y}; }
+template <typename T> __device__ __forceinline__ Two<T> operator-(Two<T> a, Two<T> b) { return {a.x - b.x, a.y - b.y}; }
+template <typename T> __device__ __forceinline__ Two<T> operator*(Two<T> a, Two<T> b) { return {a.x * b.x, a.y * b.y}; }
+template <typename T> __device__ __forceinline__ Two<T> fma2(Two<T> a, Two<T> b, Two<T> c) {
+  return {fma(a.x, b.x, c.x), fma(a.y, b.y, c.y)};
+}
+__device__ __forceinline__ float2 f2(Two<float> a) { return make_float2(a.x, a.y); }
+__device__ __forceinline__ Two<float> t2(float2 a) { return {a.x, a.y}; }
+template <> __device__ __forceinline__ Two<float> operator+(Two<float> a, Two<float> b) {
+  return t2(__fadd2_rn(f2(a), f2(b)));
+}
+template <> __device__ __forceinline__ Two<float> operator-(Two<float> a, Two<float> b) {
+  return t2(__ffma2_rn(f2(b), make_float2(-1.f, -1.f), f2(a)));
+}
+template <> __device__ __forceinline__ Two<float> operator*(Two<float> a, Two<float> b) {
+  return t2(__fmul2_rn(f2(a), f2(b)));
+}
+template <> __device__ __forceinline__ Two<float> fma2(Two<float> a, Two<float> b, Two<float> c) {
+  return t2(__ffma2_rn(f2(a), f2(b), f2(c)));
+}
+template <typename T> __device__ __forceinline__ Two<T> sel(bool px, bool py, Two<T> a, Two<T> b) {
+  return {px ? a.x : b.x, py ? a.y : b.y};
+}
+
+// x^(-1/3) for x > 0 (x >= 1e-20 here): 2^(-log2(x)/3) from the hardware
+// base-2 logarithm and exponential approximations, refined by one
+// Newton-Raphson step for f(y) = y^-3 - x, y <- y (4 - x y^3) / 3.
+__device__ __forceinline__ float rcbrt_fast(float x) {
+  float l, y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"(x));
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(-0.33333334f * l));
+  const float y3 = y * y * y;
+  return y * fmaf(-0.33333334f * x, y3, 1.33333337f);
+}
+template <typename T> __device__ __forceinline__ T rcbrt_k(T x) { return Math<T>::rcbrt(x); }
+template <> __device__ __forceinline__ float rcbrt_k<float>(float x) { return rcbrt_fast(x); }
+// The same for a pair, the Newton step in pair arithmetic.
+template <typename T> __device__ __forceinline__ Two<T> rcbrt2(Two<T> x) { return {rcbrt_k(x.x), rcbrt_k(x.y)}; }
+template <> __device__ __forceinline__ Two<float> rcbrt2<float>(Two<float> x) {
+  float lx, ly, yx, yy;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(lx) : "f"(x.x));
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(ly) : "f"(x.y));
+  const Two<float> e = Two<float>{lx, ly} * two(-0.33333334f);
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(yx) : "f"(e.x));
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(yy) : "f"(e.y));
+  const Two<float> y{yx, yy};
+  const Two<float> y3 = y * y * y;
+  return y * fma2(x * two(-0.33333334f), y3, two(1.33333337f));
+}
+
+// Adam's step m * alpha / (sqrt(v) + eps), correctly rounded square root and
+// division as TensorFlow's ApplyAdam evaluates it (the solver's trajectory
+// amplifies every rounding difference).
+template <typename T> __device__ __forceinline__ T adam_step(T m_alpha, T v, T eps) {
+  return m_alpha / (Math<T>::sqrt(v) + eps);
+}
+
 enum StencilMode { kEnergyOnly = 0, kGradient = 1, kAdamStep = 2 };
+
+// Levels in flight ahead of the one being computed.  The ring also holds the
+// level being computed and the two levels whose outputs are still pending
+// (their Adam moments and old velocities are read when they are finished).
+// The solver mode stages six tiles per level, so it looks two levels less
+// ahead to keep two CTAs per SM.
+template <int MODE> struct Ring {
+  static constexpr int ahead = MODE == kAdamStep ? 2 : 4;
+  static constexpr int stages = ahead + 3;
+};
 
 template <typename T>
 struct StencilArgs {
@@ -68,6 +155,10 @@ struct StencilArgs {
   T inv_dzeta[IGM_MAX_NZ];
   // physics
   T q, inv_p, regu2, sr_lo, sr_hi, thr, Kg, inv_n, s_w, inv_sw, regw2;
+  // working units of the kernel: sr2 = k2 sr2w (k2 = 1/(32 dx^2)), clip bounds of sr2w,
+  // and the gravity weight of each level, dzeta[k-1] + dzeta[k]
+  T k2, lo2, hi2;
+  T wgrav[IGM_MAX_NZ];
   int glen3, weert3, fnge;
   // inputs
   const T* thk;
@@ -97,52 +188,85 @@ struct StencilArgs {
   unsigned int* counter;
   double* terms;
   double inv_count;
+  int* err;  // set when a level load never arrived (bounded wait expired)
 };
 
-template <typename T, int TYC, int MODE>
+// Tensor maps of the node tiles: U/V of both solver buffers, the Adam moments
+// and the 2-D fields.
+struct StencilMaps {
+  CUtensorMap U0, V0, U1, V1, mU, mV, vU, vV;
+  CUtensorMap thk, usurf, A, C;
+};
+
+template <typename T, int TYP, int MODE>
 struct StencilSmem {
-  static constexpr int NR = TYC + 1, NC = kTX + 1;
+  static constexpr int NR = 2 * TYP + 1, BW = Box<T>::BW;
+  // elements per box, rounded up so that every box starts on a 128-byte boundary
+  static constexpr int BOXE = ((NR * BW * (int)sizeof(T) + 127) / 128) * 128 / (int)sizeof(T);
   static constexpr bool GRAD = MODE != kEnergyOnly;
   static constexpr bool ADAM = MODE == kAdamStep;
-  T F[4][NR][NC];                        // thk, usurf, B = 2 A^(-1/n), c of the node tile
-  T N[kStages][2][NR][NC];               // U, V node tiles, ring of levels
-  T M[ADAM ? kStages : 1][4][TYC][kTX];  // mU, mV, vU, vV of the output nodes, ring of levels
-  T Tr[GRAD ? 2 : 1][6][TYC][kTX];       // per-cell adjoint partials S, P, Q of U and V
-  double red[TYC];
+  static constexpr int kStages = Ring<MODE>::stages;
+  T N[kStages][2][BOXE];                        // U, V node tiles [NR][BW], ring of levels
+  T M[ADAM ? kStages : 1][ADAM ? 4 : 1][BOXE];  // mU, mV, vU, vV node tiles, ring of levels
+  T F[2][4][BOXE];                              // thk, usurf, A (then B = 2 A^(-1/n)), c: this tile, next tile
+  T Down[GRAD ? 2 : 1][2][TYP][kCW];            // [level parity][U, V]: a thread row's share of the node row below
+  double red[3][TYP];
+  uint64_t full[kStages];                       // TMA arrival of a level
+  uint64_t ffull[2];                            // TMA arrival of a tile's 2-D fields
   unsigned int ticket;
 };
 
-template <typename T> struct MinBlocks { static constexpr int value = 3; };
-template <> struct MinBlocks<double> { static constexpr int value = 2; };
+// Thread rows per CTA (each thread row = one warp = two cell rows).
+template <typename T> struct ThreadRows { static constexpr int value = 8; };
+template <> struct ThreadRows<double> { static constexpr int value = 4; };
+template <typename T, int MODE> struct MinBlocks { static constexpr int value = MODE == kEnergyOnly ? 3 : 2; };
+template <int MODE> struct MinBlocks<double, MODE> { static constexpr int value = 2; };
 
-template <typename T, int TYC, int MODE>
-__global__ void __launch_bounds__(kTX* TYC, MinBlocks<T>::value) stencil_kernel(const StencilArgs<T> a) {
-  constexpr int NT = kTX * TYC;
-  constexpr int NR = TYC + 1, NC = kTX + 1;
+struct TileGeo {
+  int j0, i0, xs, ox, b;  // first output node row / column, aligned box column, tile column 0 in the box, batch
+};
+
+// Persistent CTAs: CTA c processes tiles c, c + gridDim.x, ... (row-major over
+// x, then y, then batch), streaming the sequence (tile, level) through one
+// ring, so the loads of a tile's first levels and its 2-D fields are issued
+// while the previous tile is still being computed.
+template <typename T, int TYP, int MODE, bool TMA>
+__global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
+    stencil_kernel(const StencilArgs<T> a, const __grid_constant__ StencilMaps maps) {
+  using P = Two<T>;
+  using SmemT = StencilSmem<T, TYP, MODE>;
+  constexpr int TYC = 2 * TYP;  // cell rows per tile
+  constexpr int NT = kCW * TYP;
+  constexpr int NR = TYC + 1, NC = kCW + 1;
   constexpr int NTILE = NR * NC;
+  constexpr int BW = Box<T>::BW;
+  constexpr int AL = Box<T>::AL;
   constexpr bool GRAD = MODE != kEnergyOnly;
   constexpr bool ADAM = MODE == kAdamStep;
+  constexpr uint32_t kBoxBytes = NR * BW * sizeof(T);
+  constexpr int kAhead = Ring<MODE>::ahead, kStages = Ring<MODE>::stages;
+  static_assert(kCW == 32, "one warp per thread row");
 
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  StencilSmem<T, TYC, MODE>& SM = *reinterpret_cast<StencilSmem<T, TYC, MODE>*>(smem_raw);
-  auto& sF = SM.F;
-  auto& sN = SM.N;
-  auto& sM = SM.M;
-  auto& sT = SM.Tr;
-  double* sRed = SM.red;
-  unsigned int& sTicket = SM.ticket;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // TMA box destinations: align the base explicitly (the launch reserves 128 extra bytes).
+  unsigned char* smem_al = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  SmemT& SM = *reinterpret_cast<SmemT*>(smem_al);
 
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kCW + tx;
   const int ny = a.ny, nx = a.nx, nz = a.nz;
-  const int j0 = blockIdx.y * (TYC - 1), i0 = blockIdx.x * (kTX - 1);
   const size_t plane = (size_t)ny * nx;
-  const size_t fbase = (size_t)blockIdx.z * plane;
-  const size_t vbase = (size_t)blockIdx.z * nz * plane;
+  const int tiles_x = (nx + kCW - 2) / (kCW - 1);
+  const int tiles_y = (ny + TYC - 2) / (TYC - 1);
+  const int tiles_xy = tiles_x * tiles_y;
+  const int ntiles = tiles_xy * a.batch;
+  const int my_tiles = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
-  T* Ucur = a.U0;
-  T* Vcur = a.V0;
+  const T* Ucur = a.U0;
+  const T* Vcur = a.V0;
   T* Unxt = a.U1;
   T* Vnxt = a.V1;
+  const CUtensorMap* mapU = &maps.U0;
+  const CUtensorMap* mapV = &maps.V0;
   int iter = 0;
   T alpha = 0;
   if (MODE == kAdamStep) {
@@ -150,293 +274,457 @@ __global__ void __launch_bounds__(kTX* TYC, MinBlocks<T>::value) stencil_kernel(
     const int stopped = __ldcg(&a.ctl->stopped);
     if (stopped || iter >= a.max_iter) return;
     if (iter & 1) {
-      Ucur = a.U1; Vcur = a.V1; Unxt = a.U0; Vnxt = a.V0;
+      mapU = &maps.U1; mapV = &maps.V1; Unxt = a.U0; Vnxt = a.V0;
+      Ucur = a.U1; Vcur = a.V1;
     }
     const long long t = __ldcg(&a.ctl->adam_t0) + iter + 1;
     const T one = T(1);
     alpha = a.lr * Math<T>::sqrt(one - Math<T>::pow(a.b2, T(t))) / (one - Math<T>::pow(a.b1, T(t)));
   }
 
-  // ---- 2-D fields of the node tile -----------------------------------------
-  for (int idx = tid; idx < NTILE; idx += NT) {
-    const int r = idx / NC, c = idx - r * NC;
-    const int gj = j0 - 1 + r, gi = i0 - 1 + c;
-    T th = 0, us = 0, Bv = 0, cv = 0;
-    if (gj >= 0 && gj < ny && gi >= 0 && gi < nx) {
-      const size_t o = fbase + (size_t)gj * nx + gi;
-      th = a.thk[o];
-      us = a.usurf[o];
-      const T Av = a.A[o];
-      Bv = T(2) * (a.glen3 ? Math<T>::rcbrt(Av) : Math<T>::pow(Av, -a.inv_n));
-      cv = a.C[o];
-    }
-    sF[0][r][c] = th;
-    sF[1][r][c] = us;
-    sF[2][r][c] = Bv;
-    sF[3][r][c] = cv;
-  }
+  auto geo = [&](int i) {
+    const int t = (int)blockIdx.x + i * (int)gridDim.x;
+    const int b = t / tiles_xy, r = t - b * tiles_xy;
+    const int yt = r / tiles_x, xt = r - yt * tiles_x;
+    TileGeo g;
+    g.j0 = yt * (TYC - 1);
+    g.i0 = xt * (kCW - 1);
+    g.b = b;
+    g.xs = g.i0 >= 1 ? ((g.i0 - 1) / AL) * AL : -AL;
+    g.ox = g.i0 - 1 - g.xs;
+    return g;
+  };
 
-  // ---- asynchronous level loads: U, V node tile (+ Adam moments of the output nodes)
-  const int own_j = j0 - 1 + ty, own_i = i0 - 1 + tx;  // this thread's node (corner a of its cell)
-  const bool outnode = ty >= 1 && tx >= 1 && own_j < ny && own_i < nx;
-  // each thread's share of the node tile: fixed (row, col) slots, offsets computed once
+  if (tid == 0) {
+    for (int st = 0; st < kStages; ++st) tc::mbar_init(&SM.full[st], 1);
+    tc::mbar_init(&SM.ffull[0], 1);
+    tc::mbar_init(&SM.ffull[1], 1);
+    tc::fence_mbar_init();
+  }
+  __syncthreads();
+
+  // fixed node slots of this thread in a tile (element-wise loads and the B pass)
   constexpr int NSLOT = (NTILE + NT - 1) / NT;
-  int slot_off[NSLOT];
-  int slot_sm[NSLOT];
-  bool slot_ok[NSLOT];
+  int slot_r[NSLOT], slot_c[NSLOT];
 #pragma unroll
   for (int q = 0; q < NSLOT; ++q) {
     const int idx = tid + q * NT;
-    const int r = idx / NC, c = idx - r * NC;
-    const int gj = j0 - 1 + r, gi = i0 - 1 + c;
-    slot_ok[q] = idx < NTILE && gj >= 0 && gj < ny && gi >= 0 && gi < nx;
-    slot_off[q] = slot_ok[q] ? gj * nx + gi : 0;
-    slot_sm[q] = idx < NTILE ? idx : -1;
+    slot_r[q] = idx < NTILE ? idx / NC : -1;
+    slot_c[q] = idx < NTILE ? idx - (idx / NC) * NC : 0;
   }
-  auto issue_level = [&](int k) {
-    if (k < nz) {
-      const int st = k % kStages;
-      const T* Ub = Ucur + vbase + (size_t)k * plane;
-      const T* Vb = Vcur + vbase + (size_t)k * plane;
-      T* sU = &sN[st][0][0][0];
-      T* sV = &sN[st][1][0][0];
-#pragma unroll
-      for (int q = 0; q < NSLOT; ++q) {
-        if (slot_sm[q] >= 0) {
-          cp_async_elem(sU + slot_sm[q], Ub + slot_off[q], slot_ok[q]);
-          cp_async_elem(sV + slot_sm[q], Vb + slot_off[q], slot_ok[q]);
+  // this thread: cells (R0, tx) and (R0 + 1, tx) of the tile; output nodes (R0 + e, tx)
+  const int R0 = 2 * ty;
+
+  auto issue_fields = [&](const TileGeo& g, int fb) {  // TMA path only
+    if (tid == 0) {
+      uint64_t* bar = &SM.ffull[fb];
+      tc::mbar_expect_tx(bar, 4u * kBoxBytes);
+      tc::tma_load_3d(SM.F[fb][0], &maps.thk, g.xs, g.j0 - 1, g.b, bar);
+      tc::tma_load_3d(SM.F[fb][1], &maps.usurf, g.xs, g.j0 - 1, g.b, bar);
+      tc::tma_load_3d(SM.F[fb][2], &maps.A, g.xs, g.j0 - 1, g.b, bar);
+      tc::tma_load_3d(SM.F[fb][3], &maps.C, g.xs, g.j0 - 1, g.b, bar);
+    }
+  };
+  auto issue_level = [&](const TileGeo& g, int k, int st) {
+    if (TMA) {
+      if (tid == 0) {
+        uint64_t* bar = &SM.full[st];
+        const int z = g.b * nz + k;
+        tc::mbar_expect_tx(bar, (ADAM ? 6u : 2u) * kBoxBytes);
+        tc::tma_load_3d(SM.N[st][0], mapU, g.xs, g.j0 - 1, z, bar);
+        tc::tma_load_3d(SM.N[st][1], mapV, g.xs, g.j0 - 1, z, bar);
+        if (ADAM) {
+          tc::tma_load_3d(SM.M[st][0], &maps.mU, g.xs, g.j0 - 1, z, bar);
+          tc::tma_load_3d(SM.M[st][1], &maps.mV, g.xs, g.j0 - 1, z, bar);
+          tc::tma_load_3d(SM.M[st][2], &maps.vU, g.xs, g.j0 - 1, z, bar);
+          tc::tma_load_3d(SM.M[st][3], &maps.vV, g.xs, g.j0 - 1, z, bar);
         }
       }
-      if (ADAM) {
-        const size_t o = vbase + (size_t)k * plane + (outnode ? (size_t)own_j * nx + own_i : 0);
-        cp_async_elem(&sM[ADAM ? st : 0][0][ty][tx], a.mU + o, outnode);
-        cp_async_elem(&sM[ADAM ? st : 0][1][ty][tx], a.mV + o, outnode);
-        cp_async_elem(&sM[ADAM ? st : 0][2][ty][tx], a.vU + o, outnode);
-        cp_async_elem(&sM[ADAM ? st : 0][3][ty][tx], a.vV + o, outnode);
+    } else {
+      const size_t lo = ((size_t)g.b * nz + k) * plane;
+#pragma unroll
+      for (int q = 0; q < NSLOT; ++q) {
+        if (slot_r[q] < 0) continue;
+        const int gj = g.j0 - 1 + slot_r[q], gi = g.i0 - 1 + slot_c[q];
+        const bool ok = gj >= 0 && gj < ny && gi >= 0 && gi < nx;
+        const size_t o = lo + (ok ? (size_t)gj * nx + gi : 0);
+        const int sm = slot_r[q] * BW + slot_c[q] + g.ox;
+        cp_async_elem(SM.N[st][0] + sm, Ucur + o, ok);
+        cp_async_elem(SM.N[st][1] + sm, Vcur + o, ok);
+        if (ADAM) {
+          cp_async_elem(SM.M[st][0] + sm, a.mU + o, ok);
+          cp_async_elem(SM.M[st][1] + sm, a.mV + o, ok);
+          cp_async_elem(SM.M[st][2] + sm, a.vU + o, ok);
+          cp_async_elem(SM.M[st][3] + sm, a.vV + o, ok);
+        }
       }
     }
-    cp_async_commit();
   };
-#pragma unroll
-  for (int k = 0; k < kAhead; ++k) issue_level(k);
-  __syncthreads();
+  // issue cursor over the sequence (tile, level)
+  int iss_i = 0, iss_k = 0, iss_st = 0;
+  TileGeo ig = geo(0);
+  auto issue_next = [&]() {
+    if (iss_i < my_tiles) issue_level(ig, iss_k, iss_st);
+    if (!TMA) cp_async_commit();  // one group per sequence position, possibly empty
+    iss_st = iss_st + 1 == kStages ? 0 : iss_st + 1;
+    if (++iss_k == nz) {
+      iss_k = 0;
+      if (++iss_i < my_tiles) ig = geo(iss_i);
+    }
+  };
+  if (TMA && my_tiles > 0) issue_fields(ig, 0);
+#pragma unroll 1
+  for (int q = 0; q < kAhead; ++q) issue_next();
 
-  // ---- per-cell constants -----------------------------------------------------
-  const int cj = j0 - 1 + ty, ci = i0 - 1 + tx;  // this thread's cell
-  const bool cell_ok = cj >= 0 && cj < ny - 1 && ci >= 0 && ci < nx - 1;
-  const bool owner = cell_ok && ty >= 1 && tx >= 1;
-  const T dx = a.dx;
   const T half = T(0.5), quarter = T(0.25);
-  T thks, cs, Bs, sbx, sby, ssx, ssy;
-  {
-    const T t00 = sF[0][ty][tx], t01 = sF[0][ty][tx + 1], t10 = sF[0][ty + 1][tx], t11 = sF[0][ty + 1][tx + 1];
-    const T u00 = sF[1][ty][tx], u01 = sF[1][ty][tx + 1], u10 = sF[1][ty + 1][tx], u11 = sF[1][ty + 1][tx + 1];
-    thks = (((t11 + t10) + t01) + t00) / T(4);
-    Bs = (((sF[2][ty + 1][tx + 1] + sF[2][ty + 1][tx]) + sF[2][ty][tx + 1]) + sF[2][ty][tx]) / T(4);
-    cs = (((sF[3][ty + 1][tx + 1] + sF[3][ty + 1][tx]) + sF[3][ty][tx + 1]) + sF[3][ty][tx]) / T(4);
-    const T b00 = u00 - t00, b01 = u01 - t01, b10 = u10 - t10, b11 = u11 - t11;
-    const T two_dx = dx + dx;
-    // compute_gradient (staggered): E = 2 ds/(dx+dx), averaged over the other axis
-    sbx = half * (T(2) * (b11 - b10) / two_dx + T(2) * (b01 - b00) / two_dx);
-    sby = half * (T(2) * (b11 - b01) / two_dx + T(2) * (b10 - b00) / two_dx);
-    ssx = half * (T(2) * (u11 - u10) / two_dx + T(2) * (u01 - u00) / two_dx);
-    ssy = half * (T(2) * (u11 - u01) / two_dx + T(2) * (u10 - u00) / two_dx);
-  }
-  const T hcl = thks > a.thr ? thks : a.thr;
-  const T rh = T(1) / hcl;  // 1 / max(thk_s, thr)
-  const T idx_ = a.inv_dx;
-  const T fdamp = cs > T(0) ? T(1) : T(0.01);
-  const T gshear = thks * Bs;     // d(shear density)/d(p_term_l) = thks Bs dzeta_l
-  const T ggrav = a.Kg * thks;    // d(gravity density)/d(uds_l)  = Kg thks dzeta_l
+  const P H = two(half), Q4 = two(quarter), zero = two(T(0));
+  const P HI = two(half * a.inv_dx);
+  double acc[3] = {0.0, 0.0, 0.0};
+  bool load_ok = true;
+  int cons_st = 0;         // ring slot of the level being computed
+  uint32_t cons_ph = 0;    // its mbarrier phase parity
 
-  T e_shear = 0, e_grav = 0, e_slid = 0;
-  // previous level's cell quantities and pending adjoints
-  T pUs = 0, pVs = 0, pDxu = 0, pDyu = 0, pDxv = 0, pDyv = 0;
-  T gUs = 0, gDxu = 0, gDyu = 0, gVs = 0, gDxv = 0, gDyv = 0;
-  T prevUold = 0, prevVold = 0;  // this thread's node (a corner) at the previous level
-
-  const T inv2dx = T(1) / (dx + dx);
-  const T gsc = a.grad_scale;
-
-  // writes the per-cell partials of a completed level, then gathers them
-  auto flush_level = [&](int lvl, T Us_, T Dxu_, T Dyu_, T Vs_, T Dxv_, T Dyv_, T Uold, T Vold) {
-    const int tb = lvl & 1;
-    T S = cell_ok ? Us_ * quarter * gsc : T(0);
-    T P = cell_ok ? Dxu_ * inv2dx * gsc : T(0);
-    T Q = cell_ok ? Dyu_ * inv2dx * gsc : T(0);
-    sT[tb][0][ty][tx] = S;
-    sT[tb][1][ty][tx] = P;
-    sT[tb][2][ty][tx] = Q;
-    S = cell_ok ? Vs_ * quarter * gsc : T(0);
-    P = cell_ok ? Dxv_ * inv2dx * gsc : T(0);
-    Q = cell_ok ? Dyv_ * inv2dx * gsc : T(0);
-    sT[tb][3][ty][tx] = S;
-    sT[tb][4][ty][tx] = P;
-    sT[tb][5][ty][tx] = Q;
-    __syncthreads();
-    const int nj = j0 - 1 + ty, ni = i0 - 1 + tx;
-    if (ty >= 1 && tx >= 1 && nj < ny && ni < nx) {
-      T g[2];
+#pragma unroll 1
+  for (int i = 0; i < my_tiles; ++i) {
+    const TileGeo g = geo(i);
+    const int fb = TMA ? (i & 1) : 0;
+    if (TMA) {
+      if (i + 1 < my_tiles) issue_fields(geo(i + 1), fb ^ 1);
+      // one thread waits for the transfer; the barrier publishes it to the CTA
+      if (tid == 0 && !tc::mbar_wait(&SM.ffull[fb], (uint32_t)((i >> 1) & 1))) load_ok = false;
+      __syncthreads();
+    }
+    // 2-D fields (element-wise path: plain loads) and B = 2 A^(-1/n) in place at in-domain nodes
 #pragma unroll
-      for (int f = 0; f < 2; ++f) {
-        const T (*Sv)[kTX] = sT[tb][3 * f + 0];
-        const T (*Pv)[kTX] = sT[tb][3 * f + 1];
-        const T (*Qv)[kTX] = sT[tb][3 * f + 2];
-        g[f] = (Sv[ty][tx] - Pv[ty][tx] - Qv[ty][tx]) + (Sv[ty][tx - 1] + Pv[ty][tx - 1] - Qv[ty][tx - 1]) +
-               (Sv[ty - 1][tx] - Pv[ty - 1][tx] + Qv[ty - 1][tx]) +
-               (Sv[ty - 1][tx - 1] + Pv[ty - 1][tx - 1] + Qv[ty - 1][tx - 1]);
+    for (int q = 0; q < NSLOT; ++q) {
+      if (slot_r[q] < 0) continue;
+      const int gj = g.j0 - 1 + slot_r[q], gi = g.i0 - 1 + slot_c[q];
+      const bool ok = gj >= 0 && gj < ny && gi >= 0 && gi < nx;
+      const int sm = slot_r[q] * BW + slot_c[q] + g.ox;
+      T Av;
+      if (TMA) {
+        Av = SM.F[fb][2][sm];
+      } else {
+        const size_t o = (size_t)g.b * plane + (ok ? (size_t)gj * nx + gi : 0);
+        SM.F[0][0][sm] = ok ? a.thk[o] : T(0);
+        SM.F[0][1][sm] = ok ? a.usurf[o] : T(0);
+        SM.F[0][3][sm] = ok ? a.C[o] : T(0);
+        Av = ok ? a.A[o] : T(1);
       }
-      const size_t o = vbase + (size_t)lvl * plane + (size_t)nj * nx + ni;
-      if (MODE == kGradient) {
-        a.dU[o] = g[0];
-        a.dV[o] = g[1];
-      } else if (MODE == kAdamStep) {
-        const T b1c = T(1) - a.b1, b2c = T(1) - a.b2;
-        const int ms = ADAM ? lvl % kStages : 0;
-        T m = sM[ms][0][ty][tx], v = sM[ms][2][ty][tx];
-        m += (g[0] - m) * b1c;
-        v += (g[0] * g[0] - v) * b2c;
-        a.mU[o] = m;
-        a.vU[o] = v;
-        Unxt[o] = Uold - (m * alpha) / (Math<T>::sqrt(v) + a.eps);
-        m = sM[ms][1][ty][tx];
-        v = sM[ms][3][ty][tx];
-        m += (g[1] - m) * b1c;
-        v += (g[1] * g[1] - v) * b2c;
-        a.mV[o] = m;
-        a.vV[o] = v;
-        Vnxt[o] = Vold - (m * alpha) / (Math<T>::sqrt(v) + a.eps);
+      SM.F[fb][2][sm] = ok ? T(2) * (a.glen3 ? rcbrt_k<T>(Av) : Math<T>::pow(Av, -a.inv_n)) : T(0);
+    }
+    // these generic writes precede a later TMA write to the same buffer
+    if (TMA) tc::fence_proxy_async_smem();
+    __syncthreads();
+
+    // ---- per-cell constants of this tile --------------------------------------------
+    // Working units.  Per level the kernel keeps, per cell, the corner sums
+    //   S = a+b+c+d (= 4 Us),  DX = (b-a)+(d-c) (= Dx / hx),  DY = (c-a)+(d-b) (= Dy / hx)
+    // with hx = 1/(2dx), and per layer the strain components divided by
+    // kappa = 1/(4dx), so that the staggered averages need no multiplications
+    // and sr2 = kappa^2/2 * sr2w; every scale folds into per-tile constants.
+    const int own_sm = R0 * BW + tx + g.ox;
+    P thks, Bs, cs, sbx, sby, ssx, ssy;
+    bool cok[2], own[2], out_ok[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const T* f0 = SM.F[fb][0] + own_sm + e * BW;
+      const T* f1 = SM.F[fb][1] + own_sm + e * BW;
+      const T* f2p = SM.F[fb][2] + own_sm + e * BW;
+      const T* f3 = SM.F[fb][3] + own_sm + e * BW;
+      const T t00 = f0[0], t01 = f0[1], t10 = f0[BW], t11 = f0[BW + 1];
+      const T u00 = f1[0], u01 = f1[1], u10 = f1[BW], u11 = f1[BW + 1];
+      const T th = (((t11 + t10) + t01) + t00) * quarter;
+      const T bs = (((f2p[BW + 1] + f2p[BW]) + f2p[1]) + f2p[0]) * quarter;
+      const T cv = (((f3[BW + 1] + f3[BW]) + f3[1]) + f3[0]) * quarter;
+      const T b00 = u00 - t00, b01 = u01 - t01, b10 = u10 - t10, b11 = u11 - t11;
+      // compute_gradient (staggered): 2 ds / (dx + dx), averaged over the other axis
+      const T id = a.inv_dx;
+      const T bx = half * ((b11 - b10) * id + (b01 - b00) * id);
+      const T by = half * ((b11 - b01) * id + (b10 - b00) * id);
+      const T sx = half * ((u11 - u10) * id + (u01 - u00) * id);
+      const T sy = half * ((u11 - u01) * id + (u10 - u00) * id);
+      if (e == 0) {
+        thks.x = th; Bs.x = bs; cs.x = cv; sbx.x = bx; sby.x = by; ssx.x = sx; ssy.x = sy;
+      } else {
+        thks.y = th; Bs.y = bs; cs.y = cv; sbx.y = bx; sby.y = by; ssx.y = sx; ssy.y = sy;
       }
+      const int cj = g.j0 - 1 + R0 + e, ci = g.i0 - 1 + tx;  // cell (j, i) = node (j, i) of its top-left corner
+      cok[e] = cj >= 0 && cj < ny - 1 && ci >= 0 && ci < nx - 1;
+      own[e] = cok[e] && R0 + e >= 1 && tx >= 1;
+      out_ok[e] = R0 + e >= 1 && tx >= 1 && cj < ny && ci < nx;
+    }
+    // vertical-derivative factor dx / max(thk_s, thr), damped where there is no sliding (times 1/dzeta per layer)
+    const P rzc = {(cs.x > T(0) ? a.dx : T(0.01) * a.dx) / (thks.x > a.thr ? thks.x : a.thr),
+                   (cs.y > T(0) ? a.dx : T(0.01) * a.dx) / (thks.y > a.thr ? thks.y : a.thr)};
+    const P nsbx = sbx * two(T(-1)), nsby = sby * two(T(-1));
+    // energy: shear = esc * sum dz bq sr2w; gravity = egc * (ssx sum w S + ssy sum w SV)
+    const P esc = thks * Bs * two(a.inv_p * a.k2);
+    const P egc = thks * two(a.Kg * T(0.125));
+    // adjoint constants (grad_scale folded in; zero for cells outside the domain, whose
+    // contributions then vanish without masking)
+    const P okm = sel(cok[0], cok[1], two(a.grad_scale), zero);
+    const P gshc = esc * okm;                // dE/d(bq sr2w) per unit dzeta
+    const P gxc = egc * ssx * okm, gyc = egc * ssy * okm;  // dE/dS, dE/dSV per unit gravity weight
+    const P csg = cs * okm * Q4;             // sliding: dE/dS = csg N^(s/2-1) (Us + tb sbx)
+    // output node (R0, tx) of level 0 of this tile, as an element offset
+    const long long obase = ((long long)g.b * nz) * (long long)plane +
+                            (long long)(g.j0 - 1 + R0) * nx + (g.i0 - 1 + tx);
+
+    P e_sh = zero, eGu = zero, eGv = zero, e_slid = zero, e_gf = zero;
+    // previous level's corner sums, pending adjoint of the previous level
+    P pSu = zero, pSv = zero, pXu = zero, pYu = zero, pXv = zero, pYv = zero;
+    P gSu = zero, gXu = zero, gYu = zero, gSv = zero, gXv = zero, gYv = zero;
+    P partU = zero, partV = zero;  // own-node sums of the level awaiting its finish
+    int st_m1 = 0, st_m2 = 0;      // ring slots of the previous two levels
+
+    auto level_q = [&](const T* t, P& S, P& DX, P& DY) {
+      const T* p = t + own_sm;
+      const T a0 = p[0], b0 = p[1], a1 = p[BW], b1 = p[BW + 1], a2 = p[2 * BW], b2 = p[2 * BW + 1];
+      const T s0 = a0 + b0, s1 = a1 + b1, s2 = a2 + b2;
+      const T d0 = b0 - a0, d1 = b1 - a1, d2 = b2 - a2;
+      S = {s0 + s1, s1 + s2};
+      DX = {d0 + d1, d1 + d2};
+      DY = {s1 - s0, s2 - s1};
+    };
+    // corner contributions of a completed level's adjoint (dE/dS, dE/dDX, dE/dDY);
+    // the right-hand corners reach the next lane by shuffles, the node row below
+    // this thread row goes through shared memory
+    auto flush = [&](int lvl, P gS, P gX, P gY, int f, P& part) {
+      const P SmY = gS - gY, SpY = gS + gY;
+      const P c00 = SmY - gX, c01 = SmY + gX, c10 = SpY - gX, c11 = SpY + gX;
+      const T r1 = c01.y + c11.x;
+      const T l0 = __shfl_up_sync(0xffffffffu, c01.x, 1);
+      const T l1 = __shfl_up_sync(0xffffffffu, r1, 1);
+      const T l2 = __shfl_up_sync(0xffffffffu, c11.y, 1);
+      part = c00 + P{l0, c10.x + l1};
+      SM.Down[GRAD ? (lvl & 1) : 0][f][ty][tx] = c10.y + l2;
+    };
+    // node outputs of a flushed level (after a barrier): gradient, or the Adam update
+    auto finish = [&](int lvl, int st) {
+      const int pb = GRAD ? (lvl & 1) : 0;
+      const T upU = ty >= 1 ? SM.Down[pb][0][ty - 1][tx] : T(0);
+      const T upV = ty >= 1 ? SM.Down[pb][1][ty - 1][tx] : T(0);
+      const long long o0 = obase + (long long)lvl * (long long)plane;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        if (!out_ok[e]) continue;
+        const T gu = e ? partU.y : partU.x + upU;
+        const T gv = e ? partV.y : partV.x + upV;
+        const long long o = o0 + (e ? nx : 0);
+        if (MODE == kGradient) {
+          a.dU[o] = gu;
+          a.dV[o] = gv;
+        } else if (MODE == kAdamStep) {
+          const int sm = own_sm + e * BW;
+          const T b1c = T(1) - a.b1, b2c = T(1) - a.b2;
+          T m = SM.M[st][0][sm], v = SM.M[st][2][sm];
+          m += (gu - m) * b1c;
+          v += (gu * gu - v) * b2c;
+          a.mU[o] = m;
+          a.vU[o] = v;
+          Unxt[o] = SM.N[st][0][sm] - adam_step<T>(m * alpha, v, a.eps);
+          m = SM.M[st][1][sm];
+          v = SM.M[st][3][sm];
+          m += (gv - m) * b1c;
+          v += (gv * gv - v) * b2c;
+          a.mV[o] = m;
+          a.vV[o] = v;
+          Vnxt[o] = SM.N[st][1][sm] - adam_step<T>(m * alpha, v, a.eps);
+        }
+      }
+    };
+
+#pragma unroll 2
+    for (int k = 0; k < nz; ++k) {
+      const int nb = cons_st;
+      if (TMA) {
+        // level k landed: one thread waits (the others spend no issue slots polling)
+        if (tid == 0 && !tc::mbar_wait(&SM.full[nb], cons_ph)) load_ok = false;
+      } else {
+        cp_async_wait<kAhead - 1>();  // this thread's copies of level k have landed
+      }
+      __syncthreads();  // level k visible to all; every thread is done with the previous iteration
+      issue_next();
+      if (GRAD && k >= 2) finish(k - 2, st_m2);
+
+      P cSu, cXu, cYu, cSv, cXv, cYv;
+      level_q(SM.N[nb][0], cSu, cXu, cYu);
+      level_q(SM.N[nb][1], cSv, cXv, cYv);
+      // gravity of level k (weight dzeta[k-1] + dzeta[k]) enters its pending adjoint directly
+      const T wk = a.wgrav[k];
+      if (!a.fnge) {
+        eGu = fma2(cSu, two(wk), eGu);
+        eGv = fma2(cSv, two(wk), eGv);
+      }
+      P hSu = zero, hXu = zero, hYu = zero, hSv = zero, hXv = zero, hYv = zero;  // pending adjoint of level k
+      if (GRAD && !a.fnge) {
+        hSu = gxc * two(wk);
+        hSv = gyc * two(wk);
+      }
+
+      if (k == 0) {
+        // Weertman sliding on the basal level (cost_sliding_weertman.py:23-43)
+        const P cUs = cSu * Q4, cVs = cSv * Q4;
+        const P tb = fma2(cVs, sby, cUs * sbx);
+        const P Nn = fma2(tb, tb, fma2(cUs, cUs, cVs * cVs) + two(a.regw2));
+        P Np, dN;  // N^(s/2) and N^(s/2 - 1)
+        if (a.weert3) {
+          dN = rcbrt2(Nn);  // N^(-1/3)
+          Np = Nn * dN;     // N^(2/3)
+        } else {
+          Np = {Math<T>::pow(Nn.x, a.s_w * half), Math<T>::pow(Nn.y, a.s_w * half)};
+          dN = {Math<T>::pow(Nn.x, a.s_w * half - T(1)), Math<T>::pow(Nn.y, a.s_w * half - T(1))};
+        }
+        e_slid = cs * Np * two(a.inv_sw);
+        if (GRAD) {
+          const P gN = csg * dN;
+          hSu = fma2(gN, fma2(tb, sbx, cUs), hSu);
+          hSv = fma2(gN, fma2(tb, sby, cVs), hSv);
+        }
+        if (nz == 1) {
+          pSu = cSu; pSv = cSv; pXu = cXu; pYu = cYu; pXv = cXv; pYv = cYv;
+        }
+      }
+
+      if (k >= 1 || nz == 1) {
+        const int l = nz == 1 ? 0 : k - 1;
+        const T dz = a.dzeta[l];
+        const P rz = rzc * two(a.inv_dzeta[l]);
+        const P uz = (cSu - pSu) * rz, vz = (cSv - pSv) * rz;
+        const P X = fma2(uz, nsbx, pXu + cXu), Y = fma2(uz, nsby, pYu + cYu);
+        const P Z = fma2(vz, nsbx, pXv + cXv), W = fma2(vz, nsby, pYv + cYv);
+        const P ZY = Z + Y;  // 2 Exy (scaled)
+        const P XW = X + W;  // -Ezz (scaled)
+        const P hZY = ZY * H;
+        P t = X * X;
+        t = fma2(W, W, t);
+        t = fma2(XW, XW, t);
+        t = fma2(ZY, hZY, t);
+        const P sr2w = fma2(fma2(vz, vz, uz * uz), H, t);  // sr2 = k2 sr2w
+        const P sc = {sr2w.x < a.lo2 ? a.lo2 : (sr2w.x > a.hi2 ? a.hi2 : sr2w.x),
+                      sr2w.y < a.lo2 ? a.lo2 : (sr2w.y > a.hi2 ? a.hi2 : sr2w.y)};
+        const P base = fma2(sc, two(a.k2), two(a.regu2));
+        const P bq = a.glen3 ? rcbrt2(base) : P{Math<T>::pow(base.x, a.q), Math<T>::pow(base.y, a.q)};
+        e_sh = fma2(bq * sr2w, two(dz), e_sh);
+        P gXh = zero;  // gravity adjoint of this layer under force_negative_gravitational_energy
+        if (a.fnge) {
+          // per layer: twice the staggered u . grad(s) (scaled by 4), kept only where negative
+          P uds = fma2(cSv + pSv, ssy, (cSu + pSu) * ssx);
+          const bool gax = uds.x < T(0), gay = uds.y < T(0);
+          uds = sel(uds.x > T(0), uds.y > T(0), zero, uds);
+          e_gf = fma2(uds, two(dz), e_gf);
+          gXh = sel(gax, gay, two(dz), zero);
+        }
+        if (GRAD) {
+          const bool in_x = sr2w.x >= a.lo2 && sr2w.x <= a.hi2;
+          const bool in_y = sr2w.y >= a.lo2 && sr2w.y <= a.hi2;
+          // d(bq sr2)/d sr2 = bq + q bq / base sr2; bq / base = bq^4 for n = 3
+          P bq_base;
+          if (a.glen3) {
+            const P bq2 = bq * bq;
+            bq_base = bq2 * bq2;
+          } else {
+            bq_base = {bq.x / base.x, bq.y / base.y};
+          }
+          const P qk = {in_x ? a.q * a.k2 : T(0), in_y ? a.q * a.k2 : T(0)};
+          const P G = fma2(qk * bq_base, sr2w, bq) * (gshc * two(dz));  // dE/d sr2w
+          const P G2 = G + G;
+          const P gX = G2 * fma2(X, two(T(2)), W);
+          const P gW = G2 * fma2(W, two(T(2)), X);
+          const P gY = G * ZY;
+          const P Gu = fma2(gX, nsbx, fma2(gY, nsby, G * uz)) * rz;
+          const P Gv = fma2(gY, nsbx, fma2(gW, nsby, G * vz)) * rz;
+          P fgu = zero, fgv = zero;  // gravity under force_negative_gravitational_energy
+          if (a.fnge) {
+            fgu = gxc * gXh;
+            fgv = gyc * gXh;
+          }
+          if (nz == 1) {  // the only layer couples level 0 with itself
+            hXu = gX + gX; hYu = gY + gY; hXv = hYu; hYv = gW + gW;
+            hSu = hSu + (fgu - Gu) + (fgu + Gu);
+            hSv = hSv + (fgv - Gv) + (fgv + Gv);
+          } else {
+            // layer l couples level l (pending g*) and level l+1 (pending h*)
+            gXu = gXu + gX; gYu = gYu + gY; gXv = gXv + gY; gYv = gYv + gW;
+            gSu = gSu + (fgu - Gu);
+            gSv = gSv + (fgv - Gv);
+            hXu = gX; hYu = gY; hXv = gY; hYv = gW;
+            hSu = hSu + (fgu + Gu);
+            hSv = hSv + (fgv + Gv);
+          }
+        }
+      }
+
+      if (GRAD) {
+        if (k >= 1 && nz > 1) {
+          flush(k - 1, gSu, gXu, gYu, 0, partU);
+          flush(k - 1, gSv, gXv, gYv, 1, partV);
+        }
+        gSu = hSu; gXu = hXu; gYu = hYu; gSv = hSv; gXv = hXv; gYv = hYv;
+      }
+      pSu = cSu; pSv = cSv; pXu = cXu; pYu = cYu; pXv = cXv; pYv = cYv;
+      st_m2 = st_m1;
+      st_m1 = nb;
+      if (++cons_st == kStages) {
+        cons_st = 0;
+        cons_ph ^= 1u;
+      }
+    }
+    if (GRAD) {
+      __syncthreads();
+      if (nz >= 2) finish(nz - 2, st_m2);
+      flush(nz - 1, gSu, gXu, gYu, 0, partU);
+      flush(nz - 1, gSv, gXv, gYv, 1, partV);
+      __syncthreads();
+      finish(nz - 1, st_m1);
+    }
+    // this tile's energy densities (owned cells only)
+    const P egrav = a.fnge ? egc * e_gf : egc * fma2(ssy, eGv, ssx * eGu);
+    const P es = sel(own[0], own[1], esc * e_sh, zero);
+    const P eg = sel(own[0], own[1], egrav, zero);
+    const P el = sel(own[0], own[1], e_slid, zero);
+    acc[0] += (double)es.x + (double)es.y;
+    acc[1] += (double)el.x + (double)el.y;
+    acc[2] += (double)eg.x + (double)eg.y;
+  }
+
+  if (!load_ok && a.err) atomicExch(a.err, 1);
+  // ---- energy reduction ---------------------------------------------------------
+  const int nblocks = gridDim.x;
+  const int bid = blockIdx.x;
+  // three FP64 sums over the CTA in a fixed order; every thread gets the totals
+  auto block_sum3 = [&](double (&r)[3]) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      r[0] += __shfl_xor_sync(0xffffffffu, r[0], o);
+      r[1] += __shfl_xor_sync(0xffffffffu, r[1], o);
+      r[2] += __shfl_xor_sync(0xffffffffu, r[2], o);
+    }
+    __syncthreads();
+    if (tx == 0) {
+      SM.red[0][ty] = r[0];
+      SM.red[1][ty] = r[1];
+      SM.red[2][ty] = r[2];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      double s = 0.0;
+      for (int w = 0; w < TYP; ++w) s += SM.red[i][w];
+      r[i] = s;
     }
   };
-
-  for (int k = 0; k < nz; ++k) {
-    const int nb = k % kStages;
-    cp_async_wait<kAhead - 1>();  // this thread's copies of level k have landed
-    __syncthreads();              // ... and everyone's; level k-2's slot is free again
-    issue_level(k + kAhead);
-
-    // level-k cell quantities
-    T cUs, cVs, cDxu, cDyu, cDxv, cDyv, Uold, Vold;
-    {
-      const T a_ = sN[nb][0][ty][tx], b_ = sN[nb][0][ty][tx + 1], c_ = sN[nb][0][ty + 1][tx],
-              d_ = sN[nb][0][ty + 1][tx + 1];
-      cUs = (((d_ + c_) + b_) + a_) * quarter;
-      cDxu = ((b_ - a_) * idx_ + (d_ - c_) * idx_) * half;
-      cDyu = ((c_ - a_) * idx_ + (d_ - b_) * idx_) * half;
-      Uold = a_;
-    }
-    {
-      const T a_ = sN[nb][1][ty][tx], b_ = sN[nb][1][ty][tx + 1], c_ = sN[nb][1][ty + 1][tx],
-              d_ = sN[nb][1][ty + 1][tx + 1];
-      cVs = (((d_ + c_) + b_) + a_) * quarter;
-      cDxv = ((b_ - a_) * idx_ + (d_ - c_) * idx_) * half;
-      cDyv = ((c_ - a_) * idx_ + (d_ - b_) * idx_) * half;
-      Vold = a_;
-    }
-    T hUs = 0, hDxu = 0, hDyu = 0, hVs = 0, hDxv = 0, hDyv = 0;  // pending adjoint of level k
-
-    if (k == 0) {
-      // Weertman sliding on the basal level (cost_sliding_weertman.py:23-43)
-      const T tb = cUs * sbx + cVs * sby;
-      const T N = (cUs * cUs + cVs * cVs) + a.regw2 + tb * tb;
-      T Np, dN;  // N^(s/2) and d(N^(s/2))/dN * (1/s)*s/2 -> handled below
-      if (a.weert3) {
-        const T cr = Math<T>::cbrt(N);
-        Np = cr * cr;                       // N^(2/3)
-        dN = Math<T>::rcbrt(N);             // N^(-1/3)
-      } else {
-        Np = Math<T>::pow(N, a.s_w * half);
-        dN = Math<T>::pow(N, a.s_w * half - T(1));
-      }
-      e_slid = cs * Np * a.inv_sw;
-      if (GRAD) {
-        const T gN = cs * half * dN;        // d(c N^(s/2) / s)/dN
-        hUs += gN * (T(2) * cUs + T(2) * tb * sbx);
-        hVs += gN * (T(2) * cVs + T(2) * tb * sby);
-      }
-      if (nz == 1) {
-        pUs = cUs; pVs = cVs; pDxu = cDxu; pDyu = cDyu; pDxv = cDxv; pDyv = cDyv;
-      }
-    }
-
-    if (k >= 1 || nz == 1) {
-      const int l = nz == 1 ? 0 : k - 1;
-      const T dz = a.dzeta[l];
-      const T axu = (pDxu + cDxu) * half, ayu = (pDyu + cDyu) * half;
-      const T axv = (pDxv + cDxv) * half, ayv = (pDyv + cDyv) * half;
-      const T rz = (fdamp * a.inv_dzeta[l]) * rh;
-      const T uz = (cUs - pUs) * rz, vz = (cVs - pVs) * rz;
-      const T X = axu - uz * sbx, Y = ayu - uz * sby;
-      const T Z = axv - vz * sbx, W = ayv - vz * sby;
-      const T Exy = half * Z + half * Y, Ezz = -X - W;
-      const T srxy = half * (X * X + Exy * Exy + Exy * Exy + W * W + Ezz * Ezz);
-      const T Exz = half * uz, Eyz = half * vz;
-      const T srz = half * (Exz * Exz + Eyz * Eyz + Exz * Exz + Eyz * Eyz);
-      const T sr2 = srxy + srz;
-      const T sc = sr2 < a.sr_lo ? a.sr_lo : (sr2 > a.sr_hi ? a.sr_hi : sr2);
-      const T base = sc + a.regu2;
-      const T bq = a.glen3 ? Math<T>::rcbrt(base) : Math<T>::pow(base, a.q);
-      e_shear += dz * (bq * sr2 * a.inv_p);
-      const T Ub = (pUs + cUs) * half, Vb = (pVs + cVs) * half;
-      T uds = Ub * ssx + Vb * ssy;
-      const bool gact = !a.fnge || uds < T(0);
-      if (a.fnge && uds > T(0)) uds = T(0);
-      e_grav += dz * uds;
-      if (GRAD) {
-        const bool inside = sr2 >= a.sr_lo && sr2 <= a.sr_hi;
-        const T gp = (bq + (inside ? a.q * (bq / base) * sr2 : T(0))) * a.inv_p;  // d p_term / d sr2
-        const T gs = gshear * dz * gp;
-        const T GX = gs * (T(2) * X + W);
-        const T GW = gs * (T(2) * W + X);
-        const T GY = gs * Exy;
-        const T Guz = gs * half * uz - GX * sbx - GY * sby;
-        const T Gvz = gs * half * vz - GY * sbx - GW * sby;
-        const T gg = gact ? ggrav * dz * half : T(0);
-        // layer l couples level l (pending g*) and level l+1 (pending h*)
-        gDxu += GX * half; hDxu += GX * half;
-        gDyu += GY * half; hDyu += GY * half;
-        gDxv += GY * half; hDxv += GY * half;
-        gDyv += GW * half; hDyv += GW * half;
-        gUs += -Guz * rz + gg * ssx; hUs += Guz * rz + gg * ssx;
-        gVs += -Gvz * rz + gg * ssy; hVs += Gvz * rz + gg * ssy;
-      }
-    }
-
-    if (GRAD) {
-      if (nz == 1) {
-        hUs += gUs; hDxu += gDxu; hDyu += gDyu; hVs += gVs; hDxv += gDxv; hDyv += gDyv;
-      } else if (k >= 1) {
-        flush_level(k - 1, gUs, gDxu, gDyu, gVs, gDxv, gDyv, prevUold, prevVold);
-      }
-      gUs = hUs; gDxu = hDxu; gDyu = hDyu; gVs = hVs; gDxv = hDxv; gDyv = hDyv;
-    }
-    pUs = cUs; pVs = cVs; pDxu = cDxu; pDyu = cDyu; pDxv = cDxv; pDyv = cDyv;
-    prevUold = Uold;
-    prevVold = Vold;
-  }
-  if (GRAD) {
-    flush_level(nz - 1, gUs, gDxu, gDyu, gVs, gDxv, gDyv, prevUold, prevVold);
-  }
-
-  // ---- energy reduction ---------------------------------------------------------
-  const T es = owner ? thks * (Bs * e_shear) : T(0);
-  const T eg = owner ? a.Kg * thks * e_grav : T(0);
-  const T el = owner ? e_slid : T(0);
-  const int nblocks = gridDim.x * gridDim.y * gridDim.z;
-  const int bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-  const double s0 = block_sum<NT>((double)es, sRed, tid);
-  const double s1 = block_sum<NT>((double)el, sRed, tid);
-  const double s2 = block_sum<NT>((double)eg, sRed, tid);
+  block_sum3(acc);
   if (tid == 0) {
-    a.partials[3 * (size_t)bid + 0] = s0;
-    a.partials[3 * (size_t)bid + 1] = s1;
-    a.partials[3 * (size_t)bid + 2] = s2;
+    a.partials[3 * (size_t)bid + 0] = acc[0];
+    a.partials[3 * (size_t)bid + 1] = acc[1];
+    a.partials[3 * (size_t)bid + 2] = acc[2];
     __threadfence();
-    sTicket = atomicAdd(a.counter, 1u);
+    SM.ticket = atomicAdd(a.counter, 1u);
   }
   __syncthreads();
-  if (sTicket != (unsigned)(nblocks - 1)) return;
+  if (SM.ticket != (unsigned)(nblocks - 1)) return;
   __threadfence();
   double r[3] = {0.0, 0.0, 0.0};
   for (int i = tid; i < nblocks; i += NT) {
@@ -444,15 +732,15 @@ __global__ void __launch_bounds__(kTX* TYC, MinBlocks<T>::value) stencil_kernel(
     r[1] += __ldcg(&a.partials[3 * (size_t)i + 1]);
     r[2] += __ldcg(&a.partials[3 * (size_t)i + 2]);
   }
-  const double t0 = block_sum<NT>(r[0], sRed, tid);
-  const double t1 = block_sum<NT>(r[1], sRed, tid);
-  const double t2 = block_sum<NT>(r[2], sRed, tid);
+  block_sum3(r);
+  const double t0 = r[0], t1 = r[1], t2 = r[2];
   if (tid == 0) {
     *a.counter = 0u;
+    const bool lost = a.err && __ldcg(a.err) != 0;
     if (a.terms) {
-      a.terms[0] = t0;
-      a.terms[1] = t1;
-      a.terms[2] = t2;
+      a.terms[0] = lost ? nan("") : t0;
+      a.terms[1] = lost ? nan("") : t1;
+      a.terms[2] = lost ? nan("") : t2;
     }
     if (MODE == kAdamStep) {
       igm_solver_ctl* ctl = a.ctl;
@@ -462,7 +750,10 @@ __global__ void __launch_bounds__(kTX* TYC, MinBlocks<T>::value) stencil_kernel(
       ctl->terms[0] = t0 * a.inv_count;
       ctl->terms[1] = t1 * a.inv_count;
       ctl->terms[2] = t2 * a.inv_count;
-      if (!isfinite(cost)) {
+      if (lost) {
+        ctl->status = IGM_ERR_CUDA;
+        ctl->stopped = 1;
+      } else if (!isfinite(cost)) {
         ctl->status = IGM_ERR_NAN_DETECTED;
         ctl->stopped = 1;
       } else if (a.es_enabled) {
@@ -492,11 +783,8 @@ __global__ void __launch_bounds__(kTX* TYC, MinBlocks<T>::value) stencil_kernel(
 // host side
 // ---------------------------------------------------------------------------
 
-// Cell rows per CTA (256 threads; several CTAs per SM keep enough loads in flight).
-template <typename T> struct TileRows { static constexpr int value = 8; };
-
 static inline int grid_blocks_rows(const igm_grid* g, int tyc, dim3* grid) {
-  *grid = dim3((g->nx + kTX - 2) / (kTX - 1), (g->ny + tyc - 2) / (tyc - 1), g->batch);
+  *grid = dim3((g->nx + kCW - 2) / (kCW - 1), (g->ny + tyc - 2) / (tyc - 1), g->batch);
   return (int)(grid->x * grid->y * grid->z);
 }
 // The workspace is sized for the smaller tile (more CTAs) so one size fits both dtypes.
@@ -539,6 +827,22 @@ static void fill_common(StencilArgs<T>& s, const igm_grid* g, const igm_physics*
   s.s_w = (T)(1.0 + 1.0 / m);
   s.inv_sw = (T)(1.0 / (1.0 + 1.0 / m));
   s.regw2 = (T)(ph->regu_weertman * ph->regu_weertman);
+  const double k2 = 1.0 / (32.0 * g->dx * g->dx);
+  s.k2 = (T)k2;
+  s.lo2 = (T)((double)s.sr_lo / k2);
+  s.hi2 = (T)((double)s.sr_hi / k2);
+  for (int k = 0; k < IGM_MAX_NZ; ++k) {
+    double w = 0.0;
+    if (k < g->nz) {
+      if (g->nz == 1) {
+        w = 2.0 * g->dzeta[0];
+      } else {
+        if (k >= 1) w += g->dzeta[k - 1];
+        if (k <= g->nz - 2) w += g->dzeta[k];
+      }
+    }
+    s.wgrav[k] = (T)w;
+  }
   s.glen3 = n == 3.0;
   s.weert3 = m == 3.0;
   s.fnge = ph->force_negative_gravitational_energy != 0;
@@ -565,24 +869,105 @@ static int bind_workspace(void* ws, size_t bytes, const igm_grid* g, unsigned in
   return IGM_OK;
 }
 
-template <typename T, int MODE>
-static int launch_stencil(const StencilArgs<T>& s, const igm_grid* g, cudaStream_t st) {
-  constexpr int TYC = TileRows<T>::value;
-  constexpr size_t smem = sizeof(StencilSmem<T, TYC, MODE>);
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(stencil_kernel<T, TYC, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) {
-      set_error("stencil_kernel smem attribute: %s", cudaGetErrorString(e));
+// 3-D tensor map over [planes][ny][nx] of T with the node-tile box: planes =
+// batch * nz for the levels of U, V and the moments, batch for the 2-D fields.
+template <typename T>
+static int level_map(CUtensorMap* m, const void* base, const igm_grid* g, int planes) {
+  tc::EncodeTiledFn enc = tc::encode_tiled_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is not available from the CUDA driver");
+    return IGM_ERR_CUDA;
+  }
+  constexpr int TYC = 2 * ThreadRows<T>::value;
+  cuuint64_t dims[3] = {(cuuint64_t)g->nx, (cuuint64_t)g->ny, (cuuint64_t)planes};
+  cuuint64_t strides[2] = {(cuuint64_t)g->nx * sizeof(T), (cuuint64_t)g->ny * g->nx * sizeof(T)};
+  cuuint32_t box[3] = {(cuuint32_t)Box<T>::BW, (cuuint32_t)(TYC + 1), 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                   const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled (level tiles) failed (CUresult %d)", (int)r);
+    return IGM_ERR_CUDA;
+  }
+  return IGM_OK;
+}
+
+// SM count of the current device, looked up once per device.
+static int sm_count_current(int* out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  constexpr int kMaxDevices = 128;
+  static int cache[kMaxDevices] = {};
+  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    set_error("cudaGetDevice: %s", cudaGetErrorString(e));
+    return IGM_ERR_CUDA;
+  }
+  if (cache[dev] == 0) {
+    int n = 0;
+    e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess || n <= 0) {
+      set_error("cudaDeviceGetAttribute(MultiProcessorCount): %s", cudaGetErrorString(e));
       return IGM_ERR_CUDA;
     }
-    configured = true;
+    cache[dev] = n;
   }
-  dim3 gr;
-  grid_blocks_rows(g, TYC, &gr);
-  stencil_kernel<T, TYC, MODE><<<gr, dim3(kTX, TYC), smem, st>>>(s);
+  *out = cache[dev];
+  return IGM_OK;
+}
+
+template <typename T>
+static int field_maps(StencilMaps* maps, const igm_fields* f, const igm_grid* g) {
+  int rc;
+  if ((rc = level_map<T>(&maps->thk, f->thk, g, g->batch)) || (rc = level_map<T>(&maps->usurf, f->usurf, g, g->batch)) ||
+      (rc = level_map<T>(&maps->A, f->arrhenius, g, g->batch)) || (rc = level_map<T>(&maps->C, f->slidingco, g, g->batch)))
+    return rc;
+  return IGM_OK;
+}
+
+// TMA needs 16-byte aligned bases and a row pitch that is a multiple of 16 bytes.
+template <typename T>
+static bool tma_usable(const igm_grid* g, std::initializer_list<const void*> ptrs) {
+  if (((size_t)g->nx * sizeof(T)) % 16 != 0) return false;
+  for (const void* p : ptrs)
+    if (p == nullptr || ((uintptr_t)p & 15) != 0) return false;
+  return true;
+}
+
+// Persistent launch: as many CTAs as fit on the device at once (at most one per tile).
+template <typename T, int MODE, bool TMA>
+static int launch_stencil_t(const StencilArgs<T>& s, const StencilMaps& maps, const igm_grid* g, cudaStream_t st) {
+  constexpr int TYP = ThreadRows<T>::value;
+  constexpr int TYC = 2 * TYP;
+  constexpr size_t smem = sizeof(StencilSmem<T, TYP, MODE>) + 128;
+  auto kern = stencil_kernel<T, TYP, MODE, TMA>;
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    int n = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kCW * TYP, smem);
+    if (e != cudaSuccess) {
+      set_error("stencil_kernel configuration: %s", cudaGetErrorString(e));
+      return IGM_ERR_CUDA;
+    }
+    per_sm = n > 0 ? n : 1;
+  }
+  int sms = 0;
+  int rc = sm_count_current(&sms);
+  if (rc) return rc;
+  const long long ntiles = (long long)((g->nx + kCW - 2) / (kCW - 1)) * ((g->ny + TYC - 2) / (TYC - 1)) * g->batch;
+  const long long cap = (long long)per_sm * sms;
+  const int grid = (int)(ntiles < cap ? ntiles : cap);
+  kern<<<grid, dim3(kCW, TYP), smem, st>>>(s, maps);
   return launch_status("stencil_kernel");
+}
+
+template <typename T, int MODE>
+static int launch_stencil(const StencilArgs<T>& s, const StencilMaps& maps, bool tma, const igm_grid* g,
+                          cudaStream_t st) {
+  return tma ? launch_stencil_t<T, MODE, true>(s, maps, g, st) : launch_stencil_t<T, MODE, false>(s, maps, g, st);
 }
 
 template <typename T>
@@ -598,8 +983,18 @@ static int energy_t(const igm_grid* g, const igm_physics* ph, const igm_fields* 
   s.terms = terms;
   int rc = bind_workspace(ws, wsb, g, &s.counter, &s.partials);
   if (rc) return rc;
-  if (dU) return launch_stencil<T, kGradient>(s, g, st);
-  return launch_stencil<T, kEnergyOnly>(s, g, st);
+  s.err = (int*)((char*)ws + 4);
+  StencilMaps maps;
+  memset(&maps, 0, sizeof(maps));
+  const bool tma = tma_usable<T>(g, {U, V, f->thk, f->usurf, f->arrhenius, f->slidingco});
+  if (tma) {
+    const int nl = g->batch * g->nz;
+    if ((rc = level_map<T>(&maps.U0, U, g, nl)) || (rc = level_map<T>(&maps.V0, V, g, nl)) ||
+        (rc = field_maps<T>(&maps, f, g)))
+      return rc;
+  }
+  if (dU) return launch_stencil<T, kGradient>(s, maps, tma, g, st);
+  return launch_stencil<T, kEnergyOnly>(s, maps, tma, g, st);
 }
 
 template <typename T>
@@ -631,8 +1026,22 @@ static int solver_t(const igm_grid* g, const igm_physics* ph, const igm_fields* 
   s.grad_scale = (T)s.inv_count;
   int rc = bind_workspace(ws, wsb, g, &s.counter, &s.partials);
   if (rc) return rc;
+  s.err = (int*)((char*)ws + 4);
+  StencilMaps maps;
+  memset(&maps, 0, sizeof(maps));
+  const bool tma =
+      tma_usable<T>(g, {U0, V0, U1, V1, mU, mV, vU, vV, f->thk, f->usurf, f->arrhenius, f->slidingco});
+  if (tma) {
+    const int nl = g->batch * g->nz;
+    if ((rc = level_map<T>(&maps.U0, U0, g, nl)) || (rc = level_map<T>(&maps.V0, V0, g, nl)) ||
+        (rc = level_map<T>(&maps.U1, U1, g, nl)) || (rc = level_map<T>(&maps.V1, V1, g, nl)) ||
+        (rc = level_map<T>(&maps.mU, mU, g, nl)) || (rc = level_map<T>(&maps.mV, mV, g, nl)) ||
+        (rc = level_map<T>(&maps.vU, vU, g, nl)) || (rc = level_map<T>(&maps.vV, vV, g, nl)) ||
+        (rc = field_maps<T>(&maps, f, g)))
+      return rc;
+  }
   for (int i = 0; i < n_it; ++i) {
-    rc = launch_stencil<T, kAdamStep>(s, g, st);
+    rc = launch_stencil<T, kAdamStep>(s, maps, tma, g, st);
     if (rc) return rc;
   }
   return IGM_OK;
