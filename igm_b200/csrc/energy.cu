@@ -362,8 +362,9 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
   };
   // issue cursor over the sequence (tile, level)
   int iss_i = 0, iss_k = 0, iss_st = 0;
-  TileGeo ig = geo(0);
+  TileGeo ig = geo(0);  // geometry of the tile at the cursor
   auto issue_next = [&]() {
+    if (TMA && tid != 0) return;  // TMA: only the issuing thread tracks the cursor
     if (iss_i < my_tiles) issue_level(ig, iss_k, iss_st);
     if (!TMA) cp_async_commit();  // one group per sequence position, possibly empty
     iss_st = iss_st + 1 == kStages ? 0 : iss_st + 1;
@@ -389,7 +390,7 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
     const TileGeo g = geo(i);
     const int fb = TMA ? (i & 1) : 0;
     if (TMA) {
-      if (i + 1 < my_tiles) issue_fields(geo(i + 1), fb ^ 1);
+      if (tid == 0 && i + 1 < my_tiles) issue_fields(geo(i + 1), fb ^ 1);
       // one thread waits for the transfer; the barrier publishes it to the CTA
       if (tid == 0 && !tc::mbar_wait(&SM.ffull[fb], (uint32_t)((i >> 1) & 1))) load_ok = false;
       __syncthreads();
