@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--pretrain", type=int, default=6000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    # iterations of the untimed reference solve, as a fraction of the full schedule
+    # (small values make quick profiling runs; the timed region is unchanged)
+    ap.add_argument("--ref-scale", type=float, default=1.0)
     return ap.parse_args()
 
 
@@ -125,7 +128,7 @@ class ClockSampler:
 def make_state(args, host=False):
     import torch
     from igm_b200.state import State
-    from oracle.iceflow_oracle import valley_glacier  # synthetic input generator only
+    from igm_b200.synthetic import valley_glacier
     g = valley_glacier(args.size, args.size, 50.0, seed=0, varying_coeffs=True)
     st = State()
     for k in ["topg", "thk", "arrhenius", "slidingco"]:
@@ -213,7 +216,7 @@ def pretrain_emulator(args, nsteps):
     return run
 
 
-def converged_minimum(cfg, st):
+def converged_minimum(cfg, st, scale=1.0):
     """FP64 minimum of the state's energy (untimed): Adam from zero with a
     decreasing step size in FP32, then polished in FP64.  Returns FP32 U, V."""
     import torch
@@ -227,11 +230,13 @@ def converged_minimum(cfg, st):
     U = torch.zeros((nz,) + tuple(f[0].shape), device=f[0].device, dtype=torch.float32)
     V = torch.zeros_like(U)
     for lr, n in [(100.0, 1000), (30.0, 2000), (10.0, 2000), (3.0, 2000), (1.0, 2000), (0.3, 2000), (0.1, 2000)]:
-        U, V, _ = DeviceAdamSolver(lr).solve(U, V, *f, 50.0, dz, nbitmax=n, phys=ph, early_stopping=False)
+        U, V, _ = DeviceAdamSolver(lr).solve(U, V, *f, 50.0, dz, nbitmax=max(1, int(n * scale)), phys=ph,
+                                             early_stopping=False)
     f64 = [x.double() for x in f]
     U, V = U.double(), V.double()
     for lr, n in [(0.3, 2000), (0.1, 2000), (0.03, 2000)]:
-        U, V, _ = DeviceAdamSolver(lr).solve(U, V, *f64, 50.0, dz, nbitmax=n, phys=ph, early_stopping=False)
+        U, V, _ = DeviceAdamSolver(lr).solve(U, V, *f64, 50.0, dz, nbitmax=max(1, int(n * scale)), phys=ph,
+                                             early_stopping=False)
     return U.float(), V.float()
 
 
@@ -299,7 +304,7 @@ def run_ours(args, rank, world, dist):
     res["setup_s"] = time.time() - t0
     # the FP64 minimum of the initial state: yardstick of the emulator, start of the plain run
     t0 = time.time()
-    Ur, Vr = converged_minimum(cfg_e, st)
+    Ur, Vr = converged_minimum(cfg_e, st, args.ref_scale)
     res["reference_solve_s"] = time.time() - t0
     from igm_b200.emulator import update_iceflow_emulated
     from igm_b200.processes.iceflow import set_derived_velocities
@@ -321,8 +326,10 @@ def run_ours(args, rank, world, dist):
     clk.start()
 
     def run_em(K):
+        torch.cuda.nvtx.range_push("timed_emulated")
         for _ in range(K):
             step(cfg_e, st, mods)
+        torch.cuda.nvtx.range_pop()
     el_e, _ = timed(run_em, args.steps, sync)
     clocks = clk.stop()
     launches = lib.igm_launch_count() - l0
@@ -344,7 +351,12 @@ def run_ours(args, rank, world, dist):
         step(cfg_s, st, mods)
     t_start = float(st.t)
     it0 = st.iceflow_solver.iterations
-    el_s, _ = timed(lambda K: [step(cfg_s, st, mods) for _ in range(K)], args.steps, sync)
+    def run_sv(K):
+        torch.cuda.nvtx.range_push("timed_plain")
+        for _ in range(K):
+            step(cfg_s, st, mods)
+        torch.cuda.nvtx.range_pop()
+    el_s, _ = timed(run_sv, args.steps, sync)
     years_s = float(st.t) - t_start
     el_s = max_over_ranks(el_s)
     res["solved"] = dict(years=years_s, seconds=el_s, years_per_s=years_s / el_s,
@@ -382,12 +394,14 @@ def roofline_conv(conv_ms, size, peaks):
     byts = 2 * 64 * size * size
     achieved = byts / t / 1e9
     peak = peaks.get("hbm_gbs", 6650.0)
+    # DRAM traffic of one launch from the committed ncu capture (batch 2 x 1000 x 1000), scaled to this
+    # launch's pixels (the traffic is proportional to the pixels processed)
     traffic = None
     prof = os.path.join(ROOT, "profiles", "conv3x3_fwd_1000x1000.txt")
     if os.path.exists(prof):
         for line in open(prof):
             if line.startswith("dram_bytes_per_launch:"):
-                traffic = float(line.split(":")[1])
+                traffic = round(float(line.split(":")[1]) * (size * size) / (2 * 1000 * 1000))
     return {"kernel": "conv3x3_kernel<4,4,fwd> (tcgen05, cin 32)", "bound": "hbm", "achieved": round(achieved, 1),
             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
             "algorithmic_bytes": byts, "avg_launch_us": round(t * 1e6, 2), "launches": len(conv_ms),
@@ -404,7 +418,8 @@ def cpu_sample(args, nthreads, steps=1):
     from oracle import iceflow_oracle as O
     torch.set_num_threads(nthreads)
     nz = args.nz
-    g = O.valley_glacier(args.size, args.size, 50.0, seed=0, varying_coeffs=True)
+    from igm_b200.synthetic import valley_glacier
+    g = valley_glacier(args.size, args.size, 50.0, seed=0, varying_coeffs=True)
     f = {k: torch.as_tensor(g[k]) for k in ["thk", "usurf", "arrhenius", "slidingco", "topg"]}
     w = O.define_vertical_weight(nz, 4.0)
     dt = DT_CFL_INITIAL

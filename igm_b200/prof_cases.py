@@ -1,0 +1,57 @@
+"""One launch of each hot kernel on a case larger than L2, for profiling
+(``python -m igm_b200.prof_cases``; run it under ncu with -k and -c).
+
+Stencil (energy, energy + adjoint, one fused Adam iteration) and transport at
+1500 x 1500 x Nz 10 in FP32; the tensor-core convolution (forward, dgrad,
+wgrad) at batch 2 x 1000 x 1000 x 32 channels.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from . import kernels as K
+from .solver import DeviceAdamSolver
+from .synthetic import valley_glacier
+from .vertical import compute_levels, compute_zeta_dzeta
+
+
+def main():
+    N, nz = 1500, 10
+    st = valley_glacier(N, N, 50.0, seed=0, varying_coeffs=True)
+    f = [torch.as_tensor(st[k]).cuda() for k in ["thk", "usurf", "arrhenius", "slidingco"]]
+    dz = compute_zeta_dzeta(compute_levels(nz, 4.0))[1]
+    rng = np.random.default_rng(0)
+    U = torch.as_tensor(rng.normal(30, 20, (nz, N, N)).astype(np.float32)).cuda()
+    V = torch.as_tensor(rng.normal(0, 20, (nz, N, N)).astype(np.float32)).cuda()
+    K.energy(U, V, *f, 50.0, dz)                                  # stencil: energy
+    K.energy(U, V, *f, 50.0, dz, grad=True)                       # stencil: energy + adjoint
+    DeviceAdamSolver().solve(U, V, *f, 50.0, dz, nbitmax=1, early_stopping=False, mask=False)  # fused Adam step
+    ub, vb = U[0].contiguous(), V[0].contiguous()
+    K.transport_step(ub, vb, f[0], f[1], None, 50.0, 0.01)       # transport
+    B, H, W = 2, 1000, 1000                                       # 2 x 64 MB activations (> L2)
+    x = torch.randn(B, H, 4, W, 8, device="cuda").to(torch.bfloat16)
+    y = torch.empty_like(x)
+    y2 = torch.empty_like(x)
+    wp = (torch.randn(9 * 4 * 32 * 8, device="cuda") * 0.05).to(torch.bfloat16)
+    bias = torch.zeros(32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    lib, s = L.lib(), L.stream_ptr()
+    L.check(lib.igm_conv3x3(0, B, H, W, 32, x.data_ptr(), wp.data_ptr(), bias.data_ptr(), None, y.data_ptr(), None,
+                            0, 0.01, err.data_ptr(), s), "conv forward")
+    dbp = torch.zeros(148, 32, device="cuda")
+    L.check(lib.igm_conv3x3(1, B, H, W, 32, y.data_ptr(), wp.data_ptr(), None, x.data_ptr(), y2.data_ptr(),
+                            dbp.data_ptr(), 148, 0.01, err.data_ptr(), s), "conv dgrad")
+    part = torch.empty(148, 3, 128, 32, device="cuda")
+    L.check(lib.igm_conv3x3_wgrad(B, H, W, 32, x.data_ptr(), y.data_ptr(), part.data_ptr(), 148, err.data_ptr(), s),
+            "conv wgrad")
+    torch.cuda.synchronize()
+    if int(err.item()) != 0:
+        raise RuntimeError(f"kernel error flag {int(err.item())}")
+    print("ok")
+
+
+if __name__ == "__main__":
+    main()

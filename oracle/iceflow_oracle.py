@@ -506,70 +506,10 @@ def split_into_patches(X, nbmax):
 
 
 # --------------------------------------------------------------------------
-# synthetic glaciers (the shapes and distributions of the benchmark configs)
+# synthetic glaciers: the input generators live in the package and are
+# re-exported here for the tests
 # --------------------------------------------------------------------------
-
-
-def box_filter(a: np.ndarray, k: int = 5) -> np.ndarray:
-    """k x k moving average with edge replication."""
-    r = k // 2
-    p = np.pad(a, r, mode="edge")
-    c = np.cumsum(np.cumsum(p, 0), 1)
-    c = np.pad(c, ((1, 0), (1, 0)))
-    return (c[k:, k:] - c[:-k, k:] - c[k:, :-k] + c[:-k, :-k]) / (k * k)
-
-
-def valley_glacier(ny=100, nx=100, dx=100.0, seed=0, noise_sigma=5.0, varying_coeffs=False):
-    """Synthetic valley glacier.
-
-    The 10 km x 10 km valley of the 100x100 / dx=100 m case; larger grids map
-    their domain onto the same shape (coordinates scaled to 10 km), and the
-    bed noise is scaled with dx/100 m so its slope stays the same.
-    Bed: 3000 - 0.1 X + 0.002 (Y-5000)^2 + N(0, sigma^2);
-    thk = max(0, 300 (1-((Y-5000)/2500)^2) (1-X/10000)); usurf = topg + thk.
-    A = 78, c = 0.045 uniform, or (``varying_coeffs``) log-uniform per cell
-    in [20,150] and [0.01,0.1], smoothed with a 5-cell box filter.
-    Returns float32 numpy arrays.
-    """
-    rng = np.random.default_rng(seed)
-    Lx, Ly = nx * dx, ny * dx
-    x = np.arange(nx) * dx * (10000.0 / Lx)
-    y = np.arange(ny) * dx * (10000.0 / Ly)
-    X, Y = np.meshgrid(x, y)
-    sigma = noise_sigma * (dx / 100.0) if (nx, ny) != (100, 100) else noise_sigma
-    topg = 3000.0 - 0.1 * X + 0.002 * (Y - 5000.0) ** 2 + rng.normal(0.0, sigma, size=(ny, nx))
-    thk = np.maximum(0.0, 300.0 * (1.0 - ((Y - 5000.0) / 2500.0) ** 2) * (1.0 - X / 10000.0))
-    usurf = topg + thk
-    if varying_coeffs:
-        A = np.exp(rng.uniform(np.log(20.0), np.log(150.0), size=(ny, nx)))
-        c = np.exp(rng.uniform(np.log(0.01), np.log(0.1), size=(ny, nx)))
-        A = box_filter(A, 5)
-        c = box_filter(c, 5)
-    else:
-        A = np.full((ny, nx), 78.0)
-        c = np.full((ny, nx), 0.045)
-    f = lambda a: np.ascontiguousarray(a, dtype=np.float32)
-    return dict(topg=f(topg), thk=f(thk), usurf=f(usurf), arrhenius=f(A), slidingco=f(c), dx=float(dx))
-
-
-def ridge_glacier(n=4096, dx=25.0, seed=0, n_ridges=12):
-    """Multi-valley bed: a 0.05-slope plane plus seeded Gaussian ridges
-    (height 500-1500 m, sigma 2-8 km).  thk starts at zero (the caller spins
-    it up).  A, c log-uniform per cell as in ``valley_glacier``."""
-    rng = np.random.default_rng(seed)
-    x = np.arange(n) * dx
-    X, Y = np.meshgrid(x, x)
-    topg = 3500.0 - 0.05 * X
-    for _ in range(n_ridges):
-        cx, cy = rng.uniform(0, n * dx, size=2)
-        h = rng.uniform(500.0, 1500.0)
-        s = rng.uniform(2000.0, 8000.0)
-        topg = topg + h * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * s * s))
-    A = box_filter(np.exp(rng.uniform(np.log(20.0), np.log(150.0), size=(n, n))), 5)
-    c = box_filter(np.exp(rng.uniform(np.log(0.01), np.log(0.1), size=(n, n))), 5)
-    thk = np.zeros((n, n))
-    f = lambda a: np.ascontiguousarray(a, dtype=np.float32)
-    return dict(topg=f(topg), thk=f(thk), usurf=f(topg), arrhenius=f(A), slidingco=f(c), dx=float(dx))
+from igm_b200.synthetic import box_filter, ridge_glacier, valley_glacier  # noqa: E402,F401
 
 
 # --------------------------------------------------------------------------
