@@ -133,11 +133,13 @@ class CNN:
             if train:
                 b["g"] = [act(F), act(F)]
                 npart = self.n_sm
-                b["npart"] = npart
-                b["wpart"] = torch.empty((npart, 3, 128, F), dtype=torch.float32, device=d)
+                b["npart"] = npart          # persistent tensor-core kernels: one CTA per SM
+                b["npart2"] = 2 * npart     # head / first-layer reductions: two CTAs per SM
+                b["wpart"] = torch.empty(max(npart * 3 * 128 * F, 2 * npart * 9 * self.cin * F),
+                                         dtype=torch.float32, device=d)
                 b["dbpart"] = torch.zeros((npart, F), dtype=torch.float32, device=d)
                 hl = int(L.lib().igm_cnn_head_partial_len(self.nz))
-                b["hpart"] = torch.empty((npart, hl), dtype=torch.float32, device=d)
+                b["hpart"] = torch.empty((2 * npart, hl), dtype=torch.float32, device=d)
             self._bufs[key] = b
         return b
 
@@ -193,19 +195,19 @@ class CNN:
         (planar [B, nz, h, w]); requires forward(keep_acts=True)."""
         lib, st = L.lib(), L.stream_ptr()
         acts = buf["acts"]
-        npart = buf["npart"]
+        npart, npart2 = buf["npart"], buf["npart2"]
         hw = self.params.data_ptr() + 4 * self.offsets[2 * self.L]
         hl = buf["hpart"].shape[1]
         g = buf["g"]
         rc = lib.igm_cnn_head_backward(B, h, w, self.nz, _p(acts[self.L - 1]), hw, _p(dU), _p(dV), self.out_scale,
-                                       self.alpha, _p(g[0]), _p(buf["hpart"]), npart, st)
+                                       self.alpha, _p(g[0]), _p(buf["hpart"]), npart2, st)
         L.check(rc, "igm_cnn_head_backward")
         gp = self.grads.data_ptr()
         nh = F * self.nout
         # head kernel + bias gradients, last conv layer's bias gradient
-        L.check(lib.igm_reduce_partials(_p(buf["hpart"]), npart, nh + self.nout, hl,
+        L.check(lib.igm_reduce_partials(_p(buf["hpart"]), npart2, nh + self.nout, hl,
                                         gp + 4 * self.offsets[2 * self.L], 0, st), "reduce head")
-        L.check(lib.igm_reduce_partials(buf["hpart"].data_ptr() + 4 * (nh + self.nout), npart, F, hl,
+        L.check(lib.igm_reduce_partials(buf["hpart"].data_ptr() + 4 * (nh + self.nout), npart2, F, hl,
                                         gp + 4 * self.offsets[2 * (self.L - 1) + 1], 0, st), "reduce db")
         cur = 0
         for l in range(self.L - 1, -1, -1):
@@ -219,9 +221,9 @@ class CNN:
             else:
                 n1 = 9 * self.cin * F
                 rc = lib.igm_cnn_layer1_wgrad(B, h, w, self.cin, *[_p(f) for f in buf["fields"]], buf["dx"],
-                                              self._scales(), _p(gl), _p(buf["wpart"]), npart, st)
+                                              self._scales(), _p(gl), _p(buf["wpart"]), npart2, st)
                 L.check(rc, "igm_cnn_layer1_wgrad")
-                L.check(lib.igm_reduce_partials(_p(buf["wpart"]), npart, n1, n1, gp + 4 * self.offsets[0], 0, st),
+                L.check(lib.igm_reduce_partials(_p(buf["wpart"]), npart2, n1, n1, gp + 4 * self.offsets[0], 0, st),
                         "reduce layer-1 wgrad")
             if l > 0:
                 nxt = g[1 - cur]

@@ -177,113 +177,167 @@ __global__ void __launch_bounds__(256) head_fwd_kernel(int B, int H, int W, int 
 //   dPre16 = (dY Wh^T) * LeakyReLU'(A16)  (bf16, row-chunked),
 //   partials per block of dWh [32][nout], dbh [nout] and db16 [32].
 // ---------------------------------------------------------------------------
-constexpr int kHB = 128;  // pixels per chunk
-__global__ void __launch_bounds__(256) head_bwd_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act,
-                                                       const float* wh, const float* dU, const float* dV,
-                                                       float out_scale, float alpha, __nv_bfloat16* dpre,
-                                                       float* partial) {
-  extern __shared__ float sm[];
+// Work split: a warp takes 32 consecutive pixels; each lane loads its pixel,
+// computes that pixel's dPre16 and stages the operands in the warp's shared
+// memory; then lane l owns input channel ci = l and accumulates the outer
+// products over the 32 pixels (dWh[l][:], db16[l]) from broadcast reads --
+// no block barrier inside the pixel loop.  Warps are summed in a fixed order
+// at the end (deterministic).  NJ >= nout is the per-lane accumulator count.
+constexpr int kHeadWarps = 8;
+template <int NJ>
+struct HeadBwdSmem {
+  static constexpr int GS = NJ + 4;                     // output-gradient row stride (16-byte aligned rows)
+  static constexpr int WARP = 32 * 33 * 2 + 32 * GS;    // per warp: activations, masked dPre, gradients
+  static constexpr int RED = kF * NJ + NJ + kF;         // per-warp results for the final sum
+  static constexpr int FLOATS = NJ * kF + kHeadWarps * (WARP > RED ? WARP : RED);
+};
+template <int NJ>
+__global__ void __launch_bounds__(kHeadWarps * 32, 2)
+    head_bwd_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act, const float* wh, const float* dU,
+                    const float* dV, float out_scale, float alpha, __nv_bfloat16* dpre, float* partial) {
+  using SM_ = HeadBwdSmem<NJ>;
+  constexpr int GS = SM_::GS;
+  extern __shared__ __align__(16) float sm[];
   const int nout = 2 * nz;
-  float* sw = sm;                          // [32][nout]
-  float* sA = sw + kF * nout;              // [kHB][33]
-  float* sD = sA + kHB * 33;               // [kHB][nout + 1]
-  float* sP = sD + kHB * (nout + 1);       // [kHB][33]
-  for (int i = threadIdx.x; i < kF * nout; i += blockDim.x) sw[i] = wh[i];
+  float* swT = sm;  // [NJ][32]: swT[j][ci] = Wh[ci][j]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* wbase = sm + NJ * kF + warp * (SM_::WARP > SM_::RED ? SM_::WARP : SM_::RED);
+  float* sA = wbase;            // [32 pixels][33]
+  float* sP = sA + 32 * 33;     // [32 pixels][33]
+  float* sG = sP + 32 * 33;     // [32 pixels][GS]
+  for (int i = threadIdx.x; i < NJ * kF; i += blockDim.x) {
+    const int j = i / kF, ci = i - (i / kF) * kF;
+    swT[i] = j < nout ? wh[ci * nout + j] : 0.f;
+  }
+  __syncthreads();
+  float accw[NJ];
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) accw[j] = 0.f;
+  float accb[NJ / 32];
+#pragma unroll
+  for (int q = 0; q < NJ / 32; ++q) accb[q] = 0.f;
+  float accd = 0.f;
   const size_t plane = (size_t)H * W;
   const size_t total = plane * B;
-  const size_t nchunks = (total + kHB - 1) / kHB;
-  const int npairs = kF * nout;
-  float accw[((kF * 2 * IGM_MAX_NZ) + 255) / 256];
-  const int npt = (npairs + 255) / 256;
-  for (int r = 0; r < npt; ++r) accw[r] = 0.f;
-  float accb = 0.f, accd = 0.f;
-  __syncthreads();
+  const size_t nchunks = (total + 31) / 32;
+  const size_t nw = (size_t)gridDim.x * kHeadWarps;
   const uint4* A = reinterpret_cast<const uint4*>(act);
   uint4* DP = reinterpret_cast<uint4*>(dpre);
-  for (size_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
-    const int t = threadIdx.x;
-    if (t < kHB) {
-      const size_t i = chunk * kHB + t;
-      if (i < total) {
-        const int b = (int)(i / plane);
-        const size_t rem = i - (size_t)b * plane;
-        const int y = (int)(rem / W), x = (int)(rem - (size_t)y * W);
-        float av[kF];
+  for (size_t chunk = (size_t)blockIdx.x * kHeadWarps + warp; chunk < nchunks; chunk += nw) {
+    const size_t i = chunk * 32 + lane;
+    const bool ok = i < total;
+    int b = 0, y = 0, x = 0;
+    size_t rem = 0;
+    if (ok) {
+      b = (int)(i / plane);
+      rem = i - (size_t)b * plane;
+      y = (int)(rem / W);
+      x = (int)(rem - (size_t)y * W);
+    }
+    // this lane's pixel: activations into its sA row, output gradients into g and its sG row
 #pragma unroll
-        for (int ch = 0; ch < 4; ++ch) {
-          const uint4 u = A[(((size_t)b * H + y) * 4 + ch) * W + x];
-          const uint32_t wv[4] = {u.x, u.y, u.z, u.w};
+    for (int ch = 0; ch < 4; ++ch) {
+      uint4 u = make_uint4(0, 0, 0, 0);
+      if (ok) u = A[(((size_t)b * H + y) * 4 + ch) * W + x];
+      const uint32_t wv[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            av[ch * 8 + 2 * e] = bf_lo(wv[e]);
-            av[ch * 8 + 2 * e + 1] = bf_hi(wv[e]);
-          }
-        }
-        float da[kF];
-#pragma unroll
-        for (int ci = 0; ci < kF; ++ci) da[ci] = 0.f;
-        for (int j = 0; j < nout; ++j) {
-          const float* src = j < nz ? dU : dV;
-          const int k = j < nz ? j : j - nz;
-          const float g = src[((size_t)b * nz + k) * plane + rem] * out_scale;
-          sD[t * (nout + 1) + j] = g;
-#pragma unroll
-          for (int ci = 0; ci < kF; ++ci) da[ci] = fmaf(g, sw[ci * nout + j], da[ci]);
-        }
-#pragma unroll
-        for (int ci = 0; ci < kF; ++ci) {
-          sA[t * 33 + ci] = av[ci];
-          da[ci] *= av[ci] > 0.f ? 1.f : alpha;
-          sP[t * 33 + ci] = da[ci];
-        }
-#pragma unroll
-        for (int ch = 0; ch < 4; ++ch) {
-          uint4 o;
-          o.x = bf_pack(da[ch * 8 + 0], da[ch * 8 + 1]);
-          o.y = bf_pack(da[ch * 8 + 2], da[ch * 8 + 3]);
-          o.z = bf_pack(da[ch * 8 + 4], da[ch * 8 + 5]);
-          o.w = bf_pack(da[ch * 8 + 6], da[ch * 8 + 7]);
-          DP[(((size_t)b * H + y) * 4 + ch) * W + x] = o;
-        }
-      } else {
-        for (int j = 0; j < nout; ++j) sD[t * (nout + 1) + j] = 0.f;
-        for (int ci = 0; ci < kF; ++ci) {
-          sA[t * 33 + ci] = 0.f;
-          sP[t * 33 + ci] = 0.f;
-        }
+      for (int e = 0; e < 4; ++e) {
+        sA[lane * 33 + ch * 8 + 2 * e] = bf_lo(wv[e]);
+        sA[lane * 33 + ch * 8 + 2 * e + 1] = bf_hi(wv[e]);
       }
     }
-    __syncthreads();
-    for (int r = 0; r < npt; ++r) {
-      const int pr = threadIdx.x + r * 256;
-      if (pr < npairs) {
-        const int ci = pr / nout, j = pr - ci * nout;
-        float s = 0.f;
-        for (int p = 0; p < kHB; ++p) s = fmaf(sA[p * 33 + ci], sD[p * (nout + 1) + j], s);
-        accw[r] += s;
+    float g[NJ];
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      float v = 0.f;
+      if (ok && j < nout) {
+        const float* src = j < nz ? dU : dV;
+        const int k = j < nz ? j : j - nz;
+        v = src[((size_t)b * nz + k) * plane + rem] * out_scale;
+      }
+      g[j] = v;
+      sG[lane * GS + j] = v;
+    }
+    // dPre16 = (dY Wh^T) * LeakyReLU'(A16)
+    float da[kF];
+#pragma unroll
+    for (int ci = 0; ci < kF; ++ci) da[ci] = 0.f;
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      if (j >= nout) break;
+      const float4* wr = reinterpret_cast<const float4*>(swT + j * kF);
+#pragma unroll
+      for (int q = 0; q < kF / 4; ++q) {
+        const float4 w4 = wr[q];
+        da[4 * q + 0] = fmaf(g[j], w4.x, da[4 * q + 0]);
+        da[4 * q + 1] = fmaf(g[j], w4.y, da[4 * q + 1]);
+        da[4 * q + 2] = fmaf(g[j], w4.z, da[4 * q + 2]);
+        da[4 * q + 3] = fmaf(g[j], w4.w, da[4 * q + 3]);
       }
     }
-    if (threadIdx.x < nout) {
-      float s = 0.f;
-      for (int p = 0; p < kHB; ++p) s += sD[p * (nout + 1) + threadIdx.x];
-      accb += s;
+#pragma unroll
+    for (int ci = 0; ci < kF; ++ci) {
+      da[ci] *= sA[lane * 33 + ci] > 0.f ? 1.f : alpha;
+      sP[lane * 33 + ci] = da[ci];
     }
-    if (threadIdx.x >= 128 && threadIdx.x < 128 + kF) {
-      const int ci = threadIdx.x - 128;
-      float s = 0.f;
-      for (int p = 0; p < kHB; ++p) s += sP[p * 33 + ci];
-      accd += s;
+    if (ok) {
+#pragma unroll
+      for (int ch = 0; ch < 4; ++ch) {
+        uint4 o;
+        o.x = bf_pack(da[ch * 8 + 0], da[ch * 8 + 1]);
+        o.y = bf_pack(da[ch * 8 + 2], da[ch * 8 + 3]);
+        o.z = bf_pack(da[ch * 8 + 4], da[ch * 8 + 5]);
+        o.w = bf_pack(da[ch * 8 + 6], da[ch * 8 + 7]);
+        DP[(((size_t)b * H + y) * 4 + ch) * W + x] = o;
+      }
     }
-    __syncthreads();
+    __syncwarp();
+    // lane = input channel: outer products over the warp's 32 pixels
+    for (int p = 0; p < 32; ++p) {
+      const float av = sA[p * 33 + lane];
+      accd += sP[p * 33 + lane];
+      const float4* gr = reinterpret_cast<const float4*>(sG + p * GS);
+#pragma unroll
+      for (int q = 0; q < NJ / 4; ++q) {
+        if (4 * q >= nout) break;
+        const float4 g4 = gr[q];
+        accw[4 * q + 0] = fmaf(av, g4.x, accw[4 * q + 0]);
+        accw[4 * q + 1] = fmaf(av, g4.y, accw[4 * q + 1]);
+        accw[4 * q + 2] = fmaf(av, g4.z, accw[4 * q + 2]);
+        accw[4 * q + 3] = fmaf(av, g4.w, accw[4 * q + 3]);
+      }
+#pragma unroll
+      for (int q = 0; q < NJ / 32; ++q) accb[q] += sG[p * GS + lane + 32 * q];
+    }
+    __syncwarp();  // this warp's staging area is rewritten by its next chunk
   }
-  // partial layout per block: [dWh (32*nout)] [dbh (nout)] [db16 (32)]
+  // per-warp results, then the fixed-order sum over the block's warps
+  __syncthreads();
+  float* red = wbase;  // [32 * NJ] dWh, [NJ] dbh, [32] db16
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) red[lane * NJ + j] = accw[j];
+#pragma unroll
+  for (int q = 0; q < NJ / 32; ++q) red[kF * NJ + lane + 32 * q] = accb[q];
+  red[kF * NJ + NJ + lane] = accd;
+  __syncthreads();
+  const int stride = SM_::WARP > SM_::RED ? SM_::WARP : SM_::RED;
+  const int npairs = kF * nout;
   float* out = partial + (size_t)blockIdx.x * (npairs + nout + kF);
-  for (int r = 0; r < npt; ++r) {
-    const int pr = threadIdx.x + r * 256;
-    if (pr < npairs) out[pr] = accw[r];
+  const float* r0 = sm + NJ * kF;
+  for (int o = threadIdx.x; o < npairs + nout + kF; o += blockDim.x) {
+    int src;
+    if (o < npairs) {
+      const int ci = o / nout, j = o - (o / nout) * nout;
+      src = ci * NJ + j;
+    } else if (o < npairs + nout) {
+      src = kF * NJ + (o - npairs);
+    } else {
+      src = kF * NJ + NJ + (o - npairs - nout);
+    }
+    float s = 0.f;
+    for (int w2 = 0; w2 < kHeadWarps; ++w2) s += r0[w2 * stride + src];
+    out[o] = s;
   }
-  if (threadIdx.x < nout) out[npairs + threadIdx.x] = accb;
-  if (threadIdx.x >= 128 && threadIdx.x < 128 + kF) out[npairs + nout + threadIdx.x - 128] = accd;
 }
 
 // ---------------------------------------------------------------------------
@@ -360,66 +414,87 @@ __global__ void __launch_bounds__(256) layer1_fwd_kernel(const L1Args a) {
   }
 }
 
-// dW1[t][c][co] = sum_p X[p + off(t)][c] * G[p][co], per-block partials [9*cin*32]
-constexpr int kL1P = 64;  // pixels per chunk
-__global__ void __launch_bounds__(256) layer1_wgrad_kernel(const L1Args a, const __nv_bfloat16* g, float* partial) {
-  __shared__ float sX[kL1P][46];
-  __shared__ float sG[kL1P][kF + 1];
-  const int nw = 9 * a.cin * kF;
-  constexpr int kPer = (9 * 5 * kF + 255) / 256;
-  float acc[kPer];
+// dW1[t][c][co] = sum_p X[p + off(t)][c] * G[p][co], per-block partials [9*cin*32].
+// A warp takes 32 consecutive pixels: each lane stages its pixel's 3x3x5
+// input window and its 32 output gradients in the warp's shared memory, then
+// lane l owns output channel co = l and accumulates the 45 (tap, channel)
+// products over the 32 pixels from broadcast reads.  Warps are summed in a
+// fixed order at the end (deterministic).
+constexpr int kL1Warps = 8;
+constexpr int kL1XS = 48;  // window row stride (16-byte aligned rows)
+constexpr int kL1Warp = 32 * kL1XS + 32 * 33;
+constexpr int kL1Red = 45 * kF;
+constexpr int kL1Stride = kL1Warp > kL1Red ? kL1Warp : kL1Red;
+__global__ void __launch_bounds__(kL1Warps * 32, 2) layer1_wgrad_kernel(const L1Args a, const __nv_bfloat16* g,
+                                                                       float* partial) {
+  extern __shared__ __align__(16) float sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* sX = sm + warp * kL1Stride;  // [32 pixels][48]
+  float* sG = sX + 32 * kL1XS;        // [32 pixels][33]
+  float acc[45];
 #pragma unroll
-  for (int r = 0; r < kPer; ++r) acc[r] = 0.f;
+  for (int k = 0; k < 45; ++k) acc[k] = 0.f;
   const size_t plane = (size_t)a.H * a.W;
   const size_t total = plane * a.B;
-  const size_t nchunks = (total + kL1P - 1) / kL1P;
+  const size_t nchunks = (total + 31) / 32;
+  const size_t nw = (size_t)gridDim.x * kL1Warps;
   const uint4* G = reinterpret_cast<const uint4*>(g);
-  for (size_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
-    const int t = threadIdx.x;
-    if (t < kL1P) {
-      const size_t i = chunk * kL1P + t;
-      if (i < total) {
-        const int b = (int)(i / plane);
-        const size_t rem = i - (size_t)b * plane;
-        const int y = (int)(rem / a.W), x = (int)(rem - (size_t)y * a.W);
-        float in[9][5];
-        l1_inputs(a, b, y, x, in);
+  for (size_t chunk = (size_t)blockIdx.x * kL1Warps + warp; chunk < nchunks; chunk += nw) {
+    const size_t i = chunk * 32 + lane;
+    if (i < total) {
+      const int b = (int)(i / plane);
+      const size_t rem = i - (size_t)b * plane;
+      const int y = (int)(rem / a.W), x = (int)(rem - (size_t)y * a.W);
+      float in[9][5];
+      l1_inputs(a, b, y, x, in);
 #pragma unroll
-        for (int tp = 0; tp < 9; ++tp)
+      for (int tp = 0; tp < 9; ++tp)
 #pragma unroll
-          for (int c = 0; c < 5; ++c) sX[t][tp * 5 + c] = in[tp][c];
+        for (int c = 0; c < 5; ++c) sX[lane * kL1XS + tp * 5 + c] = in[tp][c];
 #pragma unroll
-        for (int ch = 0; ch < 4; ++ch) {
-          const uint4 u = G[(((size_t)b * a.H + y) * 4 + ch) * a.W + x];
-          const uint32_t wv[4] = {u.x, u.y, u.z, u.w};
+      for (int ch = 0; ch < 4; ++ch) {
+        const uint4 u = G[(((size_t)b * a.H + y) * 4 + ch) * a.W + x];
+        const uint32_t wv[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            sG[t][ch * 8 + 2 * e] = bf_lo(wv[e]);
-            sG[t][ch * 8 + 2 * e + 1] = bf_hi(wv[e]);
-          }
+        for (int e = 0; e < 4; ++e) {
+          sG[lane * 33 + ch * 8 + 2 * e] = bf_lo(wv[e]);
+          sG[lane * 33 + ch * 8 + 2 * e + 1] = bf_hi(wv[e]);
         }
-      } else {
-        for (int k = 0; k < 45; ++k) sX[t][k] = 0.f;
-        for (int k = 0; k < kF; ++k) sG[t][k] = 0.f;
       }
-    }
-    __syncthreads();
+    } else {
 #pragma unroll
-    for (int r = 0; r < kPer; ++r) {
-      const int o = threadIdx.x + r * 256;
-      if (o < nw) {
-        const int co = o % kF, c = (o / kF) % a.cin, tp = o / (kF * a.cin);
-        float sacc = 0.f;
-        for (int p = 0; p < kL1P; ++p) sacc = fmaf(sX[p][tp * 5 + c], sG[p][co], sacc);
-        acc[r] += sacc;
-      }
+      for (int k = 0; k < 45; ++k) sX[lane * kL1XS + k] = 0.f;
+#pragma unroll
+      for (int k = 0; k < kF; ++k) sG[lane * 33 + k] = 0.f;
     }
-    __syncthreads();
+    __syncwarp();
+    for (int p = 0; p < 32; ++p) {
+      const float gp = sG[p * 33 + lane];
+      const float4* xr = reinterpret_cast<const float4*>(sX + p * kL1XS);
+#pragma unroll
+      for (int q = 0; q < 11; ++q) {
+        const float4 x4 = xr[q];
+        acc[4 * q + 0] = fmaf(x4.x, gp, acc[4 * q + 0]);
+        acc[4 * q + 1] = fmaf(x4.y, gp, acc[4 * q + 1]);
+        acc[4 * q + 2] = fmaf(x4.z, gp, acc[4 * q + 2]);
+        acc[4 * q + 3] = fmaf(x4.w, gp, acc[4 * q + 3]);
+      }
+      acc[44] = fmaf(sX[p * kL1XS + 44], gp, acc[44]);
+    }
+    __syncwarp();  // this warp's staging area is rewritten by its next chunk
   }
+  __syncthreads();
+  float* red = sm + warp * kL1Stride;  // [45][32]
 #pragma unroll
-  for (int r = 0; r < kPer; ++r) {
-    const int o = threadIdx.x + r * 256;
-    if (o < nw) partial[(size_t)blockIdx.x * nw + o] = acc[r];
+  for (int k = 0; k < 45; ++k) red[k * kF + lane] = acc[k];
+  __syncthreads();
+  const int nw_out = 9 * a.cin * kF;
+  for (int o = threadIdx.x; o < nw_out; o += blockDim.x) {
+    const int co = o % kF, c = (o / kF) % a.cin, tp = o / (kF * a.cin);
+    const int src = (tp * 5 + c) * kF + co;
+    float s = 0.f;
+    for (int w2 = 0; w2 < kL1Warps; ++w2) s += sm[w2 * kL1Stride + src];
+    partial[(size_t)blockIdx.x * nw_out + o] = s;
   }
 }
 
@@ -581,7 +656,17 @@ extern "C" int igm_cnn_layer1_wgrad(int batch, int h, int w, int cin, const floa
   int rc = l1_args(&a, batch, h, w, cin, thk, usurf, arrhenius, slidingco, dx, scales, &dummy, nullptr, 0.f);
   if (rc) return rc;
   IGM_CHECK_ARG(g && partials && n_parts >= 1, IGM_ERR_BAD_ARGUMENT, "igm_cnn_layer1_wgrad: bad argument");
-  layer1_wgrad_kernel<<<n_parts, 256, 0, as_stream(stream)>>>(a, (const __nv_bfloat16*)g, partials);
+  constexpr size_t smem = (size_t)kL1Warps * kL1Stride * sizeof(float);
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(layer1_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+      set_error("layer1_wgrad smem attribute: %s", cudaGetErrorString(e));
+      return IGM_ERR_CUDA;
+    }
+    configured = true;
+  }
+  layer1_wgrad_kernel<<<n_parts, kL1Warps * 32, smem, as_stream(stream)>>>(a, (const __nv_bfloat16*)g, partials);
   return launch_status("layer1_wgrad_kernel");
 }
 
@@ -599,6 +684,25 @@ extern "C" int igm_cnn_head_forward(int batch, int h, int w, int nz, const void*
 
 extern "C" size_t igm_cnn_head_partial_len(int nz) { return (size_t)kF * 2 * nz + 2 * nz + kF; }
 
+template <int NJ>
+static int head_bwd_launch(int batch, int h, int w, int nz, const void* act, const float* head_w, const float* dU,
+                           const float* dV, float out_scale, float alpha, void* dpre, float* partials, int n_parts,
+                           cudaStream_t st) {
+  constexpr size_t smem = (size_t)HeadBwdSmem<NJ>::FLOATS * sizeof(float);
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(head_bwd_kernel<NJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+      set_error("head_bwd smem attribute: %s", cudaGetErrorString(e));
+      return IGM_ERR_CUDA;
+    }
+    configured = true;
+  }
+  head_bwd_kernel<NJ><<<n_parts, kHeadWarps * 32, smem, st>>>(batch, h, w, nz, (const __nv_bfloat16*)act, head_w, dU,
+                                                                dV, out_scale, alpha, (__nv_bfloat16*)dpre, partials);
+  return launch_status("head_bwd_kernel");
+}
+
 extern "C" int igm_cnn_head_backward(int batch, int h, int w, int nz, const void* act, const float* head_w,
                                      const float* dU, const float* dV, float out_scale, float alpha, void* dpre,
                                      float* partials, int n_parts, void* stream) {
@@ -607,20 +711,14 @@ extern "C" int igm_cnn_head_backward(int batch, int h, int w, int nz, const void
   IGM_CHECK_ARG(act && head_w && dU && dV && dpre && partials, IGM_ERR_BAD_ARGUMENT,
                 "igm_cnn_head_backward: NULL argument");
   const int nout = 2 * nz;
-  const size_t smem = (size_t)(kF * nout + kHB * 33 + kHB * (nout + 1) + kHB * 33) * sizeof(float);
-  static size_t configured = 0;
-  if (smem > 48 * 1024 && configured < smem) {
-    cudaError_t e = cudaFuncSetAttribute(head_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) {
-      set_error("head_bwd smem attribute: %s", cudaGetErrorString(e));
-      return IGM_ERR_CUDA;
-    }
-    configured = smem;
-  }
-  head_bwd_kernel<<<n_parts, 256, smem, as_stream(stream)>>>(batch, h, w, nz, (const __nv_bfloat16*)act, head_w, dU,
-                                                            dV, out_scale, alpha, (__nv_bfloat16*)dpre, partials);
-  return launch_status("head_bwd_kernel");
+  cudaStream_t st = as_stream(stream);
+  if (nout <= 32) return head_bwd_launch<32>(batch, h, w, nz, act, head_w, dU, dV, out_scale, alpha, dpre, partials,
+                                             n_parts, st);
+  if (nout <= 64) return head_bwd_launch<64>(batch, h, w, nz, act, head_w, dU, dV, out_scale, alpha, dpre, partials,
+                                             n_parts, st);
+  return head_bwd_launch<128>(batch, h, w, nz, act, head_w, dU, dV, out_scale, alpha, dpre, partials, n_parts, st);
 }
+
 
 extern "C" int igm_reduce_partials(const float* partials, int n_parts, int len, int stride, float* out,
                                    int accumulate, void* stream) {

@@ -82,7 +82,7 @@ __device__ __forceinline__ T maxmod(T a, T b) {
 template <typename T>
 struct TransportArgs {
   int ny, nx, slope;
-  T dx, half_dx, dt_host, ratio, sealevel;
+  T dx, rdx, half_dx, dt_host, ratio, sealevel;  // rdx = 1/dx correctly rounded in T
   const float* dt_dev;
   const T* u;
   const T* v;
@@ -95,59 +95,123 @@ struct TransportArgs {
   T* divflux;
 };
 
+// num / dx, correctly rounded (the IEEE quotient), for dx > 0 and |num| well
+// inside the normal range, from the correctly rounded reciprocal rdx = RN(1/dx)
+// by Markstein's division step (P. Markstein, "Computation of elementary
+// functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1),
+// 1990): q = RN(num rdx) is within one ulp of num/dx, the remainder
+// r = num - dx q is exact in one fma, and RN(q + r rdx) is the correctly
+// rounded quotient.  A zero numerator is returned as is (keeps its sign).
 template <typename T>
-__device__ __forceinline__ T limited_slope(T hm, T h0, T hp, T dx, int slope) {
+__device__ __forceinline__ T div_dx(T num, T dx, T rdx) {
+  if (num == T(0)) return num;
+  const T q = num * rdx;
+  const T r = fma(-q, dx, num);
+  return fma(r, rdx, q);
+}
+
+template <typename T>
+__device__ __forceinline__ T limited_slope(T hm, T h0, T hp, T dx, T rdx, int slope) {
   // slope of the cell holding h0 from its neighbours hm (left) and hp (right)
-  const T sigp = (hp - h0) / dx, sigm = (h0 - hm) / dx;
+  const T sigp = div_dx(hp - h0, dx, rdx), sigm = div_dx(h0 - hm, dx, rdx);
   if (slope == IGM_GODUNOV) return T(0);
   if (slope == IGM_MINMOD) return minmod(sigm, sigp);
   return maxmod(minmod(sigp, T(2) * sigm), minmod(sigm, T(2) * sigp));
 }
 
+// A CTA owns a 32 x 8 tile of nodes and computes every quantity once, in
+// shared memory: the limited slope of each cell, then the upwind flux of each
+// face, then the node update.  The operations and their order per quantity
+// are those of the reference (IEEE division by dx, no contraction), so the
+// result is bit-identical to evaluating each face independently.
+constexpr int kTrX = 32, kTrY = 8;
 template <typename T>
-__global__ void __launch_bounds__(256) transport_kernel(const TransportArgs<T> a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+__global__ void __launch_bounds__(kTrX* kTrY) transport_kernel(const TransportArgs<T> a) {
+  constexpr int HR = kTrY + 4, HC = kTrX + 4;  // thickness tile: rows j0-2 .. j0+9, columns i0-2 .. i0+33
+  __shared__ T sh[HR][HC + 1];
+  __shared__ T ssx[kTrY][kTrX + 2];   // x slopes of cells i0-1 .. i0+32 (rows j0 .. j0+7)
+  __shared__ T ssy[kTrY + 2][kTrX];   // y slopes of cells j0-1 .. j0+8 (columns i0 .. i0+31)
+  __shared__ T sq[kTrY][kTrX + 1];    // x-face fluxes, faces i0 .. i0+32
+  __shared__ T sr[kTrY + 1][kTrX];    // y-face fluxes, faces j0 .. j0+8
+  __shared__ T su[kTrY][kTrX + 2];    // ubar, rows j0 .. j0+7, columns i0-1 .. i0+32
+  __shared__ T sv[kTrY + 2][kTrX];    // vbar, rows j0-1 .. j0+8, columns i0 .. i0+31
   const int nx = a.nx, ny = a.ny;
-  if (i >= nx || j >= ny) return;
+  const int i0 = blockIdx.x * kTrX, j0 = blockIdx.y * kTrY;
+  const int tid = threadIdx.y * kTrX + threadIdx.x;
+  constexpr int NT = kTrX * kTrY;
   const T dt = a.dt_dev ? (T)(*a.dt_dev) : a.dt_host;
-  const T dx = a.dx;
-  auto H = [&](int jj, int ii) -> T {
-    return (jj >= 0 && jj < ny && ii >= 0 && ii < nx) ? a.h[(size_t)jj * nx + ii] : T(0);
-  };
-  // x faces i (west) and i+1 (east) of this node
-  T q[2];
-#pragma unroll
-  for (int s = 0; s < 2; ++s) {
-    const int f = i + s;
-    const T uf = f == 0 ? a.u[(size_t)j * nx] : (f == nx ? a.u[(size_t)j * nx + nx - 1]
-                                                         : T(0.5) * (a.u[(size_t)j * nx + f - 1] + a.u[(size_t)j * nx + f]));
-    const T hl = H(j, f - 1), hr = H(j, f);
-    const T sl = limited_slope(H(j, f - 2), hl, hr, dx, a.slope);
-    const T sr = limited_slope(hl, hr, H(j, f + 1), dx, a.slope);
-    const T w = hl + a.half_dx * (T(1) - uf * dt / dx) * sl;
-    const T e = hr - a.half_dx * (T(1) + uf * dt / dx) * sr;
-    q[s] = uf * (uf > T(0) ? w : e);
+  const T dx = a.dx, rdx = a.rdx;
+  // every global input of the tile is requested before the first barrier
+  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  const bool node = i < nx && j < ny;
+  const size_t o = node ? (size_t)j * nx + i : 0;
+  const T tg = node ? a.topg[o] : T(0);
+  const T sm = (node && a.smb) ? a.smb[o] : T(0);
+  for (int k = tid; k < HR * HC; k += NT) {
+    const int r = k / HC, c = k - (k / HC) * HC;
+    const int jj = j0 - 2 + r, ii = i0 - 2 + c;
+    sh[r][c] = (jj >= 0 && jj < ny && ii >= 0 && ii < nx) ? a.h[(size_t)jj * nx + ii] : T(0);
   }
-  T r[2];
-#pragma unroll
-  for (int s = 0; s < 2; ++s) {
-    const int f = j + s;
-    const T vf = f == 0 ? a.v[i] : (f == ny ? a.v[(size_t)(ny - 1) * nx + i]
-                                            : T(0.5) * (a.v[(size_t)(f - 1) * nx + i] + a.v[(size_t)f * nx + i]));
-    const T hl = H(f - 1, i), hr = H(f, i);
-    const T sl = limited_slope(H(f - 2, i), hl, hr, dx, a.slope);
-    const T sr = limited_slope(hl, hr, H(f + 1, i), dx, a.slope);
-    const T s_ = hl + a.half_dx * (T(1) - vf * dt / dx) * sl;
-    const T n_ = hr - a.half_dx * (T(1) + vf * dt / dx) * sr;
-    r[s] = vf * (vf > T(0) ? s_ : n_);
+  for (int k = tid; k < kTrY * (kTrX + 2); k += NT) {
+    const int r = k / (kTrX + 2), c = k - (k / (kTrX + 2)) * (kTrX + 2);
+    const int jj = j0 + r, ii = i0 - 1 + c;
+    su[r][c] = (jj < ny && ii >= 0 && ii < nx) ? a.u[(size_t)jj * nx + ii] : T(0);
   }
-  const T div = (q[1] - q[0]) / dx + (r[1] - r[0]) / dx;
-  const size_t o = (size_t)j * nx + i;
-  const T sm = a.smb ? a.smb[o] : T(0);
-  T hn = a.h[o] + dt * (sm - div);
+  for (int k = tid; k < (kTrY + 2) * kTrX; k += NT) {
+    const int r = k / kTrX, c = k - (k / kTrX) * kTrX;
+    const int jj = j0 - 1 + r, ii = i0 + c;
+    sv[r][c] = (jj >= 0 && jj < ny && ii < nx) ? a.v[(size_t)jj * nx + ii] : T(0);
+  }
+  __syncthreads();
+  // cell slopes: x slope of cell (j, c) from its left / right neighbours, y slope from below / above
+  for (int k = tid; k < kTrY * (kTrX + 2); k += NT) {
+    const int r = k / (kTrX + 2), c = k - (k / (kTrX + 2)) * (kTrX + 2);  // cell (j0 + r, i0 - 1 + c)
+    ssx[r][c] = limited_slope(sh[r + 2][c], sh[r + 2][c + 1], sh[r + 2][c + 2], dx, rdx, a.slope);
+  }
+  for (int k = tid; k < (kTrY + 2) * kTrX; k += NT) {
+    const int r = k / kTrX, c = k - (k / kTrX) * kTrX;  // cell (j0 - 1 + r, i0 + c)
+    ssy[r][c] = limited_slope(sh[r][c + 2], sh[r + 1][c + 2], sh[r + 2][c + 2], dx, rdx, a.slope);
+  }
+  __syncthreads();
+  // face fluxes: x face f between cells f-1 and f of row j; y face f between rows f-1 and f
+  for (int k = tid; k < kTrY * (kTrX + 1); k += NT) {
+    const int r = k / (kTrX + 1), c = k - (k / (kTrX + 1)) * (kTrX + 1);
+    const int jr = j0 + r, f = i0 + c;
+    T q = T(0);
+    if (jr < ny && f <= nx) {
+      // su[r][c] = u[j][f-1], su[r][c+1] = u[j][f]
+      const T uf = f == 0 ? su[r][c + 1] : (f == nx ? su[r][c] : T(0.5) * (su[r][c] + su[r][c + 1]));
+      const T hl = sh[r + 2][c + 1], hr = sh[r + 2][c + 2];
+      const T sl = ssx[r][c], sr_ = ssx[r][c + 1];
+      const T cu = div_dx(uf * dt, dx, rdx);
+      const T w = hl + a.half_dx * (T(1) - cu) * sl;
+      const T e = hr - a.half_dx * (T(1) + cu) * sr_;
+      q = uf * (uf > T(0) ? w : e);
+    }
+    sq[r][c] = q;
+  }
+  for (int k = tid; k < (kTrY + 1) * kTrX; k += NT) {
+    const int r = k / kTrX, c = k - (k / kTrX) * kTrX;
+    const int f = j0 + r, ic = i0 + c;
+    T q = T(0);
+    if (f <= ny && ic < nx) {
+      // sv[r][c] = v[f-1][i], sv[r+1][c] = v[f][i]
+      const T vf = f == 0 ? sv[r + 1][c] : (f == ny ? sv[r][c] : T(0.5) * (sv[r][c] + sv[r + 1][c]));
+      const T hl = sh[r + 1][c + 2], hr = sh[r + 2][c + 2];
+      const T sl = ssy[r][c], sr_ = ssy[r + 1][c];
+      const T cv = div_dx(vf * dt, dx, rdx);
+      const T s_ = hl + a.half_dx * (T(1) - cv) * sl;
+      const T n_ = hr - a.half_dx * (T(1) + cv) * sr_;
+      q = vf * (vf > T(0) ? s_ : n_);
+    }
+    sr[r][c] = q;
+  }
+  __syncthreads();
+  if (!node) return;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const T div = div_dx(sq[ty][tx + 1] - sq[ty][tx], dx, rdx) + div_dx(sr[ty + 1][tx] - sr[ty][tx], dx, rdx);
+  T hn = sh[ty + 2][tx + 2] + dt * (sm - div);
   hn = hn > T(0) ? hn : T(0);
-  const T tg = a.topg[o];
   const T fl = -a.ratio * hn + a.sealevel;
   const T ls = tg > fl ? tg : fl;
   a.h_out[o] = hn;
@@ -231,10 +295,11 @@ static int transport_t(int ny, int nx, double dx, const void* u, const void* v, 
   TransportArgs<T> a{};
   a.ny = ny; a.nx = nx; a.slope = slope;
   a.dx = (T)dx; a.half_dx = (T)(0.5 * dx); a.dt_host = (T)dt; a.ratio = (T)ratio; a.sealevel = (T)sealevel;
+  a.rdx = T(1) / a.dx;  // host IEEE division in T: the correctly rounded reciprocal
   a.dt_dev = dt_dev;
   a.u = (const T*)u; a.v = (const T*)v; a.h = (const T*)h; a.h_out = (T*)h_out; a.topg = (const T*)topg;
   a.smb = (const T*)smb; a.usurf = (T*)usurf; a.lsurf = (T*)lsurf; a.divflux = (T*)divflux;
-  dim3 blk(32, 8), grd((nx + 31) / 32, (ny + 7) / 8);
+  dim3 blk(kTrX, kTrY), grd((nx + kTrX - 1) / kTrX, (ny + kTrY - 1) / kTrY);
   transport_kernel<T><<<grd, blk, 0, st>>>(a);
   return launch_status("transport_kernel");
 }
