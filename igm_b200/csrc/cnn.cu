@@ -48,9 +48,10 @@ __host__ __device__ inline size_t param_count(int L, int cin0, int nout) {
 }
 
 // ---------------------------------------------------------------------------
-// weight packing: fp32 Keras layout -> bf16 UMMA B operands
-//  forward  layer l: [tap][k-chunk (ci)][co][8]   (layer 0: 2 k-chunks, zero above cin0)
-//  dgrad    layer l>=1: [tap'][k-chunk (co)][ci][8] with tap' = 8 - tap (flipped)
+// weight packing: fp32 Keras layout -> bf16 UMMA B operands, ordered so that
+// for one (kw, 8-channel k-chunk) the three kernel rows follow each other:
+//  forward  layer l: [kw][k-chunk (ci)][kh][co][8]   (layer 0: 2 k-chunks, zero above cin0)
+//  dgrad    layer l>=1: [kw'][k-chunk (co)][kh'][ci][8], flipped: kh' = 2 - kh, kw' = 2 - kw
 // ---------------------------------------------------------------------------
 __global__ void pack_kernel(const float* params, int L, int cin0, int nout, __nv_bfloat16* wf, __nv_bfloat16* wb) {
   const size_t n0 = (size_t)9 * 2 * kF * 8;   // layer 0, forward
@@ -63,10 +64,10 @@ __global__ void pack_kernel(const float* params, int L, int cin0, int nout, __nv
       int c8;
       if (i < n0) { l = 0; rem = (int)i; c8 = 2; }
       else { l = 1 + (int)((i - n0) / ni); rem = (int)((i - n0) % ni); c8 = 4; }
-      const int e = rem % 8, co = (rem / 8) % kF, kc = (rem / (8 * kF)) % c8, tap = rem / (8 * kF * c8);
+      const int e = rem % 8, co = (rem / 8) % kF, kh = (rem / (8 * kF)) % 3, kc = (rem / (24 * kF)) % c8,
+                kw = rem / (24 * kF * c8);
       const int ci = kc * 8 + e;
       const int cin = l == 0 ? cin0 : kF;
-      const int kh = tap / 3, kw = tap % 3;
       float v = 0.f;
       if (ci < cin) v = params[w_offset(l, cin0, nout) + (((size_t)kh * 3 + kw) * cin + ci) * kF + co];
       wf[i] = __float2bfloat16_rn(v);
@@ -74,10 +75,10 @@ __global__ void pack_kernel(const float* params, int L, int cin0, int nout, __nv
       const size_t j = i - total_f;
       const int l = 1 + (int)(j / ni);
       const int rem = (int)(j % ni);
-      const int e = rem % 8, ci = (rem / 8) % kF, kc = (rem / (8 * kF)) % 4, tapp = rem / (8 * kF * 4);
+      const int e = rem % 8, ci = (rem / 8) % kF, khp = (rem / (8 * kF)) % 3, kc = (rem / (24 * kF)) % 4,
+                kwp = rem / (24 * kF * 4);
       const int co = kc * 8 + e;
-      const int tap = 8 - tapp;
-      const int kh = tap / 3, kw = tap % 3;
+      const int kh = 2 - khp, kw = 2 - kwp;
       const float v = params[w_offset(l, cin0, nout) + (((size_t)kh * 3 + kw) * kF + ci) * kF + co];
       wb[j] = __float2bfloat16_rn(v);
     }

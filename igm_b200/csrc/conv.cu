@@ -37,7 +37,8 @@ namespace igm {
 
 constexpr int kTW = 128;        // pixels per tile row (the UMMA M)
 constexpr int kBoxW = kTW + 2;  // with the 1-pixel halo on each side
-constexpr int kCout = 32;       // output channels (the UMMA N)
+constexpr int kCout = 32;       // output channels
+constexpr int kWRowsN = 3 * kCout;  // B-operand rows per (dx, k-chunk) of a weight pack: (dy, channel)
 constexpr int kConvThreads = 192;
 
 enum ConvEpi { kEpiFwdLeaky = 0, kEpiDgrad = 1 };
@@ -181,7 +182,6 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
-      constexpr uint32_t idesc = tc::make_idesc_bf16(128, kCout, false, false);
       for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
         const int s = it % NST, use = it / NST, acc = it & 1, ause = it >> 1;
         if (!tc::mbar_wait(&tempty[acc], (ause & 1) ^ 1) || !tc::mbar_wait(&full[s], use & 1)) {
@@ -191,18 +191,36 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs
         tc::tc_fence_after();
         const uint32_t in0 = sbase + s * G::STAGE;
         const uint32_t w0 = sbase + G::OFF_W;
-#pragma unroll 1
-        for (int r = 0; r < R; ++r) {
-          const uint32_t d = tmem + (uint32_t)((acc * R + r) * kCout);
+        const uint32_t dset = tmem + (uint32_t)(acc * R * kCout);
+        // Input row i (global row y0 - 1 + i) feeds output rows o = i - dy through kernel row dy.
+        // One MMA covers all of its valid dy at once (N = 32 ndy): output row o accumulates at
+        // TMEM column 32 (R - 1 - o), so consecutive dy land in consecutive 32-column blocks.
+        // Each activation tile is thus read once per (dx, k-step), not once per tap.
 #pragma unroll
-          for (int tap = 0; tap < 9; ++tap) {
-            const int dy = tap / 3, dx = tap % 3;
+        for (int i = 0; i < R + 2; ++i) {
+          constexpr int dmax = 2;
+          const int dlo = i - (R - 1) > 0 ? i - (R - 1) : 0;
+          const int dhi = i < dmax ? i : dmax;
+          const int ndy = dhi - dlo + 1;
+          const uint32_t dcol = dset + (uint32_t)(kCout * (R - 1 - i + dlo));
+#pragma unroll
+          for (int dx = 0; dx < 3; ++dx) {
 #pragma unroll
             for (int ks = 0; ks < C8_IN / 2; ++ks) {
-              const uint32_t aaddr = in0 + (r + dy) * G::RS + dx * 16 + ks * 2 * G::P;
-              const uint32_t baddr = w0 + (tap * C8_IN + ks * 2) * (kCout * 16);
-              tc::mma_bf16(d, tc::make_desc(aaddr, G::P, 128), tc::make_desc(baddr, kCout * 16, 128), idesc,
-                           (tap | ks) != 0);
+              const uint32_t aaddr = in0 + i * G::RS + dx * 16 + ks * 2 * G::P;
+              const uint32_t baddr = w0 + ((dx * C8_IN + ks * 2) * kWRowsN + dlo * kCout) * 16;
+              const uint64_t ad = tc::make_desc(aaddr, G::P, 128);
+              if (dx == 0 && ks == 0 && dlo == 0) {
+                // output row i starts here: initialise its accumulator alone, then add to the rows above
+                tc::mma_bf16(dcol, ad, tc::make_desc(baddr, kWRowsN * 16, 128),
+                             tc::make_idesc_bf16(128, kCout, false, false), 0u);
+                if (ndy > 1)
+                  tc::mma_bf16(dcol + kCout, ad, tc::make_desc(baddr + kCout * 16, kWRowsN * 16, 128),
+                               tc::make_idesc_bf16(128, kCout * (ndy - 1), false, false), 1u);
+              } else {
+                tc::mma_bf16(dcol, ad, tc::make_desc(baddr, kWRowsN * 16, 128),
+                             tc::make_idesc_bf16(128, kCout * ndy, false, false), 1u);
+              }
             }
           }
         }
@@ -219,18 +237,32 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs
     for (int c = 0; c < kCout; ++c) dbacc[c] = 0.f;
     for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
       const int use = it >> 1, acc = it & 1;
+      const int txi = t % a.tiles_w, rest = t / a.tiles_w;
+      const int tyi = rest % a.tiles_h, b = rest / a.tiles_h;
+      const int x = txi * kTW + p;
+      // dgrad: the activation mask of all R rows is requested before waiting for the
+      // accumulators, so its latency overlaps the MMAs of this tile
+      uint4 mk[EPI == kEpiDgrad ? R : 1][4];
+      if (EPI == kEpiDgrad) {
+        const uint4* am = reinterpret_cast<const uint4*>(a.amask);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int y = tyi * R + r;
+          const bool ok = y < a.H && x < a.W;
+          const size_t pix = ok ? (((size_t)b * a.H + y) * 4) * a.W + x : 0;
+#pragma unroll
+          for (int ch = 0; ch < 4; ++ch) mk[r][ch] = ok ? am[pix + (size_t)ch * a.W] : make_uint4(0, 0, 0, 0);
+        }
+      }
       if (!tc::mbar_wait(&tfull[acc], use & 1)) {
         set_err(a.err, 3);
         break;
       }
       tc::tc_fence_after();
-      const int txi = t % a.tiles_w, rest = t / a.tiles_w;
-      const int tyi = rest % a.tiles_h, b = rest / a.tiles_h;
-      const int x = txi * kTW + p;
-#pragma unroll 1
+#pragma unroll
       for (int r = 0; r < R; ++r) {
         uint32_t v[32];
-        tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((acc * R + r) * kCout), v);
+        tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((acc * R + (R - 1 - r)) * kCout), v);
         tc::tmem_wait_ld();
         const int y = tyi * R + r;
         if (y < a.H && x < a.W) {
@@ -245,10 +277,9 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs
               f[c] = z > 0.f ? z : a.alpha * z;
             }
           } else {
-            const uint4* am = reinterpret_cast<const uint4*>(a.amask);
 #pragma unroll
             for (int ch = 0; ch < 4; ++ch) {
-              const uint4 mv = am[pix + (size_t)ch * a.W];
+              const uint4 mv = mk[EPI == kEpiDgrad ? r : 0][ch];
               const uint32_t mw[4] = {mv.x, mv.y, mv.z, mv.w};
 #pragma unroll
               for (int e = 0; e < 4; ++e) {

@@ -283,8 +283,9 @@ IGM_API size_t igm_cnn_param_count(int nb_layers, int cin, int nout);
 IGM_API size_t igm_cnn_param_offset(int nb_layers, int cin, int nout, int layer, int bias);
 
 /* fp32 parameters -> bf16 UMMA operand packs: wpack_fwd (layer 0: 9*2*32*8,
- * layers >= 1: 9*4*32*8 elements each) and wpack_bwd (layers >= 1, flipped
- * and transposed for dgrad, 9*4*32*8 each). */
+ * layers >= 1: 9*4*32*8 elements each), ordered [kw][ci/8][kh][co][ci%8], and
+ * wpack_bwd (layers >= 1, flipped and transposed for dgrad, 9*4*32*8 each),
+ * ordered [2-kw][co/8][2-kh][ci][co%8]. */
 IGM_API int igm_cnn_pack_weights(int nb_layers, int cin, int nout, const float* params, void* wpack_fwd,
                                  void* wpack_bwd, void* stream);
 

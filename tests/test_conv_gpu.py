@@ -30,21 +30,23 @@ def bf(t):
 
 
 def pack_fwd(w_kkio, cin_t):
-    """Keras kernel [3,3,cin,32] -> [9][cin_t/8][32][8] bf16."""
+    """Keras kernel [3,3,cin,32] -> [kw][cin_t/8][kh][32][8] bf16."""
     kh, kw, cin, co = w_kkio.shape
-    out = torch.zeros(9, cin_t // 8, co, 8)
-    for t in range(9):
-        for ci in range(cin):
-            out[t, ci // 8, :, ci % 8] = w_kkio[t // 3, t % 3, ci, :]
+    out = torch.zeros(3, cin_t // 8, 3, co, 8)
+    for y in range(3):
+        for x in range(3):
+            for ci in range(cin):
+                out[x, ci // 8, y, :, ci % 8] = w_kkio[y, x, ci, :]
     return out.to(torch.bfloat16).contiguous()
 
 
 def pack_bwd(w_kkio):
-    out = torch.zeros(9, 4, 32, 8)
-    for tp in range(9):
-        t = 8 - tp
-        for co in range(32):
-            out[tp, co // 8, :, co % 8] = w_kkio[t // 3, t % 3, :, co]
+    """Flipped, transposed dgrad pack: [2-kw][co/8][2-kh][ci][co%8] bf16."""
+    out = torch.zeros(3, 4, 3, 32, 8)
+    for y in range(3):
+        for x in range(3):
+            for co in range(32):
+                out[2 - x, co // 8, 2 - y, :, co % 8] = w_kkio[y, x, :, co]
     return out.to(torch.bfloat16).contiguous()
 
 
