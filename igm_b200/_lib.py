@@ -87,6 +87,7 @@ SIGNATURES = {
     "igm_conv3x3": (I, [I, I, I, I, I, P, P, P, P, P, P, I, C.c_float, P, P]),
     "igm_conv3x3_wgrad": (I, [I, I, I, I, P, P, P, I, P, P]),
     "igm_conv_sm_count": (I, []),
+    "igm_conv3x3_wgrad_partial_len": (C.c_size_t, [I]),
     "igm_cnn_param_count": (C.c_size_t, [I, I, I]),
     "igm_cnn_param_offset": (C.c_size_t, [I, I, I, I, I]),
     "igm_cnn_pack_weights": (I, [I, I, I, P, P, P, P]),

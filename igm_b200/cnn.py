@@ -135,8 +135,8 @@ class CNN:
                 npart = self.n_sm
                 b["npart"] = npart          # persistent tensor-core kernels: one CTA per SM
                 b["npart2"] = 2 * npart     # head / first-layer reductions: two CTAs per SM
-                b["wpart"] = torch.empty(max(npart * 3 * 128 * F, 2 * npart * 9 * self.cin * F),
-                                         dtype=torch.float32, device=d)
+                wlen = int(L.lib().igm_conv3x3_wgrad_partial_len(F))
+                b["wpart"] = torch.empty(max(npart * wlen, 2 * npart * 9 * self.cin * F), dtype=torch.float32, device=d)
                 b["dbpart"] = torch.zeros((npart, F), dtype=torch.float32, device=d)
                 hl = int(L.lib().igm_cnn_head_partial_len(self.nz))
                 b["hpart"] = torch.empty((2 * npart, hl), dtype=torch.float32, device=d)

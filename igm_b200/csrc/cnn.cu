@@ -133,13 +133,20 @@ __global__ void input_kernel(const InputArgs a) {
 // head forward: Y = A16 Wh + bh, written as planar U [B][Nz][H][W], V [B][Nz][H][W]
 // (Y_to_UV: channels [0,Nz) are U, [Nz, 2Nz) are V), masked where thk <= 0
 // ---------------------------------------------------------------------------
+// Two output channels per packed FP32x2 fma (the weights read as float4 rows,
+// the activation broadcast); each output accumulates over ci in order, as one
+// scalar fma chain would.  NJ >= 2 nz, multiple of 4 (padded weight rows).
+template <int NJ>
 __global__ void __launch_bounds__(256) head_fwd_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act,
                                                        const float* wh, const float* bh, float out_scale, float* U,
                                                        float* V, const float* thk_mask) {
-  extern __shared__ float sw[];  // [32][2nz] then bias [2nz]
+  __shared__ __align__(16) float sw[kF * NJ + NJ];  // [32][NJ] then bias [NJ]
   const int nout = 2 * nz;
-  for (int i = threadIdx.x; i < kF * nout; i += blockDim.x) sw[i] = wh[i];
-  for (int i = threadIdx.x; i < nout; i += blockDim.x) sw[kF * nout + i] = bh[i];
+  for (int i = threadIdx.x; i < kF * NJ; i += blockDim.x) {
+    const int ci = i / NJ, j = i - (i / NJ) * NJ;
+    sw[i] = j < nout ? wh[ci * nout + j] : 0.f;
+  }
+  for (int i = threadIdx.x; i < NJ; i += blockDim.x) sw[kF * NJ + i] = i < nout ? bh[i] : 0.f;
   __syncthreads();
   const size_t plane = (size_t)H * W;
   const size_t total = plane * B;
@@ -159,16 +166,31 @@ __global__ void __launch_bounds__(256) head_fwd_kernel(int B, int H, int W, int 
         av[ch * 8 + 2 * e + 1] = bf_hi(wv[e]);
       }
     }
-    const bool keep = thk_mask == nullptr || thk_mask[i] > 0.f;
-    for (int j = 0; j < nout; ++j) {
-      float s = 0.f;
+    float2 acc[NJ / 2];
 #pragma unroll
-      for (int ci = 0; ci < kF; ++ci) s = fmaf(av[ci], sw[ci * nout + j], s);
-      s = (s + sw[kF * nout + j]) * out_scale;
-      if (!keep) s = 0.f;
+    for (int q = 0; q < NJ / 2; ++q) acc[q] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int ci = 0; ci < kF; ++ci) {
+      const float2 aa = make_float2(av[ci], av[ci]);
+      const float4* wr = reinterpret_cast<const float4*>(sw + ci * NJ);
+#pragma unroll
+      for (int q = 0; q < NJ / 4; ++q) {
+        if (4 * q >= nout) break;
+        const float4 w4 = wr[q];
+        acc[2 * q] = __ffma2_rn(aa, make_float2(w4.x, w4.y), acc[2 * q]);
+        acc[2 * q + 1] = __ffma2_rn(aa, make_float2(w4.z, w4.w), acc[2 * q + 1]);
+      }
+    }
+    const bool keep = thk_mask == nullptr || thk_mask[i] > 0.f;
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      if (j >= nout) break;
+      const float sacc = (j & 1) ? acc[j >> 1].y : acc[j >> 1].x;
+      float sv = (sacc + sw[kF * NJ + j]) * out_scale;
+      if (!keep) sv = 0.f;
       float* dst = j < nz ? U : V;
       const int k = j < nz ? j : j - nz;
-      dst[((size_t)b * nz + k) * plane + rem] = s;
+      dst[((size_t)b * nz + k) * plane + rem] = sv;
     }
   }
 }
@@ -373,7 +395,7 @@ __device__ __forceinline__ void l1_inputs(const L1Args& a, int b, int y, int x, 
 }
 
 __global__ void __launch_bounds__(256) layer1_fwd_kernel(const L1Args a) {
-  __shared__ float sw[9 * 5 * kF + kF];
+  __shared__ __align__(16) float sw[9 * 5 * kF + kF];
   for (int i = threadIdx.x; i < 9 * a.cin * kF; i += blockDim.x) sw[i] = a.w[i];
   if (threadIdx.x < kF) sw[9 * 5 * kF + threadIdx.x] = a.b[threadIdx.x];
   __syncthreads();
@@ -386,23 +408,31 @@ __global__ void __launch_bounds__(256) layer1_fwd_kernel(const L1Args a) {
     const int y = (int)(rem / a.W), x = (int)(rem - (size_t)y * a.W);
     float in[9][5];
     l1_inputs(a, b, y, x, in);
-    float acc[kF];
+    // two output channels per packed FP32x2 fma; each channel accumulates in (tap, c) order
+    float2 acc[kF / 2];
 #pragma unroll
-    for (int co = 0; co < kF; ++co) acc[co] = sw[9 * 5 * kF + co];
+    for (int q = 0; q < kF / 2; ++q) acc[q] = make_float2(sw[9 * 5 * kF + 2 * q], sw[9 * 5 * kF + 2 * q + 1]);
 #pragma unroll
     for (int t = 0; t < 9; ++t)
-      for (int c = 0; c < a.cin; ++c) {
-        const float v = in[t][c];
-        const float* wr = &sw[(t * a.cin + c) * kF];
 #pragma unroll
-        for (int co = 0; co < kF; ++co) acc[co] = fmaf(v, wr[co], acc[co]);
+      for (int c = 0; c < 5; ++c) {
+        if (c >= a.cin) break;
+        const float2 vv = make_float2(in[t][c], in[t][c]);
+        const float4* wr = reinterpret_cast<const float4*>(&sw[(t * a.cin + c) * kF]);
+#pragma unroll
+        for (int q = 0; q < kF / 4; ++q) {
+          const float4 w4 = wr[q];
+          acc[2 * q] = __ffma2_rn(vv, make_float2(w4.x, w4.y), acc[2 * q]);
+          acc[2 * q + 1] = __ffma2_rn(vv, make_float2(w4.z, w4.w), acc[2 * q + 1]);
+        }
       }
 #pragma unroll
     for (int ch = 0; ch < 4; ++ch) {
       float z[8];
 #pragma unroll
       for (int e = 0; e < 8; ++e) {
-        const float v = acc[ch * 8 + e];
+        const int co = ch * 8 + e;
+        const float v = (co & 1) ? acc[co >> 1].y : acc[co >> 1].x;
         z[e] = v > 0.f ? v : a.alpha * v;
       }
       uint4 o;
@@ -502,26 +532,60 @@ __global__ void __launch_bounds__(kL1Warps * 32, 2) layer1_wgrad_kernel(const L1
 // ---------------------------------------------------------------------------
 // reductions of per-block partials (fixed order -> deterministic)
 // ---------------------------------------------------------------------------
+// One warp per output element: lane l sums the partials l, l + 32, ... in
+// order, then a fixed xor-shuffle tree adds the 32 lane sums -- the same
+// order on every run.
+__device__ __forceinline__ float warp_sum_fixed(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
 __global__ void reduce_partials_kernel(const float* part, int n_parts, int len, int stride, float* out,
                                        int accumulate) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < len; i += nw) {
     float s = 0.f;
-    for (int p = 0; p < n_parts; ++p) s += part[(size_t)p * stride + i];
-    out[i] = accumulate ? out[i] + s : s;
+    for (int p = lane; p < n_parts; p += 32) s += part[(size_t)p * stride + i];
+    s = warp_sum_fixed(s);
+    if (lane == 0) out[i] = accumulate ? out[i] + s : s;
   }
 }
 
-// wgrad raw partials [n_parts][dx][128][32] -> Keras kernel gradient [kh][kw][cin][32]
-// where accumulator row m = (kh) * cw + ci, cw = 8 * C/8 of the layer's input tensor.
-__global__ void wgrad_finish_kernel(const float* part, int n_parts, int cin, int cw, float* out) {
-  const int total = 9 * cin * kF;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-    const int co = i % kF, ci = (i / kF) % cin, tap = i / (kF * cin);
+// wgrad raw partials [n_parts][kw][128][jn * 32] -> Keras kernel gradient [kh][kw][cin][32].
+// Accumulator row m = r * cw + ci (input row r of the M window, cw = 8 * C/8 of the
+// layer's input tensor), column jj * 32 + co (output row jj of the N window); the
+// product belongs to kernel row kh = r - jj, so dW[kh] sums the jn pairs r = kh + jj.
+// jn = 2 for C = 32, 4 for C = 16.
+// A CTA owns the 32 output channels of one (tap, ci): lane = co reads the partials
+// coalesced, warp w sums partials w, w + 8, ... in order, and the 8 warp sums are
+// added in a fixed order -- deterministic.
+constexpr int kFinWarps = 8;
+__global__ void __launch_bounds__(kFinWarps * 32) wgrad_finish_kernel(const float* part, int n_parts, int cin,
+                                                                      int cw, float* out) {
+  __shared__ float red[kFinWarps][kF];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int jn = cw == 32 ? 2 : 4;
+  const int wn = jn * kF;
+  const int groups = 9 * cin;
+  for (int gi = blockIdx.x; gi < groups; gi += gridDim.x) {
+    const int ci = gi % cin, tap = gi / cin;
     const int kh = tap / 3, kw = tap % 3;
-    const int m = kh * cw + ci;
-    float s = 0.f;
-    for (int p = 0; p < n_parts; ++p) s += part[(((size_t)p * 3 + kw) * 128 + m) * kF + co];
-    out[i] = s;
+    float acc = 0.f;
+    for (int p = warp; p < n_parts; p += kFinWarps) {
+      const float* base = part + ((size_t)p * 3 + kw) * 128 * wn;
+      for (int jj = 0; jj < jn; ++jj) acc += base[(size_t)((kh + jj) * cw + ci) * wn + jj * kF + lane];
+    }
+    red[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0) {
+      float tsum = 0.f;
+#pragma unroll
+      for (int w2 = 0; w2 < kFinWarps; ++w2) tsum += red[w2][lane];
+      out[(size_t)gi * kF + lane] = tsum;
+    }
+    __syncthreads();
   }
 }
 
@@ -677,9 +741,16 @@ extern "C" int igm_cnn_head_forward(int batch, int h, int w, int nz, const void*
   IGM_CHECK_ARG(batch >= 1 && h >= 1 && w >= 1 && nz >= 1 && nz <= IGM_MAX_NZ, IGM_ERR_BAD_SHAPE,
                 "igm_cnn_head_forward: bad shape");
   IGM_CHECK_ARG(act && head_w && head_b && U && V, IGM_ERR_BAD_ARGUMENT, "igm_cnn_head_forward: NULL argument");
-  const size_t smem = (size_t)(kF * 2 * nz + 2 * nz) * sizeof(float);
-  head_fwd_kernel<<<grid_for((size_t)batch * h * w), 256, smem, as_stream(stream)>>>(
-      batch, h, w, nz, (const __nv_bfloat16*)act, head_w, head_b, out_scale, U, V, thk_mask);
+  const int nout = 2 * nz;
+  const int grid = grid_for((size_t)batch * h * w);
+  cudaStream_t st = as_stream(stream);
+  const __nv_bfloat16* A = (const __nv_bfloat16*)act;
+  if (nout <= 32)
+    head_fwd_kernel<32><<<grid, 256, 0, st>>>(batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask);
+  else if (nout <= 64)
+    head_fwd_kernel<64><<<grid, 256, 0, st>>>(batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask);
+  else
+    head_fwd_kernel<128><<<grid, 256, 0, st>>>(batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask);
   return launch_status("head_fwd_kernel");
 }
 
@@ -726,8 +797,8 @@ extern "C" int igm_reduce_partials(const float* partials, int n_parts, int len, 
   IGM_CHECK_ARG(partials && out && n_parts >= 1 && len >= 0 && stride >= len, IGM_ERR_BAD_ARGUMENT,
                 "igm_reduce_partials: bad argument");
   if (len == 0) return IGM_OK;
-  reduce_partials_kernel<<<grid_for(len), 256, 0, as_stream(stream)>>>(partials, n_parts, len, stride, out,
-                                                                      accumulate);
+  reduce_partials_kernel<<<grid_for((size_t)len * 32), 256, 0, as_stream(stream)>>>(partials, n_parts, len, stride,
+                                                                                   out, accumulate);
   return launch_status("reduce_partials_kernel");
 }
 
@@ -736,8 +807,7 @@ extern "C" int igm_cnn_wgrad_finish(const float* partials, int n_parts, int cin,
   IGM_CHECK_ARG(partials && out && n_parts >= 1, IGM_ERR_BAD_ARGUMENT, "igm_cnn_wgrad_finish: bad argument");
   IGM_CHECK_ARG((cin_tensor == 16 || cin_tensor == 32) && cin >= 1 && cin <= cin_tensor, IGM_ERR_BAD_SHAPE,
                 "igm_cnn_wgrad_finish: bad channel counts");
-  wgrad_finish_kernel<<<grid_for((size_t)9 * cin * kF), 256, 0, as_stream(stream)>>>(partials, n_parts, cin,
-                                                                                     cin_tensor, out);
+  wgrad_finish_kernel<<<9 * cin, kFinWarps * 32, 0, as_stream(stream)>>>(partials, n_parts, cin, cin_tensor, out);
   return launch_status("wgrad_finish_kernel");
 }
 

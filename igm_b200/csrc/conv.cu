@@ -354,7 +354,11 @@ constexpr int kWRows = 4;  // output rows per work item
 template <int C8_IN>
 struct WgradGeom {
   static constexpr int NROW = 128 / (C8_IN * 8);         // input rows covered by M = 128
-  static constexpr int XROWS = NROW + kWRows - 1;        // input rows of one item
+  // output rows covered by N: every one of them finds its three kernel rows in the M window
+  static constexpr int JN = (NROW - 2) < kWRows ? (NROW - 2) : kWRows;
+  static constexpr int NGRP = kWRows / JN;               // MMA row groups per item
+  static constexpr int WN = JN * kCout;                  // accumulator width per kw
+  static constexpr int XROWS = kWRows - JN + NROW;       // input rows of one item
   static constexpr uint32_t P = kBoxW * 16;              // X chunk plane stride
   static constexpr uint32_t RS = C8_IN * P;              // X row stride
   static constexpr uint32_t XBYTES = XROWS * RS;         // X stage
@@ -363,8 +367,9 @@ struct WgradGeom {
   static constexpr uint32_t STAGE = XBYTES + GBYTES;
   static constexpr int NST = 2;
   static constexpr uint32_t OFF_BAR = NST * STAGE;
-  static constexpr uint32_t TMEM_COLS = 128;
+  static constexpr uint32_t TMEM_COLS = 3 * WN <= 256 ? 256 : 512;
   static constexpr uint32_t SMEM = OFF_BAR + 8 * 8 + 16 + 1024;
+  static_assert(kWRows % JN == 0, "whole row groups per item");
 };
 
 template <int C8_IN>
@@ -412,7 +417,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_wgrad_kernel(const Wg
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t idesc = tc::make_idesc_bf16(128, kCout, true, true);
+      constexpr uint32_t idesc = tc::make_idesc_bf16(128, G::WN, true, true);
       for (int it = 0, t = blockIdx.x; t < a.n_items; t += gridDim.x, ++it) {
         const int s = it % G::NST, use = it / G::NST;
         if (!tc::mbar_wait(&full[s], use & 1)) {
@@ -422,17 +427,19 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_wgrad_kernel(const Wg
         tc::tc_fence_after();
         const uint32_t x0 = sbase + s * G::STAGE;
         const uint32_t g0 = x0 + G::XBYTES;
+        // Row group q: output rows y0 + q JN + jj (N = (jj, co)) against input rows
+        // y0 - 1 + q JN + m (M = (m, ci)); the product lands at kernel row kh = m - jj.
 #pragma unroll 1
-        for (int j = 0; j < kWRows; ++j) {  // output row y0 + j uses input rows y0 + j - 1 ...
+        for (int q = 0; q < G::NGRP; ++q) {
 #pragma unroll
           for (int dx = 0; dx < 3; ++dx) {
 #pragma unroll
             for (int ks = 0; ks < kTW / 16; ++ks) {
               // A: M = (input row, ci) groups of 8 channels every P bytes; K = pixels, 8-pixel groups 128 B apart
-              const uint64_t ad = tc::make_desc(x0 + j * G::RS + dx * 16 + ks * 256, 128, G::P);
-              // B: N = co groups of 8 every GP bytes; K = pixels
-              const uint64_t bd = tc::make_desc(g0 + j * 4 * G::GP + ks * 256, 128, G::GP);
-              tc::mma_bf16(tmem + dx * kCout, ad, bd, idesc, (it > 0 || j > 0 || ks > 0) ? 1u : 0u);
+              const uint64_t ad = tc::make_desc(x0 + q * G::JN * G::RS + dx * 16 + ks * 256, 128, G::P);
+              // B: N = (output row, co) groups of 8 every GP bytes; K = pixels
+              const uint64_t bd = tc::make_desc(g0 + q * G::JN * 4 * G::GP + ks * 256, 128, G::GP);
+              tc::mma_bf16(tmem + dx * G::WN, ad, bd, idesc, (it > 0 || q > 0 || ks > 0) ? 1u : 0u);
             }
           }
         }
@@ -451,19 +458,23 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_wgrad_kernel(const Wg
     }
 #pragma unroll 1
     for (int dx = 0; dx < 3; ++dx) {
-      uint32_t v[32];
-      tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(dx * kCout), v);
-      tc::tmem_wait_ld();
-      float4* dst = reinterpret_cast<float4*>(a.partial + (((size_t)blockIdx.x * 3 + dx) * 128 + m) * kCout);
+#pragma unroll 1
+      for (int cb = 0; cb < G::WN; cb += 32) {
+        uint32_t v[32];
+        tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(dx * G::WN + cb), v);
+        tc::tmem_wait_ld();
+        float4* dst =
+            reinterpret_cast<float4*>(a.partial + (((size_t)blockIdx.x * 3 + dx) * 128 + m) * G::WN + cb);
 #pragma unroll
-      for (int c = 0; c < kCout; c += 4) {
-        float4 f;
-        const bool z = my_items == 0 || !ok;
-        f.x = z ? 0.f : __uint_as_float(v[c + 0]);
-        f.y = z ? 0.f : __uint_as_float(v[c + 1]);
-        f.z = z ? 0.f : __uint_as_float(v[c + 2]);
-        f.w = z ? 0.f : __uint_as_float(v[c + 3]);
-        dst[c / 4] = f;
+        for (int c = 0; c < 32; c += 4) {
+          float4 f;
+          const bool z = my_items == 0 || !ok;
+          f.x = z ? 0.f : __uint_as_float(v[c + 0]);
+          f.y = z ? 0.f : __uint_as_float(v[c + 1]);
+          f.z = z ? 0.f : __uint_as_float(v[c + 2]);
+          f.w = z ? 0.f : __uint_as_float(v[c + 3]);
+          dst[c / 4] = f;
+        }
       }
     }
     tc::tc_fence_before();
@@ -592,6 +603,12 @@ extern "C" int igm_conv3x3_wgrad(int batch, int height, int width, int cin, cons
   cudaStream_t st = as_stream(stream);
   if (cin == 16) return wgrad_launch<2>(batch, height, width, x, g, partials, n_parts, err, st);
   return wgrad_launch<4>(batch, height, width, x, g, partials, n_parts, err, st);
+}
+
+extern "C" size_t igm_conv3x3_wgrad_partial_len(int cin) {
+  if (cin == 32) return (size_t)3 * 128 * WgradGeom<4>::WN;
+  if (cin == 16) return (size_t)3 * 128 * WgradGeom<2>::WN;
+  return 0;
 }
 
 extern "C" int igm_conv_sm_count(void) { return sm_count(); }

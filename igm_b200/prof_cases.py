@@ -44,7 +44,7 @@ def main():
     dbp = torch.zeros(148, 32, device="cuda")
     L.check(lib.igm_conv3x3(1, B, H, W, 32, y.data_ptr(), wp.data_ptr(), None, x.data_ptr(), y2.data_ptr(),
                             dbp.data_ptr(), 148, 0.01, err.data_ptr(), s), "conv dgrad")
-    part = torch.empty(148, 3, 128, 32, device="cuda")
+    part = torch.empty(148, int(lib.igm_conv3x3_wgrad_partial_len(32)), device="cuda")
     L.check(lib.igm_conv3x3_wgrad(B, H, W, 32, x.data_ptr(), y.data_ptr(), part.data_ptr(), 148, err.data_ptr(), s),
             "conv wgrad")
     torch.cuda.synchronize()

@@ -271,12 +271,15 @@ IGM_API int igm_conv3x3(int mode, int batch, int height, int width, int cin, con
                         const float* bias, const void* act_mask, void* y, float* db_partials, int db_slots,
                         float alpha, int* err, void* stream);
 
-/* Weight gradient of a 3x3 convolution: per-CTA partial sums
- * partials[n_parts][3 (kw)][128 (kh * cin + ci)][32 (co)] of X^T G over all
- * pixels (G = gradient w.r.t. the pre-activation, 32 channels).  Reduce them
- * with igm_cnn_wgrad_finish. */
+/* Weight gradient of a 3x3 convolution: per-CTA partial sums of X^T G over all
+ * pixels (G = gradient w.r.t. the pre-activation, 32 channels), laid out
+ * partials[n_parts][3 (kw)][128 (r * cin + ci)][jn * 32 (jj * 32 + co)] with
+ * jn = 2 for cin 32 and 4 for cin 16; entry (r, jj) belongs to kernel row
+ * kh = r - jj.  Each part holds igm_conv3x3_wgrad_partial_len(cin) floats.
+ * Reduce them with igm_cnn_wgrad_finish. */
 IGM_API int igm_conv3x3_wgrad(int batch, int height, int width, int cin, const void* x, const void* g,
                               float* partials, int n_parts, int* err, void* stream);
+IGM_API size_t igm_conv3x3_wgrad_partial_len(int cin);
 IGM_API int igm_conv_sm_count(void);
 
 IGM_API size_t igm_cnn_param_count(int nb_layers, int cin, int nout);

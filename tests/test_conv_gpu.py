@@ -116,7 +116,7 @@ def test_conv_wgrad(B, H, W, cin):
     ref = torch.nn.grad.conv2d_weight(x[:, :cin_real], (32, cin_real, 3, 3), gout, padding=1)  # [co, ci, kh, kw]
     ref_k = ref.permute(2, 3, 1, 0).contiguous()  # Keras [kh, kw, ci, co]
     npart = 37
-    part = torch.empty((npart, 3, 128, 32), device="cuda")
+    part = torch.empty((npart, int(L.lib().igm_conv3x3_wgrad_partial_len(cin))), device="cuda")
     out = torch.empty((3, 3, cin_real, 32), device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     xd = to_rc(x).to(torch.bfloat16).cuda()
