@@ -230,11 +230,14 @@ struct TileGeo {
 // x, then y, then batch), streaming the sequence (tile, level) through one
 // ring, so the loads of a tile's first levels and its 2-D fields are issued
 // while the previous tile is still being computed.
-template <typename T, int TYP, int MODE, bool TMA>
+template <typename T, int TYP, int MODE, bool TMA, bool STD>
 __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
     stencil_kernel(const StencilArgs<T> a, const __grid_constant__ StencilMaps maps) {
   using P = Two<T>;
   using SmemT = StencilSmem<T, TYP, MODE>;
+  // STD: the default physics (Glen n = 3, Weertman m = 3, gravitational energy not forced
+  // negative), fixed at compile time so that its branches and generic powers drop out
+  const bool glen3 = STD || a.glen3, weert3 = STD || a.weert3, fnge = !STD && a.fnge;
   constexpr int TYC = 2 * TYP;  // cell rows per tile
   constexpr int NT = kCW * TYP;
   constexpr int NR = TYC + 1, NC = kCW + 1;
@@ -412,7 +415,7 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
         SM.F[0][3][sm] = ok ? a.C[o] : T(0);
         Av = ok ? a.A[o] : T(1);
       }
-      SM.F[fb][2][sm] = ok ? T(2) * (a.glen3 ? rcbrt_k<T>(Av) : Math<T>::pow(Av, -a.inv_n)) : T(0);
+      SM.F[fb][2][sm] = ok ? T(2) * (glen3 ? rcbrt_k<T>(Av) : Math<T>::pow(Av, -a.inv_n)) : T(0);
     }
     // these generic writes precede a later TMA write to the same buffer
     if (TMA) tc::fence_proxy_async_smem();
@@ -554,12 +557,12 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
       level_q(SM.N[nb][1], cSv, cXv, cYv);
       // gravity of level k (weight dzeta[k-1] + dzeta[k]) enters its pending adjoint directly
       const T wk = a.wgrav[k];
-      if (!a.fnge) {
+      if (!fnge) {
         eGu = fma2(cSu, two(wk), eGu);
         eGv = fma2(cSv, two(wk), eGv);
       }
       P hSu = zero, hXu = zero, hYu = zero, hSv = zero, hXv = zero, hYv = zero;  // pending adjoint of level k
-      if (GRAD && !a.fnge) {
+      if (GRAD && !fnge) {
         hSu = gxc * two(wk);
         hSv = gyc * two(wk);
       }
@@ -570,7 +573,7 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
         const P tb = fma2(cVs, sby, cUs * sbx);
         const P Nn = fma2(tb, tb, fma2(cUs, cUs, cVs * cVs) + two(a.regw2));
         P Np, dN;  // N^(s/2) and N^(s/2 - 1)
-        if (a.weert3) {
+        if (weert3) {
           dN = rcbrt2(Nn);  // N^(-1/3)
           Np = Nn * dN;     // N^(2/3)
         } else {
@@ -606,10 +609,10 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
         const P sc = {sr2w.x < a.lo2 ? a.lo2 : (sr2w.x > a.hi2 ? a.hi2 : sr2w.x),
                       sr2w.y < a.lo2 ? a.lo2 : (sr2w.y > a.hi2 ? a.hi2 : sr2w.y)};
         const P base = fma2(sc, two(a.k2), two(a.regu2));
-        const P bq = a.glen3 ? rcbrt2(base) : P{Math<T>::pow(base.x, a.q), Math<T>::pow(base.y, a.q)};
+        const P bq = glen3 ? rcbrt2(base) : P{Math<T>::pow(base.x, a.q), Math<T>::pow(base.y, a.q)};
         e_sh = fma2(bq * sr2w, two(dz), e_sh);
         P gXh = zero;  // gravity adjoint of this layer under force_negative_gravitational_energy
-        if (a.fnge) {
+        if (fnge) {
           // per layer: twice the staggered u . grad(s) (scaled by 4), kept only where negative
           P uds = fma2(cSv + pSv, ssy, (cSu + pSu) * ssx);
           const bool gax = uds.x < T(0), gay = uds.y < T(0);
@@ -622,7 +625,7 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
           const bool in_y = sr2w.y >= a.lo2 && sr2w.y <= a.hi2;
           // d(bq sr2)/d sr2 = bq + q bq / base sr2; bq / base = bq^4 for n = 3
           P bq_base;
-          if (a.glen3) {
+          if (glen3) {
             const P bq2 = bq * bq;
             bq_base = bq2 * bq2;
           } else {
@@ -637,7 +640,7 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
           const P Gu = fma2(gX, nsbx, fma2(gY, nsby, G * uz)) * rz;
           const P Gv = fma2(gY, nsbx, fma2(gW, nsby, G * vz)) * rz;
           P fgu = zero, fgv = zero;  // gravity under force_negative_gravitational_energy
-          if (a.fnge) {
+          if (fnge) {
             fgu = gxc * gXh;
             fgv = gyc * gXh;
           }
@@ -681,7 +684,7 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
       finish(nz - 1, st_m1);
     }
     // this tile's energy densities (owned cells only)
-    const P egrav = a.fnge ? egc * e_gf : egc * fma2(ssy, eGv, ssx * eGu);
+    const P egrav = fnge ? egc * e_gf : egc * fma2(ssy, eGv, ssx * eGu);
     const P es = sel(own[0], own[1], esc * e_sh, zero);
     const P eg = sel(own[0], own[1], egrav, zero);
     const P el = sel(own[0], own[1], e_slid, zero);
@@ -936,12 +939,12 @@ static bool tma_usable(const igm_grid* g, std::initializer_list<const void*> ptr
 }
 
 // Persistent launch: as many CTAs as fit on the device at once (at most one per tile).
-template <typename T, int MODE, bool TMA>
+template <typename T, int MODE, bool TMA, bool STD>
 static int launch_stencil_t(const StencilArgs<T>& s, const StencilMaps& maps, const igm_grid* g, cudaStream_t st) {
   constexpr int TYP = ThreadRows<T>::value;
   constexpr int TYC = 2 * TYP;
   constexpr size_t smem = sizeof(StencilSmem<T, TYP, MODE>) + 128;
-  auto kern = stencil_kernel<T, TYP, MODE, TMA>;
+  auto kern = stencil_kernel<T, TYP, MODE, TMA, STD>;
   static int per_sm = 0;
   if (per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -968,7 +971,10 @@ static int launch_stencil_t(const StencilArgs<T>& s, const StencilMaps& maps, co
 template <typename T, int MODE>
 static int launch_stencil(const StencilArgs<T>& s, const StencilMaps& maps, bool tma, const igm_grid* g,
                           cudaStream_t st) {
-  return tma ? launch_stencil_t<T, MODE, true>(s, maps, g, st) : launch_stencil_t<T, MODE, false>(s, maps, g, st);
+  const bool std_phys = s.glen3 && s.weert3 && !s.fnge;
+  if (std_phys)
+    return tma ? launch_stencil_t<T, MODE, true, true>(s, maps, g, st) : launch_stencil_t<T, MODE, false, true>(s, maps, g, st);
+  return tma ? launch_stencil_t<T, MODE, true, false>(s, maps, g, st) : launch_stencil_t<T, MODE, false, false>(s, maps, g, st);
 }
 
 template <typename T>

@@ -132,3 +132,28 @@ def test_energy_reduction_is_deterministic():
     a = [K.energy(U, V, *f, 50.0, dz, grad=True) for _ in range(3)]
     for t, dU, dV in a[1:]:
         assert torch.equal(t, a[0][0]) and torch.equal(dU, a[0][1]) and torch.equal(dV, a[0][2])
+
+
+@pytest.mark.parametrize("n,m,fnge", [(2.5, 2.0, False), (3.0, 3.0, True), (4.0, 1.5, True)])
+def test_other_physics_against_oracle(n, m, fnge):
+    """Glen and Weertman exponents other than 3 and the forced-negative
+    gravitational energy take the kernel's general path (generic powers,
+    per-layer gravity clamp); FP64 against the FP64 oracle."""
+    nz, ny, nx = 6, 37, 45
+    rng = np.random.default_rng(int(n * 10 + m))
+    st = O.valley_glacier(ny, nx, 100.0, seed=7, varying_coeffs=True)
+    dz = O.compute_zeta_dzeta(O.compute_levels(nz, 4.0).double())[1]
+    U = rng.normal(30, 20, (nz, ny, nx))
+    V = rng.normal(0, 20, (nz, ny, nx))
+    fl = {k: torch.as_tensor(st[k]).double() for k in ["thk", "usurf", "arrhenius", "slidingco"]}
+    ph = O.Physics(exp_glen=n, exp_weertman=m, force_negative_gravitational_energy=fnge)
+    cost, means, gU, gV = O.energy_and_grad(torch.as_tensor(U), torch.as_tensor(V), fl["thk"], fl["usurf"],
+                                            fl["arrhenius"], fl["slidingco"], 100.0, dz, ph)
+    ns = (ny - 1) * (nx - 1)
+    phys = dict(exp_glen=n, exp_weertman=m, force_negative_gravitational_energy=fnge)
+    terms, dU, dV = K.energy(dev(U, torch.float64), dev(V, torch.float64), *[dev(fl[k]) for k in fl], 100.0,
+                             dz.numpy(), phys, grad=True, grad_scale=1.0 / ns)
+    np.testing.assert_allclose(terms.cpu().numpy() / ns, torch.stack(means).numpy(), rtol=1e-10,
+                               atol=1e-10 * float(cost.abs()))
+    assert rel_l2(dU.cpu().numpy(), gU.numpy()) < 1e-10
+    assert rel_l2(dV.cpu().numpy(), gV.numpy()) < 1e-10
