@@ -41,6 +41,7 @@
 #include <string.h>
 
 #include <initializer_list>
+#include <type_traits>
 #include <mutex>
 
 #include "common.cuh"
@@ -539,8 +540,10 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
       }
     };
 
-#pragma unroll 2
-    for (int k = 0; k < nz; ++k) {
+    // one level of the stream; the first level (sliding, no layer below it) is peeled
+    // off at compile time so that the steady-state loop carries no branches on k
+    auto level = [&](const int k, auto first_tag) {
+      constexpr bool FIRST = decltype(first_tag)::value;
       const int nb = cons_st;
       if (TMA) {
         // level k landed: one thread waits (the others spend no issue slots polling)
@@ -550,7 +553,7 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
       }
       __syncthreads();  // level k visible to all; every thread is done with the previous iteration
       issue_next();
-      if (GRAD && k >= 2) finish(k - 2, st_m2);
+      if (GRAD && !FIRST && k >= 2) finish(k - 2, st_m2);
 
       P cSu, cXu, cYu, cSv, cXv, cYv;
       level_q(SM.N[nb][0], cSu, cXu, cYu);
@@ -567,7 +570,7 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
         hSv = gyc * two(wk);
       }
 
-      if (k == 0) {
+      if (FIRST) {
         // Weertman sliding on the basal level (cost_sliding_weertman.py:23-43)
         const P cUs = cSu * Q4, cVs = cSv * Q4;
         const P tb = fma2(cVs, sby, cUs * sbx);
@@ -591,8 +594,8 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
         }
       }
 
-      if (k >= 1 || nz == 1) {
-        const int l = nz == 1 ? 0 : k - 1;
+      if (!FIRST || nz == 1) {
+        const int l = FIRST ? 0 : k - 1;  // a layer on the first level exists only when nz == 1
         const T dz = a.dzeta[l];
         const P rz = rzc * two(a.inv_dzeta[l]);
         const P uz = (cSu - pSu) * rz, vz = (cSv - pSv) * rz;
@@ -661,7 +664,7 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
       }
 
       if (GRAD) {
-        if (k >= 1 && nz > 1) {
+        if (!FIRST && nz > 1) {
           flush(k - 1, gSu, gXu, gYu, 0, partU);
           flush(k - 1, gSv, gXv, gYv, 1, partV);
         }
@@ -674,7 +677,10 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
         cons_st = 0;
         cons_ph ^= 1u;
       }
-    }
+    };
+    level(0, std::true_type{});
+#pragma unroll 2
+    for (int k = 1; k < nz; ++k) level(k, std::false_type{});
     if (GRAD) {
       __syncthreads();
       if (nz >= 2) finish(nz - 2, st_m2);
