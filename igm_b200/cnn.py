@@ -130,13 +130,14 @@ class CNN:
             b["U"] = torch.empty((B, self.nz, h, w), dtype=torch.float32, device=d)
             b["V"] = torch.empty_like(b["U"])
             b["fields"] = [torch.empty((B, h, w), dtype=torch.float32, device=d) for _ in range(4)]
+            b["X"] = act(16)  # split first-layer input (igm_cnn_input)
             if train:
                 b["g"] = [act(F), act(F)]
                 npart = self.n_sm
                 b["npart"] = npart          # persistent tensor-core kernels: one CTA per SM
                 b["npart2"] = 2 * npart     # head / first-layer reductions: two CTAs per SM
-                wlen = int(L.lib().igm_conv3x3_wgrad_partial_len(F))
-                b["wpart"] = torch.empty(max(npart * wlen, 2 * npart * 9 * self.cin * F), dtype=torch.float32, device=d)
+                wlen = max(int(L.lib().igm_conv3x3_wgrad_partial_len(F)), int(L.lib().igm_conv3x3_wgrad_partial_len(16)))
+                b["wpart"] = torch.empty(npart * wlen, dtype=torch.float32, device=d)
                 b["dbpart"] = torch.zeros((npart, F), dtype=torch.float32, device=d)
                 hl = int(L.lib().igm_cnn_head_partial_len(self.nz))
                 b["hpart"] = torch.empty((2 * npart, hl), dtype=torch.float32, device=d)
@@ -152,7 +153,7 @@ class CNN:
         x0 = (C.c_int * B)(*[int(b) for _, b in windows])
         sc = (C.c_float * 5)(*[float(s) for s in self.scales])
         rc = L.lib().igm_cnn_input(B, h, w, ny, nx, *[_p(f) for f in fields_full], float(dx), sc, y0, x0,
-                                   None, *[_p(f) for f in buf["fields"]], L.stream_ptr())
+                                   _p(buf["X"]), *[_p(f) for f in buf["fields"]], L.stream_ptr())
         L.check(rc, "igm_cnn_input")
         buf["dx"] = float(dx)
 
@@ -161,12 +162,13 @@ class CNN:
 
     def forward(self, buf, B, h, w, thk_mask=None, keep_acts=False):
         """Runs the network on the windowed fields of ``buf`` (prepare_input):
-        the FP32 first layer, the tensor-core layers, the head; U, V into buf."""
+        the first layer on the split (x_h, x_l, x_h) input, the 3x3 layers, the
+        head -- all convolutions on the tensor cores; U, V into buf."""
         lib, st = L.lib(), L.stream_ptr()
         acts = buf["acts"]
-        rc = lib.igm_cnn_layer1_forward(B, h, w, self.cin, *[_p(f) for f in buf["fields"]], buf["dx"], self._scales(),
-                                        self.params.data_ptr(), self._b(0), self.alpha, _p(acts[0]), st)
-        L.check(rc, "igm_cnn_layer1_forward")
+        rc = lib.igm_conv3x3(0, B, h, w, 16, _p(buf["X"]), self._wf(0), self._b(0), None, _p(acts[0]), None, 0,
+                             self.alpha, _p(self.err), st)
+        L.check(rc, "igm_conv3x3 layer 0")
         x = acts[0]
         cin_t = F
         hook = self.event_hook if (self.event_hook is not None and not keep_acts) else None
@@ -219,12 +221,11 @@ class CNN:
                 rc = lib.igm_cnn_wgrad_finish(_p(buf["wpart"]), npart, F, F, gp + 4 * self.offsets[2 * l], st)
                 L.check(rc, "igm_cnn_wgrad_finish")
             else:
-                n1 = 9 * self.cin * F
-                rc = lib.igm_cnn_layer1_wgrad(B, h, w, self.cin, *[_p(f) for f in buf["fields"]], buf["dx"],
-                                              self._scales(), _p(gl), _p(buf["wpart"]), npart2, st)
-                L.check(rc, "igm_cnn_layer1_wgrad")
-                L.check(lib.igm_reduce_partials(_p(buf["wpart"]), npart2, n1, n1, gp + 4 * self.offsets[0], 0, st),
-                        "reduce layer-1 wgrad")
+                rc = lib.igm_conv3x3_wgrad(B, h, w, 16, _p(buf["X"]), _p(gl), _p(buf["wpart"]), npart,
+                                           _p(self.err), st)
+                L.check(rc, "igm_conv3x3_wgrad layer 0")
+                rc = lib.igm_cnn_wgrad_finish_split(_p(buf["wpart"]), npart, self.cin, gp + 4 * self.offsets[0], st)
+                L.check(rc, "igm_cnn_wgrad_finish_split")
             if l > 0:
                 nxt = g[1 - cur]
                 buf["dbpart"].zero_()

@@ -50,7 +50,8 @@ __host__ __device__ inline size_t param_count(int L, int cin0, int nout) {
 // ---------------------------------------------------------------------------
 // weight packing: fp32 Keras layout -> bf16 UMMA B operands, ordered so that
 // for one (kw, 8-channel k-chunk) the three kernel rows follow each other:
-//  forward  layer l: [kw][k-chunk (ci)][kh][co][8]   (layer 0: 2 k-chunks, zero above cin0)
+//  forward  layer l: [kw][k-chunk (ci)][kh][co][8]   (layer 0: 2 k-chunks over the split
+//           input channels 3c + {0, 1, 2} of field c: W_h, W_h, W_l; zero for c >= cin0)
 //  dgrad    layer l>=1: [kw'][k-chunk (co)][kh'][ci][8], flipped: kh' = 2 - kh, kw' = 2 - kw
 // ---------------------------------------------------------------------------
 __global__ void pack_kernel(const float* params, int L, int cin0, int nout, __nv_bfloat16* wf, __nv_bfloat16* wb) {
@@ -67,9 +68,19 @@ __global__ void pack_kernel(const float* params, int L, int cin0, int nout, __nv
       const int e = rem % 8, co = (rem / 8) % kF, kh = (rem / (8 * kF)) % 3, kc = (rem / (24 * kF)) % c8,
                 kw = rem / (24 * kF * c8);
       const int ci = kc * 8 + e;
-      const int cin = l == 0 ? cin0 : kF;
       float v = 0.f;
-      if (ci < cin) v = params[w_offset(l, cin0, nout) + (((size_t)kh * 3 + kw) * cin + ci) * kF + co];
+      if (l == 0) {
+        // layer 0 reads the split input (x_h, x_l, x_h per field): weights W_h, W_h, W_l with
+        // W_h = bf16(W), W_l = bf16(W - W_h), so that x W ~ x_h W_h + x_l W_h + x_h W_l
+        const int c = ci / 3, part = ci - 3 * c;
+        if (c < cin0) {
+          const float w = params[w_offset(0, cin0, nout) + (((size_t)kh * 3 + kw) * cin0 + c) * kF + co];
+          const float wh = __bfloat162float(__float2bfloat16_rn(w));
+          v = part == 2 ? w - wh : wh;
+        }
+      } else {
+        v = params[w_offset(l, cin0, nout) + (((size_t)kh * 3 + kw) * kF + ci) * kF + co];
+      }
       wf[i] = __float2bfloat16_rn(v);
     } else {
       const size_t j = i - total_f;
@@ -115,12 +126,28 @@ __global__ void input_kernel(const InputArgs a) {
       if (a.out[c]) a.out[c][i] = v[c];
     }
     if (a.X) {
+      // each scaled field x as three BF16 channels (x_h, x_l, x_h) with x_h = bf16(x),
+      // x_l = bf16(x - x_h); channel 15 is zero
+      float ch[16];
+      const float xs[5] = {v[0] * a.scale[0], v[1] * a.scale[1], v[2] * a.scale[2], v[3] * a.scale[3],
+                           a.dx * a.scale[4]};
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        const float hi = __bfloat162float(__float2bfloat16_rn(xs[c]));
+        ch[3 * c] = hi;
+        ch[3 * c + 1] = xs[c] - hi;
+        ch[3 * c + 2] = hi;
+      }
+      ch[15] = 0.f;
       uint4 c0, c1;
-      c0.x = bf_pack(v[0] * a.scale[0], v[1] * a.scale[1]);
-      c0.y = bf_pack(v[2] * a.scale[2], v[3] * a.scale[3]);
-      c0.z = bf_pack(a.dx * a.scale[4], 0.f);
-      c0.w = 0u;
-      c1.x = c1.y = c1.z = c1.w = 0u;
+      c0.x = bf_pack(ch[0], ch[1]);
+      c0.y = bf_pack(ch[2], ch[3]);
+      c0.z = bf_pack(ch[4], ch[5]);
+      c0.w = bf_pack(ch[6], ch[7]);
+      c1.x = bf_pack(ch[8], ch[9]);
+      c1.y = bf_pack(ch[10], ch[11]);
+      c1.z = bf_pack(ch[12], ch[13]);
+      c1.w = bf_pack(ch[14], ch[15]);
       uint4* X = reinterpret_cast<uint4*>(a.X);
       const size_t row = ((size_t)b * a.h + y) * 2;
       X[(row + 0) * a.w + x] = c0;
@@ -589,6 +616,36 @@ __global__ void __launch_bounds__(kFinWarps * 32) wgrad_finish_kernel(const floa
   }
 }
 
+// Layer 0 (split input): the weight gradient of field c is the sum of the raw
+// gradients of its x_h and x_l channels (3c, 3c + 1); the duplicate x_h channel
+// (3c + 2, weights W_l) only carries the weights' low part and is not a variable.
+__global__ void __launch_bounds__(kFinWarps * 32) wgrad_finish_split_kernel(const float* part, int n_parts, int cin,
+                                                                            float* out) {
+  __shared__ float red[kFinWarps][kF];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int cw = 16, jn = 4, wn = jn * kF;  // the 16-channel input tensor's partial layout
+  const int groups = 9 * cin;
+  for (int gi = blockIdx.x; gi < groups; gi += gridDim.x) {
+    const int c = gi % cin, tap = gi / cin;
+    const int kh = tap / 3, kw = tap % 3;
+    float acc = 0.f;
+    for (int p = warp; p < n_parts; p += kFinWarps) {
+      const float* base = part + ((size_t)p * 3 + kw) * 128 * wn;
+      for (int jj = 0; jj < jn; ++jj)
+        for (int sp = 0; sp < 2; ++sp) acc += base[(size_t)((kh + jj) * cw + 3 * c + sp) * wn + jj * kF + lane];
+    }
+    red[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0) {
+      float tsum = 0.f;
+#pragma unroll
+      for (int w2 = 0; w2 < kFinWarps; ++w2) tsum += red[w2][lane];
+      out[(size_t)gi * kF + lane] = tsum;
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Adam (Keras legacy): per-variable clip_by_norm, then
 //   m += (g - m)(1 - b1); v += (g^2 - v)(1 - b2); x -= lr_t m / (sqrt(v) + eps)
@@ -809,6 +866,13 @@ extern "C" int igm_cnn_wgrad_finish(const float* partials, int n_parts, int cin,
                 "igm_cnn_wgrad_finish: bad channel counts");
   wgrad_finish_kernel<<<9 * cin, kFinWarps * 32, 0, as_stream(stream)>>>(partials, n_parts, cin, cin_tensor, out);
   return launch_status("wgrad_finish_kernel");
+}
+
+extern "C" int igm_cnn_wgrad_finish_split(const float* partials, int n_parts, int cin, float* out, void* stream) {
+  IGM_CHECK_ARG(partials && out && n_parts >= 1, IGM_ERR_BAD_ARGUMENT, "igm_cnn_wgrad_finish_split: bad argument");
+  IGM_CHECK_ARG(cin >= 1 && cin <= 5, IGM_ERR_BAD_SHAPE, "igm_cnn_wgrad_finish_split: 1..5 input fields");
+  wgrad_finish_split_kernel<<<9 * cin, kFinWarps * 32, 0, as_stream(stream)>>>(partials, n_parts, cin, out);
+  return launch_status("wgrad_finish_split_kernel");
 }
 
 extern "C" int igm_adam_clipnorm(int n_vars, const size_t* var_offsets, float* params, const float* grads,

@@ -295,8 +295,13 @@ IGM_API int igm_cnn_pack_weights(int nb_layers, int cin, int nout, const float* 
 /* Emulator input (fieldin_to_X, iceflow/utils.py:147-158, with split_into_patches
  * windows, emulate.py:283-308): X[b] = scaled (thk, usurf, arrhenius, slidingco, dx)
  * of the window at host (win_y0[b], win_x0[b]) of size h x w of the [ny][nx]
- * fields (bf16, may be NULL) and fp32 copies of the windowed fields
- * ([batch][h][w], each may be NULL).  scales: host float[5]. */
+ * fields, and fp32 copies of the windowed fields ([batch][h][w], each may be
+ * NULL).  X (may be NULL) is the row-chunked bf16 [batch][h][2][w][8] tensor of
+ * the first layer: each scaled field x in three channels (x_h, x_l, x_h) with
+ * x_h = bf16(x), x_l = bf16(x - x_h) -- with the layer-0 weight pack (W_h, W_h,
+ * W_l) the tensor-core convolution then sums x_h W_h + x_l W_h + x_h W_l, about
+ * 16 significant bits of x W, enough for the metre-scale steps of a ~3000 m
+ * surface.  scales: host float[5]. */
 IGM_API int igm_cnn_input(int batch, int h, int w, int ny, int nx, const float* thk, const float* usurf,
                           const float* arrhenius, const float* slidingco, double dx, const float* scales,
                           const int* win_y0, const int* win_x0, void* X, float* thk_out, float* usurf_out,
@@ -340,6 +345,10 @@ IGM_API int igm_reduce_partials(const float* partials, int n_parts, int len, int
  * the C of the layer's input tensor (16 or 32). */
 IGM_API int igm_cnn_wgrad_finish(const float* partials, int n_parts, int cin, int cin_tensor, float* out,
                                  void* stream);
+/* igm_conv3x3_wgrad partials of the first layer over the split input of
+ * igm_cnn_input -> its kernel gradient [3][3][cin][32] (cin <= 5 fields): the
+ * x_h and x_l channel gradients of each field added. */
+IGM_API int igm_cnn_wgrad_finish_split(const float* partials, int n_parts, int cin, float* out, void* stream);
 
 /* Keras legacy Adam with per-variable clip_by_norm (emulate.py:22-35, :267):
  * for each variable v (elements [var_offsets[v], var_offsets[v+1]) of the
