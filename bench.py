@@ -339,8 +339,11 @@ def run_ours(args, rank, world, dist):
     from igm_b200.processes.iceflow import set_derived_velocities
     update_iceflow_emulated(cfg_e, st)
     res["vel_rel_l2_vs_fp64"], res["energy_gap_vs_fp64"] = velocity_error(cfg_e, st, st.U, st.V, Ur, Vr)
+    # the CFL step follows the largest |ubar|, |vbar| of each method's own field
+    res["velbar_absmax_emulated"] = float(torch.maximum(st.ubar.abs().max(), st.vbar.abs().max()))
     st.U, st.V = Ur.clone(), Vr.clone()
     set_derived_velocities(cfg_e, st, mask=False)
+    res["velbar_absmax_fp64_minimum"] = float(torch.maximum(st.ubar.abs().max(), st.vbar.abs().max()))
     ub = st.ubar.double()
     vb = st.vbar.double()
     res["dt_cfl_initial_a"] = float(0.3 * 50.0 / torch.sqrt(ub * ub + vb * vb).max())
@@ -542,6 +545,8 @@ def main():
                                   "state vs the FP64 energy minimum of that state",
             "energy_gap_vs_fp64": res["energy_gap_vs_fp64"],
             "dt_cfl_initial_a": res["dt_cfl_initial_a"],
+            "velbar_absmax_emulated": res["velbar_absmax_emulated"],
+            "velbar_absmax_fp64_minimum": res["velbar_absmax_fp64_minimum"],
             "reference_solve_s": res["reference_solve_s"],
             "fallback_checks": len(res["fallback_log"]),
             "fallbacks": sum(1 for x in res["fallback_log"] if x["fallback"]),

@@ -133,6 +133,7 @@ class CNN:
             b["X"] = act(16)  # split first-layer input (igm_cnn_input)
             if train:
                 b["g"] = [act(F), act(F)]
+                b["dyb"] = act(F)  # head output gradient in bf16 (head backward on the tensor cores)
                 npart = self.n_sm
                 b["npart"] = npart          # persistent tensor-core kernels: one CTA per SM
                 b["npart2"] = 2 * npart     # head / first-layer reductions: two CTAs per SM
@@ -201,16 +202,33 @@ class CNN:
         hw = self.params.data_ptr() + 4 * self.offsets[2 * self.L]
         hl = buf["hpart"].shape[1]
         g = buf["g"]
-        rc = lib.igm_cnn_head_backward(B, h, w, self.nz, _p(acts[self.L - 1]), hw, _p(dU), _p(dV), self.out_scale,
-                                       self.alpha, _p(g[0]), _p(buf["hpart"]), npart2, st)
-        L.check(rc, "igm_cnn_head_backward")
         gp = self.grads.data_ptr()
         nh = F * self.nout
-        # head kernel + bias gradients, last conv layer's bias gradient
-        L.check(lib.igm_reduce_partials(_p(buf["hpart"]), npart2, nh + self.nout, hl,
-                                        gp + 4 * self.offsets[2 * self.L], 0, st), "reduce head")
-        L.check(lib.igm_reduce_partials(buf["hpart"].data_ptr() + 4 * (nh + self.nout), npart2, F, hl,
-                                        gp + 4 * self.offsets[2 * (self.L - 1) + 1], 0, st), "reduce db")
+        if self.nout <= F:
+            # pixel part on CUDA cores, the head kernel gradient A16^T dY on the tensor cores
+            rc = lib.igm_cnn_head_backward_tc(B, h, w, self.nz, _p(acts[self.L - 1]), hw, _p(dU), _p(dV),
+                                              self.out_scale, self.alpha, _p(g[0]), _p(buf["dyb"]),
+                                              _p(buf["hpart"]), npart2, st)
+            L.check(rc, "igm_cnn_head_backward_tc")
+            stride = self.nout + F
+            L.check(lib.igm_reduce_partials(_p(buf["hpart"]), npart2, self.nout, stride,
+                                            gp + 4 * self.offsets[2 * self.L + 1], 0, st), "reduce head bias")
+            L.check(lib.igm_reduce_partials(buf["hpart"].data_ptr() + 4 * self.nout, npart2, F, stride,
+                                            gp + 4 * self.offsets[2 * (self.L - 1) + 1], 0, st), "reduce db")
+            rc = lib.igm_conv3x3_wgrad(B, h, w, F, _p(acts[self.L - 1]), _p(buf["dyb"]), _p(buf["wpart"]), npart,
+                                       _p(self.err), st)
+            L.check(rc, "igm_conv3x3_wgrad head")
+            L.check(lib.igm_cnn_head_wgrad_finish(_p(buf["wpart"]), npart, self.nout, gp + 4 * self.offsets[2 * self.L],
+                                                  st), "igm_cnn_head_wgrad_finish")
+        else:
+            rc = lib.igm_cnn_head_backward(B, h, w, self.nz, _p(acts[self.L - 1]), hw, _p(dU), _p(dV),
+                                           self.out_scale, self.alpha, _p(g[0]), _p(buf["hpart"]), npart2, st)
+            L.check(rc, "igm_cnn_head_backward")
+            # head kernel + bias gradients, last conv layer's bias gradient
+            L.check(lib.igm_reduce_partials(_p(buf["hpart"]), npart2, nh + self.nout, hl,
+                                            gp + 4 * self.offsets[2 * self.L], 0, st), "reduce head")
+            L.check(lib.igm_reduce_partials(buf["hpart"].data_ptr() + 4 * (nh + self.nout), npart2, F, hl,
+                                            gp + 4 * self.offsets[2 * (self.L - 1) + 1], 0, st), "reduce db")
         cur = 0
         for l in range(self.L - 1, -1, -1):
             gl = g[cur]

@@ -19,6 +19,7 @@
 namespace igm {
 
 constexpr int kF = 32;  // filters
+constexpr int kFinWarps = 8;  // warps of the fixed-order partial-sum kernels
 
 __device__ __forceinline__ float bf_lo(uint32_t w) {
   return __low2float(*reinterpret_cast<const __nv_bfloat162*>(&w));
@@ -391,6 +392,156 @@ __global__ void __launch_bounds__(kHeadWarps * 32, 2)
 }
 
 // ---------------------------------------------------------------------------
+// head backward for up to 32 outputs, pixel part: dPre16 = (dY Wh^T) *
+// LeakyReLU'(A16) and dY itself as a row-chunked bf16 [B][H][4][W][8] tensor
+// (outputs beyond 2 Nz zero), from which the tensor-core weight-gradient kernel
+// forms dWh = A16^T dY (its centre tap, igm_cnn_head_wgrad_finish).  Per-CTA
+// partials [dbh (2 Nz)][db16 (32)]: a warp stages 32 pixels' dY and dPre, then
+// lane l sums output l and channel l over them; warps are added in a fixed
+// order (deterministic).
+// ---------------------------------------------------------------------------
+constexpr int kHpWarps = 8;
+__global__ void __launch_bounds__(kHpWarps * 32, 2)
+    head_bwd_px_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act, const float* wh, const float* dU,
+                       const float* dV, float out_scale, float alpha, __nv_bfloat16* dpre, __nv_bfloat16* dyb,
+                       float* partial) {
+  extern __shared__ __align__(16) float hp_sm[];
+  float* swT = hp_sm;                                                      // [j][ci] = Wh[ci][j], 0 for j >= 2 nz
+  auto sP = reinterpret_cast<float(*)[32][33]>(hp_sm + kF * kF);          // [warp]: dPre of 32 pixels
+  auto sG = reinterpret_cast<float(*)[32][33]>(hp_sm + kF * kF + kHpWarps * 32 * 33);  // [warp]: dY
+  const int nout = 2 * nz;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < kF * kF; i += blockDim.x) {
+    const int j = i / kF, ci = i - (i / kF) * kF;
+    swT[i] = j < nout ? wh[ci * nout + j] : 0.f;
+  }
+  __syncthreads();
+  float accb = 0.f, accd = 0.f;  // dbh[j = lane], db16[ci = lane]
+  const size_t plane = (size_t)H * W;
+  const size_t total = plane * B;
+  const size_t nchunks = (total + 31) / 32;
+  const size_t nwarps = (size_t)gridDim.x * kHpWarps;
+  const uint4* A = reinterpret_cast<const uint4*>(act);
+  uint4* DP = reinterpret_cast<uint4*>(dpre);
+  uint4* DY = reinterpret_cast<uint4*>(dyb);
+  for (size_t chunk = (size_t)blockIdx.x * kHpWarps + warp; chunk < nchunks; chunk += nwarps) {
+    const size_t i = chunk * 32 + lane;
+    const bool ok = i < total;
+    int b = 0, y = 0, x = 0;
+    size_t rem = 0;
+    if (ok) {
+      b = (int)(i / plane);
+      rem = i - (size_t)b * plane;
+      y = (int)(rem / W);
+      x = (int)(rem - (size_t)y * W);
+    }
+    uint4 au[4];
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) au[ch] = ok ? A[(((size_t)b * H + y) * 4 + ch) * W + x] : make_uint4(0, 0, 0, 0);
+    float g[kF];
+#pragma unroll
+    for (int j = 0; j < kF; ++j) {
+      float v = 0.f;
+      if (ok && j < nout) {
+        const float* src = j < nz ? dU : dV;
+        const int k = j < nz ? j : j - nz;
+        v = src[((size_t)b * nz + k) * plane + rem] * out_scale;
+      }
+      g[j] = v;
+      sG[warp][lane][j] = v;
+    }
+    // dPre = dY Wh^T, two channels per packed fma
+    float2 da[kF / 2];
+#pragma unroll
+    for (int q = 0; q < kF / 2; ++q) da[q] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < kF; ++j) {
+      if (j >= nout) break;
+      const float2 gg = make_float2(g[j], g[j]);
+      const float4* wr = reinterpret_cast<const float4*>(swT + j * kF);
+#pragma unroll
+      for (int q = 0; q < kF / 4; ++q) {
+        const float4 w4 = wr[q];
+        da[2 * q] = __ffma2_rn(gg, make_float2(w4.x, w4.y), da[2 * q]);
+        da[2 * q + 1] = __ffma2_rn(gg, make_float2(w4.z, w4.w), da[2 * q + 1]);
+      }
+    }
+    uint4 po[4], yo[4];
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+      const uint32_t wv[4] = {au[ch].x, au[ch].y, au[ch].z, au[ch].w};
+      uint32_t pk[4], yk[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int c = ch * 8 + 2 * e;
+        const float lo = da[c >> 1].x * (bf_lo(wv[e]) > 0.f ? 1.f : alpha);
+        const float hi = da[c >> 1].y * (bf_hi(wv[e]) > 0.f ? 1.f : alpha);
+        sP[warp][lane][c] = lo;
+        sP[warp][lane][c + 1] = hi;
+        pk[e] = bf_pack(lo, hi);
+        yk[e] = bf_pack(g[c], g[c + 1]);
+      }
+      po[ch] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+      yo[ch] = make_uint4(yk[0], yk[1], yk[2], yk[3]);
+    }
+    if (ok) {
+#pragma unroll
+      for (int ch = 0; ch < 4; ++ch) {
+        const size_t o = (((size_t)b * H + y) * 4 + ch) * W + x;
+        DP[o] = po[ch];
+        DY[o] = yo[ch];
+      }
+    }
+    __syncwarp();
+    for (int p = 0; p < 32; ++p) {
+      accd += sP[warp][p][lane];
+      accb += sG[warp][p][lane];
+    }
+    __syncwarp();  // this warp's staging area is rewritten by its next chunk
+  }
+  __syncthreads();
+  float* red = &sP[0][0][0];  // [warp][64]: dbh (32), db16 (32)
+  red[warp * 64 + lane] = accb;
+  red[warp * 64 + 32 + lane] = accd;
+  __syncthreads();
+  float* out = partial + (size_t)blockIdx.x * (nout + kF);
+  if (threadIdx.x < 64) {
+    float t = 0.f;
+    for (int w2 = 0; w2 < kHpWarps; ++w2) t += red[w2 * 64 + threadIdx.x];
+    if (threadIdx.x < 32) {
+      if (threadIdx.x < nout) out[threadIdx.x] = t;
+    } else {
+      out[nout + threadIdx.x - 32] = t;
+    }
+  }
+}
+
+// head kernel gradient from igm_conv3x3_wgrad partials over (A16, dY): the centre
+// tap (kh = kw = 1), i.e. accumulator entries (r, jj) with r - jj = 1, kw = 1.
+__global__ void __launch_bounds__(kFinWarps * 32) head_wgrad_finish_kernel(const float* part, int n_parts, int nout,
+                                                                           float* out) {
+  __shared__ float red[kFinWarps][kF];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int cw = 32, jn = 2, wn = jn * kF;
+  for (int ci = blockIdx.x; ci < kF; ci += gridDim.x) {
+    float acc = 0.f;
+    for (int p = warp; p < n_parts; p += kFinWarps) {
+      const float* base = part + ((size_t)p * 3 + 1) * 128 * wn;
+      for (int jj = 0; jj < jn; ++jj) acc += base[(size_t)((1 + jj) * cw + ci) * wn + jj * kF + lane];
+    }
+    red[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0) {
+      float tsum = 0.f;
+#pragma unroll
+      for (int w2 = 0; w2 < kFinWarps; ++w2) tsum += red[w2][lane];
+      if (lane < nout) out[(size_t)ci * nout + lane] = tsum;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // First layer in FP32 on CUDA cores: the raw fields (surface elevation of
 // ~3000 m varying by a few metres per cell) cannot be rounded to BF16 without
 // losing the surface slope that drives the flow, so the 5 -> 32 layer reads
@@ -588,7 +739,6 @@ __global__ void reduce_partials_kernel(const float* part, int n_parts, int len, 
 // A CTA owns the 32 output channels of one (tap, ci): lane = co reads the partials
 // coalesced, warp w sums partials w, w + 8, ... in order, and the 8 warp sums are
 // added in a fixed order -- deterministic.
-constexpr int kFinWarps = 8;
 __global__ void __launch_bounds__(kFinWarps * 32) wgrad_finish_kernel(const float* part, int n_parts, int cin,
                                                                       int cw, float* out) {
   __shared__ float red[kFinWarps][kF];
@@ -848,6 +998,36 @@ extern "C" int igm_cnn_head_backward(int batch, int h, int w, int nz, const void
   return head_bwd_launch<128>(batch, h, w, nz, act, head_w, dU, dV, out_scale, alpha, dpre, partials, n_parts, st);
 }
 
+
+extern "C" int igm_cnn_head_backward_tc(int batch, int h, int w, int nz, const void* act, const float* head_w,
+                                        const float* dU, const float* dV, float out_scale, float alpha, void* dpre,
+                                        void* dy_bf16, float* partials, int n_parts, void* stream) {
+  IGM_CHECK_ARG(batch >= 1 && h >= 1 && w >= 1 && nz >= 1 && 2 * nz <= kF && n_parts >= 1, IGM_ERR_BAD_SHAPE,
+                "igm_cnn_head_backward_tc: bad shape (needs 2 nz <= 32)");
+  IGM_CHECK_ARG(act && head_w && dU && dV && dpre && dy_bf16 && partials, IGM_ERR_BAD_ARGUMENT,
+                "igm_cnn_head_backward_tc: NULL argument");
+  constexpr size_t smem = (size_t)(kF * kF + 2 * kHpWarps * 32 * 33) * sizeof(float);
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(head_bwd_px_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+      set_error("head_bwd_px smem attribute: %s", cudaGetErrorString(e));
+      return IGM_ERR_CUDA;
+    }
+    configured = true;
+  }
+  head_bwd_px_kernel<<<n_parts, kHpWarps * 32, smem, as_stream(stream)>>>(
+      batch, h, w, nz, (const __nv_bfloat16*)act, head_w, dU, dV, out_scale, alpha, (__nv_bfloat16*)dpre,
+      (__nv_bfloat16*)dy_bf16, partials);
+  return launch_status("head_bwd_px_kernel");
+}
+
+extern "C" int igm_cnn_head_wgrad_finish(const float* partials, int n_parts, int nout, float* out, void* stream) {
+  IGM_CHECK_ARG(partials && out && n_parts >= 1 && nout >= 1 && nout <= kF, IGM_ERR_BAD_ARGUMENT,
+                "igm_cnn_head_wgrad_finish: bad argument");
+  head_wgrad_finish_kernel<<<kF, kFinWarps * 32, 0, as_stream(stream)>>>(partials, n_parts, nout, out);
+  return launch_status("head_wgrad_finish_kernel");
+}
 
 extern "C" int igm_reduce_partials(const float* partials, int n_parts, int len, int stride, float* out,
                                    int accumulate, void* stream) {

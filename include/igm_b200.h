@@ -337,6 +337,20 @@ IGM_API int igm_cnn_head_backward(int batch, int h, int w, int nz, const void* a
                                   const float* dU, const float* dV, float out_scale, float alpha, void* dpre,
                                   float* partials, int n_parts, void* stream);
 
+/* Head backward for 2 nz <= 32 outputs, with its kernel gradient on the tensor
+ * cores: writes dpre as igm_cnn_head_backward does, the output gradient
+ * dY = out_scale * (dU, dV) as a row-chunked bf16 [batch][h][4][w][8] tensor
+ * (dy_bf16; outputs beyond 2 nz zero) and per-CTA partials
+ * [n_parts][2 nz + 32] of dbh and of the last conv layer's bias gradient.
+ * The head kernel gradient is then igm_conv3x3_wgrad(act, dy_bf16) reduced by
+ * igm_cnn_head_wgrad_finish. */
+IGM_API int igm_cnn_head_backward_tc(int batch, int h, int w, int nz, const void* act, const float* head_w,
+                                     const float* dU, const float* dV, float out_scale, float alpha, void* dpre,
+                                     void* dy_bf16, float* partials, int n_parts, void* stream);
+/* igm_conv3x3_wgrad partials over (act, dy_bf16) -> head kernel gradient [32][nout]
+ * (the centre tap), nout <= 32. */
+IGM_API int igm_cnn_head_wgrad_finish(const float* partials, int n_parts, int nout, float* out, void* stream);
+
 /* out[i] (+)= sum_p partials[p * stride + i], i < len, fixed summation order. */
 IGM_API int igm_reduce_partials(const float* partials, int n_parts, int len, int stride, float* out,
                                 int accumulate, void* stream);
