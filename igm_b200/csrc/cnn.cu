@@ -20,6 +20,7 @@ namespace igm {
 
 constexpr int kF = 32;  // filters
 constexpr int kFinWarps = 8;  // warps of the fixed-order partial-sum kernels
+constexpr int kRedBatch = 8;  // partials whose loads a lane issues before adding them
 
 __device__ __forceinline__ float bf_lo(uint32_t w) {
   return __low2float(*reinterpret_cast<const __nv_bfloat162*>(&w));
@@ -30,6 +31,14 @@ __device__ __forceinline__ float bf_hi(uint32_t w) {
 __device__ __forceinline__ uint32_t bf_pack(float lo, float hi) {
   __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<uint32_t*>(&h);
+}
+
+// fixed xor-shuffle tree over the 32 lanes: the same order on every run, the
+// total in every lane
+__device__ __forceinline__ float warp_sum_fixed(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
 }
 
 // offsets (in floats) of the parameters of layer l (0-based; l == L is the head)
@@ -395,28 +404,72 @@ __global__ void __launch_bounds__(kHeadWarps * 32, 2)
 // head backward for up to 32 outputs, pixel part: dPre16 = (dY Wh^T) *
 // LeakyReLU'(A16) and dY itself as a row-chunked bf16 [B][H][4][W][8] tensor
 // (outputs beyond 2 Nz zero), from which the tensor-core weight-gradient kernel
-// forms dWh = A16^T dY (its centre tap, igm_cnn_head_wgrad_finish).  Per-CTA
-// partials [dbh (2 Nz)][db16 (32)]: a warp stages 32 pixels' dY and dPre, then
-// lane l sums output l and channel l over them; warps are added in a fixed
-// order (deterministic).
+// forms dWh = A16^T dY (its centre tap, igm_cnn_head_wgrad_finish).  A warp
+// takes 32 consecutive pixels per chunk (lane = pixel).  Each lane keeps its
+// own running sums of dY (dbh) and dPre16 (db16) in registers; at the end fixed
+// xor trees add the lanes and the warps are added in a fixed order, giving the
+// per-CTA partials [dbh (2 Nz)][db16 (32)] (deterministic).  NJ = 2 Nz rounded
+// up to a multiple of 4.
 // ---------------------------------------------------------------------------
 constexpr int kHpWarps = 8;
+
+template <int NJ>
+struct HeadPx {
+  uint4 a[4];   // A16 of the pixel, 32 bf16 channels
+  float g[NJ];  // dY of the pixel (output_scale applied), 0 beyond 2 Nz
+  bool ok;
+  size_t o;     // uint4 index of channel chunk 0 of the pixel
+};
+
+// The loads are unconditional (lanes past the end and outputs past 2 Nz read a
+// valid element and select 0), so the compiler issues all of them back to back.
+template <int NJ>
+__device__ __forceinline__ void head_px_load(HeadPx<NJ>& q, size_t chunk, size_t total, size_t plane, int H, int W,
+                                             int nz, int nout, const uint4* A, const float* dU, const float* dV,
+                                             float out_scale, int lane) {
+  const size_t i = chunk * 32 + lane;
+  q.ok = i < total;
+  const size_t ic = q.ok ? i : 0;
+  const size_t b = ic / plane;
+  const size_t rem = ic - b * plane;
+  const size_t y = rem / W;
+  const size_t x = rem - y * W;
+  q.o = ((b * H + y) * 4) * W + x;
+#pragma unroll
+  for (int ch = 0; ch < 4; ++ch) {
+    const uint4 v = A[q.o + (size_t)ch * W];
+    q.a[ch] = q.ok ? v : make_uint4(0, 0, 0, 0);
+  }
+  const float* pu = dU + b * nz * plane + rem;
+  const float* pv = dV + b * nz * plane + rem;
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) {
+    const int k = j < nz ? j : min(j - nz, nz - 1);
+    const float v = (j < nz ? pu : pv)[(size_t)k * plane];
+    q.g[j] = (q.ok && j < nout) ? v * out_scale : 0.f;
+  }
+}
+
+template <int NJ>
 __global__ void __launch_bounds__(kHpWarps * 32, 2)
     head_bwd_px_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act, const float* wh, const float* dU,
                        const float* dV, float out_scale, float alpha, __nv_bfloat16* dpre, __nv_bfloat16* dyb,
                        float* partial) {
-  extern __shared__ __align__(16) float hp_sm[];
-  float* swT = hp_sm;                                                      // [j][ci] = Wh[ci][j], 0 for j >= 2 nz
-  auto sP = reinterpret_cast<float(*)[32][33]>(hp_sm + kF * kF);          // [warp]: dPre of 32 pixels
-  auto sG = reinterpret_cast<float(*)[32][33]>(hp_sm + kF * kF + kHpWarps * 32 * 33);  // [warp]: dY
+  static_assert(NJ % 4 == 0 && NJ <= kF, "NJ");
+  __shared__ __align__(16) float swT[NJ * kF];  // [j][ci] = Wh[ci][j], 0 for j >= 2 nz
+  __shared__ float red[kHpWarps][NJ + kF];
   const int nout = 2 * nz;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int i = threadIdx.x; i < kF * kF; i += blockDim.x) {
+  for (int i = threadIdx.x; i < NJ * kF; i += blockDim.x) {
     const int j = i / kF, ci = i - (i / kF) * kF;
     swT[i] = j < nout ? wh[ci * nout + j] : 0.f;
   }
   __syncthreads();
-  float accb = 0.f, accd = 0.f;  // dbh[j = lane], db16[ci = lane]
+  float2 accb[NJ / 2], accd[kF / 2];  // this lane's sums of dY (j) and dPre16 (ci), channel pairs
+#pragma unroll
+  for (int q = 0; q < NJ / 2; ++q) accb[q] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int q = 0; q < kF / 2; ++q) accd[q] = make_float2(0.f, 0.f);
   const size_t plane = (size_t)H * W;
   const size_t total = plane * B;
   const size_t nchunks = (total + 31) / 32;
@@ -425,39 +478,17 @@ __global__ void __launch_bounds__(kHpWarps * 32, 2)
   uint4* DP = reinterpret_cast<uint4*>(dpre);
   uint4* DY = reinterpret_cast<uint4*>(dyb);
   for (size_t chunk = (size_t)blockIdx.x * kHpWarps + warp; chunk < nchunks; chunk += nwarps) {
-    const size_t i = chunk * 32 + lane;
-    const bool ok = i < total;
-    int b = 0, y = 0, x = 0;
-    size_t rem = 0;
-    if (ok) {
-      b = (int)(i / plane);
-      rem = i - (size_t)b * plane;
-      y = (int)(rem / W);
-      x = (int)(rem - (size_t)y * W);
-    }
-    uint4 au[4];
-#pragma unroll
-    for (int ch = 0; ch < 4; ++ch) au[ch] = ok ? A[(((size_t)b * H + y) * 4 + ch) * W + x] : make_uint4(0, 0, 0, 0);
-    float g[kF];
-#pragma unroll
-    for (int j = 0; j < kF; ++j) {
-      float v = 0.f;
-      if (ok && j < nout) {
-        const float* src = j < nz ? dU : dV;
-        const int k = j < nz ? j : j - nz;
-        v = src[((size_t)b * nz + k) * plane + rem] * out_scale;
-      }
-      g[j] = v;
-      sG[warp][lane][j] = v;
-    }
+    // keeps the weight reads below inside the loop: hoisted, 32 NJ of them would stay live in registers
+    asm volatile("" ::: "memory");
+    HeadPx<NJ> cur;
+    head_px_load<NJ>(cur, chunk, total, plane, H, W, nz, nout, A, dU, dV, out_scale, lane);
     // dPre = dY Wh^T, two channels per packed fma
     float2 da[kF / 2];
 #pragma unroll
     for (int q = 0; q < kF / 2; ++q) da[q] = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int j = 0; j < kF; ++j) {
-      if (j >= nout) break;
-      const float2 gg = make_float2(g[j], g[j]);
+    for (int j = 0; j < NJ; ++j) {
+      const float2 gg = make_float2(cur.g[j], cur.g[j]);
       const float4* wr = reinterpret_cast<const float4*>(swT + j * kF);
 #pragma unroll
       for (int q = 0; q < kF / 4; ++q) {
@@ -466,54 +497,89 @@ __global__ void __launch_bounds__(kHpWarps * 32, 2)
         da[2 * q + 1] = __ffma2_rn(gg, make_float2(w4.z, w4.w), da[2 * q + 1]);
       }
     }
+#pragma unroll
+    for (int q = 0; q < NJ / 2; ++q) accb[q] = __fadd2_rn(accb[q], make_float2(cur.g[2 * q], cur.g[2 * q + 1]));
     uint4 po[4], yo[4];
 #pragma unroll
     for (int ch = 0; ch < 4; ++ch) {
-      const uint32_t wv[4] = {au[ch].x, au[ch].y, au[ch].z, au[ch].w};
+      const uint32_t wv[4] = {cur.a[ch].x, cur.a[ch].y, cur.a[ch].z, cur.a[ch].w};
       uint32_t pk[4], yk[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int c = ch * 8 + 2 * e;
-        const float lo = da[c >> 1].x * (bf_lo(wv[e]) > 0.f ? 1.f : alpha);
-        const float hi = da[c >> 1].y * (bf_hi(wv[e]) > 0.f ? 1.f : alpha);
-        sP[warp][lane][c] = lo;
-        sP[warp][lane][c + 1] = hi;
-        pk[e] = bf_pack(lo, hi);
-        yk[e] = bf_pack(g[c], g[c + 1]);
+        const float2 m = make_float2(bf_lo(wv[e]) > 0.f ? 1.f : alpha, bf_hi(wv[e]) > 0.f ? 1.f : alpha);
+        const float2 d = __fmul2_rn(da[c >> 1], m);
+        accd[c >> 1] = __fadd2_rn(accd[c >> 1], d);
+        pk[e] = bf_pack(d.x, d.y);
+        yk[e] = c < NJ ? bf_pack(cur.g[c], cur.g[c + 1]) : 0u;
       }
       po[ch] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
       yo[ch] = make_uint4(yk[0], yk[1], yk[2], yk[3]);
     }
-    if (ok) {
+    if (cur.ok) {
 #pragma unroll
       for (int ch = 0; ch < 4; ++ch) {
-        const size_t o = (((size_t)b * H + y) * 4 + ch) * W + x;
-        DP[o] = po[ch];
-        DY[o] = yo[ch];
+        DP[cur.o + (size_t)ch * W] = po[ch];
+        DY[cur.o + (size_t)ch * W] = yo[ch];
       }
     }
-    __syncwarp();
-    for (int p = 0; p < 32; ++p) {
-      accd += sP[warp][p][lane];
-      accb += sG[warp][p][lane];
-    }
-    __syncwarp();  // this warp's staging area is rewritten by its next chunk
   }
-  __syncthreads();
-  float* red = &sP[0][0][0];  // [warp][64]: dbh (32), db16 (32)
-  red[warp * 64 + lane] = accb;
-  red[warp * 64 + 32 + lane] = accd;
+#pragma unroll
+  for (int q = 0; q < NJ / 2; ++q) {
+    const float x0 = warp_sum_fixed(accb[q].x), x1 = warp_sum_fixed(accb[q].y);
+    if (lane == 0) {
+      red[warp][2 * q] = x0;
+      red[warp][2 * q + 1] = x1;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kF / 2; ++q) {
+    const float x0 = warp_sum_fixed(accd[q].x), x1 = warp_sum_fixed(accd[q].y);
+    if (lane == 0) {
+      red[warp][NJ + 2 * q] = x0;
+      red[warp][NJ + 2 * q + 1] = x1;
+    }
+  }
   __syncthreads();
   float* out = partial + (size_t)blockIdx.x * (nout + kF);
-  if (threadIdx.x < 64) {
-    float t = 0.f;
-    for (int w2 = 0; w2 < kHpWarps; ++w2) t += red[w2 * 64 + threadIdx.x];
-    if (threadIdx.x < 32) {
-      if (threadIdx.x < nout) out[threadIdx.x] = t;
-    } else {
-      out[nout + threadIdx.x - 32] = t;
-    }
+  const int t = threadIdx.x;
+  if (t < nout + kF) {
+    const int src = t < nout ? t : NJ + (t - nout);
+    float v = 0.f;
+#pragma unroll
+    for (int w2 = 0; w2 < kHpWarps; ++w2) v += red[w2][src];
+    out[t] = v;
   }
+}
+
+// Sum over the partials p = warp, warp + kFinWarps, ... of the entries (kh + jj,
+// column jj) for jj < JN and input channels ci + sp, sp < NSP, in that order;
+// kRedBatch partials are loaded before they are added (absent ones add +0).
+template <int JN, int NSP>
+__device__ __forceinline__ float finish_sum(const float* part, int n_parts, int warp, int lane, int kw, int kh,
+                                            int ci, int cw) {
+  constexpr int wn = JN * kF;
+  float acc = 0.f;
+  for (int p0 = warp; p0 < n_parts; p0 += kFinWarps * kRedBatch) {
+    float v[kRedBatch][JN][NSP];
+#pragma unroll
+    for (int u = 0; u < kRedBatch; ++u) {
+      const int p = p0 + u * kFinWarps;
+      const float* base = part + ((size_t)(p < n_parts ? p : 0) * 3 + kw) * 128 * wn;
+#pragma unroll
+      for (int jj = 0; jj < JN; ++jj)
+#pragma unroll
+        for (int sp = 0; sp < NSP; ++sp)
+          v[u][jj][sp] = p < n_parts ? base[(size_t)((kh + jj) * cw + ci + sp) * wn + jj * kF + lane] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < kRedBatch; ++u)
+#pragma unroll
+      for (int jj = 0; jj < JN; ++jj)
+#pragma unroll
+        for (int sp = 0; sp < NSP; ++sp) acc += v[u][jj][sp];
+  }
+  return acc;
 }
 
 // head kernel gradient from igm_conv3x3_wgrad partials over (A16, dY): the centre
@@ -522,14 +588,9 @@ __global__ void __launch_bounds__(kFinWarps * 32) head_wgrad_finish_kernel(const
                                                                            float* out) {
   __shared__ float red[kFinWarps][kF];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int cw = 32, jn = 2, wn = jn * kF;
+  constexpr int cw = 32, jn = 2;
   for (int ci = blockIdx.x; ci < kF; ci += gridDim.x) {
-    float acc = 0.f;
-    for (int p = warp; p < n_parts; p += kFinWarps) {
-      const float* base = part + ((size_t)p * 3 + 1) * 128 * wn;
-      for (int jj = 0; jj < jn; ++jj) acc += base[(size_t)((1 + jj) * cw + ci) * wn + jj * kF + lane];
-    }
-    red[warp][lane] = acc;
+    red[warp][lane] = finish_sum<jn, 1>(part, n_parts, warp, lane, 1, 1, ci, cw);
     __syncthreads();
     if (warp == 0) {
       float tsum = 0.f;
@@ -711,21 +772,27 @@ __global__ void __launch_bounds__(kL1Warps * 32, 2) layer1_wgrad_kernel(const L1
 // reductions of per-block partials (fixed order -> deterministic)
 // ---------------------------------------------------------------------------
 // One warp per output element: lane l sums the partials l, l + 32, ... in
-// order, then a fixed xor-shuffle tree adds the 32 lane sums -- the same
-// order on every run.
-__device__ __forceinline__ float warp_sum_fixed(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
+// order, then a fixed xor-shuffle tree (warp_sum_fixed) adds the 32 lane sums
+// -- the same order on every run.
 
+// A lane issues the loads of kRedBatch partials before it adds any of them; the
+// additions keep the order p = lane, lane + 32, ... (absent partials add +0).
 __global__ void reduce_partials_kernel(const float* part, int n_parts, int len, int stride, float* out,
                                        int accumulate) {
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < len; i += nw) {
     float s = 0.f;
-    for (int p = lane; p < n_parts; p += 32) s += part[(size_t)p * stride + i];
+    for (int p0 = lane; p0 < n_parts; p0 += 32 * kRedBatch) {
+      float v[kRedBatch];
+#pragma unroll
+      for (int u = 0; u < kRedBatch; ++u) {
+        const int p = p0 + 32 * u;
+        v[u] = p < n_parts ? part[(size_t)p * stride + i] : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < kRedBatch; ++u) s += v[u];
+    }
     s = warp_sum_fixed(s);
     if (lane == 0) out[i] = accumulate ? out[i] + s : s;
   }
@@ -743,18 +810,12 @@ __global__ void __launch_bounds__(kFinWarps * 32) wgrad_finish_kernel(const floa
                                                                       int cw, float* out) {
   __shared__ float red[kFinWarps][kF];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int jn = cw == 32 ? 2 : 4;
-  const int wn = jn * kF;
   const int groups = 9 * cin;
   for (int gi = blockIdx.x; gi < groups; gi += gridDim.x) {
     const int ci = gi % cin, tap = gi / cin;
     const int kh = tap / 3, kw = tap % 3;
-    float acc = 0.f;
-    for (int p = warp; p < n_parts; p += kFinWarps) {
-      const float* base = part + ((size_t)p * 3 + kw) * 128 * wn;
-      for (int jj = 0; jj < jn; ++jj) acc += base[(size_t)((kh + jj) * cw + ci) * wn + jj * kF + lane];
-    }
-    red[warp][lane] = acc;
+    red[warp][lane] = cw == 32 ? finish_sum<2, 1>(part, n_parts, warp, lane, kw, kh, ci, cw)
+                               : finish_sum<4, 1>(part, n_parts, warp, lane, kw, kh, ci, cw);
     __syncthreads();
     if (warp == 0) {
       float tsum = 0.f;
@@ -773,18 +834,12 @@ __global__ void __launch_bounds__(kFinWarps * 32) wgrad_finish_split_kernel(cons
                                                                             float* out) {
   __shared__ float red[kFinWarps][kF];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int cw = 16, jn = 4, wn = jn * kF;  // the 16-channel input tensor's partial layout
+  constexpr int cw = 16, jn = 4;  // the 16-channel input tensor's partial layout
   const int groups = 9 * cin;
   for (int gi = blockIdx.x; gi < groups; gi += gridDim.x) {
     const int c = gi % cin, tap = gi / cin;
     const int kh = tap / 3, kw = tap % 3;
-    float acc = 0.f;
-    for (int p = warp; p < n_parts; p += kFinWarps) {
-      const float* base = part + ((size_t)p * 3 + kw) * 128 * wn;
-      for (int jj = 0; jj < jn; ++jj)
-        for (int sp = 0; sp < 2; ++sp) acc += base[(size_t)((kh + jj) * cw + 3 * c + sp) * wn + jj * kF + lane];
-    }
-    red[warp][lane] = acc;
+    red[warp][lane] = finish_sum<jn, 2>(part, n_parts, warp, lane, kw, kh, 3 * c, cw);
     __syncthreads();
     if (warp == 0) {
       float tsum = 0.f;
@@ -1006,19 +1061,21 @@ extern "C" int igm_cnn_head_backward_tc(int batch, int h, int w, int nz, const v
                 "igm_cnn_head_backward_tc: bad shape (needs 2 nz <= 32)");
   IGM_CHECK_ARG(act && head_w && dU && dV && dpre && dy_bf16 && partials, IGM_ERR_BAD_ARGUMENT,
                 "igm_cnn_head_backward_tc: NULL argument");
-  constexpr size_t smem = (size_t)(kF * kF + 2 * kHpWarps * 32 * 33) * sizeof(float);
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(head_bwd_px_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) {
-      set_error("head_bwd_px smem attribute: %s", cudaGetErrorString(e));
-      return IGM_ERR_CUDA;
-    }
-    configured = true;
+  cudaStream_t st = as_stream(stream);
+  const __nv_bfloat16* a16 = (const __nv_bfloat16*)act;
+  __nv_bfloat16 *dp = (__nv_bfloat16*)dpre, *dy = (__nv_bfloat16*)dy_bf16;
+  switch ((2 * nz + 3) / 4) {
+#define IGM_HEAD_PX(Q)                                                                                              \
+  case Q:                                                                                                           \
+    head_bwd_px_kernel<4 * Q><<<n_parts, kHpWarps * 32, 0, st>>>(batch, h, w, nz, a16, head_w, dU, dV, out_scale,  \
+                                                                 alpha, dp, dy, partials);                          \
+    break;
+    IGM_HEAD_PX(1) IGM_HEAD_PX(2) IGM_HEAD_PX(3) IGM_HEAD_PX(4) IGM_HEAD_PX(5) IGM_HEAD_PX(6) IGM_HEAD_PX(7)
+    IGM_HEAD_PX(8)
+#undef IGM_HEAD_PX
+    default:
+      return IGM_ERR_BAD_SHAPE;
   }
-  head_bwd_px_kernel<<<n_parts, kHpWarps * 32, smem, as_stream(stream)>>>(
-      batch, h, w, nz, (const __nv_bfloat16*)act, head_w, dU, dV, out_scale, alpha, (__nv_bfloat16*)dpre,
-      (__nv_bfloat16*)dy_bf16, partials);
   return launch_status("head_bwd_px_kernel");
 }
 
