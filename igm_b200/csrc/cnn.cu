@@ -177,6 +177,7 @@ template <int NJ>
 __global__ void __launch_bounds__(256) head_fwd_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act,
                                                        const float* wh, const float* bh, float out_scale, float* U,
                                                        float* V, const float* thk_mask) {
+  static_assert(NJ % 4 == 0, "NJ");
   __shared__ __align__(16) float sw[kF * NJ + NJ];  // [32][NJ] then bias [NJ]
   const int nout = 2 * nz;
   for (int i = threadIdx.x; i < kF * NJ; i += blockDim.x) {
@@ -189,36 +190,37 @@ __global__ void __launch_bounds__(256) head_fwd_kernel(int B, int H, int W, int 
   const size_t total = plane * B;
   const uint4* A = reinterpret_cast<const uint4*>(act);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const int b = (int)(i / plane);
-    const size_t rem = i - (size_t)b * plane;
-    const int y = (int)(rem / W), x = (int)(rem - (size_t)y * W);
-    float av[kF];
+    // keeps the weight reads inside the loop: hoisted, they would stay live in registers
+    asm volatile("" ::: "memory");
+    const size_t b = i / plane;
+    const size_t rem = i - b * plane;
+    const size_t y = rem / W, x = rem - y * W;
+    // every load of the pixel (activation and ice mask) is issued before the arithmetic
+    uint4 u[4];
 #pragma unroll
-    for (int ch = 0; ch < 4; ++ch) {
-      const uint4 u = A[(((size_t)b * H + y) * 4 + ch) * W + x];
-      const uint32_t wv[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        av[ch * 8 + 2 * e] = bf_lo(wv[e]);
-        av[ch * 8 + 2 * e + 1] = bf_hi(wv[e]);
-      }
-    }
+    for (int ch = 0; ch < 4; ++ch) u[ch] = A[((b * H + y) * 4 + ch) * W + x];
+    const float mk = thk_mask != nullptr ? thk_mask[i] : 1.f;
     float2 acc[NJ / 2];
 #pragma unroll
     for (int q = 0; q < NJ / 2; ++q) acc[q] = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int ci = 0; ci < kF; ++ci) {
-      const float2 aa = make_float2(av[ci], av[ci]);
-      const float4* wr = reinterpret_cast<const float4*>(sw + ci * NJ);
+    for (int ch = 0; ch < 4; ++ch) {
+      const uint32_t wv[4] = {u[ch].x, u[ch].y, u[ch].z, u[ch].w};
 #pragma unroll
-      for (int q = 0; q < NJ / 4; ++q) {
-        if (4 * q >= nout) break;
-        const float4 w4 = wr[q];
-        acc[2 * q] = __ffma2_rn(aa, make_float2(w4.x, w4.y), acc[2 * q]);
-        acc[2 * q + 1] = __ffma2_rn(aa, make_float2(w4.z, w4.w), acc[2 * q + 1]);
+      for (int e = 0; e < 8; ++e) {
+        const int ci = ch * 8 + e;
+        const float av = (e & 1) ? bf_hi(wv[e >> 1]) : bf_lo(wv[e >> 1]);
+        const float2 aa = make_float2(av, av);
+        const float4* wr = reinterpret_cast<const float4*>(sw + ci * NJ);
+#pragma unroll
+        for (int q = 0; q < NJ / 4; ++q) {
+          const float4 w4 = wr[q];
+          acc[2 * q] = __ffma2_rn(aa, make_float2(w4.x, w4.y), acc[2 * q]);
+          acc[2 * q + 1] = __ffma2_rn(aa, make_float2(w4.z, w4.w), acc[2 * q + 1]);
+        }
       }
     }
-    const bool keep = thk_mask == nullptr || thk_mask[i] > 0.f;
+    const bool keep = mk > 0.f;
 #pragma unroll
     for (int j = 0; j < NJ; ++j) {
       if (j >= nout) break;
@@ -227,7 +229,7 @@ __global__ void __launch_bounds__(256) head_fwd_kernel(int B, int H, int W, int 
       if (!keep) sv = 0.f;
       float* dst = j < nz ? U : V;
       const int k = j < nz ? j : j - nz;
-      dst[((size_t)b * nz + k) * plane + rem] = sv;
+      dst[(b * nz + k) * plane + rem] = sv;
     }
   }
 }
@@ -1007,9 +1009,19 @@ extern "C" int igm_cnn_head_forward(int batch, int h, int w, int nz, const void*
   const int grid = grid_for((size_t)batch * h * w);
   cudaStream_t st = as_stream(stream);
   const __nv_bfloat16* A = (const __nv_bfloat16*)act;
-  if (nout <= 32)
-    head_fwd_kernel<32><<<grid, 256, 0, st>>>(batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask);
-  else if (nout <= 64)
+  if (nout <= 32) {
+    switch ((nout + 3) / 4) {
+#define IGM_HEAD_FWD(Q)                                                                                      \
+  case Q:                                                                                                    \
+    head_fwd_kernel<4 * Q><<<grid, 256, 0, st>>>(batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask); \
+    break;
+      IGM_HEAD_FWD(1) IGM_HEAD_FWD(2) IGM_HEAD_FWD(3) IGM_HEAD_FWD(4) IGM_HEAD_FWD(5) IGM_HEAD_FWD(6)
+      IGM_HEAD_FWD(7) IGM_HEAD_FWD(8)
+#undef IGM_HEAD_FWD
+      default:
+        return IGM_ERR_BAD_SHAPE;
+    }
+  } else if (nout <= 64)
     head_fwd_kernel<64><<<grid, 256, 0, st>>>(batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask);
   else
     head_fwd_kernel<128><<<grid, 256, 0, st>>>(batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask);
