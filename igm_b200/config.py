@@ -4,7 +4,7 @@ The processes read ``cfg.processes.<name>.<key>`` by attribute access, so an
 OmegaConf DictConfig composed by the reference's Hydra setup works as is;
 ``default_cfg()`` builds an equivalent plain object for callers without
 Hydra.  Keys and defaults follow igm/conf/processes/iceflow.yaml,
-thk.yaml, time.yaml and smb_simple.yaml.  Keys this implementation adds are
+thk.yaml, time.yaml, smb_simple.yaml and vert_flow.yaml.  Keys this implementation adds are
 marked "(igm_b200)".
 """
 
@@ -87,6 +87,7 @@ DEFAULTS = {
         "fallback": {"every": 0, "margin": 0.02, "nbitmax": 100},
     },
     "thk": {"slope_type": "superbee", "ratio_density": 0.910, "default_sealevel": 0.0},
+    "vert_flow": {"version": 2, "method": "kinematic"},
     "time": {"start": 2000.0, "end": 2100.0, "save": 10.0, "cfl": 0.3, "step_max": 1.0},
     "smb_simple": {"update_freq": 1.0, "file": "param.txt", "array": []},
 }

@@ -220,6 +220,134 @@ __global__ void __launch_bounds__(kTrX* kTrY) transport_kernel(const TransportAr
   if (a.divflux) a.divflux[o] = div;
 }
 
+// Row-marching variant: a warp owns a strip of 30 columns (lanes 1..30; lanes 0
+// and 31 carry the columns on either side) and walks down a segment of rows.
+// x neighbours come from the adjacent lanes by shuffles; in y the thread keeps
+// a window of its column (thickness of rows j-1 .. j+2, the slope of cell j and
+// the flux through the face below node j), so every slope and face flux of the
+// interior is evaluated once.  The loads of a row are issued two rows ahead.
+// Each quantity is evaluated with the operations and order of the reference
+// (as transport_kernel), so the result is bit-identical to it.
+constexpr int kTmCols = 30;  // interior columns per warp
+constexpr int kTmWarps = 4;  // warps per CTA
+
+template <typename T, int SLOPE>
+__device__ __forceinline__ T cell_slope(T hm, T h0, T hp, T dx, T rdx) {
+  if (SLOPE == IGM_GODUNOV) return T(0);
+  const T sigp = div_dx(hp - h0, dx, rdx), sigm = div_dx(h0 - hm, dx, rdx);
+  if (SLOPE == IGM_MINMOD) return minmod(sigm, sigp);
+  return maxmod(minmod(sigp, T(2) * sigm), minmod(sigm, T(2) * sigp));
+}
+
+// upwind flux through a face with velocity uf between cells (hl, sl) and (hr, sr)
+template <typename T>
+__device__ __forceinline__ T face_flux(T uf, T hl, T hr, T sl, T sr, T dt, T dx, T rdx, T half_dx) {
+  const T cu = div_dx(uf * dt, dx, rdx);
+  const T w = hl + half_dx * (T(1) - cu) * sl;
+  const T e = hr - half_dx * (T(1) + cu) * sr;
+  return uf * (uf > T(0) ? w : e);
+}
+
+template <typename T>
+struct MarchRow {
+  T h2;  // thickness two rows below (j + 2)
+  T v1;  // vbar one row below (j + 1)
+  T u, tg, sm;
+  T he;  // edge lanes: thickness of the column beyond the strip, row j
+};
+
+template <typename T, int SLOPE>
+__global__ void __launch_bounds__(kTmWarps * 32) transport_march_kernel(const TransportArgs<T> a, int n_strips,
+                                                                       int rows_per_seg) {
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * kTmWarps + (threadIdx.x >> 5);
+  const int strip = gw % n_strips, seg = gw / n_strips;
+  const int nx = a.nx, ny = a.ny;
+  const int y0 = seg * rows_per_seg;
+  if (y0 >= ny) return;  // uniform per warp
+  const int y1 = min(y0 + rows_per_seg, ny);
+  const int i = strip * kTmCols - 1 + lane;  // this lane's column
+  const bool col = i >= 0 && i < nx;
+  const size_t ic = col ? (size_t)i : 0;
+  const int ie = lane == 0 ? i - 1 : i + 1;  // the extra column of the edge lanes
+  const bool ecol = (lane == 0 || lane == 31) && ie >= 0 && ie < nx;
+  const size_t iec = ecol ? (size_t)ie : 0;
+  const bool out_lane = lane >= 1 && lane <= kTmCols && col;
+  const T dt = a.dt_dev ? (T)(*a.dt_dev) : a.dt_host;
+  const T dx = a.dx, rdx = a.rdx, hdx = a.half_dx;
+  const T* H = a.h;
+  auto at = [&](const T* p, int j, bool ok, size_t c) -> T {
+    return (ok && j >= 0 && j < ny) ? p[(size_t)j * nx + c] : T(0);
+  };
+  auto load_row = [&](int j) {
+    MarchRow<T> r;
+    const bool live = j < y1;
+    r.h2 = at(H, j + 2, live && col, ic);
+    r.v1 = at(a.v, j + 1, live && col, ic);
+    r.u = at(a.u, j, live && col, ic);
+    r.tg = at(a.topg, j, live && col, ic);
+    r.sm = a.smb ? at(a.smb, j, live && col, ic) : T(0);
+    r.he = at(H, j, live && ecol, iec);
+    return r;
+  };
+  // prologue: the y slopes of cells y0-1 and y0 and the flux through face y0
+  T hm1 = at(H, y0 - 1, col, ic), h0 = at(H, y0, col, ic), hp1 = at(H, y0 + 1, col, ic);
+  T v0 = at(a.v, y0, col, ic);
+  T sy0, qs;
+  {
+    const T hm2 = at(H, y0 - 2, col, ic);
+    const T vm1 = at(a.v, y0 - 1, col, ic);
+    const T sym1 = cell_slope<T, SLOPE>(hm2, hm1, h0, dx, rdx);
+    sy0 = cell_slope<T, SLOPE>(hm1, h0, hp1, dx, rdx);
+    const T vf = y0 == 0 ? v0 : T(0.5) * (vm1 + v0);
+    qs = face_flux(vf, hm1, h0, sym1, sy0, dt, dx, rdx, hdx);
+  }
+  auto step = [&](int j, const MarchRow<T>& r) {
+    // y: slope of cell j+1, flux through face j+1 (between rows j and j+1)
+    const T sy1 = cell_slope<T, SLOPE>(h0, hp1, r.h2, dx, rdx);
+    const T vf = j + 1 == ny ? v0 : T(0.5) * (v0 + r.v1);
+    const T qn = face_flux(vf, h0, hp1, sy0, sy1, dt, dx, rdx, hdx);
+    // x: slope of this lane's cell, flux through its left face (face i)
+    T hl = __shfl_up_sync(0xffffffffu, h0, 1), hr = __shfl_down_sync(0xffffffffu, h0, 1);
+    if (lane == 0) hl = r.he;
+    if (lane == 31) hr = r.he;
+    const T sx = cell_slope<T, SLOPE>(hl, h0, hr, dx, rdx);
+    const T sxl = __shfl_up_sync(0xffffffffu, sx, 1);
+    const T ul = __shfl_up_sync(0xffffffffu, r.u, 1);
+    const T uf = i == 0 ? r.u : (i == nx ? ul : T(0.5) * (ul + r.u));
+    const T qw = face_flux(uf, hl, h0, sxl, sx, dt, dx, rdx, hdx);
+    const T qe = __shfl_down_sync(0xffffffffu, qw, 1);
+    if (out_lane) {
+      const T div = div_dx(qe - qw, dx, rdx) + div_dx(qn - qs, dx, rdx);
+      T hn = h0 + dt * (r.sm - div);
+      hn = hn > T(0) ? hn : T(0);
+      const T fl = -a.ratio * hn + a.sealevel;
+      const T ls = r.tg > fl ? r.tg : fl;
+      const size_t o = (size_t)j * nx + ic;
+      a.h_out[o] = hn;
+      a.usurf[o] = ls + hn;
+      if (a.lsurf) a.lsurf[o] = ls;
+      if (a.divflux) a.divflux[o] = div;
+    }
+    hm1 = h0;
+    h0 = hp1;
+    hp1 = r.h2;
+    v0 = r.v1;
+    sy0 = sy1;
+    qs = qn;
+  };
+  MarchRow<T> r0 = load_row(y0), r1 = load_row(y0 + 1);
+  for (int j = y0; j < y1; j += 2) {
+    const MarchRow<T> r2 = load_row(j + 2);
+    step(j, r0);
+    const MarchRow<T> r3 = load_row(j + 3);
+    if (j + 1 < y1) step(j + 1, r1);
+    r0 = r2;
+    r1 = r3;
+  }
+  (void)hm1;
+}
+
 template <typename T>
 __global__ void surfaces_kernel(int n, const T* thk, const T* topg, T* lsurf, T* usurf, T ratio, T sealevel) {
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
@@ -299,9 +427,174 @@ static int transport_t(int ny, int nx, double dx, const void* u, const void* v, 
   a.dt_dev = dt_dev;
   a.u = (const T*)u; a.v = (const T*)v; a.h = (const T*)h; a.h_out = (T*)h_out; a.topg = (const T*)topg;
   a.smb = (const T*)smb; a.usurf = (T*)usurf; a.lsurf = (T*)lsurf; a.divflux = (T*)divflux;
-  dim3 blk(kTrX, kTrY), grd((nx + kTrX - 1) / kTrX, (ny + kTrY - 1) / kTrY);
-  transport_kernel<T><<<grd, blk, 0, st>>>(a);
-  return launch_status("transport_kernel");
+  // segments of rows sized for about 32 resident warps per SM, at least 8 rows
+  const int n_strips = (nx + kTmCols - 1) / kTmCols;
+  const long long target = 148LL * 32;
+  int rows = (int)((n_strips * (long long)ny + target - 1) / target);
+  rows = rows < 8 ? 8 : rows;
+  rows += rows & 1;
+  const long long warps = (long long)n_strips * ((ny + rows - 1) / rows);
+  const int grid = (int)((warps + kTmWarps - 1) / kTmWarps);
+  if (slope == IGM_GODUNOV)
+    transport_march_kernel<T, IGM_GODUNOV><<<grid, kTmWarps * 32, 0, st>>>(a, n_strips, rows);
+  else if (slope == IGM_MINMOD)
+    transport_march_kernel<T, IGM_MINMOD><<<grid, kTmWarps * 32, 0, st>>>(a, n_strips, rows);
+  else
+    transport_march_kernel<T, IGM_SUPERBEE><<<grid, kTmWarps * 32, 0, st>>>(a, n_strips, rows);
+  return launch_status("transport_march_kernel");
+}
+
+// ---------------------------------------------------------------------------
+// vertical velocity, vert_flow version 2, kinematic method
+// (vert_flow/vert_flow_v2.py:17-37, 62-87, 126-147; vert_disc.py:17-23)
+// ---------------------------------------------------------------------------
+template <typename T>
+struct VertFlowArgs {
+  int nz, ny, nx;
+  T dx, rdx;               // rdx = RN(1/dx) in T
+  T lev[IGM_MAX_NZ];       // levels (zeta map of compute_levels)
+  T w[IGM_MAX_NZ];         // vert_weight
+  const T* U;
+  const T* V;
+  const T* topg;
+  const T* thk;
+  T* W;
+};
+
+template <typename T>
+__device__ __forceinline__ T ieee_div(T a, T b);
+template <>
+__device__ __forceinline__ float ieee_div<float>(float a, float b) { return __fdiv_rn(a, b); }
+template <>
+__device__ __forceinline__ double ieee_div<double>(double a, double b) { return __ddiv_rn(a, b); }
+
+// A CTA owns a 32 x 8 tile of nodes and walks the layers from the bed up (the
+// loads of the next layer are issued before the arithmetic of the current
+// one).  Each thread carries the running sums of its node(s) of the tile plus
+// a one-node halo: the layer height z_k - topg (the scan of thk (level[l+1] - level[l])),
+// the weighted sums of U and V and of the weights.  Per layer it publishes the
+// layer surface topg + z_k, the node's U, V and the fluxes (mean U) z_k,
+// (mean V) z_k to shared memory (two buffers, one barrier per layer); the
+// tile's threads then form the centred slopes and divergence with the border
+// forms of the reference and W = -div + U sx + V sy.  Operation order and
+// rounding follow the reference (no contraction: this unit is built with
+// -fmad=false; quotients are correctly rounded), so W is bit-identical.
+constexpr int kVfX = 32, kVfY = 8;
+template <typename T>
+__global__ void __launch_bounds__(kVfX* kVfY) vert_flow_kernel(const VertFlowArgs<T> a) {
+  constexpr int HX = kVfX + 2, HY = kVfY + 2, NH = HX * HY, NT = kVfX * kVfY;
+  constexpr int OWN = (NH + NT - 1) / NT;  // halo-tile nodes per thread
+  __shared__ T s_z[2][HY][HX];   // layer surface topg + z_k
+  __shared__ T s_qx[2][HY][HX];  // (mean U) z_k
+  __shared__ T s_qy[2][HY][HX];  // (mean V) z_k
+  __shared__ T s_u[2][kVfY][kVfX];
+  __shared__ T s_v[2][kVfY][kVfX];
+  const int nx = a.nx, ny = a.ny;
+  const size_t plane = (size_t)ny * nx;
+  const int i0 = blockIdx.x * kVfX, j0 = blockIdx.y * kVfY;
+  const int tid = threadIdx.y * kVfX + threadIdx.x;
+  // the halo-tile nodes this thread carries
+  size_t off[OWN];
+  bool in[OWN], inner[OWN];
+  int hr[OWN], hc[OWN];
+  T tg[OWN], th[OWN], zh[OWN], su[OWN], sv[OWN];
+#pragma unroll
+  for (int q = 0; q < OWN; ++q) {
+    const int c = tid + q * NT;
+    hr[q] = c / HX;
+    hc[q] = c - hr[q] * HX;
+    const int jj = j0 - 1 + hr[q], ii = i0 - 1 + hc[q];
+    in[q] = c < NH && jj >= 0 && jj < ny && ii >= 0 && ii < nx;
+    inner[q] = c < NH && hr[q] >= 1 && hr[q] <= kVfY && hc[q] >= 1 && hc[q] <= kVfX;
+    off[q] = in[q] ? (size_t)jj * nx + ii : 0;
+    tg[q] = in[q] ? a.topg[off[q]] : T(0);
+    th[q] = in[q] ? a.thk[off[q]] : T(0);
+    zh[q] = T(0);
+    su[q] = T(0);
+    sv[q] = T(0);
+  }
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool node = i < nx && j < ny;
+  const T dx = a.dx, rdx = a.rdx;
+  T sw = T(0);
+  // U, V of the carried nodes, one layer ahead of the arithmetic
+  T un[OWN], vn[OWN];
+#pragma unroll
+  for (int q = 0; q < OWN; ++q) {
+    un[q] = in[q] ? a.U[off[q]] : T(0);
+    vn[q] = in[q] ? a.V[off[q]] : T(0);
+  }
+  for (int k = 0; k < a.nz; ++k) {
+    const int bsel = k & 1;
+    sw = k == 0 ? a.w[0] : sw + a.w[k];
+    T uc[OWN], vc[OWN];
+#pragma unroll
+    for (int q = 0; q < OWN; ++q) {
+      uc[q] = un[q];
+      vc[q] = vn[q];
+      const bool nxt = in[q] && k + 1 < a.nz;
+      un[q] = nxt ? a.U[(size_t)(k + 1) * plane + off[q]] : T(0);
+      vn[q] = nxt ? a.V[(size_t)(k + 1) * plane + off[q]] : T(0);
+    }
+#pragma unroll
+    for (int q = 0; q < OWN; ++q) {
+      if (tid + q * NT >= NH) break;
+      const T u = uc[q];
+      const T v = vc[q];
+      if (k > 0) {
+        const T dzl = th[q] * (a.lev[k] - a.lev[k - 1]);
+        zh[q] = k == 1 ? dzl : zh[q] + dzl;
+      }
+      const T wu = a.w[k] * u, wv = a.w[k] * v;
+      su[q] = k == 0 ? wu : su[q] + wu;
+      sv[q] = k == 0 ? wv : sv[q] + wv;
+      s_z[bsel][hr[q]][hc[q]] = tg[q] + zh[q];
+      s_qx[bsel][hr[q]][hc[q]] = ieee_div(su[q], sw) * zh[q];
+      s_qy[bsel][hr[q]][hc[q]] = ieee_div(sv[q], sw) * zh[q];
+      if (inner[q]) {
+        s_u[bsel][hr[q] - 1][hc[q] - 1] = u;
+        s_v[bsel][hr[q] - 1][hc[q] - 1] = v;
+      }
+    }
+    __syncthreads();
+    if (node) {
+      const int r = ty + 1, c = tx + 1;
+      const T(*z)[HX] = s_z[bsel];
+      const T(*qx)[HX] = s_qx[bsel];
+      const T(*qy)[HX] = s_qy[bsel];
+      // faces of the layer surface (compute_gradient_layers_tf)
+      const T zw = i == 0 ? T(1.5) * z[r][c] - T(0.5) * z[r][c + 1] : T(0.5) * z[r][c - 1] + T(0.5) * z[r][c];
+      const T ze = i == nx - 1 ? T(1.5) * z[r][c] - T(0.5) * z[r][c - 1] : T(0.5) * z[r][c] + T(0.5) * z[r][c + 1];
+      const T zs = j == 0 ? T(1.5) * z[r][c] - T(0.5) * z[r + 1][c] : T(0.5) * z[r - 1][c] + T(0.5) * z[r][c];
+      const T zn = j == ny - 1 ? T(1.5) * z[r][c] - T(0.5) * z[r - 1][c] : T(0.5) * z[r][c] + T(0.5) * z[r + 1][c];
+      // faces of the fluxes (compute_divflux_layers)
+      const T fw = i == 0 ? qx[r][c] : T(0.5) * (qx[r][c - 1] + qx[r][c]);
+      const T fe = i == nx - 1 ? qx[r][c] : T(0.5) * (qx[r][c] + qx[r][c + 1]);
+      const T fs = j == 0 ? qy[r][c] : T(0.5) * (qy[r - 1][c] + qy[r][c]);
+      const T fn = j == ny - 1 ? qy[r][c] : T(0.5) * (qy[r][c] + qy[r + 1][c]);
+      const T sx = div_dx(ze - zw, dx, rdx), sy = div_dx(zn - zs, dx, rdx);
+      const T div = div_dx(fe - fw, dx, rdx) + div_dx(fn - fs, dx, rdx);
+      a.W[(size_t)k * plane + (size_t)j * nx + i] = (-div + s_u[bsel][ty][tx] * sx) + s_v[bsel][ty][tx] * sy;
+    }
+  }
+}
+
+template <typename T>
+static int vert_flow_t(int nz, int ny, int nx, double dx, const void* U, const void* V, const void* topg,
+                       const void* thk, const double* levels, const double* vert_weight, void* W, cudaStream_t st) {
+  VertFlowArgs<T> a{};
+  a.nz = nz; a.ny = ny; a.nx = nx;
+  a.dx = (T)dx;
+  a.rdx = T(1) / a.dx;
+  for (int k = 0; k < nz; ++k) {
+    a.lev[k] = (T)levels[k];
+    a.w[k] = (T)vert_weight[k];
+  }
+  a.U = (const T*)U; a.V = (const T*)V; a.topg = (const T*)topg; a.thk = (const T*)thk; a.W = (T*)W;
+  dim3 blk(kVfX, kVfY), grd((nx + kVfX - 1) / kVfX, (ny + kVfY - 1) / kVfY);
+  vert_flow_kernel<T><<<grd, blk, 0, st>>>(a);
+  return launch_status("vert_flow_kernel");
 }
 
 }  // namespace igm
@@ -408,4 +701,19 @@ extern "C" int igm_absmax2(int dtype, int n, const void* a, const void* b, float
     return IGM_ERR_BAD_ARGUMENT;
   }
   return launch_status("absmax2_kernel");
+}
+
+extern "C" int igm_vertical_velocity(int dtype, int nz, int ny, int nx, double dx, const void* U, const void* V,
+                                     const void* topg, const void* thk, const double* levels,
+                                     const double* vert_weight, void* W, void* stream) {
+  IGM_CHECK_ARG(nz >= 2 && nz <= IGM_MAX_NZ && ny >= 2 && nx >= 2, IGM_ERR_BAD_SHAPE,
+                "igm_vertical_velocity: bad shape %dx%dx%d (needs nz, ny, nx >= 2)", nz, ny, nx);
+  IGM_CHECK_ARG(U && V && topg && thk && levels && vert_weight && W, IGM_ERR_BAD_ARGUMENT,
+                "igm_vertical_velocity: NULL argument");
+  IGM_CHECK_ARG(dx > 0, IGM_ERR_BAD_ARGUMENT, "igm_vertical_velocity: dx must be positive");
+  cudaStream_t st = as_stream(stream);
+  if (dtype == IGM_F32) return vert_flow_t<float>(nz, ny, nx, dx, U, V, topg, thk, levels, vert_weight, W, st);
+  if (dtype == IGM_F64) return vert_flow_t<double>(nz, ny, nx, dx, U, V, topg, thk, levels, vert_weight, W, st);
+  set_error("igm_vertical_velocity: unknown dtype %d", dtype);
+  return IGM_ERR_BAD_ARGUMENT;
 }

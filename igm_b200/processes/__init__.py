@@ -5,4 +5,4 @@ reference's by exposing it as ``iceflow.py`` / ``thk.py`` in the experiment
 folder, which the reference's loader imports before its built-ins
 (igm/common/runner/modules/loader.py:129-176)."""
 
-from . import iceflow, smb_simple, thk, time  # noqa: F401
+from . import iceflow, smb_simple, thk, time, vert_flow  # noqa: F401

@@ -1,9 +1,9 @@
 """One launch of each hot kernel on a case larger than L2, for profiling
 (``python -m igm_b200.prof_cases``; run it under ncu with -k and -c).
 
-Stencil (energy, energy + adjoint, one fused Adam iteration) and transport at
-1500 x 1500 x Nz 10 in FP32; the tensor-core convolution (forward, dgrad,
-wgrad) at batch 2 x 1000 x 1000 x 32 channels.
+Stencil (energy, energy + adjoint, one fused Adam iteration), transport and
+the vertical velocity at 1500 x 1500 x Nz 10 in FP32; the tensor-core
+convolution (forward, dgrad, wgrad) at batch 2 x 1000 x 1000 x 32 channels.
 """
 
 from __future__ import annotations
@@ -15,7 +15,7 @@ from . import _lib as L
 from . import kernels as K
 from .solver import DeviceAdamSolver
 from .synthetic import valley_glacier
-from .vertical import compute_levels, compute_zeta_dzeta
+from .vertical import compute_levels, compute_zeta_dzeta, define_vertical_weight
 
 
 def main():
@@ -31,6 +31,8 @@ def main():
     DeviceAdamSolver().solve(U, V, *f, 50.0, dz, nbitmax=1, early_stopping=False, mask=False)  # fused Adam step
     ub, vb = U[0].contiguous(), V[0].contiguous()
     K.transport_step(ub, vb, f[0], f[1], None, 50.0, 0.01)       # transport
+    topg = torch.as_tensor(st["topg"]).cuda()
+    K.vertical_velocity(U, V, topg, f[0], compute_levels(nz, 4.0), define_vertical_weight(nz, 4.0), 50.0)  # vert_flow
     B, H, W = 2, 1000, 1000                                       # 2 x 64 MB activations (> L2)
     x = torch.randn(B, H, 4, W, 8, device="cuda").to(torch.bfloat16)
     y = torch.empty_like(x)

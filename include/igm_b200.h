@@ -226,6 +226,25 @@ IGM_API int igm_transport_step(int dtype, int ny, int nx, double dx, const void*
                        void* lsurf_out, void* divflux_out, double dt, const float* dt_device, int slope_type,
                        double ratio_density, double sealevel, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Vertical velocity, vert_flow version 2, kinematic method (the vert_flow
+ * process's default): replaces compute_vertical_velocity_kinematic_v2 /
+ * compute_w_kinematic_tf (igm/processes/vert_flow/vert_flow_v2.py:17-37,
+ * with compute_gradient_layers_tf :62-87, compute_divflux_layers :126-147 and
+ * compute_dz, igm/processes/iceflow/vert_disc.py:17-23).  For each layer k,
+ * z_k = sum_{l<k} thk (levels[l+1] - levels[l]), the layer surface topg + z_k,
+ * its centred slopes (sx, sy) with extrapolated border faces, the running
+ * weighted means ub_k = sum_{l<=k} w_l U_l / sum_{l<=k} w_l (and vb_k), and
+ *   W_k = -(d(ub_k z_k)/dx + d(vb_k z_k)/dy) + U_k sx + V_k sy.
+ * U, V, W: [nz][ny][nx]; topg, thk: [ny][nx]; levels, vert_weight: host
+ * double[nz] (compute_levels and define_vertical_weight, vert_disc.py:10-13,
+ * 43-47).  nz, ny, nx >= 2.  wvelbase and wvelsurf of the process are W_0 and
+ * W_{nz-1} (vert_flow.py:55-56).  Bit-identical to the reference in FP32/FP64.
+ * ------------------------------------------------------------------------- */
+IGM_API int igm_vertical_velocity(int dtype, int nz, int ny, int nx, double dx, const void* U, const void* V,
+                          const void* topg, const void* thk, const double* levels, const double* vert_weight,
+                          void* W, void* stream);
+
 /* Surfaces from thickness (thk.py:11-24): lsurf = max(topg, -r thk + sealevel),
  * usurf = lsurf + thk.  lsurf may be NULL. */
 IGM_API int igm_thk_surfaces(int dtype, int n, const void* thk, const void* topg, void* lsurf, void* usurf,

@@ -16,6 +16,9 @@ TensorFlow code for the path (all paths relative to the reference project):
   - the per-term ``reduce_mean`` + ``add_n`` of ``igm/processes/iceflow/solve/solve.py:57-59``
 * vertical discretisation ``igm/processes/iceflow/vert_disc.py:10-47``
 * velbase / velsurf / velbar ``igm/processes/iceflow/utils.py:21-51``
+* vertical velocity, vert_flow version 2, kinematic method
+  ``igm/processes/vert_flow/vert_flow_v2.py:17-37,62-87,126-147`` with
+  ``compute_dz`` of ``igm/processes/iceflow/vert_disc.py:17-23``
 * EarlyStopping ``igm/processes/iceflow/utils.py:80-110``
 * the plain solver loop ``igm/processes/iceflow/solve/solve.py:22-119``
 * Keras legacy Adam (TF 2.15.1, third party, not vendored): the published
@@ -359,6 +362,63 @@ def get_velsurf(U, V):
 
 def get_velbar(U, V, vert_weight):
     return torch.sum(U * vert_weight, dim=-3), torch.sum(V * vert_weight, dim=-3)
+
+
+# --------------------------------------------------------------------------
+# vertical velocity (vert_flow, version 2, kinematic method)
+# --------------------------------------------------------------------------
+
+
+def cumsum0(x):
+    """``tf.cumsum(x, axis=0)``: an inclusive scan accumulated in the tensor's
+    own dtype, level after level (``torch.cumsum`` on CPU accumulates float32
+    in double, which rounds differently)."""
+    out = [x[0]]
+    for k in range(1, x.shape[0]):
+        out.append(out[-1] + x[k])
+    return torch.stack(out)
+
+
+def compute_dz(thk, levels):
+    """vert_disc.py:17-23: layer thicknesses thk * (level[k+1] - level[k])."""
+    ddz = levels[1:] - levels[:-1]
+    return thk[None] * ddz[:, None, None]
+
+
+def gradient_layers(s, dx):
+    """compute_gradient_layers_tf (vert_flow_v2.py:62-87): centred differences
+    of face values, with the faces on the domain border extrapolated
+    (1.5 s0 - 0.5 s1); s : [L, Ny, Nx]."""
+    EX = torch.cat([1.5 * s[:, :, 0:1] - 0.5 * s[:, :, 1:2], 0.5 * s[:, :, :-1] + 0.5 * s[:, :, 1:],
+                    1.5 * s[:, :, -1:] - 0.5 * s[:, :, -2:-1]], 2)
+    EY = torch.cat([1.5 * s[:, 0:1, :] - 0.5 * s[:, 1:2, :], 0.5 * s[:, :-1, :] + 0.5 * s[:, 1:, :],
+                    1.5 * s[:, -1:, :] - 0.5 * s[:, -2:-1, :]], 1)
+    return (EX[:, :, 1:] - EX[:, :, :-1]) / dx, (EY[:, 1:, :] - EY[:, :-1, :]) / dx
+
+
+def divflux_layers(u, v, h, dx):
+    """compute_divflux_layers (vert_flow_v2.py:126-147): centred divergence of
+    (u h, v h) per layer, border faces taking the border cell's flux."""
+    Qx = u * h
+    Qy = v * h
+    fx = torch.cat([Qx[:, :, 0:1], 0.5 * (Qx[:, :, :-1] + Qx[:, :, 1:]), Qx[:, :, -1:]], 2)
+    fy = torch.cat([Qy[:, 0:1, :], 0.5 * (Qy[:, :-1, :] + Qy[:, 1:, :]), Qy[:, -1:, :]], 1)
+    return (fx[:, :, 1:] - fx[:, :, :-1]) / dx + (fy[:, 1:, :] - fy[:, :-1, :]) / dx
+
+
+def vertical_velocity_kinematic(U, V, topg, thk, levels, vert_weight, dx):
+    """compute_vertical_velocity_kinematic_v2 / compute_w_kinematic_tf
+    (vert_flow_v2.py:17-37): the layer surfaces z_k = topg + sum_{l<k} dz_l,
+    their slopes, the running vertical means of U, V from the bed up to layer
+    k (weights vert_weight), and W = -div(mean * z-height) + U dz/dx + V dz/dy.
+    U, V : [Nz, Ny, Nx]; vert_weight : [Nz, 1, 1]; returns W [Nz, Ny, Nx]."""
+    dz = compute_dz(thk, levels)
+    cumdz = torch.cat([torch.zeros_like(thk)[None], cumsum0(dz)], 0)
+    sx, sy = gradient_layers(topg + cumdz, dx)
+    ub = cumsum0(vert_weight * U) / cumsum0(vert_weight)
+    vb = cumsum0(vert_weight * V) / cumsum0(vert_weight)
+    div = divflux_layers(ub, vb, cumdz, dx)
+    return -div + U * sx + V * sy
 
 
 # --------------------------------------------------------------------------

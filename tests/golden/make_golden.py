@@ -48,7 +48,7 @@ def _stub(name, path):
 for pkg in ["", "processes", "processes/iceflow", "processes/iceflow/energy",
             "processes/iceflow/energy/sliding_laws", "processes/iceflow/emulate",
             "processes/iceflow/emulate/emulators", "processes/iceflow/solve",
-            "processes/iceflow/diagnostic", "processes/thk", "processes/time",
+            "processes/iceflow/diagnostic", "processes/thk", "processes/time", "processes/vert_flow",
             "utils", "utils/gradient", "utils/math"]:
     _stub("igm" + ("." + pkg.replace("/", ".") if pkg else ""), os.path.join(IGM, pkg))
 
@@ -65,6 +65,7 @@ emulate_mod = importlib.import_module("igm.processes.iceflow.emulate.emulate")
 divflux_mod = importlib.import_module("igm.utils.gradient.compute_divflux_slope_limiter")
 thk_mod = importlib.import_module("igm.processes.thk.thk")
 time_mod = importlib.import_module("igm.processes.time.time")
+vflow_mod = importlib.import_module("igm.processes.vert_flow.vert_flow_v2")
 
 
 def ns(d):
@@ -291,6 +292,27 @@ def emulator_case():
     save("emulator", out)
 
 
+def vert_flow_cases():
+    """compute_w_kinematic_tf (vert_flow_v2.py:30-37) on seeded glaciers, with
+    dz from compute_dz and the weights of define_vertical_weight, as
+    compute_vertical_velocity_kinematic_v2 (:17-27) calls it."""
+    out = {}
+    for tag, ny, nx, nz, sp, dx, seed, dtype in [("f32", 23, 31, 10, 4.0, 100.0, 7, torch.float32),
+                                                 ("f64", 23, 31, 10, 4.0, 100.0, 7, torch.float64),
+                                                 ("nz5_f32", 17, 12, 5, 1.0, 50.0, 8, torch.float32),
+                                                 ("nz2_f32", 9, 14, 2, 2.0, 25.0, 9, torch.float32)]:
+        g = glacier(ny, nx, dx, seed, dtype)
+        U, V = vel(nz, ny, nx, seed, dtype)
+        levels = vert_disc.compute_levels(nz, sp).to(dtype)
+        w = vert_disc.define_vertical_weight(nz, sp).to(dtype)
+        dz = vert_disc.compute_dz(g["thk"], levels)
+        W = vflow_mod.compute_w_kinematic_tf(U, V, g["topg"], g["thk"], dz, torch.tensor(dx, dtype=dtype), w)
+        out.update({f"{tag}_U": U, f"{tag}_V": V, f"{tag}_topg": g["topg"], f"{tag}_thk": g["thk"],
+                    f"{tag}_levels": levels, f"{tag}_weight": w[:, 0, 0], f"{tag}_dx": np.asarray(dx),
+                    f"{tag}_W": W})
+    save("vert_flow", out)
+
+
 def save(name, d):
     arrs = {}
     for k, v in d.items():
@@ -316,3 +338,4 @@ if __name__ == "__main__":
     transport_cases()
     time_case()
     emulator_case()
+    vert_flow_cases()

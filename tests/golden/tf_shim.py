@@ -164,6 +164,18 @@ def concat(xs, axis):
     return torch.cat([_as(x, like) for x in xs], dim=axis)
 
 
+def cumsum(x, axis=0):
+    """Inclusive scan accumulated in the tensor's own dtype, one slice after
+    the other along ``axis`` (TF's kernel; torch.cumsum on CPU accumulates
+    float32 in double)."""
+    import builtins
+    x = _as(x)
+    parts = [x.narrow(axis, 0, 1)]
+    for i in builtins.range(1, x.shape[axis]):
+        parts.append(parts[-1] + x.narrow(axis, i, 1))
+    return torch.cat(parts, dim=axis)
+
+
 def stack(xs, axis=0):
     return torch.stack([_as(x) for x in xs], dim=axis)
 

@@ -58,3 +58,13 @@ def test_argument_validation_without_gpu(lib):
     assert rc == 2 and b"NULL" in lib.igm_last_error()
     rc = lib.igm_transport_step(0, 5, 5, 100.0, 16, 32, 48, 64, 80, None, 96, None, None, 1.0, None, 9, 0.91, 0.0, None)
     assert rc == 2 and b"slope_type" in lib.igm_last_error()
+
+
+def test_vertical_velocity_validation_without_gpu(lib):
+    lv = (C.c_double * 2)(0.0, 1.0)
+    rc = lib.igm_vertical_velocity(0, 1, 5, 5, 100.0, 16, 32, 48, 64, lv, lv, 80, None)
+    assert rc == 1 and b"nz, ny, nx >= 2" in lib.igm_last_error()
+    rc = lib.igm_vertical_velocity(0, 2, 5, 5, 100.0, 16, None, 48, 64, lv, lv, 80, None)
+    assert rc == 2 and b"NULL" in lib.igm_last_error()
+    rc = lib.igm_vertical_velocity(0, 2, 5, 5, 0.0, 16, 32, 48, 64, lv, lv, 80, None)
+    assert rc == 2 and b"dx" in lib.igm_last_error()

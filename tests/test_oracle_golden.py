@@ -139,3 +139,31 @@ def test_emulator_retrain_loop(golden):
     mask = (thk > 0)[None]
     U = torch.where(mask, U[0], 0.0)
     np.testing.assert_allclose(U.numpy(), g["U"], rtol=1e-9, atol=1e-9 * np.abs(g["U"]).max())
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64", "nz5_f32", "nz2_f32"])
+def test_vertical_velocity_kinematic(golden, tag):
+    """vert_flow version 2, kinematic: bit-identical to the reference's
+    compute_w_kinematic_tf (FP32 and FP64)."""
+    g = golden("vert_flow")
+    W = O.vertical_velocity_kinematic(T(g[f"{tag}_U"]), T(g[f"{tag}_V"]), T(g[f"{tag}_topg"]), T(g[f"{tag}_thk"]),
+                                      T(g[f"{tag}_levels"]), T(g[f"{tag}_weight"])[:, None, None],
+                                      float(g[f"{tag}_dx"]))
+    np.testing.assert_array_equal(W.numpy(), g[f"{tag}_W"])
+
+
+def test_vertical_velocity_analytic():
+    """Plug flow (U, V the same on every level) over a bed of uniform slope
+    with uniform thickness: no divergence, so W = U dz/dx + V dz/dy = the bed
+    slope times the flow on every layer (away from nothing: the extrapolated
+    border faces of a linear field are exact too)."""
+    ny, nx, nz, dx = 12, 15, 6, 100.0
+    y, x = np.meshgrid(np.arange(ny) * dx, np.arange(nx) * dx, indexing="ij")
+    topg = T(2000.0 - 0.05 * x + 0.02 * y)
+    thk = T(np.full((ny, nx), 120.0))
+    U = T(np.full((nz, ny, nx), 30.0))
+    V = T(np.full((nz, ny, nx), -12.0))
+    lv = O.compute_levels(nz, 1.0, torch.float64)
+    w = O.define_vertical_weight(nz, 1.0, torch.float64)
+    W = O.vertical_velocity_kinematic(U, V, topg, thk, lv, w, dx)
+    np.testing.assert_allclose(W.numpy(), 30.0 * -0.05 + -12.0 * 0.02, rtol=1e-12)
