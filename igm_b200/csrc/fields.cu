@@ -119,115 +119,15 @@ __device__ __forceinline__ T limited_slope(T hm, T h0, T hp, T dx, T rdx, int sl
   return maxmod(minmod(sigp, T(2) * sigm), minmod(sigm, T(2) * sigp));
 }
 
-// A CTA owns a 32 x 8 tile of nodes and computes every quantity once, in
-// shared memory: the limited slope of each cell, then the upwind flux of each
-// face, then the node update.  The operations and their order per quantity
-// are those of the reference (IEEE division by dx, no contraction), so the
-// result is bit-identical to evaluating each face independently.
-constexpr int kTrX = 32, kTrY = 8;
-template <typename T>
-__global__ void __launch_bounds__(kTrX* kTrY) transport_kernel(const TransportArgs<T> a) {
-  constexpr int HR = kTrY + 4, HC = kTrX + 4;  // thickness tile: rows j0-2 .. j0+9, columns i0-2 .. i0+33
-  __shared__ T sh[HR][HC + 1];
-  __shared__ T ssx[kTrY][kTrX + 2];   // x slopes of cells i0-1 .. i0+32 (rows j0 .. j0+7)
-  __shared__ T ssy[kTrY + 2][kTrX];   // y slopes of cells j0-1 .. j0+8 (columns i0 .. i0+31)
-  __shared__ T sq[kTrY][kTrX + 1];    // x-face fluxes, faces i0 .. i0+32
-  __shared__ T sr[kTrY + 1][kTrX];    // y-face fluxes, faces j0 .. j0+8
-  __shared__ T su[kTrY][kTrX + 2];    // ubar, rows j0 .. j0+7, columns i0-1 .. i0+32
-  __shared__ T sv[kTrY + 2][kTrX];    // vbar, rows j0-1 .. j0+8, columns i0 .. i0+31
-  const int nx = a.nx, ny = a.ny;
-  const int i0 = blockIdx.x * kTrX, j0 = blockIdx.y * kTrY;
-  const int tid = threadIdx.y * kTrX + threadIdx.x;
-  constexpr int NT = kTrX * kTrY;
-  const T dt = a.dt_dev ? (T)(*a.dt_dev) : a.dt_host;
-  const T dx = a.dx, rdx = a.rdx;
-  // every global input of the tile is requested before the first barrier
-  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
-  const bool node = i < nx && j < ny;
-  const size_t o = node ? (size_t)j * nx + i : 0;
-  const T tg = node ? a.topg[o] : T(0);
-  const T sm = (node && a.smb) ? a.smb[o] : T(0);
-  for (int k = tid; k < HR * HC; k += NT) {
-    const int r = k / HC, c = k - (k / HC) * HC;
-    const int jj = j0 - 2 + r, ii = i0 - 2 + c;
-    sh[r][c] = (jj >= 0 && jj < ny && ii >= 0 && ii < nx) ? a.h[(size_t)jj * nx + ii] : T(0);
-  }
-  for (int k = tid; k < kTrY * (kTrX + 2); k += NT) {
-    const int r = k / (kTrX + 2), c = k - (k / (kTrX + 2)) * (kTrX + 2);
-    const int jj = j0 + r, ii = i0 - 1 + c;
-    su[r][c] = (jj < ny && ii >= 0 && ii < nx) ? a.u[(size_t)jj * nx + ii] : T(0);
-  }
-  for (int k = tid; k < (kTrY + 2) * kTrX; k += NT) {
-    const int r = k / kTrX, c = k - (k / kTrX) * kTrX;
-    const int jj = j0 - 1 + r, ii = i0 + c;
-    sv[r][c] = (jj >= 0 && jj < ny && ii < nx) ? a.v[(size_t)jj * nx + ii] : T(0);
-  }
-  __syncthreads();
-  // cell slopes: x slope of cell (j, c) from its left / right neighbours, y slope from below / above
-  for (int k = tid; k < kTrY * (kTrX + 2); k += NT) {
-    const int r = k / (kTrX + 2), c = k - (k / (kTrX + 2)) * (kTrX + 2);  // cell (j0 + r, i0 - 1 + c)
-    ssx[r][c] = limited_slope(sh[r + 2][c], sh[r + 2][c + 1], sh[r + 2][c + 2], dx, rdx, a.slope);
-  }
-  for (int k = tid; k < (kTrY + 2) * kTrX; k += NT) {
-    const int r = k / kTrX, c = k - (k / kTrX) * kTrX;  // cell (j0 - 1 + r, i0 + c)
-    ssy[r][c] = limited_slope(sh[r][c + 2], sh[r + 1][c + 2], sh[r + 2][c + 2], dx, rdx, a.slope);
-  }
-  __syncthreads();
-  // face fluxes: x face f between cells f-1 and f of row j; y face f between rows f-1 and f
-  for (int k = tid; k < kTrY * (kTrX + 1); k += NT) {
-    const int r = k / (kTrX + 1), c = k - (k / (kTrX + 1)) * (kTrX + 1);
-    const int jr = j0 + r, f = i0 + c;
-    T q = T(0);
-    if (jr < ny && f <= nx) {
-      // su[r][c] = u[j][f-1], su[r][c+1] = u[j][f]
-      const T uf = f == 0 ? su[r][c + 1] : (f == nx ? su[r][c] : T(0.5) * (su[r][c] + su[r][c + 1]));
-      const T hl = sh[r + 2][c + 1], hr = sh[r + 2][c + 2];
-      const T sl = ssx[r][c], sr_ = ssx[r][c + 1];
-      const T cu = div_dx(uf * dt, dx, rdx);
-      const T w = hl + a.half_dx * (T(1) - cu) * sl;
-      const T e = hr - a.half_dx * (T(1) + cu) * sr_;
-      q = uf * (uf > T(0) ? w : e);
-    }
-    sq[r][c] = q;
-  }
-  for (int k = tid; k < (kTrY + 1) * kTrX; k += NT) {
-    const int r = k / kTrX, c = k - (k / kTrX) * kTrX;
-    const int f = j0 + r, ic = i0 + c;
-    T q = T(0);
-    if (f <= ny && ic < nx) {
-      // sv[r][c] = v[f-1][i], sv[r+1][c] = v[f][i]
-      const T vf = f == 0 ? sv[r + 1][c] : (f == ny ? sv[r][c] : T(0.5) * (sv[r][c] + sv[r + 1][c]));
-      const T hl = sh[r + 1][c + 2], hr = sh[r + 2][c + 2];
-      const T sl = ssy[r][c], sr_ = ssy[r + 1][c];
-      const T cv = div_dx(vf * dt, dx, rdx);
-      const T s_ = hl + a.half_dx * (T(1) - cv) * sl;
-      const T n_ = hr - a.half_dx * (T(1) + cv) * sr_;
-      q = vf * (vf > T(0) ? s_ : n_);
-    }
-    sr[r][c] = q;
-  }
-  __syncthreads();
-  if (!node) return;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const T div = div_dx(sq[ty][tx + 1] - sq[ty][tx], dx, rdx) + div_dx(sr[ty + 1][tx] - sr[ty][tx], dx, rdx);
-  T hn = sh[ty + 2][tx + 2] + dt * (sm - div);
-  hn = hn > T(0) ? hn : T(0);
-  const T fl = -a.ratio * hn + a.sealevel;
-  const T ls = tg > fl ? tg : fl;
-  a.h_out[o] = hn;
-  a.usurf[o] = ls + hn;
-  if (a.lsurf) a.lsurf[o] = ls;
-  if (a.divflux) a.divflux[o] = div;
-}
-
-// Row-marching variant: a warp owns a strip of 30 columns (lanes 1..30; lanes 0
-// and 31 carry the columns on either side) and walks down a segment of rows.
+// A warp owns a strip of 30 columns (lanes 1..30; lanes 0 and 31 carry the
+// columns on either side) and walks down a segment of rows.
 // x neighbours come from the adjacent lanes by shuffles; in y the thread keeps
 // a window of its column (thickness of rows j-1 .. j+2, the slope of cell j and
 // the flux through the face below node j), so every slope and face flux of the
 // interior is evaluated once.  The loads of a row are issued two rows ahead.
 // Each quantity is evaluated with the operations and order of the reference
-// (as transport_kernel), so the result is bit-identical to it.
+// (IEEE division by dx through div_dx, no contraction), so the result is
+// bit-identical to evaluating each face of the reference on its own.
 constexpr int kTmCols = 30;  // interior columns per warp
 constexpr int kTmWarps = 4;  // warps per CTA
 
@@ -468,114 +368,93 @@ __device__ __forceinline__ float ieee_div<float>(float a, float b) { return __fd
 template <>
 __device__ __forceinline__ double ieee_div<double>(double a, double b) { return __ddiv_rn(a, b); }
 
-// A CTA owns a 32 x 8 tile of nodes and walks the layers from the bed up (the
-// loads of the next layer are issued before the arithmetic of the current
-// one).  Each thread carries the running sums of its node(s) of the tile plus
-// a one-node halo: the layer height z_k - topg (the scan of thk (level[l+1] - level[l])),
-// the weighted sums of U and V and of the weights.  Per layer it publishes the
-// layer surface topg + z_k, the node's U, V and the fluxes (mean U) z_k,
-// (mean V) z_k to shared memory (two buffers, one barrier per layer); the
-// tile's threads then form the centred slopes and divergence with the border
-// forms of the reference and W = -div + U sx + V sy.  Operation order and
-// rounding follow the reference (no contraction: this unit is built with
-// -fmad=false; quotients are correctly rounded), so W is bit-identical.
-constexpr int kVfX = 32, kVfY = 8;
+// A warp owns a strip of 30 columns (lanes 1..30; lanes 0 and 31 carry the
+// columns on either side) and kVfRows rows plus the row above and below; each
+// thread keeps, for its column's kVfRows + 2 nodes, the running sums of the
+// layer walk in registers: the layer height z_k - topg (the scan of
+// thk (level[l+1] - level[l])) and the weighted sums of U and V.  Per layer it
+// forms the layer surface topg + z_k and the fluxes (mean U) z_k, (mean V) z_k
+// of those nodes; y neighbours are the thread's own registers, x neighbours
+// come from the adjacent lanes by shuffles -- no shared memory, no barrier.
+// Operation order and rounding follow the reference (no contraction: this unit
+// is built with -fmad=false; every quotient is the correctly rounded one, by
+// Markstein's step from the divisor's correctly rounded reciprocal -- dx, and
+// per layer the sum of the weights), so W is bit-identical.
+constexpr int kVfRows = 8;   // output rows per warp
+constexpr int kVfCols = 30;  // output columns per warp
+constexpr int kVfWarps = 4;  // warps per CTA
 template <typename T>
-__global__ void __launch_bounds__(kVfX* kVfY) vert_flow_kernel(const VertFlowArgs<T> a) {
-  constexpr int HX = kVfX + 2, HY = kVfY + 2, NH = HX * HY, NT = kVfX * kVfY;
-  constexpr int OWN = (NH + NT - 1) / NT;  // halo-tile nodes per thread
-  __shared__ T s_z[2][HY][HX];   // layer surface topg + z_k
-  __shared__ T s_qx[2][HY][HX];  // (mean U) z_k
-  __shared__ T s_qy[2][HY][HX];  // (mean V) z_k
-  __shared__ T s_u[2][kVfY][kVfX];
-  __shared__ T s_v[2][kVfY][kVfX];
+__global__ void __launch_bounds__(kVfWarps * 32) vert_flow_kernel(const VertFlowArgs<T> a, int n_strips) {
+  constexpr int R = kVfRows + 2;
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * kVfWarps + (threadIdx.x >> 5);
+  const int strip = gw % n_strips, seg = gw / n_strips;
   const int nx = a.nx, ny = a.ny;
+  const int j0 = seg * kVfRows;
+  if (j0 >= ny) return;  // uniform per warp
+  const int i = strip * kVfCols - 1 + lane;
+  const bool col = i >= 0 && i < nx;
+  const size_t ic = col ? (size_t)i : 0;
   const size_t plane = (size_t)ny * nx;
-  const int i0 = blockIdx.x * kVfX, j0 = blockIdx.y * kVfY;
-  const int tid = threadIdx.y * kVfX + threadIdx.x;
-  // the halo-tile nodes this thread carries
-  size_t off[OWN];
-  bool in[OWN], inner[OWN];
-  int hr[OWN], hc[OWN];
-  T tg[OWN], th[OWN], zh[OWN], su[OWN], sv[OWN];
-#pragma unroll
-  for (int q = 0; q < OWN; ++q) {
-    const int c = tid + q * NT;
-    hr[q] = c / HX;
-    hc[q] = c - hr[q] * HX;
-    const int jj = j0 - 1 + hr[q], ii = i0 - 1 + hc[q];
-    in[q] = c < NH && jj >= 0 && jj < ny && ii >= 0 && ii < nx;
-    inner[q] = c < NH && hr[q] >= 1 && hr[q] <= kVfY && hc[q] >= 1 && hc[q] <= kVfX;
-    off[q] = in[q] ? (size_t)jj * nx + ii : 0;
-    tg[q] = in[q] ? a.topg[off[q]] : T(0);
-    th[q] = in[q] ? a.thk[off[q]] : T(0);
-    zh[q] = T(0);
-    su[q] = T(0);
-    sv[q] = T(0);
-  }
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i = i0 + tx, j = j0 + ty;
-  const bool node = i < nx && j < ny;
+  const bool out_lane = lane >= 1 && lane <= kVfCols && col;
   const T dx = a.dx, rdx = a.rdx;
-  T sw = T(0);
-  // U, V of the carried nodes, one layer ahead of the arithmetic
-  T un[OWN], vn[OWN];
+  T tg[R], th[R], zh[R], su[R], sv[R];
+  bool in[R];
+  size_t off[R];
 #pragma unroll
-  for (int q = 0; q < OWN; ++q) {
-    un[q] = in[q] ? a.U[off[q]] : T(0);
-    vn[q] = in[q] ? a.V[off[q]] : T(0);
+  for (int r = 0; r < R; ++r) {
+    const int j = j0 - 1 + r;
+    in[r] = col && j >= 0 && j < ny;
+    off[r] = in[r] ? (size_t)j * nx + ic : 0;
+    tg[r] = in[r] ? a.topg[off[r]] : T(0);
+    th[r] = in[r] ? a.thk[off[r]] : T(0);
+    zh[r] = T(0);
+    su[r] = T(0);
+    sv[r] = T(0);
   }
+  T sw = T(0);
   for (int k = 0; k < a.nz; ++k) {
-    const int bsel = k & 1;
+    T u[R], v[R], z[R], qx[R], qy[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      u[r] = in[r] ? a.U[(size_t)k * plane + off[r]] : T(0);
+      v[r] = in[r] ? a.V[(size_t)k * plane + off[r]] : T(0);
+    }
     sw = k == 0 ? a.w[0] : sw + a.w[k];
-    T uc[OWN], vc[OWN];
+    const T rsw = ieee_div(T(1), sw);  // the layer's one divisor: Markstein's step from its reciprocal
+    const T ddz = k > 0 ? a.lev[k] - a.lev[k - 1] : T(0);
 #pragma unroll
-    for (int q = 0; q < OWN; ++q) {
-      uc[q] = un[q];
-      vc[q] = vn[q];
-      const bool nxt = in[q] && k + 1 < a.nz;
-      un[q] = nxt ? a.U[(size_t)(k + 1) * plane + off[q]] : T(0);
-      vn[q] = nxt ? a.V[(size_t)(k + 1) * plane + off[q]] : T(0);
-    }
-#pragma unroll
-    for (int q = 0; q < OWN; ++q) {
-      if (tid + q * NT >= NH) break;
-      const T u = uc[q];
-      const T v = vc[q];
+    for (int r = 0; r < R; ++r) {
       if (k > 0) {
-        const T dzl = th[q] * (a.lev[k] - a.lev[k - 1]);
-        zh[q] = k == 1 ? dzl : zh[q] + dzl;
+        const T dzl = th[r] * ddz;
+        zh[r] = k == 1 ? dzl : zh[r] + dzl;
       }
-      const T wu = a.w[k] * u, wv = a.w[k] * v;
-      su[q] = k == 0 ? wu : su[q] + wu;
-      sv[q] = k == 0 ? wv : sv[q] + wv;
-      s_z[bsel][hr[q]][hc[q]] = tg[q] + zh[q];
-      s_qx[bsel][hr[q]][hc[q]] = ieee_div(su[q], sw) * zh[q];
-      s_qy[bsel][hr[q]][hc[q]] = ieee_div(sv[q], sw) * zh[q];
-      if (inner[q]) {
-        s_u[bsel][hr[q] - 1][hc[q] - 1] = u;
-        s_v[bsel][hr[q] - 1][hc[q] - 1] = v;
-      }
+      const T wu = a.w[k] * u[r], wv = a.w[k] * v[r];
+      su[r] = k == 0 ? wu : su[r] + wu;
+      sv[r] = k == 0 ? wv : sv[r] + wv;
+      z[r] = tg[r] + zh[r];
+      qx[r] = div_dx(su[r], sw, rsw) * zh[r];
+      qy[r] = div_dx(sv[r], sw, rsw) * zh[r];
     }
-    __syncthreads();
-    if (node) {
-      const int r = ty + 1, c = tx + 1;
-      const T(*z)[HX] = s_z[bsel];
-      const T(*qx)[HX] = s_qx[bsel];
-      const T(*qy)[HX] = s_qy[bsel];
+#pragma unroll
+    for (int r = 1; r <= kVfRows; ++r) {
+      const int j = j0 - 1 + r;
+      const T zl = __shfl_up_sync(0xffffffffu, z[r], 1), zr = __shfl_down_sync(0xffffffffu, z[r], 1);
+      const T ql = __shfl_up_sync(0xffffffffu, qx[r], 1), qr = __shfl_down_sync(0xffffffffu, qx[r], 1);
+      if (!out_lane || j >= ny) continue;
       // faces of the layer surface (compute_gradient_layers_tf)
-      const T zw = i == 0 ? T(1.5) * z[r][c] - T(0.5) * z[r][c + 1] : T(0.5) * z[r][c - 1] + T(0.5) * z[r][c];
-      const T ze = i == nx - 1 ? T(1.5) * z[r][c] - T(0.5) * z[r][c - 1] : T(0.5) * z[r][c] + T(0.5) * z[r][c + 1];
-      const T zs = j == 0 ? T(1.5) * z[r][c] - T(0.5) * z[r + 1][c] : T(0.5) * z[r - 1][c] + T(0.5) * z[r][c];
-      const T zn = j == ny - 1 ? T(1.5) * z[r][c] - T(0.5) * z[r - 1][c] : T(0.5) * z[r][c] + T(0.5) * z[r + 1][c];
+      const T zw = i == 0 ? T(1.5) * z[r] - T(0.5) * zr : T(0.5) * zl + T(0.5) * z[r];
+      const T ze = i == nx - 1 ? T(1.5) * z[r] - T(0.5) * zl : T(0.5) * z[r] + T(0.5) * zr;
+      const T zs = j == 0 ? T(1.5) * z[r] - T(0.5) * z[r + 1] : T(0.5) * z[r - 1] + T(0.5) * z[r];
+      const T zn = j == ny - 1 ? T(1.5) * z[r] - T(0.5) * z[r - 1] : T(0.5) * z[r] + T(0.5) * z[r + 1];
       // faces of the fluxes (compute_divflux_layers)
-      const T fw = i == 0 ? qx[r][c] : T(0.5) * (qx[r][c - 1] + qx[r][c]);
-      const T fe = i == nx - 1 ? qx[r][c] : T(0.5) * (qx[r][c] + qx[r][c + 1]);
-      const T fs = j == 0 ? qy[r][c] : T(0.5) * (qy[r - 1][c] + qy[r][c]);
-      const T fn = j == ny - 1 ? qy[r][c] : T(0.5) * (qy[r][c] + qy[r + 1][c]);
+      const T fw = i == 0 ? qx[r] : T(0.5) * (ql + qx[r]);
+      const T fe = i == nx - 1 ? qx[r] : T(0.5) * (qx[r] + qr);
+      const T fs = j == 0 ? qy[r] : T(0.5) * (qy[r - 1] + qy[r]);
+      const T fn = j == ny - 1 ? qy[r] : T(0.5) * (qy[r] + qy[r + 1]);
       const T sx = div_dx(ze - zw, dx, rdx), sy = div_dx(zn - zs, dx, rdx);
       const T div = div_dx(fe - fw, dx, rdx) + div_dx(fn - fs, dx, rdx);
-      a.W[(size_t)k * plane + (size_t)j * nx + i] = (-div + s_u[bsel][ty][tx] * sx) + s_v[bsel][ty][tx] * sy;
+      a.W[(size_t)k * plane + off[r]] = (-div + u[r] * sx) + v[r] * sy;
     }
   }
 }
@@ -592,8 +471,9 @@ static int vert_flow_t(int nz, int ny, int nx, double dx, const void* U, const v
     a.w[k] = (T)vert_weight[k];
   }
   a.U = (const T*)U; a.V = (const T*)V; a.topg = (const T*)topg; a.thk = (const T*)thk; a.W = (T*)W;
-  dim3 blk(kVfX, kVfY), grd((nx + kVfX - 1) / kVfX, (ny + kVfY - 1) / kVfY);
-  vert_flow_kernel<T><<<grd, blk, 0, st>>>(a);
+  const int n_strips = (nx + kVfCols - 1) / kVfCols;
+  const long long warps = (long long)n_strips * ((ny + kVfRows - 1) / kVfRows);
+  vert_flow_kernel<T><<<(int)((warps + kVfWarps - 1) / kVfWarps), kVfWarps * 32, 0, st>>>(a, n_strips);
   return launch_status("vert_flow_kernel");
 }
 

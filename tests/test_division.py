@@ -1,8 +1,9 @@
-"""The transport kernel divides by dx with Markstein's step from the correctly
-rounded reciprocal (q = RN(a y), r = a - dx q exact, RN(q + r y)); the
-reference divides in IEEE float32.  Checked here on the CPU with exact rational
-arithmetic for the two fused steps, against numpy's IEEE float32 division, for
-the grid spacings in use and numerators across the range the transport sees."""
+"""The transport and vertical-velocity kernels divide with Markstein's step
+from the divisor's correctly rounded reciprocal (q = RN(a y), r = a - d q
+exact, RN(q + r y)); the reference divides in IEEE arithmetic.  Checked here
+on the CPU with exact rational arithmetic for the two fused steps, against
+numpy's IEEE division, for the grid spacings and the per-layer weight sums in
+use and numerators across the range the kernels see."""
 
 from fractions import Fraction
 
@@ -50,3 +51,38 @@ def test_zero_numerator_keeps_sign():
     rdx = np.float32(1.0) / dx32
     for z in (np.float32(0.0), np.float32(-0.0)):
         assert np.float32(markstein_div(z, dx32, rdx)).tobytes() == (z / dx32).tobytes()
+
+
+def markstein_div64(a: float, b: float, rb: float) -> float:
+    """The same three steps in float64 (Fraction -> float rounds to nearest)."""
+    if a == 0:
+        return a
+    q = a * rb
+    r = float(Fraction(a) - Fraction(b) * Fraction(q))
+    return float(Fraction(q) + Fraction(r) * Fraction(rb))
+
+
+@pytest.mark.parametrize("nz,spacing", [(2, 1.0), (5, 1.0), (10, 4.0), (16, 4.0), (30, 2.0), (64, 4.0)])
+def test_markstein_division_by_cumulative_weights(nz, spacing):
+    """The vertical-velocity kernel divides the running weighted sums of U, V
+    by the running sum of the vertical weights (one divisor per layer) with the
+    same step from that divisor's correctly rounded reciprocal; checked against
+    IEEE division in float32 and float64 for those divisors."""
+    from igm_b200.vertical import define_vertical_weight
+    w = define_vertical_weight(nz, spacing)[:, 0, 0]
+    sums32, s = [], np.float32(0)
+    for k in range(nz):
+        s = w[0] if k == 0 else np.float32(s + w[k])
+        sums32.append(np.float32(s))
+    rng = np.random.default_rng(nz)
+    mag = 10.0 ** rng.uniform(-8, 6, size=1500)
+    a = mag * rng.choice([-1.0, 1.0], size=mag.size)
+    for b32 in sums32:
+        rb32 = np.float32(np.float32(1.0) / b32)
+        b64 = float(b32)
+        rb64 = 1.0 / b64
+        for v in a:
+            v32 = np.float32(v)
+            got = markstein_div(v32, b32, rb32)
+            assert np.float32(got).tobytes() == np.float32(v32 / b32).tobytes(), (v32, b32)
+            assert markstein_div64(float(v), b64, rb64) == float(v) / b64, (v, b64)
