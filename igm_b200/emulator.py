@@ -16,8 +16,9 @@ and diagnostic/diagnostic.py), on the device.
   the solved velocities replace the emulated ones.
 * ``save_iceflow_model`` / ``load_iceflow_model``: weights, Adam moments and
   iteration count as ``model.npz`` next to the reference's ``fieldin.dat`` and
-  ``vert_grid.dat`` text files (emulate.py:331-359).  Keras ``.h5`` files are
-  not read (no HDF5 reader in this environment).
+  ``vert_grid.dat`` text files (emulate.py:331-359); ``load_keras_h5`` reads
+  the reference's own Keras ``model.h5`` files (igm_b200.keras_h5, no h5py
+  needed), so the emulators the reference ships run as pretrained networks.
 """
 
 from __future__ import annotations
@@ -71,12 +72,19 @@ def initialize_iceflow_emulator(cfg, state):
                               scales=list(e.get("input_scales", [1.0] * 5)), device=thk.device,
                               nb_out_filter=int(net.nb_out_filter), out_scale=float(e.get("output_scale", 1.0)))
     loaded = False
-    if e.pretrained and e.name:
-        path = os.path.join(getattr(state, "original_cwd", os.getcwd()), e.name)
-        if os.path.exists(os.path.join(path, "model.npz")):
+    if e.pretrained:
+        if e.name:
+            path = os.path.join(getattr(state, "original_cwd", os.getcwd()), e.name)
+        else:
+            path = _packaged_emulator_dir(cfg)
+        if path and os.path.exists(os.path.join(path, "model.npz")):
             load_iceflow_model(state, path, cfg)
             loaded = True
-            print("Found pretrained emulator: " + e.name)
+        elif path and os.path.exists(os.path.join(path, "model.h5")):
+            load_keras_h5(state, path, cfg)
+            loaded = True
+        if loaded:
+            print("Found pretrained emulator: " + path)
     if not loaded:
         print("No pretrained emulator, start from scratch.")
     state.COST_EMULATOR = []
@@ -237,6 +245,66 @@ def save_iceflow_model(cfg, state, directory="iceflow-model"):
                                     "# param for vertical spacing (vert_spacing)"))
 
 
+def emulator_dir_name(cfg) -> str:
+    """The name under which the reference ships its pretrained emulators
+    (emulate.py:37-62): pinnbp_<Nz>_<vert_spacing>_<architecture>_<nb_layers>_
+    <nb_out_filter>_<dim_arrhenius>_1_<a (Lagrange) | e (Legendre)>."""
+    ic = cfg.processes.iceflow
+    net = ic.emulator.network
+    basis = "e" if ic.numerics.vert_basis == "Legendre" else "a"
+    return (f"pinnbp_{ic.numerics.Nz}_{int(ic.numerics.vert_spacing)}_{net.architecture}_{net.nb_layers}_"
+            f"{net.nb_out_filter}_{ic.physics.dim_arrhenius}_1_{basis}")
+
+
+def _packaged_emulator_dir(cfg):
+    """The directory of the emulators the reference package ships
+    (igm/processes/iceflow/emulate/emulators/<name>, emulate.py:64-77), found
+    through the installed ``igm`` package without importing it; None when the
+    reference is not installed or ships no emulator of that name."""
+    import importlib.util
+    try:
+        spec = importlib.util.find_spec("igm")
+    except (ImportError, ValueError):
+        return None
+    if spec is None or not spec.submodule_search_locations:
+        return None
+    for root in spec.submodule_search_locations:
+        d = os.path.join(root, "processes", "iceflow", "emulate", "emulators", emulator_dir_name(cfg))
+        if os.path.isdir(d):
+            return d
+    return None
+
+
+def _check_fieldin(directory, cfg):
+    """emulate.py:79-84: the emulator's input fields must be the configured ones."""
+    fin = os.path.join(directory, "fieldin.dat")
+    if cfg is not None and os.path.exists(fin):
+        with open(fin) as f:
+            names = [ln.split()[0] for ln in f if ln.strip()]
+        if list(cfg.processes.iceflow.emulator.fieldin) != names:
+            raise ValueError(f"{fin} lists {names}, the configuration {list(cfg.processes.iceflow.emulator.fieldin)}")
+
+
+def load_keras_h5(state, directory, cfg=None):
+    """Loads a Keras emulator saved by the reference (``model.h5``, the files it
+    ships under igm/processes/iceflow/emulate/emulators and the ones
+    ``save_iceflow_model`` writes) into the network: the weights of its
+    nb_layers 3x3 convolutions and of the 1x1 head, in Keras order.  The
+    inputs are the raw fields and the outputs the raw velocities, as in the
+    reference, so the input scales and the output scale are reset to 1.
+    Adam starts afresh, as the reference's ``opti_retrain`` does."""
+    from .keras_h5 import cnn_params_from_keras, read_keras_weights
+    _check_fieldin(directory, cfg)
+    m: CNN = state.iceflow_model
+    layers = read_keras_weights(os.path.join(directory, "model.h5"))
+    m.set_params(cnn_params_from_keras(layers, m.L, m.cin, m.nout))
+    m.scales = np.ones(5, np.float32)
+    m.out_scale = 1.0
+    m.m.zero_()
+    m.v.zero_()
+    m.opt_iterations = 0
+
+
 def load_iceflow_model(state, directory, cfg=None):
     d = np.load(os.path.join(directory, "model.npz"))
     m: CNN = state.iceflow_model
@@ -249,8 +317,4 @@ def load_iceflow_model(state, directory, cfg=None):
     m.scales = np.asarray(d["scales"], np.float32)
     if "out_scale" in d.files:
         m.out_scale = float(d["out_scale"])
-    fin = os.path.join(directory, "fieldin.dat")
-    if cfg is not None and os.path.exists(fin):
-        with open(fin) as f:
-            names = [ln.split()[0] for ln in f if ln.strip()]
-        assert list(cfg.processes.iceflow.emulator.fieldin) == names
+    _check_fieldin(directory, cfg)

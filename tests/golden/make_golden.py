@@ -313,6 +313,30 @@ def vert_flow_cases():
     save("vert_flow", out)
 
 
+def keras_h5_cases():
+    """The Keras emulators the reference ships (igm/processes/iceflow/emulate/
+    emulators/*/model.h5) read by igm_b200.keras_h5: per file the weight names,
+    shapes, float64 sums and first values, as a JSON summary (the weights
+    themselves stay in the reference)."""
+    import glob
+    import json
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from igm_b200.keras_h5 import read_keras_weights
+    root = os.path.join(IGM, "processes", "iceflow", "emulate", "emulators")
+    out = {}
+    for path in sorted(glob.glob(os.path.join(root, "**", "model.h5"), recursive=True)):
+        rel = os.path.relpath(os.path.dirname(path), root)
+        layers = read_keras_weights(path)
+        out[rel] = [{"layer": ln, "weights": [{"name": wn, "shape": list(a.shape), "sum": float(a.astype(np.float64).sum()),
+                                               "sumsq": float((a.astype(np.float64) ** 2).sum()),
+                                               "first": [float(v) for v in a.reshape(-1)[:4]]} for wn, a in ws]}
+                    for ln, ws in layers if ws]
+    dst = os.path.join(HERE, "keras_h5.json")
+    with open(dst, "w") as f:
+        json.dump(out, f, indent=0)
+    print(f"wrote {dst} ({os.path.getsize(dst)} B)")
+
+
 def save(name, d):
     arrs = {}
     for k, v in d.items():
@@ -339,3 +363,4 @@ if __name__ == "__main__":
     time_case()
     emulator_case()
     vert_flow_cases()
+    keras_h5_cases()
