@@ -82,6 +82,7 @@ SIGNATURES = {
     "igm_transport_step": (I, [I, I, I, D, P, P, P, P, P, P, P, P, P, D, P, I, D, D, P]),
     "igm_thk_surfaces": (I, [I, I, P, P, P, P, D, D, P]),
     "igm_vertical_velocity": (I, [I, I, I, I, D, P, P, P, P, P, P, P, P]),
+    "igm_vertical_velocity_incompressibility": (I, [I, I, I, I, D, P, P, P, P, P, P, P, P]),
     "igm_smb_simple": (I, [I, I, P, P, P, D, D, D, D, P]),
     "igm_absmax2": (I, [I, I, P, P, P, P]),
     "igm_cfl_dt": (I, [P, P, D, D, D, P]),

@@ -459,9 +459,116 @@ __global__ void __launch_bounds__(kVfWarps * 32) vert_flow_kernel(const VertFlow
   }
 }
 
+// vert_flow version 2, incompressibility method (vert_flow_v2.py:40-57 with
+// gradx/grady_non_flat_layers_tf :168-199), uniform spacing dX = dx.  Same
+// warp layout as vert_flow_kernel; a thread walks its column's nodes up the
+// layers carrying the layer height above the bed (the scan of
+// thk (level[k] - level[k-1])), the running sum of dz (du/dx + dv/dy) and the
+// lower layer-face values of U and V, with U, V of the next layer loaded one
+// layer ahead.  x neighbours (U and the layer surface Z) by shuffles, y
+// neighbours (V and Z) from the thread's own rows.  Operation order and
+// rounding follow the reference: division by dx by Markstein's step, by
+// vert_weight thk (per node) in IEEE division; no contraction.
+template <typename T>
+__global__ void __launch_bounds__(kVfWarps * 32) vert_flow_incomp_kernel(const VertFlowArgs<T> a, int n_strips) {
+  constexpr int R = kVfRows + 2;
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * kVfWarps + (threadIdx.x >> 5);
+  const int strip = gw % n_strips, seg = gw / n_strips;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int j0 = seg * kVfRows;
+  if (j0 >= ny) return;  // uniform per warp
+  const int i = strip * kVfCols - 1 + lane;
+  const bool col = i >= 0 && i < nx;
+  const size_t ic = col ? (size_t)i : 0;
+  const size_t plane = (size_t)ny * nx;
+  const bool out_lane = lane >= 1 && lane <= kVfCols && col;
+  const T dx = a.dx, rdx = a.rdx, h = T(0.5), o5 = T(1.5);
+  // x and y derivative of a field from this node (c), its x neighbours (l, r) and its
+  // y neighbours (s, n), with the reference's one-sided border faces
+  auto ddx = [&](T l, T c, T r) {
+    const T fw = i == 0 ? o5 * c - h * r : h * l + h * c;
+    const T fe = i == nx - 1 ? o5 * c - h * l : h * c + h * r;
+    return div_dx(fe - fw, dx, rdx);
+  };
+  auto ddy = [&](int j, T s_, T c, T n_) {
+    const T fs = j == 0 ? o5 * c - h * n_ : h * s_ + h * c;
+    const T fn = j == ny - 1 ? o5 * c - h * s_ : h * c + h * n_;
+    return div_dx(fn - fs, dx, rdx);
+  };
+  T tg[R], th[R], zc[R], uc[R], vc[R], ufl[R], vfl[R], cum[R], base[R];
+  bool in[R];
+  size_t off[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int j = j0 - 1 + r;
+    in[r] = col && j >= 0 && j < ny;
+    off[r] = in[r] ? (size_t)j * nx + ic : 0;
+    tg[r] = in[r] ? a.topg[off[r]] : T(0);
+    th[r] = in[r] ? a.thk[off[r]] : T(0);
+    uc[r] = in[r] ? a.U[off[r]] : T(0);
+    vc[r] = in[r] ? a.V[off[r]] : T(0);
+    ufl[r] = uc[r];  // the bed face is U_0 itself
+    vfl[r] = vc[r];
+    zc[r] = T(0);
+    cum[r] = T(0);
+  }
+  // U_0 dtopg/dx + V_0 dtopg/dy of the output rows (compute_gradient_tf of topg)
+#pragma unroll
+  for (int r = 1; r <= kVfRows; ++r) {
+    const T tl = __shfl_up_sync(0xffffffffu, tg[r], 1), tr = __shfl_down_sync(0xffffffffu, tg[r], 1);
+    base[r] = ddx(tl, tg[r], tr) * uc[r] + ddy(j0 - 1 + r, tg[r - 1], tg[r], tg[r + 1]) * vc[r];
+  }
+  for (int k = 0; k < nz; ++k) {
+    T un[R], vn[R];
+    const bool more = k + 1 < nz;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      un[r] = (more && in[r]) ? a.U[(size_t)(k + 1) * plane + off[r]] : T(0);
+      vn[r] = (more && in[r]) ? a.V[(size_t)(k + 1) * plane + off[r]] : T(0);
+    }
+    const T ddz = k > 0 ? a.lev[k] - a.lev[k - 1] : T(0);
+    const T wk = a.w[k];
+    T z[R], dz[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      dz[r] = k > 0 ? th[r] * ddz : T(0);
+      zc[r] = k == 0 ? dz[r] : zc[r] + dz[r];
+      z[r] = zc[r] + tg[r];
+    }
+#pragma unroll
+    for (int r = 1; r <= kVfRows; ++r) {
+      const int j = j0 - 1 + r;
+      const T zl = __shfl_up_sync(0xffffffffu, z[r], 1), zr = __shfl_down_sync(0xffffffffu, z[r], 1);
+      const T ul = __shfl_up_sync(0xffffffffu, uc[r], 1), ur = __shfl_down_sync(0xffffffffu, uc[r], 1);
+      if (!out_lane || j >= ny) continue;
+      // du/dz, dv/dz between this layer's faces, zero off the ice
+      const T ufh = more ? h * (uc[r] + un[r]) : uc[r];
+      const T vfh = more ? h * (vc[r] + vn[r]) : vc[r];
+      const T hw = wk * th[r];
+      const bool ice = th[r] > T(0);
+      const T dudz = ice ? ieee_div(ufh - ufl[r], hw) : T(0);
+      const T dvdz = ice ? ieee_div(vfh - vfl[r], hw) : T(0);
+      const T dudx = ddx(ul, uc[r], ur) - ddx(zl, z[r], zr) * dudz;
+      const T dvdy = ddy(j, vc[r - 1], vc[r], vc[r + 1]) - ddy(j, z[r - 1], z[r], z[r + 1]) * dvdz;
+      const T term = dz[r] * (dudx + dvdy);
+      cum[r] = k == 0 ? term : cum[r] + term;
+      a.W[(size_t)k * plane + off[r]] = base[r] - cum[r];
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      ufl[r] = more ? h * (uc[r] + un[r]) : uc[r];
+      vfl[r] = more ? h * (vc[r] + vn[r]) : vc[r];
+      uc[r] = un[r];
+      vc[r] = vn[r];
+    }
+  }
+}
+
 template <typename T>
 static int vert_flow_t(int nz, int ny, int nx, double dx, const void* U, const void* V, const void* topg,
-                       const void* thk, const double* levels, const double* vert_weight, void* W, cudaStream_t st) {
+                       const void* thk, const double* levels, const double* vert_weight, void* W, bool incomp,
+                       cudaStream_t st) {
   VertFlowArgs<T> a{};
   a.nz = nz; a.ny = ny; a.nx = nx;
   a.dx = (T)dx;
@@ -473,7 +580,12 @@ static int vert_flow_t(int nz, int ny, int nx, double dx, const void* U, const v
   a.U = (const T*)U; a.V = (const T*)V; a.topg = (const T*)topg; a.thk = (const T*)thk; a.W = (T*)W;
   const int n_strips = (nx + kVfCols - 1) / kVfCols;
   const long long warps = (long long)n_strips * ((ny + kVfRows - 1) / kVfRows);
-  vert_flow_kernel<T><<<(int)((warps + kVfWarps - 1) / kVfWarps), kVfWarps * 32, 0, st>>>(a, n_strips);
+  const int grid = (int)((warps + kVfWarps - 1) / kVfWarps);
+  if (incomp) {
+    vert_flow_incomp_kernel<T><<<grid, kVfWarps * 32, 0, st>>>(a, n_strips);
+    return launch_status("vert_flow_incomp_kernel");
+  }
+  vert_flow_kernel<T><<<grid, kVfWarps * 32, 0, st>>>(a, n_strips);
   return launch_status("vert_flow_kernel");
 }
 
@@ -592,8 +704,24 @@ extern "C" int igm_vertical_velocity(int dtype, int nz, int ny, int nx, double d
                 "igm_vertical_velocity: NULL argument");
   IGM_CHECK_ARG(dx > 0, IGM_ERR_BAD_ARGUMENT, "igm_vertical_velocity: dx must be positive");
   cudaStream_t st = as_stream(stream);
-  if (dtype == IGM_F32) return vert_flow_t<float>(nz, ny, nx, dx, U, V, topg, thk, levels, vert_weight, W, st);
-  if (dtype == IGM_F64) return vert_flow_t<double>(nz, ny, nx, dx, U, V, topg, thk, levels, vert_weight, W, st);
+  if (dtype == IGM_F32) return vert_flow_t<float>(nz, ny, nx, dx, U, V, topg, thk, levels, vert_weight, W, false, st);
+  if (dtype == IGM_F64) return vert_flow_t<double>(nz, ny, nx, dx, U, V, topg, thk, levels, vert_weight, W, false, st);
   set_error("igm_vertical_velocity: unknown dtype %d", dtype);
+  return IGM_ERR_BAD_ARGUMENT;
+}
+
+extern "C" int igm_vertical_velocity_incompressibility(int dtype, int nz, int ny, int nx, double dx, const void* U,
+                                                       const void* V, const void* topg, const void* thk,
+                                                       const double* levels, const double* vert_weight, void* W,
+                                                       void* stream) {
+  IGM_CHECK_ARG(nz >= 2 && nz <= IGM_MAX_NZ && ny >= 2 && nx >= 2, IGM_ERR_BAD_SHAPE,
+                "igm_vertical_velocity_incompressibility: bad shape %dx%dx%d (needs nz, ny, nx >= 2)", nz, ny, nx);
+  IGM_CHECK_ARG(U && V && topg && thk && levels && vert_weight && W, IGM_ERR_BAD_ARGUMENT,
+                "igm_vertical_velocity_incompressibility: NULL argument");
+  IGM_CHECK_ARG(dx > 0, IGM_ERR_BAD_ARGUMENT, "igm_vertical_velocity_incompressibility: dx must be positive");
+  cudaStream_t st = as_stream(stream);
+  if (dtype == IGM_F32) return vert_flow_t<float>(nz, ny, nx, dx, U, V, topg, thk, levels, vert_weight, W, true, st);
+  if (dtype == IGM_F64) return vert_flow_t<double>(nz, ny, nx, dx, U, V, topg, thk, levels, vert_weight, W, true, st);
+  set_error("igm_vertical_velocity_incompressibility: unknown dtype %d", dtype);
   return IGM_ERR_BAD_ARGUMENT;
 }

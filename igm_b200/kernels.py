@@ -106,19 +106,23 @@ def transport_step(ubar, vbar, thk, topg, smb, dx, dt, slope_type="superbee", ra
     return thk_new, usurf, lsurf, div
 
 
-def vertical_velocity(U, V, topg, thk, levels, vert_weight, dx, out=None):
-    """W [Nz, Ny, Nx] of vert_flow version 2, kinematic (igm_vertical_velocity).
-    levels and vert_weight: the Nz values of compute_levels and
-    define_vertical_weight (any array-like)."""
+def vertical_velocity(U, V, topg, thk, levels, vert_weight, dx, out=None, method="kinematic"):
+    """W [Nz, Ny, Nx] of vert_flow version 2, method "kinematic"
+    (igm_vertical_velocity) or "incompressibility"
+    (igm_vertical_velocity_incompressibility).  levels and vert_weight: the Nz
+    values of compute_levels and define_vertical_weight (any array-like)."""
     nz, ny, nx = U.shape
     W = out if out is not None else torch.empty_like(U)
     lv = np.ascontiguousarray(np.asarray(levels, dtype=np.float64).reshape(-1))
     w = np.ascontiguousarray(np.asarray(vert_weight, dtype=np.float64).reshape(-1))
     if lv.size != nz or w.size != nz:
         raise ValueError(f"levels ({lv.size}) and vert_weight ({w.size}) must have Nz = {nz} entries")
-    rc = L.lib().igm_vertical_velocity(L.dtype_code(U.dtype), nz, ny, nx, float(dx), L.ptr(U), L.ptr(V), L.ptr(topg),
-                                       L.ptr(thk), lv.ctypes.data, w.ctypes.data, L.ptr(W), L.stream_ptr())
-    L.check(rc, "igm_vertical_velocity")
+    if method not in ("kinematic", "incompressibility"):
+        raise ValueError(f"vert_flow method {method!r}")
+    name = "igm_vertical_velocity" if method == "kinematic" else "igm_vertical_velocity_incompressibility"
+    rc = getattr(L.lib(), name)(L.dtype_code(U.dtype), nz, ny, nx, float(dx), L.ptr(U), L.ptr(V), L.ptr(topg),
+                                L.ptr(thk), lv.ctypes.data, w.ctypes.data, L.ptr(W), L.stream_ptr())
+    L.check(rc, name)
     return W
 
 

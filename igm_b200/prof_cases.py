@@ -33,6 +33,8 @@ def main():
     K.transport_step(ub, vb, f[0], f[1], None, 50.0, 0.01)       # transport
     topg = torch.as_tensor(st["topg"]).cuda()
     K.vertical_velocity(U, V, topg, f[0], compute_levels(nz, 4.0), define_vertical_weight(nz, 4.0), 50.0)  # vert_flow
+    K.vertical_velocity(U, V, topg, f[0], compute_levels(nz, 4.0), define_vertical_weight(nz, 4.0), 50.0,
+                        method="incompressibility")
     B, H, W = 2, 1000, 1000                                       # 2 x 64 MB activations (> L2)
     x = torch.randn(B, H, 4, W, 8, device="cuda").to(torch.bfloat16)
     y = torch.empty_like(x)

@@ -245,6 +245,22 @@ IGM_API int igm_vertical_velocity(int dtype, int nz, int ny, int nx, double dx, 
                           const void* topg, const void* thk, const double* levels, const double* vert_weight,
                           void* W, void* stream);
 
+/* Vertical velocity, vert_flow version 2, incompressibility method: replaces
+ * compute_vertical_velocity_incompressibility_v2 (igm/processes/vert_flow/
+ * vert_flow_v2.py:40-57, with gradx/grady_non_flat_layers_tf :168-199 and
+ * compute_gradient_tf, igm/utils/gradient/compute_gradient_tf.py:6-35) for a
+ * uniform spacing dX = dx.  With z_k = sum_{l<k} thk (levels[l+1] - levels[l])
+ * and the layer surface Z_k = topg + z_k, the terrain-following derivatives
+ *   du/dx_k = (dU_k/dx) - (dZ_k/dx) (U_{k+1/2} - U_{k-1/2}) / (vert_weight_k thk)
+ * (layer faces U_{-1/2} = U_0, U_{Nz-1/2} = U_{Nz-1}, zero where thk = 0), the
+ * same for dv/dy, and
+ *   W_k = U_0 dtopg/dx + V_0 dtopg/dy - sum_{l<=k} (z_l - z_{l-1}) (du/dx + dv/dy)_l.
+ * Arguments and layouts as igm_vertical_velocity.  Bit-identical to the
+ * reference in FP32/FP64. */
+IGM_API int igm_vertical_velocity_incompressibility(int dtype, int nz, int ny, int nx, double dx, const void* U,
+                                            const void* V, const void* topg, const void* thk, const double* levels,
+                                            const double* vert_weight, void* W, void* stream);
+
 /* Surfaces from thickness (thk.py:11-24): lsurf = max(topg, -r thk + sealevel),
  * usurf = lsurf + thk.  lsurf may be NULL. */
 IGM_API int igm_thk_surfaces(int dtype, int n, const void* thk, const void* topg, void* lsurf, void* usurf,

@@ -421,6 +421,35 @@ def vertical_velocity_kinematic(U, V, topg, thk, levels, vert_weight, dx):
     return -div + U * sx + V * sy
 
 
+def _faces_mean_z(U):
+    """[U_0, (U_k + U_{k+1})/2, U_{Nz-1}]: the layer-face values of
+    gradx/grady_non_flat_layers_tf (vert_flow_v2.py:175, 192)."""
+    return torch.cat([U[0:1], 0.5 * (U[:-1] + U[1:]), U[-1:]], 0)
+
+
+def vertical_velocity_incompressibility(U, V, topg, thk, levels, vert_weight, dx):
+    """compute_vertical_velocity_incompressibility_v2 (vert_flow_v2.py:40-57)
+    with gradx/grady_non_flat_layers_tf (:168-199), compute_gradx/grady_layers_tf
+    (:90-123) and compute_gradient_tf (utils/gradient/compute_gradient_tf.py:6-35)
+    for a uniform spacing dX = dx: terrain-following horizontal derivatives
+    du/dx = (du/dx)_flat - dZ/dx du/dz on the layer surfaces Z, and
+    W_k = U_0 dtopg/dx + V_0 dtopg/dy - sum_{l<=k} dz_l (du/dx + dv/dy)_l."""
+    dz = torch.cat([torch.zeros_like(thk)[None], compute_dz(thk, levels)], 0)
+    Z = cumsum0(dz) + topg
+    sx_b, sy_b = gradient_layers(topg[None], dx)
+    sx, sy = gradient_layers(Z, dx)
+    gUx, _ = gradient_layers(U, dx)
+    _, gVy = gradient_layers(V, dx)
+    h = vert_weight * thk
+    Uf, Vf = _faces_mean_z(U), _faces_mean_z(V)
+    dUdz = torch.where(thk > 0, (Uf[1:] - Uf[:-1]) / h, torch.zeros_like(h))
+    dVdz = torch.where(thk > 0, (Vf[1:] - Vf[:-1]) / h, torch.zeros_like(h))
+    dudx = gUx - sx * dUdz
+    dvdy = gVy - sy * dVdz
+    intdwdz = cumsum0(dz * (dudx + dvdy))
+    return sx_b[0] * U[0] + sy_b[0] * V[0] - intdwdz
+
+
 # --------------------------------------------------------------------------
 # transport, time step, mass balance
 # --------------------------------------------------------------------------

@@ -307,9 +307,17 @@ def vert_flow_cases():
         w = vert_disc.define_vertical_weight(nz, sp).to(dtype)
         dz = vert_disc.compute_dz(g["thk"], levels)
         W = vflow_mod.compute_w_kinematic_tf(U, V, g["topg"], g["thk"], dz, torch.tensor(dx, dtype=dtype), w)
+        # the incompressibility method (:40-57) reads cfg and state; dX is the uniform spacing field
+        cfg = load_cfg(**{"iceflow.numerics.Nz": nz, "iceflow.numerics.vert_spacing": sp})
+        st = types.SimpleNamespace(U=U, V=V, topg=g["topg"], thk=g["thk"], vert_weight=w,
+                                   dX=torch.full_like(g["thk"], dx))
+        orig = vflow_mod.compute_levels
+        vflow_mod.compute_levels = lambda n, s_: orig(n, s_).to(dtype)  # FP64 cases: levels in the case's dtype
+        Wi = vflow_mod.compute_vertical_velocity_incompressibility_v2(cfg, st)
+        vflow_mod.compute_levels = orig
         out.update({f"{tag}_U": U, f"{tag}_V": V, f"{tag}_topg": g["topg"], f"{tag}_thk": g["thk"],
                     f"{tag}_levels": levels, f"{tag}_weight": w[:, 0, 0], f"{tag}_dx": np.asarray(dx),
-                    f"{tag}_W": W})
+                    f"{tag}_W": W, f"{tag}_Wi": Wi})
     save("vert_flow", out)
 
 

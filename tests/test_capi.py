@@ -68,3 +68,11 @@ def test_vertical_velocity_validation_without_gpu(lib):
     assert rc == 2 and b"NULL" in lib.igm_last_error()
     rc = lib.igm_vertical_velocity(0, 2, 5, 5, 0.0, 16, 32, 48, 64, lv, lv, 80, None)
     assert rc == 2 and b"dx" in lib.igm_last_error()
+
+
+def test_vertical_velocity_incompressibility_validation_without_gpu(lib):
+    lv = (C.c_double * 2)(0.0, 1.0)
+    rc = lib.igm_vertical_velocity_incompressibility(0, 1, 5, 5, 100.0, 16, 32, 48, 64, lv, lv, 80, None)
+    assert rc == 1 and b"nz, ny, nx >= 2" in lib.igm_last_error()
+    rc = lib.igm_vertical_velocity_incompressibility(7, 2, 5, 5, 100.0, 16, 32, 48, 64, lv, lv, 80, None)
+    assert rc == 2 and b"dtype" in lib.igm_last_error()

@@ -167,3 +167,14 @@ def test_vertical_velocity_analytic():
     w = O.define_vertical_weight(nz, 1.0, torch.float64)
     W = O.vertical_velocity_kinematic(U, V, topg, thk, lv, w, dx)
     np.testing.assert_allclose(W.numpy(), 30.0 * -0.05 + -12.0 * 0.02, rtol=1e-12)
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64", "nz5_f32", "nz2_f32"])
+def test_vertical_velocity_incompressibility(golden, tag):
+    """vert_flow version 2, incompressibility: bit-identical to the
+    reference's compute_vertical_velocity_incompressibility_v2 (uniform dX)."""
+    g = golden("vert_flow")
+    W = O.vertical_velocity_incompressibility(T(g[f"{tag}_U"]), T(g[f"{tag}_V"]), T(g[f"{tag}_topg"]),
+                                              T(g[f"{tag}_thk"]), T(g[f"{tag}_levels"]),
+                                              T(g[f"{tag}_weight"])[:, None, None], float(g[f"{tag}_dx"]))
+    np.testing.assert_array_equal(W.numpy(), g[f"{tag}_Wi"])
