@@ -156,16 +156,12 @@ struct MarchRow {
   T he;  // edge lanes: thickness of the column beyond the strip, row j
 };
 
-template <typename T, int SLOPE>
-__global__ void __launch_bounds__(kTmWarps * 32) transport_march_kernel(const TransportArgs<T> a, int n_strips,
-                                                                       int rows_per_seg) {
-  const int lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * kTmWarps + (threadIdx.x >> 5);
-  const int strip = gw % n_strips, seg = gw / n_strips;
+// ROWS: the segment's rows y0-2 .. y1+4 may leave the domain (the first and last
+// segments of a strip), so every row index is checked; interior segments skip
+// those checks.
+template <typename T, int SLOPE, bool ROWS>
+__device__ __forceinline__ void transport_march(const TransportArgs<T>& a, int lane, int strip, int y0, int y1) {
   const int nx = a.nx, ny = a.ny;
-  const int y0 = seg * rows_per_seg;
-  if (y0 >= ny) return;  // uniform per warp
-  const int y1 = min(y0 + rows_per_seg, ny);
   const int i = strip * kTmCols - 1 + lane;  // this lane's column
   const bool col = i >= 0 && i < nx;
   const size_t ic = col ? (size_t)i : 0;
@@ -177,11 +173,12 @@ __global__ void __launch_bounds__(kTmWarps * 32) transport_march_kernel(const Tr
   const T dx = a.dx, rdx = a.rdx, hdx = a.half_dx;
   const T* H = a.h;
   auto at = [&](const T* p, int j, bool ok, size_t c) -> T {
-    return (ok && j >= 0 && j < ny) ? p[(size_t)j * nx + c] : T(0);
+    if (ROWS) return (ok && j >= 0 && j < ny) ? p[(size_t)j * nx + c] : T(0);
+    return ok ? p[(size_t)j * nx + c] : T(0);
   };
   auto load_row = [&](int j) {
     MarchRow<T> r;
-    const bool live = j < y1;
+    const bool live = !ROWS || j < y1;
     r.h2 = at(H, j + 2, live && col, ic);
     r.v1 = at(a.v, j + 1, live && col, ic);
     r.u = at(a.u, j, live && col, ic);
@@ -246,6 +243,21 @@ __global__ void __launch_bounds__(kTmWarps * 32) transport_march_kernel(const Tr
     r1 = r3;
   }
   (void)hm1;
+}
+
+template <typename T, int SLOPE>
+__global__ void __launch_bounds__(kTmWarps * 32) transport_march_kernel(const TransportArgs<T> a, int n_strips,
+                                                                       int rows_per_seg) {
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * kTmWarps + (threadIdx.x >> 5);
+  const int strip = gw % n_strips, seg = gw / n_strips;
+  const int y0 = seg * rows_per_seg;
+  if (y0 >= a.ny) return;  // uniform per warp
+  const int y1 = min(y0 + rows_per_seg, a.ny);
+  if (y0 >= 2 && y1 + 5 <= a.ny)  // every row loaded (y0-2 .. y1+4) is in the domain
+    transport_march<T, SLOPE, false>(a, lane, strip, y0, y1);
+  else
+    transport_march<T, SLOPE, true>(a, lane, strip, y0, y1);
 }
 
 template <typename T>
