@@ -104,6 +104,7 @@ SIGNATURES = {
     "igm_cnn_wgrad_finish_split": (I, [P, I, I, P, P]),
     "igm_cnn_head_backward_tc": (I, [I, I, I, I, P, P, P, P, C.c_float, C.c_float, P, P, P, I, P]),
     "igm_cnn_head_wgrad_finish": (I, [P, I, I, P, P]),
+    "igm_cnn_input_gradient": (I, [I, I, I, I, P, P, P, P, P]),
     "igm_adam_clipnorm": (I, [I, P, P, P, P, P, P, D, D, D, D, D, C.c_int64, P]),
 }
 

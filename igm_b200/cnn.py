@@ -193,9 +193,11 @@ class CNN:
         return buf["U"], buf["V"]
 
     # ---- backward ----------------------------------------------------------
-    def backward(self, buf, B, h, w, dU, dV):
+    def backward(self, buf, B, h, w, dU, dV, field_grad=None):
         """Gradients of the parameters into self.grads, given dE/dU, dE/dV
-        (planar [B, nz, h, w]); requires forward(keep_acts=True)."""
+        (planar [B, nz, h, w]); requires forward(keep_acts=True).  With
+        ``field_grad`` (float32 [B, cin, h, w]) also the gradient with respect
+        to the raw input fields (igm_cnn_input_gradient)."""
         lib, st = L.lib(), L.stream_ptr()
         acts = buf["acts"]
         npart, npart2 = buf["npart"], buf["npart2"]
@@ -239,6 +241,11 @@ class CNN:
                 rc = lib.igm_cnn_wgrad_finish(_p(buf["wpart"]), npart, F, F, gp + 4 * self.offsets[2 * l], st)
                 L.check(rc, "igm_cnn_wgrad_finish")
             else:
+                if field_grad is not None:
+                    sc = (C.c_double * self.cin)(*[float(x) for x in self.scales[:self.cin]])
+                    rc = lib.igm_cnn_input_gradient(B, h, w, self.cin, _p(gl), self.params.data_ptr(), sc,
+                                                    _p(field_grad), st)
+                    L.check(rc, "igm_cnn_input_gradient")
                 rc = lib.igm_conv3x3_wgrad(B, h, w, 16, _p(buf["X"]), _p(gl), _p(buf["wpart"]), npart,
                                            _p(self.err), st)
                 L.check(rc, "igm_conv3x3_wgrad layer 0")

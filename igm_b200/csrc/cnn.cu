@@ -897,6 +897,60 @@ static int grid_for(size_t n, int per = 256) {
   return (int)(b < 1 ? 1 : b);
 }
 
+// ---------------------------------------------------------------------------
+// Input gradient of the first layer: from dPre0 (the gradient of the first
+// layer's pre-activation, bf16 row-chunked [B][H][4][W][8], as the second
+// layer's dgrad leaves it) to the gradient of each raw input field,
+//   dField_c[y][x] = scale_c sum_{kh,kw,co} dPre0[y-kh+1][x-kw+1][co] W0[kh][kw][c][co]
+// with the FP32 weights (the transposed "same" convolution; the BF16 split of
+// the inputs is a representation of the same x, so its gradient is x's).
+// One pixel per thread, the weights in shared memory.
+// ---------------------------------------------------------------------------
+struct InputGradScales { float s[8]; };
+
+template <int CIN>
+__global__ void __launch_bounds__(256) input_grad_kernel(int B, int H, int W, const __nv_bfloat16* dpre,
+                                                         const float* w0, InputGradScales sc, float* out) {
+  __shared__ float sw[9 * CIN * kF];  // [tap][c][co]
+  for (int i = threadIdx.x; i < 9 * CIN * kF; i += blockDim.x) sw[i] = w0[i];
+  __syncthreads();
+  const size_t plane = (size_t)H * W;
+  const size_t total = plane * B;
+  const uint4* D = reinterpret_cast<const uint4*>(dpre);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t b = i / plane, rem = i - b * plane;
+    const int y = (int)(rem / W), x = (int)(rem - (size_t)(rem / W) * W);
+    float acc[CIN];
+#pragma unroll
+    for (int c = 0; c < CIN; ++c) acc[c] = 0.f;
+#pragma unroll
+    for (int kh = 0; kh < 3; ++kh) {
+      const int yy = y - kh + 1;
+      if (yy < 0 || yy >= H) continue;
+#pragma unroll
+      for (int kw = 0; kw < 3; ++kw) {
+        const int xx = x - kw + 1;
+        if (xx < 0 || xx >= W) continue;
+        const float* wt = sw + (kh * 3 + kw) * CIN * kF;
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch) {
+          const uint4 u = D[((b * H + yy) * 4 + ch) * W + xx];
+          const uint32_t wv[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const int co = ch * 8 + e;
+            const float d = (e & 1) ? bf_hi(wv[e >> 1]) : bf_lo(wv[e >> 1]);
+#pragma unroll
+            for (int c = 0; c < CIN; ++c) acc[c] = fmaf(d, wt[c * kF + co], acc[c]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CIN; ++c) out[(b * CIN + c) * plane + rem] = acc[c] * sc.s[c];
+  }
+}
+
 }  // namespace igm
 
 using namespace igm;
@@ -1144,4 +1198,25 @@ extern "C" int igm_adam_clipnorm(int n_vars, const size_t* var_offsets, float* p
   adam_kernel<<<grid_for(vars.off[n_vars]), 256, 0, st>>>(params, grads, m, v, vars, norms, lr_t, (float)beta_1,
                                                          (float)beta_2, (float)epsilon, (float)clipnorm);
   return launch_status("adam_kernel");
+}
+
+extern "C" int igm_cnn_input_gradient(int batch, int h, int w, int cin, const void* dpre0, const float* w0,
+                                      const double* scales, float* out, void* stream) {
+  IGM_CHECK_ARG(batch >= 1 && h >= 1 && w >= 1 && cin >= 1 && cin <= 8, IGM_ERR_BAD_SHAPE,
+                "igm_cnn_input_gradient: bad shape");
+  IGM_CHECK_ARG(dpre0 && w0 && scales && out, IGM_ERR_BAD_ARGUMENT, "igm_cnn_input_gradient: NULL argument");
+  InputGradScales sc{};
+  for (int c = 0; c < cin; ++c) sc.s[c] = (float)scales[c];
+  const int grid = grid_for((size_t)batch * h * w);
+  cudaStream_t st = as_stream(stream);
+  const __nv_bfloat16* d = (const __nv_bfloat16*)dpre0;
+  switch (cin) {
+#define IGM_IG(C)                                                                      \
+  case C:                                                                              \
+    input_grad_kernel<C><<<grid, 256, 0, st>>>(batch, h, w, d, w0, sc, out);           \
+    break;
+    IGM_IG(1) IGM_IG(2) IGM_IG(3) IGM_IG(4) IGM_IG(5) IGM_IG(6) IGM_IG(7) IGM_IG(8)
+#undef IGM_IG
+  }
+  return launch_status("input_grad_kernel");
 }

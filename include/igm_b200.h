@@ -386,6 +386,17 @@ IGM_API int igm_cnn_head_backward_tc(int batch, int h, int w, int nz, const void
  * (the centre tap), nout <= 32. */
 IGM_API int igm_cnn_head_wgrad_finish(const float* partials, int n_parts, int nout, float* out, void* stream);
 
+/* Gradient of the emulator's output with respect to its raw input fields
+ * (the gradient tf.GradientTape takes through the Keras model to the fields
+ * in data assimilation, igm/processes/data_assimilation/optimize/update.py:
+ * 37-70): from dpre0, the gradient of the first layer's pre-activation (bf16
+ * [batch][h][4][w][8], as the second layer's dgrad of igm_conv3x3 leaves it),
+ * and the first layer's FP32 kernel w0 [3][3][cin][32] (Keras layout),
+ *   out[b][c][y][x] = scales[c] sum_{kh,kw,co} dpre0[b][y-kh+1][x-kw+1][co] w0[kh][kw][c][co]
+ * (zero "same" padding); scales: host double[cin], the fixed input scales. */
+IGM_API int igm_cnn_input_gradient(int batch, int h, int w, int cin, const void* dpre0, const float* w0,
+                                   const double* scales, float* out, void* stream);
+
 /* out[i] (+)= sum_p partials[p * stride + i], i < len, fixed summation order. */
 IGM_API int igm_reduce_partials(const float* partials, int n_parts, int len, int stride, float* out,
                                 int accumulate, void* stream);

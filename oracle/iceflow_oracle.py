@@ -687,3 +687,104 @@ class Clock:
         if it >= 0:
             self.t = np.float32(self.t + self.dt)
         self.continue_run = bool(self.t < self.end)
+
+
+# --------------------------------------------------------------------------
+# data assimilation: cost terms of the default configuration
+# (igm/processes/data_assimilation/cost_terms/*.py, utils.py)
+# --------------------------------------------------------------------------
+
+
+@dataclass
+class AssimParams:
+    velsurfobs_std: float = 1.0
+    velsurfobs_thr: float = 0.0
+    thkobs_std: float = 3.0
+    regu_thk: float = 10.0
+    convexity_weight: float = 0.002
+    convexity_power: float = 1.3
+    smooth_anisotropy_factor: float = 0.2
+    to_regularize: str = "topg"
+    penalty: bool = True
+    icemask_cost: bool = True
+
+
+def getmag(u, v):
+    """igm/utils/math/getmag.py: the Euclidean norm of (u, v)."""
+    return torch.sqrt(u * u + v * v)
+
+
+def da_flow_direction(uvelsurf, vvelsurf):
+    """compute_flow_direction_for_anisotropic_smoothing (utils.py:86-110): the
+    cell average of the surface velocity, smoothed by a Gaussian of 3 cells
+    (scipy, zero outside), normalised -- the y component with the already
+    normalised x component, as in the reference -- zero where undefined.
+    Returns float32 [Ny-1, Nx-1] tensors (constants of the gradient)."""
+    from scipy.ndimage import gaussian_filter
+    u = torch.where(torch.isnan(uvelsurf), torch.zeros_like(uvelsurf), uvelsurf)
+    v = torch.where(torch.isnan(vvelsurf), torch.zeros_like(vvelsurf), vvelsurf)
+    fx = (u[1:, 1:] + u[:-1, 1:] + u[1:, :-1] + u[:-1, :-1]) / 4.0
+    fy = (v[1:, 1:] + v[:-1, 1:] + v[1:, :-1] + v[:-1, :-1]) / 4.0
+    fx = torch.as_tensor(gaussian_filter(fx.detach().numpy(), 3, mode="constant"))
+    fy = torch.as_tensor(gaussian_filter(fy.detach().numpy(), 3, mode="constant"))
+    fx = fx / getmag(fx, fy)
+    fy = fy / getmag(fx, fy)
+    fx = torch.where(torch.isnan(fx), torch.zeros_like(fx), fx)
+    fy = torch.where(torch.isnan(fy), torch.zeros_like(fy), fy)
+    return fx, fy
+
+
+def da_costs(thk, usurf, uvelsurf, vvelsurf, uobs, vobs, thkobs, dens_thkobs, icemaskobs, icemask, flowdir, dx,
+             p: AssimParams):
+    """The cost terms of total_cost (cost_terms/total_cost.py:13-70) for
+    control ``thk``, costs velsurf + thk + icemask and the penalty
+    constraint: misfit_velsurf.py:8-19, misfit_thk.py:8-16, the icemask and
+    positive-thickness penalties (total_cost.py:36-46) and regu_thk.py:8-70
+    (to_regularize topg or thk, fix_opti_normalization_issue off).  Returns a
+    dict of scalar tensors."""
+    cost = {}
+    vs = torch.stack([uvelsurf, vvelsurf], -1)
+    vo = torch.stack([uobs, vobs], -1)
+    rel = (torch.linalg.vector_norm(vo, dim=-1) >= p.velsurfobs_thr)[..., None]
+    act = ~torch.isnan(vo)
+    m = act & rel
+    cost["velsurf"] = 0.5 * torch.mean(((vo[m] - vs[m]) / p.velsurfobs_std) ** 2)
+    a = ~torch.isnan(thkobs)
+    cost["thk"] = 0.5 * torch.mean(dens_thkobs[a] * ((thkobs[a] - thk[a]) / p.thkobs_std) ** 2)
+    z = torch.zeros_like(thk)
+    if p.penalty:
+        if p.icemask_cost:
+            cost["icemask"] = 10 ** 10 * torch.mean(torch.where(icemaskobs > 0.5, z, thk ** 2))
+        cost["thk_positive"] = 10 ** 10 * torch.mean(torch.where(thk >= 0, z, thk ** 2))
+    area = torch.sum(torch.where(icemask > 0.5, 1.0, 0.0)) * dx ** 2
+    gamma = p.convexity_weight * area ** (p.convexity_power - 2.0)
+    field = usurf - thk if p.to_regularize == "topg" else thk
+    f = p.smooth_anisotropy_factor
+    if f == 1:
+        dbdx = (field[:, 1:] - field[:, :-1]) / dx
+        dbdy = (field[1:, :] - field[:-1, :]) / dx
+        cost["thk_regu"] = p.regu_thk * (torch.sum(dbdx ** 2) / 2 + torch.sum(dbdy ** 2) / 2 - gamma * torch.sum(thk))
+    else:
+        fx, fy = flowdir
+        dbdx = (field[:, 1:] - field[:, :-1]) / dx
+        dbdx = (dbdx[1:, :] + dbdx[:-1, :]) / 2.0
+        dbdy = (field[1:, :] - field[:-1, :]) / dx
+        dbdy = (dbdy[:, 1:] + dbdy[:, :-1]) / 2.0
+        cost["thk_regu"] = p.regu_thk * (
+            (1.0 / np.sqrt(f)) * torch.sum((dbdx * fx + dbdy * fy) ** 2) / 2
+            + np.sqrt(f) * torch.sum((dbdx * fy - dbdy * fx) ** 2) / 2
+            - torch.sum(gamma * thk))
+    return cost
+
+
+def divflux_upwind(u, v, h, dx):
+    """compute_divflux, method upwind (utils/gradient/compute_divflux.py:17-33,
+    45-46): face velocities (edge copies at the border), upwind thickness with
+    zero outside, divergence."""
+    uf = torch.cat([u[:, 0:1], 0.5 * (u[:, :-1] + u[:, 1:]), u[:, -1:]], 1)
+    vf = torch.cat([v[0:1, :], 0.5 * (v[:-1, :] + v[1:, :]), v[-1:, :]], 0)
+    Hx = torch.nn.functional.pad(h, (1, 1, 0, 0))
+    Hy = torch.nn.functional.pad(h, (0, 0, 1, 1))
+    Qx = uf * torch.where(uf > 0, Hx[:, :-1], Hx[:, 1:])
+    Qy = vf * torch.where(vf > 0, Hy[:-1, :], Hy[1:, :])
+    return (Qx[:, 1:] - Qx[:, :-1]) / dx + (Qy[1:, :] - Qy[:-1, :]) / dx

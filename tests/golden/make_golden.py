@@ -49,7 +49,8 @@ for pkg in ["", "processes", "processes/iceflow", "processes/iceflow/energy",
             "processes/iceflow/energy/sliding_laws", "processes/iceflow/emulate",
             "processes/iceflow/emulate/emulators", "processes/iceflow/solve",
             "processes/iceflow/diagnostic", "processes/thk", "processes/time", "processes/vert_flow",
-            "utils", "utils/gradient", "utils/math"]:
+            "utils", "utils/gradient", "utils/math", "processes/data_assimilation",
+            "processes/data_assimilation/cost_terms"]:
     _stub("igm" + ("." + pkg.replace("/", ".") if pkg else ""), os.path.join(IGM, pkg))
 
 energy_pkg = sys.modules["igm.processes.iceflow.energy"]
@@ -345,6 +346,71 @@ def keras_h5_cases():
     print(f"wrote {dst} ({os.path.getsize(dst)} B)")
 
 
+def assim_cases():
+    """The data-assimilation cost terms of the default configuration (control
+    thk; costs velsurf, thk, icemask; penalty constraint; anisotropic and
+    isotropic thickness regularisation), executed from the reference's files
+    (cost_terms/misfit_velsurf.py, misfit_thk.py, regu_thk.py, the penalties of
+    total_cost.py:36-46, utils.py create_density_matrix and
+    compute_flow_direction_for_anisotropic_smoothing), with torch autograd
+    gradients w.r.t. thk and the surface velocities."""
+    dau = importlib.import_module("igm.processes.data_assimilation.utils")
+    mv = importlib.import_module("igm.processes.data_assimilation.cost_terms.misfit_velsurf")
+    mt = importlib.import_module("igm.processes.data_assimilation.cost_terms.misfit_thk")
+    rt = importlib.import_module("igm.processes.data_assimilation.cost_terms.regu_thk")
+    out = {}
+    for tag, dtype, aniso, reg in [("f64", torch.float64, True, "topg"), ("f32", torch.float32, True, "topg"),
+                                   ("iso_f64", torch.float64, False, "topg"), ("thk_f64", torch.float64, True, "thk")]:
+        rng = np.random.default_rng(11)
+        ny, nx, dx = 23, 31, 100.0
+        g = glacier(ny, nx, dx, 12, dtype)
+        f = lambda a: torch.as_tensor(np.asarray(a), dtype=dtype)  # noqa: E731
+        thk = g["thk"] + f(rng.normal(0, 10, (ny, nx)))  # some negative values: the penalty is active
+        usurf = g["usurf"]
+        icemaskobs = f((g["thk"].numpy() > 0).astype(np.float64))
+        uvs, vvs = f(rng.normal(20, 15, (ny, nx))), f(rng.normal(-5, 15, (ny, nx)))
+        uo, vo = f(rng.normal(20, 15, (ny, nx))), f(rng.normal(-5, 15, (ny, nx)))
+        uo[rng.uniform(size=(ny, nx)) < 0.2] = float("nan")
+        vo[rng.uniform(size=(ny, nx)) < 0.1] = float("nan")
+        thkobs = torch.full_like(thk, float("nan"))
+        thkobs[:, 7] = g["thk"][:, 7] + 3.0
+        thkobs[11, :] = g["thk"][11, :] - 2.0
+        cfg = load_cfg()
+        with open(os.path.join(IGM, "conf", "processes", "data_assimilation.yaml")) as fh:
+            da = yaml.safe_load(fh)["data_assimilation"]
+        da["regularization"]["smooth_anisotropy_factor"] = 0.2 if aniso else 1.0
+        da["regularization"]["to_regularize"] = reg
+        da.setdefault("cook", {"infer_params": False})
+        cfg.processes.data_assimilation = ns(da)
+        dens = dau.create_density_matrix(thkobs, kernel_size=5)
+        dens = torch.where(dens > 0, 1.0 / dens, torch.zeros_like(dens))
+        dens = torch.where(torch.isnan(thkobs), torch.zeros_like(dens), dens)
+        dens = dens / torch.mean(dens[dens > 0])
+        thk_v = thk.clone().requires_grad_(True)
+        uvs_v, vvs_v = uvs.clone().requires_grad_(True), vvs.clone().requires_grad_(True)
+        st = types.SimpleNamespace(thk=thk_v, usurf=usurf, uvelsurf=uvs_v, vvelsurf=vvs_v, uvelsurfobs=uo,
+                                   vvelsurfobs=vo, thkobs=thkobs, dens_thkobs=dens, icemaskobs=icemaskobs,
+                                   icemask=icemaskobs, dx=dx)
+        if aniso:
+            dau.compute_flow_direction_for_anisotropic_smoothing(st)
+            fx, fy = f(np.asarray(st.flowdirx)), f(np.asarray(st.flowdiry))
+            st.flowdirx, st.flowdiry = fx, fy
+        else:
+            fx = fy = torch.zeros((ny - 1, nx - 1), dtype=dtype)
+        c_vel = mv.misfit_velsurf(cfg, st)
+        c_thk = mt.misfit_thk(cfg, st)
+        c_ice = 10 ** 10 * torch.mean(torch.where(icemaskobs > 0.5, torch.zeros_like(thk_v), thk_v ** 2))
+        c_pos = 10 ** 10 * torch.mean(torch.where(thk_v >= 0, torch.zeros_like(thk_v), thk_v ** 2))
+        c_reg = rt.regu_thk(cfg, st)
+        total = c_vel + c_thk + c_ice + c_pos + c_reg
+        gt, gu, gv = torch.autograd.grad(total, [thk_v, uvs_v, vvs_v])
+        out.update({f"{tag}_{k}": v for k, v in dict(
+            thk=thk, usurf=usurf, icemaskobs=icemaskobs, uvs=uvs, vvs=vvs, uobs=uo, vobs=vo, thkobs=thkobs,
+            dens=dens, flowdirx=fx, flowdiry=fy, c_vel=c_vel, c_thk=c_thk, c_ice=c_ice, c_pos=c_pos, c_reg=c_reg,
+            g_thk=gt, g_u=gu, g_v=gv, dx=np.asarray(dx), aniso=np.asarray(aniso), to_thk=np.asarray(reg == "thk")).items()})
+    save("assim", out)
+
+
 def save(name, d):
     arrs = {}
     for k, v in d.items():
@@ -372,3 +438,4 @@ if __name__ == "__main__":
     emulator_case()
     vert_flow_cases()
     keras_h5_cases()
+    assim_cases()

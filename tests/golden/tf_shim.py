@@ -215,6 +215,24 @@ def pad(x, paddings, mode="CONSTANT", constant_values=0):
     raise NotImplementedError(mode)
 
 
+def _conv2d(x, k, strides=None, padding="SAME"):
+    """tf.nn.conv2d, NHWC input and HWIO filter, stride 1, SAME or VALID padding."""
+    xt = x.permute(0, 3, 1, 2)
+    kt = k.permute(3, 2, 0, 1).to(xt.dtype)
+    pad = (k.shape[0] // 2) if padding == "SAME" else 0
+    y = torch.nn.functional.conv2d(xt, kt, padding=pad)
+    return y.permute(0, 2, 3, 1)
+
+
+math = types.SimpleNamespace(is_nan=torch.isnan, reduce_mean=lambda x, axis=None: reduce_mean(x, axis),
+                             reduce_sum=lambda x, axis=None: reduce_sum(x, axis), log=torch.log)
+nn = types.SimpleNamespace(l2_loss=lambda x: torch.sum(x * x) / 2, conv2d=_conv2d)
+
+
+def squeeze(x, axis=None):
+    return torch.squeeze(x) if axis is None else torch.squeeze(x, axis)
+
+
 experimental = types.SimpleNamespace(numpy=types.SimpleNamespace(
     moveaxis=lambda x, src, dst: torch.movedim(x, src, dst)))
 

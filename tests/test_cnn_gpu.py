@@ -110,3 +110,31 @@ def test_physics_gradient_and_adam_step_match_oracle():
         dn = new[net.offsets[i]:net.offsets[i + 1]] - old[net.offsets[i]:net.offsets[i + 1]]
         do = (xs[i] - params[i].detach()).numpy().ravel()
         assert rel_l2(dn, do) < 1e-4, (i, rel_l2(dn, do))
+
+
+def test_input_field_gradient_matches_oracle():
+    """d(sum U RU + V RV)/d(fields) through the whole network (the gradient data
+    assimilation takes to its control fields), against torch autograd of the
+    oracle network; relative L2 per field <= 5e-2 (bf16 activations)."""
+    nl, nz, ny, nx, dx = 3, 4, 40, 70, 100.0
+    st, net, f = setup(nl, nz, ny, nx, seed=5)
+    ws, bs = oracle_params(net)
+    rng = np.random.default_rng(9)
+    RU = rng.normal(0, 1, (1, nz, ny, nx)).astype(np.float32)
+    RV = rng.normal(0, 1, (1, nz, ny, nx)).astype(np.float32)
+    fl = [torch.as_tensor(st[k]).clone().requires_grad_(True) for k in ["thk", "usurf", "arrhenius", "slidingco"]]
+    X = O.fieldin_to_X(fl + [torch.full_like(fl[0], dx)]) * torch.tensor(SCALES, dtype=torch.float32)
+    Y = O.cnn_forward(X, ws, bs, bf16=True, bf16_first=False, out_scale=OUT)
+    Uo, Vo = O.Y_to_UV(Y, nz)
+    loss = (Uo * torch.as_tensor(RU)).sum() + (Vo * torch.as_tensor(RV)).sum()
+    go = torch.autograd.grad(loss, fl)
+    buf = net.buffers(1, ny, nx, train=True)
+    net.prepare_input(f, dx, [(0, 0)], ny, nx, buf)
+    net.forward(buf, 1, ny, nx, keep_acts=True)
+    G = torch.zeros((1, 5, ny, nx), dtype=torch.float32, device="cuda")
+    net.backward(buf, 1, ny, nx, torch.as_tensor(RU).cuda(), torch.as_tensor(RV).cuda(), field_grad=G)
+    net.check_errors()
+    G = G.cpu().numpy()[0]
+    for c in range(4):
+        e = rel_l2(G[c], go[c].numpy())
+        assert e < 5e-2, (c, e)

@@ -178,3 +178,44 @@ def test_vertical_velocity_incompressibility(golden, tag):
                                               T(g[f"{tag}_thk"]), T(g[f"{tag}_levels"]),
                                               T(g[f"{tag}_weight"])[:, None, None], float(g[f"{tag}_dx"]))
     np.testing.assert_array_equal(W.numpy(), g[f"{tag}_Wi"])
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32", "iso_f64", "thk_f64"])
+def test_assimilation_costs_and_gradients(golden, tag):
+    """The data-assimilation cost terms and their gradients w.r.t. thk and the
+    surface velocities, against the reference's cost_terms executed on the
+    same inputs (FP64 to 1e-10: sums in another order; FP32 to 1e-5); the flow directions of the
+    anisotropic regularisation against the reference's utils."""
+    g = {k[len(tag) + 1:]: v for k, v in golden("assim").items() if k.startswith(tag + "_")}
+    thk = T(g["thk"]).clone().requires_grad_(True)
+    uvs, vvs = T(g["uvs"]).clone().requires_grad_(True), T(g["vvs"]).clone().requires_grad_(True)
+    if bool(g["aniso"]):
+        fx, fy = O.da_flow_direction(T(g["uvs"]), T(g["vvs"]))
+        tol_f = 1e-6 if g["thk"].dtype == np.float64 else 1e-5
+        np.testing.assert_allclose(fx.numpy(), g["flowdirx"], rtol=tol_f, atol=tol_f)
+        np.testing.assert_allclose(fy.numpy(), g["flowdiry"], rtol=tol_f, atol=tol_f)
+        flow = (T(g["flowdirx"]), T(g["flowdiry"]))
+        f = 0.2
+    else:
+        flow, f = None, 1.0
+    p = O.AssimParams(smooth_anisotropy_factor=f, to_regularize="thk" if bool(g["to_thk"]) else "topg")
+    c = O.da_costs(thk, T(g["usurf"]), uvs, vvs, T(g["uobs"]), T(g["vobs"]), T(g["thkobs"]), T(g["dens"]),
+                   T(g["icemaskobs"]), T(g["icemaskobs"]), flow, float(g["dx"]), p)
+    tol = 1e-10 if g["thk"].dtype == np.float64 else 1e-5
+    for k, ref in [("velsurf", "c_vel"), ("thk", "c_thk"), ("icemask", "c_ice"), ("thk_positive", "c_pos"),
+                   ("thk_regu", "c_reg")]:
+        np.testing.assert_allclose(float(c[k]), float(g[ref]), rtol=tol, atol=tol * abs(float(g[ref])) + 1e-30)
+    gt, gu, gv = torch.autograd.grad(sum(c.values()), [thk, uvs, vvs])
+    for a, ref in [(gt, "g_thk"), (gu, "g_u"), (gv, "g_v")]:
+        np.testing.assert_allclose(a.numpy(), g[ref], rtol=tol, atol=tol * np.abs(g[ref]).max())
+
+
+def test_divflux_upwind_conserves_mass():
+    """compute_divflux, upwind: zero flux through the border for ice away from
+    it, so the divergence sums to zero."""
+    ny = nx = 40
+    y, x = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    h = T(np.maximum(0, 100 - ((y - 20) ** 2 + (x - 20) ** 2)).astype(np.float64))
+    u = T(np.full((ny, nx), 7.0)); v = T(np.full((ny, nx), -3.0))
+    d = O.divflux_upwind(u, v, h, 50.0)
+    assert abs(float(d.sum())) < 1e-9 * float(h.sum())
