@@ -51,6 +51,13 @@ class Adam(C.Structure):
     _fields_ = [("lr", C.c_double), ("beta_1", C.c_double), ("beta_2", C.c_double), ("epsilon", C.c_double)]
 
 
+class AssimParams(C.Structure):
+    _fields_ = [("velsurfobs_std", C.c_double), ("velsurfobs_thr", C.c_double), ("thkobs_std", C.c_double),
+                ("regu_thk", C.c_double), ("gamma", C.c_double), ("aniso_factor", C.c_double), ("n_vel", C.c_double),
+                ("n_thk", C.c_double), ("penalty", C.c_int32), ("icemask_cost", C.c_int32),
+                ("regularize_thk", C.c_int32), ("mask_velsurf", C.c_int32)]
+
+
 class EarlyStop(C.Structure):
     _fields_ = [("relative_min_delta", C.c_double), ("patience", C.c_int32), ("enabled", C.c_int32)]
 
@@ -105,6 +112,10 @@ SIGNATURES = {
     "igm_cnn_head_backward_tc": (I, [I, I, I, I, P, P, P, P, C.c_float, C.c_float, P, P, P, I, P]),
     "igm_cnn_head_wgrad_finish": (I, [P, I, I, P, P]),
     "igm_cnn_input_gradient": (I, [I, I, I, I, P, P, P, P, P]),
+    "igm_assim_cost_grad": (I, [I, I, I, D] + [P] * 12 + [P, P, P, P, I, P, P]),
+    "igm_assim_flow_direction": (I, [I, I, I, P, P, P, P, P, P]),
+    "igm_divflux_upwind": (I, [I, I, I, D, P, P, P, P, P]),
+    "igm_assim_control": (I, [I, I, C.c_size_t, D, I, I, P, P, P, P, P, P, P, P, P]),
     "igm_adam_clipnorm": (I, [I, P, P, P, P, P, P, D, D, D, D, D, C.c_int64, P]),
 }
 

@@ -30,6 +30,7 @@ UNITS = {
     "fields.cu": ["-fmad=false"],
     "conv.cu": [],
     "cnn.cu": [],
+    "assim.cu": [],
 }
 
 

@@ -577,6 +577,30 @@ __global__ void __launch_bounds__(kVfWarps * 32) vert_flow_incomp_kernel(const V
   }
 }
 
+// compute_divflux, method upwind (igm/utils/gradient/compute_divflux.py:17-33,
+// 45-46): face velocities with edge copies at the border, the upwind
+// thickness (zero outside), and the divergence; bit-identical to the reference.
+template <typename T>
+__global__ void divflux_upwind_kernel(int ny, int nx, T dx, T rdx, const T* u, const T* v, const T* h, T* out) {
+  const size_t n = (size_t)ny * nx;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(o / nx), i = (int)(o - (size_t)j * nx);
+    auto hh = [&](int jj, int ii) { return (jj < 0 || jj >= ny || ii < 0 || ii >= nx) ? T(0) : h[(size_t)jj * nx + ii]; };
+    auto uu = [&](int ii) { return u[(size_t)j * nx + ii]; };
+    auto vv = [&](int jj) { return v[(size_t)jj * nx + i]; };
+    // x faces i (west) and i+1 (east)
+    const T uw = i == 0 ? uu(0) : T(0.5) * (uu(i - 1) + uu(i));
+    const T ue = i == nx - 1 ? uu(nx - 1) : T(0.5) * (uu(i) + uu(i + 1));
+    const T qw = uw * (uw > T(0) ? hh(j, i - 1) : hh(j, i));
+    const T qe = ue * (ue > T(0) ? hh(j, i) : hh(j, i + 1));
+    const T vs = j == 0 ? vv(0) : T(0.5) * (vv(j - 1) + vv(j));
+    const T vn = j == ny - 1 ? vv(ny - 1) : T(0.5) * (vv(j) + vv(j + 1));
+    const T qs = vs * (vs > T(0) ? hh(j - 1, i) : hh(j, i));
+    const T qn = vn * (vn > T(0) ? hh(j, i) : hh(j + 1, i));
+    out[o] = div_dx(qe - qw, dx, rdx) + div_dx(qn - qs, dx, rdx);
+  }
+}
+
 template <typename T>
 static int vert_flow_t(int nz, int ny, int nx, double dx, const void* U, const void* V, const void* topg,
                        const void* thk, const double* levels, const double* vert_weight, void* W, bool incomp,
@@ -736,4 +760,24 @@ extern "C" int igm_vertical_velocity_incompressibility(int dtype, int nz, int ny
   if (dtype == IGM_F64) return vert_flow_t<double>(nz, ny, nx, dx, U, V, topg, thk, levels, vert_weight, W, true, st);
   set_error("igm_vertical_velocity_incompressibility: unknown dtype %d", dtype);
   return IGM_ERR_BAD_ARGUMENT;
+}
+
+extern "C" int igm_divflux_upwind(int dtype, int ny, int nx, double dx, const void* u, const void* v, const void* h,
+                                  void* out, void* stream) {
+  IGM_CHECK_ARG(ny >= 2 && nx >= 2 && dx > 0, IGM_ERR_BAD_SHAPE, "igm_divflux_upwind: bad shape or dx");
+  IGM_CHECK_ARG(u && v && h && out, IGM_ERR_BAD_ARGUMENT, "igm_divflux_upwind: NULL argument");
+  cudaStream_t st = as_stream(stream);
+  const int grid = grid1d((size_t)ny * nx);
+  if (dtype == IGM_F32) {
+    const float d = (float)dx;
+    divflux_upwind_kernel<float><<<grid, 256, 0, st>>>(ny, nx, d, 1.0f / d, (const float*)u, (const float*)v,
+                                                       (const float*)h, (float*)out);
+  } else if (dtype == IGM_F64) {
+    divflux_upwind_kernel<double><<<grid, 256, 0, st>>>(ny, nx, dx, 1.0 / dx, (const double*)u, (const double*)v,
+                                                        (const double*)h, (double*)out);
+  } else {
+    set_error("igm_divflux_upwind: unknown dtype %d", dtype);
+    return IGM_ERR_BAD_ARGUMENT;
+  }
+  return launch_status("divflux_upwind_kernel");
 }

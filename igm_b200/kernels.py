@@ -155,3 +155,45 @@ def absmax2(a, b, out=None):
     rc = L.lib().igm_absmax2(L.dtype_code(a.dtype), a.numel(), L.ptr(a), L.ptr(b), L.ptr(vm), L.stream_ptr())
     L.check(rc, "igm_absmax2")
     return vm
+
+
+def assim_cost_grad(thk, usurf, uvs, vvs, uobs, vobs, thkobs, dens, icemaskobs, flowdir, dx, params,
+                    partials=None):
+    """Cost terms (device double[5]: velsurf, thk, icemask, thk_positive,
+    thk_regu) and gradients (dC/dthk, dC/duvelsurf, dC/dvvelsurf) of the
+    default data-assimilation configuration (igm_assim_cost_grad); ``params``
+    an _lib.AssimParams, ``flowdir`` (fx, fy) [ny-1, nx-1] or None."""
+    ny, nx = thk.shape
+    n_parts = 148 * 8
+    if partials is None:
+        partials = torch.empty(n_parts * 5, dtype=torch.float64, device=thk.device)
+    costs = torch.empty(5, dtype=torch.float64, device=thk.device)
+    g_thk, g_u, g_v = torch.empty_like(thk), torch.empty_like(thk), torch.empty_like(thk)
+    fx, fy = flowdir if flowdir is not None else (None, None)
+    rc = L.lib().igm_assim_cost_grad(L.dtype_code(thk.dtype), ny, nx, float(dx), L.ptr(thk), L.ptr(usurf),
+                                     L.ptr(uvs), L.ptr(vvs), L.ptr(uobs), L.ptr(vobs), L.ptr(thkobs), L.ptr(dens),
+                                     L.ptr(icemaskobs), L.ptr(fx), L.ptr(fy), C.byref(params), L.ptr(g_thk),
+                                     L.ptr(g_u), L.ptr(g_v), L.ptr(partials), partials.numel() // 5, L.ptr(costs),
+                                     L.stream_ptr())
+    L.check(rc, "igm_assim_cost_grad")
+    return costs, g_thk, g_u, g_v
+
+
+def assim_flow_direction(uvs, vvs):
+    """Flow directions [ny-1, nx-1] of the anisotropic regularisation."""
+    ny, nx = uvs.shape
+    fx = torch.empty((ny - 1, nx - 1), dtype=uvs.dtype, device=uvs.device)
+    fy, scratch = torch.empty_like(fx), torch.empty_like(fx)
+    rc = L.lib().igm_assim_flow_direction(L.dtype_code(uvs.dtype), ny, nx, L.ptr(uvs), L.ptr(vvs), L.ptr(fx),
+                                          L.ptr(fy), L.ptr(scratch), L.stream_ptr())
+    L.check(rc, "igm_assim_flow_direction")
+    return fx, fy
+
+
+def divflux_upwind(u, v, h, dx, out=None):
+    ny, nx = h.shape
+    out = out if out is not None else torch.empty_like(h)
+    rc = L.lib().igm_divflux_upwind(L.dtype_code(h.dtype), ny, nx, float(dx), L.ptr(u), L.ptr(v), L.ptr(h),
+                                    L.ptr(out), L.stream_ptr())
+    L.check(rc, "igm_divflux_upwind")
+    return out

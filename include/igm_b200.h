@@ -261,6 +261,71 @@ IGM_API int igm_vertical_velocity_incompressibility(int dtype, int nz, int ny, i
                                             const void* V, const void* topg, const void* thk, const double* levels,
                                             const double* vert_weight, void* W, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Data assimilation (igm/processes/data_assimilation), default configuration:
+ * control thk, costs velsurf + thk + icemask, penalty obstacle constraint,
+ * thickness regularisation.
+ * ------------------------------------------------------------------------- */
+typedef struct igm_assim_params {
+  double velsurfobs_std;   /* fitting.velsurfobs_std */
+  double velsurfobs_thr;   /* fitting.velsurfobs_thr */
+  double thkobs_std;       /* fitting.thkobs_std */
+  double regu_thk;         /* regularization.thk */
+  double gamma;            /* convexity_weight * areaicemask^(convexity_power - 2) */
+  double aniso_factor;     /* regularization.smooth_anisotropy_factor (1: isotropic branch) */
+  double n_vel;            /* number of observed velocity components used (the mean's count) */
+  double n_thk;            /* number of thickness observations */
+  int32_t penalty;         /* "penalty" in optimization.obstacle_constraint */
+  int32_t icemask_cost;    /* "icemask" in cost_list */
+  int32_t regularize_thk;  /* regularization.to_regularize == "thk" (else "topg": usurf - thk) */
+  int32_t mask_velsurf;    /* the surface velocities are where(thk > 0, U, 0): no gradient off the ice */
+} igm_assim_params;
+
+/* The cost terms of total_cost (cost_terms/total_cost.py:13-70) for the
+ * default configuration -- misfit_velsurf.py:8-19, misfit_thk.py:8-16, the
+ * icemask and positive-thickness penalties (:36-46) and regu_thk.py:8-70
+ * (fix_opti_normalization_issue off) -- and their gradients w.r.t. thk and the
+ * emulated surface velocities (uvelsurf, vvelsurf, zero where thk <= 0).
+ * Observations are NaN where missing; flowdirx/y [ny-1][nx-1] (anisotropic
+ * branch only, else NULL).  costs (device double[5]): velsurf, thk, icemask,
+ * thk_positive, thk_regu; partials: device double[n_parts * 5] scratch.
+ * All 2-D arrays [ny][nx] of the dtype. */
+IGM_API int igm_assim_cost_grad(int dtype, int ny, int nx, double dx, const void* thk, const void* usurf,
+                        const void* uvelsurf, const void* vvelsurf, const void* uvelsurfobs,
+                        const void* vvelsurfobs, const void* thkobs, const void* dens_thkobs,
+                        const void* icemaskobs, const void* flowdirx, const void* flowdiry,
+                        const igm_assim_params* params, void* grad_thk, void* grad_uvelsurf,
+                        void* grad_vvelsurf, double* partials, int n_parts, double* costs, void* stream);
+
+/* The control update around the optimizer step of optimize_update
+ * (data_assimilation/optimize/update.py:22-35, 62-103) for control thk with
+ * scaling `scale`: mode 0 (before igm_adam_clipnorm) writes the optimizer's
+ * variable thk / scale, its gradient scale (grad_direct + grad_emulator) where
+ * icemaskobs > 0.5 and 0 elsewhere, and zeroes the moments m, v (the
+ * reference re-creates the control tf.Variable at every iteration, so its Adam
+ * slots start at zero); mode 1 sets thk = variable * scale, then zero outside
+ * the ice mask (reproject_mask) and at negative values (reproject_pos).
+ * variable, grad, m, v: device float[n]; the others [n] of the dtype;
+ * grad_emulator may be NULL. */
+IGM_API int igm_assim_control(int dtype, int mode, size_t n, double scale, int reproject_mask, int reproject_pos,
+                      void* thk, const void* grad_direct, const void* grad_emulator, const void* icemaskobs,
+                      float* variable, float* grad, float* m, float* v, void* stream);
+
+/* compute_flow_direction_for_anisotropic_smoothing (data_assimilation/utils.py:
+ * 86-110): cell averages of the surface velocity (NaN as 0), a Gaussian of
+ * sigma 3 cells (radius 12, zero outside; y then x, as scipy.ndimage), then
+ * x /= |(x, y)|, y /= |(x_normalised, y)|, NaN as 0.  Outputs and scratch
+ * [ny-1][nx-1]. */
+IGM_API int igm_assim_flow_direction(int dtype, int ny, int nx, const void* uvelsurf, const void* vvelsurf,
+                             void* flowdirx, void* flowdiry, void* scratch, void* stream);
+
+/* compute_divflux, method upwind (igm/utils/gradient/compute_divflux.py:17-33,
+ * 45-46), as data assimilation computes state.divflux after each update: face
+ * velocities (edge copies at the border), upwind thickness (zero outside),
+ * d(u h)/dx + d(v h)/dy.  Bit-identical to the reference in FP32/FP64. */
+IGM_API int igm_divflux_upwind(int dtype, int ny, int nx, double dx, const void* u, const void* v, const void* h,
+                       void* out, void* stream);
+
 /* Surfaces from thickness (thk.py:11-24): lsurf = max(topg, -r thk + sealevel),
  * usurf = lsurf + thk.  lsurf may be NULL. */
 IGM_API int igm_thk_surfaces(int dtype, int n, const void* thk, const void* topg, void* lsurf, void* usurf,
