@@ -193,11 +193,12 @@ class CNN:
         return buf["U"], buf["V"]
 
     # ---- backward ----------------------------------------------------------
-    def backward(self, buf, B, h, w, dU, dV, field_grad=None):
+    def backward(self, buf, B, h, w, dU, dV, field_grad=None, param_grads=True):
         """Gradients of the parameters into self.grads, given dE/dU, dE/dV
         (planar [B, nz, h, w]); requires forward(keep_acts=True).  With
         ``field_grad`` (float32 [B, cin, h, w]) also the gradient with respect
-        to the raw input fields (igm_cnn_input_gradient)."""
+        to the raw input fields (igm_cnn_input_gradient); ``param_grads=False``
+        runs only the data-gradient chain (self.grads is then not written)."""
         lib, st = L.lib(), L.stream_ptr()
         acts = buf["acts"]
         npart, npart2 = buf["npart"], buf["npart2"]
@@ -212,6 +213,7 @@ class CNN:
                                               self.out_scale, self.alpha, _p(g[0]), _p(buf["dyb"]),
                                               _p(buf["hpart"]), npart2, st)
             L.check(rc, "igm_cnn_head_backward_tc")
+        if self.nout <= F and param_grads:
             stride = self.nout + F
             L.check(lib.igm_reduce_partials(_p(buf["hpart"]), npart2, self.nout, stride,
                                             gp + 4 * self.offsets[2 * self.L + 1], 0, st), "reduce head bias")
@@ -222,43 +224,47 @@ class CNN:
             L.check(rc, "igm_conv3x3_wgrad head")
             L.check(lib.igm_cnn_head_wgrad_finish(_p(buf["wpart"]), npart, self.nout, gp + 4 * self.offsets[2 * self.L],
                                                   st), "igm_cnn_head_wgrad_finish")
-        else:
+        elif self.nout > F:
             rc = lib.igm_cnn_head_backward(B, h, w, self.nz, _p(acts[self.L - 1]), hw, _p(dU), _p(dV),
                                            self.out_scale, self.alpha, _p(g[0]), _p(buf["hpart"]), npart2, st)
             L.check(rc, "igm_cnn_head_backward")
-            # head kernel + bias gradients, last conv layer's bias gradient
-            L.check(lib.igm_reduce_partials(_p(buf["hpart"]), npart2, nh + self.nout, hl,
-                                            gp + 4 * self.offsets[2 * self.L], 0, st), "reduce head")
-            L.check(lib.igm_reduce_partials(buf["hpart"].data_ptr() + 4 * (nh + self.nout), npart2, F, hl,
-                                            gp + 4 * self.offsets[2 * (self.L - 1) + 1], 0, st), "reduce db")
+            if param_grads:
+                # head kernel + bias gradients, last conv layer's bias gradient
+                L.check(lib.igm_reduce_partials(_p(buf["hpart"]), npart2, nh + self.nout, hl,
+                                                gp + 4 * self.offsets[2 * self.L], 0, st), "reduce head")
+                L.check(lib.igm_reduce_partials(buf["hpart"].data_ptr() + 4 * (nh + self.nout), npart2, F, hl,
+                                                gp + 4 * self.offsets[2 * (self.L - 1) + 1], 0, st), "reduce db")
         cur = 0
         for l in range(self.L - 1, -1, -1):
             gl = g[cur]
-            if l > 0:
+            if l > 0 and param_grads:
                 rc = lib.igm_conv3x3_wgrad(B, h, w, F, _p(acts[l - 1]), _p(gl), _p(buf["wpart"]), npart,
                                            _p(self.err), st)
                 L.check(rc, f"igm_conv3x3_wgrad layer {l}")
                 rc = lib.igm_cnn_wgrad_finish(_p(buf["wpart"]), npart, F, F, gp + 4 * self.offsets[2 * l], st)
                 L.check(rc, "igm_cnn_wgrad_finish")
-            else:
+            elif l == 0:
                 if field_grad is not None:
                     sc = (C.c_double * self.cin)(*[float(x) for x in self.scales[:self.cin]])
                     rc = lib.igm_cnn_input_gradient(B, h, w, self.cin, _p(gl), self.params.data_ptr(), sc,
                                                     _p(field_grad), st)
                     L.check(rc, "igm_cnn_input_gradient")
-                rc = lib.igm_conv3x3_wgrad(B, h, w, 16, _p(buf["X"]), _p(gl), _p(buf["wpart"]), npart,
-                                           _p(self.err), st)
-                L.check(rc, "igm_conv3x3_wgrad layer 0")
-                rc = lib.igm_cnn_wgrad_finish_split(_p(buf["wpart"]), npart, self.cin, gp + 4 * self.offsets[0], st)
-                L.check(rc, "igm_cnn_wgrad_finish_split")
+                if param_grads:
+                    rc = lib.igm_conv3x3_wgrad(B, h, w, 16, _p(buf["X"]), _p(gl), _p(buf["wpart"]), npart,
+                                               _p(self.err), st)
+                    L.check(rc, "igm_conv3x3_wgrad layer 0")
+                    rc = lib.igm_cnn_wgrad_finish_split(_p(buf["wpart"]), npart, self.cin, gp + 4 * self.offsets[0],
+                                                        st)
+                    L.check(rc, "igm_cnn_wgrad_finish_split")
             if l > 0:
                 nxt = g[1 - cur]
                 buf["dbpart"].zero_()
                 rc = lib.igm_conv3x3(1, B, h, w, F, _p(gl), self._wb(l), None, _p(acts[l - 1]), _p(nxt),
                                      _p(buf["dbpart"]), npart, self.alpha, _p(self.err), st)
                 L.check(rc, f"igm_conv3x3 dgrad layer {l}")
-                L.check(lib.igm_reduce_partials(_p(buf["dbpart"]), npart, F, F,
-                                                gp + 4 * self.offsets[2 * (l - 1) + 1], 0, st), "reduce db")
+                if param_grads:
+                    L.check(lib.igm_reduce_partials(_p(buf["dbpart"]), npart, F, F,
+                                                    gp + 4 * self.offsets[2 * (l - 1) + 1], 0, st), "reduce db")
                 cur = 1 - cur
 
     def adam_step(self, lr, beta_1=0.9, beta_2=0.999, epsilon=1e-7, clipnorm=1.0):

@@ -4,7 +4,8 @@ The processes read ``cfg.processes.<name>.<key>`` by attribute access, so an
 OmegaConf DictConfig composed by the reference's Hydra setup works as is;
 ``default_cfg()`` builds an equivalent plain object for callers without
 Hydra.  Keys and defaults follow igm/conf/processes/iceflow.yaml,
-thk.yaml, time.yaml, smb_simple.yaml and vert_flow.yaml.  Keys this implementation adds are
+thk.yaml, time.yaml, smb_simple.yaml, vert_flow.yaml and
+data_assimilation.yaml.  Keys this implementation adds are
 marked "(igm_b200)".
 """
 
@@ -90,6 +91,28 @@ DEFAULTS = {
     "vert_flow": {"version": 2, "method": "kinematic"},
     "time": {"start": 2000.0, "end": 2100.0, "save": 10.0, "cfl": 0.3, "step_max": 1.0},
     "smb_simple": {"update_freq": 1.0, "file": "param.txt", "array": []},
+    "data_assimilation": {
+        "control_list": ["thk"],
+        "cost_list": ["velsurf", "thk", "icemask"],
+        "optimization": {"nbitmin": 50, "nbitmax": 500, "step_size": 1.0, "step_size_decay": 0.9,
+                         "init_zero_thk": False, "sole_mask": False, "retrain_iceflow_model": True,
+                         "fix_opti_normalization_issue": False, "method": "ADAM",
+                         "obstacle_constraint": ["reproject", "penalty"], "optimizer_clipnorm": 1.0e7,
+                         "optimizer_epsilon": 1.0e-7, "pertubate": False},
+        "regularization": {"thk": 10.0, "slidingco": 1.0, "arrhenius": 10.0, "divflux": 1.0,
+                           "smooth_anisotropy_factor": 0.2, "smooth_anisotropy_factor_sl": 1.0,
+                           "convexity_weight": 0.002, "convexity_power": 1.3, "to_regularize": "topg"},
+        "fitting": {"usurfobs_std": 2.0, "velsurfobs_std": 1.0, "thkobs_std": 3.0, "divfluxobs_std": 1.0,
+                    "uniformize_thkobs": True, "include_low_speed_term": False, "velsurfobs_thr": 0.0,
+                    "log_slidingco": False},
+        "divflux": {"method": "upwind", "force_zero_sum": False},
+        "scaling": {"thk": 2.0, "usurf": 0.5, "slidingco": 0.0001, "arrhenius": 0.1},
+        "output": {"freq": 50, "plot2d_live": True, "plot2d": True, "save_result_in_ncdf": "geology-optimized.nc",
+                   "save_iterat_in_ncdf": True, "editor_plot2d": "vs",
+                   "vars_to_save": ["usurf", "thk", "slidingco", "velsurf_mag", "velsurfobs_mag", "divflux",
+                                    "icemask"]},
+        "cook": {"infer_params": False, "tidewater_glacier": False, "vol_std": 1000.0},
+    },
 }
 
 

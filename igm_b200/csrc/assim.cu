@@ -274,28 +274,33 @@ static int flow_t(int ny, int nx, const void* u, const void* v, void* fx, void* 
   return launch_status("flow_norm_kernel");
 }
 
-// Control update around the optimizer step (optimize/update.py:22-35, 62-103)
-// for control thk with scaling sc: before the step (mode 0) the optimizer's
-// variable thk / sc and its gradient sc (dC/dthk direct + through the
-// emulator), zero outside the observed ice mask; the moments start at zero
-// (the reference wraps the control in a new tf.Variable at every iteration, so
-// Adam's slots are new); after the step (mode 1) thk = variable * sc, then the
-// reprojection onto the ice mask and thk >= 0.
+// Control update of optimize_update (optimize/update.py:23-27, 38-42,
+// 56-68, 77-98) for control thk with scaling sc, at the three points where
+// the reference touches the control:
+//   mode 0, before the forward: the optimizer's variable thk / sc, then
+//     thk = variable * sc, and zero moments (the reference wraps the control
+//     in a new tf.Variable at every iteration, so Adam's slots are new);
+//   mode 1, the gradient: sc (dC/dthk direct + through the emulator) where
+//     icemaskobs > 0.5, zero elsewhere;
+//   mode 2, after the step: thk = variable * sc, then the reprojection onto
+//     the ice mask and thk >= 0.
 template <typename T>
 __global__ void assim_control_kernel(size_t n, int mode, T sc, int reproject_mask, int reproject_pos, T* thk,
-                                     const T* g_direct, const T* g_emul, const T* icemaskobs, float* var, float* grad,
-                                     float* m, float* v) {
+                                     const T* g_direct, const float* g_emul, const T* icemaskobs, float* var,
+                                     float* grad, float* m, float* v) {
   for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
-    const bool in = icemaskobs[o] > T(0.5);
     if (mode == 0) {
-      var[o] = (float)(thk[o] / sc);
-      const T g = g_direct[o] + (g_emul ? g_emul[o] : T(0));
-      grad[o] = in ? (float)(g * sc) : 0.f;
+      const float x = (float)(thk[o] / sc);
+      var[o] = x;
+      thk[o] = (T)x * sc;
       m[o] = 0.f;
       v[o] = 0.f;
+    } else if (mode == 1) {
+      const T g = g_direct[o] + (g_emul ? (T)g_emul[o] : T(0));
+      grad[o] = icemaskobs[o] > T(0.5) ? (float)(g * sc) : 0.f;
     } else {
       T t = (T)var[o] * sc;
-      if (reproject_mask && !in) t = T(0);
+      if (reproject_mask && !(icemaskobs[o] > T(0.5))) t = T(0);
       if (reproject_pos && t < T(0)) t = T(0);
       thk[o] = t;
     }
@@ -346,22 +351,23 @@ extern "C" int igm_assim_flow_direction(int dtype, int ny, int nx, const void* u
 }
 
 extern "C" int igm_assim_control(int dtype, int mode, size_t n, double scale, int reproject_mask, int reproject_pos,
-                                 void* thk, const void* grad_direct, const void* grad_emulator, const void* icemaskobs,
+                                 void* thk, const void* grad_direct, const float* grad_emulator, const void* icemaskobs,
                                  float* variable, float* grad, float* m, float* v, void* stream) {
-  IGM_CHECK_ARG((mode == 0 || mode == 1) && n >= 1 && scale > 0, IGM_ERR_BAD_ARGUMENT,
+  IGM_CHECK_ARG(mode >= 0 && mode <= 2 && n >= 1 && scale > 0, IGM_ERR_BAD_ARGUMENT,
                 "igm_assim_control: bad mode, size or scale");
-  IGM_CHECK_ARG(thk && icemaskobs && variable && (mode == 1 || (grad_direct && grad && m && v)), IGM_ERR_BAD_ARGUMENT,
-                "igm_assim_control: NULL argument");
+  IGM_CHECK_ARG(thk && (mode != 0 || (variable && m && v)) && (mode != 1 || (grad_direct && icemaskobs && grad)) &&
+                    (mode != 2 || (variable && (icemaskobs || !reproject_mask))),
+                IGM_ERR_BAD_ARGUMENT, "igm_assim_control: NULL argument");
   cudaStream_t st = as_stream(stream);
   if (dtype == IGM_F32)
     assim_control_kernel<float><<<grid_n(n), 256, 0, st>>>(n, mode, (float)scale, reproject_mask, reproject_pos,
                                                            (float*)thk, (const float*)grad_direct,
-                                                           (const float*)grad_emulator, (const float*)icemaskobs,
+                                                           grad_emulator, (const float*)icemaskobs,
                                                            variable, grad, m, v);
   else if (dtype == IGM_F64)
     assim_control_kernel<double><<<grid_n(n), 256, 0, st>>>(n, mode, scale, reproject_mask, reproject_pos,
                                                             (double*)thk, (const double*)grad_direct,
-                                                            (const double*)grad_emulator, (const double*)icemaskobs,
+                                                            grad_emulator, (const double*)icemaskobs,
                                                             variable, grad, m, v);
   else {
     set_error("igm_assim_control: unknown dtype %d", dtype);

@@ -158,17 +158,24 @@ def absmax2(a, b, out=None):
 
 
 def assim_cost_grad(thk, usurf, uvs, vvs, uobs, vobs, thkobs, dens, icemaskobs, flowdir, dx, params,
-                    partials=None):
+                    partials=None, costs=None, g_thk=None, g_u=None, g_v=None):
     """Cost terms (device double[5]: velsurf, thk, icemask, thk_positive,
     thk_regu) and gradients (dC/dthk, dC/duvelsurf, dC/dvvelsurf) of the
     default data-assimilation configuration (igm_assim_cost_grad); ``params``
-    an _lib.AssimParams, ``flowdir`` (fx, fy) [ny-1, nx-1] or None."""
+    an _lib.AssimParams, ``flowdir`` (fx, fy) [ny-1, nx-1] or None.  The
+    outputs may be given (contiguous [ny, nx] views, e.g. the top layer of a
+    [nz, ny, nx] velocity gradient)."""
     ny, nx = thk.shape
     n_parts = 148 * 8
     if partials is None:
         partials = torch.empty(n_parts * 5, dtype=torch.float64, device=thk.device)
-    costs = torch.empty(5, dtype=torch.float64, device=thk.device)
-    g_thk, g_u, g_v = torch.empty_like(thk), torch.empty_like(thk), torch.empty_like(thk)
+    costs = costs if costs is not None else torch.empty(5, dtype=torch.float64, device=thk.device)
+    g_thk = g_thk if g_thk is not None else torch.empty_like(thk)
+    g_u = g_u if g_u is not None else torch.empty_like(thk)
+    g_v = g_v if g_v is not None else torch.empty_like(thk)
+    for t in (g_thk, g_u, g_v):
+        if t.shape != thk.shape or not t.is_contiguous() or t.dtype != thk.dtype:
+            raise ValueError("assim_cost_grad: gradient outputs must be contiguous [ny, nx] of thk's dtype")
     fx, fy = flowdir if flowdir is not None else (None, None)
     rc = L.lib().igm_assim_cost_grad(L.dtype_code(thk.dtype), ny, nx, float(dx), L.ptr(thk), L.ptr(usurf),
                                      L.ptr(uvs), L.ptr(vvs), L.ptr(uobs), L.ptr(vobs), L.ptr(thkobs), L.ptr(dens),
@@ -188,6 +195,23 @@ def assim_flow_direction(uvs, vvs):
                                           L.ptr(fy), L.ptr(scratch), L.stream_ptr())
     L.check(rc, "igm_assim_flow_direction")
     return fx, fy
+
+
+def assim_control(mode, thk, scale, icemaskobs=None, variable=None, grad=None, m=None, v=None, g_direct=None,
+                  g_emul=None, reproject_mask=True, reproject_pos=True):
+    """The control update of one assimilation iteration (igm_assim_control):
+    mode 0 variable = thk / scale, thk = variable * scale, zero moments;
+    mode 1 grad = scale (g_direct + g_emul) inside the observed ice mask;
+    mode 2 thk = variable * scale with the reprojection.  variable, grad, m,
+    v, g_emul are float32."""
+    n = thk.numel()
+    if g_emul is not None and (g_emul.dtype != torch.float32 or not g_emul.is_contiguous() or g_emul.numel() != n):
+        raise ValueError("assim_control: g_emul must be contiguous float32 of thk's size")
+    rc = L.lib().igm_assim_control(L.dtype_code(thk.dtype), int(mode), n, float(scale), int(bool(reproject_mask)),
+                                   int(bool(reproject_pos)), L.ptr(thk), L.ptr(g_direct), L.ptr(g_emul),
+                                   L.ptr(icemaskobs), L.ptr(variable), L.ptr(grad), L.ptr(m), L.ptr(v),
+                                   L.stream_ptr())
+    L.check(rc, "igm_assim_control")
 
 
 def divflux_upwind(u, v, h, dx, out=None):

@@ -1,0 +1,405 @@
+"""data_assimilation process (igm/processes/data_assimilation/data_assimilation.py:16-71).
+
+Inverts the ice thickness from surface-velocity and thickness observations
+through the CNN emulator, as the reference does with its default
+configuration: control ``thk``, costs ``velsurf`` + ``thk`` + ``icemask``,
+the ``reproject`` + ``penalty`` obstacle constraints, the anisotropic (or
+isotropic) regularisation of the bed or of the thickness, ADAM with a
+learning rate decaying as step_size decay^(i/100), the emulator retrained on
+the Blatter-Pattyn energy of the current geometry after every iteration
+(gated by retrain_freq, as in the iceflow process).
+
+One iteration (optimize/update.py:15-103) is a fixed sequence of device
+launches with no host synchronisation:
+
+  igm_assim_control mode 0      thk_sc = thk / sc, thk = thk_sc sc, fresh moments
+  CNN forward (keep activations, thk mask), velsurf / velbar
+  igm_assim_flow_direction      (anisotropic regularisation only)
+  igm_assim_cost_grad           costs, dC/dthk, dC/d(top-layer U, V)
+  CNN backward, data chain only, with igm_cnn_input_gradient
+  igm_assim_control mode 1      gradient of thk_sc, zero outside the mask
+  igm_adam_clipnorm             Keras legacy Adam at iteration i + 1
+  igm_assim_control mode 2      thk = thk_sc sc, reprojection
+  igm_divflux_upwind            divflux of the emulated velbar
+  rms / std record              device reductions into the history tensor
+
+The cost history and the rms/std record stay on the device until the end of
+the loop (``costs.dat`` and ``rms_std_vol.dat`` are written from them then);
+the netCDF snapshots every ``output.freq`` iterations and the final
+``save_result_in_ncdf`` file are host copies.  The 2-D plots of the
+reference (matplotlib) are not drawn.
+
+Supported: control_list [thk]; cost_list within velsurf, thk, icemask;
+method ADAM; sole_mask, fix_opti_normalization_issue, include_low_speed_term,
+cook.infer_params and pertubate off; divflux.method upwind.  Anything else
+raises NotImplementedError.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+import torch
+
+from .. import _lib as L
+from .. import kernels as K
+from .. import state as S
+from . import iceflow as P
+
+_COST_KEYS = ["velsurf", "thk", "icemask", "thk_positive", "thk_regu"]
+
+
+def _check_supported(cfg):
+    da = cfg.processes.data_assimilation
+    o = da.optimization
+    bad = []
+    if list(da.control_list) != ["thk"]:
+        bad.append(f"control_list={list(da.control_list)} (only ['thk'])")
+    extra = [c for c in da.cost_list if c not in ("velsurf", "thk", "icemask")]
+    if extra:
+        bad.append(f"cost terms {extra} (only velsurf, thk, icemask)")
+    if o.method != "ADAM":
+        bad.append(f"optimization.method={o.method!r} (only 'ADAM')")
+    for key in ("sole_mask", "fix_opti_normalization_issue", "pertubate"):
+        if bool(o.get(key, False)):
+            bad.append(f"optimization.{key}")
+    if bool(da.fitting.include_low_speed_term):
+        bad.append("fitting.include_low_speed_term")
+    if bool(da.cook.infer_params):
+        bad.append("cook.infer_params")
+    if da.divflux.method != "upwind" or bool(da.divflux.get("force_zero_sum", False)):
+        bad.append(f"divflux.method={da.divflux.method!r} (only 'upwind' without force_zero_sum)")
+    if da.regularization.to_regularize not in ("topg", "thk"):
+        bad.append(f"to_regularize={da.regularization.to_regularize!r}")
+    if cfg.processes.iceflow.method != "emulated":
+        bad.append("iceflow.method must be 'emulated'")
+    if bad:
+        raise NotImplementedError("igm_b200 data_assimilation: unsupported configuration: " + "; ".join(bad))
+
+
+def create_density_matrix(thkobs: np.ndarray, kernel_size: int = 5) -> np.ndarray:
+    """utils.py:68-82: number of thickness observations in the
+    kernel_size x kernel_size window around each node (zero outside)."""
+    m = (~np.isnan(thkobs)).astype(np.float64)
+    r = kernel_size // 2
+    p = np.pad(m, r)
+    c = np.cumsum(np.cumsum(p, 0), 1)
+    c = np.pad(c, ((1, 0), (1, 0)))
+    k = kernel_size
+    ny, nx = m.shape
+    return c[k:k + ny, k:k + nx] - c[:ny, k:k + nx] - c[k:k + ny, :nx] + c[:ny, :nx]
+
+
+def _density_weights(thkobs: np.ndarray, uniformize: bool) -> np.ndarray:
+    """optimize/initialize.py:40-46."""
+    if not uniformize:
+        return np.ones_like(thkobs)
+    d = create_density_matrix(thkobs, 5)
+    d = np.where(d > 0, 1.0 / np.maximum(d, 1.0), 0.0)
+    d = np.where(np.isnan(thkobs), 0.0, d)
+    pos = d[d > 0]
+    return (d / pos.mean() if pos.size else d).astype(thkobs.dtype)
+
+
+class _Assim:
+    """Device buffers and constants of the assimilation loop."""
+
+    def __init__(self, cfg, state):
+        da = cfg.processes.data_assimilation
+        thk = S.get(state, "thk")
+        ny, nx = thk.shape
+        d = thk.device
+        self.ny, self.nx, self.n = ny, nx, ny * nx
+        self.dx = P._dx(state)
+        nan = torch.full((ny, nx), float("nan"), dtype=torch.float32, device=d)
+        costs = list(da.cost_list)
+        self.uobs = S.get(state, "uvelsurfobs").contiguous() if "velsurf" in costs else nan
+        self.vobs = S.get(state, "vvelsurfobs").contiguous() if "velsurf" in costs else nan
+        self.thkobs = S.get(state, "thkobs").contiguous() if "thk" in costs else nan
+        self.icemaskobs = S.get(state, "icemaskobs").contiguous()
+        self.icemask = S.get(state, "icemask").contiguous() if hasattr(state, "icemask") else self.icemaskobs
+        self.dens = S.get(state, "dens_thkobs").contiguous()
+        self.cost_list = costs
+        nz = int(cfg.processes.iceflow.numerics.Nz)
+        self.nz = nz
+        f32 = dict(dtype=torch.float32, device=d)
+        self.var, self.grad, self.m, self.v = (torch.empty(self.n, **f32) for _ in range(4))
+        self.norms = torch.empty(1, dtype=torch.float64, device=d)
+        self.offsets = (C.c_size_t * 2)(0, self.n)
+        self.dU = torch.zeros((1, nz, ny, nx), **f32)
+        self.dV = torch.zeros((1, nz, ny, nx), **f32)
+        self.g_thk = torch.empty((ny, nx), **f32)
+        self.field_grad = torch.empty((1, 5, ny, nx), **f32)
+        self.partials = torch.empty(148 * 8 * 5, dtype=torch.float64, device=d)
+        nit = int(da.optimization.nbitmax) + 1
+        self.cost_hist = torch.zeros((nit, 5), dtype=torch.float64, device=d)
+        self.rms_hist = torch.zeros((nit, 9), dtype=torch.float64, device=d)
+        # parameters of igm_assim_cost_grad
+        p = L.AssimParams()
+        f, r, o = da.fitting, da.regularization, da.optimization
+        p.velsurfobs_std, p.velsurfobs_thr, p.thkobs_std = f.velsurfobs_std, f.velsurfobs_thr, f.thkobs_std
+        p.regu_thk = r.thk
+        area = float((self.icemask > 0.5).sum().item()) * self.dx ** 2  # regu_thk.py:11
+        p.gamma = float(r.convexity_weight) * area ** (float(r.convexity_power) - 2.0) if area > 0 else 0.0
+        p.aniso_factor = float(r.smooth_anisotropy_factor)
+        vo = torch.stack([self.uobs, self.vobs], -1).double()
+        rel = torch.linalg.vector_norm(vo, dim=-1) >= float(f.velsurfobs_thr)
+        p.n_vel = float((~torch.isnan(vo) & rel[..., None]).sum().item())
+        p.n_thk = float((~torch.isnan(self.thkobs)).sum().item())
+        p.penalty = int("penalty" in o.obstacle_constraint)
+        p.icemask_cost = int("icemask" in costs)
+        p.regularize_thk = int(r.to_regularize == "thk")
+        p.mask_velsurf = 1
+        self.params = p
+        self.present = [("velsurf" in costs), ("thk" in costs), bool(p.penalty and p.icemask_cost),
+                        bool(p.penalty), True]
+        self.sc = float(da.scaling.thk)
+        self.reproject = "reproject" in o.obstacle_constraint
+
+
+def optimize_initialize(cfg, state):
+    """optimize/initialize.py:10-69 for control thk."""
+    da = cfg.processes.data_assimilation
+    if ("usurf" in da.cost_list) != ("usurf" in da.control_list):
+        raise AssertionError("usurf must be in both cost_list and control_list, or in neither")
+    thkobs = S.get(state, "thkobs").cpu().numpy()
+    if np.all(np.isnan(thkobs)) and "thk" in da.cost_list:
+        da.cost_list = [c for c in da.cost_list if c != "thk"]
+    thk = S.get(state, "thk")
+    if hasattr(state, "thkinit"):
+        thk = S.get(state, "thkinit").clone()
+    else:
+        thk = torch.zeros_like(thk)
+    if bool(da.optimization.init_zero_thk):
+        thk = thk * 0.0
+    S.put(state, "thk", thk.contiguous())
+    dens = _density_weights(thkobs.astype(np.float32), bool(da.fitting.uniformize_thkobs))
+    S.put(state, "dens_thkobs", torch.as_tensor(dens, device=thk.device))
+    sl = S.get(state, "slidingco")
+    S.put(state, "slidingco", torch.where(S.get(state, "icemaskobs") == 2, torch.zeros_like(sl), sl))
+    state._igm_assim = _Assim(cfg, state)
+
+
+def _record_rms(a: _Assim, state, i):
+    """compute_rms_std_optimization (utils.py:10-66) as device reductions
+    into row i of the history: rmsthk, stdthk, rmsvel, stdvel, rmsdiv,
+    stddiv, rmsusurf, stdusurf, vol (the means and population standard
+    deviations of the misfits over their masks)."""
+    thk = S.get(state, "thk")
+
+    def mean_std(d, mask):
+        m = mask.double()
+        cnt = m.sum()
+        dd = torch.where(mask, d.double(), torch.zeros_like(m))
+        mu = dd.sum() / cnt.clamp(min=1)
+        sd = torch.sqrt((torch.where(mask, dd - mu, torch.zeros_like(m)) ** 2).sum() / cnt.clamp(min=1))
+        return mu, sd
+
+    row = a.rms_hist[i]
+    if hasattr(state, "thkobs"):
+        tob = S.get(state, "thkobs")
+        row[0], row[1] = mean_std(thk - tob, ~torch.isnan(tob))
+    inside = a.icemaskobs > 0.5
+    if hasattr(state, "uvelsurfobs"):
+        uo, vo = S.get(state, "uvelsurfobs"), S.get(state, "vvelsurfobs")
+        vs = torch.sqrt(S.get(state, "uvelsurf") ** 2 + S.get(state, "vvelsurf") ** 2)
+        vob = torch.sqrt(uo * uo + vo * vo)
+        row[2], row[3] = mean_std(vs - vob, inside & ~torch.isnan(vob))
+    if hasattr(state, "divfluxobs"):
+        row[4], row[5] = mean_std(S.get(state, "divfluxobs") - S.get(state, "divflux"), inside)
+    if hasattr(state, "usurfobs"):
+        row[6], row[7] = mean_std(S.get(state, "usurf") - S.get(state, "usurfobs"), inside)
+    row[8] = thk.double().sum() * a.dx ** 2 / 1e9
+
+
+def optimize_update(cfg, state, cost, i):
+    """optimize/update.py:15-103: one ADAM iteration for control thk.
+    ``cost`` receives the device cost tensor (double[5] in the order
+    velsurf, thk, icemask, thk_positive, thk_regu)."""
+    da = cfg.processes.data_assimilation
+    o = da.optimization
+    a: _Assim = state._igm_assim
+    lib, st = L.lib(), L.stream_ptr()
+    thk = S.get(state, "thk").contiguous()
+    K.assim_control(0, thk, a.sc, variable=a.var, m=a.m, v=a.v)
+    S.put(state, "thk", thk)
+    lr = float(o.step_size) * (float(o.step_size_decay) ** (i / 100)) if o.step_size_decay < 1 else float(o.step_size)
+    # emulator forward, masked where thk == 0 (emulate.py:116-152), activations kept for the gradient
+    model = state.iceflow_model
+    f = [thk] + [S.get(state, k) for k in ("usurf", "arrhenius", "slidingco")]
+    buf = model.buffers(1, a.ny, a.nx, train=True)
+    model.prepare_input(f, a.dx, [(0, 0)], a.ny, a.nx, buf)
+    U, V = model.forward(buf, 1, a.ny, a.nx, thk_mask=thk, keep_acts=True)
+    state.U, state.V = U[0], V[0]
+    P.set_derived_velocities(cfg, state, mask=False)
+    uvs, vvs = S.get(state, "uvelsurf"), S.get(state, "vvelsurf")
+    flow = None
+    if float(da.regularization.smooth_anisotropy_factor) != 1.0:
+        flow = K.assim_flow_direction(uvs.contiguous(), vvs.contiguous())
+        state.flowdirx, state.flowdiry = flow
+    # total_cost and its gradient; dC/dvelsurf lands in the top layer of dU, dV (Lagrange basis)
+    K.assim_cost_grad(thk, S.get(state, "usurf"), uvs.contiguous(), vvs.contiguous(), a.uobs, a.vobs, a.thkobs,
+                      a.dens, a.icemaskobs, flow, a.dx, a.params, partials=a.partials, costs=a.cost_hist[i],
+                      g_thk=a.g_thk, g_u=a.dU[0, a.nz - 1], g_v=a.dV[0, a.nz - 1])
+    model.backward(buf, 1, a.ny, a.nx, a.dU, a.dV, field_grad=a.field_grad, param_grads=False)
+    K.assim_control(1, thk, a.sc, icemaskobs=a.icemaskobs, grad=a.grad, g_direct=a.g_thk,
+                    g_emul=a.field_grad[0, 0].reshape(-1))
+    rc = lib.igm_adam_clipnorm(1, a.offsets, L.ptr(a.var), L.ptr(a.grad), L.ptr(a.m), L.ptr(a.v), L.ptr(a.norms),
+                               lr, 0.9, 0.999, float(o.optimizer_epsilon), float(o.optimizer_clipnorm), i + 1, st)
+    L.check(rc, "igm_adam_clipnorm")
+    K.assim_control(2, thk, a.sc, icemaskobs=a.icemaskobs, variable=a.var,
+                    reproject_mask=a.reproject and "icemask" in a.cost_list, reproject_pos=a.reproject)
+    S.put(state, "thk", thk)
+    S.put(state, "divflux", K.divflux_upwind(S.get(state, "ubar").contiguous(), S.get(state, "vbar").contiguous(),
+                                             thk, a.dx))
+    cost["all"] = a.cost_hist[i]
+
+
+def _cost_dict(a: _Assim, row):
+    return {k: float(row[j]) for j, k in enumerate(_COST_KEYS) if a.present[j]}
+
+
+def _mag(u, v):
+    return torch.sqrt(u * u + v * v)
+
+
+def _snapshot_fields(cfg, state):
+    """The derived fields of output_ncdf.py:20-30, then the listed fields as
+    float32 host arrays."""
+    da = cfg.processes.data_assimilation
+    want = list(da.output.vars_to_save)
+    if "velbase_mag" in want:
+        state.velbase_mag = _mag(S.get(state, "uvelbase"), S.get(state, "vvelbase"))
+    if "velsurf_mag" in want:
+        state.velsurf_mag = _mag(S.get(state, "uvelsurf"), S.get(state, "vvelsurf"))
+    if "velsurfobs_mag" in want:
+        state.velsurfobs_mag = _mag(S.get(state, "uvelsurfobs"), S.get(state, "vvelsurfobs"))
+    if "sliding_ratio" in want:
+        vs = state.velsurf_mag
+        state.sliding_ratio = torch.where(vs > 10, state.velbase_mag / vs, torch.full_like(vs, float("nan")))
+    out = {}
+    for v in want:
+        if hasattr(state, v):
+            x = getattr(state, v)
+            out[v] = (x.detach().float().cpu().numpy() if isinstance(x, torch.Tensor)
+                      else np.asarray(x, dtype=np.float32))
+    return out
+
+
+def _coords(state, ny, nx, dx):
+    def host(name, n):
+        if hasattr(state, name):
+            x = getattr(state, name)
+            return (x.detach().cpu().numpy() if isinstance(x, torch.Tensor) else np.asarray(x)).astype(np.float32)
+        return (np.arange(n) * dx).astype(np.float32)
+    return host("x", nx), host("y", ny)
+
+
+def update_ncdf_optimize(cfg, state, it):
+    """output_ncdf.py:12-78: one (iterations, y, x) record per listed field
+    in optimize.nc (netCDF-3 through scipy)."""
+    from scipy.io import netcdf_file
+    a: _Assim = state._igm_assim
+    fields = _snapshot_fields(cfg, state)
+    if it == 0 or not os.path.exists("optimize.nc"):
+        x, y = _coords(state, a.ny, a.nx, a.dx)
+        with netcdf_file("optimize.nc", "w", version=2) as nc:
+            nc.createDimension("iterations", None)
+            e = nc.createVariable("iterations", "f4", ("iterations",))
+            e.units, e.long_name, e.axis = "None", "iterations", "ITERATIONS"
+            for name, arr, ax in [("y", y, "Y"), ("x", x, "X")]:
+                nc.createDimension(name, arr.size)
+                c = nc.createVariable(name, "f4", (name,))
+                c.units, c.long_name, c.axis = "m", name, ax
+                c[:] = arr
+            for v in fields:
+                nc.createVariable(v, "f4", ("iterations", "y", "x"))
+            e[0] = it
+            for v, arr in fields.items():
+                nc.variables[v][0] = arr
+        return
+    with netcdf_file("optimize.nc", "a") as nc:
+        d = nc.variables["iterations"].shape[0]
+        nc.variables["iterations"][d] = it
+        for v, arr in fields.items():
+            if v in nc.variables:
+                nc.variables[v][d] = arr
+
+
+def output_ncdf_optimize_final(cfg, state):
+    """output_ncdf.py:81-124: the optimised fields in save_result_in_ncdf."""
+    from scipy.io import netcdf_file
+    a: _Assim = state._igm_assim
+    fields = _snapshot_fields(cfg, state)
+    x, y = _coords(state, a.ny, a.nx, a.dx)
+    with netcdf_file(cfg.processes.data_assimilation.output.save_result_in_ncdf, "w", version=2) as nc:
+        for name, arr, ax in [("y", y, "Y"), ("x", x, "X")]:
+            nc.createDimension(name, arr.size)
+            c = nc.createVariable(name, "f4", (name,))
+            c.units, c.long_name, c.axis = "m", name, ax
+            c[:] = arr
+        for v, arr in fields.items():
+            e = nc.createVariable(v, "f4", ("y", "x"))
+            e.standard_name = v
+            e[:] = arr
+
+
+def _write_histories(cfg, state, n_it, glen):
+    """prints.py:11-32 (costs.dat) and prints.py:61-82 (rms_std_vol.dat)
+    from the device histories; the record lists on the state as in
+    utils.py:13-66."""
+    a: _Assim = state._igm_assim
+    ch = a.cost_hist[:n_it].cpu().numpy()
+    rh = a.rms_hist[:n_it].cpu().numpy()
+    names = ["rmsthk", "stdthk", "rmsvel", "stdvel", "rmsdiv", "stddiv", "rmsusurf", "stdusurf", "vol"]
+    for j, k in enumerate(names):
+        setattr(state, k, [float(x) for x in rh[:, j]])
+    keys = [k for j, k in enumerate(_COST_KEYS) if a.present[j]] + (["glen"] if glen else [])
+    with open("costs.dat", "w") as fh:
+        print("   ".join(f"{k:>12}" for k in keys), file=fh)
+        for i in range(n_it):
+            vals = [ch[i, j] for j in range(5) if a.present[j]] + ([glen[i]] if glen else [])
+            print("   ".join(f"{min(float(v), 9999999):>12.4f}" for v in vals), file=fh)
+    np.savetxt("rms_std_vol.dat", rh, fmt="%.10f", comments="",
+               header="        rmsthk      stdthk       rmsvel       stdvel       rmsdiv       stddiv       "
+                      "rmsusurf       stdusurf       vol")
+
+
+def initialize(cfg, state):
+    """data_assimilation.py:16-71."""
+    from .. import emulator as E
+    _check_supported(cfg)
+    P.initialize(cfg, state)
+    optimize_initialize(cfg, state)
+    da = cfg.processes.data_assimilation
+    o = da.optimization
+    a: _Assim = state._igm_assim
+    glen = []
+    n_it = int(o.nbitmax) + 1
+    for i in range(n_it):
+        cost = {}
+        optimize_update(cfg, state, cost, i)
+        _record_rms(a, state, i)
+        if bool(o.retrain_iceflow_model):
+            E.update_iceflow_emulator(cfg, state, i + 1, pertubate=bool(o.pertubate))
+            glen.append(state.COST_EMULATOR[-1] if state.COST_EMULATOR else float("nan"))
+        if i % int(da.output.freq) == 0 and bool(da.output.save_iterat_in_ncdf):
+            update_ncdf_optimize(cfg, state, i)
+    state.iceflow_model.check_errors()
+    # the bed from the optimised thickness (grounded ice)
+    S.put(state, "topg", S.get(state, "usurf") - S.get(state, "thk"))
+    if da.output.save_result_in_ncdf != "":
+        output_ncdf_optimize_final(cfg, state)
+    _write_histories(cfg, state, n_it, glen)
+    state.costs_data_assimilation = [_cost_dict(a, r) for r in a.cost_hist[:n_it].cpu()]
+    S.sync_host(state)
+
+
+def update(cfg, state):
+    pass
+
+
+def finalize(cfg, state):
+    pass

@@ -297,18 +297,22 @@ IGM_API int igm_assim_cost_grad(int dtype, int ny, int nx, double dx, const void
                         const igm_assim_params* params, void* grad_thk, void* grad_uvelsurf,
                         void* grad_vvelsurf, double* partials, int n_parts, double* costs, void* stream);
 
-/* The control update around the optimizer step of optimize_update
- * (data_assimilation/optimize/update.py:22-35, 62-103) for control thk with
- * scaling `scale`: mode 0 (before igm_adam_clipnorm) writes the optimizer's
- * variable thk / scale, its gradient scale (grad_direct + grad_emulator) where
- * icemaskobs > 0.5 and 0 elsewhere, and zeroes the moments m, v (the
- * reference re-creates the control tf.Variable at every iteration, so its Adam
- * slots start at zero); mode 1 sets thk = variable * scale, then zero outside
- * the ice mask (reproject_mask) and at negative values (reproject_pos).
- * variable, grad, m, v: device float[n]; the others [n] of the dtype;
- * grad_emulator may be NULL. */
+/* The control update of optimize_update
+ * (data_assimilation/optimize/update.py:23-27, 38-42, 56-68, 77-98) for
+ * control thk with scaling `scale`, at the three points where the reference
+ * touches the control:
+ *   mode 0 (before the emulator forward): variable = thk / scale, then
+ *     thk = variable * scale, and m = v = 0 (the reference re-creates the
+ *     control tf.Variable at every iteration, so its Adam slots start at zero);
+ *   mode 1 (the gradient): grad = scale (grad_direct + grad_emulator) where
+ *     icemaskobs > 0.5, 0 elsewhere;
+ *   mode 2 (after igm_adam_clipnorm): thk = variable * scale, then 0 outside
+ *     the ice mask (reproject_mask) and at negative values (reproject_pos).
+ * variable, grad, m, v and grad_emulator (the emulator's input-field gradient,
+ * igm_cnn_input_gradient) are device float[n], the others [n] of the dtype;
+ * grad_emulator may be NULL; arguments a mode does not read may be NULL. */
 IGM_API int igm_assim_control(int dtype, int mode, size_t n, double scale, int reproject_mask, int reproject_pos,
-                      void* thk, const void* grad_direct, const void* grad_emulator, const void* icemaskobs,
+                      void* thk, const void* grad_direct, const float* grad_emulator, const void* icemaskobs,
                       float* variable, float* grad, float* m, float* v, void* stream);
 
 /* compute_flow_direction_for_anisotropic_smoothing (data_assimilation/utils.py:

@@ -788,3 +788,109 @@ def divflux_upwind(u, v, h, dx):
     Qx = uf * torch.where(uf > 0, Hx[:, :-1], Hx[:, 1:])
     Qy = vf * torch.where(vf > 0, Hy[:-1, :], Hy[1:, :])
     return (Qx[:, 1:] - Qx[:, :-1]) / dx + (Qy[1:, :] - Qy[:-1, :]) / dx
+
+
+# --------------------------------------------------------------------------
+# data assimilation loop (igm/processes/data_assimilation): density weights,
+# one ADAM iteration of optimize_update for control thk, the rms/std record
+# --------------------------------------------------------------------------
+
+
+def create_density_matrix(data, kernel_size=5):
+    """utils.py:68-82: the number of non-NaN entries of ``data`` in the
+    kernel_size x kernel_size window around each node ('SAME', zero
+    outside)."""
+    m = (~torch.isnan(data)).to(data.dtype)[None, None]
+    k = torch.ones((1, 1, kernel_size, kernel_size), dtype=data.dtype)
+    return torch.nn.functional.conv2d(m, k, padding=kernel_size // 2)[0, 0]
+
+
+def da_density_weights(thkobs, uniformize=True):
+    """optimize/initialize.py:40-46: inverse observation density, zero where
+    thkobs is NaN, normalised by its mean over the positive entries."""
+    if not uniformize:
+        return torch.ones_like(thkobs)
+    d = create_density_matrix(thkobs, 5)
+    d = torch.where(d > 0, 1.0 / d, torch.zeros_like(d))
+    d = torch.where(torch.isnan(thkobs), torch.zeros_like(d), d)
+    return d / torch.mean(d[d > 0])
+
+
+@dataclass
+class AssimControl:
+    """The optimisation keys of optimize_update for control thk
+    (conf/processes/data_assimilation.yaml, optimization / scaling)."""
+    step_size: float = 1.0
+    step_size_decay: float = 0.9
+    scaling_thk: float = 2.0
+    reproject: bool = True
+    icemask_cost: bool = True
+
+
+def da_optimize_update(thk, usurf, arrhenius, slidingco, dx, weights, biases, Nz, vert_weight, obs, p: AssimParams,
+                       ctl: AssimControl, optimizer: KerasLegacyAdam, i, bf16=True, out_scale=1.0, input_scales=None):
+    """One ADAM iteration of optimize_update (optimize/update.py:15-103) for
+    control_list [thk]: thk_sc = thk / sc is a new variable (fresh Adam
+    slots, the optimizer's iteration count carries on), thk = thk_sc sc, the
+    emulator forward masked where thk == 0 (emulate.py:116-152), the flow
+    directions from the emulated surface velocities (constants of the
+    gradient: they pass through scipy), total_cost, its gradient with respect
+    to thk_sc zeroed outside icemaskobs > 0.5, the Adam step at learning rate
+    step_size decay^(i/100), thk = thk_sc sc, reprojection, the upwind flux
+    divergence of the emulated depth-averaged velocity.
+
+    ``obs``: dict uobs, vobs, thkobs, dens, icemaskobs, icemask.  Returns
+    (thk, costs dict, dict of uvelsurf, vvelsurf, ubar, vbar, divflux,
+    gradient).  ``input_scales``: per-channel factors of the network input
+    (None: the raw fields, as the reference)."""
+    sc = ctl.scaling_thk
+    thk_sc = (thk / sc).detach().clone().requires_grad_(True)
+    th = thk_sc * sc
+    dX = torch.full_like(th, dx)
+    X = fieldin_to_X([th, usurf, arrhenius, slidingco, dX])
+    if input_scales is not None:
+        X = X * torch.tensor(input_scales, dtype=X.dtype)
+    Y = cnn_forward(X, weights, biases, bf16=bf16, bf16_first=False, out_scale=out_scale)
+    U, V = Y_to_UV(Y, Nz)
+    U = torch.where(th > 0, U[0], torch.zeros_like(U[0]))
+    V = torch.where(th > 0, V[0], torch.zeros_like(V[0]))
+    uvs, vvs = U[-1], V[-1]
+    flow = None
+    if p.smooth_anisotropy_factor != 1:
+        flow = da_flow_direction(uvs.detach(), vvs.detach())
+    cost = da_costs(th, usurf, uvs, vvs, obs["uobs"], obs["vobs"], obs["thkobs"], obs["dens"], obs["icemaskobs"],
+                    obs["icemask"], flow, dx, p)
+    total = sum(cost.values())
+    (g,) = torch.autograd.grad(total, thk_sc)
+    g = torch.where(obs["icemaskobs"] > 0.5, g, torch.zeros_like(g))
+    if ctl.step_size_decay < 1:
+        optimizer.lr = ctl.step_size * (ctl.step_size_decay ** (i / 100))
+    var = thk_sc.detach().clone()
+    optimizer.apply_gradients([(g, var)])
+    thk_new = var * sc
+    if ctl.reproject:
+        if ctl.icemask_cost:
+            thk_new = torch.where(obs["icemaskobs"] > 0.5, thk_new, torch.zeros_like(thk_new))
+        thk_new = torch.where(thk_new < 0, torch.zeros_like(thk_new), thk_new)
+    U, V = U.detach(), V.detach()
+    ubar = torch.sum(U * vert_weight, 0)
+    vbar = torch.sum(V * vert_weight, 0)
+    aux = {"uvelsurf": uvs.detach(), "vvelsurf": vvs.detach(), "ubar": ubar, "vbar": vbar,
+           "divflux": divflux_upwind(ubar, vbar, thk_new, dx), "gradient": g}
+    return thk_new, {k: v.detach() for k, v in cost.items()}, aux
+
+
+def da_rms_std(thk, thkobs, uvelsurf, vvelsurf, uobs, vobs, icemaskobs, dx):
+    """compute_rms_std_optimization (utils.py:10-66) without divfluxobs /
+    usurfobs: mean and standard deviation of thk - thkobs at the thickness
+    observations and of the speed misfit inside the observed mask, the
+    volume in km^3."""
+    a = ~torch.isnan(thkobs)
+    d = (thk[a] - thkobs[a]).double()
+    rt, st = (float(d.mean()), float(d.std(unbiased=False))) if a.any() else (0.0, 0.0)
+    vs = getmag(uvelsurf, vvelsurf)
+    vo = getmag(uobs, vobs)
+    m = (icemaskobs > 0.5) & ~torch.isnan(vo)
+    e = (vs[m] - vo[m]).double()
+    return {"rmsthk": rt, "stdthk": st, "rmsvel": float(e.mean()), "stdvel": float(e.std(unbiased=False)),
+            "vol": float(thk.double().sum() * dx * dx / 1e9)}

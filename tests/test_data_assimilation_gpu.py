@@ -1,0 +1,183 @@
+"""The data_assimilation process through the process API on the device,
+against the oracle's restatement of optimize_update on the same emulator
+weights and observations.
+
+Twin experiment: the observed surface velocities are the emulator's own at
+the true thickness (10% of them removed), thickness profiles along three
+columns; the inversion starts from zero thickness with the default cost
+terms, constraints and anisotropic bed regularisation, emulator retraining
+off so that the problem stays fixed.
+
+Tolerances: the emulator's convolutions take bf16 inputs on both sides but
+accumulate in different orders, and every ADAM step starts from fresh
+moments (a sign step of size lr sc), so single pixels whose gradient is
+near zero may step the other way; the comparisons are therefore on the
+gradient in relative L2 (5e-2), on the fraction of pixels whose thickness
+step agrees to 5% of its size + 1 mm (>= 97%; where Adam's epsilon dominates
+a tiny gradient the step is proportional to it), and on the cost history
+(5% relative at every 10th iteration)."""
+
+import numpy as np
+import pytest
+import torch
+
+from igm_b200.config import default_cfg
+from igm_b200.processes import data_assimilation as DA
+from igm_b200.processes import iceflow as P
+from igm_b200.state import State
+from oracle import iceflow_oracle as O
+from tests.gpu_util import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+SCALES = [1 / 300.0, 1 / 3000.0, 1 / 100.0, 10.0, 1 / 100.0]
+OUT = 50.0
+NZ = 4
+
+
+def twin_glacier(ny=40, nx=70, dx=100.0):
+    """A tilted-plane bed with a gentle transverse undulation and a
+    parabolic tongue thinning downstream."""
+    x, y = np.arange(nx) * dx, np.arange(ny) * dx
+    X, Y = np.meshgrid(x, y)
+    topg = 2000.0 - 0.05 * X + 20.0 * np.sin(Y / 900.0)
+    thk = np.maximum(0.0, 180.0 * (1 - ((Y - 2000.0) / 1500.0) ** 2) * (1 - X / 7500.0))
+    rng = np.random.default_rng(3)
+    A = O.box_filter(np.exp(rng.uniform(np.log(20.0), np.log(150.0), (ny, nx))), 5)
+    c = O.box_filter(np.exp(rng.uniform(np.log(0.01), np.log(0.1), (ny, nx))), 5)
+    f = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+    return dict(topg=f(topg), thk=f(thk), usurf=f(topg + thk), arrhenius=f(A), slidingco=f(c), dx=dx, x=f(x),
+                y=f(y))
+
+
+def make_cfg(nbitmax, aniso=0.2, to_regularize="topg"):
+    return default_cfg({
+        "iceflow": {"numerics": {"Nz": NZ},
+                    "emulator": {"pretrained": False, "retrain_freq": 0, "input_scales": SCALES,
+                                 "output_scale": OUT, "seed": 1,
+                                 "network": {"nb_layers": 3, "weight_initialization": "he_normal"}}},
+        "data_assimilation": {"optimization": {"nbitmax": nbitmax, "retrain_iceflow_model": False},
+                              "regularization": {"smooth_anisotropy_factor": aniso,
+                                                 "to_regularize": to_regularize},
+                              "output": {"freq": 10}},
+    })
+
+
+def twin_state(cfg, g):
+    st = State()
+    dev = torch.device("cuda", 0)
+    for k in ("thk", "usurf", "topg", "arrhenius", "slidingco", "x", "y"):
+        setattr(st, k, torch.as_tensor(g[k], device=dev))
+    st.dx = g["dx"]
+    mask = torch.as_tensor((g["thk"] > 0).astype(np.float32), device=dev)
+    st.icemask, st.icemaskobs = mask, mask.clone()
+    P.initialize(cfg, st)  # emulator built and run on the true geometry
+    rng = np.random.default_rng(5)
+    hole = torch.as_tensor(rng.random(g["thk"].shape) < 0.1, device=dev)
+    nan = torch.full_like(mask, float("nan"))
+    st.uvelsurfobs = torch.where(hole, nan, st.uvelsurf.clone())
+    st.vvelsurfobs = torch.where(hole, nan, st.vvelsurf.clone())
+    tob = torch.full_like(mask, float("nan"))
+    for col in (10, 30, 50):
+        tob[:, col] = st.thk[:, col]
+    st.thkobs = tob
+    return st
+
+
+def oracle_setup(cfg, st):
+    da = cfg.processes.data_assimilation
+    v = [torch.as_tensor(a.copy()) for a in st.iceflow_model.get_variables()]
+    cpu = lambda k: getattr(st, k).detach().cpu()
+    obs = dict(uobs=cpu("uvelsurfobs"), vobs=cpu("vvelsurfobs"), thkobs=cpu("thkobs"),
+               dens=O.da_density_weights(cpu("thkobs")), icemaskobs=cpu("icemaskobs"), icemask=cpu("icemask"))
+    r, f = da.regularization, da.fitting
+    p = O.AssimParams(velsurfobs_std=f.velsurfobs_std, velsurfobs_thr=f.velsurfobs_thr, thkobs_std=f.thkobs_std,
+                      regu_thk=r.thk, convexity_weight=r.convexity_weight, convexity_power=r.convexity_power,
+                      smooth_anisotropy_factor=r.smooth_anisotropy_factor, to_regularize=r.to_regularize)
+    ctl = O.AssimControl(step_size=da.optimization.step_size, step_size_decay=da.optimization.step_size_decay,
+                         scaling_thk=da.scaling.thk)
+    opt = O.KerasLegacyAdam(lr=da.optimization.step_size, epsilon=da.optimization.optimizer_epsilon,
+                            clipnorm=da.optimization.optimizer_clipnorm)
+    fields = {k: cpu(k) for k in ("usurf", "arrhenius", "slidingco")}
+    return v[0::2], v[1::2], obs, p, ctl, opt, fields
+
+
+def oracle_step(cfg, st, thk, setup, i):
+    ws, bs, obs, p, ctl, opt, fields = setup
+    return O.da_optimize_update(thk, fields["usurf"], fields["arrhenius"], fields["slidingco"], float(st.dx), ws, bs,
+                                NZ, O.define_vertical_weight(NZ, 4.0), obs, p, ctl, opt, i, bf16=True,
+                                out_scale=OUT, input_scales=SCALES)
+
+
+@pytest.mark.parametrize("aniso,to_regularize", [(0.2, "topg"), (1.0, "thk")])
+def test_first_iterations_match_oracle(tmp_path, monkeypatch, aniso, to_regularize):
+    monkeypatch.chdir(tmp_path)
+    cfg = make_cfg(2, aniso, to_regularize)
+    g = twin_glacier()
+    st = twin_state(cfg, g)
+    setup = oracle_setup(cfg, st)
+    DA.optimize_initialize(cfg, st)
+    thk_o = st.thk.detach().cpu().clone()
+    a = st._igm_assim
+    for i in range(3):
+        cost = {}
+        thk_prev = thk_o.numpy().copy()
+        DA.optimize_update(cfg, st, cost, i)
+        thk_o, cost_o, aux = oracle_step(cfg, st, thk_o, setup, i)
+        ours = cost["all"].cpu().numpy()
+        ref = np.array([float(cost_o.get(k, 0.0)) for k in DA._COST_KEYS])
+        np.testing.assert_allclose(ours, ref, rtol=2e-2, atol=1e-3 * np.abs(ref).max())
+        assert rel_l2(a.grad.view(a.ny, a.nx).cpu().numpy(), aux["gradient"].numpy()) < 5e-2
+        # the thickness steps: where Adam's epsilon dominates (tiny gradients) the step is
+        # proportional to the gradient, so the steps are compared relative to their size
+        d_ours = st.thk.cpu().numpy() - thk_prev
+        d_ref = thk_o.numpy() - thk_prev
+        agree = np.abs(d_ours - d_ref) <= 0.05 * np.abs(d_ref) + 1e-3
+        assert agree.mean() >= 0.97, (i, agree.mean())
+        np.testing.assert_allclose(st.divflux.cpu().numpy(),
+                                   O.divflux_upwind(aux["ubar"], aux["vbar"], st.thk.cpu(), float(st.dx)).numpy(),
+                                   rtol=2e-2, atol=2e-2 * float(aux["divflux"].abs().max()))
+        # continue both from the same thickness so that pixel flips do not accumulate
+        thk_o = st.thk.detach().cpu().clone()
+
+
+def test_twin_experiment_process_api(tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)
+    n = 100
+    cfg = make_cfg(n)
+    g = twin_glacier()
+    st = twin_state(cfg, g)
+    truth = torch.as_tensor(g["thk"])
+    setup = oracle_setup(cfg, st)
+    DA.initialize(cfg, st)
+    hist = st._igm_assim.cost_hist.cpu().numpy()
+    tot = hist.sum(1)
+    assert np.all(np.isfinite(tot))
+    assert tot[-1] < 0.45 * tot[0], (tot[0], tot[-1])
+    on = truth > 0
+    err0 = float(torch.sqrt(torch.mean(truth[on] ** 2)))
+    err = float(torch.sqrt(torch.mean((st.thk.cpu()[on] - truth[on]) ** 2)))
+    assert err < 0.75 * err0, (err0, err)
+    # the same loop through the oracle
+    thk_o = torch.zeros_like(truth)
+    ref = []
+    for i in range(n + 1):
+        thk_o, c, _ = oracle_step(cfg, st, thk_o, setup, i)
+        ref.append(sum(float(v) for v in c.values()))
+    ref = np.array(ref)
+    np.testing.assert_allclose(tot[::10], ref[::10], rtol=5e-2)
+    # outputs: final geometry, costs, rms/std/volume record, optimize.nc snapshots
+    np.testing.assert_allclose(st.topg.cpu().numpy(), (st.usurf - st.thk).cpu().numpy())
+    from scipy.io import netcdf_file
+    with netcdf_file("geology-optimized.nc", "r", mmap=False) as nc:
+        np.testing.assert_allclose(nc.variables["thk"][:], st.thk.cpu().numpy())
+    with netcdf_file("optimize.nc", "r", mmap=False) as nc:
+        assert nc.variables["thk"].shape == (n // 10 + 1, 40, 70)
+    costs = np.loadtxt("costs.dat", skiprows=1)
+    assert costs.shape == (n + 1, 5)
+    rms = np.loadtxt("rms_std_vol.dat", skiprows=1)
+    assert rms.shape == (n + 1, 9)
+    np.testing.assert_allclose(rms[-1, 8], float(st.thk.double().sum()) * 100.0 ** 2 / 1e9, rtol=1e-6)
+    ro = O.da_rms_std(st.thk.cpu(), st.thkobs.cpu(), st.uvelsurf.cpu(), st.vvelsurf.cpu(), st.uvelsurfobs.cpu(),
+                      st.vvelsurfobs.cpu(), st.icemaskobs.cpu(), 100.0)
+    np.testing.assert_allclose(rms[-1, [0, 1, 8]], [ro["rmsthk"], ro["stdthk"], ro["vol"]], rtol=1e-5, atol=1e-6)
