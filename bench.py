@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--pretrain", type=int, default=6000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-da", action="store_true")
     # iterations of the untimed reference solve, as a fraction of the full schedule
     # (small values make quick profiling runs; the timed region is unchanged)
     ap.add_argument("--ref-scale", type=float, default=1.0)
@@ -534,6 +535,146 @@ def plain_kernels(args, peaks, n=10):
     return out
 
 
+def assimilation_bench(args, peaks, K_it=20, warm=3, cpu_crop=200):
+    """The data_assimilation process at size^2 x Nz (16-layer emulator, random
+    He-normal weights: the timing does not depend on their values): K_it
+    iterations of the reference's loop body (optimize_update, the rms/std
+    record, the emulator retraining gate at retrain_freq 10: one Adam step on
+    four 500^2 patches every 10th iteration) timed with CUDA events, the
+    inputs resident; the cost/gradient kernel alone after an L2 flush against
+    the measured copy bandwidth (algorithmic bytes per node: reads thk, usurf,
+    the two emulated and two observed surface velocities, thkobs, the density
+    weights, icemaskobs and the two flow directions, writes dC/dthk and
+    dC/d(u, v)surf: 14 x 4 B); the oracle's iteration (torch-CPU FP32, the
+    same network) on a cpu_crop^2 crop, scaled by the node count."""
+    import torch
+    from igm_b200 import kernels as K
+    from igm_b200.config import default_cfg
+    from igm_b200.processes import data_assimilation as DA
+    from igm_b200.processes import iceflow as P
+    from igm_b200.state import State
+    from igm_b200.synthetic import valley_glacier
+    N, nz = args.size, args.nz
+    g = valley_glacier(N, N, 50.0, seed=0, varying_coeffs=True)
+    cfg = default_cfg({"iceflow": {"numerics": {"Nz": nz},
+                                   "emulator": {"pretrained": False, "input_scales": SCALES, "seed": 0,
+                                                "output_scale": 50.0,
+                                                "network": {"weight_initialization": "he_normal"}}},
+                       "data_assimilation": {"output": {"save_iterat_in_ncdf": False}}})
+    st = State()
+    for k in ("thk", "usurf", "topg", "arrhenius", "slidingco"):
+        setattr(st, k, torch.as_tensor(g[k]).cuda())
+    st.dx = 50.0
+    st.icemask = (st.thk > 0).float()
+    st.icemaskobs = st.icemask.clone()
+    P.initialize(cfg, st)
+    rng = np.random.default_rng(0)
+    hole = torch.as_tensor(rng.random((N, N)) < 0.1).cuda()
+    nan = torch.full_like(st.thk, float("nan"))
+    st.uvelsurfobs = torch.where(hole, nan, st.uvelsurf.clone())
+    st.vvelsurfobs = torch.where(hole, nan, st.vvelsurf.clone())
+    tob = nan.clone()
+    tob[:, ::50] = st.thk[:, ::50]
+    st.thkobs = tob
+    truth = st.thk.clone()
+    DA.optimize_initialize(cfg, st)
+    a = st._igm_assim
+    from igm_b200 import emulator as E
+
+    def iteration(i):
+        DA.optimize_update(cfg, st, {}, i)
+        DA._record_rms(a, st, i)
+        E.update_iceflow_emulator(cfg, st, i + 1)
+
+    for i in range(warm):
+        iteration(i)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(warm, warm + K_it):
+        iteration(i)
+    e1.record()
+    e1.synchronize()
+    ms_it = e0.elapsed_time(e1) / K_it
+    hist = a.cost_hist[:warm + K_it].sum(1).cpu().numpy()
+    # the cost/gradient kernel alone
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    flow = (st.flowdirx, st.flowdiry)
+    uvs, vvs = st.uvelsurf.contiguous(), st.vvelsurf.contiguous()
+    call = lambda: K.assim_cost_grad(st.thk, st.usurf, uvs, vvs, a.uobs, a.vobs, a.thkobs, a.dens, a.icemaskobs,
+                                     flow, 50.0, a.params, partials=a.partials, g_thk=a.g_thk)
+    for _ in range(3):
+        call()
+    ms = []
+    for _ in range(10):
+        flush.zero_()
+        # a ~1 ms device-side wait covers the host's enqueue of the call (argument marshalling)
+        torch.cuda._sleep(2_000_000)
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record()
+        call()
+        b1.record()
+        b1.synchronize()
+        ms.append(b0.elapsed_time(b1))
+    t = float(np.mean(ms)) / 1e3
+    per_node = 14 * 4
+    peak = peaks.get("hbm_gbs", 6650.0)
+    gbs = per_node * N * N / t / 1e9
+    out = {"workload": f"thickness inversion {N}x{N}xNz{nz}, 16-layer emulator, default data_assimilation "
+                       "configuration (anisotropic bed regularisation, retraining every 10 iterations)",
+           "ms_per_iteration": round(ms_it, 3), "iterations_per_s": round(1e3 / ms_it, 1),
+           "iterations_timed": K_it, "cost_first_last": [float(hist[0]), float(hist[-1])],
+           "cost_kernel": {"kernel": "assim_cost_grad_kernel<float>", "avg_launch_us": round(t * 1e6, 2),
+                           "algorithmic_bytes_per_node": per_node, "achieved_GBs": round(gbs, 1),
+                           "frac": round(gbs / peak, 4), "peak_GBs": peak}}
+    del st, a, flush
+    torch.cuda.empty_cache()
+    if not args.no_cpu:
+        out["cpu_port"] = assimilation_cpu(args, cpu_crop)
+    return out
+
+
+def assimilation_cpu(args, crop):
+    """The oracle's optimize_update iteration (torch-CPU FP32, bf16-free
+    16-layer network, all host threads) on a crop^2 glacier, per iteration
+    and scaled to size^2 by the node count (the work is linear in nodes)."""
+    import torch
+    from oracle import iceflow_oracle as O
+    from igm_b200.synthetic import valley_glacier
+    torch.set_num_threads(os.cpu_count() or 1)
+    nz = args.nz
+    g = valley_glacier(crop, crop, 50.0, seed=0, varying_coeffs=True)
+    f = {k: torch.as_tensor(g[k]) for k in ["thk", "usurf", "arrhenius", "slidingco"]}
+    rng = np.random.default_rng(0)
+    ws, bs, c = [], [], 5
+    for _ in range(16):
+        ws.append(torch.as_tensor(rng.normal(0, np.sqrt(2 / (9 * c)), (3, 3, c, 32)).astype(np.float32)))
+        bs.append(torch.zeros(32))
+        c = 32
+    ws.append(torch.as_tensor(rng.normal(0, np.sqrt(1 / 32), (1, 1, 32, 2 * nz)).astype(np.float32)))
+    bs.append(torch.zeros(2 * nz))
+    mask = (f["thk"] > 0).float()
+    tob = torch.full_like(f["thk"], float("nan"))
+    tob[:, ::50] = f["thk"][:, ::50]
+    obs = dict(uobs=torch.ones_like(mask), vobs=torch.zeros_like(mask), thkobs=tob, dens=O.da_density_weights(tob),
+               icemaskobs=mask, icemask=mask)
+    p, ctl = O.AssimParams(), O.AssimControl()
+    opt = O.KerasLegacyAdam(lr=1.0, clipnorm=1e7)
+    w = O.define_vertical_weight(nz, 4.0)
+    thk = f["thk"]
+    times = []
+    for i in range(2):
+        t0 = time.time()
+        thk, _, _ = O.da_optimize_update(thk, f["usurf"], f["arrhenius"], f["slidingco"], 50.0, ws, bs, nz, w, obs, p,
+                                         ctl, opt, i, bf16=False, out_scale=50.0, input_scales=SCALES)
+        times.append(time.time() - t0)
+    s_it = times[-1] * (args.size / crop) ** 2
+    return {"ms_per_iteration_scaled": round(s_it * 1e3, 1), "iterations_per_s": round(1.0 / s_it, 3),
+            "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": f"one optimize_update iteration of the oracle on a {crop}x{crop} crop (second of two), "
+                      f"scaled by ({args.size}/{crop})^2; emulator retraining not included"}
+
+
 def roofline_conv(conv_ms, size, peaks):
     """Forward 3x3 conv (cin = 32): algorithmic bytes per launch = one read of
     the input activation and one write of the output, 2 x 64 B per pixel."""
@@ -675,6 +816,7 @@ def main():
             "fallbacks": sum(1 for x in res["fallback_log"] if x["fallback"]),
             "roofline": roofline_conv(conv_ms, args.size, peaks),
             "plain_kernels": plain_kernels(args, peaks) if rank == 0 else None,
+            "data_assimilation": assimilation_bench(args, peaks) if rank == 0 and not args.no_da else None,
             "clocks": clocks, "gpu_launches": int(launches), "e2e": e2e, "setup_s": res["setup_s"]}
     if rank == 0 and world == 1 and not args.no_cpu:
         try:

@@ -111,12 +111,14 @@ SIGNATURES = {
     "igm_cnn_wgrad_finish_split": (I, [P, I, I, P, P]),
     "igm_cnn_head_backward_tc": (I, [I, I, I, I, P, P, P, P, C.c_float, C.c_float, P, P, P, I, P]),
     "igm_cnn_head_wgrad_finish": (I, [P, I, I, P, P]),
-    "igm_cnn_input_gradient": (I, [I, I, I, I, P, P, P, P, P]),
+    "igm_cnn_input_gradient": (I, [I, I, I, I, I, P, P, P, P, P]),
     "igm_assim_cost_grad": (I, [I, I, I, D] + [P] * 12 + [P, P, P, P, I, P, P]),
     "igm_assim_flow_direction": (I, [I, I, I, P, P, P, P, P, P]),
     "igm_divflux_upwind": (I, [I, I, I, D, P, P, P, P, P]),
     "igm_assim_control": (I, [I, I, C.c_size_t, D, I, I, P, P, P, P, P, P, P, P, P]),
+    "igm_assim_stats": (I, [I, I, I, D] + [P] * 11 + [P, I, P, P]),
     "igm_adam_clipnorm": (I, [I, P, P, P, P, P, P, D, D, D, D, D, C.c_int64, P]),
+    "igm_adam_norms_len": (C.c_size_t, [I, P]),
 }
 
 _lib = None

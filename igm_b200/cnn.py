@@ -54,7 +54,9 @@ class CNN:
         self.grads = torch.zeros_like(self.params)
         self.m = torch.zeros_like(self.params)
         self.v = torch.zeros_like(self.params)
-        self.norms = torch.zeros(len(self.shapes), dtype=torch.float64, device=self.device)
+        offs = (C.c_size_t * len(self.offsets))(*self.offsets)
+        self.norms = torch.zeros(int(L.lib().igm_adam_norms_len(len(self.shapes), offs)), dtype=torch.float64,
+                                 device=self.device)
         self.opt_iterations = 0
         self.wpack_f = torch.zeros(9 * 2 * F * 8 + (self.L - 1) * 9 * 4 * F * 8, dtype=torch.bfloat16,
                                    device=self.device)
@@ -196,8 +198,8 @@ class CNN:
     def backward(self, buf, B, h, w, dU, dV, field_grad=None, param_grads=True):
         """Gradients of the parameters into self.grads, given dE/dU, dE/dV
         (planar [B, nz, h, w]); requires forward(keep_acts=True).  With
-        ``field_grad`` (float32 [B, cin, h, w]) also the gradient with respect
-        to the raw input fields (igm_cnn_input_gradient); ``param_grads=False``
+        ``field_grad`` (float32 [B, n, h, w], n <= cin) also the gradient with
+        respect to the first n raw input fields (igm_cnn_input_gradient); ``param_grads=False``
         runs only the data-gradient chain (self.grads is then not written)."""
         lib, st = L.lib(), L.stream_ptr()
         acts = buf["acts"]
@@ -245,8 +247,11 @@ class CNN:
                 L.check(rc, "igm_cnn_wgrad_finish")
             elif l == 0:
                 if field_grad is not None:
-                    sc = (C.c_double * self.cin)(*[float(x) for x in self.scales[:self.cin]])
-                    rc = lib.igm_cnn_input_gradient(B, h, w, self.cin, _p(gl), self.params.data_ptr(), sc,
+                    ng = int(field_grad.shape[1])
+                    if field_grad.shape != (B, ng, h, w) or not field_grad.is_contiguous() or ng > self.cin:
+                        raise ValueError("field_grad must be contiguous float32 [B, n <= cin, h, w]")
+                    sc = (C.c_double * ng)(*[float(x) for x in self.scales[:ng]])
+                    rc = lib.igm_cnn_input_gradient(B, h, w, self.cin, ng, _p(gl), self.params.data_ptr(), sc,
                                                     _p(field_grad), st)
                     L.check(rc, "igm_cnn_input_gradient")
                 if param_grads:

@@ -31,127 +31,185 @@ struct AssimArgs {
   double* partials;  // [gridDim.x][kNCost]
 };
 
-// regularisation of one cell (cj, ci): its cost and d cost / d(dbdx), d(dbdy)
+// Scale factors of the cost sums and the gradients (host-computed once per
+// call): the kernel accumulates unscaled sums, the final reduction scales.
+struct AssimScales {
+  double c_vel, c_thk, c_pen, c_reg;  // cost = scale * sum
+  double gamma;                       // convexity weight
+};
+
+// A warp owns a strip of 30 columns (lanes 1..30; lanes 0 and 31 carry the
+// columns on either side) and walks down a segment of rows.  Each lane
+// evaluates the regularisation cell (j, c) to the lower right of its node
+// once per row; the gradient of a node gathers its four cells: the left
+// neighbour's by shuffle, the previous cell row from registers.  The node
+// inputs of row j + 1 are loaded while row j is evaluated.
+constexpr int kAmCols = 30;
+constexpr int kAmWarps = 4;
+
 template <typename T>
-__device__ __forceinline__ void cell_regu(const AssimArgs<T>& a, int cj, int ci, T s_a, T s_b, double* cost,
-                                          T* gdx, T* gdy) {
-  const int nx = a.nx;
-  auto fld = [&](int j, int i) -> T {
-    const size_t o = (size_t)j * nx + i;
-    return a.p.regularize_thk ? a.thk[o] : a.usurf[o] - a.thk[o];
+struct AssimRow {
+  T th, us;               // thk, usurf (this lane's column)
+  T uo, vo, uv, vv;       // observed / emulated surface velocities
+  T to, de, im;           // thkobs, density weight, icemaskobs
+  T fx, fy;               // flow direction of cell (j, c)
+};
+
+template <typename T>
+__device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimScales& sc, int lane, int strip,
+                                            int y0, int y1, double* acc) {
+  const int nx = a.nx, ny = a.ny;
+  const auto& p = a.p;
+  const int c = strip * kAmCols - 1 + lane;
+  const bool col = c >= 0 && c < nx;
+  const size_t cc = col ? (size_t)c : 0;
+  const bool cell_col = c >= 0 && c < nx - 1;
+  const bool out = lane >= 1 && lane <= kAmCols && col;
+  const bool aniso = p.aniso_factor != 1.0;
+  const bool reg_thk = p.regularize_thk != 0;
+  const T rdx = T(1) / a.dx, hr = T(0.5) * rdx;
+  const T w = (T)p.regu_thk;
+  const T s_a = (T)(1.0 / sqrt(p.aniso_factor)), s_b = (T)sqrt(p.aniso_factor);
+  const T thr = (T)p.velsurfobs_thr;
+  const T kv = (T)(1.0 / (p.velsurfobs_std * p.velsurfobs_std * p.n_vel));
+  const T kt = (T)(1.0 / (p.thkobs_std * p.thkobs_std * p.n_thk));
+  const T kp = (T)(2e10 / ((double)ny * nx));
+  const T kg = (T)(p.regu_thk * p.gamma);
+  auto load = [&](int j, bool full) {
+    AssimRow<T> r;
+    const bool ok = col && j < ny;
+    const size_t o = (size_t)j * nx + cc;
+    r.th = ok ? a.thk[o] : T(0);
+    r.us = (ok && !reg_thk) ? a.usurf[o] : T(0);
+    const bool okn = ok && full;
+    r.uo = okn ? a.uobs[o] : T(0);
+    r.vo = okn ? a.vobs[o] : T(0);
+    r.uv = okn ? a.uvs[o] : T(0);
+    r.vv = okn ? a.vvs[o] : T(0);
+    r.to = okn ? a.thkobs[o] : T(0);
+    r.de = okn ? a.dens[o] : T(0);
+    r.im = okn ? a.icemaskobs[o] : T(0);
+    const bool okc = aniso && cell_col && j < ny - 1;
+    const size_t q = (size_t)j * (nx - 1) + cc;
+    r.fx = okc ? a.fdx[q] : T(0);
+    r.fy = okc ? a.fdy[q] : T(0);
+    return r;
   };
-  const T f00 = fld(cj, ci), f01 = fld(cj, ci + 1), f10 = fld(cj + 1, ci), f11 = fld(cj + 1, ci + 1);
-  const T dx = a.dx;
-  const T dbdx = ((f01 - f00) / dx + (f11 - f10) / dx) / T(2);
-  const T dbdy = ((f10 - f00) / dx + (f11 - f01) / dx) / T(2);
-  const size_t c = (size_t)cj * (nx - 1) + ci;
-  const T fx = a.fdx[c], fy = a.fdy[c];
-  const T A = dbdx * fx + dbdy * fy, Bv = dbdx * fy - dbdy * fx;
-  const T w = (T)a.p.regu_thk;
-  if (cost) *cost = (double)w * ((double)s_a * (double)A * (double)A / 2.0 + (double)s_b * (double)Bv * (double)Bv / 2.0);
-  *gdx = w * (s_a * A * fx + s_b * Bv * fy);
-  *gdy = w * (s_a * A * fy - s_b * Bv * fx);
+  auto field = [&](const AssimRow<T>& r) { return reg_thk ? r.th : r.us - r.th; };
+  // cell (j, c) from the fields of rows j (f0 this lane, f0r the next lane) and j + 1
+  // -> P = gdx + gdy, M = gdx - gdy and its cost; the isotropic branch: the forward
+  // differences of this node
+  struct Cell {
+    T P, M, cost, dxp, dyp;
+  };
+  auto cell = [&](int j, T f0, T f1, const AssimRow<T>& r) {
+    Cell k{T(0), T(0), T(0), T(0), T(0)};
+    const T f0r = __shfl_down_sync(0xffffffffu, f0, 1);
+    const T f1r = __shfl_down_sync(0xffffffffu, f1, 1);
+    if (aniso) {
+      if (cell_col && j >= 0 && j < ny - 1) {
+        const T dbdx = ((f0r - f0) + (f1r - f1)) * hr;
+        const T dbdy = ((f1 - f0) + (f1r - f0r)) * hr;
+        const T A = dbdx * r.fx + dbdy * r.fy, B = dbdx * r.fy - dbdy * r.fx;
+        const T gdx = w * (s_a * A * r.fx + s_b * B * r.fy);
+        const T gdy = w * (s_a * A * r.fy - s_b * B * r.fx);
+        k.P = gdx + gdy;
+        k.M = gdx - gdy;
+        k.cost = s_a * A * A * T(0.5) + s_b * B * B * T(0.5);
+      }
+    } else if (col && j >= 0) {
+      if (c + 1 < nx) k.dxp = (f0r - f0) * rdx;
+      if (j + 1 < ny) k.dyp = (f1 - f0) * rdx;
+    }
+    return k;
+  };
+  // prologue: cell row y0 - 1
+  AssimRow<T> cur = load(y0, true);
+  T f_cur = field(cur);
+  Cell prev{T(0), T(0), T(0), T(0), T(0)};
+  if (y0 >= 1) {
+    const AssimRow<T> up = load(y0 - 1, false);
+    prev = cell(y0 - 1, field(up), f_cur, up);
+  }
+  for (int j = y0; j < y1; ++j) {
+    const AssimRow<T> nxt = load(j + 1, j + 1 < y1);
+    const T f_nxt = field(nxt);
+    const Cell k = cell(j, f_cur, f_nxt, cur);
+    T gf;
+    if (aniso) {
+      const T Ml = __shfl_up_sync(0xffffffffu, k.M, 1);
+      const T Pl = __shfl_up_sync(0xffffffffu, prev.P, 1);
+      gf = hr * ((Ml - k.P) + (Pl - prev.M));
+    } else {
+      const T dxm = __shfl_up_sync(0xffffffffu, k.dxp, 1);
+      gf = w * rdx * ((dxm - k.dxp) + (prev.dyp - k.dyp));
+    }
+    if (out) {
+      const size_t o = (size_t)j * nx + cc;
+      const T th = cur.th;
+      // surface-velocity misfit (misfit_velsurf.py:8-19)
+      const T nrm = sqrt(cur.uo * cur.uo + cur.vo * cur.vo);
+      const bool rel = nrm >= thr;  // false when a component is NaN
+      T gu = T(0), gv = T(0);
+      if (rel && !isnan(cur.uo)) {
+        const T d = cur.uo - cur.uv;
+        acc[kCVel] += (double)(d * d);
+        gu = -d * kv;
+      }
+      if (rel && !isnan(cur.vo)) {
+        const T d = cur.vo - cur.vv;
+        acc[kCVel] += (double)(d * d);
+        gv = -d * kv;
+      }
+      if (p.mask_velsurf && !(th > T(0))) {
+        gu = T(0);
+        gv = T(0);
+      }
+      a.g_u[o] = gu;
+      a.g_v[o] = gv;
+      T g = T(0);
+      // thickness misfit (misfit_thk.py:8-16)
+      if (!isnan(cur.to)) {
+        const T d = cur.to - th;
+        acc[kCThk] += (double)(cur.de * d * d);
+        g -= cur.de * d * kt;
+      }
+      // penalties (total_cost.py:36-46)
+      if (p.penalty) {
+        if (p.icemask_cost && !(cur.im > T(0.5))) {
+          acc[kCIce] += (double)(th * th);
+          g += kp * th;
+        }
+        if (!(th >= T(0))) {
+          acc[kCPos] += (double)(th * th);
+          g += kp * th;
+        }
+      }
+      // regularisation (regu_thk.py:8-70): smoothness cost of cell (j, c) or of this node's
+      // forward differences, the convexity term
+      const double rc = aniso ? (double)k.cost : 0.5 * ((double)k.dxp * k.dxp + (double)k.dyp * k.dyp);
+      acc[kCReg] += rc - sc.gamma * (double)th;
+      g += (reg_thk ? gf : -gf) - kg;
+      a.g_thk[o] = g;
+    }
+    prev = k;
+    cur = nxt;
+    f_cur = f_nxt;
+  }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) assim_cost_grad_kernel(const AssimArgs<T> a) {
-  const int ny = a.ny, nx = a.nx;
-  const size_t n = (size_t)ny * nx;
-  const auto& p = a.p;
-  const T inv_n = T(1) / (T)n;
-  const T s_a = (T)(1.0 / sqrt(p.aniso_factor)), s_b = (T)sqrt(p.aniso_factor);
+__global__ void __launch_bounds__(kAmWarps * 32) assim_cost_grad_kernel(const AssimArgs<T> a, const AssimScales sc,
+                                                                       int n_strips, int rows, int n_tasks) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double acc[kNCost] = {0, 0, 0, 0, 0};
-  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
-    const int j = (int)(o / nx), i = (int)(o - (size_t)j * nx);
-    const T th = a.thk[o];
-    // surface-velocity misfit (misfit_velsurf.py:8-19): components with an observation,
-    // at nodes whose observed speed reaches the threshold
-    const T uo = a.uobs[o], vo = a.vobs[o];
-    const T nrm = sqrt(uo * uo + vo * vo);
-    const bool rel = nrm >= (T)p.velsurfobs_thr;  // false when either component is NaN
-    const T sv = (T)p.velsurfobs_std;
-    T gu = T(0), gv = T(0);
-    if (rel && !isnan(uo)) {
-      const T r = (uo - a.uvs[o]) / sv;
-      acc[kCVel] += 0.5 * (double)r * (double)r / p.n_vel;
-      gu = -r / sv / (T)p.n_vel;
-    }
-    if (rel && !isnan(vo)) {
-      const T r = (vo - a.vvs[o]) / sv;
-      acc[kCVel] += 0.5 * (double)r * (double)r / p.n_vel;
-      gv = -r / sv / (T)p.n_vel;
-    }
-    // the emulated surface velocities are where(thk > 0, U, 0): no gradient off the ice
-    if (p.mask_velsurf && !(th > T(0))) {
-      gu = T(0);
-      gv = T(0);
-    }
-    a.g_u[o] = gu;
-    a.g_v[o] = gv;
-    T g = T(0);
-    // thickness misfit (misfit_thk.py:8-16)
-    const T to = a.thkobs[o];
-    if (!isnan(to)) {
-      const T st = (T)p.thkobs_std;
-      const T r = (to - th) / st;
-      acc[kCThk] += 0.5 * (double)a.dens[o] * (double)r * (double)r / p.n_thk;
-      g += -a.dens[o] * r / st / (T)p.n_thk;
-    }
-    // penalties (total_cost.py:36-46)
-    if (p.penalty) {
-      if (p.icemask_cost && !(a.icemaskobs[o] > T(0.5))) {
-        acc[kCIce] += 1e10 * (double)th * (double)th / (double)n;
-        g += T(2e10) * th * inv_n;
-      }
-      if (!(th >= T(0))) {
-        acc[kCPos] += 1e10 * (double)th * (double)th / (double)n;
-        g += T(2e10) * th * inv_n;
-      }
-    }
-    // regularisation (regu_thk.py:8-70): convexity term, then the smoothness terms
-    acc[kCReg] -= p.regu_thk * p.gamma * (double)th;
-    T gf = T(0);  // d cost / d field at this node
-    const T dx = a.dx, inv2dx = T(0.5) / dx;
-    if (p.aniso_factor != 1.0) {
-      // the four cells around the node; the cost of cell (j, i) is counted at this node
-#pragma unroll
-      for (int dj = 0; dj < 2; ++dj)
-#pragma unroll
-        for (int di = 0; di < 2; ++di) {
-          const int cj = j - 1 + dj, ci = i - 1 + di;
-          if (cj < 0 || ci < 0 || cj >= ny - 1 || ci >= nx - 1) continue;
-          double cc = 0.0;
-          T gdx, gdy;
-          cell_regu(a, cj, ci, s_a, s_b, (dj == 1 && di == 1) ? &cc : nullptr, &gdx, &gdy);
-          acc[kCReg] += cc;
-          // this node is corner (1 - dj, 1 - di) of the cell
-          gf += gdx * ((di == 0) ? inv2dx : -inv2dx) + gdy * ((dj == 0) ? inv2dx : -inv2dx);
-        }
-    } else {
-      auto fld = [&](int jj, int ii) -> T {
-        const size_t q = (size_t)jj * nx + ii;
-        return p.regularize_thk ? a.thk[q] : a.usurf[q] - a.thk[q];
-      };
-      const T w = (T)p.regu_thk, fc = fld(j, i);
-      if (i + 1 < nx) {
-        const T d = (fld(j, i + 1) - fc) / dx;
-        acc[kCReg] += (double)w * (double)d * (double)d / 2.0;
-        gf += -w * d / dx;
-      }
-      if (i >= 1) gf += w * ((fc - fld(j, i - 1)) / dx) / dx;
-      if (j + 1 < ny) {
-        const T d = (fld(j + 1, i) - fc) / dx;
-        acc[kCReg] += (double)w * (double)d * (double)d / 2.0;
-        gf += -w * d / dx;
-      }
-      if (j >= 1) gf += w * ((fc - fld(j - 1, i)) / dx) / dx;
-    }
-    g += (p.regularize_thk ? gf : -gf) - (T)(p.regu_thk * p.gamma);
-    a.g_thk[o] = g;
+  for (int t = blockIdx.x * kAmWarps + warp; t < n_tasks; t += gridDim.x * kAmWarps) {
+    const int strip = t % n_strips, seg = t / n_strips;
+    const int y0 = seg * rows, y1 = min(y0 + rows, a.ny);
+    assim_march<T>(a, sc, lane, strip, y0, y1, acc);
   }
   // deterministic block reduction: fixed xor trees, warps in order
-  __shared__ double red[8][kNCost];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ double red[kAmWarps][kNCost];
 #pragma unroll
   for (int c = 0; c < kNCost; ++c) {
     double v = acc[c];
@@ -161,17 +219,20 @@ __global__ void __launch_bounds__(256) assim_cost_grad_kernel(const AssimArgs<T>
   __syncthreads();
   if (threadIdx.x < kNCost) {
     double v = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
+    for (int w = 0; w < kAmWarps; ++w) v += red[w][threadIdx.x];
     a.partials[(size_t)blockIdx.x * kNCost + threadIdx.x] = v;
   }
 }
 
-__global__ void assim_sum_kernel(const double* partials, int n_parts, double* costs) {
-  const int c = threadIdx.x;
-  if (c >= kNCost) return;
+// one warp per cost: lanes stride over the partials, then a fixed xor tree
+__global__ void assim_sum_kernel(const double* partials, int n_parts, AssimScales sc, double* costs) {
+  const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (c >= kNCost) return;  // uniform per warp
   double v = 0.0;
-  for (int b = 0; b < n_parts; ++b) v += partials[(size_t)b * kNCost + c];
-  costs[c] = v;
+  for (int b = lane; b < n_parts; b += 32) v += partials[(size_t)b * kNCost + c];
+  for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+  const double f = c == kCVel ? sc.c_vel : c == kCThk ? sc.c_thk : c == kCReg ? sc.c_reg : sc.c_pen;
+  if (lane == 0) costs[c] = f * v;
 }
 
 // ---- flow direction (utils.py:86-110) --------------------------------------
@@ -241,12 +302,25 @@ static int cost_grad_t(int ny, int nx, double dx, const void* thk, const void* u
   a.p = *p;
   a.g_thk = (T*)g_thk; a.g_u = (T*)g_u; a.g_v = (T*)g_v;
   a.partials = partials;
-  int grid = grid_n((size_t)ny * nx);
+  AssimScales sc{};
+  sc.c_vel = 0.5 / (p->velsurfobs_std * p->velsurfobs_std * p->n_vel);
+  sc.c_thk = 0.5 / (p->thkobs_std * p->thkobs_std * p->n_thk);
+  sc.c_pen = 1e10 / ((double)ny * nx);
+  sc.c_reg = p->regu_thk;
+  sc.gamma = p->gamma;
+  // segments of rows sized for about 32 resident warps per SM, at least 8 rows; the
+  // warps stride over the (strip, segment) tasks so the grid fits the partials
+  const int n_strips = (nx + kAmCols - 1) / kAmCols;
+  const long long target = 148LL * 32;
+  int rows = (int)((n_strips * (long long)ny + target - 1) / target);
+  rows = rows < 8 ? 8 : rows;
+  const long long tasks = (long long)n_strips * ((ny + rows - 1) / rows);
+  long long grid = (tasks + kAmWarps - 1) / kAmWarps;
   if (grid > n_parts) grid = n_parts;
-  assim_cost_grad_kernel<T><<<grid, 256, 0, st>>>(a);
+  assim_cost_grad_kernel<T><<<(int)grid, kAmWarps * 32, 0, st>>>(a, sc, n_strips, rows, (int)tasks);
   int rc = launch_status("assim_cost_grad_kernel");
   if (rc) return rc;
-  assim_sum_kernel<<<1, 32, 0, st>>>(partials, grid, costs);
+  assim_sum_kernel<<<1, 32 * kNCost, 0, st>>>(partials, (int)grid, sc, costs);
   return launch_status("assim_sum_kernel");
 }
 
@@ -305,6 +379,100 @@ __global__ void assim_control_kernel(size_t n, int mode, T sc, int reproject_mas
       thk[o] = t;
     }
   }
+}
+
+// compute_rms_std_optimization (data_assimilation/utils.py:10-66): count, sum
+// and sum of squares of the misfits thk - thkobs (at the thickness
+// observations), |velsurf| - |velsurfobs| (inside icemaskobs > 0.5 where the
+// observed speed is defined), divfluxobs - divflux and usurf - usurfobs (inside
+// the mask), and the sum of thk; per-block FP64 partials, then one warp turns
+// them into the nine record entries.
+constexpr int kNStat = 13;
+
+template <typename T>
+struct StatArgs {
+  size_t n;
+  const T *thk, *thkobs, *uvs, *vvs, *uobs, *vobs, *im, *div, *divobs, *us, *usobs;
+  double* partials;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) assim_stats_kernel(const StatArgs<T> a) {
+  double acc[kNStat];
+#pragma unroll
+  for (int k = 0; k < kNStat; ++k) acc[k] = 0.0;
+  auto add = [&](int k, T d) {
+    acc[k] += 1.0;
+    acc[k + 1] += (double)d;
+    acc[k + 2] += (double)d * (double)d;
+  };
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < a.n; o += (size_t)gridDim.x * blockDim.x) {
+    const T th = a.thk[o];
+    acc[12] += (double)th;
+    if (a.thkobs) {
+      const T to = a.thkobs[o];
+      if (!isnan(to)) add(0, th - to);
+    }
+    const bool in = a.im[o] > T(0.5);
+    if (in && a.uobs) {
+      const T uo = a.uobs[o], vo = a.vobs[o];
+      const T mo = sqrt(uo * uo + vo * vo);
+      if (!isnan(mo)) {
+        const T u = a.uvs[o], v = a.vvs[o];
+        add(3, sqrt(u * u + v * v) - mo);
+      }
+    }
+    if (in && a.divobs) add(6, a.divobs[o] - a.div[o]);
+    if (in && a.usobs) add(9, a.us[o] - a.usobs[o]);
+  }
+  __shared__ double red[8][kNStat];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kNStat; ++k) {
+    double v = acc[k];
+    for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+    if (lane == 0) red[warp][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kNStat) {
+    double v = 0.0;
+    for (int w = 0; w < 8; ++w) v += red[w][threadIdx.x];
+    a.partials[(size_t)blockIdx.x * kNStat + threadIdx.x] = v;
+  }
+}
+
+// out[9]: rmsthk, stdthk, rmsvel, stdvel, rmsdiv, stddiv, rmsusurf, stdusurf, vol
+// (means and population standard deviations; a term without data is 0, an empty
+// mask gives NaN as numpy's mean of an empty selection)
+__global__ void assim_stats_finish_kernel(const double* partials, int n_parts, double dx2, int have_thk,
+                                          int have_vel, int have_div, int have_us, double* out) {
+  const int lane = threadIdx.x;
+  double tot[kNStat];
+#pragma unroll
+  for (int k = 0; k < kNStat; ++k) {
+    double v = 0.0;
+    for (int b = lane; b < n_parts; b += 32) v += partials[(size_t)b * kNStat + k];
+    for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+    tot[k] = v;
+  }
+  if (lane != 0) return;
+  const int have[4] = {have_thk, have_vel, have_div, have_us};
+  for (int t = 0; t < 4; ++t) {
+    const double c = tot[3 * t], s1 = tot[3 * t + 1], s2 = tot[3 * t + 2];
+    double mean = 0.0, sd = 0.0;
+    if (have[t]) {
+      if (t == 0 && c == 0.0) {
+        mean = sd = 0.0;  // no thickness observation: the reference records 0
+      } else {
+        mean = s1 / c;
+        const double var = s2 / c - mean * mean;
+        sd = sqrt(var > 0.0 ? var : 0.0);
+      }
+    }
+    out[2 * t] = mean;
+    out[2 * t + 1] = sd;
+  }
+  out[8] = tot[12] * dx2 / 1e9;
 }
 
 }  // namespace igm
@@ -374,4 +542,42 @@ extern "C" int igm_assim_control(int dtype, int mode, size_t n, double scale, in
     return IGM_ERR_BAD_ARGUMENT;
   }
   return launch_status("assim_control_kernel");
+}
+
+extern "C" int igm_assim_stats(int dtype, int ny, int nx, double dx, const void* thk, const void* thkobs,
+                               const void* uvelsurf, const void* vvelsurf, const void* uvelsurfobs,
+                               const void* vvelsurfobs, const void* icemaskobs, const void* divflux,
+                               const void* divfluxobs, const void* usurf, const void* usurfobs, double* partials,
+                               int n_parts, double* out, void* stream) {
+  IGM_CHECK_ARG(ny >= 1 && nx >= 1, IGM_ERR_BAD_SHAPE, "igm_assim_stats: bad shape %dx%d", ny, nx);
+  IGM_CHECK_ARG(thk && icemaskobs && partials && out && n_parts >= 1, IGM_ERR_BAD_ARGUMENT,
+                "igm_assim_stats: NULL argument");
+  IGM_CHECK_ARG(!uvelsurfobs || (vvelsurfobs && uvelsurf && vvelsurf), IGM_ERR_BAD_ARGUMENT,
+                "igm_assim_stats: velocity observations need both components and the emulated velocities");
+  IGM_CHECK_ARG(!divfluxobs || divflux, IGM_ERR_BAD_ARGUMENT, "igm_assim_stats: divfluxobs needs divflux");
+  IGM_CHECK_ARG(!usurfobs || usurf, IGM_ERR_BAD_ARGUMENT, "igm_assim_stats: usurfobs needs usurf");
+  cudaStream_t st = as_stream(stream);
+  const size_t n = (size_t)ny * nx;
+  int grid = grid_n(n);
+  if (grid > n_parts) grid = n_parts;
+  auto run = [&](auto zero) {
+    using T = decltype(zero);
+    StatArgs<T> a{n, (const T*)thk, (const T*)thkobs, (const T*)uvelsurf, (const T*)vvelsurf,
+                  (const T*)uvelsurfobs, (const T*)vvelsurfobs, (const T*)icemaskobs, (const T*)divflux,
+                  (const T*)divfluxobs, (const T*)usurf, (const T*)usurfobs, partials};
+    assim_stats_kernel<T><<<grid, 256, 0, st>>>(a);
+  };
+  if (dtype == IGM_F32)
+    run(0.f);
+  else if (dtype == IGM_F64)
+    run(0.0);
+  else {
+    set_error("igm_assim_stats: unknown dtype %d", dtype);
+    return IGM_ERR_BAD_ARGUMENT;
+  }
+  int rc = launch_status("assim_stats_kernel");
+  if (rc) return rc;
+  assim_stats_finish_kernel<<<1, 32, 0, st>>>(partials, grid, dx * dx, thkobs != nullptr, uvelsurfobs != nullptr,
+                                              divfluxobs != nullptr, usurfobs != nullptr, out);
+  return launch_status("assim_stats_finish_kernel");
 }

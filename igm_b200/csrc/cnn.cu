@@ -857,18 +857,39 @@ __global__ void __launch_bounds__(kFinWarps * 32) wgrad_finish_split_kernel(cons
 // Adam (Keras legacy): per-variable clip_by_norm, then
 //   m += (g - m)(1 - b1); v += (g^2 - v)(1 - b2); x -= lr_t m / (sqrt(v) + eps)
 // ---------------------------------------------------------------------------
+// The squared norms in two deterministic stages: one CTA per chunk of
+// kNormChunk elements of a variable (partial sums after the norms in the
+// scratch), then one warp per variable adds its chunks in a fixed order.
+constexpr size_t kNormChunk = 4096;
+
 struct AdamVars {
   int n;
   size_t off[IGM_MAX_VARS + 1];
+  int cbase[IGM_MAX_VARS + 1];  // first chunk of each variable; cbase[n] = number of chunks
 };
 
-__global__ void __launch_bounds__(256) grad_norms_kernel(const float* g, const AdamVars vars, double* norms) {
+static int norm_chunks(size_t len) { return (int)((len + kNormChunk - 1) / kNormChunk); }
+
+__global__ void __launch_bounds__(256) grad_norm_parts_kernel(const float* g, const AdamVars vars, double* parts) {
   __shared__ double sh[8];
-  const int v = blockIdx.x;
+  const int b = blockIdx.x;
+  int v = 0;
+  while (v + 1 < vars.n && b >= vars.cbase[v + 1]) ++v;
+  const size_t lo = vars.off[v] + (size_t)(b - vars.cbase[v]) * kNormChunk;
+  const size_t hi = min(vars.off[v + 1], lo + kNormChunk);
   double s = 0.0;
-  for (size_t i = vars.off[v] + threadIdx.x; i < vars.off[v + 1]; i += blockDim.x) s += (double)g[i] * g[i];
+  for (size_t i = lo + threadIdx.x; i < hi; i += blockDim.x) s += (double)g[i] * g[i];
   s = block_sum<256>(s, sh, threadIdx.x);
-  if (threadIdx.x == 0) norms[v] = sqrt(s);
+  if (threadIdx.x == 0) parts[b] = s;
+}
+
+__global__ void grad_norm_finish_kernel(const double* parts, const AdamVars vars, double* norms) {
+  const int v = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (v >= vars.n) return;  // uniform per warp
+  double s = 0.0;
+  for (int c = vars.cbase[v] + lane; c < vars.cbase[v + 1]; c += 32) s += parts[c];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) norms[v] = sqrt(s);
 }
 
 __global__ void adam_kernel(float* x, const float* g, float* m, float* v, const AdamVars vars, const double* norms,
@@ -908,11 +929,14 @@ static int grid_for(size_t n, int per = 256) {
 // ---------------------------------------------------------------------------
 struct InputGradScales { float s[8]; };
 
-template <int CIN>
-__global__ void __launch_bounds__(256) input_grad_kernel(int B, int H, int W, const __nv_bfloat16* dpre,
+template <int NG>
+__global__ void __launch_bounds__(256) input_grad_kernel(int B, int H, int W, int cin, const __nv_bfloat16* dpre,
                                                          const float* w0, InputGradScales sc, float* out) {
-  __shared__ float sw[9 * CIN * kF];  // [tap][c][co]
-  for (int i = threadIdx.x; i < 9 * CIN * kF; i += blockDim.x) sw[i] = w0[i];
+  __shared__ float sw[9 * NG * kF];  // [tap][c][co] of the fields computed
+  for (int i = threadIdx.x; i < 9 * NG * kF; i += blockDim.x) {
+    const int tap = i / (NG * kF), r = i - tap * NG * kF;
+    sw[i] = w0[(size_t)tap * cin * kF + r];
+  }
   __syncthreads();
   const size_t plane = (size_t)H * W;
   const size_t total = plane * B;
@@ -920,9 +944,9 @@ __global__ void __launch_bounds__(256) input_grad_kernel(int B, int H, int W, co
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const size_t b = i / plane, rem = i - b * plane;
     const int y = (int)(rem / W), x = (int)(rem - (size_t)(rem / W) * W);
-    float acc[CIN];
+    float acc[NG];
 #pragma unroll
-    for (int c = 0; c < CIN; ++c) acc[c] = 0.f;
+    for (int c = 0; c < NG; ++c) acc[c] = 0.f;
 #pragma unroll
     for (int kh = 0; kh < 3; ++kh) {
       const int yy = y - kh + 1;
@@ -931,7 +955,7 @@ __global__ void __launch_bounds__(256) input_grad_kernel(int B, int H, int W, co
       for (int kw = 0; kw < 3; ++kw) {
         const int xx = x - kw + 1;
         if (xx < 0 || xx >= W) continue;
-        const float* wt = sw + (kh * 3 + kw) * CIN * kF;
+        const float* wt = sw + (kh * 3 + kw) * NG * kF;
 #pragma unroll
         for (int ch = 0; ch < 4; ++ch) {
           const uint4 u = D[((b * H + yy) * 4 + ch) * W + xx];
@@ -941,13 +965,13 @@ __global__ void __launch_bounds__(256) input_grad_kernel(int B, int H, int W, co
             const int co = ch * 8 + e;
             const float d = (e & 1) ? bf_hi(wv[e >> 1]) : bf_lo(wv[e >> 1]);
 #pragma unroll
-            for (int c = 0; c < CIN; ++c) acc[c] = fmaf(d, wt[c * kF + co], acc[c]);
+            for (int c = 0; c < NG; ++c) acc[c] = fmaf(d, wt[c * kF + co], acc[c]);
           }
         }
       }
     }
 #pragma unroll
-    for (int c = 0; c < CIN; ++c) out[(b * CIN + c) * plane + rem] = acc[c] * sc.s[c];
+    for (int c = 0; c < NG; ++c) out[(b * NG + c) * plane + rem] = acc[c] * sc.s[c];
   }
 }
 
@@ -1178,6 +1202,14 @@ extern "C" int igm_cnn_wgrad_finish_split(const float* partials, int n_parts, in
   return launch_status("wgrad_finish_split_kernel");
 }
 
+extern "C" size_t igm_adam_norms_len(int n_vars, const size_t* var_offsets) {
+  if (n_vars < 1 || n_vars > IGM_MAX_VARS || !var_offsets) return 0;
+  size_t len = (size_t)n_vars;
+  for (int i = 0; i < n_vars; ++i)
+    len += var_offsets[i + 1] > var_offsets[i] ? (size_t)norm_chunks(var_offsets[i + 1] - var_offsets[i]) : 0;
+  return len;
+}
+
 extern "C" int igm_adam_clipnorm(int n_vars, const size_t* var_offsets, float* params, const float* grads,
                                  float* m, float* v, double* norms, double lr, double beta_1, double beta_2,
                                  double epsilon, double clipnorm, int64_t iteration, void* stream) {
@@ -1188,32 +1220,41 @@ extern "C" int igm_adam_clipnorm(int n_vars, const size_t* var_offsets, float* p
   AdamVars vars{};
   vars.n = n_vars;
   for (int i = 0; i <= n_vars; ++i) vars.off[i] = var_offsets[i];
+  vars.cbase[0] = 0;
+  for (int i = 0; i < n_vars; ++i) {
+    IGM_CHECK_ARG(var_offsets[i + 1] > var_offsets[i], IGM_ERR_BAD_ARGUMENT, "igm_adam_clipnorm: empty variable %d",
+                  i);
+    vars.cbase[i + 1] = vars.cbase[i] + norm_chunks(var_offsets[i + 1] - var_offsets[i]);
+  }
   const double t = (double)iteration;
   const float b1p = powf((float)beta_1, (float)t), b2p = powf((float)beta_2, (float)t);
   const float lr_t = (float)lr * sqrtf(1.f - b2p) / (1.f - b1p);
   cudaStream_t st = as_stream(stream);
-  grad_norms_kernel<<<n_vars, 256, 0, st>>>(grads, vars, norms);
-  int rc = launch_status("grad_norms_kernel");
+  double* parts = norms + n_vars;
+  grad_norm_parts_kernel<<<vars.cbase[n_vars], 256, 0, st>>>(grads, vars, parts);
+  int rc = launch_status("grad_norm_parts_kernel");
   if (rc) return rc;
+  grad_norm_finish_kernel<<<(n_vars + 3) / 4, 128, 0, st>>>(parts, vars, norms);
+  if ((rc = launch_status("grad_norm_finish_kernel"))) return rc;
   adam_kernel<<<grid_for(vars.off[n_vars]), 256, 0, st>>>(params, grads, m, v, vars, norms, lr_t, (float)beta_1,
                                                          (float)beta_2, (float)epsilon, (float)clipnorm);
   return launch_status("adam_kernel");
 }
 
-extern "C" int igm_cnn_input_gradient(int batch, int h, int w, int cin, const void* dpre0, const float* w0,
-                                      const double* scales, float* out, void* stream) {
-  IGM_CHECK_ARG(batch >= 1 && h >= 1 && w >= 1 && cin >= 1 && cin <= 8, IGM_ERR_BAD_SHAPE,
-                "igm_cnn_input_gradient: bad shape");
+extern "C" int igm_cnn_input_gradient(int batch, int h, int w, int cin, int n_grad, const void* dpre0,
+                                      const float* w0, const double* scales, float* out, void* stream) {
+  IGM_CHECK_ARG(batch >= 1 && h >= 1 && w >= 1 && cin >= 1 && cin <= 8 && n_grad >= 1 && n_grad <= cin,
+                IGM_ERR_BAD_SHAPE, "igm_cnn_input_gradient: bad shape");
   IGM_CHECK_ARG(dpre0 && w0 && scales && out, IGM_ERR_BAD_ARGUMENT, "igm_cnn_input_gradient: NULL argument");
   InputGradScales sc{};
-  for (int c = 0; c < cin; ++c) sc.s[c] = (float)scales[c];
+  for (int c = 0; c < n_grad; ++c) sc.s[c] = (float)scales[c];
   const int grid = grid_for((size_t)batch * h * w);
   cudaStream_t st = as_stream(stream);
   const __nv_bfloat16* d = (const __nv_bfloat16*)dpre0;
-  switch (cin) {
+  switch (n_grad) {
 #define IGM_IG(C)                                                                      \
   case C:                                                                              \
-    input_grad_kernel<C><<<grid, 256, 0, st>>>(batch, h, w, d, w0, sc, out);           \
+    input_grad_kernel<C><<<grid, 256, 0, st>>>(batch, h, w, cin, d, w0, sc, out);      \
     break;
     IGM_IG(1) IGM_IG(2) IGM_IG(3) IGM_IG(4) IGM_IG(5) IGM_IG(6) IGM_IG(7) IGM_IG(8)
 #undef IGM_IG

@@ -214,6 +214,23 @@ def assim_control(mode, thk, scale, icemaskobs=None, variable=None, grad=None, m
     L.check(rc, "igm_assim_control")
 
 
+def assim_stats(thk, dx, icemaskobs, thkobs=None, uvs=None, vvs=None, uobs=None, vobs=None, divflux=None,
+                divfluxobs=None, usurf=None, usurfobs=None, out=None, partials=None):
+    """The rms/std/volume record of one assimilation iteration (igm_assim_stats):
+    device double[9] rmsthk, stdthk, rmsvel, stdvel, rmsdiv, stddiv, rmsusurf,
+    stdusurf, vol; an observation given as None gives 0 for its pair."""
+    ny, nx = thk.shape
+    out = out if out is not None else torch.empty(9, dtype=torch.float64, device=thk.device)
+    partials = partials if partials is not None else torch.empty(148 * 8 * 13, dtype=torch.float64,
+                                                                 device=thk.device)
+    rc = L.lib().igm_assim_stats(L.dtype_code(thk.dtype), ny, nx, float(dx), L.ptr(thk), L.ptr(thkobs), L.ptr(uvs),
+                                 L.ptr(vvs), L.ptr(uobs), L.ptr(vobs), L.ptr(icemaskobs), L.ptr(divflux),
+                                 L.ptr(divfluxobs), L.ptr(usurf), L.ptr(usurfobs), L.ptr(partials),
+                                 partials.numel() // 13, L.ptr(out), L.stream_ptr())
+    L.check(rc, "igm_assim_stats")
+    return out
+
+
 def divflux_upwind(u, v, h, dx, out=None):
     ny, nx = h.shape
     out = out if out is not None else torch.empty_like(h)

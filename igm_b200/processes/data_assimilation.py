@@ -126,16 +126,17 @@ class _Assim:
         self.nz = nz
         f32 = dict(dtype=torch.float32, device=d)
         self.var, self.grad, self.m, self.v = (torch.empty(self.n, **f32) for _ in range(4))
-        self.norms = torch.empty(1, dtype=torch.float64, device=d)
         self.offsets = (C.c_size_t * 2)(0, self.n)
+        self.norms = torch.empty(int(L.lib().igm_adam_norms_len(1, self.offsets)), dtype=torch.float64, device=d)
         self.dU = torch.zeros((1, nz, ny, nx), **f32)
         self.dV = torch.zeros((1, nz, ny, nx), **f32)
         self.g_thk = torch.empty((ny, nx), **f32)
-        self.field_grad = torch.empty((1, 5, ny, nx), **f32)
+        self.field_grad = torch.empty((1, 1, ny, nx), **f32)  # the thk channel only
         self.partials = torch.empty(148 * 8 * 5, dtype=torch.float64, device=d)
         nit = int(da.optimization.nbitmax) + 1
         self.cost_hist = torch.zeros((nit, 5), dtype=torch.float64, device=d)
         self.rms_hist = torch.zeros((nit, 9), dtype=torch.float64, device=d)
+        self.stat_partials = torch.empty(148 * 8 * 13, dtype=torch.float64, device=d)
         # parameters of igm_assim_cost_grad
         p = L.AssimParams()
         f, r, o = da.fitting, da.regularization, da.optimization
@@ -146,8 +147,9 @@ class _Assim:
         p.aniso_factor = float(r.smooth_anisotropy_factor)
         vo = torch.stack([self.uobs, self.vobs], -1).double()
         rel = torch.linalg.vector_norm(vo, dim=-1) >= float(f.velsurfobs_thr)
-        p.n_vel = float((~torch.isnan(vo) & rel[..., None]).sum().item())
-        p.n_thk = float((~torch.isnan(self.thkobs)).sum().item())
+        # the means' counts (an absent term has no contributions; its count is kept at 1)
+        p.n_vel = max(1.0, float((~torch.isnan(vo) & rel[..., None]).sum().item()))
+        p.n_thk = max(1.0, float((~torch.isnan(self.thkobs)).sum().item()))
         p.penalty = int("penalty" in o.obstacle_constraint)
         p.icemask_cost = int("icemask" in costs)
         p.regularize_thk = int(r.to_regularize == "thk")
@@ -183,35 +185,17 @@ def optimize_initialize(cfg, state):
 
 
 def _record_rms(a: _Assim, state, i):
-    """compute_rms_std_optimization (utils.py:10-66) as device reductions
-    into row i of the history: rmsthk, stdthk, rmsvel, stdvel, rmsdiv,
-    stddiv, rmsusurf, stdusurf, vol (the means and population standard
-    deviations of the misfits over their masks)."""
-    thk = S.get(state, "thk")
-
-    def mean_std(d, mask):
-        m = mask.double()
-        cnt = m.sum()
-        dd = torch.where(mask, d.double(), torch.zeros_like(m))
-        mu = dd.sum() / cnt.clamp(min=1)
-        sd = torch.sqrt((torch.where(mask, dd - mu, torch.zeros_like(m)) ** 2).sum() / cnt.clamp(min=1))
-        return mu, sd
-
-    row = a.rms_hist[i]
-    if hasattr(state, "thkobs"):
-        tob = S.get(state, "thkobs")
-        row[0], row[1] = mean_std(thk - tob, ~torch.isnan(tob))
-    inside = a.icemaskobs > 0.5
-    if hasattr(state, "uvelsurfobs"):
-        uo, vo = S.get(state, "uvelsurfobs"), S.get(state, "vvelsurfobs")
-        vs = torch.sqrt(S.get(state, "uvelsurf") ** 2 + S.get(state, "vvelsurf") ** 2)
-        vob = torch.sqrt(uo * uo + vo * vo)
-        row[2], row[3] = mean_std(vs - vob, inside & ~torch.isnan(vob))
-    if hasattr(state, "divfluxobs"):
-        row[4], row[5] = mean_std(S.get(state, "divfluxobs") - S.get(state, "divflux"), inside)
-    if hasattr(state, "usurfobs"):
-        row[6], row[7] = mean_std(S.get(state, "usurf") - S.get(state, "usurfobs"), inside)
-    row[8] = thk.double().sum() * a.dx ** 2 / 1e9
+    """compute_rms_std_optimization (utils.py:10-66) into row i of the
+    device history (igm_assim_stats): rmsthk, stdthk, rmsvel, stdvel, rmsdiv,
+    stddiv, rmsusurf, stdusurf, vol."""
+    g = lambda k: S.get(state, k).contiguous() if hasattr(state, k) else None
+    vel = hasattr(state, "uvelsurfobs")
+    K.assim_stats(S.get(state, "thk"), a.dx, a.icemaskobs, thkobs=g("thkobs"),
+                  uvs=g("uvelsurf") if vel else None, vvs=g("vvelsurf") if vel else None,
+                  uobs=g("uvelsurfobs"), vobs=g("vvelsurfobs"),
+                  divflux=g("divflux") if hasattr(state, "divfluxobs") else None, divfluxobs=g("divfluxobs"),
+                  usurf=g("usurf") if hasattr(state, "usurfobs") else None, usurfobs=g("usurfobs"),
+                  out=a.rms_hist[i], partials=a.stat_partials)
 
 
 def optimize_update(cfg, state, cost, i):

@@ -2,8 +2,10 @@
 (``python -m igm_b200.prof_cases``; run it under ncu with -k and -c).
 
 Stencil (energy, energy + adjoint, one fused Adam iteration), transport and
-the vertical velocity at 1500 x 1500 x Nz 10 in FP32; the tensor-core
-convolution (forward, dgrad, wgrad) at batch 2 x 1000 x 1000 x 32 channels.
+the vertical velocity at 1500 x 1500 x Nz 10 in FP32; the data-assimilation
+cost/gradient, flow direction and upwind divergence at 1500 x 1500 in FP32;
+the tensor-core convolution (forward, dgrad, wgrad) at batch 2 x 1000 x 1000
+x 32 channels.
 """
 
 from __future__ import annotations
@@ -16,6 +18,36 @@ from . import kernels as K
 from .solver import DeviceAdamSolver
 from .synthetic import valley_glacier
 from .vertical import compute_levels, compute_zeta_dzeta, define_vertical_weight
+
+
+def assimilation_inputs(N, thk, uvs, vvs, seed=0):
+    """Observations for the data-assimilation kernels: surface velocities
+    with 10% missing, thickness profiles on every 50th column, the ice mask
+    of thk > 0, uniform density weights."""
+    rng = np.random.default_rng(seed)
+    hole = torch.as_tensor(rng.random((N, N)) < 0.1, device=thk.device)
+    nan = torch.full_like(thk, float("nan"))
+    uobs = torch.where(hole, nan, uvs + 1.0)
+    vobs = torch.where(hole, nan, vvs - 1.0)
+    thkobs = nan.clone()
+    thkobs[:, ::50] = thk[:, ::50]
+    mask = (thk > 0).float()
+    p = L.AssimParams()
+    p.velsurfobs_std, p.velsurfobs_thr, p.thkobs_std, p.regu_thk = 1.0, 0.0, 3.0, 10.0
+    p.gamma, p.aniso_factor = 1e-8, 0.2
+    p.n_vel = float((~torch.isnan(uobs)).sum().item() * 2)
+    p.n_thk = float((~torch.isnan(thkobs)).sum().item())
+    p.penalty, p.icemask_cost, p.regularize_thk, p.mask_velsurf = 1, 1, 0, 1
+    return dict(uobs=uobs, vobs=vobs, thkobs=thkobs, dens=torch.ones_like(thk), mask=mask, params=p)
+
+
+def assimilation(N, f, uvs, vvs):
+    """One launch each of the data-assimilation kernels."""
+    a = assimilation_inputs(N, f[0], uvs, vvs)
+    flow = K.assim_flow_direction(uvs, vvs)                       # flow direction (3 kernels)
+    K.assim_cost_grad(f[0], f[1], uvs, vvs, a["uobs"], a["vobs"], a["thkobs"], a["dens"], a["mask"], flow, 50.0,
+                      a["params"])                                # cost terms + gradient
+    K.divflux_upwind(uvs, vvs, f[0], 50.0)                        # upwind flux divergence
 
 
 def main():
@@ -35,6 +67,7 @@ def main():
     K.vertical_velocity(U, V, topg, f[0], compute_levels(nz, 4.0), define_vertical_weight(nz, 4.0), 50.0)  # vert_flow
     K.vertical_velocity(U, V, topg, f[0], compute_levels(nz, 4.0), define_vertical_weight(nz, 4.0), 50.0,
                         method="incompressibility")
+    assimilation(N, f, U[-1].contiguous(), V[-1].contiguous())
     B, H, W = 2, 1000, 1000                                       # 2 x 64 MB activations (> L2)
     x = torch.randn(B, H, 4, W, 8, device="cuda").to(torch.bfloat16)
     y = torch.empty_like(x)

@@ -315,6 +315,22 @@ IGM_API int igm_assim_control(int dtype, int mode, size_t n, double scale, int r
                       void* thk, const void* grad_direct, const float* grad_emulator, const void* icemaskobs,
                       float* variable, float* grad, float* m, float* v, void* stream);
 
+/* compute_rms_std_optimization (data_assimilation/utils.py:10-66): out
+ * (device double[9]) = rmsthk, stdthk, rmsvel, stdvel, rmsdiv, stddiv,
+ * rmsusurf, stdusurf, vol -- the mean and population standard deviation of
+ * thk - thkobs at the thickness observations, of |velsurf| - |velsurfobs|
+ * inside icemaskobs > 0.5 where the observed speed is defined, of divfluxobs -
+ * divflux and usurf - usurfobs inside the mask, and sum(thk) dx^2 / 1e9.  An
+ * observation field passed as NULL gives 0 for its pair (the reference's
+ * "no such observation"); an empty selection gives NaN (numpy's mean of an
+ * empty array), except thk, which the reference records as 0.
+ * partials: device double[n_parts * 13] scratch. */
+IGM_API int igm_assim_stats(int dtype, int ny, int nx, double dx, const void* thk, const void* thkobs,
+                            const void* uvelsurf, const void* vvelsurf, const void* uvelsurfobs,
+                            const void* vvelsurfobs, const void* icemaskobs, const void* divflux,
+                            const void* divfluxobs, const void* usurf, const void* usurfobs, double* partials,
+                            int n_parts, double* out, void* stream);
+
 /* compute_flow_direction_for_anisotropic_smoothing (data_assimilation/utils.py:
  * 86-110): cell averages of the surface velocity (NaN as 0), a Gaussian of
  * sigma 3 cells (radius 12, zero outside; y then x, as scipy.ndimage), then
@@ -462,8 +478,10 @@ IGM_API int igm_cnn_head_wgrad_finish(const float* partials, int n_parts, int no
  * [batch][h][4][w][8], as the second layer's dgrad of igm_conv3x3 leaves it),
  * and the first layer's FP32 kernel w0 [3][3][cin][32] (Keras layout),
  *   out[b][c][y][x] = scales[c] sum_{kh,kw,co} dpre0[b][y-kh+1][x-kw+1][co] w0[kh][kw][c][co]
- * (zero "same" padding); scales: host double[cin], the fixed input scales. */
-IGM_API int igm_cnn_input_gradient(int batch, int h, int w, int cin, const void* dpre0, const float* w0,
+ * (zero "same" padding) for the first n_grad (1..cin) fields, out
+ * [batch][n_grad][h][w]; scales: host double[n_grad], the fixed input scales.
+ * (Data assimilation with control thk needs the first field only.) */
+IGM_API int igm_cnn_input_gradient(int batch, int h, int w, int cin, int n_grad, const void* dpre0, const float* w0,
                                    const double* scales, float* out, void* stream);
 
 /* out[i] (+)= sum_p partials[p * stride + i], i < len, fixed summation order. */
@@ -483,7 +501,10 @@ IGM_API int igm_cnn_wgrad_finish_split(const float* partials, int n_parts, int c
  * for each variable v (elements [var_offsets[v], var_offsets[v+1]) of the
  * vectors): g = g * c / max(|g|, c) when clipnorm c > 0, then the Adam update
  * at step `iteration` (1-based).  var_offsets: host size_t[n_vars + 1];
- * norms: device double[n_vars] scratch. */
+ * norms: device double[igm_adam_norms_len(n_vars, var_offsets)] scratch (the
+ * variables' norms in the first n_vars entries, then per-chunk partial sums of
+ * the squares: the norms are reduced deterministically across the GPU). */
+IGM_API size_t igm_adam_norms_len(int n_vars, const size_t* var_offsets);
 IGM_API int igm_adam_clipnorm(int n_vars, const size_t* var_offsets, float* params, const float* grads, float* m,
                               float* v, double* norms, double lr, double beta_1, double beta_2, double epsilon,
                               double clipnorm, int64_t iteration, void* stream);

@@ -880,17 +880,30 @@ def da_optimize_update(thk, usurf, arrhenius, slidingco, dx, weights, biases, Nz
     return thk_new, {k: v.detach() for k, v in cost.items()}, aux
 
 
-def da_rms_std(thk, thkobs, uvelsurf, vvelsurf, uobs, vobs, icemaskobs, dx):
-    """compute_rms_std_optimization (utils.py:10-66) without divfluxobs /
-    usurfobs: mean and standard deviation of thk - thkobs at the thickness
-    observations and of the speed misfit inside the observed mask, the
-    volume in km^3."""
-    a = ~torch.isnan(thkobs)
-    d = (thk[a] - thkobs[a]).double()
-    rt, st = (float(d.mean()), float(d.std(unbiased=False))) if a.any() else (0.0, 0.0)
-    vs = getmag(uvelsurf, vvelsurf)
-    vo = getmag(uobs, vobs)
-    m = (icemaskobs > 0.5) & ~torch.isnan(vo)
-    e = (vs[m] - vo[m]).double()
-    return {"rmsthk": rt, "stdthk": st, "rmsvel": float(e.mean()), "stdvel": float(e.std(unbiased=False)),
-            "vol": float(thk.double().sum() * dx * dx / 1e9)}
+def da_rms_std(thk, thkobs, uvelsurf, vvelsurf, uobs, vobs, icemaskobs, dx, divflux=None, divfluxobs=None,
+               usurf=None, usurfobs=None):
+    """compute_rms_std_optimization (utils.py:10-66): mean and population
+    standard deviation of thk - thkobs at the thickness observations (0 when
+    there are none), of the speed misfit inside the observed mask where the
+    observed speed is defined, of divfluxobs - divflux and usurf - usurfobs
+    inside the mask (0 when the observation is absent), the volume in km^3."""
+    def ms(d):
+        d = d.double()
+        return (float(d.mean()), float(d.std(unbiased=False))) if d.numel() else (float("nan"), float("nan"))
+    I = icemaskobs > 0.5
+    out = {}
+    if thkobs is not None:
+        a = ~torch.isnan(thkobs)
+        out["rmsthk"], out["stdthk"] = ms(thk[a] - thkobs[a]) if a.any() else (0.0, 0.0)
+    else:
+        out["rmsthk"], out["stdthk"] = 0.0, 0.0
+    if uobs is not None:
+        vs, vo = getmag(uvelsurf, vvelsurf), getmag(uobs, vobs)
+        m = I & ~torch.isnan(vo)
+        out["rmsvel"], out["stdvel"] = ms(vs[m] - vo[m])
+    else:
+        out["rmsvel"], out["stdvel"] = 0.0, 0.0
+    out["rmsdiv"], out["stddiv"] = ms(divfluxobs[I] - divflux[I]) if divfluxobs is not None else (0.0, 0.0)
+    out["rmsusurf"], out["stdusurf"] = ms(usurf[I] - usurfobs[I]) if usurfobs is not None else (0.0, 0.0)
+    out["vol"] = float(thk.double().sum() * dx * dx / 1e9)
+    return out

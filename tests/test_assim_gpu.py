@@ -69,3 +69,36 @@ def test_divflux_upwind_bit_exact(dtype, shape):
     ref = O.divflux_upwind(torch.as_tensor(u), torch.as_tensor(v), torch.as_tensor(h), 50.0)
     out = K.divflux_upwind(dev(u), dev(v), dev(h), 50.0)
     np.testing.assert_array_equal(out.cpu().numpy(), ref.numpy())
+
+
+STAT_KEYS = ["rmsthk", "stdthk", "rmsvel", "stdvel", "rmsdiv", "stddiv", "rmsusurf", "stdusurf", "vol"]
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("present", ["all", "none", "empty_thk"])
+def test_stats_match_oracle(dtype, present):
+    rng = np.random.default_rng(7)
+    ny, nx = 123, 301
+    npd = np.float32 if dtype == torch.float32 else np.float64
+    r = lambda *a: rng.normal(*a, (ny, nx)).astype(npd)
+    thk = np.maximum(0, r(100, 60))
+    f = dict(thk=thk, uvs=r(20, 10), vvs=r(0, 10), uobs=r(20, 10), vobs=r(0, 10), div=r(0, 1), divobs=r(0, 1),
+             us=r(2000, 100), usobs=r(2000, 100), thkobs=np.where(rng.random((ny, nx)) < 0.05, thk + r(0, 5), np.nan),
+             im=(rng.random((ny, nx)) < 0.7).astype(npd))
+    f["uobs"][rng.random((ny, nx)) < 0.1] = np.nan
+    f["vobs"][rng.random((ny, nx)) < 0.1] = np.nan
+    if present == "empty_thk":
+        f["thkobs"][:] = np.nan
+    t = {k: torch.as_tensor(v) for k, v in f.items()}
+    d = {k: dev(v) for k, v in f.items()}
+    if present == "none":
+        ours = K.assim_stats(d["thk"], 50.0, d["im"]).cpu().numpy()
+        ref = O.da_rms_std(t["thk"], None, None, None, None, None, t["im"], 50.0)
+    else:
+        ours = K.assim_stats(d["thk"], 50.0, d["im"], thkobs=d["thkobs"], uvs=d["uvs"], vvs=d["vvs"],
+                             uobs=d["uobs"], vobs=d["vobs"], divflux=d["div"], divfluxobs=d["divobs"], usurf=d["us"],
+                             usurfobs=d["usobs"]).cpu().numpy()
+        ref = O.da_rms_std(t["thk"], t["thkobs"], t["uvs"], t["vvs"], t["uobs"], t["vobs"], t["im"], 50.0,
+                           divflux=t["div"], divfluxobs=t["divobs"], usurf=t["us"], usurfobs=t["usobs"])
+    tol = 1e-5 if dtype == torch.float32 else 1e-9
+    np.testing.assert_allclose(ours, [ref[k] for k in STAT_KEYS], rtol=tol, atol=tol)

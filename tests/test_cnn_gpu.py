@@ -134,7 +134,14 @@ def test_input_field_gradient_matches_oracle():
     G = torch.zeros((1, 5, ny, nx), dtype=torch.float32, device="cuda")
     net.backward(buf, 1, ny, nx, torch.as_tensor(RU).cuda(), torch.as_tensor(RV).cuda(), field_grad=G)
     net.check_errors()
+    # the data-assimilation path: the thk field only, no parameter gradients -- the same data chain
+    G1 = torch.zeros((1, 1, ny, nx), dtype=torch.float32, device="cuda")
+    grads = net.grads.clone()
+    net.backward(buf, 1, ny, nx, torch.as_tensor(RU).cuda(), torch.as_tensor(RV).cuda(), field_grad=G1,
+                 param_grads=False)
+    assert torch.equal(net.grads, grads)
     G = G.cpu().numpy()[0]
+    np.testing.assert_array_equal(G1.cpu().numpy()[0, 0], G[0])
     for c in range(4):
         e = rel_l2(G[c], go[c].numpy())
         assert e < 5e-2, (c, e)
