@@ -553,9 +553,9 @@ def assimilation_bench(args, peaks, K_it=20, warm=3, cpu_crop=200):
     from igm_b200.processes import data_assimilation as DA
     from igm_b200.processes import iceflow as P
     from igm_b200.state import State
-    from igm_b200.synthetic import valley_glacier
+    from igm_b200.synthetic import tongue_glacier
     N, nz = args.size, args.nz
-    g = valley_glacier(N, N, 50.0, seed=0, varying_coeffs=True)
+    g = tongue_glacier(N, N, 50.0, seed=0)
     cfg = default_cfg({"iceflow": {"numerics": {"Nz": nz},
                                    "emulator": {"pretrained": False, "input_scales": SCALES, "seed": 0,
                                                 "output_scale": 50.0,
@@ -576,7 +576,6 @@ def assimilation_bench(args, peaks, K_it=20, warm=3, cpu_crop=200):
     tob = nan.clone()
     tob[:, ::50] = st.thk[:, ::50]
     st.thkobs = tob
-    truth = st.thk.clone()
     DA.optimize_initialize(cfg, st)
     a = st._igm_assim
     from igm_b200 import emulator as E
@@ -620,10 +619,12 @@ def assimilation_bench(args, peaks, K_it=20, warm=3, cpu_crop=200):
     per_node = 14 * 4
     peak = peaks.get("hbm_gbs", 6650.0)
     gbs = per_node * N * N / t / 1e9
-    out = {"workload": f"thickness inversion {N}x{N}xNz{nz}, 16-layer emulator, default data_assimilation "
-                       "configuration (anisotropic bed regularisation, retraining every 10 iterations)",
+    out = {"workload": f"thickness inversion {N}x{N}xNz{nz} (synthetic glacier tongue, dx 50 m; observed surface "
+                       "velocities the emulator's own at the true thickness, 10% missing; thickness profiles on every "
+                       "50th column), 16-layer emulator, default data_assimilation configuration (anisotropic bed "
+                       "regularisation, retraining every 10 iterations), from zero thickness",
            "ms_per_iteration": round(ms_it, 3), "iterations_per_s": round(1e3 / ms_it, 1),
-           "iterations_timed": K_it, "cost_first_last": [float(hist[0]), float(hist[-1])],
+           "iterations_timed": K_it, "costs_finite": bool(np.all(np.isfinite(hist))),
            "cost_kernel": {"kernel": "assim_cost_grad_kernel<float>", "avg_launch_us": round(t * 1e6, 2),
                            "algorithmic_bytes_per_node": per_node, "achieved_GBs": round(gbs, 1),
                            "frac": round(gbs / peak, 4), "peak_GBs": peak}}
@@ -640,10 +641,10 @@ def assimilation_cpu(args, crop):
     and scaled to size^2 by the node count (the work is linear in nodes)."""
     import torch
     from oracle import iceflow_oracle as O
-    from igm_b200.synthetic import valley_glacier
+    from igm_b200.synthetic import tongue_glacier
     torch.set_num_threads(os.cpu_count() or 1)
     nz = args.nz
-    g = valley_glacier(crop, crop, 50.0, seed=0, varying_coeffs=True)
+    g = tongue_glacier(crop, crop, 50.0, seed=0)
     f = {k: torch.as_tensor(g[k]) for k in ["thk", "usurf", "arrhenius", "slidingco"]}
     rng = np.random.default_rng(0)
     ws, bs, c = [], [], 5

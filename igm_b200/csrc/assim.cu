@@ -236,47 +236,69 @@ __global__ void assim_sum_kernel(const double* partials, int n_parts, AssimScale
 }
 
 // ---- flow direction (utils.py:86-110) --------------------------------------
-// cell averages of the surface velocity (NaN as 0)
-template <typename T>
-__global__ void flow_avg_kernel(int ny, int nx, const T* u, const T* v, T* fx, T* fy) {
-  const int cy = ny - 1, cx = nx - 1;
-  const size_t n = (size_t)cy * cx;
-  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
-    const int j = (int)(o / cx), i = (int)(o - (size_t)j * cx);
-    auto z = [](T x) { return isnan(x) ? T(0) : x; };
-    const size_t a = (size_t)j * nx + i;
-    fx[o] = (((z(u[a + nx + 1]) + z(u[a + 1])) + z(u[a + nx])) + z(u[a])) / T(4);
-    fy[o] = (((z(v[a + nx + 1]) + z(v[a + 1])) + z(v[a + nx])) + z(v[a])) / T(4);
-  }
-}
-
-// one pass of the separable Gaussian (zero outside), along y (axis 0) or x (axis 1),
-// accumulated in double and stored in T as each pass of scipy's gaussian_filter
+// the separable Gaussian of sigma 3 cells (scipy's gaussian_filter, truncate 4)
 constexpr int kGaussR = 12;  // int(4 sigma + 0.5), sigma = 3
 struct GaussW { double w[2 * kGaussR + 1]; };
 
-template <typename T>
-__global__ void gauss_pass_kernel(int ny, int nx, int axis, GaussW g, const T* in, T* out) {
-  const size_t n = (size_t)ny * nx;
-  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
-    const int j = (int)(o / nx), i = (int)(o - (size_t)j * nx);
-    double s = 0.0;
-    for (int k = -kGaussR; k <= kGaussR; ++k) {
-      const int jj = axis == 0 ? j + k : j, ii = axis == 0 ? i : i + k;
-      if (jj < 0 || jj >= ny || ii < 0 || ii >= nx) continue;
-      s += g.w[k + kGaussR] * (double)in[(size_t)jj * nx + ii];
+// The whole flow direction in one kernel: a CTA produces a TY x TX tile of
+// cells.  Per component, the cell averages of the tile and a 12-cell halo
+// (zero outside the domain) go to shared memory, then the y pass over the
+// halo columns and the x pass, each accumulated in double and stored in T as
+// scipy's gaussian_filter does between its passes; the x component waits in
+// registers for the y component, then both are normalised and stored.
+template <typename T, int TY, int TX>
+__global__ void __launch_bounds__(256) flow_direction_kernel(int ny, int nx, GaussW g, const T* u, const T* v, T* fx,
+                                                             T* fy) {
+  constexpr int HY = TY + 2 * kGaussR, HX = TX + 2 * kGaussR;
+  constexpr int PER = TY * TX / 256;
+  // the staged values are T-rounded, held in double so the taps need no conversion
+  __shared__ double A[HY][HX];
+  __shared__ double Bs[TY][HX];
+  const int cy = ny - 1, cx = nx - 1;
+  const int y0 = blockIdx.y * TY, x0 = blockIdx.x * TX;
+  T res[2][PER];
+#pragma unroll
+  for (int comp = 0; comp < 2; ++comp) {
+    const T* f = comp == 0 ? u : v;
+    auto z = [](T x) { return isnan(x) ? T(0) : x; };
+    for (int i = threadIdx.x; i < HY * HX; i += 256) {
+      const int hy = i / HX, hx = i - hy * HX;
+      const int j = y0 - kGaussR + hy, k = x0 - kGaussR + hx;
+      T val = T(0);
+      if (j >= 0 && j < cy && k >= 0 && k < cx) {
+        const size_t a = (size_t)j * nx + k;
+        val = (((z(f[a + nx + 1]) + z(f[a + 1])) + z(f[a + nx])) + z(f[a])) / T(4);
+      }
+      A[hy][hx] = (double)val;
     }
-    out[o] = (T)s;
+    __syncthreads();
+    for (int i = threadIdx.x; i < TY * HX; i += 256) {
+      const int r = i / HX, hx = i - r * HX;
+      double sacc = 0.0;
+#pragma unroll
+      for (int k = 0; k <= 2 * kGaussR; ++k) sacc += g.w[k] * A[r + k][hx];
+      Bs[r][hx] = (double)(T)sacc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int idx = threadIdx.x + 256 * q, r = idx / TX, c = idx - r * TX;
+      double sacc = 0.0;
+#pragma unroll
+      for (int k = 0; k <= 2 * kGaussR; ++k) sacc += g.w[k] * Bs[r][c + k];
+      res[comp][q] = (T)sacc;
+    }
+    __syncthreads();
   }
-}
-
-// normalisation, the y component with the already normalised x, as the reference
-template <typename T>
-__global__ void flow_norm_kernel(size_t n, T* fx, T* fy) {
-  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
-    T x = fx[o], y = fy[o];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int idx = threadIdx.x + 256 * q, r = idx / TX, c = idx - r * TX;
+    const int j = y0 + r, k = x0 + c;
+    if (j >= cy || k >= cx) continue;
+    T x = res[0][q], y = res[1][q];
     x = x / sqrt(x * x + y * y);
     y = y / sqrt(x * x + y * y);
+    const size_t o = (size_t)j * cx + k;
     fx[o] = isnan(x) ? T(0) : x;
     fy[o] = isnan(y) ? T(0) : y;
   }
@@ -326,26 +348,16 @@ static int cost_grad_t(int ny, int nx, double dx, const void* thk, const void* u
 
 template <typename T>
 static int flow_t(int ny, int nx, const void* u, const void* v, void* fx, void* fy, void* scratch, cudaStream_t st) {
+  (void)scratch;
   const int cy = ny - 1, cx = nx - 1;
-  const size_t n = (size_t)cy * cx;
-  T* X = (T*)fx;
-  T* Y = (T*)fy;
-  T* S = (T*)scratch;
-  flow_avg_kernel<T><<<grid_n(n), 256, 0, st>>>(ny, nx, (const T*)u, (const T*)v, X, Y);
-  int rc = launch_status("flow_avg_kernel");
-  if (rc) return rc;
   GaussW g{};
   double sum = 0.0;
   for (int k = -kGaussR; k <= kGaussR; ++k) sum += (g.w[k + kGaussR] = exp(-0.5 * k * k / 9.0));
   for (int k = 0; k < 2 * kGaussR + 1; ++k) g.w[k] /= sum;
-  for (T* f : {X, Y}) {
-    gauss_pass_kernel<T><<<grid_n(n), 256, 0, st>>>(cy, cx, 0, g, f, S);
-    if ((rc = launch_status("gauss_pass_kernel"))) return rc;
-    gauss_pass_kernel<T><<<grid_n(n), 256, 0, st>>>(cy, cx, 1, g, S, f);
-    if ((rc = launch_status("gauss_pass_kernel"))) return rc;
-  }
-  flow_norm_kernel<T><<<grid_n(n), 256, 0, st>>>(n, X, Y);
-  return launch_status("flow_norm_kernel");
+  constexpr int TY = sizeof(T) == 4 ? 32 : 16, TX = 32;
+  const dim3 grid((cx + TX - 1) / TX, (cy + TY - 1) / TY);
+  flow_direction_kernel<T, TY, TX><<<grid, 256, 0, st>>>(ny, nx, g, (const T*)u, (const T*)v, (T*)fx, (T*)fy);
+  return launch_status("flow_direction_kernel");
 }
 
 // Control update of optimize_update (optimize/update.py:23-27, 38-42,
@@ -446,16 +458,17 @@ __global__ void __launch_bounds__(256) assim_stats_kernel(const StatArgs<T> a) {
 // mask gives NaN as numpy's mean of an empty selection)
 __global__ void assim_stats_finish_kernel(const double* partials, int n_parts, double dx2, int have_thk,
                                           int have_vel, int have_div, int have_us, double* out) {
-  const int lane = threadIdx.x;
-  double tot[kNStat];
-#pragma unroll
-  for (int k = 0; k < kNStat; ++k) {
+  // warp k adds up statistic k (lane-strided, fixed xor tree); then thread 0 forms the record
+  __shared__ double tot[kNStat];
+  const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (k < kNStat) {
     double v = 0.0;
     for (int b = lane; b < n_parts; b += 32) v += partials[(size_t)b * kNStat + k];
     for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
-    tot[k] = v;
+    if (lane == 0) tot[k] = v;
   }
-  if (lane != 0) return;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
   const int have[4] = {have_thk, have_vel, have_div, have_us};
   for (int t = 0; t < 4; ++t) {
     const double c = tot[3 * t], s1 = tot[3 * t + 1], s2 = tot[3 * t + 2];
@@ -509,7 +522,7 @@ extern "C" int igm_assim_cost_grad(int dtype, int ny, int nx, double dx, const v
 extern "C" int igm_assim_flow_direction(int dtype, int ny, int nx, const void* uvelsurf, const void* vvelsurf,
                                         void* flowdirx, void* flowdiry, void* scratch, void* stream) {
   IGM_CHECK_ARG(ny >= 2 && nx >= 2, IGM_ERR_BAD_SHAPE, "igm_assim_flow_direction: bad shape %dx%d", ny, nx);
-  IGM_CHECK_ARG(uvelsurf && vvelsurf && flowdirx && flowdiry && scratch, IGM_ERR_BAD_ARGUMENT,
+  IGM_CHECK_ARG(uvelsurf && vvelsurf && flowdirx && flowdiry, IGM_ERR_BAD_ARGUMENT,
                 "igm_assim_flow_direction: NULL argument");
   cudaStream_t st = as_stream(stream);
   if (dtype == IGM_F32) return flow_t<float>(ny, nx, uvelsurf, vvelsurf, flowdirx, flowdiry, scratch, st);
@@ -577,7 +590,7 @@ extern "C" int igm_assim_stats(int dtype, int ny, int nx, double dx, const void*
   }
   int rc = launch_status("assim_stats_kernel");
   if (rc) return rc;
-  assim_stats_finish_kernel<<<1, 32, 0, st>>>(partials, grid, dx * dx, thkobs != nullptr, uvelsurfobs != nullptr,
+  assim_stats_finish_kernel<<<1, 32 * kNStat, 0, st>>>(partials, grid, dx * dx, thkobs != nullptr, uvelsurfobs != nullptr,
                                               divfluxobs != nullptr, usurfobs != nullptr, out);
   return launch_status("assim_stats_finish_kernel");
 }

@@ -925,53 +925,66 @@ static int grid_for(size_t n, int per = 256) {
 //   dField_c[y][x] = scale_c sum_{kh,kw,co} dPre0[y-kh+1][x-kw+1][co] W0[kh][kw][c][co]
 // with the FP32 weights (the transposed "same" convolution; the BF16 split of
 // the inputs is a representation of the same x, so its gradient is x's).
-// One pixel per thread, the weights in shared memory.
+// A CTA stages the 10 x 34 halo tile of dPre0 in shared memory and produces
+// an 8 x 32 tile of pixels, one per thread; the weights in shared memory too.
 // ---------------------------------------------------------------------------
 struct InputGradScales { float s[8]; };
+
+constexpr int kIgTY = 8, kIgTX = 32;  // output tile of one CTA (256 threads, one pixel each)
 
 template <int NG>
 __global__ void __launch_bounds__(256) input_grad_kernel(int B, int H, int W, int cin, const __nv_bfloat16* dpre,
                                                          const float* w0, InputGradScales sc, float* out) {
-  __shared__ float sw[9 * NG * kF];  // [tap][c][co] of the fields computed
+  __shared__ __align__(16) float sw[9 * NG * kF];                // [tap][c][co] of the fields computed
+  __shared__ uint4 tile[kIgTY + 2][4][kIgTX + 2];                // dPre0 rows y0-1 .. y0+8, 8-channel chunks
   for (int i = threadIdx.x; i < 9 * NG * kF; i += blockDim.x) {
     const int tap = i / (NG * kF), r = i - tap * NG * kF;
     sw[i] = w0[(size_t)tap * cin * kF + r];
   }
-  __syncthreads();
-  const size_t plane = (size_t)H * W;
-  const size_t total = plane * B;
+  const int b = blockIdx.z, y0 = blockIdx.y * kIgTY, x0 = blockIdx.x * kIgTX;
   const uint4* D = reinterpret_cast<const uint4*>(dpre);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const size_t b = i / plane, rem = i - b * plane;
-    const int y = (int)(rem / W), x = (int)(rem - (size_t)(rem / W) * W);
-    float acc[NG];
+  for (int i = threadIdx.x; i < (kIgTY + 2) * 4 * (kIgTX + 2); i += blockDim.x) {
+    const int hy = i / (4 * (kIgTX + 2)), rem = i - hy * 4 * (kIgTX + 2);
+    const int ch = rem / (kIgTX + 2), hx = rem - ch * (kIgTX + 2);
+    const int yy = y0 - 1 + hy, xx = x0 - 1 + hx;
+    uint4 val = make_uint4(0u, 0u, 0u, 0u);  // bf16 zeros: the "same" padding
+    if (yy >= 0 && yy < H && xx >= 0 && xx < W) val = D[(((size_t)b * H + yy) * 4 + ch) * W + xx];
+    tile[hy][ch][hx] = val;
+  }
+  __syncthreads();
+  const int r = threadIdx.x / kIgTX, c = threadIdx.x - r * kIgTX;
+  const int y = y0 + r, x = x0 + c;
+  float acc[NG];
 #pragma unroll
-    for (int c = 0; c < NG; ++c) acc[c] = 0.f;
+  for (int k = 0; k < NG; ++k) acc[k] = 0.f;
 #pragma unroll
-    for (int kh = 0; kh < 3; ++kh) {
-      const int yy = y - kh + 1;
-      if (yy < 0 || yy >= H) continue;
+  for (int kh = 0; kh < 3; ++kh) {
 #pragma unroll
-      for (int kw = 0; kw < 3; ++kw) {
-        const int xx = x - kw + 1;
-        if (xx < 0 || xx >= W) continue;
-        const float* wt = sw + (kh * 3 + kw) * NG * kF;
+    for (int kw = 0; kw < 3; ++kw) {
+      // dPre0[y - kh + 1][x - kw + 1] sits at tile[r + 2 - kh][.][c + 2 - kw]
+      const float* wt = sw + (kh * 3 + kw) * NG * kF;
 #pragma unroll
-        for (int ch = 0; ch < 4; ++ch) {
-          const uint4 u = D[((b * H + yy) * 4 + ch) * W + xx];
-          const uint32_t wv[4] = {u.x, u.y, u.z, u.w};
+      for (int ch = 0; ch < 4; ++ch) {
+        const uint4 u = tile[r + 2 - kh][ch][c + 2 - kw];
+        const uint32_t wv[4] = {u.x, u.y, u.z, u.w};
+        float d[8];
 #pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const int co = ch * 8 + e;
-            const float d = (e & 1) ? bf_hi(wv[e >> 1]) : bf_lo(wv[e >> 1]);
+        for (int e = 0; e < 8; ++e) d[e] = (e & 1) ? bf_hi(wv[e >> 1]) : bf_lo(wv[e >> 1]);
 #pragma unroll
-            for (int c = 0; c < NG; ++c) acc[c] = fmaf(d, wt[c * kF + co], acc[c]);
-          }
+        for (int k = 0; k < NG; ++k) {
+          const float4 wa = *reinterpret_cast<const float4*>(wt + k * kF + ch * 8);
+          const float4 wb = *reinterpret_cast<const float4*>(wt + k * kF + ch * 8 + 4);
+          const float wk[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+#pragma unroll
+          for (int e = 0; e < 8; ++e) acc[k] = fmaf(d[e], wk[e], acc[k]);
         }
       }
     }
+  }
+  if (y < H && x < W) {
+    const size_t plane = (size_t)H * W, rem = (size_t)y * W + x;
 #pragma unroll
-    for (int c = 0; c < NG; ++c) out[(b * NG + c) * plane + rem] = acc[c] * sc.s[c];
+    for (int k = 0; k < NG; ++k) out[((size_t)b * NG + k) * plane + rem] = acc[k] * sc.s[k];
   }
 }
 
@@ -1248,7 +1261,8 @@ extern "C" int igm_cnn_input_gradient(int batch, int h, int w, int cin, int n_gr
   IGM_CHECK_ARG(dpre0 && w0 && scales && out, IGM_ERR_BAD_ARGUMENT, "igm_cnn_input_gradient: NULL argument");
   InputGradScales sc{};
   for (int c = 0; c < n_grad; ++c) sc.s[c] = (float)scales[c];
-  const int grid = grid_for((size_t)batch * h * w);
+  IGM_CHECK_ARG(batch <= 65535, IGM_ERR_BAD_SHAPE, "igm_cnn_input_gradient: batch above 65535");
+  const dim3 grid((w + kIgTX - 1) / kIgTX, (h + kIgTY - 1) / kIgTY, batch);
   cudaStream_t st = as_stream(stream);
   const __nv_bfloat16* d = (const __nv_bfloat16*)dpre0;
   switch (n_grad) {

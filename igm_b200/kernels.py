@@ -190,9 +190,9 @@ def assim_flow_direction(uvs, vvs):
     """Flow directions [ny-1, nx-1] of the anisotropic regularisation."""
     ny, nx = uvs.shape
     fx = torch.empty((ny - 1, nx - 1), dtype=uvs.dtype, device=uvs.device)
-    fy, scratch = torch.empty_like(fx), torch.empty_like(fx)
+    fy = torch.empty_like(fx)
     rc = L.lib().igm_assim_flow_direction(L.dtype_code(uvs.dtype), ny, nx, L.ptr(uvs), L.ptr(vvs), L.ptr(fx),
-                                          L.ptr(fy), L.ptr(scratch), L.stream_ptr())
+                                          L.ptr(fy), None, L.stream_ptr())
     L.check(rc, "igm_assim_flow_direction")
     return fx, fy
 

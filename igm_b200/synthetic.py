@@ -67,3 +67,25 @@ def ridge_glacier(n=4096, dx=25.0, seed=0, n_ridges=12):
     thk = np.zeros((n, n))
     f = lambda a: np.ascontiguousarray(a, dtype=np.float32)
     return dict(topg=f(topg), thk=f(thk), usurf=f(topg), arrhenius=f(A), slidingco=f(c), dx=float(dx))
+
+
+def tongue_glacier(ny=40, nx=70, dx=100.0, seed=3):
+    """Glacier tongue for thickness inversions: a 0.05-slope plane bed with a
+    transverse undulation (amplitude 20 m, wavelength 1.41 Ly) and a
+    parabolic-in-y, linearly thinning-in-x tongue centred on the domain, half
+    width 0.375 Ly, vanishing at 1.07 Lx, maximum thickness 180 sqrt(Ly / 4 km)
+    m (Lx = nx dx, Ly = ny dx).  A, c log-uniform per cell in [20, 150] and
+    [0.01, 0.1], smoothed with a 5-cell box filter.  Returns float32 arrays
+    plus x, y coordinates."""
+    x, y = np.arange(nx) * dx, np.arange(ny) * dx
+    X, Y = np.meshgrid(x, y)
+    Lx, Ly = nx * dx, ny * dx
+    topg = 2000.0 - 0.05 * X + 20.0 * np.sin(Y * (4000.0 / 900.0) / Ly)
+    hmax = 180.0 * np.sqrt(Ly / 4000.0)
+    thk = np.maximum(0.0, hmax * (1 - ((Y - 0.5 * Ly) / (0.375 * Ly)) ** 2) * (1 - X / (Lx * 7500.0 / 7000.0)))
+    rng = np.random.default_rng(seed)
+    A = box_filter(np.exp(rng.uniform(np.log(20.0), np.log(150.0), (ny, nx))), 5)
+    c = box_filter(np.exp(rng.uniform(np.log(0.01), np.log(0.1), (ny, nx))), 5)
+    f = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+    return dict(topg=f(topg), thk=f(thk), usurf=f(topg + thk), arrhenius=f(A), slidingco=f(c), dx=float(dx), x=f(x),
+                y=f(y))

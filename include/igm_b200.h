@@ -334,8 +334,8 @@ IGM_API int igm_assim_stats(int dtype, int ny, int nx, double dx, const void* th
 /* compute_flow_direction_for_anisotropic_smoothing (data_assimilation/utils.py:
  * 86-110): cell averages of the surface velocity (NaN as 0), a Gaussian of
  * sigma 3 cells (radius 12, zero outside; y then x, as scipy.ndimage), then
- * x /= |(x, y)|, y /= |(x_normalised, y)|, NaN as 0.  Outputs and scratch
- * [ny-1][nx-1]. */
+ * x /= |(x, y)|, y /= |(x_normalised, y)|, NaN as 0, in one tiled kernel.
+ * Outputs [ny-1][nx-1]; scratch is not used (kept for callers that pass it). */
 IGM_API int igm_assim_flow_direction(int dtype, int ny, int nx, const void* uvelsurf, const void* vvelsurf,
                              void* flowdirx, void* flowdiry, void* scratch, void* stream);
 

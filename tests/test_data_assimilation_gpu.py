@@ -25,6 +25,7 @@ from igm_b200.config import default_cfg
 from igm_b200.processes import data_assimilation as DA
 from igm_b200.processes import iceflow as P
 from igm_b200.state import State
+from igm_b200.synthetic import tongue_glacier
 from oracle import iceflow_oracle as O
 from tests.gpu_util import rel_l2
 
@@ -38,16 +39,7 @@ NZ = 4
 def twin_glacier(ny=40, nx=70, dx=100.0):
     """A tilted-plane bed with a gentle transverse undulation and a
     parabolic tongue thinning downstream."""
-    x, y = np.arange(nx) * dx, np.arange(ny) * dx
-    X, Y = np.meshgrid(x, y)
-    topg = 2000.0 - 0.05 * X + 20.0 * np.sin(Y / 900.0)
-    thk = np.maximum(0.0, 180.0 * (1 - ((Y - 2000.0) / 1500.0) ** 2) * (1 - X / 7500.0))
-    rng = np.random.default_rng(3)
-    A = O.box_filter(np.exp(rng.uniform(np.log(20.0), np.log(150.0), (ny, nx))), 5)
-    c = O.box_filter(np.exp(rng.uniform(np.log(0.01), np.log(0.1), (ny, nx))), 5)
-    f = lambda a: np.ascontiguousarray(a, dtype=np.float32)
-    return dict(topg=f(topg), thk=f(thk), usurf=f(topg + thk), arrhenius=f(A), slidingco=f(c), dx=dx, x=f(x),
-                y=f(y))
+    return tongue_glacier(ny, nx, dx, seed=3)
 
 
 def make_cfg(nbitmax, aniso=0.2, to_regularize="topg"):
