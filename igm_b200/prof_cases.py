@@ -6,6 +6,11 @@ the vertical velocity at 1500 x 1500 x Nz 10 in FP32; the data-assimilation
 cost/gradient, flow direction and upwind divergence at 1500 x 1500 in FP32;
 the tensor-core convolution (forward, dgrad, wgrad) at batch 2 x 1000 x 1000
 x 32 channels.
+
+``python -m igm_b200.prof_cases assimilation_iteration`` instead sets up the
+data-assimilation loop on the 1000 x 1000 x Nz 10 glacier tongue (default
+configuration, 16-layer emulator), runs 5 iterations, then one more between
+cudaProfilerStart and cudaProfilerStop (for ncu --profile-from-start off).
 """
 
 from __future__ import annotations
@@ -90,5 +95,51 @@ def main():
     print("ok")
 
 
+def assimilation_iteration(N=1000, nz=10, warm=5):
+    """One data-assimilation iteration (optimize_update + the rms/std
+    record) bracketed for the profiler, after ``warm`` iterations."""
+    from .config import default_cfg
+    from .processes import data_assimilation as DA
+    from .processes import iceflow as P
+    from .state import State
+    from .synthetic import tongue_glacier
+    g = tongue_glacier(N, N, 50.0, seed=0)
+    scales = [1 / 300.0, 1 / 3000.0, 1 / 100.0, 10.0, 1 / 50.0]
+    cfg = default_cfg({"iceflow": {"numerics": {"Nz": nz},
+                                   "emulator": {"pretrained": False, "input_scales": scales, "seed": 0,
+                                                "output_scale": 50.0,
+                                                "network": {"weight_initialization": "he_normal"}}},
+                       "data_assimilation": {"output": {"save_iterat_in_ncdf": False}}})
+    st = State()
+    for k in ("thk", "usurf", "topg", "arrhenius", "slidingco"):
+        setattr(st, k, torch.as_tensor(g[k]).cuda())
+    st.dx = 50.0
+    st.icemask = (st.thk > 0).float()
+    st.icemaskobs = st.icemask.clone()
+    P.initialize(cfg, st)
+    obs = assimilation_inputs(N, st.thk, st.uvelsurf.contiguous(), st.vvelsurf.contiguous())
+    st.uvelsurfobs, st.vvelsurfobs, st.thkobs = obs["uobs"], obs["vobs"], obs["thkobs"]
+    DA.optimize_initialize(cfg, st)
+    a = st._igm_assim
+
+    def it(i):
+        DA.optimize_update(cfg, st, {}, i)
+        DA._record_rms(a, st, i)
+
+    for i in range(warm):
+        it(i)
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()
+    it(warm)
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStop()
+    st.iceflow_model.check_errors()
+    print("ok")
+
+
 if __name__ == "__main__":
-    main()
+    import sys
+    if len(sys.argv) > 1 and sys.argv[1] == "assimilation_iteration":
+        assimilation_iteration()
+    else:
+        main()
