@@ -51,6 +51,13 @@ class Adam(C.Structure):
     _fields_ = [("lr", C.c_double), ("beta_1", C.c_double), ("beta_2", C.c_double), ("epsilon", C.c_double)]
 
 
+class DivfluxCostParams(C.Structure):
+    """igm_divflux_cost_params."""
+    _fields_ = [("kind", C.c_int32), ("method", C.c_int32), ("force_zero_sum", C.c_int32), ("reserved", C.c_int32),
+                ("divfluxobs_std", C.c_double), ("regu_divflux", C.c_double), ("slope", C.c_double),
+                ("intercept", C.c_double)]
+
+
 class AssimParams(C.Structure):
     _fields_ = [("velsurfobs_std", C.c_double), ("velsurfobs_thr", C.c_double), ("thkobs_std", C.c_double),
                 ("regu_thk", C.c_double), ("gamma", C.c_double), ("aniso_factor", C.c_double), ("n_vel", C.c_double),
@@ -117,6 +124,9 @@ SIGNATURES = {
     "igm_divflux_upwind": (I, [I, I, I, D, P, P, P, P, P]),
     "igm_assim_control": (I, [I, I, C.c_size_t, D, I, I, P, P, P, P, P, P, P, P, P]),
     "igm_assim_stats": (I, [I, I, I, D] + [P] * 11 + [P, I, P, P]),
+    "igm_divflux": (I, [I, I, I, I, D, P, P, P, P, P]),
+    "igm_assim_divflux_cost_grad": (I, [I, I, I, D, I, P] + [P] * 8 + [P, P, P, P, P, P, I, P, P]),
+    "igm_assim_divflux_partials_len": (C.c_size_t, [I]),
     "igm_adam_clipnorm": (I, [I, P, P, P, P, P, P, D, D, D, D, D, C.c_int64, P]),
     "igm_adam_norms_len": (C.c_size_t, [I, P]),
 }

@@ -488,6 +488,203 @@ __global__ void assim_stats_finish_kernel(const double* partials, int n_parts, d
   out[8] = tot[12] * dx2 / 1e9;
 }
 
+// ---- flux-divergence cost terms --------------------------------------------
+// cost_divfluxobs (cost_terms/cost_divfluxobs.py:9-29): 0.5 mean over the
+// observed nodes of ((obs - D) / std)^2 + regu 0.5 (mean (dD/dx)^2 + mean
+// (dD/dy)^2); cost_divfluxfcz (cost_terms/cost_divfluxfcz.py:10-38): the
+// target intercept + slope usurf, 0.5 mean over icemaskobs > 0.5 of
+// ((target - D) / std)^2; both + 0.5 1000 mean_mask(D / std)^2 with
+// force_zero_sum.  D = compute_divflux(ubar, vbar, thk).  Four launches: the
+// global sums (counts, sum of D in the mask), dC/dD per node, the adjoint of
+// compute_divflux into dC/dthk and dC/dU, dC/dV of every level (velbar =
+// sum_k w_k U_k, zero where the thk mask is off), the cost.
+template <typename T>
+struct DivCostArgs {
+  int ny, nx, nz, kind, method, fzs;
+  T dx, rdx;
+  double sd, regu, slope, intercept;
+  const T *ubar, *vbar, *thk, *D, *obs, *usurf, *im, *mask;
+  T *g_thk, *dU, *dV, *gD;
+  T w[IGM_MAX_NZ];
+  double* partials;  // [n_parts][3] sums, then [n_parts][3] cost sums
+  int n_parts;
+  double* scal;      // count_act, count_mask, sum_mask D
+  double* cost;
+};
+
+template <typename T>
+__device__ __forceinline__ void block_reduce3(double v0, double v1, double v2, double* out) {
+  __shared__ double red[8][3];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double v[3] = {v0, v1, v2};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    for (int s = 16; s > 0; s >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], s);
+    if (lane == 0) red[warp][c] = v[c];
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w][threadIdx.x];
+    out[(size_t)blockIdx.x * 3 + threadIdx.x] = t;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) divcost_sums_kernel(const DivCostArgs<T> a) {
+  const size_t n = (size_t)a.ny * a.nx;
+  double c_act = 0.0, c_m = 0.0, s_m = 0.0;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    const bool in = a.im[o] > T(0.5);
+    if (a.kind == 0) c_act += isnan(a.obs[o]) ? 0.0 : 1.0;
+    if (in) {
+      c_m += 1.0;
+      s_m += (double)a.D[o];
+    }
+  }
+  block_reduce3<T>(c_act, c_m, s_m, a.partials);
+}
+
+// fixed-order sums of n_parts rows of 3 (one warp per column)
+__global__ void divcost_finish3_kernel(const double* partials, int n_parts, double* out) {
+  const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (c >= 3) return;
+  double v = 0.0;
+  for (int b = lane; b < n_parts; b += 32) v += partials[(size_t)b * 3 + c];
+  for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+  if (lane == 0) out[c] = v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) divcost_gradD_kernel(const DivCostArgs<T> a) {
+  const int ny = a.ny, nx = a.nx;
+  const size_t n = (size_t)ny * nx;
+  const double n_act = a.kind == 0 ? a.scal[0] : a.scal[1];
+  const double n_m = a.scal[1];
+  const T kd = (T)(1.0 / (a.sd * a.sd * n_act));
+  const T ksx = (T)(a.regu / ((double)ny * (nx - 1))), ksy = (T)(a.regu / ((double)(ny - 1) * nx));
+  const T kz = a.fzs ? (T)(1000.0 * (a.scal[2] / (a.sd * n_m)) / (a.sd * n_m)) : T(0);
+  const T rdx = a.rdx;
+  double c_r = 0.0, c_x = 0.0, c_y = 0.0;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(o / nx), i = (int)(o - (size_t)j * nx);
+    const T D0 = a.D[o];
+    const bool in = a.im[o] > T(0.5);
+    T g = T(0);
+    if (a.kind == 0) {
+      const T ob = a.obs[o];
+      if (!isnan(ob)) {
+        const T r = ob - D0;
+        c_r += (double)r * (double)r;
+        g -= r * kd;
+      }
+      // smoothness of D: forward differences owned by this node, backward ones from the neighbours
+      if (i + 1 < nx) {
+        const T d = (a.D[o + 1] - D0) * rdx;
+        c_x += (double)d * (double)d;
+        g -= ksx * d * rdx;
+      }
+      if (i >= 1) g += ksx * ((D0 - a.D[o - 1]) * rdx) * rdx;
+      if (j + 1 < ny) {
+        const T d = (a.D[o + nx] - D0) * rdx;
+        c_y += (double)d * (double)d;
+        g -= ksy * d * rdx;
+      }
+      if (j >= 1) g += ksy * ((D0 - a.D[o - nx]) * rdx) * rdx;
+    } else if (in) {
+      const T r = (T)(a.intercept + a.slope * (double)a.usurf[o]) - D0;
+      c_r += (double)r * (double)r;
+      g -= r * kd;
+    }
+    if (in) g += kz;
+    a.gD[o] = g;
+  }
+  block_reduce3<T>(c_r, c_x, c_y, a.partials + (size_t)a.n_parts * 3);
+}
+
+// the adjoint of compute_divflux at node (j, i): the faces i, i+1 (x) and j, j+1 (y)
+template <typename T, int METHOD>
+__global__ void __launch_bounds__(256) divcost_adjoint_kernel(const DivCostArgs<T> a) {
+  const int ny = a.ny, nx = a.nx;
+  const size_t n = (size_t)ny * nx;
+  const T rdx = a.rdx;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(o / nx), i = (int)(o - (size_t)j * nx);
+    auto gd = [&](int jj, int ii) {
+      return (jj < 0 || jj >= ny || ii < 0 || ii >= nx) ? T(0) : a.gD[(size_t)jj * nx + ii];
+    };
+    auto hh = [&](int jj, int ii) {
+      return (jj < 0 || jj >= ny || ii < 0 || ii >= nx) ? T(0) : a.thk[(size_t)jj * nx + ii];
+    };
+    // d C / d Q of the faces: Q(f) enters D(f - 1) with + 1/dx and D(f) with - 1/dx
+    const T gqw = (gd(j, i - 1) - gd(j, i)) * rdx, gqe = (gd(j, i) - gd(j, i + 1)) * rdx;
+    const T gqs = (gd(j - 1, i) - gd(j, i)) * rdx, gqn = (gd(j, i) - gd(j + 1, i)) * rdx;
+    const T cw = i == 0 ? T(1) : T(0.5), ce = i == nx - 1 ? T(1) : T(0.5);
+    const T cs = j == 0 ? T(1) : T(0.5), cn = j == ny - 1 ? T(1) : T(0.5);
+    const T u0 = a.ubar[o], v0 = a.vbar[o], h0 = a.thk[o];
+    T gu, gv, gh;
+    if (METHOD == IGM_DIVFLUX_UPWIND) {
+      auto uu = [&](int ii) { return a.ubar[(size_t)j * nx + ii]; };
+      auto vv = [&](int jj) { return a.vbar[(size_t)jj * nx + i]; };
+      const T uw = i == 0 ? uu(0) : T(0.5) * (uu(i - 1) + u0);
+      const T ue = i == nx - 1 ? uu(nx - 1) : T(0.5) * (u0 + uu(i + 1));
+      const T vs = j == 0 ? vv(0) : T(0.5) * (vv(j - 1) + v0);
+      const T vn = j == ny - 1 ? vv(ny - 1) : T(0.5) * (v0 + vv(j + 1));
+      const T hw = uw > T(0) ? hh(j, i - 1) : h0, he = ue > T(0) ? h0 : hh(j, i + 1);
+      const T hs = vs > T(0) ? hh(j - 1, i) : h0, hn = vn > T(0) ? h0 : hh(j + 1, i);
+      gu = gqw * hw * cw + gqe * he * ce;
+      gv = gqs * hs * cs + gqn * hn * cn;
+      // this node's thickness is the upwind value of face i when uw <= 0, of face i+1 when ue > 0
+      gh = (uw > T(0) ? T(0) : gqw * uw) + (ue > T(0) ? gqe * ue : T(0)) + (vs > T(0) ? T(0) : gqs * vs) +
+           (vn > T(0) ? gqn * vn : T(0));
+    } else {
+      // centered: Q(f) averages q = u h of its two nodes (an edge copy at the border)
+      const T gqx = gqw * cw + gqe * ce, gqy = gqs * cs + gqn * cn;
+      gu = gqx * h0;
+      gv = gqy * h0;
+      gh = gqx * u0 + gqy * v0;
+    }
+    a.g_thk[o] += gh;
+    const bool on = a.mask == nullptr || a.mask[o] > T(0);
+    const size_t plane = n;
+    for (int k = 0; k < a.nz; ++k) {
+      const T du = on ? a.w[k] * gu : T(0), dv = on ? a.w[k] * gv : T(0);
+      const size_t q = (size_t)k * plane + o;
+      if (k == a.nz - 1) {
+        a.dU[q] += du;
+        a.dV[q] += dv;
+      } else {
+        a.dU[q] = du;
+        a.dV[q] = dv;
+      }
+    }
+  }
+}
+
+template <typename T>
+__global__ void divcost_cost_kernel(const DivCostArgs<T> a) {
+  __shared__ double t[3];
+  const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (c < 3) {
+    double v = 0.0;
+    const double* p = a.partials + (size_t)a.n_parts * 3;
+    for (int b = lane; b < a.n_parts; b += 32) v += p[(size_t)b * 3 + c];
+    for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+    if (lane == 0) t[c] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const double n_act = a.kind == 0 ? a.scal[0] : a.scal[1];
+  double cst = 0.5 * t[0] / (a.sd * a.sd * n_act);
+  if (a.kind == 0)
+    cst += a.regu * 0.5 * (t[1] / ((double)a.ny * (a.nx - 1)) + t[2] / ((double)(a.ny - 1) * a.nx));
+  if (a.fzs) {
+    const double m = a.scal[2] / (a.sd * a.scal[1]);
+    cst += 0.5 * 1000.0 * m * m;
+  }
+  *a.cost = cst;
+}
+
 }  // namespace igm
 
 using namespace igm;
@@ -594,3 +791,59 @@ extern "C" int igm_assim_stats(int dtype, int ny, int nx, double dx, const void*
                                               divfluxobs != nullptr, usurfobs != nullptr, out);
   return launch_status("assim_stats_finish_kernel");
 }
+
+extern "C" int igm_assim_divflux_cost_grad(int dtype, int ny, int nx, double dx, int nz, const double* vert_weight,
+                                           const void* ubar, const void* vbar, const void* thk, const void* divflux,
+                                           const void* divfluxobs, const void* usurf, const void* icemaskobs,
+                                           const void* mask_thk, const igm_divflux_cost_params* params,
+                                           void* grad_thk, void* dU, void* dV, void* scratch, double* partials,
+                                           int n_parts, double* cost, void* stream) {
+  IGM_CHECK_ARG(ny >= 2 && nx >= 2 && dx > 0 && nz >= 1 && nz <= IGM_MAX_NZ, IGM_ERR_BAD_SHAPE,
+                "igm_assim_divflux_cost_grad: bad shape");
+  IGM_CHECK_ARG(params && vert_weight && ubar && vbar && thk && divflux && icemaskobs && grad_thk && dU && dV &&
+                    scratch && partials && cost && n_parts >= 1,
+                IGM_ERR_BAD_ARGUMENT, "igm_assim_divflux_cost_grad: NULL argument");
+  IGM_CHECK_ARG((params->kind == 0 && divfluxobs) || (params->kind == 1 && usurf), IGM_ERR_BAD_ARGUMENT,
+                "igm_assim_divflux_cost_grad: kind 0 needs divfluxobs, kind 1 needs usurf");
+  IGM_CHECK_ARG(params->method == IGM_DIVFLUX_UPWIND || params->method == IGM_DIVFLUX_CENTERED,
+                IGM_ERR_BAD_ARGUMENT, "igm_assim_divflux_cost_grad: unknown method");
+  IGM_CHECK_ARG(params->divfluxobs_std > 0, IGM_ERR_BAD_ARGUMENT, "igm_assim_divflux_cost_grad: std <= 0");
+  cudaStream_t st = as_stream(stream);
+  const size_t n = (size_t)ny * nx;
+  int grid = grid_n(n);
+  if (grid > n_parts) grid = n_parts;
+  auto run = [&](auto zero) -> int {
+    using T = decltype(zero);
+    DivCostArgs<T> a{};
+    a.ny = ny; a.nx = nx; a.nz = nz;
+    a.kind = params->kind; a.method = params->method; a.fzs = params->force_zero_sum;
+    a.dx = (T)dx; a.rdx = T(1) / a.dx;
+    a.sd = params->divfluxobs_std; a.regu = params->regu_divflux; a.slope = params->slope;
+    a.intercept = params->intercept;
+    a.ubar = (const T*)ubar; a.vbar = (const T*)vbar; a.thk = (const T*)thk; a.D = (const T*)divflux;
+    a.obs = (const T*)divfluxobs; a.usurf = (const T*)usurf; a.im = (const T*)icemaskobs; a.mask = (const T*)mask_thk;
+    a.g_thk = (T*)grad_thk; a.dU = (T*)dU; a.dV = (T*)dV; a.gD = (T*)scratch;
+    for (int k = 0; k < nz; ++k) a.w[k] = (T)vert_weight[k];
+    a.partials = partials; a.n_parts = grid; a.scal = partials + (size_t)6 * grid; a.cost = cost;
+    divcost_sums_kernel<T><<<grid, 256, 0, st>>>(a);
+    int rc = launch_status("divcost_sums_kernel");
+    if (rc) return rc;
+    divcost_finish3_kernel<<<1, 96, 0, st>>>(partials, grid, a.scal);
+    if ((rc = launch_status("divcost_finish3_kernel"))) return rc;
+    divcost_gradD_kernel<T><<<grid, 256, 0, st>>>(a);
+    if ((rc = launch_status("divcost_gradD_kernel"))) return rc;
+    if (a.method == IGM_DIVFLUX_UPWIND)
+      divcost_adjoint_kernel<T, IGM_DIVFLUX_UPWIND><<<grid_n(n), 256, 0, st>>>(a);
+    else
+      divcost_adjoint_kernel<T, IGM_DIVFLUX_CENTERED><<<grid_n(n), 256, 0, st>>>(a);
+    if ((rc = launch_status("divcost_adjoint_kernel"))) return rc;
+    divcost_cost_kernel<T><<<1, 96, 0, st>>>(a);
+    return launch_status("divcost_cost_kernel");
+  };
+  if (dtype == IGM_F32) return run(0.f);
+  if (dtype == IGM_F64) return run(0.0);
+  set_error("igm_assim_divflux_cost_grad: unknown dtype %d", dtype);
+  return IGM_ERR_BAD_ARGUMENT;
+}
+
+extern "C" size_t igm_assim_divflux_partials_len(int n_parts) { return (size_t)6 * n_parts + 3; }

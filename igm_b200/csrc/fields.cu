@@ -577,26 +577,38 @@ __global__ void __launch_bounds__(kVfWarps * 32) vert_flow_incomp_kernel(const V
   }
 }
 
-// compute_divflux, method upwind (igm/utils/gradient/compute_divflux.py:17-33,
-// 45-46): face velocities with edge copies at the border, the upwind
-// thickness (zero outside), and the divergence; bit-identical to the reference.
-template <typename T>
-__global__ void divflux_upwind_kernel(int ny, int nx, T dx, T rdx, const T* u, const T* v, const T* h, T* out) {
+// compute_divflux (igm/utils/gradient/compute_divflux.py:6-51): upwind (face
+// velocities with edge copies at the border, the upwind thickness, zero
+// outside) or centered (face averages of u h, edge copies), then the
+// divergence; bit-identical to the reference.
+template <typename T, int METHOD>
+__global__ void divflux_kernel(int ny, int nx, T dx, T rdx, const T* u, const T* v, const T* h, T* out) {
   const size_t n = (size_t)ny * nx;
   for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
     const int j = (int)(o / nx), i = (int)(o - (size_t)j * nx);
     auto hh = [&](int jj, int ii) { return (jj < 0 || jj >= ny || ii < 0 || ii >= nx) ? T(0) : h[(size_t)jj * nx + ii]; };
     auto uu = [&](int ii) { return u[(size_t)j * nx + ii]; };
     auto vv = [&](int jj) { return v[(size_t)jj * nx + i]; };
-    // x faces i (west) and i+1 (east)
-    const T uw = i == 0 ? uu(0) : T(0.5) * (uu(i - 1) + uu(i));
-    const T ue = i == nx - 1 ? uu(nx - 1) : T(0.5) * (uu(i) + uu(i + 1));
-    const T qw = uw * (uw > T(0) ? hh(j, i - 1) : hh(j, i));
-    const T qe = ue * (ue > T(0) ? hh(j, i) : hh(j, i + 1));
-    const T vs = j == 0 ? vv(0) : T(0.5) * (vv(j - 1) + vv(j));
-    const T vn = j == ny - 1 ? vv(ny - 1) : T(0.5) * (vv(j) + vv(j + 1));
-    const T qs = vs * (vs > T(0) ? hh(j - 1, i) : hh(j, i));
-    const T qn = vn * (vn > T(0) ? hh(j, i) : hh(j + 1, i));
+    T qw, qe, qs, qn;
+    if (METHOD == IGM_DIVFLUX_UPWIND) {
+      // x faces i (west) and i+1 (east)
+      const T uw = i == 0 ? uu(0) : T(0.5) * (uu(i - 1) + uu(i));
+      const T ue = i == nx - 1 ? uu(nx - 1) : T(0.5) * (uu(i) + uu(i + 1));
+      qw = uw * (uw > T(0) ? hh(j, i - 1) : hh(j, i));
+      qe = ue * (ue > T(0) ? hh(j, i) : hh(j, i + 1));
+      const T vs = j == 0 ? vv(0) : T(0.5) * (vv(j - 1) + vv(j));
+      const T vn = j == ny - 1 ? vv(ny - 1) : T(0.5) * (vv(j) + vv(j + 1));
+      qs = vs * (vs > T(0) ? hh(j - 1, i) : hh(j, i));
+      qn = vn * (vn > T(0) ? hh(j, i) : hh(j + 1, i));
+    } else {
+      // centered: the face averages of u h and v h, edge copies at the border
+      auto qx = [&](int ii) { return uu(ii) * hh(j, ii); };
+      auto qy = [&](int jj) { return vv(jj) * hh(jj, i); };
+      qw = i == 0 ? qx(0) : T(0.5) * (qx(i - 1) + qx(i));
+      qe = i == nx - 1 ? qx(nx - 1) : T(0.5) * (qx(i) + qx(i + 1));
+      qs = j == 0 ? qy(0) : T(0.5) * (qy(j - 1) + qy(j));
+      qn = j == ny - 1 ? qy(ny - 1) : T(0.5) * (qy(j) + qy(j + 1));
+    }
     out[o] = div_dx(qe - qw, dx, rdx) + div_dx(qn - qs, dx, rdx);
   }
 }
@@ -762,22 +774,36 @@ extern "C" int igm_vertical_velocity_incompressibility(int dtype, int nz, int ny
   return IGM_ERR_BAD_ARGUMENT;
 }
 
-extern "C" int igm_divflux_upwind(int dtype, int ny, int nx, double dx, const void* u, const void* v, const void* h,
-                                  void* out, void* stream) {
-  IGM_CHECK_ARG(ny >= 2 && nx >= 2 && dx > 0, IGM_ERR_BAD_SHAPE, "igm_divflux_upwind: bad shape or dx");
-  IGM_CHECK_ARG(u && v && h && out, IGM_ERR_BAD_ARGUMENT, "igm_divflux_upwind: NULL argument");
+extern "C" int igm_divflux(int dtype, int method, int ny, int nx, double dx, const void* u, const void* v,
+                           const void* h, void* out, void* stream) {
+  IGM_CHECK_ARG(ny >= 2 && nx >= 2 && dx > 0, IGM_ERR_BAD_SHAPE, "igm_divflux: bad shape or dx");
+  IGM_CHECK_ARG(u && v && h && out, IGM_ERR_BAD_ARGUMENT, "igm_divflux: NULL argument");
+  IGM_CHECK_ARG(method == IGM_DIVFLUX_UPWIND || method == IGM_DIVFLUX_CENTERED, IGM_ERR_BAD_ARGUMENT,
+                "igm_divflux: unknown method %d", method);
   cudaStream_t st = as_stream(stream);
   const int grid = grid1d((size_t)ny * nx);
-  if (dtype == IGM_F32) {
-    const float d = (float)dx;
-    divflux_upwind_kernel<float><<<grid, 256, 0, st>>>(ny, nx, d, 1.0f / d, (const float*)u, (const float*)v,
-                                                       (const float*)h, (float*)out);
-  } else if (dtype == IGM_F64) {
-    divflux_upwind_kernel<double><<<grid, 256, 0, st>>>(ny, nx, dx, 1.0 / dx, (const double*)u, (const double*)v,
-                                                        (const double*)h, (double*)out);
-  } else {
-    set_error("igm_divflux_upwind: unknown dtype %d", dtype);
+  auto run = [&](auto zero) {
+    using T = decltype(zero);
+    const T d = (T)dx;
+    if (method == IGM_DIVFLUX_UPWIND)
+      divflux_kernel<T, IGM_DIVFLUX_UPWIND><<<grid, 256, 0, st>>>(ny, nx, d, T(1) / d, (const T*)u, (const T*)v,
+                                                                  (const T*)h, (T*)out);
+    else
+      divflux_kernel<T, IGM_DIVFLUX_CENTERED><<<grid, 256, 0, st>>>(ny, nx, d, T(1) / d, (const T*)u, (const T*)v,
+                                                                    (const T*)h, (T*)out);
+  };
+  if (dtype == IGM_F32)
+    run(0.f);
+  else if (dtype == IGM_F64)
+    run(0.0);
+  else {
+    set_error("igm_divflux: unknown dtype %d", dtype);
     return IGM_ERR_BAD_ARGUMENT;
   }
-  return launch_status("divflux_upwind_kernel");
+  return launch_status("divflux_kernel");
+}
+
+extern "C" int igm_divflux_upwind(int dtype, int ny, int nx, double dx, const void* u, const void* v, const void* h,
+                                  void* out, void* stream) {
+  return igm_divflux(dtype, IGM_DIVFLUX_UPWIND, ny, nx, dx, u, v, h, out, stream);
 }

@@ -231,10 +231,53 @@ def assim_stats(thk, dx, icemaskobs, thkobs=None, uvs=None, vvs=None, uobs=None,
     return out
 
 
-def divflux_upwind(u, v, h, dx, out=None):
+DIVFLUX_METHODS = {"upwind": 0, "centered": 1}
+
+
+def divflux(u, v, h, dx, method="upwind", out=None):
+    """compute_divflux (igm_divflux), method "upwind" or "centered"."""
+    if method not in DIVFLUX_METHODS:
+        raise NotImplementedError(f"divflux method {method!r}")
     ny, nx = h.shape
     out = out if out is not None else torch.empty_like(h)
-    rc = L.lib().igm_divflux_upwind(L.dtype_code(h.dtype), ny, nx, float(dx), L.ptr(u), L.ptr(v), L.ptr(h),
-                                    L.ptr(out), L.stream_ptr())
-    L.check(rc, "igm_divflux_upwind")
+    rc = L.lib().igm_divflux(L.dtype_code(h.dtype), DIVFLUX_METHODS[method], ny, nx, float(dx), L.ptr(u), L.ptr(v),
+                             L.ptr(h), L.ptr(out), L.stream_ptr())
+    L.check(rc, "igm_divflux")
     return out
+
+
+def divflux_upwind(u, v, h, dx, out=None):
+    return divflux(u, v, h, dx, "upwind", out)
+
+
+def assim_divflux_cost_grad(kind, ubar, vbar, thk, D, dx, icemaskobs, g_thk, dU, dV, vert_weight, *, divfluxobs=None,
+                            usurf=None, slope=0.0, intercept=0.0, std=1.0, regu=1.0, force_zero_sum=False,
+                            method="upwind", mask_thk=None, scratch=None, partials=None, cost=None):
+    """The flux-divergence cost (igm_assim_divflux_cost_grad), kind "obs"
+    (cost_divfluxobs) or "fcz" (cost_divfluxfcz): returns the device cost
+    (double[1]); adds dC/dthk into g_thk and dC/d(ubar, vbar) times the
+    vertical weights into dU, dV [nz, ny, nx] (added on the top level,
+    assigned below)."""
+    ny, nx = thk.shape
+    nz = int(dU.shape[-3])
+    lib = L.lib()
+    n_parts = 148 * 8
+    if partials is None:
+        partials = torch.empty(int(lib.igm_assim_divflux_partials_len(n_parts)), dtype=torch.float64,
+                               device=thk.device)
+    else:
+        n_parts = (partials.numel() - 3) // 6
+    scratch = scratch if scratch is not None else torch.empty_like(thk)
+    cost = cost if cost is not None else torch.empty(1, dtype=torch.float64, device=thk.device)
+    p = L.DivfluxCostParams()
+    p.kind = {"obs": 0, "fcz": 1}[kind]
+    p.method = DIVFLUX_METHODS[method]
+    p.force_zero_sum = int(bool(force_zero_sum))
+    p.divfluxobs_std, p.regu_divflux, p.slope, p.intercept = float(std), float(regu), float(slope), float(intercept)
+    w = (C.c_double * nz)(*[float(x) for x in np.asarray(vert_weight, dtype=np.float64).reshape(-1)[:nz]])
+    rc = lib.igm_assim_divflux_cost_grad(L.dtype_code(thk.dtype), ny, nx, float(dx), nz, w, L.ptr(ubar), L.ptr(vbar),
+                                         L.ptr(thk), L.ptr(D), L.ptr(divfluxobs), L.ptr(usurf), L.ptr(icemaskobs),
+                                         L.ptr(mask_thk), C.byref(p), L.ptr(g_thk), L.ptr(dU), L.ptr(dV),
+                                         L.ptr(scratch), L.ptr(partials), n_parts, L.ptr(cost), L.stream_ptr())
+    L.check(rc, "igm_assim_divflux_cost_grad")
+    return cost

@@ -16,6 +16,7 @@ launches with no host synchronisation:
   CNN forward (keep activations, thk mask), velsurf / velbar
   igm_assim_flow_direction      (anisotropic regularisation only)
   igm_assim_cost_grad           costs, dC/dthk, dC/d(top-layer U, V)
+  igm_divflux + igm_assim_divflux_cost_grad (divfluxobs / divfluxfcz only)
   CNN backward, data chain only, with igm_cnn_input_gradient
   igm_assim_control mode 1      gradient of thk_sc, zero outside the mask
   igm_adam_clipnorm             Keras legacy Adam at iteration i + 1
@@ -29,10 +30,11 @@ the netCDF snapshots every ``output.freq`` iterations and the final
 ``save_result_in_ncdf`` file are host copies.  The 2-D plots of the
 reference (matplotlib) are not drawn.
 
-Supported: control_list [thk]; cost_list within velsurf, thk, icemask;
-method ADAM; sole_mask, fix_opti_normalization_issue, include_low_speed_term,
-cook.infer_params and pertubate off; divflux.method upwind.  Anything else
-raises NotImplementedError.
+Supported: control_list [thk]; cost_list within velsurf, thk, icemask,
+divfluxobs, divfluxfcz (the flux-divergence terms, with or without
+force_zero_sum); method ADAM; sole_mask, fix_opti_normalization_issue,
+include_low_speed_term, cook.infer_params and pertubate off; divflux.method
+upwind or centered.  Anything else raises NotImplementedError.
 """
 
 from __future__ import annotations
@@ -48,7 +50,8 @@ from .. import kernels as K
 from .. import state as S
 from . import iceflow as P
 
-_COST_KEYS = ["velsurf", "thk", "icemask", "thk_positive", "thk_regu"]
+_COST_KEYS = ["velsurf", "thk", "icemask", "thk_positive", "thk_regu"]  # the columns of igm_assim_cost_grad
+_ALL_KEYS = ["velsurf", "thk", "divflux", "icemask", "thk_positive", "thk_regu"]  # total_cost.py's order
 
 
 def _check_supported(cfg):
@@ -57,9 +60,9 @@ def _check_supported(cfg):
     bad = []
     if list(da.control_list) != ["thk"]:
         bad.append(f"control_list={list(da.control_list)} (only ['thk'])")
-    extra = [c for c in da.cost_list if c not in ("velsurf", "thk", "icemask")]
+    extra = [c for c in da.cost_list if c not in ("velsurf", "thk", "icemask", "divfluxobs", "divfluxfcz")]
     if extra:
-        bad.append(f"cost terms {extra} (only velsurf, thk, icemask)")
+        bad.append(f"cost terms {extra} (only velsurf, thk, icemask, divfluxobs, divfluxfcz)")
     if o.method != "ADAM":
         bad.append(f"optimization.method={o.method!r} (only 'ADAM')")
     for key in ("sole_mask", "fix_opti_normalization_issue", "pertubate"):
@@ -69,8 +72,8 @@ def _check_supported(cfg):
         bad.append("fitting.include_low_speed_term")
     if bool(da.cook.infer_params):
         bad.append("cook.infer_params")
-    if da.divflux.method != "upwind" or bool(da.divflux.get("force_zero_sum", False)):
-        bad.append(f"divflux.method={da.divflux.method!r} (only 'upwind' without force_zero_sum)")
+    if da.divflux.method not in K.DIVFLUX_METHODS:
+        bad.append(f"divflux.method={da.divflux.method!r} (upwind or centered)")
     if da.regularization.to_regularize not in ("topg", "thk"):
         bad.append(f"to_regularize={da.regularization.to_regularize!r}")
     if cfg.processes.iceflow.method != "emulated":
@@ -157,6 +160,18 @@ class _Assim:
         self.params = p
         self.present = [("velsurf" in costs), ("thk" in costs), bool(p.penalty and p.icemask_cost),
                         bool(p.penalty), True]
+        # flux-divergence cost (total_cost.py:23-27: divfluxfcz before divfluxobs)
+        self.div_kind = "fcz" if "divfluxfcz" in costs else ("obs" if "divfluxobs" in costs else None)
+        self.div_method = str(da.divflux.method)
+        self.div_hist = torch.zeros(nit, dtype=torch.float64, device=d)
+        self.div_res = None  # (slope, intercept) of cost_divfluxfcz's regression
+        if self.div_kind is not None:
+            self.D = torch.empty((ny, nx), **f32)
+            self.div_scratch = torch.empty((ny, nx), **f32)
+            self.div_partials = torch.empty(int(L.lib().igm_assim_divflux_partials_len(148 * 8)),
+                                            dtype=torch.float64, device=d)
+            self.divfluxobs = S.get(state, "divfluxobs").contiguous() if self.div_kind == "obs" else None
+            self.vert_weight = np.asarray(torch.as_tensor(state.vert_weight).cpu(), dtype=np.float64).reshape(-1)
         self.sc = float(da.scaling.thk)
         self.reproject = "reproject" in o.obstacle_constraint
 
@@ -177,6 +192,8 @@ def optimize_initialize(cfg, state):
     if bool(da.optimization.init_zero_thk):
         thk = thk * 0.0
     S.put(state, "thk", thk.contiguous())
+    if "divfluxobs" in da.cost_list and not hasattr(state, "divfluxobs"):
+        S.put(state, "divfluxobs", S.get(state, "smb") - S.get(state, "dhdt"))
     dens = _density_weights(thkobs.astype(np.float32), bool(da.fitting.uniformize_thkobs))
     S.put(state, "dens_thkobs", torch.as_tensor(dens, device=thk.device))
     sl = S.get(state, "slidingco")
@@ -227,6 +244,8 @@ def optimize_update(cfg, state, cost, i):
     K.assim_cost_grad(thk, S.get(state, "usurf"), uvs.contiguous(), vvs.contiguous(), a.uobs, a.vobs, a.thkobs,
                       a.dens, a.icemaskobs, flow, a.dx, a.params, partials=a.partials, costs=a.cost_hist[i],
                       g_thk=a.g_thk, g_u=a.dU[0, a.nz - 1], g_v=a.dV[0, a.nz - 1])
+    if a.div_kind is not None:
+        _divflux_cost(cfg, state, a, thk, i)
     model.backward(buf, 1, a.ny, a.nx, a.dU, a.dV, field_grad=a.field_grad, param_grads=False)
     K.assim_control(1, thk, a.sc, icemaskobs=a.icemaskobs, grad=a.grad, g_direct=a.g_thk,
                     g_emul=a.field_grad[0, 0].reshape(-1))
@@ -236,13 +255,47 @@ def optimize_update(cfg, state, cost, i):
     K.assim_control(2, thk, a.sc, icemaskobs=a.icemaskobs, variable=a.var,
                     reproject_mask=a.reproject and "icemask" in a.cost_list, reproject_pos=a.reproject)
     S.put(state, "thk", thk)
-    S.put(state, "divflux", K.divflux_upwind(S.get(state, "ubar").contiguous(), S.get(state, "vbar").contiguous(),
-                                             thk, a.dx))
+    S.put(state, "divflux", K.divflux(S.get(state, "ubar").contiguous(), S.get(state, "vbar").contiguous(), thk,
+                                      a.dx, a.div_method))
     cost["all"] = a.cost_hist[i]
+    if a.div_kind is not None:
+        cost["divflux"] = a.div_hist[i]
 
 
-def _cost_dict(a: _Assim, row):
-    return {k: float(row[j]) for j, k in enumerate(_COST_KEYS) if a.present[j]}
+def _divflux_cost(cfg, state, a: _Assim, thk, i):
+    """cost_divfluxobs / cost_divfluxfcz (cost_terms/cost_divfluxobs.py:9-29,
+    cost_divfluxfcz.py:10-38) of the emulated velbar and the current
+    thickness: the cost into the history, dC/dthk added to the direct
+    gradient, dC/dvelbar spread over the levels of dU, dV.  cost_divfluxfcz
+    refits its target (scipy's linregress of divflux on usurf inside the mask,
+    on the host) at every 10th iteration, as the reference."""
+    da = cfg.processes.data_assimilation
+    ub, vb = S.get(state, "ubar").contiguous(), S.get(state, "vbar").contiguous()
+    D = K.divflux(ub, vb, thk, a.dx, a.div_method, out=a.D)
+    usurf = S.get(state, "usurf").contiguous()
+    if a.div_kind == "fcz" and (i % 10 == 0 or a.div_res is None):
+        from scipy import stats
+        act = (a.icemaskobs > 0.5).cpu().numpy()
+        res = stats.linregress(usurf.cpu().numpy()[act], D.cpu().numpy()[act])
+        a.div_res = (float(res.slope), float(res.intercept))
+        state.res = res
+    slope, intercept = a.div_res if a.div_res is not None else (0.0, 0.0)
+    K.assim_divflux_cost_grad(a.div_kind, ub, vb, thk, D, a.dx, a.icemaskobs, a.g_thk, a.dU[0], a.dV[0],
+                              a.vert_weight, divfluxobs=a.divfluxobs, usurf=usurf if a.div_kind == "fcz" else None,
+                              slope=slope, intercept=intercept, std=float(da.fitting.divfluxobs_std),
+                              regu=float(da.regularization.divflux),
+                              force_zero_sum=bool(da.divflux.get("force_zero_sum", False)), method=a.div_method,
+                              mask_thk=thk, scratch=a.div_scratch, partials=a.div_partials, cost=a.div_hist[i:i + 1])
+
+
+def _cost_table(a: _Assim, n_it):
+    """The per-iteration costs in total_cost's order: (keys, [n_it, k] array)."""
+    ch = a.cost_hist[:n_it].cpu().numpy()
+    cols = {k: ch[:, j] for j, k in enumerate(_COST_KEYS) if a.present[j]}
+    if a.div_kind is not None:
+        cols["divflux"] = a.div_hist[:n_it].cpu().numpy()
+    keys = [k for k in _ALL_KEYS if k in cols]
+    return keys, np.stack([cols[k] for k in keys], axis=1)
 
 
 def _mag(u, v):
@@ -335,16 +388,16 @@ def _write_histories(cfg, state, n_it, glen):
     from the device histories; the record lists on the state as in
     utils.py:13-66."""
     a: _Assim = state._igm_assim
-    ch = a.cost_hist[:n_it].cpu().numpy()
+    keys, ch = _cost_table(a, n_it)
     rh = a.rms_hist[:n_it].cpu().numpy()
     names = ["rmsthk", "stdthk", "rmsvel", "stdvel", "rmsdiv", "stddiv", "rmsusurf", "stdusurf", "vol"]
     for j, k in enumerate(names):
         setattr(state, k, [float(x) for x in rh[:, j]])
-    keys = [k for j, k in enumerate(_COST_KEYS) if a.present[j]] + (["glen"] if glen else [])
+    keys = keys + (["glen"] if glen else [])
     with open("costs.dat", "w") as fh:
         print("   ".join(f"{k:>12}" for k in keys), file=fh)
         for i in range(n_it):
-            vals = [ch[i, j] for j in range(5) if a.present[j]] + ([glen[i]] if glen else [])
+            vals = list(ch[i]) + ([glen[i]] if glen else [])
             print("   ".join(f"{min(float(v), 9999999):>12.4f}" for v in vals), file=fh)
     np.savetxt("rms_std_vol.dat", rh, fmt="%.10f", comments="",
                header="        rmsthk      stdthk       rmsvel       stdvel       rmsdiv       stddiv       "
@@ -377,7 +430,8 @@ def initialize(cfg, state):
     if da.output.save_result_in_ncdf != "":
         output_ncdf_optimize_final(cfg, state)
     _write_histories(cfg, state, n_it, glen)
-    state.costs_data_assimilation = [_cost_dict(a, r) for r in a.cost_hist[:n_it].cpu()]
+    keys, table = _cost_table(a, n_it)
+    state.costs_data_assimilation = [dict(zip(keys, map(float, r))) for r in table]
     S.sync_host(state)
 
 

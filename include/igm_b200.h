@@ -56,6 +56,7 @@ typedef enum igm_status {
 typedef enum igm_dtype { IGM_F32 = 0, IGM_F64 = 1 } igm_dtype;
 
 typedef enum igm_slope_type { IGM_GODUNOV = 0, IGM_MINMOD = 1, IGM_SUPERBEE = 2 } igm_slope_type;
+typedef enum igm_divflux_method { IGM_DIVFLUX_UPWIND = 0, IGM_DIVFLUX_CENTERED = 1 } igm_divflux_method;
 
 typedef enum igm_conv_mode {
   IGM_CONV_FWD_LEAKY = 0, /* y = LeakyReLU(conv3x3(x) + bias) */
@@ -331,6 +332,39 @@ IGM_API int igm_assim_stats(int dtype, int ny, int nx, double dx, const void* th
                             const void* divfluxobs, const void* usurf, const void* usurfobs, double* partials,
                             int n_parts, double* out, void* stream);
 
+/* Parameters of the flux-divergence cost terms. */
+typedef struct igm_divflux_cost_params {
+  int32_t kind;            /* 0: cost_divfluxobs, 1: cost_divfluxfcz */
+  int32_t method;          /* igm_divflux_method: divflux.method */
+  int32_t force_zero_sum;  /* divflux.force_zero_sum */
+  int32_t reserved;
+  double divfluxobs_std;   /* fitting.divfluxobs_std */
+  double regu_divflux;     /* regularization.divflux (kind 0: weight of the smoothness of divflux) */
+  double slope, intercept; /* kind 1: the regression of divflux on usurf (a constant of the gradient) */
+} igm_divflux_cost_params;
+
+/* The flux-divergence cost terms of data assimilation and their gradient:
+ * cost_divfluxobs (cost_terms/cost_divfluxobs.py:9-29): 0.5 mean over the
+ * observed nodes of ((divfluxobs - D) / std)^2 + regu 0.5 (mean (dD/dx)^2 +
+ * mean (dD/dy)^2); cost_divfluxfcz (cost_terms/cost_divfluxfcz.py:10-38): the
+ * target intercept + slope usurf inside icemaskobs > 0.5, 0.5 mean over the
+ * mask of ((target - D) / std)^2; both + 0.5 1000 mean_mask(D / std)^2 with
+ * force_zero_sum.  divflux = D = igm_divflux(ubar, vbar, thk) of the same
+ * method.  Writes *cost (device double) and the gradient: grad_thk[n] +=
+ * dC/dthk (through the flux's thickness), dU, dV [nz][ny][nx] = vert_weight[k]
+ * dC/dubar (velbar = sum_k vert_weight[k] U_k), zero where mask_thk <= 0
+ * (NULL: no mask), ADDED to the top level nz - 1 (which holds dC/dvelsurf of
+ * igm_assim_cost_grad) and assigned to the others.  vert_weight: host
+ * double[nz]; scratch: device [n] of the dtype; partials: device
+ * double[igm_assim_divflux_partials_len(n_parts)]. */
+IGM_API int igm_assim_divflux_cost_grad(int dtype, int ny, int nx, double dx, int nz, const double* vert_weight,
+                                        const void* ubar, const void* vbar, const void* thk, const void* divflux,
+                                        const void* divfluxobs, const void* usurf, const void* icemaskobs,
+                                        const void* mask_thk, const igm_divflux_cost_params* params,
+                                        void* grad_thk, void* dU, void* dV, void* scratch, double* partials,
+                                        int n_parts, double* cost, void* stream);
+IGM_API size_t igm_assim_divflux_partials_len(int n_parts);
+
 /* compute_flow_direction_for_anisotropic_smoothing (data_assimilation/utils.py:
  * 86-110): cell averages of the surface velocity (NaN as 0), a Gaussian of
  * sigma 3 cells (radius 12, zero outside; y then x, as scipy.ndimage), then
@@ -339,10 +373,15 @@ IGM_API int igm_assim_stats(int dtype, int ny, int nx, double dx, const void* th
 IGM_API int igm_assim_flow_direction(int dtype, int ny, int nx, const void* uvelsurf, const void* vvelsurf,
                              void* flowdirx, void* flowdiry, void* scratch, void* stream);
 
-/* compute_divflux, method upwind (igm/utils/gradient/compute_divflux.py:17-33,
- * 45-46), as data assimilation computes state.divflux after each update: face
- * velocities (edge copies at the border), upwind thickness (zero outside),
- * d(u h)/dx + d(v h)/dy.  Bit-identical to the reference in FP32/FP64. */
+/* compute_divflux (igm/utils/gradient/compute_divflux.py:6-51), as data
+ * assimilation computes state.divflux after each update and in its
+ * flux-divergence costs: method IGM_DIVFLUX_UPWIND (face velocities with edge
+ * copies at the border, upwind thickness, zero outside) or
+ * IGM_DIVFLUX_CENTERED (face averages of u h, edge copies), then
+ * d(u h)/dx + d(v h)/dy.  Bit-identical to the reference in FP32/FP64.
+ * igm_divflux_upwind is igm_divflux with IGM_DIVFLUX_UPWIND. */
+IGM_API int igm_divflux(int dtype, int method, int ny, int nx, double dx, const void* u, const void* v, const void* h,
+                        void* out, void* stream);
 IGM_API int igm_divflux_upwind(int dtype, int ny, int nx, double dx, const void* u, const void* v, const void* h,
                        void* out, void* stream);
 

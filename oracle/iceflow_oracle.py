@@ -828,7 +828,8 @@ class AssimControl:
 
 
 def da_optimize_update(thk, usurf, arrhenius, slidingco, dx, weights, biases, Nz, vert_weight, obs, p: AssimParams,
-                       ctl: AssimControl, optimizer: KerasLegacyAdam, i, bf16=True, out_scale=1.0, input_scales=None):
+                       ctl: AssimControl, optimizer: KerasLegacyAdam, i, bf16=True, out_scale=1.0, input_scales=None,
+                       divflux_cost=None):
     """One ADAM iteration of optimize_update (optimize/update.py:15-103) for
     control_list [thk]: thk_sc = thk / sc is a new variable (fresh Adam
     slots, the optimizer's iteration count carries on), thk = thk_sc sc, the
@@ -842,7 +843,11 @@ def da_optimize_update(thk, usurf, arrhenius, slidingco, dx, weights, biases, Nz
     ``obs``: dict uobs, vobs, thkobs, dens, icemaskobs, icemask.  Returns
     (thk, costs dict, dict of uvelsurf, vvelsurf, ubar, vbar, divflux,
     gradient).  ``input_scales``: per-channel factors of the network input
-    (None: the raw fields, as the reference)."""
+    (None: the raw fields, as the reference).  ``divflux_cost``: None or a
+    dict (kind "obs"/"fcz", method, std, regu, force_zero_sum, divfluxobs)
+    adding cost_divfluxobs / cost_divfluxfcz of the emulated velbar
+    (total_cost.py:23-27); for "fcz" the regression is refitted at every 10th
+    iteration and kept in the dict ("slope", "intercept")."""
     sc = ctl.scaling_thk
     thk_sc = (thk / sc).detach().clone().requires_grad_(True)
     th = thk_sc * sc
@@ -860,6 +865,17 @@ def da_optimize_update(thk, usurf, arrhenius, slidingco, dx, weights, biases, Nz
         flow = da_flow_direction(uvs.detach(), vvs.detach())
     cost = da_costs(th, usurf, uvs, vvs, obs["uobs"], obs["vobs"], obs["thkobs"], obs["dens"], obs["icemaskobs"],
                     obs["icemask"], flow, dx, p)
+    if divflux_cost is not None:
+        dc = divflux_cost
+        ub_g, vb_g = torch.sum(U * vert_weight, 0), torch.sum(V * vert_weight, 0)
+        if dc["kind"] == "fcz" and (i % 10 == 0 or "slope" not in dc):
+            act = obs["icemaskobs"] > 0.5
+            D0 = compute_divflux(ub_g.detach(), vb_g.detach(), th.detach(), dx, dc["method"])
+            dc["slope"], dc["intercept"] = linregress(usurf[act].numpy(), D0[act].numpy())
+        cost["divflux"] = da_cost_divflux(dc["kind"], ub_g, vb_g, th, dx, obs["icemaskobs"],
+                                          divfluxobs=dc.get("divfluxobs"), usurf=usurf, slope=dc.get("slope"),
+                                          intercept=dc.get("intercept"), std=dc["std"], regu=dc["regu"],
+                                          force_zero_sum=dc["force_zero_sum"], method=dc["method"])
     total = sum(cost.values())
     (g,) = torch.autograd.grad(total, thk_sc)
     g = torch.where(obs["icemaskobs"] > 0.5, g, torch.zeros_like(g))
@@ -875,8 +891,9 @@ def da_optimize_update(thk, usurf, arrhenius, slidingco, dx, weights, biases, Nz
     U, V = U.detach(), V.detach()
     ubar = torch.sum(U * vert_weight, 0)
     vbar = torch.sum(V * vert_weight, 0)
+    method = divflux_cost["method"] if divflux_cost is not None else "upwind"
     aux = {"uvelsurf": uvs.detach(), "vvelsurf": vvs.detach(), "ubar": ubar, "vbar": vbar,
-           "divflux": divflux_upwind(ubar, vbar, thk_new, dx), "gradient": g}
+           "divflux": compute_divflux(ubar, vbar, thk_new, dx, method), "gradient": g}
     return thk_new, {k: v.detach() for k, v in cost.items()}, aux
 
 
@@ -907,3 +924,53 @@ def da_rms_std(thk, thkobs, uvelsurf, vvelsurf, uobs, vobs, icemaskobs, dx, divf
     out["rmsusurf"], out["stdusurf"] = ms(usurf[I] - usurfobs[I]) if usurfobs is not None else (0.0, 0.0)
     out["vol"] = float(thk.double().sum() * dx * dx / 1e9)
     return out
+
+
+def compute_divflux(u, v, h, dx, method="upwind"):
+    """compute_divflux (utils/gradient/compute_divflux.py:6-51): upwind (the
+    face velocity carries the upwind thickness, zero outside) or centered (the
+    face average of u h, edge copies at the border)."""
+    if method == "upwind":
+        return divflux_upwind(u, v, h, dx)
+    if method != "centered":
+        raise ValueError(method)
+    qx, qy = u * h, v * h
+    Qx = torch.cat([qx[:, 0:1], 0.5 * (qx[:, :-1] + qx[:, 1:]), qx[:, -1:]], 1)
+    Qy = torch.cat([qy[0:1, :], 0.5 * (qy[:-1, :] + qy[1:, :]), qy[-1:, :]], 0)
+    return (Qx[:, 1:] - Qx[:, :-1]) / dx + (Qy[1:, :] - Qy[:-1, :]) / dx
+
+
+def linregress(x, y):
+    """Least-squares line y = intercept + slope x (scipy.stats.linregress's
+    slope and intercept), in float64."""
+    x, y = np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64)
+    xm, ym = x.mean(), y.mean()
+    sxx = ((x - xm) ** 2).mean()
+    sxy = ((x - xm) * (y - ym)).mean()
+    slope = sxy / sxx
+    return slope, ym - slope * xm
+
+
+def da_cost_divflux(kind, ubar, vbar, thk, dx, icemaskobs, divfluxobs=None, usurf=None, slope=None,
+                    intercept=None, std=1.0, regu=1.0, force_zero_sum=False, method="upwind"):
+    """cost_divfluxobs (cost_terms/cost_divfluxobs.py:9-29, kind "obs"):
+    0.5 mean(((obs - D) / std)^2) over the observed nodes + regu 0.5
+    (mean(dD/dx^2) + mean(dD/dy^2)); cost_divfluxfcz
+    (cost_terms/cost_divfluxfcz.py:10-38, kind "fcz"): the target intercept +
+    slope usurf inside icemaskobs > 0.5 (the regression is a constant of the
+    gradient), 0.5 mean(((target - D) / std)^2) over the mask; both plus
+    0.5 1000 mean(D / std)^2 over the mask with force_zero_sum."""
+    D = compute_divflux(ubar, vbar, thk, dx, method)
+    act_m = icemaskobs > 0.5
+    if kind == "obs":
+        act = ~torch.isnan(divfluxobs)
+        c = 0.5 * torch.mean(((divfluxobs[act] - D[act]) / std) ** 2)
+        dddx = (D[:, 1:] - D[:, :-1]) / dx
+        dddy = (D[1:, :] - D[:-1, :]) / dx
+        c = c + regu * 0.5 * (torch.mean(dddx ** 2) + torch.mean(dddy ** 2))
+    else:
+        tar = torch.where(act_m, intercept + slope * usurf, torch.zeros_like(usurf))
+        c = 0.5 * torch.mean(((tar[act_m] - D[act_m]) / std) ** 2)
+    if force_zero_sum:
+        c = c + 0.5 * 1000 * torch.mean(D[act_m] / std) ** 2
+    return c

@@ -411,6 +411,64 @@ def assim_cases():
     save("assim", out)
 
 
+def divflux_cases():
+    """compute_divflux (utils/gradient/compute_divflux.py:6-51), both methods,
+    and the flux-divergence cost terms cost_divfluxobs (with and without
+    force_zero_sum) and cost_divfluxfcz, executed from the reference's files,
+    with torch autograd gradients w.r.t. ubar, vbar and thk.  cost_divfluxfcz
+    is called twice, as in the reference's loop: at i = 0 on detached inputs
+    (its scipy regression sets state.res), then at i = 1 with gradients."""
+    cd = importlib.import_module("igm.utils.gradient.compute_divflux")
+    co = importlib.import_module("igm.processes.data_assimilation.cost_terms.cost_divfluxobs")
+    cf = importlib.import_module("igm.processes.data_assimilation.cost_terms.cost_divfluxfcz")
+    out = {}
+    for tag, dtype in [("f64", torch.float64), ("f32", torch.float32)]:
+        rng = np.random.default_rng(17)
+        ny, nx, dx = 19, 27, 100.0
+        g = glacier(ny, nx, dx, 13, dtype)
+        f = lambda a: torch.as_tensor(np.asarray(a), dtype=dtype)  # noqa: E731
+        thk = g["thk"] + f(np.abs(rng.normal(0, 5, (ny, nx))))
+        usurf = g["usurf"]
+        u, v = f(rng.normal(15, 20, (ny, nx))), f(rng.normal(0, 20, (ny, nx)))
+        for m in ("upwind", "centered"):
+            out[f"{tag}_div_{m}"] = cd.compute_divflux(u, v, thk, dx, dx, method=m)
+        icemaskobs = f((g["thk"].numpy() > 0).astype(np.float64))
+        dobs = f(rng.normal(0, 2, (ny, nx)))
+        dobs[rng.uniform(size=(ny, nx)) < 0.3] = float("nan")
+        out.update({f"{tag}_{k}": x for k, x in dict(u=u, v=v, thk=thk, usurf=usurf, icemaskobs=icemaskobs,
+                                                     divfluxobs=dobs, dx=np.asarray(dx)).items()})
+        with open(os.path.join(IGM, "conf", "processes", "data_assimilation.yaml")) as fh:
+            da = yaml.safe_load(fh)["data_assimilation"]
+        for method in ("upwind", "centered"):
+            for kind, fzs in (("obs", False), ("obs", True), ("fcz", False), ("fcz", True)):
+                cfg = load_cfg()
+                da["divflux"]["method"] = method
+                da["divflux"]["force_zero_sum"] = fzs
+                da["fitting"]["divfluxobs_std"] = 0.7
+                da["regularization"]["divflux"] = 3.0
+                cfg.processes.data_assimilation = ns(da)
+                key = f"{tag}_{method}_{kind}{'_zs' if fzs else ''}"
+
+                def state(grad):
+                    w = (lambda t: t.clone().requires_grad_(True)) if grad else (lambda t: t.clone())
+                    return types.SimpleNamespace(ubar=w(u), vbar=w(v), thk=w(thk), usurf=usurf, dx=dx,
+                                                 divfluxobs=dobs, icemaskobs=icemaskobs)
+                if kind == "obs":
+                    st = state(True)
+                    c = co.cost_divfluxobs(cfg, st, 0)
+                else:
+                    st0 = state(False)
+                    cf.cost_divfluxfcz(cfg, st0, 0)
+                    st = state(True)
+                    st.res = st0.res
+                    c = cf.cost_divfluxfcz(cfg, st, 1)
+                    out[f"{key}_slope"] = np.asarray(st0.res.slope)
+                    out[f"{key}_intercept"] = np.asarray(st0.res.intercept)
+                gu, gv, gh = torch.autograd.grad(c, [st.ubar, st.vbar, st.thk])
+                out.update({f"{key}_cost": c, f"{key}_g_u": gu, f"{key}_g_v": gv, f"{key}_g_h": gh})
+    save("divflux", out)
+
+
 def save(name, d):
     arrs = {}
     for k, v in d.items():
@@ -437,5 +495,6 @@ if __name__ == "__main__":
     time_case()
     emulator_case()
     vert_flow_cases()
+    divflux_cases()
     keras_h5_cases()
     assim_cases()

@@ -102,3 +102,69 @@ def test_stats_match_oracle(dtype, present):
                            divflux=t["div"], divfluxobs=t["divobs"], usurf=t["us"], usurfobs=t["usobs"])
     tol = 1e-5 if dtype == torch.float32 else 1e-9
     np.testing.assert_allclose(ours, [ref[k] for k in STAT_KEYS], rtol=tol, atol=tol)
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("method", ["upwind", "centered"])
+def test_divflux_methods_match_reference(golden, tag, method):
+    """compute_divflux of the reference source, bit for bit."""
+    g = golden("divflux")
+    dt = torch.float64 if tag == "f64" else torch.float32
+    u, v, h = (dev(g[f"{tag}_{k}"], dt) for k in ("u", "v", "thk"))
+    out = K.divflux(u, v, h, float(g[f"{tag}_dx"]), method)
+    np.testing.assert_array_equal(out.cpu().numpy(), g[f"{tag}_div_{method}"])
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("method", ["upwind", "centered"])
+@pytest.mark.parametrize("kind", ["obs", "obs_zs", "fcz", "fcz_zs"])
+def test_divflux_cost_terms_match_reference(golden, tag, method, kind):
+    """cost_divfluxobs / cost_divfluxfcz of the reference source and their
+    gradients w.r.t. ubar, vbar (one level of weight 1, no mask) and thk."""
+    g = golden("divflux")
+    dt = torch.float64 if tag == "f64" else torch.float32
+    key = f"{tag}_{method}_{kind}"
+    d = {k: dev(g[f"{tag}_{k}"], dt) for k in ("u", "v", "thk", "usurf", "icemaskobs", "divfluxobs")}
+    dx = float(g[f"{tag}_dx"])
+    D = K.divflux(d["u"], d["v"], d["thk"], dx, method)
+    ny, nx = D.shape
+    gt = torch.zeros_like(D)
+    dU, dV = torch.zeros((1, ny, nx), dtype=dt, device="cuda"), torch.zeros((1, ny, nx), dtype=dt, device="cuda")
+    fcz = kind.startswith("fcz")
+    c = K.assim_divflux_cost_grad("fcz" if fcz else "obs", d["u"], d["v"], d["thk"], D, dx, d["icemaskobs"], gt, dU,
+                                  dV, [1.0], divfluxobs=None if fcz else d["divfluxobs"],
+                                  usurf=d["usurf"] if fcz else None,
+                                  slope=float(g[f"{key}_slope"]) if fcz else 0.0,
+                                  intercept=float(g[f"{key}_intercept"]) if fcz else 0.0, std=0.7, regu=3.0,
+                                  force_zero_sum=kind.endswith("_zs"), method=method)
+    tol = 1e-9 if tag == "f64" else 1e-4
+    np.testing.assert_allclose(float(c.item()), float(g[f"{key}_cost"]), rtol=tol)
+    for a, k in [(gt, "g_h"), (dU[0], "g_u"), (dV[0], "g_v")]:
+        ref = g[f"{key}_{k}"]
+        np.testing.assert_allclose(a.cpu().numpy(), ref, rtol=tol, atol=tol * np.abs(ref).max())
+
+
+def test_divflux_gradient_levels_and_mask(golden):
+    """The velbar gradient spread over the levels with the vertical weights,
+    zero where the thk mask is off, added on the top level (which holds the
+    surface-velocity gradient) and assigned below."""
+    g = golden("divflux")
+    d = {k: dev(g[f"f64_{k}"], torch.float64) for k in ("u", "v", "thk", "icemaskobs", "divfluxobs")}
+    D = K.divflux(d["u"], d["v"], d["thk"], 100.0, "upwind")
+    ny, nx = D.shape
+    w = [0.2, 0.5, 0.3]
+    mask = d["thk"].clone()
+    mask[:, :5] = 0.0
+    top_u = torch.rand((ny, nx), dtype=torch.float64, device="cuda")
+    dU = torch.full((3, ny, nx), 7.0, dtype=torch.float64, device="cuda")
+    dV = torch.full((3, ny, nx), 7.0, dtype=torch.float64, device="cuda")
+    dU[2], dV[2] = top_u, top_u
+    gt = torch.zeros_like(D)
+    K.assim_divflux_cost_grad("obs", d["u"], d["v"], d["thk"], D, 100.0, d["icemaskobs"], gt, dU, dV, w,
+                              divfluxobs=d["divfluxobs"], std=0.7, regu=3.0, mask_thk=mask)
+    ref_u = torch.as_tensor(g["f64_upwind_obs_g_u"], device="cuda") * (mask > 0)
+    ref_v = torch.as_tensor(g["f64_upwind_obs_g_v"], device="cuda") * (mask > 0)
+    for k in range(3):
+        extra = top_u if k == 2 else 0.0
+        torch.testing.assert_close(dU[k], w[k] * ref_u + extra, rtol=1e-9, atol=1e-12)
+        torch.testing.assert_close(dV[k], w[k] * ref_v + extra, rtol=1e-9, atol=1e-12)

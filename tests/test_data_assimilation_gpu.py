@@ -94,11 +94,11 @@ def oracle_setup(cfg, st):
     return v[0::2], v[1::2], obs, p, ctl, opt, fields
 
 
-def oracle_step(cfg, st, thk, setup, i):
+def oracle_step(cfg, st, thk, setup, i, divflux_cost=None):
     ws, bs, obs, p, ctl, opt, fields = setup
     return O.da_optimize_update(thk, fields["usurf"], fields["arrhenius"], fields["slidingco"], float(st.dx), ws, bs,
-                                NZ, O.define_vertical_weight(NZ, 4.0), obs, p, ctl, opt, i, bf16=True,
-                                out_scale=OUT, input_scales=SCALES)
+                                NZ, torch.as_tensor(O.define_vertical_weight(NZ, 4.0)), obs, p, ctl, opt, i,
+                                bf16=True, out_scale=OUT, input_scales=SCALES, divflux_cost=divflux_cost)
 
 
 @pytest.mark.parametrize("aniso,to_regularize", [(0.2, "topg"), (1.0, "thk")])
@@ -173,3 +173,47 @@ def test_twin_experiment_process_api(tmp_path, monkeypatch):
     ro = O.da_rms_std(st.thk.cpu(), st.thkobs.cpu(), st.uvelsurf.cpu(), st.vvelsurf.cpu(), st.uvelsurfobs.cpu(),
                       st.vvelsurfobs.cpu(), st.icemaskobs.cpu(), 100.0)
     np.testing.assert_allclose(rms[-1, [0, 1, 8]], [ro["rmsthk"], ro["stdthk"], ro["vol"]], rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("kind,method,zero_sum", [("divfluxobs", "upwind", False), ("divfluxobs", "centered", True),
+                                                  ("divfluxfcz", "upwind", True)])
+def test_divflux_costs_in_the_loop_match_oracle(tmp_path, monkeypatch, kind, method, zero_sum):
+    """The default costs plus a flux-divergence term (its gradient reaches
+    every emulator level through velbar): three iterations against the
+    oracle's loop, as test_first_iterations_match_oracle."""
+    monkeypatch.chdir(tmp_path)
+    cfg = make_cfg(2)
+    da = cfg.processes.data_assimilation
+    da.cost_list = list(da.cost_list) + [kind]
+    da.divflux.method, da.divflux.force_zero_sum = method, zero_sum
+    da.fitting.divfluxobs_std, da.regularization.divflux = 2.0, 1.0
+    g = twin_glacier()
+    st = twin_state(cfg, g)
+    rng = np.random.default_rng(4)
+    dobs = rng.normal(0, 3, g["thk"].shape).astype(np.float32)
+    dobs[rng.random(dobs.shape) < 0.3] = np.nan
+    st.divfluxobs = torch.as_tensor(dobs, device="cuda")
+    setup = oracle_setup(cfg, st)
+    dc = {"kind": "obs" if kind == "divfluxobs" else "fcz", "method": method, "std": 2.0, "regu": 1.0,
+          "force_zero_sum": zero_sum, "divfluxobs": torch.as_tensor(dobs)}
+    DA.optimize_initialize(cfg, st)
+    thk_o = st.thk.detach().cpu().clone()
+    a = st._igm_assim
+    for i in range(3):
+        cost = {}
+        thk_prev = thk_o.numpy().copy()
+        DA.optimize_update(cfg, st, cost, i)
+        thk_o, cost_o, aux = oracle_step(cfg, st, thk_o, setup, i, divflux_cost=dc)
+        assert "divflux" in cost
+        np.testing.assert_allclose(float(cost["divflux"].item()), float(cost_o["divflux"]), rtol=2e-2,
+                                   atol=1e-6)
+        assert rel_l2(a.grad.view(a.ny, a.nx).cpu().numpy(), aux["gradient"].numpy()) < 5e-2
+        d_ours = st.thk.cpu().numpy() - thk_prev
+        d_ref = thk_o.numpy() - thk_prev
+        agree = np.abs(d_ours - d_ref) <= 0.05 * np.abs(d_ref) + 1e-3
+        assert agree.mean() >= 0.97, (i, agree.mean())
+        np.testing.assert_allclose(st.divflux.cpu().numpy(),
+                                   O.compute_divflux(aux["ubar"], aux["vbar"], st.thk.cpu(), float(st.dx),
+                                                     method).numpy(),
+                                   rtol=2e-2, atol=2e-2 * float(aux["divflux"].abs().max()))
+        thk_o = st.thk.detach().cpu().clone()

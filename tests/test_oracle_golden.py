@@ -219,3 +219,44 @@ def test_divflux_upwind_conserves_mass():
     u = T(np.full((ny, nx), 7.0)); v = T(np.full((ny, nx), -3.0))
     d = O.divflux_upwind(u, v, h, 50.0)
     assert abs(float(d.sum())) < 1e-9 * float(h.sum())
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+def test_compute_divflux_both_methods(golden, tag):
+    """compute_divflux of the reference source, upwind and centered."""
+    g = golden("divflux")
+    u, v, h = (torch.as_tensor(g[f"{tag}_{k}"]) for k in ("u", "v", "thk"))
+    for m in ("upwind", "centered"):
+        out = O.compute_divflux(u, v, h, float(g[f"{tag}_dx"]), m).numpy()
+        np.testing.assert_array_equal(out, g[f"{tag}_div_{m}"])
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("method", ["upwind", "centered"])
+@pytest.mark.parametrize("kind", ["obs", "obs_zs", "fcz", "fcz_zs"])
+def test_divflux_cost_terms(golden, tag, method, kind):
+    """cost_divfluxobs / cost_divfluxfcz of the reference source, with their
+    gradients w.r.t. ubar, vbar, thk; the fcz regression of the oracle against
+    scipy's (run by the reference)."""
+    g = golden("divflux")
+    key = f"{tag}_{method}_{kind}"
+    t = {k: torch.as_tensor(g[f"{tag}_{k}"]) for k in ("u", "v", "thk", "usurf", "icemaskobs", "divfluxobs")}
+    u, v, h = (t[k].clone().requires_grad_(True) for k in ("u", "v", "thk"))
+    dx = float(g[f"{tag}_dx"])
+    kw = dict(std=0.7, regu=3.0, force_zero_sum=kind.endswith("_zs"), method=method)
+    if kind.startswith("fcz"):
+        act = t["icemaskobs"] > 0.5
+        D = O.compute_divflux(t["u"], t["v"], t["thk"], dx, method)
+        slope, intercept = O.linregress(t["usurf"][act].numpy(), D[act].numpy())
+        tol_r = 1e-9 if tag == "f64" else 1e-4
+        np.testing.assert_allclose([slope, intercept], [g[f"{key}_slope"], g[f"{key}_intercept"]], rtol=tol_r)
+        c = O.da_cost_divflux("fcz", u, v, h, dx, t["icemaskobs"], usurf=t["usurf"],
+                              slope=float(g[f"{key}_slope"]), intercept=float(g[f"{key}_intercept"]), **kw)
+    else:
+        c = O.da_cost_divflux("obs", u, v, h, dx, t["icemaskobs"], divfluxobs=t["divfluxobs"], **kw)
+    gu, gv, gh = torch.autograd.grad(c, [u, v, h])
+    tol = 1e-12 if tag == "f64" else 2e-5
+    np.testing.assert_allclose(float(c), float(g[f"{key}_cost"]), rtol=tol)
+    for a, k in [(gu, "g_u"), (gv, "g_v"), (gh, "g_h")]:
+        ref = g[f"{key}_{k}"]
+        np.testing.assert_allclose(a.numpy(), ref, rtol=tol, atol=tol * np.abs(ref).max())
