@@ -62,7 +62,15 @@ class AssimParams(C.Structure):
     _fields_ = [("velsurfobs_std", C.c_double), ("velsurfobs_thr", C.c_double), ("thkobs_std", C.c_double),
                 ("regu_thk", C.c_double), ("gamma", C.c_double), ("aniso_factor", C.c_double), ("n_vel", C.c_double),
                 ("n_thk", C.c_double), ("penalty", C.c_int32), ("icemask_cost", C.c_int32),
-                ("regularize_thk", C.c_int32), ("mask_velsurf", C.c_int32)]
+                ("regularize_thk", C.c_int32), ("mask_velsurf", C.c_int32), ("usurfobs_std", C.c_double),
+                ("n_usurf", C.c_double), ("usurf_cost", C.c_int32), ("no_thk_control", C.c_int32)]
+
+
+class AssimControlParams(C.Structure):
+    """igm_assim_control_params."""
+    _fields_ = [("mode", C.c_int32), ("transform", C.c_int32), ("mask", C.c_int32), ("reproject", C.c_int32),
+                ("reproject_mask", C.c_int32), ("reserved", C.c_int32), ("scale", C.c_double),
+                ("lower", C.c_double)]
 
 
 class EarlyStop(C.Structure):
@@ -119,10 +127,11 @@ SIGNATURES = {
     "igm_cnn_head_backward_tc": (I, [I, I, I, I, P, P, P, P, C.c_float, C.c_float, P, P, P, I, P]),
     "igm_cnn_head_wgrad_finish": (I, [P, I, I, P, P]),
     "igm_cnn_input_gradient": (I, [I, I, I, I, I, P, P, P, P, P]),
-    "igm_assim_cost_grad": (I, [I, I, I, D] + [P] * 12 + [P, P, P, P, I, P, P]),
+    "igm_assim_cost_grad": (I, [I, I, I, D] + [P] * 12 + [P, P, P, P, P, P, I, P, P]),
+    "igm_assim_field_regu": (I, [I, I, I, D, P, P, P, D, D, I, D, P, P, I, P, P]),
     "igm_assim_flow_direction": (I, [I, I, I, P, P, P, P, P, P]),
     "igm_divflux_upwind": (I, [I, I, I, D, P, P, P, P, P]),
-    "igm_assim_control": (I, [I, I, C.c_size_t, D, I, I, P, P, P, P, P, P, P, P, P]),
+    "igm_assim_control": (I, [I, C.c_size_t, P, P, P, P, P, P, P, P, P, P]),
     "igm_assim_stats": (I, [I, I, I, D] + [P] * 11 + [P, I, P, P]),
     "igm_divflux": (I, [I, I, I, I, D, P, P, P, P, P]),
     "igm_assim_divflux_cost_grad": (I, [I, I, I, D, I, P] + [P] * 8 + [P, P, P, P, P, P, I, P, P]),

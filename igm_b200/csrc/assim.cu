@@ -7,7 +7,7 @@
 namespace igm {
 
 // cost indices of igm_assim_cost_grad
-enum { kCVel = 0, kCThk = 1, kCIce = 2, kCPos = 3, kCReg = 4, kNCost = 5 };
+enum { kCVel = 0, kCThk = 1, kCIce = 2, kCPos = 3, kCReg = 4, kCUs = 5, kNCost = 6 };
 
 template <typename T>
 struct AssimArgs {
@@ -24,17 +24,21 @@ struct AssimArgs {
   const T* icemaskobs;
   const T* fdx;   // flow directions [ny-1][nx-1] (anisotropic branch)
   const T* fdy;
+  const T* usobs;  // usurfobs (misfit_usurf) or NULL
   igm_assim_params p;
-  T* g_thk;  // dC/dthk
+  T* g_thk;  // dC/dthk (field-only mode: dC/dfield)
   T* g_u;    // dC/duvs
   T* g_v;
+  T* g_us;   // dC/dusurf or NULL
+  int field_only;  // the regularisation and positivity penalty of one field (thk holds it)
+  T pos_thr;       // field-only: the penalty applies below this value
   double* partials;  // [gridDim.x][kNCost]
 };
 
 // Scale factors of the cost sums and the gradients (host-computed once per
 // call): the kernel accumulates unscaled sums, the final reduction scales.
 struct AssimScales {
-  double c_vel, c_thk, c_pen, c_reg;  // cost = scale * sum
+  double c_vel, c_thk, c_pen, c_reg, c_us;  // cost = scale * sum
   double gamma;                       // convexity weight
 };
 
@@ -49,7 +53,7 @@ constexpr int kAmWarps = 4;
 
 template <typename T>
 struct AssimRow {
-  T th, us;               // thk, usurf (this lane's column)
+  T th, us, uso;          // thk (field-only mode: the field), usurf, usurfobs (this lane's column)
   T uo, vo, uv, vv;       // observed / emulated surface velocities
   T to, de, im;           // thkobs, density weight, icemaskobs
   T fx, fy;               // flow direction of cell (j, c)
@@ -67,6 +71,10 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
   const bool out = lane >= 1 && lane <= kAmCols && col;
   const bool aniso = p.aniso_factor != 1.0;
   const bool reg_thk = p.regularize_thk != 0;
+  const bool fo = a.field_only != 0;
+  const bool us_cost = !fo && p.usurf_cost != 0;
+  const bool thk_ctl = p.no_thk_control == 0;
+  const T kus = (T)(1.0 / (p.usurfobs_std * p.usurfobs_std * (p.n_usurf > 0 ? p.n_usurf : 1.0)));
   const T rdx = T(1) / a.dx, hr = T(0.5) * rdx;
   const T w = (T)p.regu_thk;
   const T s_a = (T)(1.0 / sqrt(p.aniso_factor)), s_b = (T)sqrt(p.aniso_factor);
@@ -80,8 +88,9 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
     const bool ok = col && j < ny;
     const size_t o = (size_t)j * nx + cc;
     r.th = ok ? a.thk[o] : T(0);
-    r.us = (ok && !reg_thk) ? a.usurf[o] : T(0);
-    const bool okn = ok && full;
+    r.us = (ok && !fo && (!reg_thk || us_cost)) ? a.usurf[o] : T(0);
+    const bool okn = ok && full && !fo;
+    r.uso = (okn && us_cost) ? a.usobs[o] : T(0);
     r.uo = okn ? a.uobs[o] : T(0);
     r.vo = okn ? a.vobs[o] : T(0);
     r.uv = okn ? a.uvs[o] : T(0);
@@ -95,7 +104,7 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
     r.fy = okc ? a.fdy[q] : T(0);
     return r;
   };
-  auto field = [&](const AssimRow<T>& r) { return reg_thk ? r.th : r.us - r.th; };
+  auto field = [&](const AssimRow<T>& r) { return (reg_thk || fo) ? r.th : r.us - r.th; };
   // cell (j, c) from the fields of rows j (f0 this lane, f0r the next lane) and j + 1
   // -> P = gdx + gdy, M = gdx - gdy and its cost; the isotropic branch: the forward
   // differences of this node
@@ -144,7 +153,19 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
       const T dxm = __shfl_up_sync(0xffffffffu, k.dxp, 1);
       gf = w * rdx * ((dxm - k.dxp) + (prev.dyp - k.dyp));
     }
-    if (out) {
+    if (out && fo) {
+      // one control field (regu_slidingco.py:8-52, regu_arrhenius.py:5-24, total_cost.py:45-54):
+      // its regularisation and positivity penalty
+      const size_t o = (size_t)j * nx + cc;
+      const T f = cur.th;
+      T g = gf;
+      if (p.penalty && !(f >= a.pos_thr)) {
+        acc[kCPos] += (double)(f * f);
+        g += kp * f;
+      }
+      acc[kCReg] += aniso ? (double)k.cost : 0.5 * ((double)k.dxp * k.dxp + (double)k.dyp * k.dyp);
+      a.g_thk[o] = g;
+    } else if (out) {
       const size_t o = (size_t)j * nx + cc;
       const T th = cur.th;
       // surface-velocity misfit (misfit_velsurf.py:8-19)
@@ -180,7 +201,7 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
           acc[kCIce] += (double)(th * th);
           g += kp * th;
         }
-        if (!(th >= T(0))) {
+        if (thk_ctl && !(th >= T(0))) {
           acc[kCPos] += (double)(th * th);
           g += kp * th;
         }
@@ -188,9 +209,24 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
       // regularisation (regu_thk.py:8-70): smoothness cost of cell (j, c) or of this node's
       // forward differences, the convexity term
       const double rc = aniso ? (double)k.cost : 0.5 * ((double)k.dxp * k.dxp + (double)k.dyp * k.dyp);
-      acc[kCReg] += rc - sc.gamma * (double)th;
-      g += (reg_thk ? gf : -gf) - kg;
+      if (thk_ctl) {
+        acc[kCReg] += rc - sc.gamma * (double)th;
+        g += (reg_thk ? gf : -gf) - kg;
+      }
       a.g_thk[o] = g;
+      if (a.g_us) {
+        // dC/dusurf: misfit_usurf (misfit_usurf.py:5-15) and the bed usurf - thk of regu_thk
+        T gs = (reg_thk || !thk_ctl) ? T(0) : gf;
+        if (us_cost && cur.im > T(0.5)) {
+          const T d = cur.us - cur.uso;
+          acc[kCUs] += (double)(d * d);
+          gs += d * kus;
+        }
+        a.g_us[o] = gs;
+      } else if (us_cost && cur.im > T(0.5)) {
+        const T d = cur.us - cur.uso;
+        acc[kCUs] += (double)(d * d);
+      }
     }
     prev = k;
     cur = nxt;
@@ -202,7 +238,7 @@ template <typename T>
 __global__ void __launch_bounds__(kAmWarps * 32) assim_cost_grad_kernel(const AssimArgs<T> a, const AssimScales sc,
                                                                        int n_strips, int rows, int n_tasks) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double acc[kNCost] = {0, 0, 0, 0, 0};
+  double acc[kNCost] = {0, 0, 0, 0, 0, 0};
   for (int t = blockIdx.x * kAmWarps + warp; t < n_tasks; t += gridDim.x * kAmWarps) {
     const int strip = t % n_strips, seg = t / n_strips;
     const int y0 = seg * rows, y1 = min(y0 + rows, a.ny);
@@ -231,7 +267,8 @@ __global__ void assim_sum_kernel(const double* partials, int n_parts, AssimScale
   double v = 0.0;
   for (int b = lane; b < n_parts; b += 32) v += partials[(size_t)b * kNCost + c];
   for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
-  const double f = c == kCVel ? sc.c_vel : c == kCThk ? sc.c_thk : c == kCReg ? sc.c_reg : sc.c_pen;
+  const double f = c == kCVel ? sc.c_vel : c == kCThk ? sc.c_thk : c == kCReg ? sc.c_reg : c == kCUs ? sc.c_us
+                                                                                                   : sc.c_pen;
   if (lane == 0) costs[c] = f * v;
 }
 
@@ -311,27 +348,10 @@ static int grid_n(size_t n) {
 }
 
 template <typename T>
-static int cost_grad_t(int ny, int nx, double dx, const void* thk, const void* usurf, const void* uvs,
-                       const void* vvs, const void* uobs, const void* vobs, const void* thkobs, const void* dens,
-                       const void* icemaskobs, const void* fdx, const void* fdy, const igm_assim_params* p,
-                       void* g_thk, void* g_u, void* g_v, double* partials, int n_parts, double* costs,
-                       cudaStream_t st) {
-  AssimArgs<T> a{};
-  a.ny = ny; a.nx = nx; a.dx = (T)dx;
-  a.thk = (const T*)thk; a.usurf = (const T*)usurf; a.uvs = (const T*)uvs; a.vvs = (const T*)vvs;
-  a.uobs = (const T*)uobs; a.vobs = (const T*)vobs; a.thkobs = (const T*)thkobs; a.dens = (const T*)dens;
-  a.icemaskobs = (const T*)icemaskobs; a.fdx = (const T*)fdx; a.fdy = (const T*)fdy;
-  a.p = *p;
-  a.g_thk = (T*)g_thk; a.g_u = (T*)g_u; a.g_v = (T*)g_v;
-  a.partials = partials;
-  AssimScales sc{};
-  sc.c_vel = 0.5 / (p->velsurfobs_std * p->velsurfobs_std * p->n_vel);
-  sc.c_thk = 0.5 / (p->thkobs_std * p->thkobs_std * p->n_thk);
-  sc.c_pen = 1e10 / ((double)ny * nx);
-  sc.c_reg = p->regu_thk;
-  sc.gamma = p->gamma;
+static int march_launch(AssimArgs<T>& a, const AssimScales& sc, int n_parts, double* costs, cudaStream_t st) {
   // segments of rows sized for about 32 resident warps per SM, at least 8 rows; the
   // warps stride over the (strip, segment) tasks so the grid fits the partials
+  const int ny = a.ny, nx = a.nx;
   const int n_strips = (nx + kAmCols - 1) / kAmCols;
   const long long target = 148LL * 32;
   int rows = (int)((n_strips * (long long)ny + target - 1) / target);
@@ -342,8 +362,54 @@ static int cost_grad_t(int ny, int nx, double dx, const void* thk, const void* u
   assim_cost_grad_kernel<T><<<(int)grid, kAmWarps * 32, 0, st>>>(a, sc, n_strips, rows, (int)tasks);
   int rc = launch_status("assim_cost_grad_kernel");
   if (rc) return rc;
-  assim_sum_kernel<<<1, 32 * kNCost, 0, st>>>(partials, (int)grid, sc, costs);
+  assim_sum_kernel<<<1, 32 * kNCost, 0, st>>>(a.partials, (int)grid, sc, costs);
   return launch_status("assim_sum_kernel");
+}
+
+template <typename T>
+static int cost_grad_t(int ny, int nx, double dx, const void* thk, const void* usurf, const void* uvs,
+                       const void* vvs, const void* uobs, const void* vobs, const void* thkobs, const void* dens,
+                       const void* icemaskobs, const void* fdx, const void* fdy, const void* usobs,
+                       const igm_assim_params* p, void* g_thk, void* g_u, void* g_v, void* g_us, double* partials,
+                       int n_parts, double* costs, cudaStream_t st) {
+  AssimArgs<T> a{};
+  a.ny = ny; a.nx = nx; a.dx = (T)dx;
+  a.thk = (const T*)thk; a.usurf = (const T*)usurf; a.uvs = (const T*)uvs; a.vvs = (const T*)vvs;
+  a.uobs = (const T*)uobs; a.vobs = (const T*)vobs; a.thkobs = (const T*)thkobs; a.dens = (const T*)dens;
+  a.icemaskobs = (const T*)icemaskobs; a.fdx = (const T*)fdx; a.fdy = (const T*)fdy; a.usobs = (const T*)usobs;
+  a.p = *p;
+  a.g_thk = (T*)g_thk; a.g_u = (T*)g_u; a.g_v = (T*)g_v; a.g_us = (T*)g_us;
+  a.partials = partials;
+  AssimScales sc{};
+  sc.c_vel = 0.5 / (p->velsurfobs_std * p->velsurfobs_std * p->n_vel);
+  sc.c_thk = 0.5 / (p->thkobs_std * p->thkobs_std * p->n_thk);
+  sc.c_pen = 1e10 / ((double)ny * nx);
+  sc.c_reg = p->regu_thk;
+  sc.c_us = p->usurf_cost ? 0.5 / (p->usurfobs_std * p->usurfobs_std * (p->n_usurf > 0 ? p->n_usurf : 1.0)) : 0.0;
+  sc.gamma = p->gamma;
+  return march_launch<T>(a, sc, n_parts, costs, st);
+}
+
+template <typename T>
+static int field_regu_t(int ny, int nx, double dx, const void* field, const void* fdx, const void* fdy, double regu,
+                        double aniso, int penalty, double pos_thr, void* grad, double* partials, int n_parts,
+                        double* costs, cudaStream_t st) {
+  AssimArgs<T> a{};
+  a.ny = ny; a.nx = nx; a.dx = (T)dx;
+  a.thk = (const T*)field; a.fdx = (const T*)fdx; a.fdy = (const T*)fdy;
+  a.p.regu_thk = regu;
+  a.p.aniso_factor = aniso;
+  a.p.penalty = penalty;
+  a.p.velsurfobs_std = a.p.thkobs_std = a.p.usurfobs_std = 1.0;
+  a.p.n_vel = a.p.n_thk = a.p.n_usurf = 1.0;
+  a.field_only = 1;
+  a.pos_thr = (T)pos_thr;
+  a.g_thk = (T*)grad;
+  a.partials = partials;
+  AssimScales sc{};
+  sc.c_pen = 1e10 / ((double)ny * nx);
+  sc.c_reg = regu;
+  return march_launch<T>(a, sc, n_parts, costs, st);
 }
 
 template <typename T>
@@ -360,35 +426,39 @@ static int flow_t(int ny, int nx, const void* u, const void* v, void* fx, void* 
   return launch_status("flow_direction_kernel");
 }
 
-// Control update of optimize_update (optimize/update.py:23-27, 38-42,
-// 56-68, 77-98) for control thk with scaling sc, at the three points where
-// the reference touches the control:
-//   mode 0, before the forward: the optimizer's variable thk / sc, then
-//     thk = variable * sc, and zero moments (the reference wraps the control
-//     in a new tf.Variable at every iteration, so Adam's slots are new);
-//   mode 1, the gradient: sc (dC/dthk direct + through the emulator) where
-//     icemaskobs > 0.5, zero elsewhere;
-//   mode 2, after the step: thk = variable * sc, then the reprojection onto
-//     the ice mask and thk >= 0.
+// Control update of optimize_update (optimize/update.py:22-42, 56-98) for one
+// control x with scaling sc (see igm_assim_control): mode 0 before the
+// forward (the variable, x from it, zero moments), mode 1 the gradient of the
+// variable with the control's mask, mode 2 x from the variable and the
+// reprojection.
 template <typename T>
-__global__ void assim_control_kernel(size_t n, int mode, T sc, int reproject_mask, int reproject_pos, T* thk,
-                                     const T* g_direct, const float* g_emul, const T* icemaskobs, float* var,
-                                     float* grad, float* m, float* v) {
+__global__ void assim_control_kernel(size_t n, igm_assim_control_params p, const T* g_direct, const float* g_emul,
+                                     const T* icemaskobs, T* x, float* var, float* grad, float* m, float* v) {
+  const T sc = (T)p.scale;
   for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
-    if (mode == 0) {
-      const float x = (float)(thk[o] / sc);
-      var[o] = x;
-      thk[o] = (T)x * sc;
+    if (p.mode == 0) {
+      const float w = p.transform ? (float)sqrt(x[o] / sc) : (float)(x[o] / sc);
+      var[o] = w;
+      x[o] = p.transform ? ((T)w * (T)w) * sc : (T)w * sc;
       m[o] = 0.f;
       v[o] = 0.f;
-    } else if (mode == 1) {
+    } else if (p.mode == 1) {
+      bool on = true;
+      if (p.mask == 1) on = icemaskobs[o] > T(0.5);
+      if (p.mask == 2) on = icemaskobs[o] == T(1);
       const T g = g_direct[o] + (g_emul ? (T)g_emul[o] : T(0));
-      grad[o] = icemaskobs[o] > T(0.5) ? (float)(g * sc) : 0.f;
+      const T dxdw = p.transform ? T(2) * (T)var[o] * sc : sc;
+      grad[o] = on ? (float)(g * dxdw) : 0.f;
     } else {
-      T t = (T)var[o] * sc;
-      if (reproject_mask && !(icemaskobs[o] > T(0.5))) t = T(0);
-      if (reproject_pos && t < T(0)) t = T(0);
-      thk[o] = t;
+      const T w = (T)var[o];
+      T t = p.transform ? (w * w) * sc : w * sc;
+      if (p.reproject == 1) {
+        if (p.reproject_mask && !(icemaskobs[o] > T(0.5))) t = T(0);
+        if (t < T(0)) t = T(0);
+      } else if (p.reproject == 2) {
+        if (t < (T)p.lower) t = (T)p.lower;
+      }
+      x[o] = t;
     }
   }
 }
@@ -693,26 +763,49 @@ extern "C" int igm_assim_cost_grad(int dtype, int ny, int nx, double dx, const v
                                    const void* uvelsurf, const void* vvelsurf, const void* uvelsurfobs,
                                    const void* vvelsurfobs, const void* thkobs, const void* dens_thkobs,
                                    const void* icemaskobs, const void* flowdirx, const void* flowdiry,
-                                   const igm_assim_params* params, void* grad_thk, void* grad_uvelsurf,
-                                   void* grad_vvelsurf, double* partials, int n_parts, double* costs, void* stream) {
+                                   const void* usurfobs, const igm_assim_params* params, void* grad_thk,
+                                   void* grad_uvelsurf, void* grad_vvelsurf, void* grad_usurf, double* partials,
+                                   int n_parts, double* costs, void* stream) {
   IGM_CHECK_ARG(ny >= 2 && nx >= 2, IGM_ERR_BAD_SHAPE, "igm_assim_cost_grad: bad shape %dx%d", ny, nx);
   IGM_CHECK_ARG(thk && usurf && uvelsurf && vvelsurf && uvelsurfobs && vvelsurfobs && thkobs && dens_thkobs &&
                     icemaskobs && params && grad_thk && grad_uvelsurf && grad_vvelsurf && partials && costs,
                 IGM_ERR_BAD_ARGUMENT, "igm_assim_cost_grad: NULL argument");
   IGM_CHECK_ARG(params->aniso_factor == 1.0 || (flowdirx && flowdiry), IGM_ERR_BAD_ARGUMENT,
                 "igm_assim_cost_grad: the anisotropic regularisation needs flowdirx, flowdiry");
+  IGM_CHECK_ARG(!params->usurf_cost || (usurfobs && params->usurfobs_std > 0), IGM_ERR_BAD_ARGUMENT,
+                "igm_assim_cost_grad: misfit_usurf needs usurfobs and usurfobs_std > 0");
   IGM_CHECK_ARG(params->aniso_factor > 0 && params->n_vel >= 1 && params->n_thk >= 1 && n_parts >= 1 && dx > 0,
                 IGM_ERR_BAD_ARGUMENT, "igm_assim_cost_grad: bad parameter");
   cudaStream_t st = as_stream(stream);
   if (dtype == IGM_F32)
     return cost_grad_t<float>(ny, nx, dx, thk, usurf, uvelsurf, vvelsurf, uvelsurfobs, vvelsurfobs, thkobs,
-                              dens_thkobs, icemaskobs, flowdirx, flowdiry, params, grad_thk, grad_uvelsurf,
-                              grad_vvelsurf, partials, n_parts, costs, st);
+                              dens_thkobs, icemaskobs, flowdirx, flowdiry, usurfobs, params, grad_thk,
+                              grad_uvelsurf, grad_vvelsurf, grad_usurf, partials, n_parts, costs, st);
   if (dtype == IGM_F64)
     return cost_grad_t<double>(ny, nx, dx, thk, usurf, uvelsurf, vvelsurf, uvelsurfobs, vvelsurfobs, thkobs,
-                               dens_thkobs, icemaskobs, flowdirx, flowdiry, params, grad_thk, grad_uvelsurf,
-                               grad_vvelsurf, partials, n_parts, costs, st);
+                               dens_thkobs, icemaskobs, flowdirx, flowdiry, usurfobs, params, grad_thk,
+                               grad_uvelsurf, grad_vvelsurf, grad_usurf, partials, n_parts, costs, st);
   set_error("igm_assim_cost_grad: unknown dtype %d", dtype);
+  return IGM_ERR_BAD_ARGUMENT;
+}
+
+extern "C" int igm_assim_field_regu(int dtype, int ny, int nx, double dx, const void* field, const void* flowdirx,
+                                    const void* flowdiry, double regu, double aniso_factor, int penalty,
+                                    double penalty_threshold, void* grad, double* partials, int n_parts,
+                                    double* costs, void* stream) {
+  IGM_CHECK_ARG(ny >= 2 && nx >= 2 && dx > 0, IGM_ERR_BAD_SHAPE, "igm_assim_field_regu: bad shape %dx%d", ny, nx);
+  IGM_CHECK_ARG(field && grad && partials && costs && n_parts >= 1 && aniso_factor > 0, IGM_ERR_BAD_ARGUMENT,
+                "igm_assim_field_regu: bad argument");
+  IGM_CHECK_ARG(aniso_factor == 1.0 || (flowdirx && flowdiry), IGM_ERR_BAD_ARGUMENT,
+                "igm_assim_field_regu: the anisotropic regularisation needs flowdirx, flowdiry");
+  cudaStream_t st = as_stream(stream);
+  if (dtype == IGM_F32)
+    return field_regu_t<float>(ny, nx, dx, field, flowdirx, flowdiry, regu, aniso_factor, penalty, penalty_threshold,
+                               grad, partials, n_parts, costs, st);
+  if (dtype == IGM_F64)
+    return field_regu_t<double>(ny, nx, dx, field, flowdirx, flowdiry, regu, aniso_factor, penalty,
+                                penalty_threshold, grad, partials, n_parts, costs, st);
+  set_error("igm_assim_field_regu: unknown dtype %d", dtype);
   return IGM_ERR_BAD_ARGUMENT;
 }
 
@@ -728,25 +821,25 @@ extern "C" int igm_assim_flow_direction(int dtype, int ny, int nx, const void* u
   return IGM_ERR_BAD_ARGUMENT;
 }
 
-extern "C" int igm_assim_control(int dtype, int mode, size_t n, double scale, int reproject_mask, int reproject_pos,
-                                 void* thk, const void* grad_direct, const float* grad_emulator, const void* icemaskobs,
+extern "C" int igm_assim_control(int dtype, size_t n, const igm_assim_control_params* params, void* x,
+                                 const void* grad_direct, const float* grad_emulator, const void* icemaskobs,
                                  float* variable, float* grad, float* m, float* v, void* stream) {
-  IGM_CHECK_ARG(mode >= 0 && mode <= 2 && n >= 1 && scale > 0, IGM_ERR_BAD_ARGUMENT,
-                "igm_assim_control: bad mode, size or scale");
-  IGM_CHECK_ARG(thk && (mode != 0 || (variable && m && v)) && (mode != 1 || (grad_direct && icemaskobs && grad)) &&
-                    (mode != 2 || (variable && (icemaskobs || !reproject_mask))),
+  IGM_CHECK_ARG(params && n >= 1 && params->scale > 0 && params->mode >= 0 && params->mode <= 2,
+                IGM_ERR_BAD_ARGUMENT, "igm_assim_control: bad mode, size or scale");
+  const igm_assim_control_params& p = *params;
+  IGM_CHECK_ARG(x && variable && (p.mode != 0 || (m && v)) && (p.mode != 1 || (grad_direct && grad)) &&
+                    ((p.mode == 1 && p.mask != 0) || (p.mode == 2 && p.reproject == 1 && p.reproject_mask)
+                         ? icemaskobs != nullptr
+                         : true),
                 IGM_ERR_BAD_ARGUMENT, "igm_assim_control: NULL argument");
   cudaStream_t st = as_stream(stream);
   if (dtype == IGM_F32)
-    assim_control_kernel<float><<<grid_n(n), 256, 0, st>>>(n, mode, (float)scale, reproject_mask, reproject_pos,
-                                                           (float*)thk, (const float*)grad_direct,
-                                                           grad_emulator, (const float*)icemaskobs,
-                                                           variable, grad, m, v);
+    assim_control_kernel<float><<<grid_n(n), 256, 0, st>>>(n, p, (const float*)grad_direct, grad_emulator,
+                                                           (const float*)icemaskobs, (float*)x, variable, grad, m, v);
   else if (dtype == IGM_F64)
-    assim_control_kernel<double><<<grid_n(n), 256, 0, st>>>(n, mode, scale, reproject_mask, reproject_pos,
-                                                            (double*)thk, (const double*)grad_direct,
-                                                            grad_emulator, (const double*)icemaskobs,
-                                                            variable, grad, m, v);
+    assim_control_kernel<double><<<grid_n(n), 256, 0, st>>>(n, p, (const double*)grad_direct, grad_emulator,
+                                                            (const double*)icemaskobs, (double*)x, variable, grad, m,
+                                                            v);
   else {
     set_error("igm_assim_control: unknown dtype %d", dtype);
     return IGM_ERR_BAD_ARGUMENT;

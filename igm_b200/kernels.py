@@ -158,32 +158,52 @@ def absmax2(a, b, out=None):
 
 
 def assim_cost_grad(thk, usurf, uvs, vvs, uobs, vobs, thkobs, dens, icemaskobs, flowdir, dx, params,
-                    partials=None, costs=None, g_thk=None, g_u=None, g_v=None):
-    """Cost terms (device double[5]: velsurf, thk, icemask, thk_positive,
-    thk_regu) and gradients (dC/dthk, dC/duvelsurf, dC/dvvelsurf) of the
-    default data-assimilation configuration (igm_assim_cost_grad); ``params``
-    an _lib.AssimParams, ``flowdir`` (fx, fy) [ny-1, nx-1] or None.  The
-    outputs may be given (contiguous [ny, nx] views, e.g. the top layer of a
-    [nz, ny, nx] velocity gradient)."""
+                    partials=None, costs=None, g_thk=None, g_u=None, g_v=None, usurfobs=None, g_us=None):
+    """Cost terms (device double[6]: velsurf, thk, icemask, thk_positive,
+    thk_regu, usurf) and gradients (dC/dthk, dC/duvelsurf, dC/dvvelsurf, and
+    dC/dusurf into ``g_us`` when given) of the thk/usurf cost terms
+    (igm_assim_cost_grad); ``params`` an _lib.AssimParams, ``flowdir`` (fx,
+    fy) [ny-1, nx-1] or None.  The outputs may be given (contiguous [ny, nx]
+    views, e.g. the top layer of a [nz, ny, nx] velocity gradient)."""
     ny, nx = thk.shape
     n_parts = 148 * 8
     if partials is None:
-        partials = torch.empty(n_parts * 5, dtype=torch.float64, device=thk.device)
-    costs = costs if costs is not None else torch.empty(5, dtype=torch.float64, device=thk.device)
+        partials = torch.empty(n_parts * 6, dtype=torch.float64, device=thk.device)
+    costs = costs if costs is not None else torch.empty(6, dtype=torch.float64, device=thk.device)
     g_thk = g_thk if g_thk is not None else torch.empty_like(thk)
     g_u = g_u if g_u is not None else torch.empty_like(thk)
     g_v = g_v if g_v is not None else torch.empty_like(thk)
-    for t in (g_thk, g_u, g_v):
+    for t in (g_thk, g_u, g_v) + ((g_us,) if g_us is not None else ()):
         if t.shape != thk.shape or not t.is_contiguous() or t.dtype != thk.dtype:
             raise ValueError("assim_cost_grad: gradient outputs must be contiguous [ny, nx] of thk's dtype")
     fx, fy = flowdir if flowdir is not None else (None, None)
     rc = L.lib().igm_assim_cost_grad(L.dtype_code(thk.dtype), ny, nx, float(dx), L.ptr(thk), L.ptr(usurf),
                                      L.ptr(uvs), L.ptr(vvs), L.ptr(uobs), L.ptr(vobs), L.ptr(thkobs), L.ptr(dens),
-                                     L.ptr(icemaskobs), L.ptr(fx), L.ptr(fy), C.byref(params), L.ptr(g_thk),
-                                     L.ptr(g_u), L.ptr(g_v), L.ptr(partials), partials.numel() // 5, L.ptr(costs),
-                                     L.stream_ptr())
+                                     L.ptr(icemaskobs), L.ptr(fx), L.ptr(fy), L.ptr(usurfobs), C.byref(params),
+                                     L.ptr(g_thk), L.ptr(g_u), L.ptr(g_v), L.ptr(g_us), L.ptr(partials),
+                                     partials.numel() // 6, L.ptr(costs), L.stream_ptr())
     L.check(rc, "igm_assim_cost_grad")
     return costs, g_thk, g_u, g_v
+
+
+def assim_field_regu(field, dx, regu, aniso=1.0, flowdir=None, penalty=True, threshold=0.0, grad=None, costs=None,
+                     partials=None):
+    """The regularisation and positivity penalty of a slidingco / arrhenius
+    control (igm_assim_field_regu): returns (costs double[6] with [3] the
+    penalty and [4] the regularisation, dC/dfield)."""
+    ny, nx = field.shape
+    n_parts = 148 * 8
+    partials = partials if partials is not None else torch.empty(n_parts * 6, dtype=torch.float64,
+                                                                 device=field.device)
+    costs = costs if costs is not None else torch.empty(6, dtype=torch.float64, device=field.device)
+    grad = grad if grad is not None else torch.empty_like(field)
+    fx, fy = flowdir if flowdir is not None else (None, None)
+    rc = L.lib().igm_assim_field_regu(L.dtype_code(field.dtype), ny, nx, float(dx), L.ptr(field), L.ptr(fx),
+                                      L.ptr(fy), float(regu), float(aniso), int(bool(penalty)), float(threshold),
+                                      L.ptr(grad), L.ptr(partials), partials.numel() // 6, L.ptr(costs),
+                                      L.stream_ptr())
+    L.check(rc, "igm_assim_field_regu")
+    return costs, grad
 
 
 def assim_flow_direction(uvs, vvs):
@@ -197,18 +217,21 @@ def assim_flow_direction(uvs, vvs):
     return fx, fy
 
 
-def assim_control(mode, thk, scale, icemaskobs=None, variable=None, grad=None, m=None, v=None, g_direct=None,
-                  g_emul=None, reproject_mask=True, reproject_pos=True):
-    """The control update of one assimilation iteration (igm_assim_control):
-    mode 0 variable = thk / scale, thk = variable * scale, zero moments;
-    mode 1 grad = scale (g_direct + g_emul) inside the observed ice mask;
-    mode 2 thk = variable * scale with the reprojection.  variable, grad, m,
-    v, g_emul are float32."""
-    n = thk.numel()
+def assim_control(mode, x, scale, icemaskobs=None, variable=None, grad=None, m=None, v=None, g_direct=None,
+                  g_emul=None, transform=0, mask=1, reproject=1, reproject_mask=True, lower=0.0):
+    """The control update of one assimilation iteration (igm_assim_control)
+    for control x: mode 0 variable from x, x from the variable, zero moments;
+    mode 1 the variable's gradient dx/dvariable (g_direct + g_emul) with the
+    mask (0 none, 1 icemaskobs > 0.5, 2 icemaskobs == 1); mode 2 x from the
+    variable and the reprojection (0 none, 1 thk, 2 x >= lower).  transform
+    1: x = variable^2 scale.  variable, grad, m, v, g_emul are float32."""
+    n = x.numel()
     if g_emul is not None and (g_emul.dtype != torch.float32 or not g_emul.is_contiguous() or g_emul.numel() != n):
-        raise ValueError("assim_control: g_emul must be contiguous float32 of thk's size")
-    rc = L.lib().igm_assim_control(L.dtype_code(thk.dtype), int(mode), n, float(scale), int(bool(reproject_mask)),
-                                   int(bool(reproject_pos)), L.ptr(thk), L.ptr(g_direct), L.ptr(g_emul),
+        raise ValueError("assim_control: g_emul must be contiguous float32 of x's size")
+    p = L.AssimControlParams()
+    p.mode, p.transform, p.mask, p.reproject = int(mode), int(transform), int(mask), int(reproject)
+    p.reproject_mask, p.scale, p.lower = int(bool(reproject_mask)), float(scale), float(lower)
+    rc = L.lib().igm_assim_control(L.dtype_code(x.dtype), n, C.byref(p), L.ptr(x), L.ptr(g_direct), L.ptr(g_emul),
                                    L.ptr(icemaskobs), L.ptr(variable), L.ptr(grad), L.ptr(m), L.ptr(v),
                                    L.stream_ptr())
     L.check(rc, "igm_assim_control")

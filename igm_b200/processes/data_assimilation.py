@@ -12,15 +12,16 @@ the Blatter-Pattyn energy of the current geometry after every iteration
 One iteration (optimize/update.py:15-103) is a fixed sequence of device
 launches with no host synchronisation:
 
-  igm_assim_control mode 0      thk_sc = thk / sc, thk = thk_sc sc, fresh moments
+  igm_assim_control mode 0      per control: x_sc = x / sc, x = x_sc sc, fresh moments
   CNN forward (keep activations, thk mask), velsurf / velbar
   igm_assim_flow_direction      (anisotropic regularisation only)
   igm_assim_cost_grad           costs, dC/dthk, dC/d(top-layer U, V)
   igm_divflux + igm_assim_divflux_cost_grad (divfluxobs / divfluxfcz only)
+  igm_assim_field_regu          slidingco / arrhenius regularisation and penalty (those controls only)
   CNN backward, data chain only, with igm_cnn_input_gradient
-  igm_assim_control mode 1      gradient of thk_sc, zero outside the mask
-  igm_adam_clipnorm             Keras legacy Adam at iteration i + 1
-  igm_assim_control mode 2      thk = thk_sc sc, reprojection
+  igm_assim_control mode 1      per control: the gradient of x_sc with its mask
+  igm_adam_clipnorm             Keras legacy Adam at iteration i + 1, one variable per control
+  igm_assim_control mode 2      per control: x = x_sc sc, reprojection
   igm_divflux_upwind            divflux of the emulated velbar
   rms / std record              device reductions into the history tensor
 
@@ -30,7 +31,8 @@ the netCDF snapshots every ``output.freq`` iterations and the final
 ``save_result_in_ncdf`` file are host copies.  The 2-D plots of the
 reference (matplotlib) are not drawn.
 
-Supported: control_list [thk]; cost_list within velsurf, thk, icemask,
+Supported: control_list within thk, usurf, slidingco (log_slidingco or not),
+arrhenius (dim_arrhenius 2); cost_list within velsurf, thk, icemask, usurf,
 divfluxobs, divfluxfcz (the flux-divergence terms, with or without
 force_zero_sum); method ADAM; sole_mask, fix_opti_normalization_issue,
 include_low_speed_term, cook.infer_params and pertubate off; divflux.method
@@ -50,19 +52,24 @@ from .. import kernels as K
 from .. import state as S
 from . import iceflow as P
 
-_COST_KEYS = ["velsurf", "thk", "icemask", "thk_positive", "thk_regu"]  # the columns of igm_assim_cost_grad
-_ALL_KEYS = ["velsurf", "thk", "divflux", "icemask", "thk_positive", "thk_regu"]  # total_cost.py's order
+_COST_KEYS = ["velsurf", "thk", "icemask", "thk_positive", "thk_regu", "usurf"]  # igm_assim_cost_grad's columns
+# total_cost.py:13-71's order of the cost dictionary
+_ALL_KEYS = ["velsurf", "thk", "divflux", "usurf", "icemask", "thk_positive", "slidingco_positive",
+             "arrhenius_positive", "thk_regu", "slid_regu", "arrh_regu"]
+# the controls: emulator input channel (fieldin order thk, usurf, arrhenius, slidingco)
+_CHANNEL = {"thk": 0, "usurf": 1, "arrhenius": 2, "slidingco": 3}
 
 
 def _check_supported(cfg):
     da = cfg.processes.data_assimilation
     o = da.optimization
     bad = []
-    if list(da.control_list) != ["thk"]:
-        bad.append(f"control_list={list(da.control_list)} (only ['thk'])")
-    extra = [c for c in da.cost_list if c not in ("velsurf", "thk", "icemask", "divfluxobs", "divfluxfcz")]
+    ctl = list(da.control_list)
+    if not ctl or any(c not in _CHANNEL for c in ctl) or len(set(ctl)) != len(ctl):
+        bad.append(f"control_list={ctl} (thk, usurf, slidingco, arrhenius)")
+    extra = [c for c in da.cost_list if c not in ("velsurf", "thk", "icemask", "usurf", "divfluxobs", "divfluxfcz")]
     if extra:
-        bad.append(f"cost terms {extra} (only velsurf, thk, icemask, divfluxobs, divfluxfcz)")
+        bad.append(f"cost terms {extra} (only velsurf, thk, icemask, usurf, divfluxobs, divfluxfcz)")
     if o.method != "ADAM":
         bad.append(f"optimization.method={o.method!r} (only 'ADAM')")
     for key in ("sole_mask", "fix_opti_normalization_issue", "pertubate"):
@@ -118,9 +125,13 @@ class _Assim:
         self.dx = P._dx(state)
         nan = torch.full((ny, nx), float("nan"), dtype=torch.float32, device=d)
         costs = list(da.cost_list)
+        f, r, o = da.fitting, da.regularization, da.optimization
+        self.controls = list(da.control_list)
+        nc = len(self.controls)
         self.uobs = S.get(state, "uvelsurfobs").contiguous() if "velsurf" in costs else nan
         self.vobs = S.get(state, "vvelsurfobs").contiguous() if "velsurf" in costs else nan
         self.thkobs = S.get(state, "thkobs").contiguous() if "thk" in costs else nan
+        self.usurfobs = S.get(state, "usurfobs").contiguous() if "usurf" in costs else None
         self.icemaskobs = S.get(state, "icemaskobs").contiguous()
         self.icemask = S.get(state, "icemask").contiguous() if hasattr(state, "icemask") else self.icemaskobs
         self.dens = S.get(state, "dens_thkobs").contiguous()
@@ -128,21 +139,26 @@ class _Assim:
         nz = int(cfg.processes.iceflow.numerics.Nz)
         self.nz = nz
         f32 = dict(dtype=torch.float32, device=d)
-        self.var, self.grad, self.m, self.v = (torch.empty(self.n, **f32) for _ in range(4))
-        self.offsets = (C.c_size_t * 2)(0, self.n)
-        self.norms = torch.empty(int(L.lib().igm_adam_norms_len(1, self.offsets)), dtype=torch.float64, device=d)
+        # the optimizer's variables, one block of n per control (Adam clips each separately)
+        self.var, self.grad, self.m, self.v = (torch.empty(nc * self.n, **f32) for _ in range(4))
+        self.offsets = (C.c_size_t * (nc + 1))(*[k * self.n for k in range(nc + 1)])
+        self.norms = torch.empty(int(L.lib().igm_adam_norms_len(nc, self.offsets)), dtype=torch.float64, device=d)
         self.dU = torch.zeros((1, nz, ny, nx), **f32)
         self.dV = torch.zeros((1, nz, ny, nx), **f32)
         self.g_thk = torch.empty((ny, nx), **f32)
-        self.field_grad = torch.empty((1, 1, ny, nx), **f32)  # the thk channel only
-        self.partials = torch.empty(148 * 8 * 5, dtype=torch.float64, device=d)
-        nit = int(da.optimization.nbitmax) + 1
-        self.cost_hist = torch.zeros((nit, 5), dtype=torch.float64, device=d)
+        self.g_us = torch.empty((ny, nx), **f32) if "usurf" in self.controls else None
+        self.g_field = {c: torch.empty((ny, nx), **f32) for c in ("slidingco", "arrhenius") if c in self.controls}
+        # the emulator's input-field gradient, channels 0 .. the last one a control needs
+        self.n_grad = 1 + max(_CHANNEL[c] for c in self.controls)
+        self.field_grad = torch.empty((1, self.n_grad, ny, nx), **f32)
+        self.partials = torch.empty(148 * 8 * 6, dtype=torch.float64, device=d)
+        nit = int(o.nbitmax) + 1
+        self.cost_hist = torch.zeros((nit, 6), dtype=torch.float64, device=d)
+        self.field_hist = {c: torch.zeros((nit, 6), dtype=torch.float64, device=d) for c in self.g_field}
         self.rms_hist = torch.zeros((nit, 9), dtype=torch.float64, device=d)
         self.stat_partials = torch.empty(148 * 8 * 13, dtype=torch.float64, device=d)
         # parameters of igm_assim_cost_grad
         p = L.AssimParams()
-        f, r, o = da.fitting, da.regularization, da.optimization
         p.velsurfobs_std, p.velsurfobs_thr, p.thkobs_std = f.velsurfobs_std, f.velsurfobs_thr, f.thkobs_std
         p.regu_thk = r.thk
         area = float((self.icemask > 0.5).sum().item()) * self.dx ** 2  # regu_thk.py:11
@@ -157,9 +173,19 @@ class _Assim:
         p.icemask_cost = int("icemask" in costs)
         p.regularize_thk = int(r.to_regularize == "thk")
         p.mask_velsurf = 1
+        p.usurf_cost = int("usurf" in costs)
+        p.usurfobs_std = float(f.usurfobs_std)
+        p.n_usurf = max(1.0, float((self.icemaskobs > 0.5).sum().item()))
+        p.no_thk_control = int("thk" not in self.controls)
         self.params = p
-        self.present = [("velsurf" in costs), ("thk" in costs), bool(p.penalty and p.icemask_cost),
-                        bool(p.penalty), True]
+        self.log_slidingco = bool(f.log_slidingco)
+        pen = bool(p.penalty)
+        self.present = {"velsurf": "velsurf" in costs, "thk": "thk" in costs, "usurf": "usurf" in costs,
+                        "icemask": pen and bool(p.icemask_cost), "thk_positive": pen and "thk" in self.controls,
+                        "slidingco_positive": pen and "slidingco" in self.controls and not self.log_slidingco,
+                        "arrhenius_positive": pen and "arrhenius" in self.controls,
+                        "thk_regu": "thk" in self.controls, "slid_regu": "slidingco" in self.controls,
+                        "arrh_regu": "arrhenius" in self.controls}
         # flux-divergence cost (total_cost.py:23-27: divfluxfcz before divfluxobs)
         self.div_kind = "fcz" if "divfluxfcz" in costs else ("obs" if "divfluxobs" in costs else None)
         self.div_method = str(da.divflux.method)
@@ -172,18 +198,43 @@ class _Assim:
                                             dtype=torch.float64, device=d)
             self.divfluxobs = S.get(state, "divfluxobs").contiguous() if self.div_kind == "obs" else None
             self.vert_weight = np.asarray(torch.as_tensor(state.vert_weight).cpu(), dtype=np.float64).reshape(-1)
-        self.sc = float(da.scaling.thk)
+        self.scale = {c: float(getattr(da.scaling, c)) for c in self.controls}
         self.reproject = "reproject" in o.obstacle_constraint
+        self.aniso = float(r.smooth_anisotropy_factor)
+        self.aniso_sl = float(r.smooth_anisotropy_factor_sl)
+
+    def control_kw(self, c):
+        """igm_assim_control's transform, mask and reprojection for control c
+        (optimize/update.py:23-27, 58-68, 84-98; sole_mask off)."""
+        transform = int(c == "slidingco" and self.log_slidingco)
+        mask = 0 if c == "slidingco" else 1
+        if not self.reproject:
+            rep, lower = 0, 0.0
+        elif c == "thk":
+            rep, lower = 1, 0.0
+        elif c == "slidingco":
+            rep, lower = 2, 0.0
+        elif c == "arrhenius":
+            rep, lower = 2, 1.0
+        else:
+            rep, lower = 0, 0.0
+        return dict(transform=transform, mask=mask, reproject=rep, lower=lower,
+                    reproject_mask="icemask" in self.cost_list)
+
+    def block(self, t, k):
+        return t[k * self.n:(k + 1) * self.n]
 
 
 def optimize_initialize(cfg, state):
-    """optimize/initialize.py:10-69 for control thk."""
+    """optimize/initialize.py:10-69."""
     da = cfg.processes.data_assimilation
     if ("usurf" in da.cost_list) != ("usurf" in da.control_list):
         raise AssertionError("usurf must be in both cost_list and control_list, or in neither")
     thkobs = S.get(state, "thkobs").cpu().numpy()
     if np.all(np.isnan(thkobs)) and "thk" in da.cost_list:
         da.cost_list = [c for c in da.cost_list if c != "thk"]
+    if "usurf" in da.control_list and not hasattr(state, "usurfobs"):
+        raise ValueError("control usurf needs state.usurfobs")
     thk = S.get(state, "thk")
     if hasattr(state, "thkinit"):
         thk = S.get(state, "thkinit").clone()
@@ -216,20 +267,26 @@ def _record_rms(a: _Assim, state, i):
 
 
 def optimize_update(cfg, state, cost, i):
-    """optimize/update.py:15-103: one ADAM iteration for control thk.
-    ``cost`` receives the device cost tensor (double[5] in the order
-    velsurf, thk, icemask, thk_positive, thk_regu)."""
+    """optimize/update.py:15-103: one ADAM iteration over the controls.
+    ``cost`` receives device cost tensors: "all" (double[6], velsurf, thk,
+    icemask, thk_positive, thk_regu, usurf), "divflux", "slidingco" and
+    "arrhenius" (double[6], [3] the penalty, [4] the regularisation) when
+    present."""
     da = cfg.processes.data_assimilation
     o = da.optimization
     a: _Assim = state._igm_assim
     lib, st = L.lib(), L.stream_ptr()
-    thk = S.get(state, "thk").contiguous()
-    K.assim_control(0, thk, a.sc, variable=a.var, m=a.m, v=a.v)
-    S.put(state, "thk", thk)
+    x = {}
+    for k, c in enumerate(a.controls):
+        x[c] = S.get(state, c).contiguous()
+        K.assim_control(0, x[c], a.scale[c], variable=a.block(a.var, k), m=a.block(a.m, k), v=a.block(a.v, k),
+                        **a.control_kw(c))
+        S.put(state, c, x[c])
     lr = float(o.step_size) * (float(o.step_size_decay) ** (i / 100)) if o.step_size_decay < 1 else float(o.step_size)
+    thk = S.get(state, "thk").contiguous()
     # emulator forward, masked where thk == 0 (emulate.py:116-152), activations kept for the gradient
     model = state.iceflow_model
-    f = [thk] + [S.get(state, k) for k in ("usurf", "arrhenius", "slidingco")]
+    f = [thk] + [S.get(state, k).contiguous() for k in ("usurf", "arrhenius", "slidingco")]
     buf = model.buffers(1, a.ny, a.nx, train=True)
     model.prepare_input(f, a.dx, [(0, 0)], a.ny, a.nx, buf)
     U, V = model.forward(buf, 1, a.ny, a.nx, thk_mask=thk, keep_acts=True)
@@ -237,29 +294,46 @@ def optimize_update(cfg, state, cost, i):
     P.set_derived_velocities(cfg, state, mask=False)
     uvs, vvs = S.get(state, "uvelsurf"), S.get(state, "vvelsurf")
     flow = None
-    if float(da.regularization.smooth_anisotropy_factor) != 1.0:
+    if a.aniso != 1.0 or ("slidingco" in a.controls and a.aniso_sl != 1.0):
         flow = K.assim_flow_direction(uvs.contiguous(), vvs.contiguous())
         state.flowdirx, state.flowdiry = flow
     # total_cost and its gradient; dC/dvelsurf lands in the top layer of dU, dV (Lagrange basis)
-    K.assim_cost_grad(thk, S.get(state, "usurf"), uvs.contiguous(), vvs.contiguous(), a.uobs, a.vobs, a.thkobs,
-                      a.dens, a.icemaskobs, flow, a.dx, a.params, partials=a.partials, costs=a.cost_hist[i],
-                      g_thk=a.g_thk, g_u=a.dU[0, a.nz - 1], g_v=a.dV[0, a.nz - 1])
+    K.assim_cost_grad(thk, f[1], uvs.contiguous(), vvs.contiguous(), a.uobs, a.vobs, a.thkobs, a.dens, a.icemaskobs,
+                      flow if a.aniso != 1.0 else None, a.dx, a.params, partials=a.partials, costs=a.cost_hist[i],
+                      g_thk=a.g_thk, g_u=a.dU[0, a.nz - 1], g_v=a.dV[0, a.nz - 1], usurfobs=a.usurfobs,
+                      g_us=a.g_us)
     if a.div_kind is not None:
         _divflux_cost(cfg, state, a, thk, i)
+    r = da.regularization
+    for c, g in a.g_field.items():
+        # regu_slidingco / regu_arrhenius and the positivity penalties (total_cost.py:45-54, 63-69)
+        aniso = a.aniso_sl if c == "slidingco" else 1.0
+        pen = bool(a.params.penalty) and not (c == "slidingco" and a.log_slidingco)
+        K.assim_field_regu(S.get(state, c).contiguous(), a.dx, float(getattr(r, c)), aniso,
+                           flow if aniso != 1.0 else None, penalty=pen, threshold=1.0 if c == "arrhenius" else 0.0,
+                           grad=g, costs=a.field_hist[c][i], partials=a.partials)
     model.backward(buf, 1, a.ny, a.nx, a.dU, a.dV, field_grad=a.field_grad, param_grads=False)
-    K.assim_control(1, thk, a.sc, icemaskobs=a.icemaskobs, grad=a.grad, g_direct=a.g_thk,
-                    g_emul=a.field_grad[0, 0].reshape(-1))
-    rc = lib.igm_adam_clipnorm(1, a.offsets, L.ptr(a.var), L.ptr(a.grad), L.ptr(a.m), L.ptr(a.v), L.ptr(a.norms),
-                               lr, 0.9, 0.999, float(o.optimizer_epsilon), float(o.optimizer_clipnorm), i + 1, st)
+    direct = {"thk": a.g_thk, "usurf": a.g_us, **a.g_field}
+    for k, c in enumerate(a.controls):
+        K.assim_control(1, x[c], a.scale[c], icemaskobs=a.icemaskobs, variable=a.block(a.var, k),
+                        grad=a.block(a.grad, k), g_direct=direct[c],
+                        g_emul=a.field_grad[0, _CHANNEL[c]].reshape(-1), **a.control_kw(c))
+    rc = lib.igm_adam_clipnorm(len(a.controls), a.offsets, L.ptr(a.var), L.ptr(a.grad), L.ptr(a.m), L.ptr(a.v),
+                               L.ptr(a.norms), lr, 0.9, 0.999, float(o.optimizer_epsilon),
+                               float(o.optimizer_clipnorm), i + 1, st)
     L.check(rc, "igm_adam_clipnorm")
-    K.assim_control(2, thk, a.sc, icemaskobs=a.icemaskobs, variable=a.var,
-                    reproject_mask=a.reproject and "icemask" in a.cost_list, reproject_pos=a.reproject)
-    S.put(state, "thk", thk)
+    for k, c in enumerate(a.controls):
+        K.assim_control(2, x[c], a.scale[c], icemaskobs=a.icemaskobs, variable=a.block(a.var, k),
+                        **a.control_kw(c))
+        S.put(state, c, x[c])
+    thk = S.get(state, "thk").contiguous()
     S.put(state, "divflux", K.divflux(S.get(state, "ubar").contiguous(), S.get(state, "vbar").contiguous(), thk,
                                       a.dx, a.div_method))
     cost["all"] = a.cost_hist[i]
     if a.div_kind is not None:
         cost["divflux"] = a.div_hist[i]
+    for c in a.g_field:
+        cost[c] = a.field_hist[c][i]
 
 
 def _divflux_cost(cfg, state, a: _Assim, thk, i):
@@ -291,10 +365,16 @@ def _divflux_cost(cfg, state, a: _Assim, thk, i):
 def _cost_table(a: _Assim, n_it):
     """The per-iteration costs in total_cost's order: (keys, [n_it, k] array)."""
     ch = a.cost_hist[:n_it].cpu().numpy()
-    cols = {k: ch[:, j] for j, k in enumerate(_COST_KEYS) if a.present[j]}
+    cols = {k: ch[:, j] for j, k in enumerate(_COST_KEYS)}
     if a.div_kind is not None:
         cols["divflux"] = a.div_hist[:n_it].cpu().numpy()
-    keys = [k for k in _ALL_KEYS if k in cols]
+    for c, pen, reg in (("slidingco", "slidingco_positive", "slid_regu"), ("arrhenius", "arrhenius_positive",
+                                                                          "arrh_regu")):
+        if c in a.field_hist:
+            fh = a.field_hist[c][:n_it].cpu().numpy()
+            cols[pen], cols[reg] = fh[:, 3], fh[:, 4]
+    present = dict(a.present, divflux=a.div_kind is not None)
+    keys = [k for k in _ALL_KEYS if present.get(k, False)]
     return keys, np.stack([cols[k] for k in keys], axis=1)
 
 

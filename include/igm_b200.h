@@ -280,41 +280,75 @@ typedef struct igm_assim_params {
   int32_t icemask_cost;    /* "icemask" in cost_list */
   int32_t regularize_thk;  /* regularization.to_regularize == "thk" (else "topg": usurf - thk) */
   int32_t mask_velsurf;    /* the surface velocities are where(thk > 0, U, 0): no gradient off the ice */
+  double usurfobs_std;     /* fitting.usurfobs_std (misfit_usurf) */
+  double n_usurf;          /* number of nodes inside icemaskobs > 0.5 (misfit_usurf's count) */
+  int32_t usurf_cost;      /* "usurf" in cost_list */
+  int32_t no_thk_control;  /* thk not in control_list: no thk_positive penalty, no regu_thk */
 } igm_assim_params;
 
-/* The cost terms of total_cost (cost_terms/total_cost.py:13-70) for the
- * default configuration -- misfit_velsurf.py:8-19, misfit_thk.py:8-16, the
- * icemask and positive-thickness penalties (:36-46) and regu_thk.py:8-70
- * (fix_opti_normalization_issue off) -- and their gradients w.r.t. thk and the
- * emulated surface velocities (uvelsurf, vvelsurf, zero where thk <= 0).
- * Observations are NaN where missing; flowdirx/y [ny-1][nx-1] (anisotropic
- * branch only, else NULL).  costs (device double[5]): velsurf, thk, icemask,
- * thk_positive, thk_regu; partials: device double[n_parts * 5] scratch.
- * All 2-D arrays [ny][nx] of the dtype. */
+/* The cost terms of total_cost (cost_terms/total_cost.py:13-70) that depend
+ * on thk and usurf -- misfit_velsurf.py:8-19, misfit_thk.py:8-16, the icemask
+ * and positive-thickness penalties (:36-46), regu_thk.py:8-70
+ * (fix_opti_normalization_issue off) and, with usurf_cost, misfit_usurf.py:5-15
+ * -- and their gradients w.r.t. thk, the emulated surface velocities
+ * (uvelsurf, vvelsurf, zero where thk <= 0) and, when grad_usurf is given,
+ * usurf (misfit_usurf and regu_thk's bed usurf - thk).  Observations are NaN
+ * where missing; flowdirx/y [ny-1][nx-1] (anisotropic branch only, else NULL);
+ * usurfobs only with usurf_cost.  costs (device double[6]): velsurf, thk,
+ * icemask, thk_positive, thk_regu, usurf; partials: device double[n_parts * 6]
+ * scratch.  All 2-D arrays [ny][nx] of the dtype. */
 IGM_API int igm_assim_cost_grad(int dtype, int ny, int nx, double dx, const void* thk, const void* usurf,
                         const void* uvelsurf, const void* vvelsurf, const void* uvelsurfobs,
                         const void* vvelsurfobs, const void* thkobs, const void* dens_thkobs,
-                        const void* icemaskobs, const void* flowdirx, const void* flowdiry,
-                        const igm_assim_params* params, void* grad_thk, void* grad_uvelsurf,
-                        void* grad_vvelsurf, double* partials, int n_parts, double* costs, void* stream);
+                        const void* icemaskobs, const void* flowdirx, const void* flowdiry, const void* usurfobs,
+                        const igm_assim_params* params, void* grad_thk, void* grad_uvelsurf, void* grad_vvelsurf,
+                        void* grad_usurf, double* partials, int n_parts, double* costs, void* stream);
 
-/* The control update of optimize_update
- * (data_assimilation/optimize/update.py:23-27, 38-42, 56-68, 77-98) for
- * control thk with scaling `scale`, at the three points where the reference
- * touches the control:
- *   mode 0 (before the emulator forward): variable = thk / scale, then
- *     thk = variable * scale, and m = v = 0 (the reference re-creates the
- *     control tf.Variable at every iteration, so its Adam slots start at zero);
- *   mode 1 (the gradient): grad = scale (grad_direct + grad_emulator) where
- *     icemaskobs > 0.5, 0 elsewhere;
- *   mode 2 (after igm_adam_clipnorm): thk = variable * scale, then 0 outside
- *     the ice mask (reproject_mask) and at negative values (reproject_pos).
+/* The regularisation and positivity penalty of another control field:
+ * regu_slidingco (cost_terms/regu_slidingco.py:8-52; isotropic, or anisotropic
+ * with aniso_factor = smooth_anisotropy_factor_sl and the flow directions),
+ * regu_arrhenius (cost_terms/regu_arrhenius.py:5-24; isotropic), both with
+ * sole_mask and fix_opti_normalization_issue off, weight regu, and with
+ * penalty the 1e10 mean(field^2 where field < penalty_threshold) of
+ * total_cost.py:45-54 (threshold 0 for slidingco, 1 for arrhenius).  grad:
+ * dC/dfield [ny][nx]; costs (device double[6], the layout of
+ * igm_assim_cost_grad): [3] the penalty, [4] the regularisation, the others 0. */
+IGM_API int igm_assim_field_regu(int dtype, int ny, int nx, double dx, const void* field, const void* flowdirx,
+                                 const void* flowdiry, double regu, double aniso_factor, int penalty,
+                                 double penalty_threshold, void* grad, double* partials, int n_parts,
+                                 double* costs, void* stream);
+
+/* The control update of optimize_update (data_assimilation/optimize/update.py:
+ * 22-42, 56-98) for one control x (thk, usurf, slidingco or arrhenius) with
+ * scaling `scale`, at the three points where the reference touches it:
+ *   mode 0 (before the emulator forward): variable = x / scale (transform 1,
+ *     fitting.log_slidingco: sqrt(x / scale)), then x from the variable, and
+ *     m = v = 0 (the reference re-creates the control tf.Variable at every
+ *     iteration, so its Adam slots start at zero);
+ *   mode 1 (the gradient): grad = dx/dvariable (grad_direct + grad_emulator),
+ *     zero where the mask is off (mask 1: icemaskobs > 0.5, as for thk, usurf
+ *     and arrhenius; 2: icemaskobs == 1, slidingco with sole_mask; 0: none);
+ *   mode 2 (after igm_adam_clipnorm): x from the variable, then the
+ *     reprojection (reproject 1, thk: 0 outside icemaskobs > 0.5 when
+ *     reproject_mask, then x >= 0; 2: x >= lower, 0 for slidingco, 1 for
+ *     arrhenius; 0: none).
  * variable, grad, m, v and grad_emulator (the emulator's input-field gradient,
- * igm_cnn_input_gradient) are device float[n], the others [n] of the dtype;
- * grad_emulator may be NULL; arguments a mode does not read may be NULL. */
-IGM_API int igm_assim_control(int dtype, int mode, size_t n, double scale, int reproject_mask, int reproject_pos,
-                      void* thk, const void* grad_direct, const float* grad_emulator, const void* icemaskobs,
-                      float* variable, float* grad, float* m, float* v, void* stream);
+ * igm_cnn_input_gradient) are device float[n], x, grad_direct and icemaskobs
+ * [n] of the dtype; grad_emulator may be NULL; arguments a mode does not read
+ * may be NULL. */
+typedef struct igm_assim_control_params {
+  int32_t mode;            /* 0, 1, 2 as above */
+  int32_t transform;       /* 0: x = variable scale; 1: x = variable^2 scale */
+  int32_t mask;            /* 0 none, 1 icemaskobs > 0.5, 2 icemaskobs == 1 */
+  int32_t reproject;       /* 0 none, 1 thk, 2 lower bound */
+  int32_t reproject_mask;  /* reproject 1: zero outside the mask ("icemask" in cost_list) */
+  int32_t reserved;
+  double scale;            /* scaling.<control> */
+  double lower;            /* reproject 2 */
+} igm_assim_control_params;
+IGM_API int igm_assim_control(int dtype, size_t n, const igm_assim_control_params* params, void* x,
+                              const void* grad_direct, const float* grad_emulator, const void* icemaskobs,
+                              float* variable, float* grad, float* m, float* v, void* stream);
 
 /* compute_rms_std_optimization (data_assimilation/utils.py:10-66): out
  * (device double[9]) = rmsthk, stdthk, rmsvel, stdvel, rmsdiv, stddiv,

@@ -735,7 +735,7 @@ def da_flow_direction(uvelsurf, vvelsurf):
 
 
 def da_costs(thk, usurf, uvelsurf, vvelsurf, uobs, vobs, thkobs, dens_thkobs, icemaskobs, icemask, flowdir, dx,
-             p: AssimParams):
+             p: AssimParams, thk_control=True):
     """The cost terms of total_cost (cost_terms/total_cost.py:13-70) for
     control ``thk``, costs velsurf + thk + icemask and the penalty
     constraint: misfit_velsurf.py:8-19, misfit_thk.py:8-16, the icemask and
@@ -755,7 +755,10 @@ def da_costs(thk, usurf, uvelsurf, vvelsurf, uobs, vobs, thkobs, dens_thkobs, ic
     if p.penalty:
         if p.icemask_cost:
             cost["icemask"] = 10 ** 10 * torch.mean(torch.where(icemaskobs > 0.5, z, thk ** 2))
-        cost["thk_positive"] = 10 ** 10 * torch.mean(torch.where(thk >= 0, z, thk ** 2))
+        if thk_control:
+            cost["thk_positive"] = 10 ** 10 * torch.mean(torch.where(thk >= 0, z, thk ** 2))
+    if not thk_control:
+        return cost
     area = torch.sum(torch.where(icemask > 0.5, 1.0, 0.0)) * dx ** 2
     gamma = p.convexity_weight * area ** (p.convexity_power - 2.0)
     field = usurf - thk if p.to_regularize == "topg" else thk
@@ -827,32 +830,54 @@ class AssimControl:
     icemask_cost: bool = True
 
 
-def da_optimize_update(thk, usurf, arrhenius, slidingco, dx, weights, biases, Nz, vert_weight, obs, p: AssimParams,
-                       ctl: AssimControl, optimizer: KerasLegacyAdam, i, bf16=True, out_scale=1.0, input_scales=None,
-                       divflux_cost=None):
-    """One ADAM iteration of optimize_update (optimize/update.py:15-103) for
-    control_list [thk]: thk_sc = thk / sc is a new variable (fresh Adam
-    slots, the optimizer's iteration count carries on), thk = thk_sc sc, the
-    emulator forward masked where thk == 0 (emulate.py:116-152), the flow
-    directions from the emulated surface velocities (constants of the
-    gradient: they pass through scipy), total_cost, its gradient with respect
-    to thk_sc zeroed outside icemaskobs > 0.5, the Adam step at learning rate
-    step_size decay^(i/100), thk = thk_sc sc, reprojection, the upwind flux
-    divergence of the emulated depth-averaged velocity.
+@dataclass
+class AssimControls:
+    """The controls of optimize_update and the keys of their cost terms
+    (conf/processes/data_assimilation.yaml: control_list, scaling,
+    fitting.log_slidingco, regularization.slidingco / arrhenius /
+    smooth_anisotropy_factor_sl, fitting.usurfobs_std)."""
+    controls: list = field(default_factory=lambda: ["thk"])
+    scaling: dict = field(default_factory=lambda: {"thk": 2.0, "usurf": 0.5, "slidingco": 1e-4, "arrhenius": 0.1})
+    log_slidingco: bool = False
+    regu_slidingco: float = 1.0
+    regu_arrhenius: float = 10.0
+    aniso_sl: float = 1.0
+    usurfobs_std: float = 2.0
 
-    ``obs``: dict uobs, vobs, thkobs, dens, icemaskobs, icemask.  Returns
-    (thk, costs dict, dict of uvelsurf, vvelsurf, ubar, vbar, divflux,
-    gradient).  ``input_scales``: per-channel factors of the network input
-    (None: the raw fields, as the reference).  ``divflux_cost``: None or a
-    dict (kind "obs"/"fcz", method, std, regu, force_zero_sum, divfluxobs)
-    adding cost_divfluxobs / cost_divfluxfcz of the emulated velbar
-    (total_cost.py:23-27); for "fcz" the regression is refitted at every 10th
-    iteration and kept in the dict ("slope", "intercept")."""
-    sc = ctl.scaling_thk
-    thk_sc = (thk / sc).detach().clone().requires_grad_(True)
-    th = thk_sc * sc
+
+def da_optimize_step(fields, dx, weights, biases, Nz, vert_weight, obs, p: AssimParams, ctl: AssimControl,
+                     optimizer: KerasLegacyAdam, i, mc: AssimControls, bf16=True, out_scale=1.0, input_scales=None,
+                     divflux_cost=None):
+    """One ADAM iteration of optimize_update (optimize/update.py:15-103) over
+    the controls of ``mc``: each control becomes a new variable x / scale
+    (sqrt(x / scale) for slidingco with log_slidingco: fresh Adam slots, the
+    optimizer's iteration count carries on), the fields are rebuilt from the
+    variables, the emulator forward is masked where thk == 0
+    (emulate.py:116-152), the flow directions come from the emulated surface
+    velocities (constants of the gradient: they pass through scipy), then
+    total_cost (total_cost.py:13-71: the costs of da_costs, misfit_usurf with
+    "usurfobs" in obs, the flux-divergence term of ``divflux_cost``, the
+    slidingco / arrhenius penalties and regularisations), its gradient w.r.t.
+    the variables (zero outside icemaskobs > 0.5 except for slidingco), one
+    Adam step at step_size decay^(i/100), the fields from the variables, the
+    reprojection (thk: mask and >= 0; slidingco >= 0; arrhenius >= 1), the
+    flux divergence of the emulated depth-averaged velocity.
+
+    ``fields``: dict thk, usurf, arrhenius, slidingco.  Returns (new fields,
+    costs dict, dict of uvelsurf, vvelsurf, ubar, vbar, divflux and the
+    variables' gradients under "gradient_<control>")."""
+    sc = mc.scaling
+    var, x = {}, dict(fields)
+    for c in mc.controls:
+        if c == "slidingco" and mc.log_slidingco:
+            var[c] = torch.sqrt(fields[c] / sc[c]).detach().clone().requires_grad_(True)
+            x[c] = (var[c] ** 2) * sc[c]
+        else:
+            var[c] = (fields[c] / sc[c]).detach().clone().requires_grad_(True)
+            x[c] = var[c] * sc[c]
+    th, us, ar, sl = x["thk"], x["usurf"], x["arrhenius"], x["slidingco"]
     dX = torch.full_like(th, dx)
-    X = fieldin_to_X([th, usurf, arrhenius, slidingco, dX])
+    X = fieldin_to_X([th, us, ar, sl, dX])
     if input_scales is not None:
         X = X * torch.tensor(input_scales, dtype=X.dtype)
     Y = cnn_forward(X, weights, biases, bf16=bf16, bf16_first=False, out_scale=out_scale)
@@ -861,40 +886,78 @@ def da_optimize_update(thk, usurf, arrhenius, slidingco, dx, weights, biases, Nz
     V = torch.where(th > 0, V[0], torch.zeros_like(V[0]))
     uvs, vvs = U[-1], V[-1]
     flow = None
-    if p.smooth_anisotropy_factor != 1:
+    if p.smooth_anisotropy_factor != 1 or ("slidingco" in mc.controls and mc.aniso_sl != 1):
         flow = da_flow_direction(uvs.detach(), vvs.detach())
-    cost = da_costs(th, usurf, uvs, vvs, obs["uobs"], obs["vobs"], obs["thkobs"], obs["dens"], obs["icemaskobs"],
-                    obs["icemask"], flow, dx, p)
+    cost = da_costs(th, us, uvs, vvs, obs["uobs"], obs["vobs"], obs["thkobs"], obs["dens"], obs["icemaskobs"],
+                    obs["icemask"], flow if p.smooth_anisotropy_factor != 1 else None, dx, p,
+                    thk_control="thk" in mc.controls)
     if divflux_cost is not None:
         dc = divflux_cost
         ub_g, vb_g = torch.sum(U * vert_weight, 0), torch.sum(V * vert_weight, 0)
         if dc["kind"] == "fcz" and (i % 10 == 0 or "slope" not in dc):
             act = obs["icemaskobs"] > 0.5
             D0 = compute_divflux(ub_g.detach(), vb_g.detach(), th.detach(), dx, dc["method"])
-            dc["slope"], dc["intercept"] = linregress(usurf[act].numpy(), D0[act].numpy())
+            dc["slope"], dc["intercept"] = linregress(us[act].detach().numpy(), D0[act].numpy())
         cost["divflux"] = da_cost_divflux(dc["kind"], ub_g, vb_g, th, dx, obs["icemaskobs"],
-                                          divfluxobs=dc.get("divfluxobs"), usurf=usurf, slope=dc.get("slope"),
+                                          divfluxobs=dc.get("divfluxobs"), usurf=us.detach(), slope=dc.get("slope"),
                                           intercept=dc.get("intercept"), std=dc["std"], regu=dc["regu"],
                                           force_zero_sum=dc["force_zero_sum"], method=dc["method"])
+    if "usurfobs" in obs:
+        cost["usurf"] = da_misfit_usurf(us, obs["usurfobs"], obs["icemaskobs"], mc.usurfobs_std)
+    if p.penalty:
+        if "slidingco" in mc.controls and not mc.log_slidingco:
+            cost["slidingco_positive"] = da_penalty(sl, 0.0)
+        if "arrhenius" in mc.controls:
+            cost["arrhenius_positive"] = da_penalty(ar, 1.0)
+    if "slidingco" in mc.controls:
+        cost["slid_regu"] = da_regu_field(sl, dx, mc.regu_slidingco, mc.aniso_sl, flow)
+    if "arrhenius" in mc.controls:
+        cost["arrh_regu"] = da_regu_field(ar, dx, mc.regu_arrhenius)
     total = sum(cost.values())
-    (g,) = torch.autograd.grad(total, thk_sc)
-    g = torch.where(obs["icemaskobs"] > 0.5, g, torch.zeros_like(g))
+    grads = torch.autograd.grad(total, [var[c] for c in mc.controls])
+    inside = obs["icemaskobs"] > 0.5
+    grads = [g if c == "slidingco" else torch.where(inside, g, torch.zeros_like(g))
+             for c, g in zip(mc.controls, grads)]
     if ctl.step_size_decay < 1:
         optimizer.lr = ctl.step_size * (ctl.step_size_decay ** (i / 100))
-    var = thk_sc.detach().clone()
-    optimizer.apply_gradients([(g, var)])
-    thk_new = var * sc
+    new_vars = [var[c].detach().clone() for c in mc.controls]
+    optimizer.apply_gradients(list(zip(grads, new_vars)))
+    out = dict(fields)
+    for c, w in zip(mc.controls, new_vars):
+        out[c] = (w ** 2) * sc[c] if (c == "slidingco" and mc.log_slidingco) else w * sc[c]
     if ctl.reproject:
-        if ctl.icemask_cost:
-            thk_new = torch.where(obs["icemaskobs"] > 0.5, thk_new, torch.zeros_like(thk_new))
-        thk_new = torch.where(thk_new < 0, torch.zeros_like(thk_new), thk_new)
+        if "thk" in mc.controls:
+            t = out["thk"]
+            if ctl.icemask_cost:
+                t = torch.where(inside, t, torch.zeros_like(t))
+            out["thk"] = torch.where(t < 0, torch.zeros_like(t), t)
+        if "slidingco" in mc.controls:
+            out["slidingco"] = torch.where(out["slidingco"] < 0, torch.zeros_like(out["slidingco"]), out["slidingco"])
+        if "arrhenius" in mc.controls:
+            out["arrhenius"] = torch.where(out["arrhenius"] < 1.0, torch.ones_like(out["arrhenius"]),
+                                           out["arrhenius"])
     U, V = U.detach(), V.detach()
     ubar = torch.sum(U * vert_weight, 0)
     vbar = torch.sum(V * vert_weight, 0)
     method = divflux_cost["method"] if divflux_cost is not None else "upwind"
     aux = {"uvelsurf": uvs.detach(), "vvelsurf": vvs.detach(), "ubar": ubar, "vbar": vbar,
-           "divflux": compute_divflux(ubar, vbar, thk_new, dx, method), "gradient": g}
-    return thk_new, {k: v.detach() for k, v in cost.items()}, aux
+           "divflux": compute_divflux(ubar, vbar, out["thk"], dx, method)}
+    aux.update({f"gradient_{c}": g for c, g in zip(mc.controls, grads)})
+    return out, {k: v.detach() for k, v in cost.items()}, aux
+
+
+def da_optimize_update(thk, usurf, arrhenius, slidingco, dx, weights, biases, Nz, vert_weight, obs, p: AssimParams,
+                       ctl: AssimControl, optimizer: KerasLegacyAdam, i, bf16=True, out_scale=1.0, input_scales=None,
+                       divflux_cost=None):
+    """da_optimize_step for control_list [thk] with scaling ctl.scaling_thk:
+    returns (thk, costs dict, aux with the gradient of thk's variable under
+    "gradient")."""
+    mc = AssimControls(controls=["thk"], scaling={"thk": ctl.scaling_thk})
+    out, cost, aux = da_optimize_step({"thk": thk, "usurf": usurf, "arrhenius": arrhenius, "slidingco": slidingco},
+                                      dx, weights, biases, Nz, vert_weight, obs, p, ctl, optimizer, i, mc, bf16=bf16,
+                                      out_scale=out_scale, input_scales=input_scales, divflux_cost=divflux_cost)
+    aux["gradient"] = aux["gradient_thk"]
+    return out["thk"], cost, aux
 
 
 def da_rms_std(thk, thkobs, uvelsurf, vvelsurf, uobs, vobs, icemaskobs, dx, divflux=None, divfluxobs=None,
@@ -974,3 +1037,36 @@ def da_cost_divflux(kind, ubar, vbar, thk, dx, icemaskobs, divfluxobs=None, usur
     if force_zero_sum:
         c = c + 0.5 * 1000 * torch.mean(D[act_m] / std) ** 2
     return c
+
+
+def da_regu_field(f, dx, weight, aniso=1.0, flowdir=None):
+    """regu_slidingco (cost_terms/regu_slidingco.py:8-52) and regu_arrhenius
+    (cost_terms/regu_arrhenius.py:5-24) with sole_mask and
+    fix_opti_normalization_issue off: weight (l2_loss(df/dx) + l2_loss(df/dy))
+    on the node differences (aniso == 1), or the cell-centred differences
+    split along and across the flow direction weighted 1/sqrt(aniso) and
+    sqrt(aniso)."""
+    if aniso == 1.0:
+        dadx = (f[:, 1:] - f[:, :-1]) / dx
+        dady = (f[1:, :] - f[:-1, :]) / dx
+        return weight * (torch.sum(dadx ** 2) / 2 + torch.sum(dady ** 2) / 2)
+    dadx = (f[:, 1:] - f[:, :-1]) / dx
+    dadx = (dadx[1:, :] + dadx[:-1, :]) / 2.0
+    dady = (f[1:, :] - f[:-1, :]) / dx
+    dady = (dady[:, 1:] + dady[:, :-1]) / 2.0
+    fx, fy = flowdir
+    return weight * ((1.0 / np.sqrt(aniso)) * torch.sum((dadx * fx + dady * fy) ** 2) / 2
+                     + np.sqrt(aniso) * torch.sum((dadx * fy - dady * fx) ** 2) / 2)
+
+
+def da_penalty(f, threshold):
+    """The positivity penalties of total_cost.py:40-54: 1e10 mean of f^2
+    where f < threshold (0 for thk and slidingco, 1 for arrhenius)."""
+    return 1e10 * torch.mean(torch.where(f >= threshold, torch.zeros_like(f), f ** 2))
+
+
+def da_misfit_usurf(usurf, usurfobs, icemaskobs, std):
+    """misfit_usurf (cost_terms/misfit_usurf.py:5-15): 0.5 mean over
+    icemaskobs > 0.5 of ((usurf - usurfobs) / std)^2."""
+    act = icemaskobs > 0.5
+    return 0.5 * torch.mean(((usurf[act] - usurfobs[act]) / std) ** 2)

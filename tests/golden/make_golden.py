@@ -469,6 +469,79 @@ def divflux_cases():
     save("divflux", out)
 
 
+def assim_control_cases():
+    """The cost terms of the other controls, executed from the reference's
+    files: regu_slidingco (isotropic, and anisotropic with
+    smooth_anisotropy_factor_sl), regu_arrhenius, misfit_usurf, the
+    slidingco / arrhenius positivity penalties of total_cost.py:45-54, and
+    regu_thk's dependence on usurf (to_regularize "topg"), with torch
+    autograd gradients w.r.t. the fields."""
+    dau = importlib.import_module("igm.processes.data_assimilation.utils")
+    rs = importlib.import_module("igm.processes.data_assimilation.cost_terms.regu_slidingco")
+    ra = importlib.import_module("igm.processes.data_assimilation.cost_terms.regu_arrhenius")
+    mu = importlib.import_module("igm.processes.data_assimilation.cost_terms.misfit_usurf")
+    rt = importlib.import_module("igm.processes.data_assimilation.cost_terms.regu_thk")
+    out = {}
+    for tag, dtype in [("f64", torch.float64), ("f32", torch.float32)]:
+        rng = np.random.default_rng(23)
+        ny, nx, dx = 21, 29, 100.0
+        g = glacier(ny, nx, dx, 14, dtype)
+        f = lambda a: torch.as_tensor(np.asarray(a), dtype=dtype)  # noqa: E731
+        thk = g["thk"] + f(np.abs(rng.normal(0, 5, (ny, nx))))
+        usurf = g["usurf"] + f(rng.normal(0, 2, (ny, nx)))
+        sl = f(np.abs(rng.normal(0.05, 0.03, (ny, nx))))
+        sl[rng.uniform(size=(ny, nx)) < 0.05] *= -1.0  # a few negative values: the penalty is active
+        ar = f(rng.normal(60, 30, (ny, nx)))
+        ar[rng.uniform(size=(ny, nx)) < 0.05] = 0.5   # below 1: the arrhenius penalty is active
+        usobs = usurf + f(rng.normal(0, 3, (ny, nx)))
+        icemaskobs = f((g["thk"].numpy() > 0).astype(np.float64))
+        uvs, vvs = f(rng.normal(20, 15, (ny, nx))), f(rng.normal(-5, 15, (ny, nx)))
+        with open(os.path.join(IGM, "conf", "processes", "data_assimilation.yaml")) as fh:
+            da = yaml.safe_load(fh)["data_assimilation"]
+        da.setdefault("cook", {"infer_params": False})
+        out.update({f"{tag}_{k}": x for k, x in dict(thk=thk, usurf=usurf, slidingco=sl, arrhenius=ar, usurfobs=usobs,
+                                                     icemaskobs=icemaskobs, uvs=uvs, vvs=vvs,
+                                                     dx=np.asarray(dx)).items()})
+        for aniso_sl in (1.0, 0.3):
+            cfg = load_cfg()
+            da["regularization"]["smooth_anisotropy_factor_sl"] = aniso_sl
+            da["regularization"]["slidingco"] = 7.0
+            da["regularization"]["arrhenius"] = 2.0
+            da["fitting"]["usurfobs_std"] = 1.5
+            cfg.processes.data_assimilation = ns(da)
+            st = types.SimpleNamespace(thk=thk, usurf=usurf.clone().requires_grad_(True),
+                                       slidingco=sl.clone().requires_grad_(True),
+                                       arrhenius=ar.clone().requires_grad_(True), usurfobs=usobs,
+                                       icemaskobs=icemaskobs, icemask=icemaskobs, uvelsurf=uvs, vvelsurf=vvs, dx=dx)
+            dau.compute_flow_direction_for_anisotropic_smoothing(st)
+            st.flowdirx, st.flowdiry = f(np.asarray(st.flowdirx)), f(np.asarray(st.flowdiry))
+            key = f"{tag}_sl{'aniso' if aniso_sl != 1.0 else 'iso'}"
+            c = rs.regu_slidingco(cfg, st)
+            (gs,) = torch.autograd.grad(c, [st.slidingco])
+            out.update({f"{key}_regu_slidingco": c, f"{key}_g_slidingco": gs, f"{key}_flowdirx": st.flowdirx,
+                        f"{key}_flowdiry": st.flowdiry})
+        c = ra.regu_arrhenius(cfg, st)
+        (ga,) = torch.autograd.grad(c, [st.arrhenius])
+        cp_s = 10 ** 10 * torch.mean(torch.where(st.slidingco >= 0, torch.zeros_like(st.slidingco),
+                                                 st.slidingco ** 2))
+        cp_a = 10 ** 10 * torch.mean(torch.where(st.arrhenius >= 1, torch.zeros_like(st.arrhenius),
+                                                 st.arrhenius ** 2))
+        (gps,) = torch.autograd.grad(cp_s, [st.slidingco])
+        (gpa,) = torch.autograd.grad(cp_a, [st.arrhenius])
+        cu = mu.misfit_usurf(cfg, st)
+        (gu,) = torch.autograd.grad(cu, [st.usurf])
+        # regu_thk (topg, isotropic) depends on usurf through the bed usurf - thk
+        da["regularization"]["smooth_anisotropy_factor"] = 1.0
+        cfg.processes.data_assimilation = ns(da)
+        crt = rt.regu_thk(cfg, st)
+        (gru,) = torch.autograd.grad(crt, [st.usurf])
+        out.update({f"{tag}_regu_arrhenius": c, f"{tag}_g_arrhenius": ga, f"{tag}_pen_slidingco": cp_s,
+                    f"{tag}_g_pen_slidingco": gps, f"{tag}_pen_arrhenius": cp_a, f"{tag}_g_pen_arrhenius": gpa,
+                    f"{tag}_misfit_usurf": cu, f"{tag}_g_usurf": gu, f"{tag}_regu_thk_topg": crt,
+                    f"{tag}_g_usurf_regu_thk": gru})
+    save("assim_controls", out)
+
+
 def save(name, d):
     arrs = {}
     for k, v in d.items():
@@ -496,5 +569,6 @@ if __name__ == "__main__":
     emulator_case()
     vert_flow_cases()
     divflux_cases()
+    assim_control_cases()
     keras_h5_cases()
     assim_cases()

@@ -41,7 +41,7 @@ def test_cost_and_gradient_match_reference(golden, tag):
                                           d["thkobs"], d["dens"], d["icemaskobs"], flow, float(g["dx"]),
                                           _params(g, aniso))
     tol = 1e-9 if dt == torch.float64 else 1e-4
-    c = costs.cpu().numpy()
+    c = costs.cpu().numpy()[:5]
     ref = [float(g[k]) for k in ["c_vel", "c_thk", "c_ice", "c_pos", "c_reg"]]
     np.testing.assert_allclose(c, ref, rtol=tol, atol=tol * max(abs(x) for x in ref))
     for a, k in [(gt, "g_thk"), (gu, "g_u"), (gv, "g_v")]:
@@ -168,3 +168,51 @@ def test_divflux_gradient_levels_and_mask(golden):
         extra = top_u if k == 2 else 0.0
         torch.testing.assert_close(dU[k], w[k] * ref_u + extra, rtol=1e-9, atol=1e-12)
         torch.testing.assert_close(dV[k], w[k] * ref_v + extra, rtol=1e-9, atol=1e-12)
+
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+def test_other_control_terms_match_reference(golden, tag):
+    """regu_slidingco (isotropic, anisotropic), regu_arrhenius and the
+    slidingco / arrhenius penalties through igm_assim_field_regu; misfit_usurf
+    and regu_thk's usurf gradient (bed usurf - thk) through
+    igm_assim_cost_grad's usurf output; against the reference source."""
+    g = golden("assim_controls")
+    dt = torch.float64 if tag == "f64" else torch.float32
+    d = {k: dev(g[f"{tag}_{k}"], dt) for k in ("thk", "usurf", "slidingco", "arrhenius", "usurfobs", "icemaskobs")}
+    dx = float(g[f"{tag}_dx"])
+    tol = 1e-9 if tag == "f64" else 1e-4
+
+    def close(a, ref):
+        ref = np.asarray(ref)
+        np.testing.assert_allclose(np.asarray(a), ref, rtol=tol, atol=tol * max(np.abs(ref).max(), 1e-30))
+
+    for mode, aniso in (("sliso", 1.0), ("slaniso", 0.3)):
+        flow = (dev(g[f"{tag}_{mode}_flowdirx"], dt), dev(g[f"{tag}_{mode}_flowdiry"], dt))
+        c, gr = K.assim_field_regu(d["slidingco"], dx, 7.0, aniso, flow if aniso != 1.0 else None, penalty=False)
+        close(c[4].item(), g[f"{tag}_{mode}_regu_slidingco"])
+        close(gr.cpu().numpy(), g[f"{tag}_{mode}_g_slidingco"])
+    c, gr = K.assim_field_regu(d["slidingco"], dx, 0.0, penalty=True, threshold=0.0)
+    close(c[3].item(), g[f"{tag}_pen_slidingco"])
+    close(gr.cpu().numpy(), g[f"{tag}_g_pen_slidingco"])
+    c, gr = K.assim_field_regu(d["arrhenius"], dx, 2.0, penalty=True, threshold=1.0)
+    close(c[4].item(), g[f"{tag}_regu_arrhenius"])
+    close(c[3].item(), g[f"{tag}_pen_arrhenius"])
+    close(gr.cpu().numpy(), g[f"{tag}_g_arrhenius"] + g[f"{tag}_g_pen_arrhenius"])
+    # misfit_usurf + regu_thk (topg, isotropic): dC/dusurf
+    p = L.AssimParams()
+    p.velsurfobs_std, p.velsurfobs_thr, p.thkobs_std, p.regu_thk = 1.0, 0.0, 3.0, 10.0
+    area = float((g[f"{tag}_icemaskobs"] > 0.5).sum()) * dx ** 2
+    p.gamma, p.aniso_factor, p.n_vel, p.n_thk = 0.002 * area ** (1.3 - 2.0), 1.0, 1.0, 1.0
+    p.penalty, p.icemask_cost, p.regularize_thk, p.mask_velsurf = 0, 0, 0, 1
+    p.usurf_cost, p.usurfobs_std = 1, 1.5
+    p.n_usurf = float((g[f"{tag}_icemaskobs"] > 0.5).sum())
+    nan = torch.full_like(d["thk"], float("nan"))
+    zero = torch.zeros_like(d["thk"])
+    g_us = torch.empty_like(d["thk"])
+    costs, _, _, _ = K.assim_cost_grad(d["thk"], d["usurf"], zero, zero, nan, nan, nan, zero, d["icemaskobs"], None, dx,
+                                       p, usurfobs=d["usurfobs"], g_us=g_us)
+    c = costs.cpu().numpy()
+    close(c[5], g[f"{tag}_misfit_usurf"])
+    close(c[4], g[f"{tag}_regu_thk_topg"])
+    close(g_us.cpu().numpy(), g[f"{tag}_g_usurf"] + g[f"{tag}_g_usurf_regu_thk"])

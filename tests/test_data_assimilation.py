@@ -42,7 +42,7 @@ def test_density_matrix_counts():
 
 
 def test_unsupported_configurations_raise():
-    for over in ({"control_list": ["thk", "slidingco"]}, {"cost_list": ["velsurf", "usurf"]}, {"divflux": {"method": "flux-limiter"}},
+    for over in ({"control_list": ["thk", "topg"]}, {"control_list": ["thk", "thk"]}, {"cost_list": ["velsurf", "vol"]}, {"divflux": {"method": "flux-limiter"}},
                  {"optimization": {"method": "L-BFGS"}}, {"cook": {"infer_params": True}}):
         cfg = default_cfg({"data_assimilation": over})
         with pytest.raises(NotImplementedError):

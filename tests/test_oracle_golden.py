@@ -260,3 +260,45 @@ def test_divflux_cost_terms(golden, tag, method, kind):
     for a, k in [(gu, "g_u"), (gv, "g_v"), (gh, "g_h")]:
         ref = g[f"{key}_{k}"]
         np.testing.assert_allclose(a.numpy(), ref, rtol=tol, atol=tol * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+def test_other_control_cost_terms(golden, tag):
+    """regu_slidingco (isotropic and anisotropic), regu_arrhenius,
+    misfit_usurf, the slidingco / arrhenius penalties and regu_thk's usurf
+    gradient, against the reference source."""
+    g = golden("assim_controls")
+    t = {k: torch.as_tensor(g[f"{tag}_{k}"]) for k in ("thk", "usurf", "slidingco", "arrhenius", "usurfobs",
+                                                       "icemaskobs")}
+    dx = float(g[f"{tag}_dx"])
+    tol = 1e-12 if tag == "f64" else 2e-5
+
+    def check(c, gr, kc, kg, tol=tol):
+        np.testing.assert_allclose(float(c.detach()), float(g[kc]), rtol=tol)
+        ref = g[kg]
+        np.testing.assert_allclose(gr.numpy(), ref, rtol=tol, atol=tol * np.abs(ref).max())
+
+    for mode, aniso in (("sliso", 1.0), ("slaniso", 0.3)):
+        s = t["slidingco"].clone().requires_grad_(True)
+        flow = (torch.as_tensor(g[f"{tag}_{mode}_flowdirx"]), torch.as_tensor(g[f"{tag}_{mode}_flowdiry"]))
+        c = O.da_regu_field(s, dx, 7.0, aniso, flow)
+        check(c, torch.autograd.grad(c, s)[0], f"{tag}_{mode}_regu_slidingco", f"{tag}_{mode}_g_slidingco")
+    a = t["arrhenius"].clone().requires_grad_(True)
+    c = O.da_regu_field(a, dx, 2.0)
+    check(c, torch.autograd.grad(c, a)[0], f"{tag}_regu_arrhenius", f"{tag}_g_arrhenius")
+    c = O.da_penalty(a, 1.0)
+    check(c, torch.autograd.grad(c, a)[0], f"{tag}_pen_arrhenius", f"{tag}_g_pen_arrhenius")
+    s = t["slidingco"].clone().requires_grad_(True)
+    c = O.da_penalty(s, 0.0)
+    check(c, torch.autograd.grad(c, s)[0], f"{tag}_pen_slidingco", f"{tag}_g_pen_slidingco")
+    u = t["usurf"].clone().requires_grad_(True)
+    c = O.da_misfit_usurf(u, t["usurfobs"], t["icemaskobs"], 1.5)
+    check(c, torch.autograd.grad(c, u)[0], f"{tag}_misfit_usurf", f"{tag}_g_usurf")
+    u = t["usurf"].clone().requires_grad_(True)
+    p = O.AssimParams(regu_thk=10.0, smooth_anisotropy_factor=1.0, to_regularize="topg")
+    c = O.da_costs(t["thk"], u, t["thk"] * 0, t["thk"] * 0, t["thk"] * 0, t["thk"] * 0,
+                   torch.full_like(t["thk"], float("nan")), t["thk"] * 0, t["icemaskobs"], t["icemaskobs"], None, dx,
+                   p)["thk_regu"]
+    # the reference sums the ice-mask area in float32 (tf.where(..., 1.0, 0.0)): 1e-10 in FP64
+    check(c, torch.autograd.grad(c, u)[0], f"{tag}_regu_thk_topg", f"{tag}_g_usurf_regu_thk",
+          tol=max(tol, 1e-10))
