@@ -472,7 +472,8 @@ def plain_kernels(args, peaks, n=10):
     Algorithmic bytes per node: energy 4(2 Nz + 4); energy + adjoint
     4(2 Nz + 4) + 8 Nz; one fused Adam iteration 4(12 Nz + 4); transport
     (reads ubar, vbar, thk, topg, smb; writes thk, usurf, lsurf, divflux) 36;
-    vertical velocity, either method (reads U, V, topg, thk; writes W) 4(3 Nz + 2)."""
+    vertical velocity, either method (reads U, V, topg, thk; writes W) 4(3 Nz + 2);
+    velocity reduction (reads U, V; writes velbar, velbase, velsurf) 4(2 Nz + 6)."""
     import torch
     from igm_b200 import kernels as K
     from igm_b200.solver import DeviceAdamSolver
@@ -505,6 +506,8 @@ def plain_kernels(args, peaks, n=10):
          lambda: K.vertical_velocity(U, V, topg, f[0], levels, w, 50.0, out=W)),
         ("vertical_velocity_incompressibility", "vert_flow_incomp_kernel (incompressibility v2)", 4 * (3 * nz + 2),
          lambda: K.vertical_velocity(U, V, topg, f[0], levels, w, 50.0, out=W, method="incompressibility")),
+        ("velocity_reduce", "velocity_reduce_kernel (velbar, velbase, velsurf, CFL max)", 4 * (2 * nz + 6),
+         lambda: K.velocity_reduce(U, V, f[0], w, mask=False)),
     ]
     peak = peaks.get("hbm_gbs", 6650.0)
     out = {}

@@ -32,6 +32,9 @@ struct AssimArgs {
   T* g_us;   // dC/dusurf or NULL
   int field_only;  // the regularisation and positivity penalty of one field (thk holds it)
   T pos_thr;       // field-only: the penalty applies below this value
+  // regularisation weights: 1 (half sums) or, fix_opti_normalization_issue, the means' 1/count
+  T kx, ky, kcell;
+  double kconv;    // the convexity term: 1, or 0.5 / (ny nx)
   double* partials;  // [gridDim.x][kNCost]
 };
 
@@ -82,7 +85,7 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
   const T kv = (T)(1.0 / (p.velsurfobs_std * p.velsurfobs_std * p.n_vel));
   const T kt = (T)(1.0 / (p.thkobs_std * p.thkobs_std * p.n_thk));
   const T kp = (T)(2e10 / ((double)ny * nx));
-  const T kg = (T)(p.regu_thk * p.gamma);
+  const T kg = (T)(p.regu_thk * p.gamma * a.kconv);
   auto load = [&](int j, bool full) {
     AssimRow<T> r;
     const bool ok = col && j < ny;
@@ -120,11 +123,12 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
         const T dbdx = ((f0r - f0) + (f1r - f1)) * hr;
         const T dbdy = ((f1 - f0) + (f1r - f0r)) * hr;
         const T A = dbdx * r.fx + dbdy * r.fy, B = dbdx * r.fy - dbdy * r.fx;
-        const T gdx = w * (s_a * A * r.fx + s_b * B * r.fy);
-        const T gdy = w * (s_a * A * r.fy - s_b * B * r.fx);
+        const T wc = w * a.kcell;
+        const T gdx = wc * (s_a * A * r.fx + s_b * B * r.fy);
+        const T gdy = wc * (s_a * A * r.fy - s_b * B * r.fx);
         k.P = gdx + gdy;
         k.M = gdx - gdy;
-        k.cost = s_a * A * A * T(0.5) + s_b * B * B * T(0.5);
+        k.cost = (s_a * A * A * T(0.5) + s_b * B * B * T(0.5)) * a.kcell;
       }
     } else if (col && j >= 0) {
       if (c + 1 < nx) k.dxp = (f0r - f0) * rdx;
@@ -151,7 +155,7 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
       gf = hr * ((Ml - k.P) + (Pl - prev.M));
     } else {
       const T dxm = __shfl_up_sync(0xffffffffu, k.dxp, 1);
-      gf = w * rdx * ((dxm - k.dxp) + (prev.dyp - k.dyp));
+      gf = w * rdx * (a.kx * (dxm - k.dxp) + a.ky * (prev.dyp - k.dyp));
     }
     if (out && fo) {
       // one control field (regu_slidingco.py:8-52, regu_arrhenius.py:5-24, total_cost.py:45-54):
@@ -163,7 +167,8 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
         acc[kCPos] += (double)(f * f);
         g += kp * f;
       }
-      acc[kCReg] += aniso ? (double)k.cost : 0.5 * ((double)k.dxp * k.dxp + (double)k.dyp * k.dyp);
+      acc[kCReg] += aniso ? (double)k.cost
+                          : 0.5 * ((double)a.kx * k.dxp * k.dxp + (double)a.ky * k.dyp * k.dyp);
       a.g_thk[o] = g;
     } else if (out) {
       const size_t o = (size_t)j * nx + cc;
@@ -208,9 +213,10 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
       }
       // regularisation (regu_thk.py:8-70): smoothness cost of cell (j, c) or of this node's
       // forward differences, the convexity term
-      const double rc = aniso ? (double)k.cost : 0.5 * ((double)k.dxp * k.dxp + (double)k.dyp * k.dyp);
+      const double rc = aniso ? (double)k.cost
+                              : 0.5 * ((double)a.kx * k.dxp * k.dxp + (double)a.ky * k.dyp * k.dyp);
       if (thk_ctl) {
-        acc[kCReg] += rc - sc.gamma * (double)th;
+        acc[kCReg] += rc - sc.gamma * a.kconv * (double)th;
         g += (reg_thk ? gf : -gf) - kg;
       }
       a.g_thk[o] = g;
@@ -348,6 +354,15 @@ static int grid_n(size_t n) {
 }
 
 template <typename T>
+static void set_norm(AssimArgs<T>& a, int fix_normalization) {
+  const double ny = a.ny, nx = a.nx;
+  a.kx = fix_normalization ? (T)(1.0 / (ny * (nx - 1))) : T(1);
+  a.ky = fix_normalization ? (T)(1.0 / ((ny - 1) * nx)) : T(1);
+  a.kcell = fix_normalization ? (T)(1.0 / ((ny - 1) * (nx - 1))) : T(1);
+  a.kconv = fix_normalization ? 0.5 / (ny * nx) : 1.0;
+}
+
+template <typename T>
 static int march_launch(AssimArgs<T>& a, const AssimScales& sc, int n_parts, double* costs, cudaStream_t st) {
   // segments of rows sized for about 32 resident warps per SM, at least 8 rows; the
   // warps stride over the (strip, segment) tasks so the grid fits the partials
@@ -387,13 +402,14 @@ static int cost_grad_t(int ny, int nx, double dx, const void* thk, const void* u
   sc.c_reg = p->regu_thk;
   sc.c_us = p->usurf_cost ? 0.5 / (p->usurfobs_std * p->usurfobs_std * (p->n_usurf > 0 ? p->n_usurf : 1.0)) : 0.0;
   sc.gamma = p->gamma;
+  set_norm(a, p->fix_normalization);
   return march_launch<T>(a, sc, n_parts, costs, st);
 }
 
 template <typename T>
 static int field_regu_t(int ny, int nx, double dx, const void* field, const void* fdx, const void* fdy, double regu,
-                        double aniso, int penalty, double pos_thr, void* grad, double* partials, int n_parts,
-                        double* costs, cudaStream_t st) {
+                        double aniso, int penalty, double pos_thr, int fix_normalization, void* grad,
+                        double* partials, int n_parts, double* costs, cudaStream_t st) {
   AssimArgs<T> a{};
   a.ny = ny; a.nx = nx; a.dx = (T)dx;
   a.thk = (const T*)field; a.fdx = (const T*)fdx; a.fdy = (const T*)fdy;
@@ -409,6 +425,7 @@ static int field_regu_t(int ny, int nx, double dx, const void* field, const void
   AssimScales sc{};
   sc.c_pen = 1e10 / ((double)ny * nx);
   sc.c_reg = regu;
+  set_norm(a, fix_normalization);
   return march_launch<T>(a, sc, n_parts, costs, st);
 }
 
@@ -791,8 +808,8 @@ extern "C" int igm_assim_cost_grad(int dtype, int ny, int nx, double dx, const v
 
 extern "C" int igm_assim_field_regu(int dtype, int ny, int nx, double dx, const void* field, const void* flowdirx,
                                     const void* flowdiry, double regu, double aniso_factor, int penalty,
-                                    double penalty_threshold, void* grad, double* partials, int n_parts,
-                                    double* costs, void* stream) {
+                                    double penalty_threshold, int fix_normalization, void* grad, double* partials,
+                                    int n_parts, double* costs, void* stream) {
   IGM_CHECK_ARG(ny >= 2 && nx >= 2 && dx > 0, IGM_ERR_BAD_SHAPE, "igm_assim_field_regu: bad shape %dx%d", ny, nx);
   IGM_CHECK_ARG(field && grad && partials && costs && n_parts >= 1 && aniso_factor > 0, IGM_ERR_BAD_ARGUMENT,
                 "igm_assim_field_regu: bad argument");
@@ -801,10 +818,10 @@ extern "C" int igm_assim_field_regu(int dtype, int ny, int nx, double dx, const 
   cudaStream_t st = as_stream(stream);
   if (dtype == IGM_F32)
     return field_regu_t<float>(ny, nx, dx, field, flowdirx, flowdiry, regu, aniso_factor, penalty, penalty_threshold,
-                               grad, partials, n_parts, costs, st);
+                               fix_normalization, grad, partials, n_parts, costs, st);
   if (dtype == IGM_F64)
     return field_regu_t<double>(ny, nx, dx, field, flowdirx, flowdiry, regu, aniso_factor, penalty,
-                                penalty_threshold, grad, partials, n_parts, costs, st);
+                                penalty_threshold, fix_normalization, grad, partials, n_parts, costs, st);
   set_error("igm_assim_field_regu: unknown dtype %d", dtype);
   return IGM_ERR_BAD_ARGUMENT;
 }

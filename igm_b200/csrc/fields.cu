@@ -35,18 +35,45 @@ __global__ void __launch_bounds__(256) velocity_reduce_kernel(const VelArgs<T> a
     const size_t base = b * a.nz * plane + p;
     const bool keep = !a.mask || a.thk[idx] > T(0);
     T su = 0, sv = 0, u0 = 0, v0 = 0, u1 = 0, v1 = 0;
-    for (int k = 0; k < a.nz; ++k) {
-      T u = a.U[base + k * plane], v = a.V[base + k * plane];
-      if (!keep) {
-        u = T(0);
-        v = T(0);
-        a.U[base + k * plane] = u;
-        a.V[base + k * plane] = v;
+    if (!keep) {
+      // masked column: zeros, nothing to read
+      for (int k = 0; k < a.nz; ++k) {
+        a.U[base + k * plane] = T(0);
+        a.V[base + k * plane] = T(0);
       }
-      su += u * a.w[k];
-      sv += v * a.w[k];
-      if (k == 0) { u0 = u; v0 = v; }
-      if (k == a.nz - 1) { u1 = u; v1 = v; }
+    } else {
+      // the column's loads issued eight levels at a time (no store in this branch, so they need
+      // not wait for one another); the sums in level order, as the reference's reduce_sum
+      for (int k0 = 0; k0 < a.nz; k0 += 8) {
+        T u[8], v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int k = k0 + q;
+          u[q] = k < a.nz ? a.U[base + k * plane] : T(0);
+          v[q] = k < a.nz ? a.V[base + k * plane] : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int k = k0 + q;
+          if (k < a.nz) {
+            su += u[q] * a.w[k];
+            sv += v[q] * a.w[k];
+          }
+        }
+        if (k0 == 0) {
+          u0 = u[0];
+          v0 = v[0];
+        }
+        const int kl = a.nz - 1 - k0;
+        if (kl >= 0 && kl < 8) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (q == kl) {
+              u1 = u[q];
+              v1 = v[q];
+            }
+        }
+      }
     }
     if (a.ubar) a.ubar[idx] = su;
     if (a.vbar) a.vbar[idx] = sv;

@@ -34,8 +34,8 @@ reference (matplotlib) are not drawn.
 Supported: control_list within thk, usurf, slidingco (log_slidingco or not),
 arrhenius (dim_arrhenius 2); cost_list within velsurf, thk, icemask, usurf,
 divfluxobs, divfluxfcz (the flux-divergence terms, with or without
-force_zero_sum); method ADAM; sole_mask, fix_opti_normalization_issue,
-include_low_speed_term, cook.infer_params and pertubate off; divflux.method
+force_zero_sum); fix_opti_normalization_issue on or off; method ADAM;
+sole_mask, include_low_speed_term, cook.infer_params and pertubate off; divflux.method
 upwind or centered.  Anything else raises NotImplementedError.
 """
 
@@ -72,7 +72,7 @@ def _check_supported(cfg):
         bad.append(f"cost terms {extra} (only velsurf, thk, icemask, usurf, divfluxobs, divfluxfcz)")
     if o.method != "ADAM":
         bad.append(f"optimization.method={o.method!r} (only 'ADAM')")
-    for key in ("sole_mask", "fix_opti_normalization_issue", "pertubate"):
+    for key in ("sole_mask", "pertubate"):
         if bool(o.get(key, False)):
             bad.append(f"optimization.{key}")
     if bool(da.fitting.include_low_speed_term):
@@ -177,6 +177,7 @@ class _Assim:
         p.usurfobs_std = float(f.usurfobs_std)
         p.n_usurf = max(1.0, float((self.icemaskobs > 0.5).sum().item()))
         p.no_thk_control = int("thk" not in self.controls)
+        p.fix_normalization = int(bool(o.fix_opti_normalization_issue))
         self.params = p
         self.log_slidingco = bool(f.log_slidingco)
         pen = bool(p.penalty)
@@ -311,7 +312,8 @@ def optimize_update(cfg, state, cost, i):
         pen = bool(a.params.penalty) and not (c == "slidingco" and a.log_slidingco)
         K.assim_field_regu(S.get(state, c).contiguous(), a.dx, float(getattr(r, c)), aniso,
                            flow if aniso != 1.0 else None, penalty=pen, threshold=1.0 if c == "arrhenius" else 0.0,
-                           grad=g, costs=a.field_hist[c][i], partials=a.partials)
+                           grad=g, costs=a.field_hist[c][i], partials=a.partials,
+                           fix_normalization=bool(a.params.fix_normalization))
     model.backward(buf, 1, a.ny, a.nx, a.dU, a.dV, field_grad=a.field_grad, param_grads=False)
     direct = {"thk": a.g_thk, "usurf": a.g_us, **a.g_field}
     for k, c in enumerate(a.controls):

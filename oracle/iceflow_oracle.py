@@ -707,6 +707,7 @@ class AssimParams:
     to_regularize: str = "topg"
     penalty: bool = True
     icemask_cost: bool = True
+    fix_normalization: bool = False  # optimization.fix_opti_normalization_issue
 
 
 def getmag(u, v):
@@ -766,17 +767,28 @@ def da_costs(thk, usurf, uvelsurf, vvelsurf, uobs, vobs, thkobs, dens_thkobs, ic
     if f == 1:
         dbdx = (field[:, 1:] - field[:, :-1]) / dx
         dbdy = (field[1:, :] - field[:-1, :]) / dx
-        cost["thk_regu"] = p.regu_thk * (torch.sum(dbdx ** 2) / 2 + torch.sum(dbdy ** 2) / 2 - gamma * torch.sum(thk))
+        if p.fix_normalization:
+            cost["thk_regu"] = p.regu_thk * 0.5 * (torch.mean(dbdx ** 2) + torch.mean(dbdy ** 2)
+                                                   - gamma * torch.mean(thk))
+        else:
+            cost["thk_regu"] = p.regu_thk * (torch.sum(dbdx ** 2) / 2 + torch.sum(dbdy ** 2) / 2
+                                             - gamma * torch.sum(thk))
     else:
         fx, fy = flowdir
         dbdx = (field[:, 1:] - field[:, :-1]) / dx
         dbdx = (dbdx[1:, :] + dbdx[:-1, :]) / 2.0
         dbdy = (field[1:, :] - field[:-1, :]) / dx
         dbdy = (dbdy[:, 1:] + dbdy[:, :-1]) / 2.0
-        cost["thk_regu"] = p.regu_thk * (
-            (1.0 / np.sqrt(f)) * torch.sum((dbdx * fx + dbdy * fy) ** 2) / 2
-            + np.sqrt(f) * torch.sum((dbdx * fy - dbdy * fx) ** 2) / 2
-            - torch.sum(gamma * thk))
+        if p.fix_normalization:
+            cost["thk_regu"] = p.regu_thk * 0.5 * (
+                (1.0 / np.sqrt(f)) * torch.mean((dbdx * fx + dbdy * fy) ** 2)
+                + np.sqrt(f) * torch.mean((dbdx * fy - dbdy * fx) ** 2)
+                - torch.mean(gamma * thk))
+        else:
+            cost["thk_regu"] = p.regu_thk * (
+                (1.0 / np.sqrt(f)) * torch.sum((dbdx * fx + dbdy * fy) ** 2) / 2
+                + np.sqrt(f) * torch.sum((dbdx * fy - dbdy * fx) ** 2) / 2
+                - torch.sum(gamma * thk))
     return cost
 
 
@@ -910,9 +922,9 @@ def da_optimize_step(fields, dx, weights, biases, Nz, vert_weight, obs, p: Assim
         if "arrhenius" in mc.controls:
             cost["arrhenius_positive"] = da_penalty(ar, 1.0)
     if "slidingco" in mc.controls:
-        cost["slid_regu"] = da_regu_field(sl, dx, mc.regu_slidingco, mc.aniso_sl, flow)
+        cost["slid_regu"] = da_regu_field(sl, dx, mc.regu_slidingco, mc.aniso_sl, flow, normalize=p.fix_normalization)
     if "arrhenius" in mc.controls:
-        cost["arrh_regu"] = da_regu_field(ar, dx, mc.regu_arrhenius)
+        cost["arrh_regu"] = da_regu_field(ar, dx, mc.regu_arrhenius, normalize=p.fix_normalization)
     total = sum(cost.values())
     grads = torch.autograd.grad(total, [var[c] for c in mc.controls])
     inside = obs["icemaskobs"] > 0.5
@@ -1039,24 +1051,26 @@ def da_cost_divflux(kind, ubar, vbar, thk, dx, icemaskobs, divfluxobs=None, usur
     return c
 
 
-def da_regu_field(f, dx, weight, aniso=1.0, flowdir=None):
+def da_regu_field(f, dx, weight, aniso=1.0, flowdir=None, normalize=False):
     """regu_slidingco (cost_terms/regu_slidingco.py:8-52) and regu_arrhenius
     (cost_terms/regu_arrhenius.py:5-24) with sole_mask and
     fix_opti_normalization_issue off: weight (l2_loss(df/dx) + l2_loss(df/dy))
     on the node differences (aniso == 1), or the cell-centred differences
     split along and across the flow direction weighted 1/sqrt(aniso) and
-    sqrt(aniso)."""
+    sqrt(aniso); with ``normalize`` (fix_opti_normalization_issue) weight 0.5
+    times the means instead of the half sums."""
+    red = (lambda x: 0.5 * torch.mean(x)) if normalize else (lambda x: torch.sum(x) / 2)
     if aniso == 1.0:
         dadx = (f[:, 1:] - f[:, :-1]) / dx
         dady = (f[1:, :] - f[:-1, :]) / dx
-        return weight * (torch.sum(dadx ** 2) / 2 + torch.sum(dady ** 2) / 2)
+        return weight * (red(dadx ** 2) + red(dady ** 2))
     dadx = (f[:, 1:] - f[:, :-1]) / dx
     dadx = (dadx[1:, :] + dadx[:-1, :]) / 2.0
     dady = (f[1:, :] - f[:-1, :]) / dx
     dady = (dady[:, 1:] + dady[:, :-1]) / 2.0
     fx, fy = flowdir
-    return weight * ((1.0 / np.sqrt(aniso)) * torch.sum((dadx * fx + dady * fy) ** 2) / 2
-                     + np.sqrt(aniso) * torch.sum((dadx * fy - dady * fx) ** 2) / 2)
+    return weight * ((1.0 / np.sqrt(aniso)) * red((dadx * fx + dady * fy) ** 2)
+                     + np.sqrt(aniso) * red((dadx * fy - dady * fx) ** 2))
 
 
 def da_penalty(f, threshold):

@@ -539,6 +539,27 @@ def assim_control_cases():
                     f"{tag}_g_pen_slidingco": gps, f"{tag}_pen_arrhenius": cp_a, f"{tag}_g_pen_arrhenius": gpa,
                     f"{tag}_misfit_usurf": cu, f"{tag}_g_usurf": gu, f"{tag}_regu_thk_topg": crt,
                     f"{tag}_g_usurf_regu_thk": gru})
+        # fix_opti_normalization_issue: the regularisations as means
+        da["optimization"]["fix_opti_normalization_issue"] = True
+        for aniso in (1.0, 0.2):
+            da["regularization"]["smooth_anisotropy_factor"] = aniso
+            da["regularization"]["smooth_anisotropy_factor_sl"] = 0.3 if aniso != 1.0 else 1.0
+            cfg.processes.data_assimilation = ns(da)
+            key = f"{tag}_norm_{'aniso' if aniso != 1.0 else 'iso'}"
+            th = thk.clone().requires_grad_(True)
+            st2 = types.SimpleNamespace(thk=th, usurf=usurf, slidingco=sl.clone().requires_grad_(True),
+                                        arrhenius=ar.clone().requires_grad_(True), icemaskobs=icemaskobs,
+                                        icemask=icemaskobs, dx=dx, flowdirx=st.flowdirx, flowdiry=st.flowdiry)
+            c_t = rt.regu_thk(cfg, st2)
+            (g_t,) = torch.autograd.grad(c_t, [th])
+            c_s = rs.regu_slidingco(cfg, st2)
+            (g_s,) = torch.autograd.grad(c_s, [st2.slidingco])
+            c_a = ra.regu_arrhenius(cfg, st2)
+            (g_a,) = torch.autograd.grad(c_a, [st2.arrhenius])
+            out.update({f"{key}_regu_thk": c_t, f"{key}_g_thk": g_t, f"{key}_regu_slidingco": c_s,
+                        f"{key}_g_slidingco": g_s, f"{key}_regu_arrhenius": c_a, f"{key}_g_arrhenius": g_a})
+        da["optimization"]["fix_opti_normalization_issue"] = False
+        da["regularization"]["smooth_anisotropy_factor"] = 0.2
     save("assim_controls", out)
 
 

@@ -42,8 +42,8 @@ def twin_glacier(ny=40, nx=70, dx=100.0):
     return tongue_glacier(ny, nx, dx, seed=3)
 
 
-def make_cfg(nbitmax, aniso=0.2, to_regularize="topg"):
-    return default_cfg({
+def make_cfg(nbitmax, aniso=0.2, to_regularize="topg", normalize=False):
+    cfg = default_cfg({
         "iceflow": {"numerics": {"Nz": NZ},
                     "emulator": {"pretrained": False, "retrain_freq": 0, "input_scales": SCALES,
                                  "output_scale": OUT, "seed": 1,
@@ -53,6 +53,8 @@ def make_cfg(nbitmax, aniso=0.2, to_regularize="topg"):
                                                  "to_regularize": to_regularize},
                               "output": {"freq": 10}},
     })
+    cfg.processes.data_assimilation.optimization.fix_opti_normalization_issue = normalize
+    return cfg
 
 
 def twin_state(cfg, g):
@@ -85,7 +87,8 @@ def oracle_setup(cfg, st):
     r, f = da.regularization, da.fitting
     p = O.AssimParams(velsurfobs_std=f.velsurfobs_std, velsurfobs_thr=f.velsurfobs_thr, thkobs_std=f.thkobs_std,
                       regu_thk=r.thk, convexity_weight=r.convexity_weight, convexity_power=r.convexity_power,
-                      smooth_anisotropy_factor=r.smooth_anisotropy_factor, to_regularize=r.to_regularize)
+                      smooth_anisotropy_factor=r.smooth_anisotropy_factor, to_regularize=r.to_regularize,
+                      fix_normalization=bool(da.optimization.fix_opti_normalization_issue))
     ctl = O.AssimControl(step_size=da.optimization.step_size, step_size_decay=da.optimization.step_size_decay,
                          scaling_thk=da.scaling.thk)
     opt = O.KerasLegacyAdam(lr=da.optimization.step_size, epsilon=da.optimization.optimizer_epsilon,
@@ -101,10 +104,11 @@ def oracle_step(cfg, st, thk, setup, i, divflux_cost=None):
                                 bf16=True, out_scale=OUT, input_scales=SCALES, divflux_cost=divflux_cost)
 
 
-@pytest.mark.parametrize("aniso,to_regularize", [(0.2, "topg"), (1.0, "thk")])
-def test_first_iterations_match_oracle(tmp_path, monkeypatch, aniso, to_regularize):
+@pytest.mark.parametrize("aniso,to_regularize,normalize", [(0.2, "topg", False), (1.0, "thk", False),
+                                                            (0.2, "topg", True)])
+def test_first_iterations_match_oracle(tmp_path, monkeypatch, aniso, to_regularize, normalize):
     monkeypatch.chdir(tmp_path)
-    cfg = make_cfg(2, aniso, to_regularize)
+    cfg = make_cfg(2, aniso, to_regularize, normalize)
     g = twin_glacier()
     st = twin_state(cfg, g)
     setup = oracle_setup(cfg, st)
@@ -219,9 +223,11 @@ def test_divflux_costs_in_the_loop_match_oracle(tmp_path, monkeypatch, kind, met
         thk_o = st.thk.detach().cpu().clone()
 
 
-@pytest.mark.parametrize("controls,log_sl", [(["thk", "slidingco"], False), (["thk", "slidingco"], True),
-                                             (["thk", "arrhenius"], False), (["thk", "usurf"], False)])
-def test_other_controls_in_the_loop_match_oracle(tmp_path, monkeypatch, controls, log_sl):
+@pytest.mark.parametrize("controls,log_sl,normalize", [(["thk", "slidingco"], False, False),
+                                                       (["thk", "slidingco"], True, False),
+                                                       (["thk", "arrhenius"], False, True),
+                                                       (["thk", "usurf"], False, False)])
+def test_other_controls_in_the_loop_match_oracle(tmp_path, monkeypatch, controls, log_sl, normalize):
     """Several controls at once (one Adam variable each, clipped separately):
     three iterations against the oracle's da_optimize_step -- the costs, each
     variable's gradient, and each control's step (relative to its size, as
@@ -229,7 +235,7 @@ def test_other_controls_in_the_loop_match_oracle(tmp_path, monkeypatch, controls
     no mask, so off the ice its gradient is the small smoothness term alone and
     Adam's steps there are proportional to it)."""
     monkeypatch.chdir(tmp_path)
-    cfg = make_cfg(2)
+    cfg = make_cfg(2, normalize=normalize)
     da = cfg.processes.data_assimilation
     da.control_list = list(controls)
     da.fitting.log_slidingco = log_sl
