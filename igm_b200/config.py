@@ -91,6 +91,13 @@ DEFAULTS = {
     "vert_flow": {"version": 2, "method": "kinematic"},
     "time": {"start": 2000.0, "end": 2100.0, "save": 10.0, "cfl": 0.3, "step_max": 1.0},
     "smb_simple": {"update_freq": 1.0, "file": "param.txt", "array": []},
+}
+
+# Processes whose configuration is present only when a run uses them (the
+# reference composes cfg.processes from the selected processes, and the
+# emulator's pertubate option tests for data_assimilation's presence):
+# default_cfg adds them when the overrides or ``with_processes`` name them.
+OPTIONAL = {
     "data_assimilation": {
         "control_list": ["thk"],
         "cost_list": ["velsurf", "thk", "icemask"],
@@ -141,9 +148,15 @@ def _merge(base: dict, over: dict):
             base[k] = v
 
 
-def default_cfg(overrides: dict | None = None, **dotted):
-    """``default_cfg({"iceflow": {"method": "solved"}}, **{"iceflow.numerics.Nz": 5})``"""
+def default_cfg(overrides: dict | None = None, with_processes=(), **dotted):
+    """``default_cfg({"iceflow": {"method": "solved"}}, **{"iceflow.numerics.Nz": 5})``;
+    the optional processes (data_assimilation) are included when ``overrides``
+    or ``with_processes`` name them."""
     d = copy.deepcopy(DEFAULTS)
+    for name, block in OPTIONAL.items():
+        if name in with_processes or (overrides and name in overrides) or any(
+                k.split(".")[0] == name for k in dotted):
+            d[name] = copy.deepcopy(block)
     if overrides:
         _merge(d, overrides)
     for path, val in dotted.items():

@@ -6,7 +6,8 @@ and diagnostic/diagnostic.py), on the device.
   (emulate.py:116-152).
 * ``update_iceflow_emulator``: physics-informed retraining by minimising the
   Blatter-Pattyn energy of the emulated velocities, one Adam step per patch
-  (split_into_patches, emulate.py:155-308), gated by retrain_freq / warm_up_it.
+  (split_into_patches, emulate.py:155-308), gated by retrain_freq / warm_up_it,
+  optionally on the perturbed copies of pertubate_X (emulate.py:310-328).
 * ``update_iceflow_diagnostic``: every 10 model years the plain solver is run
   from the emulated velocities and the L1/L2 velbar misfit is logged
   (diagnostic.py:34-84).
@@ -132,31 +133,57 @@ def update_iceflow_emulator(cfg, state, it, pertubate=False):
     warm_up = int(it <= e.warm_up_it)
     if not (warm_up or run_it):
         return
-    if pertubate:
-        raise NotImplementedError("emulator.pertubate is not supported")
     model: CNN = state.iceflow_model
     f = _fields(state)
     ny, nx = f[0].shape
     wins, ly, lx = _patch_windows(ny, nx, int(e.framesizemax))
+    copies = 1
+    if pertubate:
+        f, copies = _pertubate_fields(cfg, f)
     nbit, lr = (int(e.nbit_init), float(e.lr_init)) if warm_up else (int(e.nbit), float(e.lr))
     phys = P.physics(cfg)
     dx = P._dx(state)
     state.COST_EMULATOR = []
     state.GRAD_EMULATOR = []
     parallel = e.split_patch_method == "parrallel"
+    # a patch's batch: its window in each (perturbed) copy, the copies stacked along y
+    batch = lambda ws: [(k * ny + y0, x0) for (y0, x0) in ws for k in range(copies)]  # noqa: E731
     for _ in range(nbit):
         sums = []
         if parallel:
-            sums.append(train_step(model, f, dx, wins, ly, lx, state.dzeta, phys, lr, state.opti_retrain))
+            sums.append(train_step(model, f, dx, batch(wins), ly, lx, state.dzeta, phys, lr, state.opti_retrain))
         else:
             for i, win in enumerate(wins):
                 lr_i = lr * (e.lr_decay ** (i / 1000)) if e.lr_decay < 1 else lr
-                sums.append(train_step(model, f, dx, [win], ly, lx, state.dzeta, phys, lr_i, state.opti_retrain))
-        count = (ly - 1) * (lx - 1) * (len(wins) if parallel else 1)
+                sums.append(train_step(model, f, dx, batch([win]), ly, lx, state.dzeta, phys, lr_i,
+                                       state.opti_retrain))
+        count = (ly - 1) * (lx - 1) * copies * (len(wins) if parallel else 1)
         state.COST_EMULATOR.append(float(torch.stack(sums).sum(1).sum().item()) / count)
     model.check_errors()
     if len(e.save_cost) > 0:
         np.savetxt(e.save_cost + "-" + str(it) + ".dat", np.array(state.COST_EMULATOR), fmt="%5.10f")
+
+
+def _pertubate_fields(cfg, f):
+    """pertubate_X (emulate.py:310-328): the input and, for each perturbed
+    field, copies with that field scaled by 1.2 and 0.8 -- the fields of
+    data_assimilation's control_list when that process is configured, else
+    thk and usurf -- stacked along y (each copy ny rows).  Returns (stacked
+    [thk, usurf, arrhenius, slidingco], number of copies)."""
+    names = ["thk", "usurf", "arrhenius", "slidingco"]
+    if hasattr(cfg.processes, "data_assimilation"):
+        which = [n for n in names if n in list(cfg.processes.data_assimilation.control_list)]
+    else:
+        which = ["thk", "usurf"]
+    copies = [list(f)]
+    for n in which:
+        c = names.index(n)
+        for s in (1.2, 0.8):
+            g = list(f)
+            g[c] = f[c] * s
+            copies.append(g)
+    stacked = [torch.cat([cp[c] for cp in copies], 0).contiguous() for c in range(4)]
+    return stacked, len(copies)
 
 
 def initialize_iceflow_diagnostic(cfg, state):

@@ -35,7 +35,7 @@ Supported: control_list within thk, usurf, slidingco (log_slidingco or not),
 arrhenius (dim_arrhenius 2); cost_list within velsurf, thk, icemask, usurf,
 divfluxobs, divfluxfcz (the flux-divergence terms, with or without
 force_zero_sum); fix_opti_normalization_issue on or off; method ADAM;
-sole_mask, include_low_speed_term, cook.infer_params and pertubate off; divflux.method
+sole_mask, include_low_speed_term and cook.infer_params off; divflux.method
 upwind or centered.  Anything else raises NotImplementedError.
 """
 
@@ -72,7 +72,7 @@ def _check_supported(cfg):
         bad.append(f"cost terms {extra} (only velsurf, thk, icemask, usurf, divfluxobs, divfluxfcz)")
     if o.method != "ADAM":
         bad.append(f"optimization.method={o.method!r} (only 'ADAM')")
-    for key in ("sole_mask", "pertubate"):
+    for key in ("sole_mask",):
         if bool(o.get(key, False)):
             bad.append(f"optimization.{key}")
     if bool(da.fitting.include_low_speed_term):

@@ -618,18 +618,40 @@ class EmulatorTraining:
     framesizemax: int = 750
 
 
+def pertubate_X(X, channels):
+    """pertubate_X (emulate.py:310-328): X and, for each channel in
+    ``channels``, copies with that channel scaled by 1.2 and 0.8, along the
+    batch axis."""
+    XX = [X]
+    for c in channels:
+        vec = torch.zeros(X.shape[-1], dtype=X.dtype)
+        vec[c] = 1.0
+        XX.append(X + X * vec * 0.2)
+        XX.append(X - X * vec * 0.2)
+    return torch.cat(XX, 0)
+
+
 def emulator_retrain(weights, biases, optimizer: KerasLegacyAdam, X, it, tr: EmulatorTraining,
-                     Nz, dzeta, ph: Physics | None = None, bf16=False):
-    """emulate.py:155-281 ("sequential" patches, no perturbation, no borders).
+                     Nz, dzeta, ph: Physics | None = None, bf16=False, pertubate_channels=None,
+                     input_scales=None, out_scale=1.0):
+    """emulate.py:155-281 ("sequential" patches, no borders).
 
     ``weights``/``biases`` are leaf tensors updated in place; X is
     [1, ny, nx, 5] (thk, usurf, arrhenius, slidingco, dX).  Returns the list
     of per-epoch summed costs, or None when this iteration does not retrain.
+    ``pertubate_channels``: the channels pertubate_X scales (the retraining
+    batch then holds 1 + 2 len(channels) samples per patch; each sample's
+    energy uses its own fields -- the reference's cost_shear.py:75-76
+    broadcasts dzeta[None, :, None, None] against thk [B, ny, nx], which
+    fails for a batch B > 1 other than Nz - 1, so this restates the intent).
+    ``input_scales`` multiply the network input only.
     """
     run_it = tr.retrain_freq > 0 and (it % tr.retrain_freq == 0)
     warm_up = int(it <= tr.warm_up_it)
     if not (warm_up or run_it):
         return None
+    if pertubate_channels:
+        X = pertubate_X(X, pertubate_channels)
     Xp = split_into_patches(X, tr.framesizemax)
     nbit, lr = (tr.nbit_init, tr.lr_init) if warm_up else (tr.nbit, tr.lr)
     optimizer.lr = lr
@@ -644,7 +666,9 @@ def emulator_retrain(weights, biases, optimizer: KerasLegacyAdam, X, it, tr: Emu
                 optimizer.lr = lr * (tr.lr_decay ** (i / 1000))
             Xi = Xp[i]
             ps = [p.detach().clone().requires_grad_(True) for p in params]
-            Y = cnn_forward(Xi, ps[0::2], ps[1::2], bf16=bf16)
+            Xin = Xi * torch.tensor(input_scales, dtype=Xi.dtype) if input_scales is not None else Xi
+            Y = cnn_forward(Xin, ps[0::2], ps[1::2], bf16=bf16, bf16_first=input_scales is None,
+                            out_scale=out_scale)
             U, V = Y_to_UV(Y, Nz)
             cost, _ = energy(U, V, Xi[..., 0], Xi[..., 1], Xi[..., 2], Xi[..., 3], Xi[0, 0, 0, 4], dzeta, ph)
             grads = torch.autograd.grad(cost, ps)

@@ -145,3 +145,47 @@ def test_input_field_gradient_matches_oracle():
     for c in range(4):
         e = rel_l2(G[c], go[c].numpy())
         assert e < 5e-2, (c, e)
+
+
+@pytest.mark.parametrize("with_da", [False, True])
+def test_perturbed_retraining_gradient_matches_oracle(with_da):
+    """Retraining on pertubate_X's copies (emulate.py:310-328): thk and usurf
+    scaled by 1.2 and 0.8 (without data assimilation), or the control fields
+    (with it: control_list [thk, slidingco]); the batch's energy and its
+    gradient against the oracle (relative L2 <= 5e-2, bf16 activations)."""
+    from igm_b200 import emulator as E
+    from igm_b200.config import default_cfg
+    from igm_b200.state import State
+    nl, nz, ny, nx, dx = 3, 4, 40, 70, 100.0
+    st, net, f = setup(nl, nz, ny, nx, seed=6)
+    ws, bs = oracle_params(net)
+    params = []
+    for w, b in zip(ws, bs):
+        params += [w.clone().requires_grad_(True), b.clone().requires_grad_(True)]
+    dz = O.compute_zeta_dzeta(O.compute_levels(nz, 4.0))[1]
+    over = {"iceflow": {"numerics": {"Nz": nz}, "emulator": {"retrain_freq": 1, "nbit": 1, "lr": 1e-3,
+                                                             "framesizemax": 1000}}}
+    if with_da:
+        over["data_assimilation"] = {"control_list": ["thk", "slidingco"]}
+    cfg = default_cfg(over)
+    s = State()
+    s.thk, s.usurf, s.arrhenius, s.slidingco = f
+    s.dx, s.dzeta = dx, dz.numpy()
+    s.iceflow_model = net
+    s.opti_retrain = E.EmulatorOptimizer(lr=1e-3, epsilon=1e-7, clipnorm=1.0)
+    E.update_iceflow_emulator(cfg, s, 1, pertubate=True)
+    net.check_errors()
+    chans = [0, 3] if with_da else [0, 1]
+    fl = [torch.as_tensor(st[k]) for k in ["thk", "usurf", "arrhenius", "slidingco"]]
+    Xr = O.pertubate_X(O.fieldin_to_X(fl + [torch.full_like(fl[0], dx)]), chans)
+    assert Xr.shape[0] == 5
+    Y = O.cnn_forward(Xr * torch.tensor(SCALES, dtype=torch.float32), params[0::2], params[1::2], bf16=True,
+                      bf16_first=False, out_scale=OUT)
+    Uo, Vo = O.Y_to_UV(Y, nz)
+    cost, _ = O.energy(Uo, Vo, Xr[..., 0], Xr[..., 1], Xr[..., 2], Xr[..., 3], dx, dz)
+    grads = torch.autograd.grad(cost, params)
+    np.testing.assert_allclose(s.COST_EMULATOR[-1], float(cost), rtol=2e-2)
+    g = net.grads.cpu().numpy()
+    for i, (sh, gr) in enumerate(zip(net.shapes, grads)):
+        e = rel_l2(g[net.offsets[i]:net.offsets[i + 1]].reshape(sh), gr.numpy())
+        assert e < 5e-2, (i, sh, e)
