@@ -130,6 +130,7 @@ SIGNATURES = {
     "igm_cnn_input_gradient": (I, [I, I, I, I, I, P, P, P, P, P]),
     "igm_assim_cost_grad": (I, [I, I, I, D] + [P] * 12 + [P, P, P, P, P, P, I, P, P]),
     "igm_assim_field_regu": (I, [I, I, I, D, P, P, P, D, D, I, D, I, P, P, I, P, P]),
+    "igm_assim_low_speed": (I, [I, I, I, P, P, P, P, P, P, P, I, P, P]),
     "igm_assim_flow_direction": (I, [I, I, I, P, P, P, P, P, P]),
     "igm_divflux_upwind": (I, [I, I, I, D, P, P, P, P, P]),
     "igm_assim_control": (I, [I, C.c_size_t, P, P, P, P, P, P, P, P, P, P]),

@@ -772,6 +772,58 @@ __global__ void divcost_cost_kernel(const DivCostArgs<T> a) {
   *a.cost = cst;
 }
 
+// include_low_speed_term of misfit_velsurf (cost_terms/misfit_velsurf.py:21-28):
+// 0.5 100 log((|vs| + 1) / (|obs| + 1))^2 with |.| the norm of all observed
+// components (the reference selects velsurf[ACT], a 1-D vector).  Sums of the
+// squares per block, then one warp forms the norms, adds the term to the
+// velsurf cost and stores the gradient factor c = 100 L / ((|vs| + 1) |vs|),
+// then dC/dvs += c vs on the observed components.
+template <typename T>
+__global__ void __launch_bounds__(256) low_speed_sums_kernel(size_t n, const T* uvs, const T* vvs, const T* uobs,
+                                                             const T* vobs, double* partials) {
+  double s_v = 0.0, s_o = 0.0;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    const T uo = uobs[o], vo = vobs[o];
+    if (!isnan(uo)) {
+      s_v += (double)uvs[o] * (double)uvs[o];
+      s_o += (double)uo * (double)uo;
+    }
+    if (!isnan(vo)) {
+      s_v += (double)vvs[o] * (double)vvs[o];
+      s_o += (double)vo * (double)vo;
+    }
+  }
+  block_reduce3<T>(s_v, s_o, 0.0, partials);
+}
+
+__global__ void low_speed_finish_kernel(const double* partials, int n_parts, double* cost, double* factor) {
+  const int lane = threadIdx.x;
+  double sv = 0.0, so = 0.0;
+  for (int b = lane; b < n_parts; b += 32) {
+    sv += partials[(size_t)b * 3];
+    so += partials[(size_t)b * 3 + 1];
+  }
+  for (int s = 16; s > 0; s >>= 1) {
+    sv += __shfl_xor_sync(0xffffffffu, sv, s);
+    so += __shfl_xor_sync(0xffffffffu, so, s);
+  }
+  if (lane != 0) return;
+  const double nv = sqrt(sv), no = sqrt(so);
+  const double L = log((nv + 1.0) / (no + 1.0));
+  *cost += 0.5 * 100.0 * L * L;
+  *factor = nv > 0.0 ? 100.0 * L / ((nv + 1.0) * nv) : 0.0;
+}
+
+template <typename T>
+__global__ void low_speed_grad_kernel(size_t n, const T* uvs, const T* vvs, const T* uobs, const T* vobs,
+                                      const double* factor, T* g_u, T* g_v) {
+  const T c = (T)*factor;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+    if (!isnan(uobs[o])) g_u[o] += c * uvs[o];
+    if (!isnan(vobs[o])) g_v[o] += c * vvs[o];
+  }
+}
+
 }  // namespace igm
 
 using namespace igm;
@@ -957,3 +1009,34 @@ extern "C" int igm_assim_divflux_cost_grad(int dtype, int ny, int nx, double dx,
 }
 
 extern "C" size_t igm_assim_divflux_partials_len(int n_parts) { return (size_t)6 * n_parts + 3; }
+
+extern "C" int igm_assim_low_speed(int dtype, int ny, int nx, const void* uvelsurf, const void* vvelsurf,
+                                   const void* uvelsurfobs, const void* vvelsurfobs, void* grad_uvelsurf,
+                                   void* grad_vvelsurf, double* partials, int n_parts, double* cost, void* stream) {
+  IGM_CHECK_ARG(ny >= 1 && nx >= 1, IGM_ERR_BAD_SHAPE, "igm_assim_low_speed: bad shape");
+  IGM_CHECK_ARG(uvelsurf && vvelsurf && uvelsurfobs && vvelsurfobs && grad_uvelsurf && grad_vvelsurf && partials &&
+                    cost && n_parts >= 1,
+                IGM_ERR_BAD_ARGUMENT, "igm_assim_low_speed: NULL argument");
+  cudaStream_t st = as_stream(stream);
+  const size_t n = (size_t)ny * nx;
+  int grid = grid_n(n);
+  if (grid > n_parts) grid = n_parts;
+  double* factor = partials + (size_t)3 * grid;
+  auto run = [&](auto zero) -> int {
+    using T = decltype(zero);
+    low_speed_sums_kernel<T><<<grid, 256, 0, st>>>(n, (const T*)uvelsurf, (const T*)vvelsurf,
+                                                   (const T*)uvelsurfobs, (const T*)vvelsurfobs, partials);
+    int rc = launch_status("low_speed_sums_kernel");
+    if (rc) return rc;
+    low_speed_finish_kernel<<<1, 32, 0, st>>>(partials, grid, cost, factor);
+    if ((rc = launch_status("low_speed_finish_kernel"))) return rc;
+    low_speed_grad_kernel<T><<<grid_n(n), 256, 0, st>>>(n, (const T*)uvelsurf, (const T*)vvelsurf,
+                                                        (const T*)uvelsurfobs, (const T*)vvelsurfobs, factor,
+                                                        (T*)grad_uvelsurf, (T*)grad_vvelsurf);
+    return launch_status("low_speed_grad_kernel");
+  };
+  if (dtype == IGM_F32) return run(0.f);
+  if (dtype == IGM_F64) return run(0.0);
+  set_error("igm_assim_low_speed: unknown dtype %d", dtype);
+  return IGM_ERR_BAD_ARGUMENT;
+}

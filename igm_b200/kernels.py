@@ -207,6 +207,19 @@ def assim_field_regu(field, dx, regu, aniso=1.0, flowdir=None, penalty=True, thr
     return costs, grad
 
 
+def assim_low_speed(uvs, vvs, uobs, vobs, g_u, g_v, cost, partials=None):
+    """include_low_speed_term (igm_assim_low_speed): adds the term to the
+    device double ``cost`` (a 1-element view) and its gradient to g_u, g_v."""
+    ny, nx = uvs.shape
+    n_parts = 148 * 8
+    partials = partials if partials is not None else torch.empty(3 * n_parts + 1, dtype=torch.float64,
+                                                                 device=uvs.device)
+    rc = L.lib().igm_assim_low_speed(L.dtype_code(uvs.dtype), ny, nx, L.ptr(uvs), L.ptr(vvs), L.ptr(uobs),
+                                     L.ptr(vobs), L.ptr(g_u), L.ptr(g_v), L.ptr(partials), (partials.numel() - 1) // 3,
+                                     L.ptr(cost), L.stream_ptr())
+    L.check(rc, "igm_assim_low_speed")
+
+
 def assim_flow_direction(uvs, vvs):
     """Flow directions [ny-1, nx-1] of the anisotropic regularisation."""
     ny, nx = uvs.shape

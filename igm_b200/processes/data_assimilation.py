@@ -34,8 +34,8 @@ reference (matplotlib) are not drawn.
 Supported: control_list within thk, usurf, slidingco (log_slidingco or not),
 arrhenius (dim_arrhenius 2); cost_list within velsurf, thk, icemask, usurf,
 divfluxobs, divfluxfcz (the flux-divergence terms, with or without
-force_zero_sum); fix_opti_normalization_issue on or off; method ADAM;
-sole_mask, include_low_speed_term and cook.infer_params off; divflux.method
+force_zero_sum); fix_opti_normalization_issue and include_low_speed_term on
+or off; method ADAM; sole_mask and cook.infer_params off; divflux.method
 upwind or centered.  Anything else raises NotImplementedError.
 """
 
@@ -75,8 +75,6 @@ def _check_supported(cfg):
     for key in ("sole_mask",):
         if bool(o.get(key, False)):
             bad.append(f"optimization.{key}")
-    if bool(da.fitting.include_low_speed_term):
-        bad.append("fitting.include_low_speed_term")
     if bool(da.cook.infer_params):
         bad.append("cook.infer_params")
     if da.divflux.method not in K.DIVFLUX_METHODS:
@@ -157,6 +155,7 @@ class _Assim:
         self.field_hist = {c: torch.zeros((nit, 6), dtype=torch.float64, device=d) for c in self.g_field}
         self.rms_hist = torch.zeros((nit, 9), dtype=torch.float64, device=d)
         self.stat_partials = torch.empty(148 * 8 * 13, dtype=torch.float64, device=d)
+        self.low_partials = torch.empty(3 * 148 * 8 + 1, dtype=torch.float64, device=d)
         # parameters of igm_assim_cost_grad
         p = L.AssimParams()
         p.velsurfobs_std, p.velsurfobs_thr, p.thkobs_std = f.velsurfobs_std, f.velsurfobs_thr, f.thkobs_std
@@ -303,6 +302,9 @@ def optimize_update(cfg, state, cost, i):
                       flow if a.aniso != 1.0 else None, a.dx, a.params, partials=a.partials, costs=a.cost_hist[i],
                       g_thk=a.g_thk, g_u=a.dU[0, a.nz - 1], g_v=a.dV[0, a.nz - 1], usurfobs=a.usurfobs,
                       g_us=a.g_us)
+    if bool(da.fitting.include_low_speed_term) and "velsurf" in a.cost_list:
+        K.assim_low_speed(uvs.contiguous(), vvs.contiguous(), a.uobs, a.vobs, a.dU[0, a.nz - 1], a.dV[0, a.nz - 1],
+                          a.cost_hist[i, 0:1], partials=a.low_partials)
     if a.div_kind is not None:
         _divflux_cost(cfg, state, a, thk, i)
     r = da.regularization

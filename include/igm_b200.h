@@ -371,6 +371,16 @@ IGM_API int igm_assim_stats(int dtype, int ny, int nx, double dx, const void* th
                             const void* divfluxobs, const void* usurf, const void* usurfobs, double* partials,
                             int n_parts, double* out, void* stream);
 
+/* include_low_speed_term of misfit_velsurf (cost_terms/misfit_velsurf.py:
+ * 21-28): adds 0.5 100 log((|vs| + 1) / (|obs| + 1))^2 to *cost (device
+ * double: the velsurf entry of igm_assim_cost_grad's costs) and its gradient
+ * to grad_uvelsurf / grad_vvelsurf, where |.| is the norm of all components
+ * with an observation (the reference's velsurf[ACT] is a 1-D selection; no
+ * speed threshold here).  partials: device double[3 n_parts + 1] scratch. */
+IGM_API int igm_assim_low_speed(int dtype, int ny, int nx, const void* uvelsurf, const void* vvelsurf,
+                                const void* uvelsurfobs, const void* vvelsurfobs, void* grad_uvelsurf,
+                                void* grad_vvelsurf, double* partials, int n_parts, double* cost, void* stream);
+
 /* Parameters of the flux-divergence cost terms. */
 typedef struct igm_divflux_cost_params {
   int32_t kind;            /* 0: cost_divfluxobs, 1: cost_divfluxfcz */

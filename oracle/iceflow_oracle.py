@@ -732,6 +732,7 @@ class AssimParams:
     penalty: bool = True
     icemask_cost: bool = True
     fix_normalization: bool = False  # optimization.fix_opti_normalization_issue
+    low_speed: bool = False          # fitting.include_low_speed_term
 
 
 def getmag(u, v):
@@ -759,6 +760,26 @@ def da_flow_direction(uvelsurf, vvelsurf):
     return fx, fy
 
 
+def da_misfit_velsurf(uvelsurf, vvelsurf, uobs, vobs, std, thr, low_speed=False):
+    """misfit_velsurf (cost_terms/misfit_velsurf.py:8-30): 0.5 mean over the
+    observed components at nodes whose observed speed reaches thr of
+    ((obs - vs) / std)^2; with include_low_speed_term + 0.5 100
+    log((|vs| + 1) / (|obs| + 1))^2, where -- velsurf[ACT] being the 1-D
+    selection of the observed components, without the threshold -- |.| is the
+    norm of all of them."""
+    vs = torch.stack([uvelsurf, vvelsurf], -1)
+    vo = torch.stack([uobs, vobs], -1)
+    rel = (torch.linalg.vector_norm(vo, dim=-1) >= thr)[..., None]
+    m = ~torch.isnan(vo) & rel
+    c = 0.5 * torch.mean(((vo[m] - vs[m]) / std) ** 2)
+    if low_speed:
+        # the reference selects with ACT alone here (no speed threshold)
+        act = ~torch.isnan(vo)
+        c = c + 0.5 * 100 * torch.log((torch.linalg.vector_norm(vs[act]) + 1) /
+                                      (torch.linalg.vector_norm(vo[act]) + 1)) ** 2
+    return c
+
+
 def da_costs(thk, usurf, uvelsurf, vvelsurf, uobs, vobs, thkobs, dens_thkobs, icemaskobs, icemask, flowdir, dx,
              p: AssimParams, thk_control=True):
     """The cost terms of total_cost (cost_terms/total_cost.py:13-70) for
@@ -767,13 +788,8 @@ def da_costs(thk, usurf, uvelsurf, vvelsurf, uobs, vobs, thkobs, dens_thkobs, ic
     positive-thickness penalties (total_cost.py:36-46) and regu_thk.py:8-70
     (to_regularize topg or thk, fix_opti_normalization_issue off).  Returns a
     dict of scalar tensors."""
-    cost = {}
-    vs = torch.stack([uvelsurf, vvelsurf], -1)
-    vo = torch.stack([uobs, vobs], -1)
-    rel = (torch.linalg.vector_norm(vo, dim=-1) >= p.velsurfobs_thr)[..., None]
-    act = ~torch.isnan(vo)
-    m = act & rel
-    cost["velsurf"] = 0.5 * torch.mean(((vo[m] - vs[m]) / p.velsurfobs_std) ** 2)
+    cost = {"velsurf": da_misfit_velsurf(uvelsurf, vvelsurf, uobs, vobs, p.velsurfobs_std, p.velsurfobs_thr,
+                                         p.low_speed)}
     a = ~torch.isnan(thkobs)
     cost["thk"] = 0.5 * torch.mean(dens_thkobs[a] * ((thkobs[a] - thk[a]) / p.thkobs_std) ** 2)
     z = torch.zeros_like(thk)

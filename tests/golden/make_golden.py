@@ -539,6 +539,24 @@ def assim_control_cases():
                     f"{tag}_g_pen_slidingco": gps, f"{tag}_pen_arrhenius": cp_a, f"{tag}_g_pen_arrhenius": gpa,
                     f"{tag}_misfit_usurf": cu, f"{tag}_g_usurf": gu, f"{tag}_regu_thk_topg": crt,
                     f"{tag}_g_usurf_regu_thk": gru})
+        # include_low_speed_term of misfit_velsurf (a global-norm term)
+        uo, vo = f(rng.normal(20, 15, (ny, nx))), f(rng.normal(-5, 15, (ny, nx)))
+        uo[rng.uniform(size=(ny, nx)) < 0.2] = float("nan")
+        vo[rng.uniform(size=(ny, nx)) < 0.1] = float("nan")
+        mv = importlib.import_module("igm.processes.data_assimilation.cost_terms.misfit_velsurf")
+        for thr, flag in ((0.0, False), (0.0, True), (15.0, True)):
+            da["fitting"]["include_low_speed_term"] = flag
+            da["fitting"]["velsurfobs_thr"] = thr
+            cfg.processes.data_assimilation = ns(da)
+            stv = types.SimpleNamespace(uvelsurf=uvs.clone().requires_grad_(True),
+                                        vvelsurf=vvs.clone().requires_grad_(True), uvelsurfobs=uo, vvelsurfobs=vo)
+            c = mv.misfit_velsurf(cfg, stv)
+            gu_, gv_ = torch.autograd.grad(c, [stv.uvelsurf, stv.vvelsurf])
+            key = f"{tag}_vel_thr{int(thr)}_{'low' if flag else 'plain'}"
+            out.update({f"{key}_cost": c, f"{key}_g_u": gu_, f"{key}_g_v": gv_})
+        out.update({f"{tag}_uobs": uo, f"{tag}_vobs": vo})
+        da["fitting"]["include_low_speed_term"] = False
+        da["fitting"]["velsurfobs_thr"] = 0.0
         # fix_opti_normalization_issue: the regularisations as means
         da["optimization"]["fix_opti_normalization_issue"] = True
         for aniso in (1.0, 0.2):

@@ -254,3 +254,32 @@ def test_normalised_regularisations_match_reference(golden, tag, mode):
                                    fix_normalization=True)
         close(c[4].item(), g[f"{key}_regu_{field}"])
         close(gr.cpu().numpy(), g[f"{key}_g_{field}"])
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("thr", [0.0, 15.0])
+def test_low_speed_term_matches_reference(golden, tag, thr):
+    """misfit_velsurf with include_low_speed_term: igm_assim_cost_grad's
+    velsurf cost and gradient plus igm_assim_low_speed, against the
+    reference source."""
+    g = golden("assim_controls")
+    dt = torch.float64 if tag == "f64" else torch.float32
+    d = {k: dev(g[f"{tag}_{k}"], dt) for k in ("thk", "usurf", "uvs", "vvs", "uobs", "vobs", "icemaskobs")}
+    p = L.AssimParams()
+    p.velsurfobs_std, p.velsurfobs_thr, p.thkobs_std, p.regu_thk = 1.0, thr, 3.0, 0.0
+    p.gamma, p.aniso_factor, p.n_thk = 0.0, 1.0, 1.0
+    vo = np.stack([g[f"{tag}_uobs"], g[f"{tag}_vobs"]], -1).astype(np.float64)
+    rel = np.sqrt((vo ** 2).sum(-1)) >= thr
+    p.n_vel = float((~np.isnan(vo) & rel[..., None]).sum())
+    p.penalty, p.icemask_cost, p.regularize_thk, p.mask_velsurf = 0, 0, 0, 0
+    nan = torch.full_like(d["thk"], float("nan"))
+    zero = torch.zeros_like(d["thk"])
+    costs, _, gu, gv = K.assim_cost_grad(d["thk"], d["usurf"], d["uvs"], d["vvs"], d["uobs"], d["vobs"], nan, zero,
+                                         d["icemaskobs"], None, 100.0, p)
+    K.assim_low_speed(d["uvs"], d["vvs"], d["uobs"], d["vobs"], gu, gv, costs[0:1])
+    key = f"{tag}_vel_thr{int(thr)}_low"
+    tol = 1e-9 if tag == "f64" else 1e-4
+    np.testing.assert_allclose(float(costs[0].item()), float(g[f"{key}_cost"]), rtol=tol)
+    for a, k in ((gu, "g_u"), (gv, "g_v")):
+        ref = g[f"{key}_{k}"]
+        np.testing.assert_allclose(a.cpu().numpy(), ref, rtol=tol, atol=tol * np.abs(ref).max())

@@ -88,7 +88,8 @@ def oracle_setup(cfg, st):
     p = O.AssimParams(velsurfobs_std=f.velsurfobs_std, velsurfobs_thr=f.velsurfobs_thr, thkobs_std=f.thkobs_std,
                       regu_thk=r.thk, convexity_weight=r.convexity_weight, convexity_power=r.convexity_power,
                       smooth_anisotropy_factor=r.smooth_anisotropy_factor, to_regularize=r.to_regularize,
-                      fix_normalization=bool(da.optimization.fix_opti_normalization_issue))
+                      fix_normalization=bool(da.optimization.fix_opti_normalization_issue),
+                      low_speed=bool(da.fitting.include_low_speed_term))
     ctl = O.AssimControl(step_size=da.optimization.step_size, step_size_decay=da.optimization.step_size_decay,
                          scaling_thk=da.scaling.thk)
     opt = O.KerasLegacyAdam(lr=da.optimization.step_size, epsilon=da.optimization.optimizer_epsilon,
@@ -104,11 +105,13 @@ def oracle_step(cfg, st, thk, setup, i, divflux_cost=None):
                                 bf16=True, out_scale=OUT, input_scales=SCALES, divflux_cost=divflux_cost)
 
 
-@pytest.mark.parametrize("aniso,to_regularize,normalize", [(0.2, "topg", False), (1.0, "thk", False),
-                                                            (0.2, "topg", True)])
-def test_first_iterations_match_oracle(tmp_path, monkeypatch, aniso, to_regularize, normalize):
+@pytest.mark.parametrize("aniso,to_regularize,normalize,low_speed", [(0.2, "topg", False, False),
+                                                                      (1.0, "thk", False, False),
+                                                                      (0.2, "topg", True, True)])
+def test_first_iterations_match_oracle(tmp_path, monkeypatch, aniso, to_regularize, normalize, low_speed):
     monkeypatch.chdir(tmp_path)
     cfg = make_cfg(2, aniso, to_regularize, normalize)
+    cfg.processes.data_assimilation.fitting.include_low_speed_term = low_speed
     g = twin_glacier()
     st = twin_state(cfg, g)
     setup = oracle_setup(cfg, st)

@@ -332,3 +332,23 @@ def test_normalised_regularisations(golden, tag, mode):
         np.testing.assert_allclose(float(c.detach()), float(g[f"{key}_regu_{field}"]), rtol=tol)
         ref = g[f"{key}_g_{field}"]
         np.testing.assert_allclose(gr.numpy(), ref, rtol=tol, atol=tol * np.abs(ref).max())
+
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("case", ["thr0_plain", "thr0_low", "thr15_low"])
+def test_velsurf_misfit_low_speed_term(golden, tag, case):
+    """misfit_velsurf with and without include_low_speed_term and a speed
+    threshold, against the reference source."""
+    g = golden("assim_controls")
+    u, v = (torch.as_tensor(g[f"{tag}_{k}"]).clone().requires_grad_(True) for k in ("uvs", "vvs"))
+    uo, vo = torch.as_tensor(g[f"{tag}_uobs"]), torch.as_tensor(g[f"{tag}_vobs"])
+    thr = 15.0 if case.startswith("thr15") else 0.0
+    c = O.da_misfit_velsurf(u, v, uo, vo, 1.0, thr, case.endswith("low"))
+    gu, gv = torch.autograd.grad(c, [u, v])
+    key = f"{tag}_vel_{case}"
+    tol = 1e-12 if tag == "f64" else 2e-5
+    np.testing.assert_allclose(float(c.detach()), float(g[f"{key}_cost"]), rtol=tol)
+    for a, k in ((gu, "g_u"), (gv, "g_v")):
+        ref = g[f"{key}_{k}"]
+        np.testing.assert_allclose(a.numpy(), ref, rtol=tol, atol=tol * np.abs(ref).max())
