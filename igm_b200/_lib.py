@@ -64,7 +64,7 @@ class AssimParams(C.Structure):
                 ("n_thk", C.c_double), ("penalty", C.c_int32), ("icemask_cost", C.c_int32),
                 ("regularize_thk", C.c_int32), ("mask_velsurf", C.c_int32), ("usurfobs_std", C.c_double),
                 ("n_usurf", C.c_double), ("usurf_cost", C.c_int32), ("no_thk_control", C.c_int32),
-                ("fix_normalization", C.c_int32), ("reserved", C.c_int32)]
+                ("fix_normalization", C.c_int32), ("sole_mask", C.c_int32)]
 
 
 class AssimControlParams(C.Structure):
@@ -129,7 +129,7 @@ SIGNATURES = {
     "igm_cnn_head_wgrad_finish": (I, [P, I, I, P, P]),
     "igm_cnn_input_gradient": (I, [I, I, I, I, I, P, P, P, P, P]),
     "igm_assim_cost_grad": (I, [I, I, I, D] + [P] * 12 + [P, P, P, P, P, P, I, P, P]),
-    "igm_assim_field_regu": (I, [I, I, I, D, P, P, P, D, D, I, D, I, P, P, I, P, P]),
+    "igm_assim_field_regu": (I, [I, I, I, D, P, P, P, D, D, I, D, I, P, I, P, P, I, P, P]),
     "igm_assim_low_speed": (I, [I, I, I, P, P, P, P, P, P, P, I, P, P]),
     "igm_assim_flow_direction": (I, [I, I, I, P, P, P, P, P, P]),
     "igm_divflux_upwind": (I, [I, I, I, D, P, P, P, P, P]),

@@ -35,6 +35,8 @@ struct AssimArgs {
   // regularisation weights: 1 (half sums) or, fix_opti_normalization_issue, the means' 1/count
   T kx, ky, kcell;
   double kconv;    // the convexity term: 1, or 0.5 / (ny nx)
+  int sole_mask;   // optimization.sole_mask: differences only between nodes of the observed ice
+  int mask_eq1;    // ... where icemaskobs == 1 (isotropic slidingco / arrhenius) instead of > 0.5
   double* partials;  // [gridDim.x][kNCost]
 };
 
@@ -77,6 +79,7 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
   const bool fo = a.field_only != 0;
   const bool us_cost = !fo && p.usurf_cost != 0;
   const bool thk_ctl = p.no_thk_control == 0;
+  const bool sole = a.sole_mask != 0, eq1 = a.mask_eq1 != 0;
   const T kus = (T)(1.0 / (p.usurfobs_std * p.usurfobs_std * (p.n_usurf > 0 ? p.n_usurf : 1.0)));
   const T rdx = T(1) / a.dx, hr = T(0.5) * rdx;
   const T w = (T)p.regu_thk;
@@ -94,13 +97,13 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
     r.us = (ok && !fo && (!reg_thk || us_cost)) ? a.usurf[o] : T(0);
     const bool okn = ok && full && !fo;
     r.uso = (okn && us_cost) ? a.usobs[o] : T(0);
+    r.im = (ok && (okn || sole)) ? a.icemaskobs[o] : T(0);
     r.uo = okn ? a.uobs[o] : T(0);
     r.vo = okn ? a.vobs[o] : T(0);
     r.uv = okn ? a.uvs[o] : T(0);
     r.vv = okn ? a.vvs[o] : T(0);
     r.to = okn ? a.thkobs[o] : T(0);
     r.de = okn ? a.dens[o] : T(0);
-    r.im = okn ? a.icemaskobs[o] : T(0);
     const bool okc = aniso && cell_col && j < ny - 1;
     const size_t q = (size_t)j * (nx - 1) + cc;
     r.fx = okc ? a.fdx[q] : T(0);
@@ -114,12 +117,18 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
   struct Cell {
     T P, M, cost, dxp, dyp;
   };
-  auto cell = [&](int j, T f0, T f1, const AssimRow<T>& r) {
+  auto cell = [&](int j, T f0, T f1, const AssimRow<T>& r, T im1) {
     Cell k{T(0), T(0), T(0), T(0), T(0)};
     const T f0r = __shfl_down_sync(0xffffffffu, f0, 1);
     const T f1r = __shfl_down_sync(0xffffffffu, f1, 1);
+    // sole_mask (regu_thk.py:29-31, 47-50; regu_slidingco.py:12-14, 30-33; regu_arrhenius.py:9-11):
+    // a cell needs its four corners > 0.5, an isotropic difference its two nodes (> 0.5 or == 1)
+    const int g0 = r.im > T(0.5), g1 = im1 > T(0.5);
+    const int e0 = eq1 ? (r.im == T(1)) : g0, e1 = eq1 ? (im1 == T(1)) : g1;
+    const int g0r = __shfl_down_sync(0xffffffffu, g0, 1), g1r = __shfl_down_sync(0xffffffffu, g1, 1);
+    const int e0r = __shfl_down_sync(0xffffffffu, e0, 1);
     if (aniso) {
-      if (cell_col && j >= 0 && j < ny - 1) {
+      if (cell_col && j >= 0 && j < ny - 1 && (!sole || (g0 && g0r && g1 && g1r))) {
         const T dbdx = ((f0r - f0) + (f1r - f1)) * hr;
         const T dbdy = ((f1 - f0) + (f1r - f0r)) * hr;
         const T A = dbdx * r.fx + dbdy * r.fy, B = dbdx * r.fy - dbdy * r.fx;
@@ -131,8 +140,8 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
         k.cost = (s_a * A * A * T(0.5) + s_b * B * B * T(0.5)) * a.kcell;
       }
     } else if (col && j >= 0) {
-      if (c + 1 < nx) k.dxp = (f0r - f0) * rdx;
-      if (j + 1 < ny) k.dyp = (f1 - f0) * rdx;
+      if (c + 1 < nx && (!sole || (e0 && e0r))) k.dxp = (f0r - f0) * rdx;
+      if (j + 1 < ny && (!sole || (e0 && e1))) k.dyp = (f1 - f0) * rdx;
     }
     return k;
   };
@@ -142,12 +151,12 @@ __device__ __forceinline__ void assim_march(const AssimArgs<T>& a, const AssimSc
   Cell prev{T(0), T(0), T(0), T(0), T(0)};
   if (y0 >= 1) {
     const AssimRow<T> up = load(y0 - 1, false);
-    prev = cell(y0 - 1, field(up), f_cur, up);
+    prev = cell(y0 - 1, field(up), f_cur, up, cur.im);
   }
   for (int j = y0; j < y1; ++j) {
     const AssimRow<T> nxt = load(j + 1, j + 1 < y1);
     const T f_nxt = field(nxt);
-    const Cell k = cell(j, f_cur, f_nxt, cur);
+    const Cell k = cell(j, f_cur, f_nxt, cur, nxt.im);
     T gf;
     if (aniso) {
       const T Ml = __shfl_up_sync(0xffffffffu, k.M, 1);
@@ -403,13 +412,14 @@ static int cost_grad_t(int ny, int nx, double dx, const void* thk, const void* u
   sc.c_us = p->usurf_cost ? 0.5 / (p->usurfobs_std * p->usurfobs_std * (p->n_usurf > 0 ? p->n_usurf : 1.0)) : 0.0;
   sc.gamma = p->gamma;
   set_norm(a, p->fix_normalization);
+  a.sole_mask = p->sole_mask;
   return march_launch<T>(a, sc, n_parts, costs, st);
 }
 
 template <typename T>
 static int field_regu_t(int ny, int nx, double dx, const void* field, const void* fdx, const void* fdy, double regu,
-                        double aniso, int penalty, double pos_thr, int fix_normalization, void* grad,
-                        double* partials, int n_parts, double* costs, cudaStream_t st) {
+                        double aniso, int penalty, double pos_thr, int fix_normalization, const void* icemaskobs,
+                        int sole_mask, void* grad, double* partials, int n_parts, double* costs, cudaStream_t st) {
   AssimArgs<T> a{};
   a.ny = ny; a.nx = nx; a.dx = (T)dx;
   a.thk = (const T*)field; a.fdx = (const T*)fdx; a.fdy = (const T*)fdy;
@@ -422,6 +432,9 @@ static int field_regu_t(int ny, int nx, double dx, const void* field, const void
   a.pos_thr = (T)pos_thr;
   a.g_thk = (T*)grad;
   a.partials = partials;
+  a.icemaskobs = (const T*)icemaskobs;
+  a.sole_mask = sole_mask;
+  a.mask_eq1 = 1;
   AssimScales sc{};
   sc.c_pen = 1e10 / ((double)ny * nx);
   sc.c_reg = regu;
@@ -860,20 +873,23 @@ extern "C" int igm_assim_cost_grad(int dtype, int ny, int nx, double dx, const v
 
 extern "C" int igm_assim_field_regu(int dtype, int ny, int nx, double dx, const void* field, const void* flowdirx,
                                     const void* flowdiry, double regu, double aniso_factor, int penalty,
-                                    double penalty_threshold, int fix_normalization, void* grad, double* partials,
-                                    int n_parts, double* costs, void* stream) {
+                                    double penalty_threshold, int fix_normalization, const void* icemaskobs,
+                                    int sole_mask, void* grad, double* partials, int n_parts, double* costs,
+                                    void* stream) {
   IGM_CHECK_ARG(ny >= 2 && nx >= 2 && dx > 0, IGM_ERR_BAD_SHAPE, "igm_assim_field_regu: bad shape %dx%d", ny, nx);
   IGM_CHECK_ARG(field && grad && partials && costs && n_parts >= 1 && aniso_factor > 0, IGM_ERR_BAD_ARGUMENT,
                 "igm_assim_field_regu: bad argument");
   IGM_CHECK_ARG(aniso_factor == 1.0 || (flowdirx && flowdiry), IGM_ERR_BAD_ARGUMENT,
                 "igm_assim_field_regu: the anisotropic regularisation needs flowdirx, flowdiry");
+  IGM_CHECK_ARG(!sole_mask || icemaskobs, IGM_ERR_BAD_ARGUMENT, "igm_assim_field_regu: sole_mask needs icemaskobs");
   cudaStream_t st = as_stream(stream);
   if (dtype == IGM_F32)
     return field_regu_t<float>(ny, nx, dx, field, flowdirx, flowdiry, regu, aniso_factor, penalty, penalty_threshold,
-                               fix_normalization, grad, partials, n_parts, costs, st);
+                               fix_normalization, icemaskobs, sole_mask, grad, partials, n_parts, costs, st);
   if (dtype == IGM_F64)
     return field_regu_t<double>(ny, nx, dx, field, flowdirx, flowdiry, regu, aniso_factor, penalty,
-                                penalty_threshold, fix_normalization, grad, partials, n_parts, costs, st);
+                                penalty_threshold, fix_normalization, icemaskobs, sole_mask, grad, partials, n_parts,
+                                costs, st);
   set_error("igm_assim_field_regu: unknown dtype %d", dtype);
   return IGM_ERR_BAD_ARGUMENT;
 }

@@ -187,7 +187,7 @@ def assim_cost_grad(thk, usurf, uvs, vvs, uobs, vobs, thkobs, dens, icemaskobs, 
 
 
 def assim_field_regu(field, dx, regu, aniso=1.0, flowdir=None, penalty=True, threshold=0.0, grad=None, costs=None,
-                     partials=None, fix_normalization=False):
+                     partials=None, fix_normalization=False, sole_mask_icemaskobs=None):
     """The regularisation and positivity penalty of a slidingco / arrhenius
     control (igm_assim_field_regu): returns (costs double[6] with [3] the
     penalty and [4] the regularisation, dC/dfield)."""
@@ -200,7 +200,8 @@ def assim_field_regu(field, dx, regu, aniso=1.0, flowdir=None, penalty=True, thr
     fx, fy = flowdir if flowdir is not None else (None, None)
     rc = L.lib().igm_assim_field_regu(L.dtype_code(field.dtype), ny, nx, float(dx), L.ptr(field), L.ptr(fx),
                                       L.ptr(fy), float(regu), float(aniso), int(bool(penalty)), float(threshold),
-                                      int(bool(fix_normalization)), L.ptr(grad), L.ptr(partials),
+                                      int(bool(fix_normalization)), L.ptr(sole_mask_icemaskobs),
+                                      int(sole_mask_icemaskobs is not None), L.ptr(grad), L.ptr(partials),
                                       partials.numel() // 6, L.ptr(costs),
                                       L.stream_ptr())
     L.check(rc, "igm_assim_field_regu")

@@ -34,8 +34,8 @@ reference (matplotlib) are not drawn.
 Supported: control_list within thk, usurf, slidingco (log_slidingco or not),
 arrhenius (dim_arrhenius 2); cost_list within velsurf, thk, icemask, usurf,
 divfluxobs, divfluxfcz (the flux-divergence terms, with or without
-force_zero_sum); fix_opti_normalization_issue and include_low_speed_term on
-or off; method ADAM; sole_mask and cook.infer_params off; divflux.method
+force_zero_sum); fix_opti_normalization_issue, include_low_speed_term and
+sole_mask on or off; method ADAM; cook.infer_params off; divflux.method
 upwind or centered.  Anything else raises NotImplementedError.
 """
 
@@ -72,9 +72,6 @@ def _check_supported(cfg):
         bad.append(f"cost terms {extra} (only velsurf, thk, icemask, usurf, divfluxobs, divfluxfcz)")
     if o.method != "ADAM":
         bad.append(f"optimization.method={o.method!r} (only 'ADAM')")
-    for key in ("sole_mask",):
-        if bool(o.get(key, False)):
-            bad.append(f"optimization.{key}")
     if bool(da.cook.infer_params):
         bad.append("cook.infer_params")
     if da.divflux.method not in K.DIVFLUX_METHODS:
@@ -177,6 +174,7 @@ class _Assim:
         p.n_usurf = max(1.0, float((self.icemaskobs > 0.5).sum().item()))
         p.no_thk_control = int("thk" not in self.controls)
         p.fix_normalization = int(bool(o.fix_opti_normalization_issue))
+        p.sole_mask = int(bool(o.sole_mask))
         self.params = p
         self.log_slidingco = bool(f.log_slidingco)
         pen = bool(p.penalty)
@@ -207,7 +205,7 @@ class _Assim:
         """igm_assim_control's transform, mask and reprojection for control c
         (optimize/update.py:23-27, 58-68, 84-98; sole_mask off)."""
         transform = int(c == "slidingco" and self.log_slidingco)
-        mask = 0 if c == "slidingco" else 1
+        mask = (2 if self.params.sole_mask else 0) if c == "slidingco" else 1
         if not self.reproject:
             rep, lower = 0, 0.0
         elif c == "thk":
@@ -315,7 +313,8 @@ def optimize_update(cfg, state, cost, i):
         K.assim_field_regu(S.get(state, c).contiguous(), a.dx, float(getattr(r, c)), aniso,
                            flow if aniso != 1.0 else None, penalty=pen, threshold=1.0 if c == "arrhenius" else 0.0,
                            grad=g, costs=a.field_hist[c][i], partials=a.partials,
-                           fix_normalization=bool(a.params.fix_normalization))
+                           fix_normalization=bool(a.params.fix_normalization),
+                           sole_mask_icemaskobs=a.icemaskobs if a.params.sole_mask else None)
     model.backward(buf, 1, a.ny, a.nx, a.dU, a.dV, field_grad=a.field_grad, param_grads=False)
     direct = {"thk": a.g_thk, "usurf": a.g_us, **a.g_field}
     for k, c in enumerate(a.controls):

@@ -285,7 +285,7 @@ typedef struct igm_assim_params {
   int32_t usurf_cost;      /* "usurf" in cost_list */
   int32_t no_thk_control;  /* thk not in control_list: no thk_positive penalty, no regu_thk */
   int32_t fix_normalization; /* optimization.fix_opti_normalization_issue: regularisation means, not sums */
-  int32_t reserved;
+  int32_t sole_mask;       /* optimization.sole_mask: regu_thk's differences only inside icemaskobs > 0.5 */
 } igm_assim_params;
 
 /* The cost terms of total_cost (cost_terms/total_cost.py:13-70) that depend
@@ -311,17 +311,21 @@ IGM_API int igm_assim_cost_grad(int dtype, int ny, int nx, double dx, const void
  * regu_slidingco (cost_terms/regu_slidingco.py:8-52; isotropic, or anisotropic
  * with aniso_factor = smooth_anisotropy_factor_sl and the flow directions),
  * regu_arrhenius (cost_terms/regu_arrhenius.py:5-24; isotropic), both with
- * sole_mask off, weight regu (fix_normalization: 0.5 regu times the means
+ * weight regu (fix_normalization: 0.5 regu times the means
  * of the squared differences instead of their half sums, as
  * fix_opti_normalization_issue), and with penalty the 1e10 mean(field^2
  * where field < penalty_threshold) of
- * total_cost.py:45-54 (threshold 0 for slidingco, 1 for arrhenius).  grad:
+ * total_cost.py:45-54 (threshold 0 for slidingco, 1 for arrhenius).  With
+ * sole_mask (icemaskobs given) only the differences between two nodes with
+ * icemaskobs == 1 (isotropic) or the cells whose four corners are > 0.5
+ * (anisotropic) count, as regu_slidingco / regu_arrhenius mask them.  grad:
  * dC/dfield [ny][nx]; costs (device double[6], the layout of
  * igm_assim_cost_grad): [3] the penalty, [4] the regularisation, the others 0. */
 IGM_API int igm_assim_field_regu(int dtype, int ny, int nx, double dx, const void* field, const void* flowdirx,
                                  const void* flowdiry, double regu, double aniso_factor, int penalty,
-                                 double penalty_threshold, int fix_normalization, void* grad, double* partials,
-                                 int n_parts, double* costs, void* stream);
+                                 double penalty_threshold, int fix_normalization, const void* icemaskobs,
+                                 int sole_mask, void* grad, double* partials, int n_parts, double* costs,
+                                 void* stream);
 
 /* The control update of optimize_update (data_assimilation/optimize/update.py:
  * 22-42, 56-98) for one control x (thk, usurf, slidingco or arrhenius) with

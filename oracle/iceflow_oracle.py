@@ -733,6 +733,7 @@ class AssimParams:
     icemask_cost: bool = True
     fix_normalization: bool = False  # optimization.fix_opti_normalization_issue
     low_speed: bool = False          # fitting.include_low_speed_term
+    sole_mask: bool = False          # optimization.sole_mask
 
 
 def getmag(u, v):
@@ -807,6 +808,10 @@ def da_costs(thk, usurf, uvelsurf, vvelsurf, uobs, vobs, thkobs, dens_thkobs, ic
     if f == 1:
         dbdx = (field[:, 1:] - field[:, :-1]) / dx
         dbdy = (field[1:, :] - field[:-1, :]) / dx
+        if p.sole_mask:
+            im = icemaskobs > 0.5
+            dbdx = torch.where(im[:, 1:] & im[:, :-1], dbdx, torch.zeros_like(dbdx))
+            dbdy = torch.where(im[1:, :] & im[:-1, :], dbdy, torch.zeros_like(dbdy))
         if p.fix_normalization:
             cost["thk_regu"] = p.regu_thk * 0.5 * (torch.mean(dbdx ** 2) + torch.mean(dbdy ** 2)
                                                    - gamma * torch.mean(thk))
@@ -819,6 +824,11 @@ def da_costs(thk, usurf, uvelsurf, vvelsurf, uobs, vobs, thkobs, dens_thkobs, ic
         dbdx = (dbdx[1:, :] + dbdx[:-1, :]) / 2.0
         dbdy = (field[1:, :] - field[:-1, :]) / dx
         dbdy = (dbdy[:, 1:] + dbdy[:, :-1]) / 2.0
+        if p.sole_mask:
+            im = icemaskobs > 0.5
+            cm = im[1:, 1:] & im[1:, :-1] & im[:-1, 1:] & im[:-1, :-1]
+            dbdx = torch.where(cm, dbdx, torch.zeros_like(dbdx))
+            dbdy = torch.where(cm, dbdy, torch.zeros_like(dbdy))
         if p.fix_normalization:
             cost["thk_regu"] = p.regu_thk * 0.5 * (
                 (1.0 / np.sqrt(f)) * torch.mean((dbdx * fx + dbdy * fy) ** 2)
@@ -961,15 +971,20 @@ def da_optimize_step(fields, dx, weights, biases, Nz, vert_weight, obs, p: Assim
             cost["slidingco_positive"] = da_penalty(sl, 0.0)
         if "arrhenius" in mc.controls:
             cost["arrhenius_positive"] = da_penalty(ar, 1.0)
+    smask = obs["icemaskobs"] if p.sole_mask else None
     if "slidingco" in mc.controls:
-        cost["slid_regu"] = da_regu_field(sl, dx, mc.regu_slidingco, mc.aniso_sl, flow, normalize=p.fix_normalization)
+        cost["slid_regu"] = da_regu_field(sl, dx, mc.regu_slidingco, mc.aniso_sl, flow, normalize=p.fix_normalization,
+                                          icemaskobs=smask)
     if "arrhenius" in mc.controls:
-        cost["arrh_regu"] = da_regu_field(ar, dx, mc.regu_arrhenius, normalize=p.fix_normalization)
+        cost["arrh_regu"] = da_regu_field(ar, dx, mc.regu_arrhenius, normalize=p.fix_normalization,
+                                          icemaskobs=smask)
     total = sum(cost.values())
     grads = torch.autograd.grad(total, [var[c] for c in mc.controls])
     inside = obs["icemaskobs"] > 0.5
-    grads = [g if c == "slidingco" else torch.where(inside, g, torch.zeros_like(g))
-             for c, g in zip(mc.controls, grads)]
+    # update.py:58-68: slidingco's gradient unmasked, or (sole_mask) where icemaskobs == 1
+    sl_mask = obs["icemaskobs"] == 1
+    grads = [(torch.where(sl_mask, g, torch.zeros_like(g)) if p.sole_mask else g) if c == "slidingco"
+             else torch.where(inside, g, torch.zeros_like(g)) for c, g in zip(mc.controls, grads)]
     if ctl.step_size_decay < 1:
         optimizer.lr = ctl.step_size * (ctl.step_size_decay ** (i / 100))
     new_vars = [var[c].detach().clone() for c in mc.controls]
@@ -1091,7 +1106,7 @@ def da_cost_divflux(kind, ubar, vbar, thk, dx, icemaskobs, divfluxobs=None, usur
     return c
 
 
-def da_regu_field(f, dx, weight, aniso=1.0, flowdir=None, normalize=False):
+def da_regu_field(f, dx, weight, aniso=1.0, flowdir=None, normalize=False, icemaskobs=None):
     """regu_slidingco (cost_terms/regu_slidingco.py:8-52) and regu_arrhenius
     (cost_terms/regu_arrhenius.py:5-24) with sole_mask and
     fix_opti_normalization_issue off: weight (l2_loss(df/dx) + l2_loss(df/dy))
@@ -1103,11 +1118,20 @@ def da_regu_field(f, dx, weight, aniso=1.0, flowdir=None, normalize=False):
     if aniso == 1.0:
         dadx = (f[:, 1:] - f[:, :-1]) / dx
         dady = (f[1:, :] - f[:-1, :]) / dx
+        if icemaskobs is not None:  # sole_mask: both nodes with icemaskobs == 1
+            m = icemaskobs == 1
+            dadx = torch.where(m[:, 1:] & m[:, :-1], dadx, torch.zeros_like(dadx))
+            dady = torch.where(m[1:, :] & m[:-1, :], dady, torch.zeros_like(dady))
         return weight * (red(dadx ** 2) + red(dady ** 2))
     dadx = (f[:, 1:] - f[:, :-1]) / dx
     dadx = (dadx[1:, :] + dadx[:-1, :]) / 2.0
     dady = (f[1:, :] - f[:-1, :]) / dx
     dady = (dady[:, 1:] + dady[:, :-1]) / 2.0
+    if icemaskobs is not None:  # sole_mask: the four corners with icemaskobs > 0.5
+        m = icemaskobs > 0.5
+        cm = m[1:, 1:] & m[1:, :-1] & m[:-1, 1:] & m[:-1, :-1]
+        dadx = torch.where(cm, dadx, torch.zeros_like(dadx))
+        dady = torch.where(cm, dady, torch.zeros_like(dady))
     fx, fy = flowdir
     return weight * ((1.0 / np.sqrt(aniso)) * red((dadx * fx + dady * fy) ** 2)
                      + np.sqrt(aniso) * red((dadx * fy - dady * fx) ** 2))

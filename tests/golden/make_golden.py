@@ -577,6 +577,29 @@ def assim_control_cases():
             out.update({f"{key}_regu_thk": c_t, f"{key}_g_thk": g_t, f"{key}_regu_slidingco": c_s,
                         f"{key}_g_slidingco": g_s, f"{key}_regu_arrhenius": c_a, f"{key}_g_arrhenius": g_a})
         da["optimization"]["fix_opti_normalization_issue"] = False
+        # sole_mask: the regularisations restricted to the observed ice (a mask with values 0, 1, 2)
+        im3 = icemaskobs.clone()
+        im3[(rng.uniform(size=(ny, nx)) < 0.15) & (g["thk"].numpy() > 0)] = 2.0
+        da["optimization"]["sole_mask"] = True
+        for aniso in (1.0, 0.2):
+            da["regularization"]["smooth_anisotropy_factor"] = aniso
+            da["regularization"]["smooth_anisotropy_factor_sl"] = 0.3 if aniso != 1.0 else 1.0
+            cfg.processes.data_assimilation = ns(da)
+            key = f"{tag}_sole_{'aniso' if aniso != 1.0 else 'iso'}"
+            th = thk.clone().requires_grad_(True)
+            st3 = types.SimpleNamespace(thk=th, usurf=usurf, slidingco=sl.clone().requires_grad_(True),
+                                        arrhenius=ar.clone().requires_grad_(True), icemaskobs=im3,
+                                        icemask=icemaskobs, dx=dx, flowdirx=st.flowdirx, flowdiry=st.flowdiry)
+            c_t = rt.regu_thk(cfg, st3)
+            (g_t,) = torch.autograd.grad(c_t, [th])
+            c_s = rs.regu_slidingco(cfg, st3)
+            (g_s,) = torch.autograd.grad(c_s, [st3.slidingco])
+            c_a = ra.regu_arrhenius(cfg, st3)
+            (g_a,) = torch.autograd.grad(c_a, [st3.arrhenius])
+            out.update({f"{key}_regu_thk": c_t, f"{key}_g_thk": g_t, f"{key}_regu_slidingco": c_s,
+                        f"{key}_g_slidingco": g_s, f"{key}_regu_arrhenius": c_a, f"{key}_g_arrhenius": g_a})
+        out[f"{tag}_icemaskobs3"] = im3
+        da["optimization"]["sole_mask"] = False
         da["regularization"]["smooth_anisotropy_factor"] = 0.2
     save("assim_controls", out)
 

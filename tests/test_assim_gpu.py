@@ -283,3 +283,39 @@ def test_low_speed_term_matches_reference(golden, tag, thr):
     for a, k in ((gu, "g_u"), (gv, "g_v")):
         ref = g[f"{key}_{k}"]
         np.testing.assert_allclose(a.cpu().numpy(), ref, rtol=tol, atol=tol * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("mode", ["iso", "aniso"])
+def test_sole_mask_regularisations_match_reference(golden, tag, mode):
+    """regu_thk (igm_assim_cost_grad), regu_slidingco and regu_arrhenius
+    (igm_assim_field_regu) with sole_mask, against the reference source."""
+    g = golden("assim_controls")
+    dt = torch.float64 if tag == "f64" else torch.float32
+    d = {k: dev(g[f"{tag}_{k}"], dt) for k in ("thk", "usurf", "slidingco", "arrhenius", "icemaskobs3")}
+    dx = float(g[f"{tag}_dx"])
+    key = f"{tag}_sole_{mode}"
+    tol = 1e-9 if tag == "f64" else 1e-4
+    flow = (dev(g[f"{tag}_slaniso_flowdirx"], dt), dev(g[f"{tag}_slaniso_flowdiry"], dt))
+
+    def close(a, ref):
+        ref = np.asarray(ref)
+        np.testing.assert_allclose(np.asarray(a), ref, rtol=tol, atol=tol * max(np.abs(ref).max(), 1e-30))
+
+    p = L.AssimParams()
+    p.velsurfobs_std, p.velsurfobs_thr, p.thkobs_std, p.regu_thk = 1.0, 0.0, 3.0, 10.0
+    area = float((g[f"{tag}_icemaskobs"] > 0.5).sum()) * dx ** 2
+    p.gamma, p.n_vel, p.n_thk = 0.002 * area ** (1.3 - 2.0), 1.0, 1.0
+    p.aniso_factor = 0.2 if mode == "aniso" else 1.0
+    p.penalty, p.icemask_cost, p.regularize_thk, p.mask_velsurf, p.sole_mask = 0, 0, 0, 1, 1
+    nan = torch.full_like(d["thk"], float("nan"))
+    zero = torch.zeros_like(d["thk"])
+    costs, gt, _, _ = K.assim_cost_grad(d["thk"], d["usurf"], zero, zero, nan, nan, nan, zero, d["icemaskobs3"],
+                                        flow if mode == "aniso" else None, dx, p)
+    close(costs.cpu().numpy()[4], g[f"{key}_regu_thk"])
+    close(gt.cpu().numpy(), g[f"{key}_g_thk"])
+    for field, w, an in (("slidingco", 7.0, 0.3 if mode == "aniso" else 1.0), ("arrhenius", 2.0, 1.0)):
+        c, gr = K.assim_field_regu(d[field], dx, w, an, flow if an != 1.0 else None, penalty=False,
+                                   sole_mask_icemaskobs=d["icemaskobs3"])
+        close(c[4].item(), g[f"{key}_regu_{field}"])
+        close(gr.cpu().numpy(), g[f"{key}_g_{field}"])

@@ -43,7 +43,7 @@ def test_density_matrix_counts():
 
 def test_unsupported_configurations_raise():
     for over in ({"control_list": ["thk", "topg"]}, {"control_list": ["thk", "thk"]}, {"cost_list": ["velsurf", "vol"]}, {"divflux": {"method": "flux-limiter"}},
-                 {"optimization": {"method": "L-BFGS"}}, {"optimization": {"sole_mask": True}}, {"cook": {"infer_params": True}}):
+                 {"optimization": {"method": "L-BFGS"}}, {"cook": {"infer_params": True}}):
         cfg = default_cfg({"data_assimilation": over})
         with pytest.raises(NotImplementedError):
             DA._check_supported(cfg)

@@ -89,7 +89,8 @@ def oracle_setup(cfg, st):
                       regu_thk=r.thk, convexity_weight=r.convexity_weight, convexity_power=r.convexity_power,
                       smooth_anisotropy_factor=r.smooth_anisotropy_factor, to_regularize=r.to_regularize,
                       fix_normalization=bool(da.optimization.fix_opti_normalization_issue),
-                      low_speed=bool(da.fitting.include_low_speed_term))
+                      low_speed=bool(da.fitting.include_low_speed_term),
+                      sole_mask=bool(da.optimization.sole_mask))
     ctl = O.AssimControl(step_size=da.optimization.step_size, step_size_decay=da.optimization.step_size_decay,
                          scaling_thk=da.scaling.thk)
     opt = O.KerasLegacyAdam(lr=da.optimization.step_size, epsilon=da.optimization.optimizer_epsilon,
@@ -226,11 +227,12 @@ def test_divflux_costs_in_the_loop_match_oracle(tmp_path, monkeypatch, kind, met
         thk_o = st.thk.detach().cpu().clone()
 
 
-@pytest.mark.parametrize("controls,log_sl,normalize", [(["thk", "slidingco"], False, False),
-                                                       (["thk", "slidingco"], True, False),
-                                                       (["thk", "arrhenius"], False, True),
-                                                       (["thk", "usurf"], False, False)])
-def test_other_controls_in_the_loop_match_oracle(tmp_path, monkeypatch, controls, log_sl, normalize):
+@pytest.mark.parametrize("controls,log_sl,normalize,sole", [(["thk", "slidingco"], False, False, False),
+                                                            (["thk", "slidingco"], True, False, False),
+                                                            (["thk", "arrhenius"], False, True, False),
+                                                            (["thk", "usurf"], False, False, False),
+                                                            (["thk", "slidingco"], False, False, True)])
+def test_other_controls_in_the_loop_match_oracle(tmp_path, monkeypatch, controls, log_sl, normalize, sole):
     """Several controls at once (one Adam variable each, clipped separately):
     three iterations against the oracle's da_optimize_step -- the costs, each
     variable's gradient, and each control's step (relative to its size, as
@@ -242,6 +244,7 @@ def test_other_controls_in_the_loop_match_oracle(tmp_path, monkeypatch, controls
     da = cfg.processes.data_assimilation
     da.control_list = list(controls)
     da.fitting.log_slidingco = log_sl
+    da.optimization.sole_mask = sole
     da.regularization.smooth_anisotropy_factor_sl = 0.5
     if "usurf" in controls:
         da.cost_list = list(da.cost_list) + ["usurf"]

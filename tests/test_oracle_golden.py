@@ -352,3 +352,34 @@ def test_velsurf_misfit_low_speed_term(golden, tag, case):
     for a, k in ((gu, "g_u"), (gv, "g_v")):
         ref = g[f"{key}_{k}"]
         np.testing.assert_allclose(a.numpy(), ref, rtol=tol, atol=tol * np.abs(ref).max())
+
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("mode", ["iso", "aniso"])
+def test_sole_mask_regularisations(golden, tag, mode):
+    """regu_thk, regu_slidingco, regu_arrhenius with sole_mask (an ice mask
+    with values 0, 1 and 2), against the reference source."""
+    g = golden("assim_controls")
+    t = {k: torch.as_tensor(g[f"{tag}_{k}"]) for k in ("thk", "usurf", "slidingco", "arrhenius", "icemaskobs",
+                                                       "icemaskobs3")}
+    dx = float(g[f"{tag}_dx"])
+    key = f"{tag}_sole_{mode}"
+    tol = 1e-10 if tag == "f64" else 2e-5
+    aniso = 0.2 if mode == "aniso" else 1.0
+    flow = (torch.as_tensor(g[f"{tag}_slaniso_flowdirx"]), torch.as_tensor(g[f"{tag}_slaniso_flowdiry"]))
+    th = t["thk"].clone().requires_grad_(True)
+    p = O.AssimParams(regu_thk=10.0, smooth_anisotropy_factor=aniso, to_regularize="topg", sole_mask=True)
+    nan = torch.full_like(th, float("nan"))
+    c = O.da_costs(th, t["usurf"], th * 0, th * 0, nan, nan, nan, th * 0, t["icemaskobs3"], t["icemaskobs"], flow,
+                   dx, p)["thk_regu"]
+    gr = torch.autograd.grad(c, th)[0]
+    np.testing.assert_allclose(float(c.detach()), float(g[f"{key}_regu_thk"]), rtol=tol)
+    np.testing.assert_allclose(gr.numpy(), g[f"{key}_g_thk"], rtol=tol, atol=tol * np.abs(g[f"{key}_g_thk"]).max())
+    for field, w, an in (("slidingco", 7.0, 0.3 if mode == "aniso" else 1.0), ("arrhenius", 2.0, 1.0)):
+        x = t[field].clone().requires_grad_(True)
+        c = O.da_regu_field(x, dx, w, an, flow, icemaskobs=t["icemaskobs3"])
+        gr = torch.autograd.grad(c, x)[0]
+        np.testing.assert_allclose(float(c.detach()), float(g[f"{key}_regu_{field}"]), rtol=tol)
+        ref = g[f"{key}_g_{field}"]
+        np.testing.assert_allclose(gr.numpy(), ref, rtol=tol, atol=tol * np.abs(ref).max())
