@@ -47,3 +47,54 @@ def test_unsupported_configurations_raise():
         cfg = default_cfg({"data_assimilation": over})
         with pytest.raises(NotImplementedError):
             DA._check_supported(cfg)
+
+
+def _fake(**kw):
+    import types
+    return types.SimpleNamespace(**kw)
+
+
+def test_control_update_settings_per_control():
+    """Transform, gradient mask and reprojection of each control
+    (optimize/update.py:23-27, 58-68, 84-98)."""
+    a = _fake(reproject=True, log_slidingco=False, params=_fake(sole_mask=0), cost_list=["velsurf", "icemask"])
+    kw = lambda c: DA._Assim.control_kw(a, c)  # noqa: E731
+    assert kw("thk") == dict(transform=0, mask=1, reproject=1, lower=0.0, reproject_mask=True)
+    assert kw("slidingco") == dict(transform=0, mask=0, reproject=2, lower=0.0, reproject_mask=True)
+    assert kw("arrhenius") == dict(transform=0, mask=1, reproject=2, lower=1.0, reproject_mask=True)
+    assert kw("usurf") == dict(transform=0, mask=1, reproject=0, lower=0.0, reproject_mask=True)
+    a.log_slidingco, a.params.sole_mask, a.reproject, a.cost_list = True, 1, False, ["velsurf"]
+    assert kw("slidingco") == dict(transform=1, mask=2, reproject=0, lower=0.0, reproject_mask=False)
+    assert kw("thk")["reproject"] == 0
+
+
+def test_cost_table_follows_total_cost_order():
+    """costs.dat columns: total_cost.py's dictionary order over the terms present."""
+    n = 3
+    hist = torch.arange(n * 6, dtype=torch.float64).reshape(n, 6)  # velsurf thk icemask thk_positive thk_regu usurf
+    field = torch.zeros((n, 6), dtype=torch.float64)
+    field[:, 3], field[:, 4] = 100.0, 200.0
+    present = {"velsurf": True, "thk": True, "usurf": True, "icemask": True, "thk_positive": True,
+               "slidingco_positive": True, "arrhenius_positive": False, "thk_regu": True, "slid_regu": True,
+               "arrh_regu": False}
+    a = _fake(cost_hist=hist, present=present, div_kind="obs", div_hist=torch.full((n,), 7.0, dtype=torch.float64),
+              field_hist={"slidingco": field})
+    keys, table = DA._cost_table(a, n)
+    assert keys == ["velsurf", "thk", "divflux", "usurf", "icemask", "thk_positive", "slidingco_positive",
+                    "thk_regu", "slid_regu"]
+    np.testing.assert_array_equal(table[1], [6, 7, 7.0, 11, 8, 9, 100.0, 10, 200.0])
+
+
+def test_pertubate_field_selection():
+    """pertubate_X's copies: thk and usurf without data assimilation, the
+    controls with it; each scaled copy stacked along y."""
+    from igm_b200 import emulator as E
+    f = [torch.full((2, 3), float(k + 1)) for k in range(4)]
+    st, n = E._pertubate_fields(default_cfg(), f)
+    assert n == 5 and st[0].shape == (10, 3)
+    np.testing.assert_allclose(st[0][:, 0].numpy(), [1, 1, 1.2, 1.2, 0.8, 0.8, 1, 1, 1, 1])
+    np.testing.assert_allclose(st[1][:, 0].numpy(), [2, 2, 2, 2, 2, 2, 2.4, 2.4, 1.6, 1.6])
+    st, n = E._pertubate_fields(default_cfg({"data_assimilation": {"control_list": ["slidingco"]}}), f)
+    assert n == 3
+    np.testing.assert_allclose(st[3][:, 0].numpy(), [4, 4, 4.8, 4.8, 3.2, 3.2])
+    np.testing.assert_allclose(st[0][:, 0].numpy(), [1] * 6)
