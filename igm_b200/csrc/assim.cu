@@ -302,7 +302,10 @@ template <typename T, int TY, int TX>
 __global__ void __launch_bounds__(256) flow_direction_kernel(int ny, int nx, GaussW g, const T* u, const T* v, T* fx,
                                                              T* fy) {
   constexpr int HY = TY + 2 * kGaussR, HX = TX + 2 * kGaussR;
-  constexpr int PER = TY * TX / 256;
+  constexpr int PER = TY * TX / 256;  // outputs per thread: PER consecutive columns of one row
+  constexpr int RB = 4;               // rows per thread in the y pass
+  static_assert(TY % RB == 0 && TX % PER == 0, "tile");
+  const int xr = threadIdx.x / (TX / PER), xc0 = (threadIdx.x % (TX / PER)) * PER;
   // the staged values are T-rounded, held in double so the taps need no conversion
   __shared__ double A[HY][HX];
   __shared__ double Bs[TY][HX];
@@ -324,27 +327,44 @@ __global__ void __launch_bounds__(256) flow_direction_kernel(int ny, int nx, Gau
       A[hy][hx] = (double)val;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < TY * HX; i += 256) {
-      const int r = i / HX, hx = i - r * HX;
-      double sacc = 0.0;
+    // y pass: a thread takes RB consecutive rows of one column (RB + 24 reads for RB outputs);
+    // each output adds its 25 taps in the order of the single-output loop
+    for (int it = threadIdx.x; it < (TY / RB) * HX; it += 256) {
+      const int rb = it / HX, hx = it - rb * HX, r0 = rb * RB;
+      double sacc[RB];
 #pragma unroll
-      for (int k = 0; k <= 2 * kGaussR; ++k) sacc += g.w[k] * A[r + k][hx];
-      Bs[r][hx] = (double)(T)sacc;
+      for (int q = 0; q < RB; ++q) sacc[q] = 0.0;
+#pragma unroll
+      for (int k = 0; k < 2 * kGaussR + RB; ++k) {
+        const double v = A[r0 + k][hx];
+#pragma unroll
+        for (int q = 0; q < RB; ++q)
+          if (k - q >= 0 && k - q <= 2 * kGaussR) sacc[q] += g.w[k - q] * v;
+      }
+#pragma unroll
+      for (int q = 0; q < RB; ++q) Bs[r0 + q][hx] = (double)(T)sacc[q];
     }
     __syncthreads();
+    // x pass: a thread takes PER consecutive columns of one row
+    {
+      double sacc[PER];
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-      const int idx = threadIdx.x + 256 * q, r = idx / TX, c = idx - r * TX;
-      double sacc = 0.0;
+      for (int q = 0; q < PER; ++q) sacc[q] = 0.0;
 #pragma unroll
-      for (int k = 0; k <= 2 * kGaussR; ++k) sacc += g.w[k] * Bs[r][c + k];
-      res[comp][q] = (T)sacc;
+      for (int k = 0; k < 2 * kGaussR + PER; ++k) {
+        const double v = Bs[xr][xc0 + k];
+#pragma unroll
+        for (int q = 0; q < PER; ++q)
+          if (k - q >= 0 && k - q <= 2 * kGaussR) sacc[q] += g.w[k - q] * v;
+      }
+#pragma unroll
+      for (int q = 0; q < PER; ++q) res[comp][q] = (T)sacc[q];
     }
     __syncthreads();
   }
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
-    const int idx = threadIdx.x + 256 * q, r = idx / TX, c = idx - r * TX;
+    const int r = xr, c = xc0 + q;
     const int j = y0 + r, k = x0 + c;
     if (j >= cy || k >= cx) continue;
     T x = res[0][q], y = res[1][q];
