@@ -211,9 +211,11 @@ class CNN:
         nh = F * self.nout
         if self.nout <= F:
             # pixel part on CUDA cores, the head kernel gradient A16^T dY on the tensor cores
+            # data-only backward: no bf16 dY for the head's weight gradient, no partial sums
             rc = lib.igm_cnn_head_backward_tc(B, h, w, self.nz, _p(acts[self.L - 1]), hw, _p(dU), _p(dV),
-                                              self.out_scale, self.alpha, _p(g[0]), _p(buf["dyb"]),
-                                              _p(buf["hpart"]), npart2, st)
+                                              self.out_scale, self.alpha, _p(g[0]),
+                                              _p(buf["dyb"]) if param_grads else None,
+                                              _p(buf["hpart"]) if param_grads else None, npart2, st)
             L.check(rc, "igm_cnn_head_backward_tc")
         if self.nout <= F and param_grads:
             stride = self.nout + F

@@ -452,7 +452,7 @@ __device__ __forceinline__ void head_px_load(HeadPx<NJ>& q, size_t chunk, size_t
   }
 }
 
-template <int NJ>
+template <int NJ, bool PARAMS>
 __global__ void __launch_bounds__(kHpWarps * 32, 2)
     head_bwd_px_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act, const float* wh, const float* dU,
                        const float* dV, float out_scale, float alpha, __nv_bfloat16* dpre, __nv_bfloat16* dyb,
@@ -467,11 +467,12 @@ __global__ void __launch_bounds__(kHpWarps * 32, 2)
     swT[i] = j < nout ? wh[ci * nout + j] : 0.f;
   }
   __syncthreads();
-  float2 accb[NJ / 2], accd[kF / 2];  // this lane's sums of dY (j) and dPre16 (ci), channel pairs
+  // this lane's sums of dY (j) and dPre16 (ci) for the parameter gradients, channel pairs
+  float2 accb[PARAMS ? NJ / 2 : 1], accd[PARAMS ? kF / 2 : 1];
 #pragma unroll
-  for (int q = 0; q < NJ / 2; ++q) accb[q] = make_float2(0.f, 0.f);
+  for (int q = 0; q < (PARAMS ? NJ / 2 : 1); ++q) accb[q] = make_float2(0.f, 0.f);
 #pragma unroll
-  for (int q = 0; q < kF / 2; ++q) accd[q] = make_float2(0.f, 0.f);
+  for (int q = 0; q < (PARAMS ? kF / 2 : 1); ++q) accd[q] = make_float2(0.f, 0.f);
   const size_t plane = (size_t)H * W;
   const size_t total = plane * B;
   const size_t nchunks = (total + 31) / 32;
@@ -484,48 +485,51 @@ __global__ void __launch_bounds__(kHpWarps * 32, 2)
     asm volatile("" ::: "memory");
     HeadPx<NJ> cur;
     head_px_load<NJ>(cur, chunk, total, plane, H, W, nz, nout, A, dU, dV, out_scale, lane);
-    // dPre = dY Wh^T, two channels per packed fma
-    float2 da[kF / 2];
+    if (PARAMS) {
 #pragma unroll
-    for (int q = 0; q < kF / 2; ++q) da[q] = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int j = 0; j < NJ; ++j) {
-      const float2 gg = make_float2(cur.g[j], cur.g[j]);
-      const float4* wr = reinterpret_cast<const float4*>(swT + j * kF);
-#pragma unroll
-      for (int q = 0; q < kF / 4; ++q) {
-        const float4 w4 = wr[q];
-        da[2 * q] = __ffma2_rn(gg, make_float2(w4.x, w4.y), da[2 * q]);
-        da[2 * q + 1] = __ffma2_rn(gg, make_float2(w4.z, w4.w), da[2 * q + 1]);
-      }
+      for (int q = 0; q < NJ / 2; ++q)
+        accb[q] = __fadd2_rn(accb[q], make_float2(cur.g[2 * q], cur.g[2 * q + 1]));
     }
+    // dPre = dY Wh^T, two channels per packed fma, in two halves of the input channels (16 each)
+    // so that only half of the sums are live at once
 #pragma unroll
-    for (int q = 0; q < NJ / 2; ++q) accb[q] = __fadd2_rn(accb[q], make_float2(cur.g[2 * q], cur.g[2 * q + 1]));
-    uint4 po[4], yo[4];
+    for (int hf = 0; hf < 2; ++hf) {
+      float2 da[kF / 4];
 #pragma unroll
-    for (int ch = 0; ch < 4; ++ch) {
-      const uint32_t wv[4] = {cur.a[ch].x, cur.a[ch].y, cur.a[ch].z, cur.a[ch].w};
-      uint32_t pk[4], yk[4];
+      for (int q = 0; q < kF / 4; ++q) da[q] = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int c = ch * 8 + 2 * e;
-        const float2 m = make_float2(bf_lo(wv[e]) > 0.f ? 1.f : alpha, bf_hi(wv[e]) > 0.f ? 1.f : alpha);
-        const float2 d = __fmul2_rn(da[c >> 1], m);
-        accd[c >> 1] = __fadd2_rn(accd[c >> 1], d);
-        pk[e] = bf_pack(d.x, d.y);
-        yk[e] = c < NJ ? bf_pack(cur.g[c], cur.g[c + 1]) : 0u;
+      for (int j = 0; j < NJ; ++j) {
+        const float2 gg = make_float2(cur.g[j], cur.g[j]);
+        const float4* wr = reinterpret_cast<const float4*>(swT + j * kF + hf * (kF / 2));
+#pragma unroll
+        for (int q = 0; q < kF / 8; ++q) {
+          const float4 w4 = wr[q];
+          da[2 * q] = __ffma2_rn(gg, make_float2(w4.x, w4.y), da[2 * q]);
+          da[2 * q + 1] = __ffma2_rn(gg, make_float2(w4.z, w4.w), da[2 * q + 1]);
+        }
       }
-      po[ch] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-      yo[ch] = make_uint4(yk[0], yk[1], yk[2], yk[3]);
-    }
-    if (cur.ok) {
 #pragma unroll
-      for (int ch = 0; ch < 4; ++ch) {
-        DP[cur.o + (size_t)ch * W] = po[ch];
-        DY[cur.o + (size_t)ch * W] = yo[ch];
+      for (int cc = 0; cc < 2; ++cc) {
+        const int ch = 2 * hf + cc;  // 8-channel chunk
+        const uint32_t wv[4] = {cur.a[ch].x, cur.a[ch].y, cur.a[ch].z, cur.a[ch].w};
+        uint32_t pk[4], yk[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int c = ch * 8 + 2 * e;
+          const float2 m = make_float2(bf_lo(wv[e]) > 0.f ? 1.f : alpha, bf_hi(wv[e]) > 0.f ? 1.f : alpha);
+          const float2 d = __fmul2_rn(da[(c - hf * (kF / 2)) >> 1], m);
+          if (PARAMS) accd[c >> 1] = __fadd2_rn(accd[c >> 1], d);
+          pk[e] = bf_pack(d.x, d.y);
+          yk[e] = c < NJ ? bf_pack(cur.g[c], cur.g[c + 1]) : 0u;
+        }
+        if (cur.ok) {
+          DP[cur.o + (size_t)ch * W] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          if (PARAMS) DY[cur.o + (size_t)ch * W] = make_uint4(yk[0], yk[1], yk[2], yk[3]);
+        }
       }
     }
   }
+  if (!PARAMS) return;  // uniform: no partials in the data-only variant
 #pragma unroll
   for (int q = 0; q < NJ / 2; ++q) {
     const float x0 = warp_sum_fixed(accb[q].x), x1 = warp_sum_fixed(accb[q].y);
@@ -1162,16 +1166,21 @@ extern "C" int igm_cnn_head_backward_tc(int batch, int h, int w, int nz, const v
                                         void* dy_bf16, float* partials, int n_parts, void* stream) {
   IGM_CHECK_ARG(batch >= 1 && h >= 1 && w >= 1 && nz >= 1 && 2 * nz <= kF && n_parts >= 1, IGM_ERR_BAD_SHAPE,
                 "igm_cnn_head_backward_tc: bad shape (needs 2 nz <= 32)");
-  IGM_CHECK_ARG(act && head_w && dU && dV && dpre && dy_bf16 && partials, IGM_ERR_BAD_ARGUMENT,
-                "igm_cnn_head_backward_tc: NULL argument");
+  IGM_CHECK_ARG(act && head_w && dU && dV && dpre && ((dy_bf16 == nullptr) == (partials == nullptr)),
+                IGM_ERR_BAD_ARGUMENT, "igm_cnn_head_backward_tc: NULL argument");
   cudaStream_t st = as_stream(stream);
   const __nv_bfloat16* a16 = (const __nv_bfloat16*)act;
   __nv_bfloat16 *dp = (__nv_bfloat16*)dpre, *dy = (__nv_bfloat16*)dy_bf16;
+  const bool params = partials != nullptr;  // NULL dy_bf16 and partials: the data gradient only
   switch ((2 * nz + 3) / 4) {
 #define IGM_HEAD_PX(Q)                                                                                              \
   case Q:                                                                                                           \
-    head_bwd_px_kernel<4 * Q><<<n_parts, kHpWarps * 32, 0, st>>>(batch, h, w, nz, a16, head_w, dU, dV, out_scale,  \
-                                                                 alpha, dp, dy, partials);                          \
+    if (params)                                                                                                     \
+      head_bwd_px_kernel<4 * Q, true><<<n_parts, kHpWarps * 32, 0, st>>>(batch, h, w, nz, a16, head_w, dU, dV,     \
+                                                                         out_scale, alpha, dp, dy, partials);       \
+    else                                                                                                            \
+      head_bwd_px_kernel<4 * Q, false><<<n_parts, kHpWarps * 32, 0, st>>>(batch, h, w, nz, a16, head_w, dU, dV,    \
+                                                                          out_scale, alpha, dp, dy, partials);      \
     break;
     IGM_HEAD_PX(1) IGM_HEAD_PX(2) IGM_HEAD_PX(3) IGM_HEAD_PX(4) IGM_HEAD_PX(5) IGM_HEAD_PX(6) IGM_HEAD_PX(7)
     IGM_HEAD_PX(8)

@@ -555,7 +555,9 @@ IGM_API int igm_cnn_head_backward(int batch, int h, int w, int nz, const void* a
  * (dy_bf16; outputs beyond 2 nz zero) and per-CTA partials
  * [n_parts][2 nz + 32] of dbh and of the last conv layer's bias gradient.
  * The head kernel gradient is then igm_conv3x3_wgrad(act, dy_bf16) reduced by
- * igm_cnn_head_wgrad_finish. */
+ * igm_cnn_head_wgrad_finish.  With dy_bf16 and partials both NULL only dpre is
+ * written (the data gradient, as the input-field gradient of data
+ * assimilation needs). */
 IGM_API int igm_cnn_head_backward_tc(int batch, int h, int w, int nz, const void* act, const float* head_w,
                                      const float* dU, const float* dV, float out_scale, float alpha, void* dpre,
                                      void* dy_bf16, float* partials, int n_parts, void* stream);
