@@ -265,8 +265,6 @@ class CNN:
                     L.check(rc, "igm_cnn_wgrad_finish_split")
             if l > 0:
                 nxt = g[1 - cur]
-                if param_grads:
-                    buf["dbpart"].zero_()
                 rc = lib.igm_conv3x3(1, B, h, w, F, _p(gl), self._wb(l), None, _p(acts[l - 1]), _p(nxt),
                                      _p(buf["dbpart"]) if param_grads else None, npart, self.alpha, _p(self.err), st)
                 L.check(rc, f"igm_conv3x3 dgrad layer {l}")

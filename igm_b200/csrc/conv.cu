@@ -543,6 +543,16 @@ static int conv_launch(int B, int H, int W, const void* x, const void* wpack, co
     a.db_partial = db_partial;
   }
   if (grid < 1) grid = 1;
+  if (db_partial && grid < db_slots) {
+    // each CTA writes its own slot of bias-gradient partials; the slots beyond the grid are zeroed
+    // here, so the caller's reduction over all db_slots needs no cleared buffer
+    cudaError_t e = cudaMemsetAsync(db_partial + (size_t)grid * kCout, 0,
+                                    (size_t)(db_slots - grid) * kCout * sizeof(float), st);
+    if (e != cudaSuccess) {
+      set_error("igm_conv3x3: clearing the partials: %s", cudaGetErrorString(e));
+      return IGM_ERR_CUDA;
+    }
+  }
   conv3x3_kernel<C8_IN, kRows, EPI><<<grid, kConvThreads, G::SMEM, st>>>(a);
   return launch_status("conv3x3_kernel");
 }

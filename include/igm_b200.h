@@ -477,7 +477,8 @@ IGM_API int igm_cfl_dt(const float* velomax, float* dt_out, double cfl, double d
  *    layer's dgrad pack; y = (dL/d input of the layer) * (act_mask > 0 ? 1 : alpha),
  *    i.e. the gradient w.r.t. the previous layer's pre-activation.  When
  *    db_partials is not NULL it receives per-CTA sums of y over the pixels
- *    ([db_slots][32]; slots beyond the CTAs used are left untouched).
+ *    ([db_slots][32]; slots beyond the CTAs used are zeroed, so every slot is
+ *    written and a fixed-order reduction over all db_slots needs no clearing).
  * err (device int, may be NULL) is set non-zero if a pipeline wait timed out. */
 IGM_API int igm_conv3x3(int mode, int batch, int height, int width, int cin, const void* x, const void* wpack,
                         const float* bias, const void* act_mask, void* y, float* db_partials, int db_slots,
