@@ -156,6 +156,10 @@ __device__ __forceinline__ T limited_slope(T hm, T h0, T hp, T dx, T rdx, int sl
 // (IEEE division by dx through div_dx, no contraction), so the result is
 // bit-identical to evaluating each face of the reference on its own.
 constexpr int kTmCols = 30;  // interior columns per warp
+#ifndef IGM_TM_MIN_ROWS
+#define IGM_TM_MIN_ROWS 8
+#endif
+constexpr int kTmMinRows = IGM_TM_MIN_ROWS;  // shortest row segment of a warp (even)
 constexpr int kTmWarps = 4;  // warps per CTA
 
 template <typename T, int SLOPE>
@@ -366,11 +370,11 @@ static int transport_t(int ny, int nx, double dx, const void* u, const void* v, 
   a.dt_dev = dt_dev;
   a.u = (const T*)u; a.v = (const T*)v; a.h = (const T*)h; a.h_out = (T*)h_out; a.topg = (const T*)topg;
   a.smb = (const T*)smb; a.usurf = (T*)usurf; a.lsurf = (T*)lsurf; a.divflux = (T*)divflux;
-  // segments of rows sized for about 32 resident warps per SM, at least 8 rows
+  // segments of rows sized for about 32 resident warps per SM, at least kTmMinRows rows
   const int n_strips = (nx + kTmCols - 1) / kTmCols;
   const long long target = 148LL * 32;
   int rows = (int)((n_strips * (long long)ny + target - 1) / target);
-  rows = rows < 8 ? 8 : rows;
+  rows = rows < kTmMinRows ? kTmMinRows : rows;
   rows += rows & 1;
   const long long warps = (long long)n_strips * ((ny + rows - 1) / rows);
   const int grid = (int)((warps + kTmWarps - 1) / kTmWarps);
