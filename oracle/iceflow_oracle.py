@@ -16,9 +16,9 @@ TensorFlow code for the path (all paths relative to the reference project):
   - the per-term ``reduce_mean`` + ``add_n`` of ``igm/processes/iceflow/solve/solve.py:57-59``
 * vertical discretisation ``igm/processes/iceflow/vert_disc.py:10-47``
 * velbase / velsurf / velbar ``igm/processes/iceflow/utils.py:21-51``
-* vertical velocity, vert_flow version 2, kinematic method
-  ``igm/processes/vert_flow/vert_flow_v2.py:17-37,62-87,126-147`` with
-  ``compute_dz`` of ``igm/processes/iceflow/vert_disc.py:17-23``
+* vertical velocity, vert_flow version 2, kinematic and incompressibility
+  methods ``igm/processes/vert_flow/vert_flow_v2.py:17-60,62-87,126-147``
+  with ``compute_dz`` of ``igm/processes/iceflow/vert_disc.py:17-23``
 * EarlyStopping ``igm/processes/iceflow/utils.py:80-110``
 * the plain solver loop ``igm/processes/iceflow/solve/solve.py:22-119``
 * Keras legacy Adam (TF 2.15.1, third party, not vendored): the published
@@ -33,7 +33,16 @@ TensorFlow code for the path (all paths relative to the reference project):
 * ELA mass balance ``igm/processes/smb_simple/smb_simple.py:24-50``
 * the CNN emulator ``igm/processes/iceflow/emulate/neural_network.py:9-66``
   (Conv2D 3x3 "same" + bias + LeakyReLU(0.01), 1x1 head), with the NHWC
-  layout conversions of ``igm/processes/iceflow/utils.py:133-158``.
+  layout conversions of ``igm/processes/iceflow/utils.py:133-158``; its
+  retraining loop ``igm/processes/iceflow/emulate/emulate.py:155-328``
+  (patches, pertubate_X)
+* data assimilation ``igm/processes/data_assimilation``: the cost terms of
+  ``cost_terms/*.py`` (misfit_velsurf with the low-speed term, misfit_thk,
+  misfit_usurf, regu_thk, regu_slidingco, regu_arrhenius, cost_divfluxobs,
+  cost_divfluxfcz, the penalties of total_cost), ``compute_divflux``
+  (``igm/utils/gradient/compute_divflux.py:6-51``), the flow direction and
+  density weights and the rms/std record of ``utils.py``, and one ADAM
+  iteration of ``optimize/update.py:15-103`` over the controls.
 
 All functions take and return ``torch`` CPU tensors; the dtype of the inputs
 (float32 or float64) is the arithmetic precision.  Gradients of the energy are
@@ -48,7 +57,6 @@ TensorFlow cannot be installed here) and stores the results as fixtures;
 
 from __future__ import annotations
 
-import math
 from dataclasses import dataclass, field
 
 import numpy as np
