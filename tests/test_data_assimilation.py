@@ -83,18 +83,3 @@ def test_cost_table_follows_total_cost_order():
     assert keys == ["velsurf", "thk", "divflux", "usurf", "icemask", "thk_positive", "slidingco_positive",
                     "thk_regu", "slid_regu"]
     np.testing.assert_array_equal(table[1], [6, 7, 7.0, 11, 8, 9, 100.0, 10, 200.0])
-
-
-def test_pertubate_field_selection():
-    """pertubate_X's copies: thk and usurf without data assimilation, the
-    controls with it; each scaled copy stacked along y."""
-    from igm_b200 import emulator as E
-    f = [torch.full((2, 3), float(k + 1)) for k in range(4)]
-    st, n = E._pertubate_fields(default_cfg(), f)
-    assert n == 5 and st[0].shape == (10, 3)
-    np.testing.assert_allclose(st[0][:, 0].numpy(), [1, 1, 1.2, 1.2, 0.8, 0.8, 1, 1, 1, 1])
-    np.testing.assert_allclose(st[1][:, 0].numpy(), [2, 2, 2, 2, 2, 2, 2.4, 2.4, 1.6, 1.6])
-    st, n = E._pertubate_fields(default_cfg({"data_assimilation": {"control_list": ["slidingco"]}}), f)
-    assert n == 3
-    np.testing.assert_allclose(st[3][:, 0].numpy(), [4, 4, 4.8, 4.8, 3.2, 3.2])
-    np.testing.assert_allclose(st[0][:, 0].numpy(), [1] * 6)
