@@ -76,3 +76,60 @@ def test_vertical_velocity_incompressibility_validation_without_gpu(lib):
     assert rc == 1 and b"nz, ny, nx >= 2" in lib.igm_last_error()
     rc = lib.igm_vertical_velocity_incompressibility(7, 2, 5, 5, 100.0, 16, 32, 48, 64, lv, lv, 80, None)
     assert rc == 2 and b"dtype" in lib.igm_last_error()
+
+
+def test_assimilation_entries_validate_without_gpu(lib):
+    """The data-assimilation entry points reject bad arguments before any
+    launch, with the status and message of the C ABI."""
+    p = L.AssimParams()
+    p.velsurfobs_std, p.thkobs_std, p.regu_thk, p.aniso_factor, p.n_vel, p.n_thk = 1.0, 3.0, 10.0, 1.0, 1.0, 1.0
+    args = [16] * 11  # thk .. flowdiry: placeholders, never dereferenced on these paths
+    rc = lib.igm_assim_cost_grad(0, 1, 5, 100.0, *args, None, C.byref(p), 16, 16, 16, None, 16, 4, 16, None)
+    assert rc == 1 and b"bad shape" in lib.igm_last_error()
+    rc = lib.igm_assim_cost_grad(0, 5, 5, 100.0, None, *args[1:], None, C.byref(p), 16, 16, 16, None, 16, 4, 16, None)
+    assert rc == 2 and b"NULL" in lib.igm_last_error()
+    p.aniso_factor = 0.2
+    a2 = args[:9] + [None, None]
+    rc = lib.igm_assim_cost_grad(0, 5, 5, 100.0, *a2, None, C.byref(p), 16, 16, 16, None, 16, 4, 16, None)
+    assert rc == 2 and b"flowdirx" in lib.igm_last_error()
+    p.aniso_factor, p.usurf_cost, p.usurfobs_std = 1.0, 1, 2.0
+    rc = lib.igm_assim_cost_grad(0, 5, 5, 100.0, *args, None, C.byref(p), 16, 16, 16, None, 16, 4, 16, None)
+    assert rc == 2 and b"misfit_usurf" in lib.igm_last_error()
+    rc = lib.igm_assim_field_regu(0, 5, 5, 100.0, 16, None, None, 1.0, 1.0, 1, 0.0, 0, None, 1, 16, 16, 4, 16, None)
+    assert rc == 2 and b"sole_mask" in lib.igm_last_error()
+    rc = lib.igm_assim_field_regu(0, 5, 5, 100.0, 16, None, None, 1.0, 0.3, 1, 0.0, 0, None, 0, 16, 16, 4, 16, None)
+    assert rc == 2 and b"flowdirx" in lib.igm_last_error()
+    cp = L.AssimControlParams()
+    cp.mode, cp.scale = 3, 1.0
+    rc = lib.igm_assim_control(0, 25, C.byref(cp), 16, 16, None, 16, 16, 16, 16, 16, None)
+    assert rc == 2 and b"bad mode" in lib.igm_last_error()
+    cp.mode, cp.mask = 1, 1
+    rc = lib.igm_assim_control(0, 25, C.byref(cp), 16, None, None, 16, 16, 16, 16, 16, None)
+    assert rc == 2 and b"NULL" in lib.igm_last_error()
+    rc = lib.igm_divflux(0, 5, 5, 5, 100.0, 16, 16, 16, 16, None)
+    assert rc == 2 and b"unknown method" in lib.igm_last_error()
+    dp = L.DivfluxCostParams()
+    dp.kind, dp.divfluxobs_std = 0, 1.0
+    w = (C.c_double * 1)(1.0)
+    rc = lib.igm_assim_divflux_cost_grad(0, 5, 5, 100.0, 1, w, 16, 16, 16, 16, None, None, 16, None, C.byref(dp), 16,
+                                         16, 16, 16, 16, 4, 16, None)
+    assert rc == 2 and b"kind 0 needs divfluxobs" in lib.igm_last_error()
+    rc = lib.igm_assim_stats(0, 5, 5, 100.0, None, None, None, None, None, None, 16, None, None, None, None, 16, 4,
+                             16, None)
+    assert rc == 2 and b"NULL" in lib.igm_last_error()
+    rc = lib.igm_assim_low_speed(0, 5, 5, 16, 16, None, 16, 16, 16, 16, 4, 16, None)
+    assert rc == 2 and b"NULL" in lib.igm_last_error()
+
+
+def test_emulator_entries_validate_without_gpu(lib):
+    sc = (C.c_double * 5)(*[1.0] * 5)
+    rc = lib.igm_cnn_input_gradient(1, 8, 8, 5, 6, 16, 16, sc, 16, None)
+    assert rc == 1 and b"bad shape" in lib.igm_last_error()
+    rc = lib.igm_cnn_head_backward_tc(1, 8, 8, 10, 16, 16, 16, 16, 1.0, 0.01, 16, None, 16, 4, None)
+    assert rc == 2 and b"NULL" in lib.igm_last_error()
+    offs = (C.c_size_t * 3)(0, 5000, 5001)
+    assert lib.igm_adam_norms_len(2, offs) == 2 + 2 + 1  # the norms, then 4096-element chunks per variable
+    assert lib.igm_adam_norms_len(0, offs) == 0
+    empty = (C.c_size_t * 3)(0, 10, 10)
+    rc = lib.igm_adam_clipnorm(2, empty, 16, 16, 16, 16, 16, 1e-3, 0.9, 0.999, 1e-7, 1.0, 1, None)
+    assert rc == 2 and b"empty variable" in lib.igm_last_error()
