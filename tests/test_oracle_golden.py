@@ -204,7 +204,7 @@ def test_assimilation_costs_and_gradients(golden, tag):
     tol = 1e-10 if g["thk"].dtype == np.float64 else 1e-5
     for k, ref in [("velsurf", "c_vel"), ("thk", "c_thk"), ("icemask", "c_ice"), ("thk_positive", "c_pos"),
                    ("thk_regu", "c_reg")]:
-        np.testing.assert_allclose(float(c[k]), float(g[ref]), rtol=tol, atol=tol * abs(float(g[ref])) + 1e-30)
+        np.testing.assert_allclose(c[k].item(), float(g[ref]), rtol=tol, atol=tol * abs(float(g[ref])) + 1e-30)
     gt, gu, gv = torch.autograd.grad(sum(c.values()), [thk, uvs, vvs])
     for a, ref in [(gt, "g_thk"), (gu, "g_u"), (gv, "g_v")]:
         np.testing.assert_allclose(a.numpy(), g[ref], rtol=tol, atol=tol * np.abs(g[ref]).max())
@@ -256,7 +256,7 @@ def test_divflux_cost_terms(golden, tag, method, kind):
         c = O.da_cost_divflux("obs", u, v, h, dx, t["icemaskobs"], divfluxobs=t["divfluxobs"], **kw)
     gu, gv, gh = torch.autograd.grad(c, [u, v, h])
     tol = 1e-12 if tag == "f64" else 2e-5
-    np.testing.assert_allclose(float(c), float(g[f"{key}_cost"]), rtol=tol)
+    np.testing.assert_allclose(c.item(), float(g[f"{key}_cost"]), rtol=tol)
     for a, k in [(gu, "g_u"), (gv, "g_v"), (gh, "g_h")]:
         ref = g[f"{key}_{k}"]
         np.testing.assert_allclose(a.numpy(), ref, rtol=tol, atol=tol * np.abs(ref).max())
