@@ -4,7 +4,6 @@ ELA mass balance from a [time, gradabl, gradacc, ela, maxacc] table."""
 from __future__ import annotations
 
 import numpy as np
-import torch
 
 from .. import kernels as K
 from .. import state as S
