@@ -499,6 +499,8 @@ __global__ void assim_control_kernel(size_t n, igm_assim_control_params p, const
       const T g = g_direct[o] + (g_emul ? (T)g_emul[o] : T(0));
       const T dxdw = p.transform ? T(2) * (T)var[o] * sc : sc;
       grad[o] = on ? (float)(g * dxdw) : 0.f;
+    } else if (p.mode == 3) {
+      if (!(icemaskobs[o] > T(0.5))) x[o] = T(0);
     } else {
       const T w = (T)var[o];
       T t = p.transform ? (w * w) * sc : w * sc;
@@ -929,11 +931,13 @@ extern "C" int igm_assim_flow_direction(int dtype, int ny, int nx, const void* u
 extern "C" int igm_assim_control(int dtype, size_t n, const igm_assim_control_params* params, void* x,
                                  const void* grad_direct, const float* grad_emulator, const void* icemaskobs,
                                  float* variable, float* grad, float* m, float* v, void* stream) {
-  IGM_CHECK_ARG(params && n >= 1 && params->scale > 0 && params->mode >= 0 && params->mode <= 2,
+  IGM_CHECK_ARG(params && n >= 1 && params->scale > 0 && params->mode >= 0 && params->mode <= 3,
                 IGM_ERR_BAD_ARGUMENT, "igm_assim_control: bad mode, size or scale");
   const igm_assim_control_params& p = *params;
-  IGM_CHECK_ARG(x && variable && (p.mode != 0 || (m && v)) && (p.mode != 1 || (grad_direct && grad)) &&
-                    ((p.mode == 1 && p.mask != 0) || (p.mode == 2 && p.reproject == 1 && p.reproject_mask)
+  IGM_CHECK_ARG(x && (variable || p.mode == 3) && (p.mode != 0 || (m && v)) &&
+                    (p.mode != 1 || (grad_direct && grad)) &&
+                    ((p.mode == 1 && p.mask != 0) || (p.mode == 2 && p.reproject == 1 && p.reproject_mask) ||
+                             p.mode == 3
                          ? icemaskobs != nullptr
                          : true),
                 IGM_ERR_BAD_ARGUMENT, "igm_assim_control: NULL argument");

@@ -747,6 +747,7 @@ __global__ void __launch_bounds__(kCW* TYP, MinBlocks<T, MODE>::value)
   if (tid == 0) {
     *a.counter = 0u;
     const bool lost = a.err && __ldcg(a.err) != 0;
+    if (lost) *a.err = 0;  // reported through this launch's terms / status; the next launch starts clean
     if (a.terms) {
       a.terms[0] = lost ? nan("") : t0;
       a.terms[1] = lost ? nan("") : t1;

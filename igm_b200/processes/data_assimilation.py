@@ -329,6 +329,11 @@ def optimize_update(cfg, state, cost, i):
         K.assim_control(2, x[c], a.scale[c], icemaskobs=a.icemaskobs, variable=a.block(a.var, k),
                         **a.control_kw(c))
         S.put(state, c, x[c])
+    if a.reproject and "icemask" in a.cost_list and "thk" not in a.controls:
+        # update.py:84-88: thk is masked by the reprojection even when it is not a control
+        thk = S.get(state, "thk").contiguous()
+        K.assim_control(3, thk, 1.0, icemaskobs=a.icemaskobs)
+        S.put(state, "thk", thk)
     thk = S.get(state, "thk").contiguous()
     S.put(state, "divflux", K.divflux(S.get(state, "ubar").contiguous(), S.get(state, "vbar").contiguous(), thk,
                                       a.dx, a.div_method))

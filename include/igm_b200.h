@@ -167,7 +167,9 @@ IGM_API int igm_energy(int dtype, const igm_grid* grid, const igm_physics* phys,
  *    batch 2) is rejected with IGM_ERR_WORKSPACE and no launch.
  *  - The first call on a device looks up the array's device address
  *    (cudaGetSymbolAddress) with that device current; make that first call
- *    before any stream capture.
+ *    before any stream capture.  The address is kept for the life of the
+ *    process: the library does not survive a cudaDeviceReset (or a reset of
+ *    the primary context) -- reload it after one.
  *  - All calls share the one array, which keeps the last call's contents;
  *    each call clears the counter it needs at zero on its stream.  Calls that
  *    overlap on the GPU (other streams, other host threads) race on the array:
@@ -340,13 +342,17 @@ IGM_API int igm_assim_field_regu(int dtype, int ny, int nx, double dx, const voi
  *   mode 2 (after igm_adam_clipnorm): x from the variable, then the
  *     reprojection (reproject 1, thk: 0 outside icemaskobs > 0.5 when
  *     reproject_mask, then x >= 0; 2: x >= lower, 0 for slidingco, 1 for
- *     arrhenius; 0: none).
+ *     arrhenius; 0: none);
+ *   mode 3 (after mode 2, for a thk that is not a control): x = 0 outside
+ *     icemaskobs > 0.5 -- the reference's reprojection applies this whenever
+ *     "reproject" is an obstacle constraint and "icemask" is in cost_list
+ *     (optimize/update.py:84-88); reads only x and icemaskobs.
  * variable, grad, m, v and grad_emulator (the emulator's input-field gradient,
  * igm_cnn_input_gradient) are device float[n], x, grad_direct and icemaskobs
  * [n] of the dtype; grad_emulator may be NULL; arguments a mode does not read
  * may be NULL. */
 typedef struct igm_assim_control_params {
-  int32_t mode;            /* 0, 1, 2 as above */
+  int32_t mode;            /* 0, 1, 2, 3 as above */
   int32_t transform;       /* 0: x = variable scale; 1: x = variable^2 scale */
   int32_t mask;            /* 0 none, 1 icemaskobs > 0.5, 2 icemaskobs == 1 */
   int32_t reproject;       /* 0 none, 1 thk, 2 lower bound */

@@ -1001,10 +1001,12 @@ def da_optimize_step(fields, dx, weights, biases, Nz, vert_weight, obs, p: Assim
     for c, w in zip(mc.controls, new_vars):
         out[c] = (w ** 2) * sc[c] if (c == "slidingco" and mc.log_slidingco) else w * sc[c]
     if ctl.reproject:
+        # update.py:84-91: the icemask reprojection of thk applies whenever "icemask" is a cost, thk a control
+        # or not; the bound thk >= 0 only when thk is a control
+        if ctl.icemask_cost:
+            out["thk"] = torch.where(inside, out["thk"], torch.zeros_like(out["thk"]))
         if "thk" in mc.controls:
             t = out["thk"]
-            if ctl.icemask_cost:
-                t = torch.where(inside, t, torch.zeros_like(t))
             out["thk"] = torch.where(t < 0, torch.zeros_like(t), t)
         if "slidingco" in mc.controls:
             out["slidingco"] = torch.where(out["slidingco"] < 0, torch.zeros_like(out["slidingco"]), out["slidingco"])

@@ -100,7 +100,7 @@ def test_assimilation_entries_validate_without_gpu(lib):
     rc = lib.igm_assim_field_regu(0, 5, 5, 100.0, 16, None, None, 1.0, 0.3, 1, 0.0, 0, None, 0, 16, 16, 4, 16, None)
     assert rc == 2 and b"flowdirx" in lib.igm_last_error()
     cp = L.AssimControlParams()
-    cp.mode, cp.scale = 3, 1.0
+    cp.mode, cp.scale = 4, 1.0
     rc = lib.igm_assim_control(0, 25, C.byref(cp), 16, 16, None, 16, 16, 16, 16, 16, None)
     assert rc == 2 and b"bad mode" in lib.igm_last_error()
     cp.mode, cp.mask = 1, 1

@@ -189,3 +189,43 @@ def test_perturbed_retraining_gradient_matches_oracle(with_da):
     for i, (sh, gr) in enumerate(zip(net.shapes, grads)):
         e = rel_l2(g[net.offsets[i]:net.offsets[i + 1]].reshape(sh), gr.numpy())
         assert e < 5e-2, (i, sh, e)
+
+
+def test_production_network_forward_and_gradient_match_oracle():
+    """The network of the benchmark, 16 layers of 3x3 x 32 filters and the
+    1x1 head to 2 Nz = 20 channels, at 128 x 128: forward and the physics
+    gradient of every variable against the oracle (same bf16 operand
+    rounding).  Over 16 layers an activation that lands on the other side of
+    a bf16 rounding boundary (different FP32 accumulation orders) carries
+    its one-ulp difference forward, so the bounds are 2e-2 (forward) and
+    1e-1 (parameter gradients, relative L2 per variable)."""
+    nl, nz, ny, nx, dx = 16, 10, 128, 128, 100.0
+    st, net, f = setup(nl, nz, ny, nx, seed=11)
+    ws, bs = oracle_params(net)
+    params = []
+    for w, b in zip(ws, bs):
+        params += [w.clone().requires_grad_(True), b.clone().requires_grad_(True)]
+    X = oracle_X(st, dx)
+    Y = O.cnn_forward(X, params[0::2], params[1::2], bf16=True, bf16_first=False, out_scale=OUT)
+    Uo, Vo = O.Y_to_UV(Y, nz)
+    buf = net.buffers(1, ny, nx, train=False)
+    net.prepare_input(f, dx, [(0, 0)], ny, nx, buf)
+    U, V = net.forward(buf, 1, ny, nx)
+    eu, ev = rel_l2(U.cpu().numpy(), Uo.detach().numpy()), rel_l2(V.cpu().numpy(), Vo.detach().numpy())
+    print(f"16-layer forward: U {eu:.2e}, V {ev:.2e}")
+    assert eu < 2e-2 and ev < 2e-2
+    dz = O.compute_zeta_dzeta(O.compute_levels(nz, 4.0))[1]
+    fl = [torch.as_tensor(st[k])[None] for k in ["thk", "usurf", "arrhenius", "slidingco"]]
+    cost, _ = O.energy(Uo, Vo, *fl, dx, dz)
+    grads = torch.autograd.grad(cost, params)
+    opt = EmulatorOptimizer(lr=1e-3, epsilon=1e-7, clipnorm=1.0)
+    terms = train_step(net, f, dx, [(0, 0)], ny, nx, dz.numpy(), None, 1e-3, opt)
+    net.check_errors()
+    np.testing.assert_allclose(float(terms.sum()) / ((ny - 1) * (nx - 1)), float(cost), rtol=2e-2)
+    g = net.grads.cpu().numpy()
+    worst = 0.0
+    for i, (s, gr) in enumerate(zip(net.shapes, grads)):
+        e = rel_l2(g[net.offsets[i]:net.offsets[i + 1]].reshape(s), gr.numpy())
+        worst = max(worst, e)
+        assert e < 1e-1, (i, s, e)
+    print(f"16-layer parameter gradients: worst relative L2 {worst:.2e}")

@@ -293,3 +293,47 @@ def test_other_controls_in_the_loop_match_oracle(tmp_path, monkeypatch, controls
             assert agree.mean() >= 0.95, (c, i, agree.mean())
         # carry on from the same fields on both sides
         fields = {k: getattr(st, k).detach().cpu().clone() for k in ("thk", "usurf", "arrhenius", "slidingco")}
+
+
+def test_icemask_reprojection_when_thk_is_not_a_control(tmp_path, monkeypatch):
+    """optimize/update.py:84-88: with "reproject" among the obstacle
+    constraints and "icemask" among the costs, thk is set to zero outside
+    icemaskobs > 0.5 after every iteration even when only slidingco is
+    inverted.  The thickness starts from thkinit (the true tongue) while the
+    observed mask leaves out its downstream third; two iterations against the
+    oracle's da_optimize_step: the thickness bit for bit, slidingco's gradient
+    and the costs as test_other_controls_in_the_loop_match_oracle."""
+    monkeypatch.chdir(tmp_path)
+    cfg = make_cfg(2)
+    da = cfg.processes.data_assimilation
+    da.control_list = ["slidingco"]
+    assert "reproject" in da.optimization.obstacle_constraint and "icemask" in da.cost_list
+    g = twin_glacier()
+    st = twin_state(cfg, g)
+    st.icemaskobs[:, 47:] = 0.0
+    st.thkinit = st.thk.clone()
+    setup = oracle_setup(cfg, st)
+    ws, bs, obs, p, ctl, opt, _ = setup
+    r = da.regularization
+    mc = O.AssimControls(controls=["slidingco"], scaling={"slidingco": float(da.scaling.slidingco)},
+                         regu_slidingco=float(r.slidingco), aniso_sl=float(r.smooth_anisotropy_factor_sl))
+    DA.optimize_initialize(cfg, st)
+    a = st._igm_assim
+    fields = {k: getattr(st, k).detach().cpu().clone() for k in ("thk", "usurf", "arrhenius", "slidingco")}
+    outside = (st.icemaskobs.cpu() <= 0.5) & (fields["thk"] > 0)
+    assert int(outside.sum()) > 50
+    for i in range(2):
+        cost = {}
+        DA.optimize_update(cfg, st, cost, i)
+        fields_o, cost_o, aux = O.da_optimize_step(fields, float(st.dx), ws, bs, NZ,
+                                                   torch.as_tensor(O.define_vertical_weight(NZ, 4.0)), obs, p, ctl,
+                                                   opt, i, mc, bf16=True, out_scale=OUT, input_scales=SCALES)
+        np.testing.assert_array_equal(st.thk.cpu().numpy(), fields_o["thk"].numpy())
+        assert float(st.thk.cpu()[outside].abs().max()) == 0.0
+        ours = dict(zip(DA._COST_KEYS, cost["all"].cpu().numpy()))
+        fc = cost["slidingco"].cpu().numpy()
+        ours["slidingco_positive"], ours["slid_regu"] = fc[3], fc[4]
+        for k, v in cost_o.items():
+            np.testing.assert_allclose(ours[k], float(v), rtol=2e-2, atol=1e-6, err_msg=f"{k} at {i}")
+        assert rel_l2(a.block(a.grad, 0).view(a.ny, a.nx).cpu().numpy(), aux["gradient_slidingco"].numpy()) < 5e-2
+        fields = {k: getattr(st, k).detach().cpu().clone() for k in ("thk", "usurf", "arrhenius", "slidingco")}

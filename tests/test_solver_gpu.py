@@ -119,3 +119,19 @@ def test_max_iter_caps_and_no_early_stop():
     _, _, c = s.solve(Z, Z, *[dev(st[k]) for k in ["thk", "usurf", "arrhenius", "slidingco"]], 100.0, dz,
                       nbitmax=7, early_stopping=False)
     assert len(c) == 7 and s.iterations == 7
+
+
+@pytest.mark.parametrize("n", [1, 10])
+def test_fp32_solver_matches_fp32_oracle_to_1e5(n):
+    """FP32 against the FP32 restatement of the reference solver on the same
+    inputs, relative L2 of the velocities <= 1e-5, where the comparison is
+    well posed: after 1 and 10 iterations the trajectory has not yet
+    amplified the two sides' different FP32 summation orders (at 100
+    iterations it has: see test_fp32_solver_error_against_fp64)."""
+    st = O.valley_glacier(40, 36, 100.0, seed=2)
+    ref, cref = _oracle_solve(st, 10, torch.float32, n)
+    got, c = _device_solve(st, 10, torch.float32, n)
+    e = rel_l2(got, ref)
+    print(f"n={n}: device FP32 vs oracle FP32 {e:.3e}")
+    assert e <= 1e-5, e
+    np.testing.assert_allclose(c, cref, rtol=1e-5)

@@ -67,6 +67,11 @@ def test_noalloc_matches_workspace_version_on_two_calls(dtype):
 def test_noalloc_rejects_grid_beyond_its_scratch():
     U, V, f, dz = _case(20, 20, 4, torch.float32, 3)
     g = L.make_grid(2, 4, 4096, 4096, 100.0, dz)  # needs more than the fixed array; nothing is launched
+    # the buffers below are 20 x 20: the call is made only while this grid's scratch exceeds the
+    # fixed array, so that the size check, not the launch, decides the outcome
+    need = int(L.lib().igm_workspace_size(C.byref(g)))
+    if need <= (2 << 20):
+        pytest.fail(f"grid needs only {need} bytes of scratch: it would not be rejected, not calling")
     ph = L.make_physics()
     fs = K.fields_struct(*f)
     terms = torch.zeros(3, dtype=torch.float64, device="cuda")
