@@ -108,6 +108,7 @@ SIGNATURES = {
     "igm_vertical_velocity_incompressibility": (I, [I, I, I, I, D, P, P, P, P, P, P, P, P]),
     "igm_smb_simple": (I, [I, I, P, P, P, D, D, D, D, P]),
     "igm_absmax2": (I, [I, I, P, P, P, P]),
+    "igm_force_max_velbar": (I, [I, C.c_size_t, P, P, D, P]),
     "igm_cfl_dt": (I, [P, P, D, D, D, P]),
     "igm_conv3x3": (I, [I, I, I, I, I, P, P, P, P, P, P, I, C.c_float, P, P]),
     "igm_conv3x3_wgrad": (I, [I, I, I, I, P, P, P, I, P, P]),

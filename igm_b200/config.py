@@ -39,7 +39,9 @@ DEFAULTS = {
         },
         "numerics": {"Nz": 10, "vert_spacing": 4.0, "staggered_grid": 1, "vert_basis": "Lagrange"},
         "solver": {"step_size": 1.0, "nbitmax": 100, "stop_if_no_decrease": True, "optimizer": "Adam",
-                   "lbfgs": False, "save_cost": "", "plot_sol": False},
+                   "lbfgs": False, "save_cost": "", "plot_sol": False,
+                   # (igm_b200) EarlyStopping(2e-4, 10) of solve.py:36,112; False runs nbitmax iterations
+                   "early_stopping": True},
         "emulator": {
             "fieldin": ["thk", "usurf", "arrhenius", "slidingco", "dX"],
             "retrain_freq": 10,
@@ -84,8 +86,10 @@ DEFAULTS = {
         # (igm_b200) emulator fallback / judge: every `every` updates the plain
         # solver is run from the emulated velocities; when the emulated energy
         # exceeds the solved one by more than `margin` (relative), the solved
-        # velocities replace the emulated ones.  every <= 0 disables it.
-        "fallback": {"every": 0, "margin": 0.02, "nbitmax": 100},
+        # velocities replace the emulated ones: until the next check, each update
+        # then a warm-started solve ("takeover"), or for that update alone
+        # ("step").  every <= 0 disables it.
+        "fallback": {"every": 0, "margin": 0.02, "nbitmax": 100, "mode": "takeover"},
     },
     "thk": {"slope_type": "superbee", "ratio_density": 0.910, "default_sealevel": 0.0},
     "vert_flow": {"version": 2, "method": "kinematic"},

@@ -322,6 +322,24 @@ __global__ void absmax2_kernel(int n, const T* a, const T* b, float* out) {
   if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, m);
 }
 
+// force_max_velbar (igm/processes/iceflow/utils.py:182-194, Lagrange basis):
+// per node and level, with mag = |(U, V)| (tf.norm of the stacked pair:
+// sqrt(U U + V V), no fused multiply-add), U = cap (U / mag) and V = cap
+// (V / mag) where mag >= cap, else unchanged; IEEE division, as the reference
+// graph.
+template <typename T>
+__global__ void force_max_velbar_kernel(size_t n, T* U, T* V, T cap) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const T u = U[i], v = V[i];
+    // this unit is compiled with -fmad=false and IEEE division / square root
+    const T mag = Math<T>::sqrt(u * u + v * v);
+    if (mag >= cap) {
+      U[i] = cap * (u / mag);
+      V[i] = cap * (v / mag);
+    }
+  }
+}
+
 __global__ void cfl_dt_kernel(const float* velomax, float* dt, float cfl_dx, float step_max) {
   const float vm = *velomax;
   float d = step_max;
@@ -772,6 +790,22 @@ extern "C" int igm_absmax2(int dtype, int n, const void* a, const void* b, float
     return IGM_ERR_BAD_ARGUMENT;
   }
   return launch_status("absmax2_kernel");
+}
+
+extern "C" int igm_force_max_velbar(int dtype, size_t n, void* U, void* V, double cap, void* stream) {
+  IGM_CHECK_ARG(U && V, IGM_ERR_BAD_ARGUMENT, "igm_force_max_velbar: NULL argument");
+  IGM_CHECK_ARG(cap > 0, IGM_ERR_BAD_ARGUMENT, "igm_force_max_velbar: the cap must be positive");
+  if (n == 0) return IGM_OK;
+  cudaStream_t st = as_stream(stream);
+  if (dtype == IGM_F32)
+    force_max_velbar_kernel<float><<<grid1d(n), 256, 0, st>>>(n, (float*)U, (float*)V, (float)cap);
+  else if (dtype == IGM_F64)
+    force_max_velbar_kernel<double><<<grid1d(n), 256, 0, st>>>(n, (double*)U, (double*)V, cap);
+  else {
+    set_error("igm_force_max_velbar: unknown dtype %d", dtype);
+    return IGM_ERR_BAD_ARGUMENT;
+  }
+  return launch_status("force_max_velbar_kernel");
 }
 
 extern "C" int igm_vertical_velocity(int dtype, int nz, int ny, int nx, double dx, const void* U, const void* V,

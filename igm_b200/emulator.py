@@ -11,10 +11,13 @@ and diagnostic/diagnostic.py), on the device.
 * ``update_iceflow_diagnostic``: every 10 model years the plain solver is run
   from the emulated velocities and the L1/L2 velbar misfit is logged
   (diagnostic.py:34-84).
-* ``update_iceflow_fallback`` (this implementation's addition): every
-  ``fallback.every`` updates the solver judges the emulator; when the emulated
-  energy exceeds the solved one by more than ``fallback.margin`` (relative)
-  the solved velocities replace the emulated ones.
+* ``update_iceflow_fallback`` / ``update_iceflow_takeover`` (this
+  implementation's addition): every ``fallback.every`` updates the solver
+  judges the emulator; when the emulated energy exceeds the solved one by
+  more than ``fallback.margin`` (relative) the solved velocities replace the
+  emulated ones -- for that update alone (fallback.mode "step") or for the
+  updates until the next check, each a warm-started solve (mode "takeover",
+  the default).
 * ``save_iceflow_model`` / ``load_iceflow_model``: weights, Adam moments and
   iteration count as ``model.npz`` next to the reference's ``fieldin.dat`` and
   ``vert_grid.dat`` text files (emulate.py:331-359); ``load_keras_h5`` reads
@@ -105,8 +108,8 @@ def update_iceflow_emulated(cfg, state):
     model.prepare_input(f, P._dx(state), [(0, 0)], ny, nx, buf)
     U, V = model.forward(buf, 1, ny, nx, thk_mask=f[0])
     state.U, state.V = U[0], V[0]
-    if cfg.processes.iceflow.force_max_velbar > 0:
-        raise NotImplementedError("force_max_velbar > 0 is not supported")
+    if cfg.processes.iceflow.force_max_velbar > 0:  # emulate.py:147-148
+        K.force_max_velbar(state.U, state.V, cfg.processes.iceflow.force_max_velbar)
     P.set_derived_velocities(cfg, state, mask=False)
     S.sync_host(state)
 
@@ -252,6 +255,57 @@ def update_iceflow_fallback(cfg, state):
         state.U, state.V = U, V
         P.set_derived_velocities(cfg, state, mask=False)
         S.sync_host(state)
+
+
+def update_iceflow_takeover(cfg, state):
+    """The emulator with the plain solver as its fallback, taking over
+    (fallback.mode "takeover"): every ``fallback.every`` updates the solver
+    judges the emulator -- it solves from its own last solution (the
+    emulated velocities the first time), and the emulated energy is compared
+    with the solved one -- and the outcome holds until the next check: while
+    the emulator passes, each update is one network evaluation; after a
+    failed check each update is a solve warm-started from the previous one,
+    as the plain method runs, while the emulator keeps retraining on the
+    states the run produces.  Every check is logged in state.fallback_log."""
+    fb = cfg.processes.iceflow.fallback
+    n = state.__dict__.setdefault("_igm_fallback_counter", 0)
+    state._igm_fallback_counter = n + 1
+    f = _fields(state)
+    dx = P._dx(state)
+    phys = P.physics(cfg)
+    solved = state.__dict__.get("_igm_solved")
+    if n % int(fb.every) == 0:
+        update_iceflow_emulated(cfg, state)
+        U0, V0 = solved if solved is not None else (state.U, state.V)
+        U, V, costs = state.iceflow_solver.solve(U0, V0, *f, dx, state.dzeta, nbitmax=int(fb.nbitmax), phys=phys,
+                                                 relative_min_delta=0.0002, patience=10)
+        ny, nx = f[0].shape
+        ns = (ny - 1) * (nx - 1)
+        e_em = float(K.energy(state.U, state.V, *f, dx, state.dzeta, phys)[0].sum().item()) / ns
+        e_sv = float(K.energy(U, V, *f, dx, state.dzeta, phys)[0].sum().item()) / ns
+        du = torch.cat([(state.U - U).reshape(-1), (state.V - V).reshape(-1)])
+        ref = torch.cat([U.reshape(-1), V.reshape(-1)])
+        rel = float(torch.linalg.vector_norm(du.double()) / torch.linalg.vector_norm(ref.double()).clamp_min(1e-30))
+        fallback = e_em > e_sv + float(fb.margin) * abs(e_sv)
+        state.__dict__.setdefault("fallback_log", []).append(
+            dict(t=float(state.t), it=int(state.it), e_emulated=e_em, e_solved=e_sv, vel_rel_l2=rel,
+                 fallback=bool(fallback), solver_iterations=len(costs)))
+        state._igm_solved = (U, V)
+        state._igm_fallback_active = bool(fallback)
+        if fallback:
+            state.U, state.V = U, V
+            P.set_derived_velocities(cfg, state, mask=False)
+            S.sync_host(state)
+        return
+    if state.__dict__.get("_igm_fallback_active", False):
+        U, V, _ = state.iceflow_solver.solve(solved[0], solved[1], *f, dx, state.dzeta, nbitmax=int(fb.nbitmax),
+                                             phys=phys, relative_min_delta=0.0002, patience=10)
+        state._igm_solved = (U, V)
+        state.U, state.V = U, V
+        P.set_derived_velocities(cfg, state, mask=False)
+        S.sync_host(state)
+    else:
+        update_iceflow_emulated(cfg, state)
 
 
 def save_iceflow_model(cfg, state, directory="iceflow-model"):

@@ -90,6 +90,16 @@ def velocity_reduce(U, V, thk, vert_weight, mask=True, want_velomax=True):
     return (*outs, vm)
 
 
+def force_max_velbar(U, V, cap):
+    """In place: where |(U, V)| >= cap, (U, V) = cap (U, V) / |(U, V)|
+    (igm_force_max_velbar)."""
+    if U.shape != V.shape or U.dtype != V.dtype or not (U.is_contiguous() and V.is_contiguous()):
+        raise ValueError("force_max_velbar: U and V must be contiguous tensors of one shape and dtype")
+    rc = L.lib().igm_force_max_velbar(L.dtype_code(U.dtype), U.numel(), L.ptr(U), L.ptr(V), float(cap),
+                                      L.stream_ptr())
+    L.check(rc, "igm_force_max_velbar")
+
+
 def transport_step(ubar, vbar, thk, topg, smb, dx, dt, slope_type="superbee", ratio_density=0.910, sealevel=0.0,
                    want_lsurf=True, want_divflux=True, dt_device=None):
     """Returns (thk_new, usurf, lsurf, divflux) (the last two may be None)."""

@@ -7,7 +7,9 @@ emulator and retrains it on the same energy every ``retrain_freq`` updates;
 model years and logs the misfit.  This implementation adds an optional
 fallback (``cfg.processes.iceflow.fallback``): in emulated mode the solver
 judges the emulator every ``every`` updates and replaces its velocities when
-the emulated energy exceeds the solved one by more than ``margin``.
+the emulated energy exceeds the solved one by more than ``margin`` -- until
+the next check (``mode`` "takeover", the default) or for that update
+alone (``mode`` "step").
 
 Supported configuration: vert_basis "Lagrange", staggered_grid 1, the
 default energy components, no sliding_law, dim_arrhenius 2, architecture
@@ -89,11 +91,14 @@ def initialize_iceflow_solver(cfg, state):
 
 
 def solve_iceflow(cfg, state, U, V):
-    """solve.py:22-119 (Adam, EarlyStopping(2e-4, 10), mask thk == 0)."""
+    """solve.py:22-119 (Adam, EarlyStopping(2e-4, 10), mask thk == 0); the
+    early stopping can be switched off (solver.early_stopping, an igm_b200
+    key) to run nbitmax iterations per solve."""
     thk, usurf, A, c = _fieldin(state)
+    sv = cfg.processes.iceflow.solver
     return state.iceflow_solver.solve(
-        U, V, thk, usurf, A, c, _dx(state), state.dzeta, nbitmax=int(cfg.processes.iceflow.solver.nbitmax),
-        phys=physics(cfg), relative_min_delta=0.0002, patience=10)
+        U, V, thk, usurf, A, c, _dx(state), state.dzeta, nbitmax=int(sv.nbitmax),
+        phys=physics(cfg), relative_min_delta=0.0002, patience=10, early_stopping=bool(sv.get("early_stopping", True)))
 
 
 def set_derived_velocities(cfg, state, mask):
@@ -113,8 +118,8 @@ def set_derived_velocities(cfg, state, mask):
 def update_iceflow_solved(cfg, state):
     """solve.py:169-188."""
     state.U, state.V, costs = solve_iceflow(cfg, state, state.U, state.V)
-    if cfg.processes.iceflow.force_max_velbar > 0:
-        raise NotImplementedError("force_max_velbar > 0 is not supported")
+    if cfg.processes.iceflow.force_max_velbar > 0:  # solve.py:178-179
+        K.force_max_velbar(state.U, state.V, cfg.processes.iceflow.force_max_velbar)
     if len(cfg.processes.iceflow.solver.save_cost) > 0:
         np.savetxt(cfg.processes.iceflow.emulator.output_directory + cfg.processes.iceflow.solver.save_cost
                    + "-" + str(state.it) + ".dat", np.array(costs), fmt="%5.10f")
@@ -157,6 +162,9 @@ def update(cfg, state):
         from .. import emulator as E
         if (ic.emulator.retrain_freq > 0) & (state.it > 0):
             E.update_iceflow_emulator(cfg, state, state.it, pertubate=ic.emulator.pertubate)
+        if ic.method == "emulated" and ic.fallback.every > 0 and ic.fallback.get("mode", "takeover") == "takeover":
+            E.update_iceflow_takeover(cfg, state)
+            return
         E.update_iceflow_emulated(cfg, state)
         if ic.method == "diagnostic":
             E.update_iceflow_diagnostic(cfg, state)

@@ -459,6 +459,14 @@ IGM_API int igm_smb_simple(int dtype, int n, const void* usurf, const void* icem
  * (time.py:36-39 when ubar/vbar did not come from igm_velocity_reduce). */
 IGM_API int igm_absmax2(int dtype, int n, const void* a, const void* b, float* out, void* stream);
 
+/* force_max_velbar (igm/processes/iceflow/utils.py:182-194, Lagrange basis;
+ * applied by emulate.py:147-148 and solve.py:178-179 when the option is > 0):
+ * in place over n nodes of U and V ([nz, ny, nx] flattened), where
+ * mag = sqrt(U^2 + V^2) >= cap: U = cap (U / mag), V = cap (V / mag).
+ * Bit-identical to the reference graph (no fused multiply-add, IEEE division
+ * and square root). */
+IGM_API int igm_force_max_velbar(int dtype, size_t n, void* U, void* V, double cap, void* stream);
+
 /* CFL step on the device (time.py:36-50, without the save-time snapping):
  * dt_out = velomax > 0 ? min(cfl dx / velomax, step_max) : step_max. */
 IGM_API int igm_cfl_dt(const float* velomax, float* dt_out, double cfl, double dx, double step_max, void* stream);

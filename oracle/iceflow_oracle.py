@@ -81,6 +81,14 @@ class Physics:
     force_negative_gravitational_energy: bool = False
 
 
+def sqrt_ieee(t):
+    """Correctly rounded square root of a CPU tensor (numpy's, IEEE 754):
+    torch's vectorised CPU sqrt is not correctly rounded in every element,
+    while the reference's arithmetic and the device kernels are.  No
+    autograd through it."""
+    return torch.from_numpy(np.asarray(np.sqrt(t.detach().numpy()))).to(t.dtype)
+
+
 def _t(x, dtype=None):
     if isinstance(x, torch.Tensor):
         return x if dtype is None else x.to(dtype)
@@ -294,7 +302,7 @@ class KerasLegacyAdam:
         for g, x in grads_and_vars:
             dt = x.dtype
             if self.clipnorm is not None:
-                n = torch.sqrt(torch.sum(g.to(torch.float64) ** 2)).to(g.dtype)
+                n = sqrt_ieee(torch.sum(g.to(torch.float64) ** 2)).to(g.dtype)
                 g = g * self.clipnorm / torch.maximum(n, torch.tensor(self.clipnorm, dtype=g.dtype))
             # slots are keyed by the variable object; holding the variable in its
             # slot keeps its id from being reused by a later variable (TF variables
@@ -306,10 +314,10 @@ class KerasLegacyAdam:
             one = torch.tensor(1.0, dtype=dt)
             b1p = torch.tensor(self.b1, dtype=dt) ** t
             b2p = torch.tensor(self.b2, dtype=dt) ** t
-            alpha = self.lr * torch.sqrt(one - b2p) / (one - b1p)
+            alpha = self.lr * sqrt_ieee(one - b2p) / (one - b1p)
             m += (g - m) * (1 - self.b1)
             v += (g * g - v) * (1 - self.b2)
-            x -= (m * alpha) / (torch.sqrt(v) + self.eps)
+            x -= (m * alpha) / (sqrt_ieee(v) + self.eps)
         self.iterations += 1
 
 
@@ -358,6 +366,15 @@ def solve_iceflow(U, V, thk, usurf, arrhenius, slidingco, dx, dzeta, optimizer: 
     U = torch.where(mask, U, torch.zeros_like(U))
     V = torch.where(mask, V, torch.zeros_like(V))
     return U, V, costs
+
+
+def force_max_velbar(U, V, cap):
+    """utils.py:182-194 (Lagrange basis): where |(U, V)| >= cap, both
+    components scaled to that speed; the magnitude as tf.norm of the stacked
+    pair, sqrt(U U + V V)."""
+    mag = sqrt_ieee(U * U + V * V)
+    c = torch.tensor(cap, dtype=U.dtype)
+    return torch.where(mag >= c, c * (U / mag), U), torch.where(mag >= c, c * (V / mag), V)
 
 
 def get_velbase(U, V):

@@ -8,8 +8,9 @@ xarray, OGGM and the rest of the model, so the packages on the path are
 registered as bare namespace stubs and only the hot-path modules are loaded
 from their files.
 
-Run from the repository root:  python tests/golden/make_golden.py [REF_ROOT]
-(REF_ROOT defaults to /root/reference).  Writes ``*.npz`` next to this file.
+Run from the repository root:  python tests/golden/make_golden.py REF_ROOT
+(REF_ROOT: the root of the reference's source tree, the directory holding
+``igm/``; or set IGM_REFERENCE_ROOT).  Writes ``*.npz`` next to this file.
 The generated inputs are seeded; re-running reproduces the files bit for bit.
 """
 
@@ -31,7 +32,10 @@ import tf_shim  # noqa: E402
 tf_shim.install()
 import tensorflow as tf  # noqa: E402  (the shim)
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("IGM_REFERENCE_ROOT", "")
+if not REF or not os.path.isdir(os.path.join(REF, "igm")):
+    sys.exit("usage: python tests/golden/make_golden.py REF_ROOT (the reference source tree, holding igm/), "
+             "or set IGM_REFERENCE_ROOT")
 IGM = os.path.join(REF, "igm")
 
 

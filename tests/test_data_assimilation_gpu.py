@@ -302,7 +302,8 @@ def test_icemask_reprojection_when_thk_is_not_a_control(tmp_path, monkeypatch):
     inverted.  The thickness starts from thkinit (the true tongue) while the
     observed mask leaves out its downstream third; two iterations against the
     oracle's da_optimize_step: the thickness bit for bit, slidingco's gradient
-    and the costs as test_other_controls_in_the_loop_match_oracle."""
+    and the costs as test_other_controls_in_the_loop_match_oracle (slidingco
+    starts off its true value, so that the velocity misfit is not zero)."""
     monkeypatch.chdir(tmp_path)
     cfg = make_cfg(2)
     da = cfg.processes.data_assimilation
@@ -312,6 +313,10 @@ def test_icemask_reprojection_when_thk_is_not_a_control(tmp_path, monkeypatch):
     st = twin_state(cfg, g)
     st.icemaskobs[:, 47:] = 0.0
     st.thkinit = st.thk.clone()
+    # slidingco off its true value, so that the velocity misfit (zero at the truth) is not
+    rng = np.random.default_rng(8)
+    st.slidingco = st.slidingco * torch.as_tensor(rng.uniform(0.5, 1.5, g["thk"].shape).astype(np.float32),
+                                                  device="cuda")
     setup = oracle_setup(cfg, st)
     ws, bs, obs, p, ctl, opt, _ = setup
     r = da.regularization

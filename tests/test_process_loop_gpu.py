@@ -227,31 +227,41 @@ def device_emulated(st):
     return U[0].clone(), V[0].clone()
 
 
+@pytest.mark.parametrize("mode", ["step", "takeover"])
 @pytest.mark.parametrize("margin,expect", [(-10.0, True), (1e9, False)])
-def test_fallback_decision(margin, expect):
+def test_fallback_decision(margin, expect, mode):
     """margin -10 makes every check fall back (the emulated energy always
     exceeds the solved one minus ten times its magnitude); 1e9 never does.
-    On fallback the state's velocities are the solver's, started from the
-    emulated ones (checked against the oracle's solve from the same start);
-    otherwise they stay the emulated ones, bit for bit."""
+    A check solves from the solver's last solution (the emulated velocities
+    the first time) and is logged.  On fallback the state's velocities are
+    that solve's (checked against the oracle's solve from the same start);
+    mode "step" returns to the emulator at the next update, mode "takeover"
+    keeps solving, warm-started from the previous solve, until the next check.
+    Without fallback the velocities stay the emulated ones, bit for bit."""
     cfg = make_cfg("emulated", retrain_freq=0, fallback_every=2, margin=margin)
+    cfg.processes.iceflow.fallback.mode = mode
     st = make_state(seed=6)
     mods = init(cfg, st)
     for k in range(4):
         s = snapshot(st)
         Ue, Ve = device_emulated(st)
+        prev = st.__dict__.get("_igm_solved")
+        prev = (cpu(prev[0]), cpu(prev[1])) if prev is not None else None
         for m in mods:
             m.update(cfg, st)
         st.it += 1
         log = st.fallback_log
         checked = len(log) > 0 and log[-1]["it"] == s["it"]
         assert checked == (k % 2 == 0)
-        if checked and expect:
-            assert log[-1]["fallback"]
-            Us, Vs, costs = oracle_solve(s, cpu(Ue), cpu(Ve), s["solver_iterations"], 20)
-            assert log[-1]["solver_iterations"] == len(costs)
-            assert rel_l2(cpu(st.U).numpy(), Us.numpy()) < 1e-4
-            assert rel_l2(cpu(st.V).numpy(), Vs.numpy()) < 1e-4
+        solving = expect and (checked or mode == "takeover")
+        if solving:
+            start = prev if (mode == "takeover" and prev is not None) else (cpu(Ue), cpu(Ve))
+            Us, Vs, costs = oracle_solve(s, start[0], start[1], s["solver_iterations"], 20)
+            if checked:
+                assert log[-1]["fallback"] and log[-1]["solver_iterations"] == len(costs)
+            assert st.iceflow_solver.iterations - s["solver_iterations"] == len(costs)
+            assert rel_l2(cpu(st.U).numpy(), Us.numpy()) < 1e-4, k
+            assert rel_l2(cpu(st.V).numpy(), Vs.numpy()) < 1e-4, k
             assert not torch.equal(st.U, Ue)
         else:
             assert not (checked and log[-1]["fallback"])
@@ -293,3 +303,23 @@ def test_save_load_round_trip(tmp_path, monkeypatch):
     E.update_iceflow_emulated(cfg, st)
     E.update_iceflow_emulated(cfg2, st2)
     assert torch.equal(st.U, st2.U) and torch.equal(st.V, st2.V)
+
+
+@pytest.mark.parametrize("method", ["emulated", "solved"])
+def test_force_max_velbar_in_the_process(method):
+    """With force_max_velbar > 0 the velocities the process leaves are capped
+    (emulate.py:147-148, solve.py:178-179) before velbar, velbase and velsurf
+    are derived from them."""
+    cfg = make_cfg(method, retrain_freq=0)
+    cfg.processes.iceflow.force_max_velbar = 5.0
+    st = make_state(seed=8)
+    mods = init(cfg, st)
+    for m in mods:
+        m.update(cfg, st)
+    st.it += 1
+    speed = torch.sqrt(st.U * st.U + st.V * st.V)
+    assert float(speed.max()) <= 5.0 * (1 + 1e-6)
+    w = torch.as_tensor(iceflow.define_vertical_weight(NZ, 4.0))
+    ub, _ = O.get_velbar(cpu(st.U), cpu(st.V), w)
+    assert rel_l2(cpu(st.ubar).numpy(), ub.numpy()) < 1e-6
+    assert torch.equal(st.uvelsurf, st.U[-1]) and torch.equal(st.uvelbase, st.U[0])

@@ -100,3 +100,22 @@ def test_velocity_reduce_and_mask():
     expect = max(np.abs(ub.cpu().numpy()).max(), np.abs(vb.cpu().numpy()).max())
     assert vm.item() == expect
     assert K.absmax2(ub, vb).item() == expect
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_force_max_velbar_bit_identical(dtype):
+    """force_max_velbar (utils.py:182-194) against the oracle, bit for bit:
+    speeds above the cap scaled to it, the rest (and zero speeds) unchanged."""
+    rng = np.random.default_rng(7)
+    U = rng.normal(0, 300, (5, 37, 53))
+    V = rng.normal(0, 300, (5, 37, 53))
+    U[0, :3] = 0.0
+    V[0, :3] = 0.0
+    Ut, Vt = torch.as_tensor(U).to(dtype), torch.as_tensor(V).to(dtype)
+    Uo, Vo = O.force_max_velbar(Ut, Vt, 250.0)
+    Ud, Vd = Ut.cuda().contiguous(), Vt.cuda().contiguous()
+    K.force_max_velbar(Ud, Vd, 250.0)
+    np.testing.assert_array_equal(Ud.cpu().numpy(), Uo.numpy())
+    np.testing.assert_array_equal(Vd.cpu().numpy(), Vo.numpy())
+    assert float(torch.sqrt(Ud * Ud + Vd * Vd).max()) <= 250.0 * (1 + 1e-6)
+    assert int((torch.sqrt(Ut * Ut + Vt * Vt) >= 250.0).sum()) > 100
