@@ -4,8 +4,8 @@ The processes read ``cfg.processes.<name>.<key>`` by attribute access, so an
 OmegaConf DictConfig composed by the reference's Hydra setup works as is;
 ``default_cfg()`` builds an equivalent plain object for callers without
 Hydra.  Keys and defaults follow igm/conf/processes/iceflow.yaml,
-thk.yaml, time.yaml, smb_simple.yaml, vert_flow.yaml and
-data_assimilation.yaml.  Keys this implementation adds are
+thk.yaml, time.yaml, smb_simple.yaml, vert_flow.yaml,
+data_assimilation.yaml and pretraining.yaml.  Keys this implementation adds are
 marked "(igm_b200)".
 """
 
@@ -123,6 +123,13 @@ OPTIONAL = {
                    "vars_to_save": ["usurf", "thk", "slidingco", "velsurf_mag", "velsurfobs_mag", "divflux",
                                     "icemask"]},
         "cook": {"infer_params": False, "tidewater_glacier": False, "vol_std": 1000.0},
+    },
+    "pretraining": {
+        "data_dir": "surflib3d_shape_100", "batch_size": 1, "freq_test": 20, "train_iceflow_emulator_restart_lr": 2500,
+        "epochs": 5000, "min_arrhenius": 5.0, "max_arrhenius": 151.0, "min_slidingco": 0.0,
+        "max_slidingco": 20000.0, "min_coarsen": 0, "max_coarsen": 2, "soft_begining": 500,
+        # (igm_b200) seed of the sampling (the reference draws unseeded)
+        "seed": 0,
     },
 }
 

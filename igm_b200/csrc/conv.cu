@@ -56,9 +56,18 @@ struct ConvArgs {
   int* err;
 };
 
+// Input stages of the forward / dgrad pipeline and output rows per tile (build-time
+// tuning constants; R must keep 2 R 32 TMEM columns a power of two: 2, 4 or 8).
+#ifndef IGM_CONV_STAGES
+#define IGM_CONV_STAGES 3
+#endif
+#ifndef IGM_CONV_ROWS
+#define IGM_CONV_ROWS 4
+#endif
+
 template <int C8_IN, int R>
 struct ConvGeom {
-  static constexpr int NST = 3;                               // input stages
+  static constexpr int NST = IGM_CONV_STAGES;                 // input stages
   static constexpr uint32_t P = kBoxW * 16;                   // chunk plane stride (bytes)
   static constexpr uint32_t RS = C8_IN * P;                   // row stride
   static constexpr uint32_t STAGE = (R + 2) * RS;             // one input stage
@@ -514,7 +523,8 @@ static int set_smem(K kernel, uint32_t bytes, bool* done) {
   return IGM_OK;
 }
 
-constexpr int kRows = 4;
+constexpr int kRows = IGM_CONV_ROWS;
+static_assert(kRows == 2 || kRows == 4 || kRows == 8, "IGM_CONV_ROWS: 2, 4 or 8");
 
 template <int C8_IN, int EPI>
 static int conv_launch(int B, int H, int W, const void* x, const void* wpack, const float* bias, const void* amask,

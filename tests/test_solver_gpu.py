@@ -121,17 +121,21 @@ def test_max_iter_caps_and_no_early_stop():
     assert len(c) == 7 and s.iterations == 7
 
 
-@pytest.mark.parametrize("n", [1, 10])
-def test_fp32_solver_matches_fp32_oracle_to_1e5(n):
+def test_fp32_solver_matches_fp32_oracle_to_1e5():
     """FP32 against the FP32 restatement of the reference solver on the same
-    inputs, relative L2 of the velocities <= 1e-5, where the comparison is
-    well posed: after 1 and 10 iterations the trajectory has not yet
-    amplified the two sides' different FP32 summation orders (at 100
-    iterations it has: see test_fp32_solver_error_against_fp64)."""
+    inputs, relative L2 of the velocities <= 1e-5, after one iteration -- the
+    number of iterations at which that bound is well posed: Adam at lr 1
+    moves each velocity by about +-1 per iteration with the sign of its
+    gradient, so a rounding difference that flips a near-zero gradient moves
+    that node by a full step.  Measured on the oracle alone (this glacier,
+    relative L2 of the solution after a 1e-7 relative perturbation of the
+    inputs): 3.8e-6 after 1 iteration, 8.6e-5 after 3 and 4.4e-4 after 10;
+    beyond one iteration parity is held by
+    test_fp32_solver_error_against_fp64 against that sensitivity."""
     st = O.valley_glacier(40, 36, 100.0, seed=2)
-    ref, cref = _oracle_solve(st, 10, torch.float32, n)
-    got, c = _device_solve(st, 10, torch.float32, n)
+    ref, cref = _oracle_solve(st, 10, torch.float32, 1)
+    got, c = _device_solve(st, 10, torch.float32, 1)
     e = rel_l2(got, ref)
-    print(f"n={n}: device FP32 vs oracle FP32 {e:.3e}")
+    print(f"one iteration: device FP32 vs oracle FP32 {e:.3e}")
     assert e <= 1e-5, e
     np.testing.assert_allclose(c, cref, rtol=1e-5)
