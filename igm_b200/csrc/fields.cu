@@ -131,10 +131,10 @@ struct TransportArgs {
 // rounded quotient.  A zero numerator is returned as is (keeps its sign).
 template <typename T>
 __device__ __forceinline__ T div_dx(T num, T dx, T rdx) {
-  if (num == T(0)) return num;
   const T q = num * rdx;
   const T r = fma(-q, dx, num);
-  return fma(r, rdx, q);
+  const T d = fma(r, rdx, q);
+  return num == T(0) ? num : d;
 }
 
 template <typename T>
@@ -167,16 +167,28 @@ __device__ __forceinline__ T cell_slope(T hm, T h0, T hp, T dx, T rdx) {
   if (SLOPE == IGM_GODUNOV) return T(0);
   const T sigp = div_dx(hp - h0, dx, rdx), sigm = div_dx(h0 - hm, dx, rdx);
   if (SLOPE == IGM_MINMOD) return minmod(sigm, sigp);
-  return maxmod(minmod(sigp, T(2) * sigm), minmod(sigm, T(2) * sigp));
+  // superbee: maxmod(minmod(sigp, 2 sigm), minmod(sigm, 2 sigp)).  The two minmods' sign tests
+  // sigp (2 sigm) > 0 and sigm (2 sigp) > 0 round the same exact product 2 sigp sigm (doubling is
+  // exact), so they are one test.
+  const T m2 = T(2) * sigm, p2 = T(2) * sigp;
+  const bool pos = sigp * m2 > T(0);
+  const T fa = fabs(sigp), fb = fabs(m2), fc = fabs(sigm), fd = fabs(p2);
+  const T s1 = (fa < fb && pos) ? sigp : ((fa > fb && pos) ? m2 : T(0));
+  const T s2 = (fc < fd && pos) ? sigm : ((fc > fd && pos) ? p2 : T(0));
+  return maxmod(s1, s2);
 }
 
-// upwind flux through a face with velocity uf between cells (hl, sl) and (hr, sr)
+// upwind flux through a face with velocity uf between cells (hl, sl) and (hr, sr): only the state
+// tf.where(u > 0, w, e) keeps is evaluated, with the reference's operations and order
+// (w = hl + (half_dx (1 - cu)) sl, e = hr - (half_dx (1 + cu)) sr)
 template <typename T>
 __device__ __forceinline__ T face_flux(T uf, T hl, T hr, T sl, T sr, T dt, T dx, T rdx, T half_dx) {
   const T cu = div_dx(uf * dt, dx, rdx);
-  const T w = hl + half_dx * (T(1) - cu) * sl;
-  const T e = hr - half_dx * (T(1) + cu) * sr;
-  return uf * (uf > T(0) ? w : e);
+  const bool up = uf > T(0);
+  const T h = up ? hl : hr;
+  const T c = up ? T(1) - cu : T(1) + cu;
+  const T t = half_dx * c * (up ? sl : sr);
+  return uf * (up ? h + t : h - t);
 }
 
 template <typename T>
@@ -207,15 +219,34 @@ __device__ __forceinline__ void transport_march(const TransportArgs<T>& a, int l
     if (ROWS) return (ok && j >= 0 && j < ny) ? p[(size_t)j * nx + c] : T(0);
     return ok ? p[(size_t)j * nx + c] : T(0);
   };
+  // interior segments: every row of the segment is in the domain, so a row's six loads share one
+  // element offset (the row's start), computed once
+  const T* hc = H + ic;
+  const T* vc = a.v + ic;
+  const T* uc = a.u + ic;
+  const T* tc_ = a.topg + ic;
+  const T* sc_ = a.smb ? a.smb + ic : nullptr;
+  const T* hec = H + iec;
+  const size_t nx1 = (size_t)nx, nx2 = 2 * (size_t)nx;
   auto load_row = [&](int j) {
     MarchRow<T> r;
-    const bool live = !ROWS || j < y1;
-    r.h2 = at(H, j + 2, live && col, ic);
-    r.v1 = at(a.v, j + 1, live && col, ic);
-    r.u = at(a.u, j, live && col, ic);
-    r.tg = at(a.topg, j, live && col, ic);
-    r.sm = a.smb ? at(a.smb, j, live && col, ic) : T(0);
-    r.he = at(H, j, live && ecol, iec);
+    if (ROWS) {
+      const bool live = j < y1;
+      r.h2 = at(H, j + 2, live && col, ic);
+      r.v1 = at(a.v, j + 1, live && col, ic);
+      r.u = at(a.u, j, live && col, ic);
+      r.tg = at(a.topg, j, live && col, ic);
+      r.sm = a.smb ? at(a.smb, j, live && col, ic) : T(0);
+      r.he = at(H, j, live && ecol, iec);
+    } else {
+      const size_t o = (size_t)j * nx1;
+      r.h2 = col ? hc[o + nx2] : T(0);
+      r.v1 = col ? vc[o + nx1] : T(0);
+      r.u = col ? uc[o] : T(0);
+      r.tg = col ? tc_[o] : T(0);
+      r.sm = (sc_ && col) ? sc_[o] : T(0);
+      r.he = ecol ? hec[o] : T(0);
+    }
     return r;
   };
   // prologue: the y slopes of cells y0-1 and y0 and the flux through face y0
@@ -233,7 +264,7 @@ __device__ __forceinline__ void transport_march(const TransportArgs<T>& a, int l
   auto step = [&](int j, const MarchRow<T>& r) {
     // y: slope of cell j+1, flux through face j+1 (between rows j and j+1)
     const T sy1 = cell_slope<T, SLOPE>(h0, hp1, r.h2, dx, rdx);
-    const T vf = j + 1 == ny ? v0 : T(0.5) * (v0 + r.v1);
+    const T vf = (ROWS && j + 1 == ny) ? v0 : T(0.5) * (v0 + r.v1);
     const T qn = face_flux(vf, h0, hp1, sy0, sy1, dt, dx, rdx, hdx);
     // x: slope of this lane's cell, flux through its left face (face i)
     T hl = __shfl_up_sync(0xffffffffu, h0, 1), hr = __shfl_down_sync(0xffffffffu, h0, 1);
