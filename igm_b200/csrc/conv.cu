@@ -15,14 +15,17 @@
 // nine taps is then just a shifted descriptor start address:
 // (row + dy) * row_stride + (dx) * 16 bytes.
 //
-// Forward / dgrad kernel (persistent, one CTA per SM, 6 warps):
+// Forward / dgrad kernel (persistent, one CTA per SM, 10 warps):
 //   warp 0  producer: bulk copies of the input tile (and TMEM allocator),
-//   warp 1  MMA issuer: per tile R rows x 9 taps x C/16 MMAs of M=128 (pixels),
-//           N=32 (output channels), K=16 into R TMEM accumulators,
-//   warps 2-5 epilogue: TMEM -> registers (one pixel per thread), bias +
-//           LeakyReLU (forward) or the LeakyReLU derivative mask of the previous
-//           activation (dgrad, plus the bias-gradient partial sums), bf16 store.
-//   Three input stages and two accumulator sets overlap load, MMA and epilogue.
+//   warp 1  MMA issuer: per tile of R = 8 rows (R + 2 input rows x 3 kernel
+//           columns x C/16 MMAs of M=128 pixels, the kernel rows folded into N),
+//           K=16, into R TMEM accumulators,
+//   warps 2-9 epilogue, two per TMEM lane quarter (each half of the rows):
+//           TMEM -> registers (one pixel per thread), bias + LeakyReLU (forward)
+//           or the LeakyReLU derivative mask of the previous activation (dgrad,
+//           plus the bias-gradient partial sums), bf16 store.
+//   Two input stages and two accumulator sets overlap load, MMA and epilogue
+//   (rows, stages and sets are build-time constants; 8 / 2 / 2 measured best).
 // Weight-gradient kernel: D[(input row, ci)][co] += X^T G over the pixels of
 // four output rows per work item, with both operands MN-major: M = 128 spans
 // 128/(C/8*8) consecutive input rows x C input channels (row stride = C/8
@@ -39,7 +42,12 @@ constexpr int kTW = 128;        // pixels per tile row (the UMMA M)
 constexpr int kBoxW = kTW + 2;  // with the 1-pixel halo on each side
 constexpr int kCout = 32;       // output channels
 constexpr int kWRowsN = 3 * kCout;  // B-operand rows per (dx, k-chunk) of a weight pack: (dy, channel)
-constexpr int kConvThreads = 192;
+constexpr int kConvThreads = 192;      // weight-gradient kernel: producer, MMA issuer, 4 epilogue warps
+// forward / dgrad kernel: producer, MMA issuer and kConvEpiWarps epilogue warps -- two per TMEM lane
+// quarter, each finishing half of a tile's rows, so that every scheduler has two epilogue warps to
+// interleave
+constexpr int kConvEpiWarps = 8;
+constexpr int kConvFwdThreads = 64 + 32 * kConvEpiWarps;
 
 enum ConvEpi { kEpiFwdLeaky = 0, kEpiDgrad = 1 };
 
@@ -59,10 +67,14 @@ struct ConvArgs {
 // Input stages of the forward / dgrad pipeline and output rows per tile (build-time
 // tuning constants; R must keep 2 R 32 TMEM columns a power of two: 2, 4 or 8).
 #ifndef IGM_CONV_STAGES
-#define IGM_CONV_STAGES 3
+#define IGM_CONV_STAGES 2
 #endif
 #ifndef IGM_CONV_ROWS
-#define IGM_CONV_ROWS 4
+#define IGM_CONV_ROWS 8
+#endif
+// TMEM accumulator sets of the forward / dgrad pipeline (2 or 4; NACC R 32 columns a power of two)
+#ifndef IGM_CONV_ACC_SETS
+#define IGM_CONV_ACC_SETS 2
 #endif
 
 template <int C8_IN, int R>
@@ -74,7 +86,10 @@ struct ConvGeom {
   static constexpr uint32_t WBYTES = 9 * C8_IN * kCout * 16;  // packed weights
   static constexpr uint32_t OFF_W = NST * STAGE;
   static constexpr uint32_t OFF_BAR = OFF_W + WBYTES;
-  static constexpr uint32_t TMEM_COLS = 2 * R * kCout;  // two accumulator sets
+  static constexpr int NACC = IGM_CONV_ACC_SETS;              // accumulator sets
+  static constexpr uint32_t TMEM_COLS = NACC * R * kCout;
+  static_assert(TMEM_COLS <= 512 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "TMEM columns: a power of two <= 512");
+  static_assert(2 * NST + 2 * NACC <= 16, "barrier slots");
   static constexpr uint32_t SMEM = OFF_BAR + 16 * 8 + 16 + 32 * 4 + 1024;
 };
 
@@ -131,7 +146,7 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
 }
 
 template <int C8_IN, int R, int EPI>
-__global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs a) {
+__global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_kernel(const ConvArgs a) {
   using G = ConvGeom<C8_IN, R>;
   constexpr int NST = G::NST;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -139,8 +154,9 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
   uint64_t* full = bars;               // [NST] loads -> MMA
   uint64_t* empty = bars + NST;        // [NST] MMA -> loads
-  uint64_t* tfull = bars + 2 * NST;    // [2] MMA -> epilogue
-  uint64_t* tempty = bars + 2 * NST + 2;  // [2] epilogue -> MMA
+  constexpr int NACC = G::NACC;
+  uint64_t* tfull = bars + 2 * NST;    // [NACC] MMA -> epilogue
+  uint64_t* tempty = bars + 2 * NST + NACC;  // [NACC] epilogue -> MMA
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + G::OFF_BAR + 128);
   float* sbias = reinterpret_cast<float*>(smem + G::OFF_BAR + 144);
 
@@ -150,7 +166,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs
   {
     const uint4* src = reinterpret_cast<const uint4*>(a.wpack);
     uint4* dst = reinterpret_cast<uint4*>(smem + G::OFF_W);
-    for (int i = threadIdx.x; i < (int)(G::WBYTES / 16); i += kConvThreads) dst[i] = src[i];
+    for (int i = threadIdx.x; i < (int)(G::WBYTES / 16); i += kConvFwdThreads) dst[i] = src[i];
     if (threadIdx.x < kCout) sbias[threadIdx.x] = (EPI == kEpiFwdLeaky && a.bias) ? a.bias[threadIdx.x] : 0.f;
   }
   if (threadIdx.x == 0) {
@@ -158,9 +174,9 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs
       tc::mbar_init(&full[s], 1);
       tc::mbar_init(&empty[s], 1);
     }
-    for (int s = 0; s < 2; ++s) {
+    for (int s = 0; s < NACC; ++s) {
       tc::mbar_init(&tfull[s], 1);
-      tc::mbar_init(&tempty[s], 128);
+      tc::mbar_init(&tempty[s], 32 * kConvEpiWarps);
     }
     tc::fence_mbar_init();
   }
@@ -192,7 +208,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
       for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
-        const int s = it % NST, use = it / NST, acc = it & 1, ause = it >> 1;
+        const int s = it % NST, use = it / NST, acc = it % NACC, ause = it / NACC;
         if (!tc::mbar_wait(&tempty[acc], (ause & 1) ^ 1) || !tc::mbar_wait(&full[s], use & 1)) {
           set_err(a.err, 2);
           break;
@@ -238,25 +254,28 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs
       }
     }
   } else {
-    // ---------------- epilogue (warps 2..5) ----------------
+    // ---------------- epilogue (warps 2 .. 2 + kConvEpiWarps - 1) ----------------
+    static_assert(kConvEpiWarps == 8 && R % 2 == 0, "two epilogue warps per lane quarter, each half the rows");
+    constexpr int RH = R / 2;         // rows of a tile this warp finishes
     const int q = warp & 3;           // TMEM lane quarter this warp may access
+    const int r0 = ((warp - 2) >> 2) * RH;  // its first row
     const int p = q * 32 + lane;      // pixel within the tile = TMEM lane
     float dbacc[kCout];
 #pragma unroll
     for (int c = 0; c < kCout; ++c) dbacc[c] = 0.f;
     for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
-      const int use = it >> 1, acc = it & 1;
+      const int use = it / NACC, acc = it % NACC;
       const int txi = t % a.tiles_w, rest = t / a.tiles_w;
       const int tyi = rest % a.tiles_h, b = rest / a.tiles_h;
       const int x = txi * kTW + p;
-      // dgrad: the activation mask of all R rows is requested before waiting for the
+      // dgrad: the activation mask of this warp's rows is requested before waiting for the
       // accumulators, so its latency overlaps the MMAs of this tile
-      uint4 mk[EPI == kEpiDgrad ? R : 1][4];
+      uint4 mk[EPI == kEpiDgrad ? RH : 1][4];
       if (EPI == kEpiDgrad) {
         const uint4* am = reinterpret_cast<const uint4*>(a.amask);
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int y = tyi * R + r;
+        for (int r = 0; r < RH; ++r) {
+          const int y = tyi * R + r0 + r;
           const bool ok = y < a.H && x < a.W;
           const size_t pix = ok ? (((size_t)b * a.H + y) * 4) * a.W + x : 0;
 #pragma unroll
@@ -269,7 +288,8 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs
       }
       tc::tc_fence_after();
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
+      for (int rr = 0; rr < RH; ++rr) {
+        const int r = r0 + rr;  // row of the tile
         uint32_t v[32];
         tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((acc * R + (R - 1 - r)) * kCout), v);
         tc::tmem_wait_ld();
@@ -288,7 +308,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs
           } else {
 #pragma unroll
             for (int ch = 0; ch < 4; ++ch) {
-              const uint4 mv = mk[EPI == kEpiDgrad ? r : 0][ch];
+              const uint4 mv = mk[EPI == kEpiDgrad ? rr : 0][ch];
               const uint32_t mw[4] = {mv.x, mv.y, mv.z, mv.w};
 #pragma unroll
               for (int e = 0; e < 4; ++e) {
@@ -336,9 +356,10 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_kernel(const ConvArgs
   __syncthreads();
   if (EPI == kEpiDgrad && a.db_partial && threadIdx.x < kCout) {
     const float* red = reinterpret_cast<const float*>(smem + G::OFF_W);
-    a.db_partial[(size_t)blockIdx.x * kCout + threadIdx.x] =
-        ((red[0 * kCout + threadIdx.x] + red[1 * kCout + threadIdx.x]) + red[2 * kCout + threadIdx.x]) +
-        red[3 * kCout + threadIdx.x];
+    float sum = red[threadIdx.x];
+#pragma unroll
+    for (int w = 1; w < kConvEpiWarps; ++w) sum += red[w * kCout + threadIdx.x];  // fixed order
+    a.db_partial[(size_t)blockIdx.x * kCout + threadIdx.x] = sum;
   }
   if (warp == 0) {
     tc::tc_fence_after();
@@ -563,7 +584,7 @@ static int conv_launch(int B, int H, int W, const void* x, const void* wpack, co
       return IGM_ERR_CUDA;
     }
   }
-  conv3x3_kernel<C8_IN, kRows, EPI><<<grid, kConvThreads, G::SMEM, st>>>(a);
+  conv3x3_kernel<C8_IN, kRows, EPI><<<grid, kConvFwdThreads, G::SMEM, st>>>(a);
   return launch_status("conv3x3_kernel");
 }
 
