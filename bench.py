@@ -881,7 +881,10 @@ def config5(args, spinup_years=50.0, pretrain_steps=3000, K5=10, nz=16, n=4096):
     from igm_b200.processes import thk as thk_mod
     thk_mod.initialize(cfg_e, st)
     t0 = time.time()
-    net = CNN(nb_layers=16, cin=5, nout=2 * nz, init="he_normal", seed=0, scales=SCALES, out_scale=OUTPUT_SCALE)
+    # the network's fixed output scale, matched to this glacier's speeds (a few m/a after the spin-up,
+    # against ~28,000 m/a for the 1000^2 valley's 200)
+    out_scale = 10.0
+    net = CNN(nb_layers=16, cin=5, nout=2 * nz, init="he_normal", seed=0, scales=SCALES, out_scale=out_scale)
     net.init_weights("he_normal", 0, head_gain=0.01)
     from igm_b200.vertical import compute_levels, compute_zeta_dzeta
     dz = compute_zeta_dzeta(compute_levels(nz, 4.0))[1]
@@ -909,7 +912,7 @@ def config5(args, spinup_years=50.0, pretrain_steps=3000, K5=10, nz=16, n=4096):
     np.savez(os.path.join(path, "model.npz"), params=net.params.cpu().numpy(), adam_m=net.m.cpu().numpy(),
              adam_v=net.v.cpu().numpy(), iterations=np.array(net.opt_iterations), nb_layers=np.array(16),
              nout=np.array(2 * nz), cin=np.array(5), scales=np.asarray(SCALES, np.float32),
-             out_scale=np.array(OUTPUT_SCALE))
+             out_scale=np.array(out_scale))
     del net
     cfg_e.processes.iceflow.emulator.pretrained = True
     cfg_e.processes.iceflow.emulator.name = path
@@ -1052,8 +1055,11 @@ def write_emulator(args):
     a snapshot of thk and usurf every 15 steps), the initial state and two
     copies of it with the thickness scaled by 0.85 and 1.15 (usurf = topg +
     thk): 4000 Adam steps cycling through the 23 states on the Blatter-Pattyn
-    energy, the learning rate on a cosine from 1e-4 to 1e-5, fresh moments.
-    Saved (weights; zero moments) in the layout save_iceflow_model writes."""
+    energy, the learning rate on a cosine from 1e-4 to 1e-5, fresh moments;
+    then the emulated run's own states (300 time steps with that network, a
+    snapshot every 15) join the set for 3000 more steps (cosine 5e-5 to
+    5e-6).  Saved (weights; zero moments) in the layout save_iceflow_model
+    writes."""
     import torch
     from igm_b200.build import build
     from igm_b200.emulator import EmulatorOptimizer, train_step
@@ -1083,16 +1089,36 @@ def write_emulator(args):
         states.append((th, st.topg + th))
     A, C = f[2], f[3]
     ph = physics(cfg)
-    opt = EmulatorOptimizer(1e-4, 1e-7, 1.0)
-    net.m.zero_()
-    net.v.zero_()
-    n = 4000
     ny, nx = A.shape
-    for i in range(n):
-        th, us = states[i % len(states)]
-        lr = 1e-5 + 0.5 * (1e-4 - 1e-5) * (1 + np.cos(np.pi * i / n))
-        train_step(net, [th, us, A, C], 50.0, [(0, 0)], ny, nx, st.dzeta, ph, lr, opt)
-    net.check_errors()
+
+    def fine_tune(states, n, lr0, lr1):
+        opt = EmulatorOptimizer(lr0, 1e-7, 1.0)
+        net.m.zero_()
+        net.v.zero_()
+        for i in range(n):
+            th, us = states[i % len(states)]
+            lr = lr1 + 0.5 * (lr0 - lr1) * (1 + np.cos(np.pi * i / n))
+            train_step(net, [th, us, A, C], 50.0, [(0, 0)], ny, nx, st.dzeta, ph, lr, opt)
+        net.check_errors()
+
+    fine_tune(states, 4000, 1e-4, 1e-5)
+    # third stage: the states of the emulated run itself (300 time steps with this network, the
+    # fallback judge off), added to the training set
+    cfg_r = make_cfg(args, "emulated")
+    cfg_r.processes.iceflow.fallback.every = 0
+    sr = make_state(args)
+    cfg_r.processes.iceflow.emulator.pretrained = False
+    mods_r = init_run(cfg_r, sr)
+    sr.iceflow_model.set_params(net.params.cpu().numpy())
+    sr.iceflow_model.m.zero_()
+    sr.iceflow_model.v.zero_()
+    sr.iceflow_model.opt_iterations = 0
+    for k in range(300):
+        step(cfg_r, sr, mods_r)
+        if k % 15 == 14:
+            states.append((sr.thk.clone(), sr.usurf.clone()))
+    del sr, mods_r
+    fine_tune(states, 3000, 5e-5, 5e-6)
     torch.cuda.synchronize()
     os.makedirs(args.write_emulator, exist_ok=True)
     pr = net.params.cpu().numpy()

@@ -379,7 +379,14 @@ struct WgradArgs {
   int* err;
 };
 
-constexpr int kWRows = 4;  // output rows per work item
+// Weight-gradient kernel: output rows per work item and input stages (build-time constants)
+#ifndef IGM_WGRAD_ROWS
+#define IGM_WGRAD_ROWS 4
+#endif
+#ifndef IGM_WGRAD_STAGES
+#define IGM_WGRAD_STAGES 2
+#endif
+constexpr int kWRows = IGM_WGRAD_ROWS;  // output rows per work item
 
 template <int C8_IN>
 struct WgradGeom {
@@ -395,9 +402,10 @@ struct WgradGeom {
   static constexpr uint32_t GP = kTW * 16;               // G chunk plane stride
   static constexpr uint32_t GBYTES = kWRows * 4 * GP;    // G stage (32 channels, kWRows rows)
   static constexpr uint32_t STAGE = XBYTES + GBYTES;
-  static constexpr int NST = 2;
+  static constexpr int NST = IGM_WGRAD_STAGES;
   static constexpr uint32_t OFF_BAR = NST * STAGE;
   static constexpr uint32_t TMEM_COLS = 3 * WN <= 256 ? 256 : 512;
+  static_assert(2 * NST + 1 <= 8, "barrier slots");
   static constexpr uint32_t SMEM = OFF_BAR + 8 * 8 + 16 + 1024;
   static_assert(kWRows % JN == 0, "whole row groups per item");
 };
@@ -408,9 +416,9 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_wgrad_kernel(const Wg
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
-  uint64_t* full = bars;          // [3]
-  uint64_t* empty = bars + 3;     // [3]
-  uint64_t* done = bars + 6;      // [1]
+  uint64_t* full = bars;               // [NST]
+  uint64_t* empty = bars + G::NST;     // [NST]
+  uint64_t* done = bars + 2 * G::NST;  // [1]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + G::OFF_BAR + 64);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
