@@ -1220,6 +1220,9 @@ extern "C" int igm_cnn_wgrad_finish(const float* partials, int n_parts, int cin,
 extern "C" int igm_cnn_wgrad_finish_split(const float* partials, int n_parts, int cin, float* out, void* stream) {
   IGM_CHECK_ARG(partials && out && n_parts >= 1, IGM_ERR_BAD_ARGUMENT, "igm_cnn_wgrad_finish_split: bad argument");
   IGM_CHECK_ARG(cin >= 1 && cin <= 5, IGM_ERR_BAD_SHAPE, "igm_cnn_wgrad_finish_split: 1..5 input fields");
+  // the kernel reads the 16-channel weight-gradient partials with row groups of 4 (3 x 128 x 4 x 32 floats)
+  IGM_CHECK_ARG(igm_conv3x3_wgrad_partial_len(16) == (size_t)3 * 128 * 4 * kF, IGM_ERR_UNSUPPORTED,
+                "igm_cnn_wgrad_finish_split: the weight-gradient partial layout is not the one this kernel reads");
   wgrad_finish_split_kernel<<<9 * cin, kFinWarps * 32, 0, as_stream(stream)>>>(partials, n_parts, cin, out);
   return launch_status("wgrad_finish_split_kernel");
 }

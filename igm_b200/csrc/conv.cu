@@ -379,14 +379,10 @@ struct WgradArgs {
   int* err;
 };
 
-// Weight-gradient kernel: output rows per work item and input stages (build-time constants)
-#ifndef IGM_WGRAD_ROWS
-#define IGM_WGRAD_ROWS 4
-#endif
-#ifndef IGM_WGRAD_STAGES
-#define IGM_WGRAD_STAGES 2
-#endif
-constexpr int kWRows = IGM_WGRAD_ROWS;  // output rows per work item
+// Output rows per work item of the weight-gradient kernel.  The finish kernels
+// (csrc/cnn.cu) read the partials of the 16-channel input tensor with the row-group
+// width this gives (JN = 4), so the two change together.
+constexpr int kWRows = 4;
 
 template <int C8_IN>
 struct WgradGeom {
@@ -402,7 +398,7 @@ struct WgradGeom {
   static constexpr uint32_t GP = kTW * 16;               // G chunk plane stride
   static constexpr uint32_t GBYTES = kWRows * 4 * GP;    // G stage (32 channels, kWRows rows)
   static constexpr uint32_t STAGE = XBYTES + GBYTES;
-  static constexpr int NST = IGM_WGRAD_STAGES;
+  static constexpr int NST = 2;
   static constexpr uint32_t OFF_BAR = NST * STAGE;
   static constexpr uint32_t TMEM_COLS = 3 * WN <= 256 ? 256 : 512;
   static_assert(2 * NST + 1 <= 8, "barrier slots");
