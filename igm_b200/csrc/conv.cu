@@ -379,31 +379,42 @@ struct WgradArgs {
   int* err;
 };
 
-// Output rows per work item of the weight-gradient kernel.  The finish kernels
-// (csrc/cnn.cu) read the partials of the 16-channel input tensor with the row-group
-// width this gives (JN = 4), so the two change together.
-constexpr int kWRows = 4;
+// Output rows per work item of the weight-gradient kernel, and its input stages.
+// The 16-channel input tensor keeps 4 rows: the finish kernel of the first layer
+// (csrc/cnn.cu) reads its partials with the row-group width that gives (JN = 4).
+// For 32 channels JN = 2 for 2 or 4 rows, so the partial layout does not depend on
+// the build-time choice IGM_WGRAD_ROWS_32 (2 or 4) / IGM_WGRAD_STAGES_32.
+#ifndef IGM_WGRAD_ROWS_32
+#define IGM_WGRAD_ROWS_32 4
+#endif
+#ifndef IGM_WGRAD_STAGES_32
+#define IGM_WGRAD_STAGES_32 2
+#endif
 
 template <int C8_IN>
 struct WgradGeom {
+  static constexpr int WR = C8_IN == 4 ? IGM_WGRAD_ROWS_32 : 4;  // output rows per work item
   static constexpr int NROW = 128 / (C8_IN * 8);         // input rows covered by M = 128
   // output rows covered by N: every one of them finds its three kernel rows in the M window
-  static constexpr int JN = (NROW - 2) < kWRows ? (NROW - 2) : kWRows;
-  static constexpr int NGRP = kWRows / JN;               // MMA row groups per item
+  static constexpr int JN = (NROW - 2) < WR ? (NROW - 2) : WR;
+  static_assert(C8_IN != 4 || JN == 2, "the 32-channel partial layout has row groups of 2");
+  static_assert(C8_IN != 2 || JN == 4, "the 16-channel partial layout has row groups of 4");
+  static constexpr int NGRP = WR / JN;                   // MMA row groups per item
   static constexpr int WN = JN * kCout;                  // accumulator width per kw
-  static constexpr int XROWS = kWRows - JN + NROW;       // input rows of one item
+  static constexpr int XROWS = WR - JN + NROW;           // input rows of one item
   static constexpr uint32_t P = kBoxW * 16;              // X chunk plane stride
   static constexpr uint32_t RS = C8_IN * P;              // X row stride
   static constexpr uint32_t XBYTES = XROWS * RS;         // X stage
   static constexpr uint32_t GP = kTW * 16;               // G chunk plane stride
-  static constexpr uint32_t GBYTES = kWRows * 4 * GP;    // G stage (32 channels, kWRows rows)
+  static constexpr uint32_t GBYTES = WR * 4 * GP;        // G stage (32 channels, WR rows)
   static constexpr uint32_t STAGE = XBYTES + GBYTES;
-  static constexpr int NST = 2;
+  static constexpr int NST = C8_IN == 4 ? IGM_WGRAD_STAGES_32 : 2;
   static constexpr uint32_t OFF_BAR = NST * STAGE;
   static constexpr uint32_t TMEM_COLS = 3 * WN <= 256 ? 256 : 512;
   static_assert(2 * NST + 1 <= 8, "barrier slots");
   static constexpr uint32_t SMEM = OFF_BAR + 8 * 8 + 16 + 1024;
-  static_assert(kWRows % JN == 0, "whole row groups per item");
+  static_assert(WR % JN == 0, "whole row groups per item");
+  static_assert(OFF_BAR + 8 * 8 + 16 + 1024 <= 232448, "shared memory");
 };
 
 template <int C8_IN>
@@ -445,9 +456,9 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_wgrad_kernel(const Wg
         break;
       }
       const int sx = t % a.segs_w, rest = t / a.segs_w;
-      const int y0 = (rest % a.yblocks) * kWRows, b = rest / a.yblocks;
+      const int y0 = (rest % a.yblocks) * G::WR, b = rest / a.yblocks;
       load_tile(a.x, a.H, a.W, C8_IN, b, y0 - 1, G::XROWS, sx * kTW - 1, kBoxW, smem + s * G::STAGE, &full[s], lane);
-      load_tile(a.g, a.H, a.W, 4, b, y0, kWRows, sx * kTW, kTW, smem + s * G::STAGE + G::XBYTES, &full[s], lane);
+      load_tile(a.g, a.H, a.W, 4, b, y0, G::WR, sx * kTW, kTW, smem + s * G::STAGE + G::XBYTES, &full[s], lane);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -604,7 +615,7 @@ static int wgrad_launch(int B, int H, int W, const void* x, const void* g, float
   WgradArgs a{};
   a.B = B; a.H = H; a.W = W;
   a.segs_w = (W + kTW - 1) / kTW;
-  a.yblocks = (H + kWRows - 1) / kWRows;
+  a.yblocks = (H + G::WR - 1) / G::WR;
   a.n_items = B * a.yblocks * a.segs_w;
   a.x = (const __nv_bfloat16*)x;
   a.g = (const __nv_bfloat16*)g;
