@@ -32,6 +32,9 @@ accuracy    velocity error (relative L2 of the staggered velocities over ice
             of the timed window.
 config1     the 100 x 100 plain-solver run (100 iterations per time step, ELA
             transport) against the oracle on the same first time steps.
+config3     the emulator training recipe alone: a fresh He-initialised network,
+            2000 Adam steps at lr 1e-4 on batches of 8 windows of 64 x 64
+            cells, its whole-domain velocity error against the judge.
 config5     4096 x 4096 x Nz 16 (ridge bed, plain spin-up): emulator vs plain.
 --impl reference   the oracle's restatement of the same emulated run
             (torch-CPU FP32, all host threads, the same network weights) on a
@@ -81,6 +84,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-da", action="store_true")
     ap.add_argument("--no-config1", action="store_true")
+    ap.add_argument("--no-config3", action="store_true")
     ap.add_argument("--no-config5", action="store_true")
     ap.add_argument("--no-kernels", action="store_true")
     ap.add_argument("--write-emulator", default="", help="pretrain the bench's emulator, write it to this "
@@ -374,6 +378,55 @@ def judge_error(cfg, st, U, V, Ur, Vr):
     return J.velocity_rel_l2(U, V, Ur, Vr, f[0]), (e - er) / abs(er)
 
 
+def emulator_recipe(args, cfg, st, Uj, Vj, steps=2000, batch=8, patch=64, lr=1e-4, seed=0):
+    """The emulator training recipe on its own: a fresh 16 x 3x3 x 32 network
+    (He-initialised from ``seed``; the head's initial weights scaled by 0.01
+    so that the first outputs stay near zero), trained physics-informed on
+    batches of ``batch`` windows of ``patch`` x ``patch`` cells (the
+    convolutions zero-pad each window's border), drawn with a seeded RNG among
+    the windows whose centre lies on ice, by Adam at ``lr`` for ``steps``
+    steps -- the loss and update of update_iceflow_emulator
+    (emulate.py:155-281).  Reported: the velocity error and energy gap of the
+    whole-domain prediction against the judge's minimiser (Uj, Vj), and the
+    training time (CUDA events)."""
+    import torch
+    from igm_b200.cnn import CNN
+    from igm_b200.emulator import EmulatorOptimizer, train_step
+    from igm_b200.processes.iceflow import physics
+    f = fields(st)
+    ny, nx = f[0].shape
+    dz = np.asarray(st.dzeta, np.float64)
+    e = cfg.processes.iceflow.emulator
+    net = CNN(nb_layers=16, cin=5, nout=2 * args.nz, init="he_normal", seed=seed, scales=SCALES,
+              out_scale=OUTPUT_SCALE)
+    net.init_weights("he_normal", seed, head_gain=0.01)
+    opt = EmulatorOptimizer(lr, e.optimizer_epsilon, e.optimizer_clipnorm)
+    h = patch // 2
+    ice = torch.nonzero(f[0][h:ny - patch + h + 1, h:nx - patch + h + 1] > 0).cpu().numpy()
+    rng = np.random.default_rng(seed)
+    ph = physics(cfg)
+    cost = []
+    s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for i in range(steps):
+        wins = [(int(y), int(x)) for y, x in ice[rng.integers(0, len(ice), batch)]]
+        terms = train_step(net, f, 50.0, wins, patch, patch, dz, ph, lr, opt)
+        if i % 100 == 0 or i == steps - 1:
+            cost.append(terms.sum())
+    t.record()
+    torch.cuda.synchronize()
+    net.check_errors()
+    n_cell = batch * (patch - 1) ** 2
+    buf = net.buffers(1, ny, nx, train=False)
+    net.prepare_input(f, 50.0, [(0, 0)], ny, nx, buf)
+    U, V = net.forward(buf, 1, ny, nx, thk_mask=f[0])
+    err, gap = judge_error(cfg, st, U[0], V[0], Uj, Vj)
+    return {"steps": steps, "batch": batch, "patch": patch, "lr": lr, "seed": seed,
+            "train_ms_per_step": s.elapsed_time(t) / steps,
+            "patch_energy_per_cell_every_100_steps": [float(c) / n_cell for c in cost],
+            "vel_rel_l2_vs_fp64": err, "energy_gap_vs_fp64": gap}
+
+
 def velbar_absmax(st):
     import torch
     return float(torch.maximum(st.ubar.abs().max(), st.vbar.abs().max()))
@@ -423,6 +476,8 @@ def run_ours(args, rank, world, dist):
     # the emulator's field on the initial state (after the iceflow initialisation's retraining)
     res["vel_rel_l2_vs_fp64"], res["energy_gap_vs_fp64"] = judge_error(cfg_e, st, st.U, st.V, Uj, Vj)
     det["velbar_absmax_emulated_initial"] = velbar_absmax(st)
+    if rank == 0 and not args.no_config3:
+        det["config3"] = emulator_recipe(args, cfg_e, st, Uj, Vj)
     U_init, V_init = Uj.float(), Vj.float()
     run_cycles(cfg_e, st, mods, W)
     conv_ev = []
@@ -1208,6 +1263,8 @@ def main():
             if "cpu" in c1 and "gpu_first_steps" in c1:
                 line["config1_first_steps_gpu_vs_cpu"] = (c1["gpu_first_steps"]["years_per_s"]
                                                           / c1["cpu"]["years_per_s"])
+        if "config3" in det:
+            line["config3_recipe_vel_rel_l2_vs_fp64"] = det["config3"]["vel_rel_l2_vs_fp64"]
         if "config5" in det:
             line["config5_speedup_vs_plain"] = det["config5"]["speedup_vs_plain"]
             line["config5_emulated_years_per_s"] = det["config5"]["emulated"]["years_per_s"]

@@ -18,11 +18,13 @@ and diagnostic/diagnostic.py), on the device.
   emulated ones -- for that update alone (fallback.mode "step") or for the
   updates until the next check, each a warm-started solve (mode "takeover",
   the default).
-* ``save_iceflow_model`` / ``load_iceflow_model``: weights, Adam moments and
-  iteration count as ``model.npz`` next to the reference's ``fieldin.dat`` and
-  ``vert_grid.dat`` text files (emulate.py:331-359); ``load_keras_h5`` reads
-  the reference's own Keras ``model.h5`` files (igm_b200.keras_h5, no h5py
-  needed), so the emulators the reference ships run as pretrained networks.
+* ``save_iceflow_model`` / ``load_iceflow_model``: the reference's Keras
+  ``model.h5`` (written by igm_b200.keras_h5, no h5py needed) with its
+  ``fieldin.dat`` and ``vert_grid.dat`` text files (emulate.py:331-359), and
+  beside them weights, Adam moments and iteration count as ``model.npz``;
+  ``load_keras_h5`` reads Keras ``model.h5`` files, so the emulators the
+  reference ships run as pretrained networks and the reference loads the
+  networks trained here.
 """
 
 from __future__ import annotations
@@ -308,12 +310,31 @@ def update_iceflow_takeover(cfg, state):
         update_iceflow_emulated(cfg, state)
 
 
+def keras_variables(m: CNN):
+    """The network as the reference's Keras ``cnn`` computes it on the raw
+    fields: the input scales folded into the first kernel (input channel c
+    times scales[c]) and the output scale into the head's kernel and bias."""
+    v = [np.array(a, dtype=np.float32) for a in m.get_variables()]
+    v[0] = v[0] * m.scales[None, None, :v[0].shape[2], None]
+    v[-2] = v[-2] * np.float32(m.out_scale)
+    v[-1] = v[-1] * np.float32(m.out_scale)
+    return v
+
+
 def save_iceflow_model(cfg, state, directory="iceflow-model"):
-    """emulate.py:331-359, with model.npz in place of model.h5."""
+    """emulate.py:331-359: model.h5 (a Keras HDF5 model file of the network on
+    raw fields, which the reference's load_model reads), fieldin.dat and
+    vert_grid.dat; beside them model.npz, the exact parameters with their
+    input and output scales and the Adam state, which this package's loader
+    prefers."""
+    from .keras_h5 import write_keras_cnn
     if os.path.exists(directory):
         shutil.rmtree(directory)
     os.mkdir(directory)
     m: CNN = state.iceflow_model
+    net = cfg.processes.iceflow.emulator.network
+    write_keras_cnn(os.path.join(directory, "model.h5"), keras_variables(m), m.L, m.cin, m.nout, alpha=m.alpha,
+                    init=str(net.weight_initialization))
     np.savez(os.path.join(directory, "model.npz"), params=m.params.cpu().numpy(), adam_m=m.m.cpu().numpy(),
              adam_v=m.v.cpu().numpy(), iterations=np.array(m.opt_iterations), nb_layers=np.array(m.L),
              nout=np.array(m.nout), cin=np.array(m.cin), scales=m.scales, out_scale=np.array(m.out_scale))

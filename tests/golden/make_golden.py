@@ -8,9 +8,10 @@ xarray, OGGM and the rest of the model, so the packages on the path are
 registered as bare namespace stubs and only the hot-path modules are loaded
 from their files.
 
-Run from the repository root:  python tests/golden/make_golden.py REF_ROOT
+Run from the repository root:  python tests/golden/make_golden.py REF_ROOT [case ...]
 (REF_ROOT: the root of the reference's source tree, the directory holding
-``igm/``; or set IGM_REFERENCE_ROOT).  Writes ``*.npz`` next to this file.
+``igm/``; or set IGM_REFERENCE_ROOT; the optional case names, functions of
+this file, run those cases alone).  Writes ``*.npz`` / ``*.json`` next to this file.
 The generated inputs are seeded; re-running reproduces the files bit for bit.
 """
 
@@ -350,6 +351,42 @@ def keras_h5_cases():
     print(f"wrote {dst} ({os.path.getsize(dst)} B)")
 
 
+def keras_h5_layout_case():
+    """The file layout of the newest emulator the reference ships without
+    dropout layers (pinnbp_5_4_cnn_16_32_2_1_e, written by tf.keras 2.15):
+    the SHA-256 and length of its model_config, its layer and weight names,
+    its root attribute names, and the raw bytes of the superblock's format
+    fields and of the header messages of one kernel dataset -- what
+    igm_b200.keras_h5's writer must reproduce for the reference's
+    load_model to read the networks trained here."""
+    import hashlib
+    import json
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from igm_b200.keras_h5 import _File
+    path = os.path.join(IGM, "processes", "iceflow", "emulate", "emulators", "pinnbp_5_4_cnn_16_32_2_1_e", "model.h5")
+    f = _File(path)
+    attrs = f.attributes(f.root)
+    mc = str(attrs["model_config"].reshape(-1)[0]).encode()
+    mw = f.lookup("model_weights")
+    lnames = [str(x) for x in f.attributes(mw)["layer_names"].reshape(-1)]
+    kids = f.children(mw)
+    layer_weights = {n: [str(x) for x in np.asarray(f.attributes(kids[n])["weight_names"]).reshape(-1)] for n in lnames}
+    conv = f.children(kids["conv2d"])["conv2d"]
+    kern = f.children(conv)["kernel:0"]
+    msgs = {"0x%02x" % t: f.b[p - 8:p + n].hex() for t, p, n in f.messages(kern) if t in (1, 3, 5)}
+    layout = [f.b[p:p + 2].hex() for t, p, n in f.messages(kern) if t == 8]
+    out = {"file": os.path.relpath(path, IGM), "model_config_sha256": hashlib.sha256(mc).hexdigest(),
+           "model_config_len": len(mc), "root_attributes": sorted(attrs),
+           "keras_version": str(attrs["keras_version"].reshape(-1)[0]),
+           "model_weights_attributes": sorted(f.attributes(mw)), "layer_names": lnames,
+           "weight_names": layer_weights, "superblock_format": f.b[8:24].hex(),
+           "kernel_messages": msgs, "kernel_layout_version_class": layout[0]}
+    dst = os.path.join(HERE, "keras_h5_layout.json")
+    with open(dst, "w") as fh:
+        json.dump(out, fh, indent=1)
+    print(f"wrote {dst} ({os.path.getsize(dst)} B)")
+
+
 def assim_cases():
     """The data-assimilation cost terms of the default configuration (control
     thk; costs velsurf, thk, icemask; penalty constraint; anisotropic and
@@ -619,7 +656,11 @@ def save(name, d):
     print(f"wrote {path} ({os.path.getsize(path)} B)")
 
 
-if __name__ == "__main__":
+if __name__ == "__main__" and len(sys.argv) > 2:  # only the named cases: make_golden.py REF_ROOT case ...
+    torch.set_num_threads(1)
+    for name in sys.argv[2:]:
+        globals()[name]()
+elif __name__ == "__main__":
     torch.set_num_threads(1)
     vert_cases()
     energy_case("small_f64", 13, 11, 4, 100.0, 1, torch.float64, c_neg=True)

@@ -22,6 +22,8 @@ difference is caught where it is made instead of accumulating:
   that the oracle's solve from the emulated velocities gives.
 """
 
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -303,6 +305,46 @@ def test_save_load_round_trip(tmp_path, monkeypatch):
     E.update_iceflow_emulated(cfg, st)
     E.update_iceflow_emulated(cfg2, st2)
     assert torch.equal(st.U, st2.U) and torch.equal(st.V, st2.V)
+
+
+def test_saved_keras_file_loads(tmp_path, monkeypatch):
+    """The model.h5 that save_iceflow_model writes (the network on raw fields,
+    its scales folded into the weights) loads through the reference's route
+    -- a pretrained emulator directory holding model.h5 and fieldin.dat
+    (emulate.py:64-93) -- and gives the saved network's velocities to the
+    BF16 rounding of the refolded weights."""
+    import shutil
+    monkeypatch.chdir(tmp_path)
+    cfg = make_cfg("emulated", retrain_freq=1)
+    cfg.processes.iceflow.emulator.save_model = True
+    st = make_state(seed=7)
+    mods = init(cfg, st)
+    for _ in range(2):
+        for m in mods:
+            m.update(cfg, st)
+        st.it += 1
+    iceflow.finalize(cfg, st)
+    os.mkdir(tmp_path / "keras-only")
+    for f in ("model.h5", "fieldin.dat", "vert_grid.dat"):
+        shutil.copy(tmp_path / "iceflow-model" / f, tmp_path / "keras-only" / f)
+    cfg2 = make_cfg("emulated", retrain_freq=1)
+    cfg2.processes.iceflow.emulator.pretrained = True
+    cfg2.processes.iceflow.emulator.name = "keras-only"
+    st2 = make_state(seed=7)
+    st2.original_cwd = str(tmp_path)
+    thk.initialize(cfg2, st2)
+    E.initialize_iceflow_emulator(cfg2, st2)
+    net2 = st2.iceflow_model
+    assert net2.out_scale == 1.0 and np.all(net2.scales == 1.0)
+    st.dzeta = st2.dzeta = iceflow.compute_zeta_dzeta(iceflow.compute_levels(NZ, 4.0))[1]
+    st2.vert_weight = iceflow.define_vertical_weight(NZ, 4.0)
+    for k in ("thk", "usurf"):
+        setattr(st2, k, getattr(st, k).clone())
+    E.update_iceflow_emulated(cfg, st)
+    E.update_iceflow_emulated(cfg2, st2)
+    assert float(st.U.abs().max()) > 0
+    assert rel_l2(cpu(st2.U).numpy(), cpu(st.U).numpy()) < 2e-2
+    assert rel_l2(cpu(st2.V).numpy(), cpu(st.V).numpy()) < 2e-2
 
 
 @pytest.mark.parametrize("method", ["emulated", "solved"])
