@@ -207,6 +207,10 @@ __global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_kernel(const ConvA
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
+      // descriptors as (low word + compile-time offset, fixed high word): a few integer
+      // instructions per MMA keep this one thread ahead of the tensor cores
+      constexpr uint32_t a_hi = tc::desc_hi(128), b_hi = tc::desc_hi(128);
+      const uint32_t w_lo = tc::desc_lo(sbase + G::OFF_W, kWRowsN * 16);
       for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
         const int s = it % NST, use = it / NST, acc = it % NACC, ause = it / NACC;
         if (!tc::mbar_wait(&tempty[acc], (ause & 1) ^ 1) || !tc::mbar_wait(&full[s], use & 1)) {
@@ -214,8 +218,7 @@ __global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_kernel(const ConvA
           break;
         }
         tc::tc_fence_after();
-        const uint32_t in0 = sbase + s * G::STAGE;
-        const uint32_t w0 = sbase + G::OFF_W;
+        const uint32_t in_lo = tc::desc_lo(sbase + s * G::STAGE, G::P);
         const uint32_t dset = tmem + (uint32_t)(acc * R * kCout);
         // Input row i (global row y0 - 1 + i) feeds output rows o = i - dy through kernel row dy.
         // One MMA covers all of its valid dy at once (N = 32 ndy): output row o accumulates at
@@ -232,18 +235,18 @@ __global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_kernel(const ConvA
           for (int dx = 0; dx < 3; ++dx) {
 #pragma unroll
             for (int ks = 0; ks < C8_IN / 2; ++ks) {
-              const uint32_t aaddr = in0 + i * G::RS + dx * 16 + ks * 2 * G::P;
-              const uint32_t baddr = w0 + ((dx * C8_IN + ks * 2) * kWRowsN + dlo * kCout) * 16;
-              const uint64_t ad = tc::make_desc(aaddr, G::P, 128);
+              const uint32_t aoff = (i * G::RS + dx * 16 + ks * 2 * G::P) >> 4;
+              const uint32_t boff = (((dx * C8_IN + ks * 2) * kWRowsN + dlo * kCout) * 16) >> 4;
+              const uint64_t ad = tc::desc_join(in_lo + aoff, a_hi);
               if (dx == 0 && ks == 0 && dlo == 0) {
                 // output row i starts here: initialise its accumulator alone, then add to the rows above
-                tc::mma_bf16(dcol, ad, tc::make_desc(baddr, kWRowsN * 16, 128),
-                             tc::make_idesc_bf16(128, kCout, false, false), 0u);
+                tc::mma_bf16(dcol, ad, tc::desc_join(w_lo + boff, b_hi), tc::make_idesc_bf16(128, kCout, false, false),
+                             0u);
                 if (ndy > 1)
-                  tc::mma_bf16(dcol + kCout, ad, tc::make_desc(baddr + kCout * 16, kWRowsN * 16, 128),
+                  tc::mma_bf16(dcol + kCout, ad, tc::desc_join(w_lo + boff + ((kCout * 16) >> 4), b_hi),
                                tc::make_idesc_bf16(128, kCout * (ndy - 1), false, false), 1u);
               } else {
-                tc::mma_bf16(dcol, ad, tc::make_desc(baddr, kWRowsN * 16, 128),
+                tc::mma_bf16(dcol, ad, tc::desc_join(w_lo + boff, b_hi),
                              tc::make_idesc_bf16(128, kCout * ndy, false, false), 1u);
               }
             }
@@ -463,6 +466,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_wgrad_kernel(const Wg
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t idesc = tc::make_idesc_bf16(128, G::WN, true, true);
+      constexpr uint32_t x_hi = tc::desc_hi(G::P), g_hi = tc::desc_hi(G::GP);
       for (int it = 0, t = blockIdx.x; t < a.n_items; t += gridDim.x, ++it) {
         const int s = it % G::NST, use = it / G::NST;
         if (!tc::mbar_wait(&full[s], use & 1)) {
@@ -470,21 +474,23 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_wgrad_kernel(const Wg
           break;
         }
         tc::tc_fence_after();
-        const uint32_t x0 = sbase + s * G::STAGE;
-        const uint32_t g0 = x0 + G::XBYTES;
+        // A: M = (input row, ci) groups of 8 channels every P bytes; K = pixels, 8-pixel groups 128 B apart.
+        // B: N = (output row, co) groups of 8 every GP bytes; K = pixels.
+        const uint32_t x_lo = tc::desc_lo(sbase + s * G::STAGE, 128);
+        const uint32_t g_lo = tc::desc_lo(sbase + s * G::STAGE + G::XBYTES, 128);
         // Row group q: output rows y0 + q JN + jj (N = (jj, co)) against input rows
         // y0 - 1 + q JN + m (M = (m, ci)); the product lands at kernel row kh = m - jj.
 #pragma unroll 1
         for (int q = 0; q < G::NGRP; ++q) {
+          const uint32_t xq = x_lo + ((q * G::JN * G::RS) >> 4), gq = g_lo + ((q * G::JN * 4 * G::GP) >> 4);
+          const uint32_t acc0 = (it > 0 || q > 0) ? 1u : 0u;
 #pragma unroll
           for (int dx = 0; dx < 3; ++dx) {
 #pragma unroll
             for (int ks = 0; ks < kTW / 16; ++ks) {
-              // A: M = (input row, ci) groups of 8 channels every P bytes; K = pixels, 8-pixel groups 128 B apart
-              const uint64_t ad = tc::make_desc(x0 + q * G::JN * G::RS + dx * 16 + ks * 256, 128, G::P);
-              // B: N = (output row, co) groups of 8 every GP bytes; K = pixels
-              const uint64_t bd = tc::make_desc(g0 + q * G::JN * 4 * G::GP + ks * 256, 128, G::GP);
-              tc::mma_bf16(tmem + dx * G::WN, ad, bd, idesc, (it > 0 || q > 0 || ks > 0) ? 1u : 0u);
+              const uint64_t ad = tc::desc_join(xq + ((dx * 16 + ks * 256) >> 4), x_hi);
+              const uint64_t bd = tc::desc_join(gq + ((ks * 256) >> 4), g_hi);
+              tc::mma_bf16(tmem + dx * G::WN, ad, bd, idesc, ks > 0 ? 1u : acc0);
             }
           }
         }

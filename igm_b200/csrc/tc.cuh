@@ -108,6 +108,21 @@ __device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint
   return d;                // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
 }
 
+// The same descriptor as two 32-bit words, for issue loops: the start address
+// occupies the low 14 bits of the low word and shared-memory addresses stay
+// below 256 KB, so an operand moved by a 16-byte multiple that keeps it inside
+// shared memory is the low word plus (offset >> 4), with no carry into the
+// reserved bits above it; the high word (SBO, version) stays fixed.
+__device__ __forceinline__ uint32_t desc_lo(uint32_t saddr, uint32_t lbo) {
+  return ((saddr >> 4) & 0x3FFFu) | (((lbo >> 4) & 0x3FFFu) << 16);
+}
+__host__ __device__ constexpr uint32_t desc_hi(uint32_t sbo) { return ((sbo >> 4) & 0x3FFFu) | (1u << 14); }
+__device__ __forceinline__ uint64_t desc_join(uint32_t lo, uint32_t hi) {
+  uint64_t d;
+  asm("mov.b64 %0, {%1, %2};\n" : "=l"(d) : "r"(lo), "r"(hi));
+  return d;
+}
+
 // Instruction descriptor of tcgen05.mma kind::f16: BF16 x BF16 -> FP32.
 __host__ __device__ constexpr uint32_t make_idesc_bf16(int M, int N, bool a_mn_major, bool b_mn_major) {
   return (1u << 4)                        // D format: F32
