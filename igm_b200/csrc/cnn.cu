@@ -65,6 +65,7 @@ __host__ __device__ inline size_t param_count(int L, int cin0, int nout) {
 //  dgrad    layer l>=1: [kw'][k-chunk (co)][kh'][ci][8], flipped: kh' = 2 - kh, kw' = 2 - kw
 // ---------------------------------------------------------------------------
 __global__ void pack_kernel(const float* params, int L, int cin0, int nout, __nv_bfloat16* wf, __nv_bfloat16* wb) {
+  grid_dep_wait();
   const size_t n0 = (size_t)9 * 2 * kF * 8;   // layer 0, forward
   const size_t ni = (size_t)9 * 4 * kF * 8;   // other layers, per pack
   const size_t total_f = n0 + (size_t)(L - 1) * ni;
@@ -122,6 +123,7 @@ struct InputArgs {
 };
 
 __global__ void input_kernel(const InputArgs a) {
+  grid_dep_wait();
   const size_t plane = (size_t)a.h * a.w;
   const size_t total = plane * a.B;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
@@ -177,6 +179,7 @@ template <int NJ>
 __global__ void __launch_bounds__(256) head_fwd_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act,
                                                        const float* wh, const float* bh, float out_scale, float* U,
                                                        float* V, const float* thk_mask) {
+  grid_dep_wait();
   static_assert(NJ % 4 == 0, "NJ");
   __shared__ __align__(16) float sw[kF * NJ + NJ];  // [32][NJ] then bias [NJ]
   const int nout = 2 * nz;
@@ -257,6 +260,7 @@ template <int NJ>
 __global__ void __launch_bounds__(kHeadWarps * 32, 2)
     head_bwd_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act, const float* wh, const float* dU,
                     const float* dV, float out_scale, float alpha, __nv_bfloat16* dpre, float* partial) {
+  grid_dep_wait();
   using SM_ = HeadBwdSmem<NJ>;
   constexpr int GS = SM_::GS;
   extern __shared__ __align__(16) float sm[];
@@ -457,6 +461,7 @@ __global__ void __launch_bounds__(kHpWarps * 32, 2)
     head_bwd_px_kernel(int B, int H, int W, int nz, const __nv_bfloat16* act, const float* wh, const float* dU,
                        const float* dV, float out_scale, float alpha, __nv_bfloat16* dpre, __nv_bfloat16* dyb,
                        float* partial) {
+  grid_dep_wait();
   static_assert(NJ % 4 == 0 && NJ <= kF, "NJ");
   __shared__ __align__(16) float swT[NJ * kF];  // [j][ci] = Wh[ci][j], 0 for j >= 2 nz
   __shared__ float red[kHpWarps][NJ + kF];
@@ -592,6 +597,7 @@ __device__ __forceinline__ float finish_sum(const float* part, int n_parts, int 
 // tap (kh = kw = 1), i.e. accumulator entries (r, jj) with r - jj = 1, kw = 1.
 __global__ void __launch_bounds__(kFinWarps * 32) head_wgrad_finish_kernel(const float* part, int n_parts, int nout,
                                                                            float* out) {
+  grid_dep_wait();
   __shared__ float red[kFinWarps][kF];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int cw = 32, jn = 2;
@@ -640,6 +646,7 @@ __device__ __forceinline__ void l1_inputs(const L1Args& a, int b, int y, int x, 
 }
 
 __global__ void __launch_bounds__(256) layer1_fwd_kernel(const L1Args a) {
+  grid_dep_wait();
   __shared__ __align__(16) float sw[9 * 5 * kF + kF];
   for (int i = threadIdx.x; i < 9 * a.cin * kF; i += blockDim.x) sw[i] = a.w[i];
   if (threadIdx.x < kF) sw[9 * 5 * kF + threadIdx.x] = a.b[threadIdx.x];
@@ -703,6 +710,7 @@ constexpr int kL1Red = 45 * kF;
 constexpr int kL1Stride = kL1Warp > kL1Red ? kL1Warp : kL1Red;
 __global__ void __launch_bounds__(kL1Warps * 32, 2) layer1_wgrad_kernel(const L1Args a, const __nv_bfloat16* g,
                                                                        float* partial) {
+  grid_dep_wait();
   extern __shared__ __align__(16) float sm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* sX = sm + warp * kL1Stride;  // [32 pixels][48]
@@ -785,6 +793,7 @@ __global__ void __launch_bounds__(kL1Warps * 32, 2) layer1_wgrad_kernel(const L1
 // additions keep the order p = lane, lane + 32, ... (absent partials add +0).
 __global__ void reduce_partials_kernel(const float* part, int n_parts, int len, int stride, float* out,
                                        int accumulate) {
+  grid_dep_wait();
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < len; i += nw) {
@@ -814,6 +823,7 @@ __global__ void reduce_partials_kernel(const float* part, int n_parts, int len, 
 // added in a fixed order -- deterministic.
 __global__ void __launch_bounds__(kFinWarps * 32) wgrad_finish_kernel(const float* part, int n_parts, int cin,
                                                                       int cw, float* out) {
+  grid_dep_wait();
   __shared__ float red[kFinWarps][kF];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int groups = 9 * cin;
@@ -838,6 +848,7 @@ __global__ void __launch_bounds__(kFinWarps * 32) wgrad_finish_kernel(const floa
 // (3c + 2, weights W_l) only carries the weights' low part and is not a variable.
 __global__ void __launch_bounds__(kFinWarps * 32) wgrad_finish_split_kernel(const float* part, int n_parts, int cin,
                                                                             float* out) {
+  grid_dep_wait();
   __shared__ float red[kFinWarps][kF];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int cw = 16, jn = 4;  // the 16-channel input tensor's partial layout
@@ -875,6 +886,7 @@ struct AdamVars {
 static int norm_chunks(size_t len) { return (int)((len + kNormChunk - 1) / kNormChunk); }
 
 __global__ void __launch_bounds__(256) grad_norm_parts_kernel(const float* g, const AdamVars vars, double* parts) {
+  grid_dep_wait();
   __shared__ double sh[8];
   const int b = blockIdx.x;
   int v = 0;
@@ -888,6 +900,7 @@ __global__ void __launch_bounds__(256) grad_norm_parts_kernel(const float* g, co
 }
 
 __global__ void grad_norm_finish_kernel(const double* parts, const AdamVars vars, double* norms) {
+  grid_dep_wait();
   const int v = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (v >= vars.n) return;  // uniform per warp
   double s = 0.0;
@@ -898,6 +911,7 @@ __global__ void grad_norm_finish_kernel(const double* parts, const AdamVars vars
 
 __global__ void adam_kernel(float* x, const float* g, float* m, float* v, const AdamVars vars, const double* norms,
                             float lr_t, float b1, float b2, float eps, float clipnorm) {
+  grid_dep_wait();
   const size_t total = vars.off[vars.n];
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     int k = 0;
@@ -939,6 +953,7 @@ constexpr int kIgTY = 8, kIgTX = 32;  // output tile of one CTA (256 threads, on
 template <int NG>
 __global__ void __launch_bounds__(256) input_grad_kernel(int B, int H, int W, int cin, const __nv_bfloat16* dpre,
                                                          const float* w0, InputGradScales sc, float* out) {
+  grid_dep_wait();
   __shared__ __align__(16) float sw[9 * NG * kF];                // [tap][c][co] of the fields computed
   __shared__ uint4 tile[kIgTY + 2][4][kIgTX + 2];                // dPre0 rows y0-1 .. y0+8, 8-channel chunks
   for (int i = threadIdx.x; i < 9 * NG * kF; i += blockDim.x) {
@@ -1013,7 +1028,7 @@ extern "C" int igm_cnn_pack_weights(int nb_layers, int cin, int nout, const floa
   IGM_CHECK_ARG(params && wpack_fwd && (wpack_bwd || nb_layers == 1), IGM_ERR_BAD_ARGUMENT,
                 "igm_cnn_pack_weights: NULL argument");
   const size_t total = (size_t)9 * 2 * kF * 8 + (size_t)(nb_layers - 1) * 9 * 4 * kF * 8 * 2;
-  pack_kernel<<<grid_for(total), 256, 0, as_stream(stream)>>>(params, nb_layers, cin, nout,
+  launch_pdl(pack_kernel, dim3(grid_for(total)), dim3(256), 0, as_stream(stream), params, nb_layers, cin, nout,
                                                               (__nv_bfloat16*)wpack_fwd, (__nv_bfloat16*)wpack_bwd);
   return launch_status("pack_kernel");
 }
@@ -1039,7 +1054,7 @@ extern "C" int igm_cnn_input(int batch, int h, int w, int ny, int nx, const floa
   }
   a.X = (__nv_bfloat16*)X;
   a.out[0] = thk_out; a.out[1] = usurf_out; a.out[2] = arrhenius_out; a.out[3] = slidingco_out;
-  input_kernel<<<grid_for((size_t)batch * h * w), 256, 0, as_stream(stream)>>>(a);
+  launch_pdl(input_kernel, dim3(grid_for((size_t)batch * h * w)), dim3(256), 0, as_stream(stream), a);
   return launch_status("input_kernel");
 }
 
@@ -1068,7 +1083,7 @@ extern "C" int igm_cnn_layer1_forward(int batch, int h, int w, int cin, const fl
   if (rc) return rc;
   IGM_CHECK_ARG(b1 && act, IGM_ERR_BAD_ARGUMENT, "igm_cnn_layer1_forward: NULL argument");
   a.out = (__nv_bfloat16*)act;
-  layer1_fwd_kernel<<<grid_for((size_t)batch * h * w), 256, 0, as_stream(stream)>>>(a);
+  launch_pdl(layer1_fwd_kernel, dim3(grid_for((size_t)batch * h * w)), dim3(256), 0, as_stream(stream), a);
   return launch_status("layer1_fwd_kernel");
 }
 
@@ -1090,7 +1105,7 @@ extern "C" int igm_cnn_layer1_wgrad(int batch, int h, int w, int cin, const floa
     }
     configured = true;
   }
-  layer1_wgrad_kernel<<<n_parts, kL1Warps * 32, smem, as_stream(stream)>>>(a, (const __nv_bfloat16*)g, partials);
+  launch_pdl(layer1_wgrad_kernel, dim3(n_parts), dim3(kL1Warps * 32), smem, as_stream(stream), a, (const __nv_bfloat16*)g, partials);
   return launch_status("layer1_wgrad_kernel");
 }
 
@@ -1108,7 +1123,7 @@ extern "C" int igm_cnn_head_forward(int batch, int h, int w, int nz, const void*
     switch ((nout + 3) / 4) {
 #define IGM_HEAD_FWD(Q)                                                                                      \
   case Q:                                                                                                    \
-    head_fwd_kernel<4 * Q><<<grid, 256, 0, st>>>(batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask); \
+    launch_pdl(head_fwd_kernel<4 * Q>, dim3(grid), dim3(256), 0, st, batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask); \
     break;
       IGM_HEAD_FWD(1) IGM_HEAD_FWD(2) IGM_HEAD_FWD(3) IGM_HEAD_FWD(4) IGM_HEAD_FWD(5) IGM_HEAD_FWD(6)
       IGM_HEAD_FWD(7) IGM_HEAD_FWD(8)
@@ -1117,9 +1132,9 @@ extern "C" int igm_cnn_head_forward(int batch, int h, int w, int nz, const void*
         return IGM_ERR_BAD_SHAPE;
     }
   } else if (nout <= 64)
-    head_fwd_kernel<64><<<grid, 256, 0, st>>>(batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask);
+    launch_pdl(head_fwd_kernel<64>, dim3(grid), dim3(256), 0, st, batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask);
   else
-    head_fwd_kernel<128><<<grid, 256, 0, st>>>(batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask);
+    launch_pdl(head_fwd_kernel<128>, dim3(grid), dim3(256), 0, st, batch, h, w, nz, A, head_w, head_b, out_scale, U, V, thk_mask);
   return launch_status("head_fwd_kernel");
 }
 
@@ -1139,7 +1154,7 @@ static int head_bwd_launch(int batch, int h, int w, int nz, const void* act, con
     }
     configured = true;
   }
-  head_bwd_kernel<NJ><<<n_parts, kHeadWarps * 32, smem, st>>>(batch, h, w, nz, (const __nv_bfloat16*)act, head_w, dU,
+  launch_pdl(head_bwd_kernel<NJ>, dim3(n_parts), dim3(kHeadWarps * 32), smem, st, batch, h, w, nz, (const __nv_bfloat16*)act, head_w, dU,
                                                                 dV, out_scale, alpha, (__nv_bfloat16*)dpre, partials);
   return launch_status("head_bwd_kernel");
 }
@@ -1176,10 +1191,10 @@ extern "C" int igm_cnn_head_backward_tc(int batch, int h, int w, int nz, const v
 #define IGM_HEAD_PX(Q)                                                                                              \
   case Q:                                                                                                           \
     if (params)                                                                                                     \
-      head_bwd_px_kernel<4 * Q, true><<<n_parts, kHpWarps * 32, 0, st>>>(batch, h, w, nz, a16, head_w, dU, dV,     \
+      launch_pdl(head_bwd_px_kernel<4 * Q, true>, dim3(n_parts), dim3(kHpWarps * 32), 0, st, batch, h, w, nz, a16, head_w, dU, dV,     \
                                                                          out_scale, alpha, dp, dy, partials);       \
     else                                                                                                            \
-      head_bwd_px_kernel<4 * Q, false><<<n_parts, kHpWarps * 32, 0, st>>>(batch, h, w, nz, a16, head_w, dU, dV,    \
+      launch_pdl(head_bwd_px_kernel<4 * Q, false>, dim3(n_parts), dim3(kHpWarps * 32), 0, st, batch, h, w, nz, a16, head_w, dU, dV,    \
                                                                           out_scale, alpha, dp, dy, partials);      \
     break;
     IGM_HEAD_PX(1) IGM_HEAD_PX(2) IGM_HEAD_PX(3) IGM_HEAD_PX(4) IGM_HEAD_PX(5) IGM_HEAD_PX(6) IGM_HEAD_PX(7)
@@ -1194,7 +1209,7 @@ extern "C" int igm_cnn_head_backward_tc(int batch, int h, int w, int nz, const v
 extern "C" int igm_cnn_head_wgrad_finish(const float* partials, int n_parts, int nout, float* out, void* stream) {
   IGM_CHECK_ARG(partials && out && n_parts >= 1 && nout >= 1 && nout <= kF, IGM_ERR_BAD_ARGUMENT,
                 "igm_cnn_head_wgrad_finish: bad argument");
-  head_wgrad_finish_kernel<<<kF, kFinWarps * 32, 0, as_stream(stream)>>>(partials, n_parts, nout, out);
+  launch_pdl(head_wgrad_finish_kernel, dim3(kF), dim3(kFinWarps * 32), 0, as_stream(stream), partials, n_parts, nout, out);
   return launch_status("head_wgrad_finish_kernel");
 }
 
@@ -1203,7 +1218,7 @@ extern "C" int igm_reduce_partials(const float* partials, int n_parts, int len, 
   IGM_CHECK_ARG(partials && out && n_parts >= 1 && len >= 0 && stride >= len, IGM_ERR_BAD_ARGUMENT,
                 "igm_reduce_partials: bad argument");
   if (len == 0) return IGM_OK;
-  reduce_partials_kernel<<<grid_for((size_t)len * 32), 256, 0, as_stream(stream)>>>(partials, n_parts, len, stride,
+  launch_pdl(reduce_partials_kernel, dim3(grid_for((size_t)len * 32)), dim3(256), 0, as_stream(stream), partials, n_parts, len, stride,
                                                                                    out, accumulate);
   return launch_status("reduce_partials_kernel");
 }
@@ -1213,7 +1228,7 @@ extern "C" int igm_cnn_wgrad_finish(const float* partials, int n_parts, int cin,
   IGM_CHECK_ARG(partials && out && n_parts >= 1, IGM_ERR_BAD_ARGUMENT, "igm_cnn_wgrad_finish: bad argument");
   IGM_CHECK_ARG((cin_tensor == 16 || cin_tensor == 32) && cin >= 1 && cin <= cin_tensor, IGM_ERR_BAD_SHAPE,
                 "igm_cnn_wgrad_finish: bad channel counts");
-  wgrad_finish_kernel<<<9 * cin, kFinWarps * 32, 0, as_stream(stream)>>>(partials, n_parts, cin, cin_tensor, out);
+  launch_pdl(wgrad_finish_kernel, dim3(9 * cin), dim3(kFinWarps * 32), 0, as_stream(stream), partials, n_parts, cin, cin_tensor, out);
   return launch_status("wgrad_finish_kernel");
 }
 
@@ -1223,7 +1238,7 @@ extern "C" int igm_cnn_wgrad_finish_split(const float* partials, int n_parts, in
   // the kernel reads the 16-channel weight-gradient partials with row groups of 4 (3 x 128 x 4 x 32 floats)
   IGM_CHECK_ARG(igm_conv3x3_wgrad_partial_len(16) == (size_t)3 * 128 * 4 * kF, IGM_ERR_UNSUPPORTED,
                 "igm_cnn_wgrad_finish_split: the weight-gradient partial layout is not the one this kernel reads");
-  wgrad_finish_split_kernel<<<9 * cin, kFinWarps * 32, 0, as_stream(stream)>>>(partials, n_parts, cin, out);
+  launch_pdl(wgrad_finish_split_kernel, dim3(9 * cin), dim3(kFinWarps * 32), 0, as_stream(stream), partials, n_parts, cin, out);
   return launch_status("wgrad_finish_split_kernel");
 }
 
@@ -1256,12 +1271,12 @@ extern "C" int igm_adam_clipnorm(int n_vars, const size_t* var_offsets, float* p
   const float lr_t = (float)lr * sqrtf(1.f - b2p) / (1.f - b1p);
   cudaStream_t st = as_stream(stream);
   double* parts = norms + n_vars;
-  grad_norm_parts_kernel<<<vars.cbase[n_vars], 256, 0, st>>>(grads, vars, parts);
+  launch_pdl(grad_norm_parts_kernel, dim3(vars.cbase[n_vars]), dim3(256), 0, st, grads, vars, parts);
   int rc = launch_status("grad_norm_parts_kernel");
   if (rc) return rc;
-  grad_norm_finish_kernel<<<(n_vars + 3) / 4, 128, 0, st>>>(parts, vars, norms);
+  launch_pdl(grad_norm_finish_kernel, dim3((n_vars + 3) / 4), dim3(128), 0, st, parts, vars, norms);
   if ((rc = launch_status("grad_norm_finish_kernel"))) return rc;
-  adam_kernel<<<grid_for(vars.off[n_vars]), 256, 0, st>>>(params, grads, m, v, vars, norms, lr_t, (float)beta_1,
+  launch_pdl(adam_kernel, dim3(grid_for(vars.off[n_vars])), dim3(256), 0, st, params, grads, m, v, vars, norms, lr_t, (float)beta_1,
                                                          (float)beta_2, (float)epsilon, (float)clipnorm);
   return launch_status("adam_kernel");
 }
@@ -1280,7 +1295,7 @@ extern "C" int igm_cnn_input_gradient(int batch, int h, int w, int cin, int n_gr
   switch (n_grad) {
 #define IGM_IG(C)                                                                      \
   case C:                                                                              \
-    input_grad_kernel<C><<<grid, 256, 0, st>>>(batch, h, w, cin, d, w0, sc, out);      \
+    launch_pdl(input_grad_kernel<C>, dim3(grid), dim3(256), 0, st, batch, h, w, cin, d, w0, sc, out);      \
     break;
     IGM_IG(1) IGM_IG(2) IGM_IG(3) IGM_IG(4) IGM_IG(5) IGM_IG(6) IGM_IG(7) IGM_IG(8)
 #undef IGM_IG

@@ -162,6 +162,9 @@ __global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_kernel(const ConvA
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
+  // the next kernel may launch now: its CTAs wait for this grid to complete (grid_dep_wait)
+  grid_dep_launch();
+  grid_dep_wait();  // inputs, weights and outputs are touched only after the previous grid completed
   // packed weights -> shared memory, bias, barriers
   {
     const uint4* src = reinterpret_cast<const uint4*>(a.wpack);
@@ -432,6 +435,8 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_wgrad_kernel(const Wg
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + G::OFF_BAR + 64);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
+  grid_dep_launch();
+  grid_dep_wait();
   if (threadIdx.x == 0) {
     for (int s = 0; s < G::NST; ++s) {
       tc::mbar_init(&full[s], 2);  // the X and the G tile loads each arrive once
@@ -605,7 +610,7 @@ static int conv_launch(int B, int H, int W, const void* x, const void* wpack, co
       return IGM_ERR_CUDA;
     }
   }
-  conv3x3_kernel<C8_IN, kRows, EPI><<<grid, kConvFwdThreads, G::SMEM, st>>>(a);
+  launch_pdl(conv3x3_kernel<C8_IN, kRows, EPI>, dim3(grid), dim3(kConvFwdThreads), G::SMEM, st, a);
   return launch_status("conv3x3_kernel");
 }
 
@@ -627,7 +632,7 @@ static int wgrad_launch(int B, int H, int W, const void* x, const void* g, float
   a.g = (const __nv_bfloat16*)g;
   a.partial = partial;
   a.err = err;
-  conv3x3_wgrad_kernel<C8_IN><<<n_parts, kConvThreads, G::SMEM, st>>>(a);
+  launch_pdl(conv3x3_wgrad_kernel<C8_IN>, dim3(n_parts), dim3(kConvThreads), G::SMEM, st, a);
   return launch_status("conv3x3_wgrad_kernel");
 }
 
