@@ -242,6 +242,18 @@ class CNN:
         for l in range(self.L - 1, -1, -1):
             gl = g[cur]
             if l > 0 and param_grads:
+                # both gradients of the layer in one pass (igm_conv3x3_backward)
+                nxt = g[1 - cur]
+                rc = lib.igm_conv3x3_backward(B, h, w, _p(gl), self._wb(l), _p(acts[l - 1]), _p(nxt),
+                                              _p(buf["dbpart"]), _p(buf["wpart"]), npart, self.alpha, _p(self.err), st)
+                L.check(rc, f"igm_conv3x3_backward layer {l}")
+                L.check(lib.igm_cnn_wgrad_finish(_p(buf["wpart"]), npart, F, F, gp + 4 * self.offsets[2 * l], st),
+                        "igm_cnn_wgrad_finish")
+                L.check(lib.igm_reduce_partials(_p(buf["dbpart"]), npart, F, F, gp + 4 * self.offsets[2 * (l - 1) + 1],
+                                                0, st), "reduce db")
+                cur = 1 - cur
+                continue
+            if l > 0 and param_grads:
                 rc = lib.igm_conv3x3_wgrad(B, h, w, F, _p(acts[l - 1]), _p(gl), _p(buf["wpart"]), npart,
                                            _p(self.err), st)
                 L.check(rc, f"igm_conv3x3_wgrad layer {l}")

@@ -543,6 +543,325 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_wgrad_kernel(const Wg
 }
 
 // ---------------------------------------------------------------------------
+// fused backward of a 32 -> 32 channel layer: data gradient + weight gradient
+// ---------------------------------------------------------------------------
+// Both gradients of layer l read the gradient G_l of its pre-activation, and the
+// data gradient's LeakyReLU mask is the layer's input X = act_{l-1}, which the
+// weight gradient reads as well.  One kernel streams each 4-row tile of G_l and
+// of X once (haloed boxes, 6 rows x 130 pixels), and per tile
+//   * accumulates the data gradient in TMEM exactly as conv3x3_kernel<4, 4, dgrad>
+//     does (A = the G box, B = the flipped weights), the epilogue masking it with
+//     the X box read from shared memory (no global mask read) and storing
+//     G_{l-1}, with the per-CTA bias-gradient sums;
+//   * adds X^T G over the tile's pixels into the CTA's weight-gradient
+//     accumulators exactly as conv3x3_wgrad_kernel<4> does for its 4-row work
+//     item (A = the X box, MN-major; B = rows 1..4 of the G box from pixel 1).
+// The work items are the weight-gradient kernel's (the same 4-row blocks in the
+// same order per CTA), so the partials are those of conv3x3_wgrad_kernel<4>
+// bit for bit, and each output row's data gradient sums its taps in the order of
+// conv3x3_kernel's.  Shared memory: 2 stages x (G box + X box) + the weights;
+// TMEM: 2 x 4 x 32 data-gradient columns, then 3 x 64 weight-gradient columns.
+// A stage is released when its MMAs completed (one commit) and each of the 8
+// epilogue warps has read its mask rows (one arrival each).
+struct BwdGeom {
+  static constexpr int R = 4;                           // output rows per tile
+  static constexpr int C8 = 4;                          // 32 channels
+  static constexpr int NST = 2;
+  static constexpr int NACC = 2;                        // data-gradient accumulator sets
+  static constexpr uint32_t P = kBoxW * 16;             // chunk plane stride
+  static constexpr uint32_t RS = C8 * P;                // row stride
+  static constexpr uint32_t BOX = (R + 2) * RS;         // one haloed box
+  static constexpr uint32_t STAGE = 2 * BOX;            // G box, then X box
+  static constexpr uint32_t WBYTES = 9 * C8 * kCout * 16;
+  static constexpr uint32_t OFF_W = NST * STAGE;
+  static constexpr uint32_t OFF_BAR = OFF_W + WBYTES;
+  static constexpr uint32_t SMEM = OFF_BAR + 128 + 16 + 1024;
+  // weight gradient (conv3x3_wgrad_kernel<4>'s item geometry)
+  static constexpr int NROW = 128 / (C8 * 8);           // input rows per M = 128
+  static constexpr int JN = NROW - 2;                   // output rows per MMA (N = JN x 32)
+  static constexpr int NGRP = R / JN;
+  static constexpr int WN = JN * kCout;
+  static constexpr uint32_t DCOLS = NACC * R * kCout;   // data-gradient TMEM columns
+  static constexpr uint32_t TMEM_COLS = 512;
+  static_assert(JN == WgradGeom<4>::JN && WN == WgradGeom<4>::WN && R == WgradGeom<4>::WR,
+                "the weight-gradient partials keep conv3x3_wgrad_kernel<4>'s layout");
+  static_assert(DCOLS + 3 * WN <= TMEM_COLS, "TMEM columns");
+  static_assert(SMEM <= 232448, "shared memory");
+};
+
+struct BwdArgs {
+  int B, H, W;
+  int tiles_w, tiles_h, n_tiles;
+  const __nv_bfloat16* g;      // G_l [B][H][4][W][8]
+  const __nv_bfloat16* x;      // X = act_{l-1} [B][H][4][W][8]
+  const __nv_bfloat16* wpack;  // the layer's dgrad pack [9][4][32][8]
+  __nv_bfloat16* out;          // G_{l-1} [B][H][4][W][8]
+  float* db_partial;           // [gridDim.x][32]
+  float* w_partial;            // [gridDim.x][3][128][WN]
+  float alpha;
+  int* err;
+};
+
+__global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_bwd_kernel(const BwdArgs a) {
+  using G = BwdGeom;
+  constexpr int R = G::R, NST = G::NST, NACC = G::NACC;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
+  uint64_t* full = bars;                     // [NST] both boxes landed
+  uint64_t* empty = bars + NST;              // [NST] MMAs done + masks read
+  uint64_t* tfull = bars + 2 * NST;          // [NACC]
+  uint64_t* tempty = bars + 2 * NST + NACC;  // [NACC]
+  uint64_t* done = bars + 2 * NST + 2 * NACC;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + G::OFF_BAR + 128);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  grid_dep_launch();
+  grid_dep_wait();
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(a.wpack);
+    uint4* dst = reinterpret_cast<uint4*>(smem + G::OFF_W);
+    for (int i = threadIdx.x; i < (int)(G::WBYTES / 16); i += kConvFwdThreads) dst[i] = src[i];
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NST; ++s) {
+      tc::mbar_init(&full[s], 2);                   // the two boxes' loads
+      tc::mbar_init(&empty[s], 1 + kConvEpiWarps);  // MMA commit + one arrival per epilogue warp
+    }
+    for (int s = 0; s < NACC; ++s) {
+      tc::mbar_init(&tfull[s], 1);
+      tc::mbar_init(&tempty[s], 32 * kConvEpiWarps);
+    }
+    tc::mbar_init(done, 1);
+    tc::fence_mbar_init();
+  }
+  tc::fence_proxy_async_smem();
+  if (warp == 0) {
+    tc::tmem_alloc(tmem_slot, G::TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t sbase = tc::smem_u32(smem);
+  const int my_tiles = (int)blockIdx.x < a.n_tiles ? (a.n_tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+  if (warp == 0) {
+    // ---------------- producer ----------------
+    for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
+      const int s = it % NST, use = it / NST;
+      if (!tc::mbar_wait(&empty[s], (use & 1) ^ 1)) {
+        if (lane == 0) set_err(a.err, 21);
+        break;
+      }
+      const int txi = t % a.tiles_w, rest = t / a.tiles_w;
+      const int tyi = rest % a.tiles_h, b = rest / a.tiles_h;
+      unsigned char* st = smem + s * G::STAGE;
+      load_tile(a.g, a.H, a.W, G::C8, b, tyi * R - 1, R + 2, txi * kTW - 1, kBoxW, st, &full[s], lane);
+      load_tile(a.x, a.H, a.W, G::C8, b, tyi * R - 1, R + 2, txi * kTW - 1, kBoxW, st + G::BOX, &full[s], lane);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      constexpr uint32_t d_hi = tc::desc_hi(128), p_hi = tc::desc_hi(G::P);
+      constexpr uint32_t wg_idesc = tc::make_idesc_bf16(128, G::WN, true, true);
+      const uint32_t w_lo = tc::desc_lo(sbase + G::OFF_W, kWRowsN * 16);
+      const uint32_t wtm = tmem + G::DCOLS;  // weight-gradient accumulators [3][WN]
+      bool ok = true;
+      for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
+        const int s = it % NST, use = it / NST, acc = it % NACC, ause = it / NACC;
+        if (!tc::mbar_wait(&tempty[acc], (ause & 1) ^ 1) || !tc::mbar_wait(&full[s], use & 1)) {
+          set_err(a.err, 22);
+          ok = false;
+          break;
+        }
+        tc::tc_fence_after();
+        const uint32_t gbox = sbase + s * G::STAGE, xbox = gbox + G::BOX;
+        // data gradient: conv3x3_kernel's sliding-window accumulation over the G box
+        const uint32_t in_lo = tc::desc_lo(gbox, G::P);
+        const uint32_t dset = tmem + (uint32_t)(acc * R * kCout);
+#pragma unroll
+        for (int i = 0; i < R + 2; ++i) {
+          const int dlo = i - (R - 1) > 0 ? i - (R - 1) : 0;
+          const int dhi = i < 2 ? i : 2;
+          const int ndy = dhi - dlo + 1;
+          const uint32_t dcol = dset + (uint32_t)(kCout * (R - 1 - i + dlo));
+#pragma unroll
+          for (int dx = 0; dx < 3; ++dx) {
+#pragma unroll
+            for (int ks = 0; ks < G::C8 / 2; ++ks) {
+              const uint32_t aoff = (i * G::RS + dx * 16 + ks * 2 * G::P) >> 4;
+              const uint32_t boff = (((dx * G::C8 + ks * 2) * kWRowsN + dlo * kCout) * 16) >> 4;
+              const uint64_t ad = tc::desc_join(in_lo + aoff, d_hi);
+              if (dx == 0 && ks == 0 && dlo == 0) {
+                tc::mma_bf16(dcol, ad, tc::desc_join(w_lo + boff, d_hi), tc::make_idesc_bf16(128, kCout, false, false),
+                             0u);
+                if (ndy > 1)
+                  tc::mma_bf16(dcol + kCout, ad, tc::desc_join(w_lo + boff + ((kCout * 16) >> 4), d_hi),
+                               tc::make_idesc_bf16(128, kCout * (ndy - 1), false, false), 1u);
+              } else {
+                tc::mma_bf16(dcol, ad, tc::desc_join(w_lo + boff, d_hi),
+                             tc::make_idesc_bf16(128, kCout * ndy, false, false), 1u);
+              }
+            }
+          }
+        }
+        // weight gradient: conv3x3_wgrad_kernel<4>'s item over the X box and rows 1..R of the G box
+        const uint32_t x_lo = tc::desc_lo(xbox, 128), g_lo = tc::desc_lo(gbox + G::RS + 16, 128);
+#pragma unroll 1
+        for (int q = 0; q < G::NGRP; ++q) {
+          const uint32_t xq = x_lo + ((q * G::JN * G::RS) >> 4), gq = g_lo + ((q * G::JN * G::RS) >> 4);
+          const uint32_t acc0 = (it > 0 || q > 0) ? 1u : 0u;
+#pragma unroll
+          for (int dx = 0; dx < 3; ++dx) {
+#pragma unroll
+            for (int ks = 0; ks < kTW / 16; ++ks) {
+              const uint64_t ad = tc::desc_join(xq + ((dx * 16 + ks * 256) >> 4), p_hi);
+              const uint64_t bd = tc::desc_join(gq + ((ks * 256) >> 4), p_hi);
+              tc::mma_bf16(wtm + dx * G::WN, ad, bd, wg_idesc, ks > 0 ? 1u : acc0);
+            }
+          }
+        }
+        tc::mma_commit(&empty[s]);
+        tc::mma_commit(&tfull[acc]);
+      }
+      if (ok) tc::mma_commit(done);
+    }
+  } else {
+    // ---------------- epilogue (warps 2 .. 9) ----------------
+    constexpr int RH = R / 2;
+    const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const int r0 = half * RH;
+    const int p = q * 32 + lane;
+    float dbacc[kCout];
+#pragma unroll
+    for (int c = 0; c < kCout; ++c) dbacc[c] = 0.f;
+    bool ok = true;
+    for (int it = 0, t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
+      const int s = it % NST, use = it / NST, acc = it % NACC, ause = it / NACC;
+      const int txi = t % a.tiles_w, rest = t / a.tiles_w;
+      const int tyi = rest % a.tiles_h, b = rest / a.tiles_h;
+      const int x = txi * kTW + p;
+      if (!tc::mbar_wait(&full[s], use & 1)) {
+        set_err(a.err, 23);
+        ok = false;
+        break;
+      }
+      // this warp's mask rows from the X box (row r of the tile = box row r + 1, pixel p = box pixel p + 1)
+      uint4 mk[RH][4];
+      const unsigned char* xb = smem + s * G::STAGE + G::BOX;
+#pragma unroll
+      for (int rr = 0; rr < RH; ++rr)
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch)
+          mk[rr][ch] = *reinterpret_cast<const uint4*>(xb + (r0 + rr + 1) * G::RS + ch * G::P + (p + 1) * 16);
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&empty[s]);
+      if (!tc::mbar_wait(&tfull[acc], ause & 1)) {
+        set_err(a.err, 24);
+        ok = false;
+        break;
+      }
+      tc::tc_fence_after();
+#pragma unroll
+      for (int rr = 0; rr < RH; ++rr) {
+        const int r = r0 + rr;
+        uint32_t v[32];
+        tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((acc * R + (R - 1 - r)) * kCout), v);
+        tc::tmem_wait_ld();
+        const int y = tyi * R + r;
+        if (y < a.H && x < a.W) {
+          const size_t pix = (((size_t)b * a.H + y) * 4) * a.W + x;
+          float f[kCout];
+#pragma unroll
+          for (int c = 0; c < kCout; ++c) f[c] = __uint_as_float(v[c]);
+#pragma unroll
+          for (int ch = 0; ch < 4; ++ch) {
+            const uint32_t mw[4] = {mk[rr][ch].x, mk[rr][ch].y, mk[rr][ch].z, mk[rr][ch].w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&mw[e]);
+              const float lo = __low2float(h), hi = __high2float(h);
+              const int c = ch * 8 + e * 2;
+              f[c] *= lo > 0.f ? 1.f : a.alpha;
+              f[c + 1] *= hi > 0.f ? 1.f : a.alpha;
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < kCout; ++c) dbacc[c] += f[c];
+          uint4* o = reinterpret_cast<uint4*>(a.out);
+#pragma unroll
+          for (int ch = 0; ch < 4; ++ch) {
+            uint4 w;
+            w.x = pack_bf16x2(f[ch * 8 + 0], f[ch * 8 + 1]);
+            w.y = pack_bf16x2(f[ch * 8 + 2], f[ch * 8 + 3]);
+            w.z = pack_bf16x2(f[ch * 8 + 4], f[ch * 8 + 5]);
+            w.w = pack_bf16x2(f[ch * 8 + 6], f[ch * 8 + 7]);
+            o[pix + (size_t)ch * a.W] = w;
+          }
+        }
+      }
+      tc::tc_fence_before();
+      tc::mbar_arrive(&tempty[acc]);
+    }
+    // weight-gradient accumulators -> this CTA's partials: warp (q, half) takes lane quarter q and
+    // the half-th 32 of each kernel column's WN = 64 accumulator columns
+    if (ok && my_tiles > 0) {
+      ok = tc::mbar_wait(done, 0);
+      if (!ok) set_err(a.err, 25);
+      tc::tc_fence_after();
+    }
+    const int m = q * 32 + lane;
+#pragma unroll 1
+    for (int dx = 0; dx < 3; ++dx) {
+      const int cb = half * 32;
+      uint32_t v[32];
+      tc::tmem_ld32(tmem + G::DCOLS + ((uint32_t)(q * 32) << 16) + (uint32_t)(dx * G::WN + cb), v);
+      tc::tmem_wait_ld();
+      float4* dst = reinterpret_cast<float4*>(a.w_partial + (((size_t)blockIdx.x * 3 + dx) * 128 + m) * G::WN + cb);
+#pragma unroll
+      for (int c = 0; c < 32; c += 4) {
+        const bool z = my_tiles == 0 || !ok;
+        float4 f4;
+        f4.x = z ? 0.f : __uint_as_float(v[c + 0]);
+        f4.y = z ? 0.f : __uint_as_float(v[c + 1]);
+        f4.z = z ? 0.f : __uint_as_float(v[c + 2]);
+        f4.w = z ? 0.f : __uint_as_float(v[c + 3]);
+        dst[c / 4] = f4;
+      }
+    }
+    // bias-gradient partial sums: warp reduction, then a fixed-order CTA sum below
+#pragma unroll
+    for (int c = 0; c < kCout; ++c) {
+      float v = dbacc[c];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      dbacc[c] = v;
+    }
+    // every MMA of this CTA has completed (the last tfull / done wait), so the weight area is free
+    float* red = reinterpret_cast<float*>(smem + G::OFF_W);
+    if (lane == 0) {
+#pragma unroll
+      for (int c = 0; c < kCout; ++c) red[(warp - 2) * kCout + c] = dbacc[c];
+    }
+    tc::tc_fence_before();
+  }
+  __syncthreads();
+  if (threadIdx.x < kCout) {
+    const float* red = reinterpret_cast<const float*>(smem + G::OFF_W);
+    float sum = red[threadIdx.x];
+#pragma unroll
+    for (int w = 1; w < kConvEpiWarps; ++w) sum += red[w * kCout + threadIdx.x];  // fixed order
+    a.db_partial[(size_t)blockIdx.x * kCout + threadIdx.x] = sum;
+  }
+  if (warp == 0) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem, G::TMEM_COLS);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 
@@ -670,6 +989,36 @@ extern "C" int igm_conv3x3_wgrad(int batch, int height, int width, int cin, cons
   cudaStream_t st = as_stream(stream);
   if (cin == 16) return wgrad_launch<2>(batch, height, width, x, g, partials, n_parts, err, st);
   return wgrad_launch<4>(batch, height, width, x, g, partials, n_parts, err, st);
+}
+
+extern "C" int igm_conv3x3_backward(int batch, int height, int width, const void* g, const void* wpack_bwd,
+                                    const void* x, void* g_prev, float* db_partials, float* w_partials, int n_parts,
+                                    float alpha, int* err, void* stream) {
+  using G = BwdGeom;
+  IGM_CHECK_ARG(batch >= 1 && height >= 1 && width >= 1 && batch <= 65535, IGM_ERR_BAD_SHAPE,
+                "igm_conv3x3_backward: bad shape %dx%dx%d", batch, height, width);
+  IGM_CHECK_ARG(g && wpack_bwd && x && g_prev && db_partials && w_partials && n_parts >= 1, IGM_ERR_BAD_ARGUMENT,
+                "igm_conv3x3_backward: NULL argument");
+  IGM_CHECK_ARG(((uintptr_t)g & 15) == 0 && ((uintptr_t)x & 15) == 0 && ((uintptr_t)g_prev & 15) == 0,
+                IGM_ERR_BAD_ARGUMENT, "igm_conv3x3_backward: activations must be 16-byte aligned");
+  static bool configured = false;
+  int rc = set_smem(conv3x3_bwd_kernel, G::SMEM, &configured);
+  if (rc) return rc;
+  BwdArgs a{};
+  a.B = batch; a.H = height; a.W = width;
+  a.tiles_w = (width + kTW - 1) / kTW;
+  a.tiles_h = (height + G::R - 1) / G::R;
+  a.n_tiles = batch * a.tiles_w * a.tiles_h;
+  a.g = (const __nv_bfloat16*)g;
+  a.x = (const __nv_bfloat16*)x;
+  a.wpack = (const __nv_bfloat16*)wpack_bwd;
+  a.out = (__nv_bfloat16*)g_prev;
+  a.db_partial = db_partials;
+  a.w_partial = w_partials;
+  a.alpha = alpha;
+  a.err = err;
+  launch_pdl(conv3x3_bwd_kernel, dim3(n_parts), dim3(kConvFwdThreads), G::SMEM, as_stream(stream), a);
+  return launch_status("conv3x3_bwd_kernel");
 }
 
 extern "C" size_t igm_conv3x3_wgrad_partial_len(int cin) {

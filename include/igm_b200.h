@@ -507,6 +507,20 @@ IGM_API int igm_conv3x3(int mode, int batch, int height, int width, int cin, con
 IGM_API int igm_conv3x3_wgrad(int batch, int height, int width, int cin, const void* x, const void* g,
                               float* partials, int n_parts, int* err, void* stream);
 IGM_API size_t igm_conv3x3_wgrad_partial_len(int cin);
+/* Both gradients of a 32 -> 32 channel layer in one pass over its inputs
+ * (replaces igm_conv3x3(IGM_CONV_DGRAD) + igm_conv3x3_wgrad for the hidden
+ * layers; the Keras GradientTape of emulate.py:252 through Conv2D(3x3) +
+ * LeakyReLU): from g, the gradient w.r.t. the layer's pre-activation, the
+ * layer's dgrad pack and x, the layer's input activation (which is also the
+ * LeakyReLU mask of the data gradient):
+ *   g_prev      = (dL/dx) * (x > 0 ? 1 : alpha), as IGM_CONV_DGRAD writes it;
+ *   db_partials = per-CTA sums of g_prev over the pixels, [n_parts][32];
+ *   w_partials  = the igm_conv3x3_wgrad(cin 32) partials of (x, g), [n_parts]
+ *                 x igm_conv3x3_wgrad_partial_len(32) floats, for igm_cnn_wgrad_finish.
+ * Every slot of both partial buffers is written.  err as for igm_conv3x3. */
+IGM_API int igm_conv3x3_backward(int batch, int height, int width, const void* g, const void* wpack_bwd,
+                                 const void* x, void* g_prev, float* db_partials, float* w_partials, int n_parts,
+                                 float alpha, int* err, void* stream);
 IGM_API int igm_conv_sm_count(void);
 
 IGM_API size_t igm_cnn_param_count(int nb_layers, int cin, int nout);

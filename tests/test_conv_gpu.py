@@ -127,3 +127,50 @@ def test_conv_wgrad(B, H, W, cin):
     L.check(L.lib().igm_cnn_wgrad_finish(part.data_ptr(), npart, cin_real, cin, out.data_ptr(), L.stream_ptr()))
     assert int(err.item()) == 0
     np.testing.assert_allclose(out.cpu().numpy(), ref_k.numpy(), rtol=1e-4, atol=1e-4 * float(ref_k.abs().max()))
+
+
+@pytest.mark.parametrize("B,H,W,npart", [(1, 8, 128, 148), (2, 11, 173, 37), (1, 5, 1000, 148), (1, 1000, 1000, 148),
+                                         (3, 4, 40, 148), (1, 2, 7, 5)])
+def test_conv_backward_fused(B, H, W, npart):
+    """igm_conv3x3_backward (both gradients of a 32-channel layer in one pass):
+    the data gradient bit for bit as igm_conv3x3(IGM_CONV_DGRAD) writes it, the
+    weight-gradient partials bit for bit as igm_conv3x3_wgrad's (the same work
+    items in the same order per CTA), the bias gradient to the rounding of its
+    summation order, and both against torch-CPU float32."""
+    g = torch.Generator().manual_seed(B * 1000 + H + W)
+    gout = bf(torch.randn(B, 32, H, W, generator=g))
+    aprev = bf(torch.randn(B, 32, H, W, generator=g))
+    w = torch.randn(3, 3, 32, 32, generator=g) * (1.0 / np.sqrt(288))
+    lib, st = L.lib(), L.stream_ptr()
+    gd = to_rc(gout).to(torch.bfloat16).cuda()
+    ad = to_rc(aprev).to(torch.bfloat16).cuda()
+    wd = pack_bwd(w).cuda()
+    plen = int(lib.igm_conv3x3_wgrad_partial_len(32))
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    y1 = torch.empty((B, H, 4, W, 8), dtype=torch.bfloat16, device="cuda")
+    db1 = torch.zeros((npart, 32), device="cuda")
+    p1 = torch.full((npart, plen), float("nan"), device="cuda")
+    L.check(lib.igm_conv3x3(1, B, H, W, 32, gd.data_ptr(), wd.data_ptr(), None, ad.data_ptr(), y1.data_ptr(),
+                            db1.data_ptr(), npart, 0.01, err.data_ptr(), st))
+    L.check(lib.igm_conv3x3_wgrad(B, H, W, 32, ad.data_ptr(), gd.data_ptr(), p1.data_ptr(), npart, err.data_ptr(), st))
+    y2 = torch.empty_like(y1)
+    db2 = torch.full((npart, 32), float("nan"), device="cuda")
+    p2 = torch.full((npart, plen), float("nan"), device="cuda")
+    L.check(lib.igm_conv3x3_backward(B, H, W, gd.data_ptr(), wd.data_ptr(), ad.data_ptr(), y2.data_ptr(),
+                                     db2.data_ptr(), p2.data_ptr(), npart, 0.01, err.data_ptr(), st))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert torch.equal(y1, y2)
+    assert torch.equal(p1, p2)
+    assert bool(torch.isfinite(db2).all())
+    s1, s2 = db1.sum(0).double(), db2.sum(0).double()
+    assert float((s1 - s2).abs().max()) <= 1e-5 * float(s1.abs().max()) + 1e-6
+    # against torch
+    dx = torch.nn.grad.conv2d_input((B, 32, H, W), bf(keras_to_torch(w)), gout, padding=1)
+    ref = dx * torch.where(aprev > 0, 1.0, 0.01)
+    np.testing.assert_allclose(from_rc(y2.float().cpu()).numpy(), ref.numpy(), rtol=8e-3,
+                               atol=2e-3 * float(ref.abs().max()))
+    ref_w = torch.nn.grad.conv2d_weight(aprev, (32, 32, 3, 3), gout, padding=1).permute(2, 3, 1, 0).contiguous()
+    out = torch.empty((3, 3, 32, 32), device="cuda")
+    L.check(lib.igm_cnn_wgrad_finish(p2.data_ptr(), npart, 32, 32, out.data_ptr(), st))
+    np.testing.assert_allclose(out.cpu().numpy(), ref_w.numpy(), rtol=1e-4, atol=1e-4 * float(ref_w.abs().max()))
