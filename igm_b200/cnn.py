@@ -63,7 +63,8 @@ class CNN:
         self.wpack_b = torch.zeros(max(self.L - 1, 1) * 9 * 4 * F * 8, dtype=torch.bfloat16, device=self.device)
         self.init_weights(init, seed)
         self._bufs = {}
-        self.event_hook = None  # list: (start, end) CUDA events of each 32-channel forward conv launch
+        self.event_hook = None  # list: (start, end) CUDA events of each inference's 32-channel conv stack
+        self._epoch = 0  # tile-flag epoch of the conv stack launches
         self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.n_sm = int(lib.igm_conv_sm_count())
 
@@ -144,6 +145,8 @@ class CNN:
                 b["dbpart"] = torch.zeros((npart, F), dtype=torch.float32, device=d)
                 hl = int(L.lib().igm_cnn_head_partial_len(self.nz))
                 b["hpart"] = torch.empty((2 * npart, hl), dtype=torch.float32, device=d)
+            nst = max(self.L - 1, 1)
+            b["flags"] = torch.zeros(int(L.lib().igm_conv3x3_stack_flags_len(B, h, w, nst)), dtype=torch.int32, device=d)
             self._bufs[key] = b
         return b
 
@@ -173,20 +176,25 @@ class CNN:
                              self.alpha, _p(self.err), st)
         L.check(rc, "igm_conv3x3 layer 0")
         x = acts[0]
-        cin_t = F
-        hook = self.event_hook if (self.event_hook is not None and not keep_acts) else None
-        for l in range(1, self.L):
-            y = acts[l] if keep_acts else acts[l % 2]
-            if hook is not None and l > 0:
+        if self.L > 1:
+            # the 32-channel layers 1 .. L-1 in one launch (igm_conv3x3_stack)
+            n = self.L - 1
+            ys = [acts[l] if keep_acts else acts[l % 2] for l in range(1, self.L)]
+            outs = (C.c_void_p * n)(*[_p(y) for y in ys])
+            wps = (C.c_void_p * n)(*[self._wf(l) for l in range(1, self.L)])
+            bs = (C.c_void_p * n)(*[self._b(l) for l in range(1, self.L)])
+            self._epoch = self._epoch % 2147483646 + 1
+            hook = self.event_hook if (self.event_hook is not None and not keep_acts) else None
+            if hook is not None:
                 ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                 ev[0].record()
-            rc = lib.igm_conv3x3(0, B, h, w, cin_t, _p(x), self._wf(l), self._b(l), None, _p(y), None, 0,
-                                 self.alpha, _p(self.err), st)
-            L.check(rc, f"igm_conv3x3 layer {l}")
-            if hook is not None and l > 0:
+            rc = lib.igm_conv3x3_stack(B, h, w, n, _p(x), outs, wps, bs, _p(buf["flags"]), self._epoch, self.alpha,
+                                       _p(self.err), st)
+            L.check(rc, "igm_conv3x3_stack")
+            if hook is not None:
                 ev[1].record()
                 hook.append(ev)
-            x, cin_t = y, F
+            x = ys[-1]
         hw = self.params.data_ptr() + 4 * self.offsets[2 * self.L]
         hb = self.params.data_ptr() + 4 * self.offsets[2 * self.L + 1]
         rc = lib.igm_cnn_head_forward(B, h, w, self.nz, _p(x), hw, hb, self.out_scale, _p(buf["U"]), _p(buf["V"]),

@@ -374,6 +374,250 @@ __global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_kernel(const ConvA
 }
 
 // ---------------------------------------------------------------------------
+// forward of a stack of 32 -> 32 channel layers in one persistent launch
+// ---------------------------------------------------------------------------
+// conv3x3_kernel<4, R, fwd> per layer, for layers k = 0 .. nlayers-1 of a stack
+// (layer k reads the output of layer k - 1), with the tile pipeline running on
+// across the layer boundaries: each CTA takes the same tiles in every layer, and
+// before it loads tile t of layer k its producer waits until the (up to nine)
+// tiles of layer k - 1 around t are stored -- a per-tile flag set to this
+// launch's epoch.  Those are the only tiles whose outputs tile t reads, and the
+// only tiles of layer k - 1 that read the rows tile t overwrites when layers
+// alternate between two buffers, so the wait also orders that reuse.  A CTA's
+// own earlier tiles never wait on its later ones, so with every CTA resident (a
+// cooperative launch) all waits end; each is bounded all the same.  Each
+// layer's weights are copied into one of two shared-memory buffers on the
+// barrier of that layer's first tile.
+constexpr int kStackMax = 16;
+
+struct StackArgs {
+  int B, H, W;
+  int tiles_w, tiles_h, n_tiles;  // per layer
+  int nlayers;
+  const __nv_bfloat16* in;        // input of layer 0 [B][H][4][W][8]
+  __nv_bfloat16* out[kStackMax];  // output of layer k
+  const __nv_bfloat16* wpack[kStackMax];
+  const float* bias[kStackMax];
+  int* flags;                     // [nlayers][n_tiles]
+  int epoch;
+  float alpha;
+  int* err;
+};
+
+template <int R>
+__global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_stack_kernel(const StackArgs a) {
+  using G = ConvGeom<4, R>;
+  constexpr int NST = G::NST, NACC = G::NACC;
+  constexpr uint32_t OFF_BAR = G::OFF_W + 2 * G::WBYTES;  // two weight buffers
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + OFF_BAR);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + NST;
+  uint64_t* tfull = bars + 2 * NST;
+  uint64_t* tempty = bars + 2 * NST + NACC;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + OFF_BAR + 128);
+  volatile int* abort_epi = reinterpret_cast<volatile int*>(smem + OFF_BAR + 132);  // an epilogue wait gave up
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int per = a.n_tiles;
+
+  if (threadIdx.x == 0) {
+    *abort_epi = 0;
+    for (int s = 0; s < NST; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    for (int s = 0; s < NACC; ++s) {
+      tc::mbar_init(&tfull[s], 1);
+      tc::mbar_init(&tempty[s], 32 * kConvEpiWarps);
+    }
+    tc::fence_mbar_init();
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tmem_slot, G::TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t sbase = tc::smem_u32(smem);
+
+  if (warp == 0) {
+    // ---------------- producer ----------------
+    int it = 0;
+    bool ok = true;
+    for (int k = 0; k < a.nlayers && ok; ++k) {
+      const __nv_bfloat16* src = k == 0 ? a.in : a.out[k - 1];
+      for (int t = blockIdx.x; t < per; t += gridDim.x, ++it) {
+        const int s = it % NST, use = it / NST;
+        if (!tc::mbar_wait(&empty[s], (use & 1) ^ 1)) {
+          if (lane == 0) set_err(a.err, 31);
+          ok = false;
+          break;
+        }
+        const int txi = t % a.tiles_w, rest = t / a.tiles_w;
+        const int tyi = rest % a.tiles_h, b = rest / a.tiles_h;
+        if (k > 0) {
+          // the tiles of layer k - 1 whose outputs this tile reads
+          bool got = true;
+          if (lane < 9) {
+            const int ny = tyi + lane / 3 - 1, nx = txi + lane % 3 - 1;
+            if (ny >= 0 && ny < a.tiles_h && nx >= 0 && nx < a.tiles_w) {
+              const int* f = a.flags + (size_t)(k - 1) * per + ((size_t)b * a.tiles_h + ny) * a.tiles_w + nx;
+              uint32_t n = 0;
+              while (tc::ld_acquire_gpu(f) != a.epoch) {
+                if (++n > (1u << 22)) {
+                  got = false;
+                  break;
+                }
+                __nanosleep(64);
+              }
+            }
+          }
+          if (!__all_sync(0xffffffffu, got)) {
+            if (lane == 0) set_err(a.err, 32);
+            ok = false;
+            break;
+          }
+          tc::fence_proxy_async_global();  // the acquired data is read next by the bulk-copy (async) proxy
+        }
+        unsigned char* st = smem + s * G::STAGE;
+        if (t == (int)blockIdx.x && lane == 0) {
+          // this layer's weights, on the barrier of its first tile (their buffer's last reader, layer
+          // k - 2, completed: the commit that released this stage covers every earlier MMA)
+          tc::mbar_expect_tx_only(&full[s], G::WBYTES);
+          tc::bulk_load(smem + G::OFF_W + (k & 1) * G::WBYTES, a.wpack[k], G::WBYTES, &full[s]);
+        }
+        __syncwarp();
+        load_tile(src, a.H, a.W, 4, b, tyi * R - 1, R + 2, txi * kTW - 1, kBoxW, st, &full[s], lane);
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      constexpr uint32_t a_hi = tc::desc_hi(128), b_hi = tc::desc_hi(128);
+      int it = 0;
+      bool ok = true;
+      for (int k = 0; k < a.nlayers && ok; ++k) {
+        const uint32_t w_lo = tc::desc_lo(sbase + G::OFF_W + (k & 1) * G::WBYTES, kWRowsN * 16);
+        for (int t = blockIdx.x; t < per; t += gridDim.x, ++it) {
+          const int s = it % NST, use = it / NST, acc = it % NACC, ause = it / NACC;
+          if (!tc::mbar_wait(&tempty[acc], (ause & 1) ^ 1) || !tc::mbar_wait(&full[s], use & 1)) {
+            set_err(a.err, 33);
+            ok = false;
+            break;
+          }
+          tc::tc_fence_after();
+          const uint32_t in_lo = tc::desc_lo(sbase + s * G::STAGE, G::P);
+          const uint32_t dset = tmem + (uint32_t)(acc * R * kCout);
+#pragma unroll
+          for (int i = 0; i < R + 2; ++i) {
+            const int dlo = i - (R - 1) > 0 ? i - (R - 1) : 0;
+            const int dhi = i < 2 ? i : 2;
+            const int ndy = dhi - dlo + 1;
+            const uint32_t dcol = dset + (uint32_t)(kCout * (R - 1 - i + dlo));
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) {
+#pragma unroll
+              for (int ks = 0; ks < 2; ++ks) {
+                const uint32_t aoff = (i * G::RS + dx * 16 + ks * 2 * G::P) >> 4;
+                const uint32_t boff = (((dx * 4 + ks * 2) * kWRowsN + dlo * kCout) * 16) >> 4;
+                const uint64_t ad = tc::desc_join(in_lo + aoff, a_hi);
+                if (dx == 0 && ks == 0 && dlo == 0) {
+                  tc::mma_bf16(dcol, ad, tc::desc_join(w_lo + boff, b_hi),
+                               tc::make_idesc_bf16(128, kCout, false, false), 0u);
+                  if (ndy > 1)
+                    tc::mma_bf16(dcol + kCout, ad, tc::desc_join(w_lo + boff + ((kCout * 16) >> 4), b_hi),
+                                 tc::make_idesc_bf16(128, kCout * (ndy - 1), false, false), 1u);
+                } else {
+                  tc::mma_bf16(dcol, ad, tc::desc_join(w_lo + boff, b_hi),
+                               tc::make_idesc_bf16(128, kCout * ndy, false, false), 1u);
+                }
+              }
+            }
+          }
+          tc::mma_commit(&empty[s]);
+          tc::mma_commit(&tfull[acc]);
+        }
+      }
+    }
+  } else {
+    // ---------------- epilogue (warps 2 .. 9) ----------------
+    constexpr int RH = R / 2;
+    const int q = warp & 3;
+    const int r0 = ((warp - 2) >> 2) * RH;
+    const int p = q * 32 + lane;
+    int it = 0;
+    bool ok = true;
+    for (int k = 0; k < a.nlayers && ok; ++k) {
+      float bias[kCout];
+#pragma unroll
+      for (int c = 0; c < kCout; ++c) bias[c] = __ldg(a.bias[k] + c);
+      uint4* o = reinterpret_cast<uint4*>(a.out[k]);
+      for (int t = blockIdx.x; t < per; t += gridDim.x, ++it) {
+        const int use = it / NACC, acc = it % NACC;
+        const int txi = t % a.tiles_w, rest = t / a.tiles_w;
+        const int tyi = rest % a.tiles_h, b = rest / a.tiles_h;
+        const int x = txi * kTW + p;
+        if (!tc::mbar_wait(&tfull[acc], use & 1)) {
+          set_err(a.err, 34);
+          ok = false;
+        }
+        tc::tc_fence_after();
+#pragma unroll
+        for (int rr = 0; rr < RH && ok; ++rr) {
+          const int r = r0 + rr;
+          uint32_t v[32];
+          tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((acc * R + (R - 1 - r)) * kCout), v);
+          tc::tmem_wait_ld();
+          const int y = tyi * R + r;
+          if (y < a.H && x < a.W) {
+            const size_t pix = (((size_t)b * a.H + y) * 4) * a.W + x;
+            float f[kCout];
+#pragma unroll
+            for (int c = 0; c < kCout; ++c) {
+              const float z = __uint_as_float(v[c]) + bias[c];
+              f[c] = z > 0.f ? z : a.alpha * z;
+            }
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch) {
+              uint4 w;
+              w.x = pack_bf16x2(f[ch * 8 + 0], f[ch * 8 + 1]);
+              w.y = pack_bf16x2(f[ch * 8 + 2], f[ch * 8 + 3]);
+              w.z = pack_bf16x2(f[ch * 8 + 4], f[ch * 8 + 5]);
+              w.w = pack_bf16x2(f[ch * 8 + 6], f[ch * 8 + 7]);
+              o[pix + (size_t)ch * a.W] = w;
+            }
+          }
+        }
+        tc::tc_fence_before();
+        tc::mbar_arrive(&tempty[acc]);
+        // the tile's output is complete once all eight epilogue warps stored their rows: publish it;
+        // the eight warps leave together when any of them gave up a wait (the shared abort flag,
+        // written before the barrier, read after it), so none is left alone at the next barrier
+        tc::fence_proxy_async_global();
+        if (!ok) *abort_epi = 1;
+        asm volatile("bar.sync 1, %0;\n" ::"n"(32 * kConvEpiWarps) : "memory");
+        if (*abort_epi) {
+          ok = false;
+          break;
+        }
+        if (warp == 2 && lane == 0) {
+          __threadfence();
+          tc::st_release_gpu(a.flags + (size_t)k * per + t, a.epoch);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem, G::TMEM_COLS);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // weight gradient
 // ---------------------------------------------------------------------------
 struct WgradArgs {
@@ -1019,6 +1263,61 @@ extern "C" int igm_conv3x3_backward(int batch, int height, int width, const void
   a.err = err;
   launch_pdl(conv3x3_bwd_kernel, dim3(n_parts), dim3(kConvFwdThreads), G::SMEM, as_stream(stream), a);
   return launch_status("conv3x3_bwd_kernel");
+}
+
+extern "C" int igm_conv3x3_stack(int batch, int height, int width, int nlayers, const void* x, void* const* outs,
+                                 const void* const* wpacks, const float* const* biases, int* flags, int epoch,
+                                 float alpha, int* err, void* stream) {
+  constexpr int R = kRows;
+  using G = ConvGeom<4, R>;
+  constexpr uint32_t SMEM = G::OFF_W + 2 * G::WBYTES + 128 + 16 + 1024;
+  static_assert(SMEM <= 232448, "shared memory");
+  IGM_CHECK_ARG(batch >= 1 && height >= 1 && width >= 1 && batch <= 65535, IGM_ERR_BAD_SHAPE,
+                "igm_conv3x3_stack: bad shape %dx%dx%d", batch, height, width);
+  IGM_CHECK_ARG(nlayers >= 1 && nlayers <= kStackMax, IGM_ERR_BAD_SHAPE, "igm_conv3x3_stack: 1 .. %d layers",
+                kStackMax);
+  IGM_CHECK_ARG(x && outs && wpacks && biases && flags && epoch != 0, IGM_ERR_BAD_ARGUMENT,
+                "igm_conv3x3_stack: NULL argument or zero epoch");
+  StackArgs a{};
+  a.B = batch; a.H = height; a.W = width;
+  a.tiles_w = (width + kTW - 1) / kTW;
+  a.tiles_h = (height + R - 1) / R;
+  a.n_tiles = batch * a.tiles_w * a.tiles_h;
+  a.nlayers = nlayers;
+  a.in = (const __nv_bfloat16*)x;
+  IGM_CHECK_ARG(((uintptr_t)x & 15) == 0, IGM_ERR_BAD_ARGUMENT, "igm_conv3x3_stack: activations must be 16-byte aligned");
+  for (int k = 0; k < nlayers; ++k) {
+    IGM_CHECK_ARG(outs[k] && wpacks[k] && biases[k] && ((uintptr_t)outs[k] & 15) == 0 && ((uintptr_t)wpacks[k] & 15) == 0,
+                  IGM_ERR_BAD_ARGUMENT, "igm_conv3x3_stack: layer %d: NULL or unaligned pointer", k);
+    a.out[k] = (__nv_bfloat16*)outs[k];
+    a.wpack[k] = (const __nv_bfloat16*)wpacks[k];
+    a.bias[k] = biases[k];
+  }
+  a.flags = flags;
+  a.epoch = epoch;
+  a.alpha = alpha;
+  a.err = err;
+  static bool configured = false;
+  int rc = set_smem(conv3x3_stack_kernel<R>, SMEM, &configured);
+  if (rc) return rc;
+  const int grid = a.n_tiles < sm_count() ? a.n_tiles : sm_count();
+  // cooperative: every CTA resident at once, which the inter-CTA tile flags rely on
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kConvFwdThreads);
+  cfg.dynamicSmemBytes = SMEM;
+  cfg.stream = as_stream(stream);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, conv3x3_stack_kernel<R>, a);
+  return launch_status("conv3x3_stack_kernel");
+}
+
+extern "C" size_t igm_conv3x3_stack_flags_len(int batch, int height, int width, int nlayers) {
+  return (size_t)nlayers * batch * ((width + kTW - 1) / kTW) * ((height + kRows - 1) / kRows);
 }
 
 extern "C" size_t igm_conv3x3_wgrad_partial_len(int cin) {

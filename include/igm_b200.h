@@ -507,6 +507,19 @@ IGM_API int igm_conv3x3(int mode, int batch, int height, int width, int cin, con
 IGM_API int igm_conv3x3_wgrad(int batch, int height, int width, int cin, const void* x, const void* g,
                               float* partials, int n_parts, int* err, void* stream);
 IGM_API size_t igm_conv3x3_wgrad_partial_len(int cin);
+/* nlayers (1..16) forward 3x3 convolutions of 32 -> 32 channels in one launch,
+ * as nlayers calls of igm_conv3x3(IGM_CONV_FWD_LEAKY) would compute them: layer
+ * k reads x (k = 0) or outs[k-1] and writes outs[k] = LeakyReLU(conv(., wpacks[k])
+ * + biases[k]); outs may alternate between two buffers (outs[k] == outs[k-2]).
+ * The tiles of a layer start as soon as the tiles of the previous layer they
+ * read are stored (a cooperative launch with per-tile flags).  flags: a device
+ * int buffer of igm_conv3x3_stack_flags_len ints holding no value equal to
+ * epoch (a zeroed buffer and a per-call counter from 1 serve).  outs, wpacks,
+ * biases: host arrays of nlayers device pointers. */
+IGM_API int igm_conv3x3_stack(int batch, int height, int width, int nlayers, const void* x, void* const* outs,
+                              const void* const* wpacks, const float* const* biases, int* flags, int epoch,
+                              float alpha, int* err, void* stream);
+IGM_API size_t igm_conv3x3_stack_flags_len(int batch, int height, int width, int nlayers);
 /* Both gradients of a 32 -> 32 channel layer in one pass over its inputs
  * (replaces igm_conv3x3(IGM_CONV_DGRAD) + igm_conv3x3_wgrad for the hidden
  * layers; the Keras GradientTape of emulate.py:252 through Conv2D(3x3) +

@@ -174,3 +174,41 @@ def test_conv_backward_fused(B, H, W, npart):
     out = torch.empty((3, 3, 32, 32), device="cuda")
     L.check(lib.igm_cnn_wgrad_finish(p2.data_ptr(), npart, 32, 32, out.data_ptr(), st))
     np.testing.assert_allclose(out.cpu().numpy(), ref_w.numpy(), rtol=1e-4, atol=1e-4 * float(ref_w.abs().max()))
+
+
+@pytest.mark.parametrize("B,H,W,nl,pingpong", [(1, 8, 128, 1, True), (1, 37, 300, 3, True), (2, 11, 173, 4, False),
+                                               (1, 1000, 1000, 15, True), (1, 1000, 1000, 15, False),
+                                               (3, 5, 40, 2, True), (1, 200, 1000, 16, True)])
+def test_conv_stack(B, H, W, nl, pingpong):
+    """igm_conv3x3_stack: nl forward layers in one launch, bit for bit what nl
+    igm_conv3x3 calls write, with the outputs alternating between two buffers
+    or in one buffer per layer; a second call on the same flag buffer (the
+    next epoch) gives the same result."""
+    g = torch.Generator().manual_seed(B * 7 + H * 3 + W + nl)
+    lib, st = L.lib(), L.stream_ptr()
+    x = to_rc(bf(torch.randn(B, 32, H, W, generator=g))).to(torch.bfloat16).cuda()
+    ws = [pack_fwd(torch.randn(3, 3, 32, 32, generator=g) * (1.3 / np.sqrt(288)), 32).cuda() for _ in range(nl)]
+    bs = [(torch.randn(32, generator=g) * 0.1).cuda() for _ in range(nl)]
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ref, cur = [], x
+    for k in range(nl):
+        y = torch.empty_like(x)
+        L.check(lib.igm_conv3x3(0, B, H, W, 32, cur.data_ptr(), ws[k].data_ptr(), bs[k].data_ptr(), None,
+                                y.data_ptr(), None, 0, 0.01, err.data_ptr(), st))
+        ref.append(y)
+        cur = y
+    bufs = [torch.full_like(x, float("nan")) for _ in range(2 if pingpong else nl)]
+    outs = [bufs[k % 2] if pingpong else bufs[k] for k in range(nl)]
+    P = __import__("ctypes").c_void_p
+    flags = torch.zeros(int(lib.igm_conv3x3_stack_flags_len(B, H, W, nl)), dtype=torch.int32, device="cuda")
+    for epoch in (1, 2):
+        L.check(lib.igm_conv3x3_stack(B, H, W, nl, x.data_ptr(), (P * nl)(*[o.data_ptr() for o in outs]),
+                                      (P * nl)(*[w.data_ptr() for w in ws]), (P * nl)(*[b.data_ptr() for b in bs]),
+                                      flags.data_ptr(), epoch, 0.01, err.data_ptr(), st))
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0
+        assert bool((flags == epoch).all())
+        assert torch.equal(outs[-1], ref[-1])
+        if not pingpong:
+            for k in range(nl):
+                assert torch.equal(outs[k], ref[k]), k
