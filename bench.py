@@ -768,26 +768,28 @@ def assimilation_cpu(args, crop):
             "sample": f"one optimize_update iteration of the oracle on a {crop}x{crop} crop (second of two), "
                       f"scaled by ({args.size}/{crop})^2; emulator retraining not included"}
 
-def roofline_conv(conv_ms, size, peaks):
-    """Forward 3x3 conv (cin = 32): algorithmic bytes per launch = one read of
-    the input activation and one write of the output, 2 x 64 B per pixel."""
+def roofline_conv(conv_ms, size, peaks, layers=15):
+    """The forward conv stack (15 layers of 3x3 conv, 32 -> 32 channels, in one
+    launch): algorithmic bytes per launch = per layer one read of the input
+    activation and one write of the output, 2 x 64 B per pixel."""
     if not conv_ms:
         return None
     t = float(np.mean(conv_ms)) / 1e3
-    byts = 2 * 64 * size * size
+    byts = layers * 2 * 64 * size * size
     achieved = byts / t / 1e9
     peak = peaks.get("hbm_gbs", 6650.0)
-    # DRAM traffic of one launch from the committed ncu capture (batch 2 x 1000 x 1000), scaled to this
-    # launch's pixels (the traffic is proportional to the pixels processed)
+    # DRAM traffic of one launch from the committed ncu capture of the same launch (15 layers,
+    # batch 1 x 1000 x 1000), scaled to this launch's pixels
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "conv3x3_fwd_1000x1000.txt")
+    prof = os.path.join(ROOT, "profiles", "conv3x3_stack_15x1000x1000.txt")
     if os.path.exists(prof):
         for line in open(prof):
             if line.startswith("dram_bytes_per_launch:"):
-                traffic = round(float(line.split(":")[1]) * (size * size) / (2 * 1000 * 1000))
-    return {"kernel": "conv3x3_kernel<4,8,fwd> (tcgen05, cin 32)", "bound": "hbm", "achieved": round(achieved, 1),
-            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-            "algorithmic_bytes": byts, "avg_launch_us": round(t * 1e6, 2), "launches": len(conv_ms),
+                traffic = round(float(line.split(":")[1]) * (size * size) / (1000 * 1000))
+    return {"kernel": f"conv3x3_stack_kernel<8> (tcgen05, {layers} layers of cin 32 per launch)", "bound": "hbm",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": traffic, "algorithmic_bytes": byts, "avg_launch_us": round(t * 1e6, 2),
+            "avg_layer_us": round(t * 1e6 / layers, 2), "launches": len(conv_ms),
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback"}
 
 
@@ -1254,7 +1256,7 @@ def main():
             "fallback_checks": res["fallback_checks"], "fallbacks": res["fallbacks"],
             "years_per_time_step_emulated": em["years"] / (K * TIME_STEPS_PER_STEP),
             "years_per_time_step_plain": sv["years"] / (K * TIME_STEPS_PER_STEP),
-            "roofline": roofline_conv(conv_ms, args.size, peaks),
+            "roofline": roofline_conv(conv_ms, args.size, peaks, layers=15),
             "clocks": clocks, "gpu_launches": int(launches), "e2e": e2e}
     if rank == 0:
         if "config1" in det:

@@ -4,8 +4,9 @@
 Stencil (energy, energy + adjoint, one fused Adam iteration), transport and
 the vertical velocity at 1500 x 1500 x Nz 10 in FP32; the data-assimilation
 cost/gradient, flow direction and upwind divergence at 1500 x 1500 in FP32;
-the tensor-core convolution (forward, dgrad, wgrad) at batch 2 x 1000 x 1000
-x 32 channels.
+the tensor-core convolution (forward, dgrad, wgrad, the fused backward) at
+batch 2 x 1000 x 1000 x 32 channels, and the forward stack of 15 such layers
+at batch 1.
 
 ``python -m igm_b200.prof_cases assimilation_iteration`` instead sets up the
 data-assimilation loop on the 1000 x 1000 x Nz 10 glacier tongue (default
@@ -89,6 +90,17 @@ def main():
     part = torch.empty(148, int(lib.igm_conv3x3_wgrad_partial_len(32)), device="cuda")
     L.check(lib.igm_conv3x3_wgrad(B, H, W, 32, x.data_ptr(), y.data_ptr(), part.data_ptr(), 148, err.data_ptr(), s),
             "conv wgrad")
+    L.check(lib.igm_conv3x3_backward(B, H, W, y.data_ptr(), wp.data_ptr(), x.data_ptr(), y2.data_ptr(),
+                                     dbp.data_ptr(), part.data_ptr(), 148, 0.01, err.data_ptr(), s), "conv backward")
+    # the forward stack: 15 layers of batch 1 x 1000 x 1000, outputs alternating between two buffers
+    import ctypes as C
+    nl = 15
+    outs = (C.c_void_p * nl)(*[(y if k % 2 == 0 else y2).data_ptr() for k in range(nl)])
+    wps = (C.c_void_p * nl)(*([wp.data_ptr()] * nl))
+    bss = (C.c_void_p * nl)(*([bias.data_ptr()] * nl))
+    flags = torch.zeros(int(lib.igm_conv3x3_stack_flags_len(1, H, W, nl)), dtype=torch.int32, device="cuda")
+    L.check(lib.igm_conv3x3_stack(1, H, W, nl, x.data_ptr(), outs, wps, bss, flags.data_ptr(), 1, 0.01,
+                                  err.data_ptr(), s), "conv stack")
     torch.cuda.synchronize()
     if int(err.item()) != 0:
         raise RuntimeError(f"kernel error flag {int(err.item())}")
