@@ -143,6 +143,11 @@ class CNN:
                 wlen = max(int(L.lib().igm_conv3x3_wgrad_partial_len(F)), int(L.lib().igm_conv3x3_wgrad_partial_len(16)))
                 b["wpart"] = torch.empty(npart * wlen, dtype=torch.float32, device=d)
                 b["dbpart"] = torch.zeros((npart, F), dtype=torch.float32, device=d)
+                # the hidden layers' fused backward alternates between two partial buffers: each call
+                # finishes the previous call's partials while it writes its own
+                plen = int(L.lib().igm_conv3x3_wgrad_partial_len(F))
+                b["wpart2"] = [torch.empty(npart * plen, dtype=torch.float32, device=d) for _ in range(2)]
+                b["dbpart2"] = [torch.zeros((npart, F), dtype=torch.float32, device=d) for _ in range(2)]
                 hl = int(L.lib().igm_cnn_head_partial_len(self.nz))
                 b["hpart"] = torch.empty((2 * npart, hl), dtype=torch.float32, device=d)
             nst = max(self.L - 1, 1)
@@ -247,20 +252,32 @@ class CNN:
                 L.check(lib.igm_reduce_partials(buf["hpart"].data_ptr() + 4 * (nh + self.nout), npart2, F, hl,
                                                 gp + 4 * self.offsets[2 * (self.L - 1) + 1], 0, st), "reduce db")
         cur = 0
+        prev = None  # the hidden layer whose partials the next fused call finishes
         for l in range(self.L - 1, -1, -1):
             gl = g[cur]
             if l > 0 and param_grads:
-                # both gradients of the layer in one pass (igm_conv3x3_backward)
+                # both gradients of the layer in one pass (igm_conv3x3_backward), which also finishes
+                # the layer above's weight and bias gradients from the previous call's partials
                 nxt = g[1 - cur]
-                rc = lib.igm_conv3x3_backward(B, h, w, _p(gl), self._wb(l), _p(acts[l - 1]), _p(nxt),
-                                              _p(buf["dbpart"]), _p(buf["wpart"]), npart, self.alpha, _p(self.err), st)
+                wp, dbp = buf["wpart2"][l % 2], buf["dbpart2"][l % 2]
+                if prev is None:
+                    fin = (None, None, None, None)
+                else:
+                    fin = (_p(buf["wpart2"][prev % 2]), _p(buf["dbpart2"][prev % 2]), gp + 4 * self.offsets[2 * prev],
+                           gp + 4 * self.offsets[2 * (prev - 1) + 1])
+                rc = lib.igm_conv3x3_backward(B, h, w, _p(gl), self._wb(l), _p(acts[l - 1]), _p(nxt), _p(dbp), _p(wp),
+                                              npart, self.alpha, _p(self.err), *fin, st)
                 L.check(rc, f"igm_conv3x3_backward layer {l}")
-                L.check(lib.igm_cnn_wgrad_finish(_p(buf["wpart"]), npart, F, F, gp + 4 * self.offsets[2 * l], st),
-                        "igm_cnn_wgrad_finish")
-                L.check(lib.igm_reduce_partials(_p(buf["dbpart"]), npart, F, F, gp + 4 * self.offsets[2 * (l - 1) + 1],
-                                                0, st), "reduce db")
+                prev = l
                 cur = 1 - cur
                 continue
+            if prev is not None and param_grads:
+                # the last fused call's partials (layer 1)
+                L.check(lib.igm_cnn_wgrad_finish(_p(buf["wpart2"][prev % 2]), npart, F, F,
+                                                 gp + 4 * self.offsets[2 * prev], st), "igm_cnn_wgrad_finish")
+                L.check(lib.igm_reduce_partials(_p(buf["dbpart2"][prev % 2]), npart, F, F,
+                                                gp + 4 * self.offsets[2 * (prev - 1) + 1], 0, st), "reduce db")
+                prev = None
             if l > 0 and param_grads:
                 rc = lib.igm_conv3x3_wgrad(B, h, w, F, _p(acts[l - 1]), _p(gl), _p(buf["wpart"]), npart,
                                            _p(self.err), st)

@@ -15,12 +15,12 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "reduce.cuh"
 
 namespace igm {
 
 constexpr int kF = 32;  // filters
-constexpr int kFinWarps = 8;  // warps of the fixed-order partial-sum kernels
-constexpr int kRedBatch = 8;  // partials whose loads a lane issues before adding them
+static_assert(kF == kFinCols, "the finishing reductions sum 32-channel rows");
 
 __device__ __forceinline__ float bf_lo(uint32_t w) {
   return __low2float(*reinterpret_cast<const __nv_bfloat162*>(&w));
@@ -31,14 +31,6 @@ __device__ __forceinline__ float bf_hi(uint32_t w) {
 __device__ __forceinline__ uint32_t bf_pack(float lo, float hi) {
   __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<uint32_t*>(&h);
-}
-
-// fixed xor-shuffle tree over the 32 lanes: the same order on every run, the
-// total in every lane
-__device__ __forceinline__ float warp_sum_fixed(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
 }
 
 // offsets (in floats) of the parameters of layer l (0-based; l == L is the head)
@@ -563,36 +555,6 @@ __global__ void __launch_bounds__(kHpWarps * 32, 2)
   }
 }
 
-// Sum over the partials p = warp, warp + kFinWarps, ... of the entries (kh + jj,
-// column jj) for jj < JN and input channels ci + sp, sp < NSP, in that order;
-// kRedBatch partials are loaded before they are added (absent ones add +0).
-template <int JN, int NSP>
-__device__ __forceinline__ float finish_sum(const float* part, int n_parts, int warp, int lane, int kw, int kh,
-                                            int ci, int cw) {
-  constexpr int wn = JN * kF;
-  float acc = 0.f;
-  for (int p0 = warp; p0 < n_parts; p0 += kFinWarps * kRedBatch) {
-    float v[kRedBatch][JN][NSP];
-#pragma unroll
-    for (int u = 0; u < kRedBatch; ++u) {
-      const int p = p0 + u * kFinWarps;
-      const float* base = part + ((size_t)(p < n_parts ? p : 0) * 3 + kw) * 128 * wn;
-#pragma unroll
-      for (int jj = 0; jj < JN; ++jj)
-#pragma unroll
-        for (int sp = 0; sp < NSP; ++sp)
-          v[u][jj][sp] = p < n_parts ? base[(size_t)((kh + jj) * cw + ci + sp) * wn + jj * kF + lane] : 0.f;
-    }
-#pragma unroll
-    for (int u = 0; u < kRedBatch; ++u)
-#pragma unroll
-      for (int jj = 0; jj < JN; ++jj)
-#pragma unroll
-        for (int sp = 0; sp < NSP; ++sp) acc += v[u][jj][sp];
-  }
-  return acc;
-}
-
 // head kernel gradient from igm_conv3x3_wgrad partials over (A16, dY): the centre
 // tap (kh = kw = 1), i.e. accumulator entries (r, jj) with r - jj = 1, kw = 1.
 __global__ void __launch_bounds__(kFinWarps * 32) head_wgrad_finish_kernel(const float* part, int n_parts, int nout,
@@ -797,18 +759,7 @@ __global__ void reduce_partials_kernel(const float* part, int n_parts, int len, 
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < len; i += nw) {
-    float s = 0.f;
-    for (int p0 = lane; p0 < n_parts; p0 += 32 * kRedBatch) {
-      float v[kRedBatch];
-#pragma unroll
-      for (int u = 0; u < kRedBatch; ++u) {
-        const int p = p0 + 32 * u;
-        v[u] = p < n_parts ? part[(size_t)p * stride + i] : 0.f;
-      }
-#pragma unroll
-      for (int u = 0; u < kRedBatch; ++u) s += v[u];
-    }
-    s = warp_sum_fixed(s);
+    const float s = partial_sum(part, n_parts, stride, i, lane);
     if (lane == 0) out[i] = accumulate ? out[i] + s : s;
   }
 }

@@ -34,6 +34,7 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "reduce.cuh"
 #include "tc.cuh"
 
 namespace igm {
@@ -819,7 +820,8 @@ struct BwdGeom {
   static constexpr uint32_t WBYTES = 9 * C8 * kCout * 16;
   static constexpr uint32_t OFF_W = NST * STAGE;
   static constexpr uint32_t OFF_BAR = OFF_W + WBYTES;
-  static constexpr uint32_t SMEM = OFF_BAR + 128 + 16 + 1024;
+  static constexpr uint32_t OFF_RED = OFF_BAR + 256;    // the finishing reductions' [8][32] exchange
+  static constexpr uint32_t SMEM = OFF_RED + kFinWarps * kFinCols * 4 + 1024;
   // weight gradient (conv3x3_wgrad_kernel<4>'s item geometry)
   static constexpr int NROW = 128 / (C8 * 8);           // input rows per M = 128
   static constexpr int JN = NROW - 2;                   // output rows per MMA (N = JN x 32)
@@ -844,6 +846,11 @@ struct BwdArgs {
   float* w_partial;            // [gridDim.x][3][128][WN]
   float alpha;
   int* err;
+  // the previous launch's (the layer above's) partials and where their sums go; NULL: none
+  const float* prev_w_partial;  // [gridDim.x][3][128][WN] -> prev_w_out [3][3][32][32]
+  const float* prev_db_partial; // [gridDim.x][32] -> prev_db_out [32]
+  float* prev_w_out;
+  float* prev_db_out;
 };
 
 __global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_bwd_kernel(const BwdArgs a) {
@@ -979,6 +986,31 @@ __global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_bwd_kernel(const B
     const int half = (warp - 2) >> 2;
     const int r0 = half * RH;
     const int p = q * 32 + lane;
+    if (a.prev_w_partial) {
+      // The layer above's weight and bias gradients from its partials, while this kernel's first
+      // tiles load: the eight epilogue warps are the eight warps of wgrad_finish_kernel (one
+      // (tap, ci) row per step, the same partials in the same order) and of reduce_partials_kernel.
+      static_assert(kConvEpiWarps == kFinWarps, "the epilogue warps are the finishing reduction's warps");
+      float(*red)[kFinCols] = reinterpret_cast<float(*)[kFinCols]>(smem + G::OFF_RED);
+      const int ew = warp - 2;
+      for (int gi = blockIdx.x; gi < 9 * kCout; gi += gridDim.x) {
+        const int ci = gi % kCout, tap = gi / kCout;
+        red[ew][lane] = finish_sum<2, 1>(a.prev_w_partial, (int)gridDim.x, ew, lane, tap % 3, tap / 3, ci, 32);
+        asm volatile("bar.sync 1, %0;\n" ::"n"(32 * kConvEpiWarps) : "memory");
+        if (ew == 0) {
+          float tsum = 0.f;
+#pragma unroll
+          for (int w2 = 0; w2 < kFinWarps; ++w2) tsum += red[w2][lane];
+          a.prev_w_out[(size_t)gi * kFinCols + lane] = tsum;
+        }
+        asm volatile("bar.sync 1, %0;\n" ::"n"(32 * kConvEpiWarps) : "memory");
+      }
+      if (ew == 0)
+        for (int i = blockIdx.x; i < kCout; i += gridDim.x) {
+          const float sdb = partial_sum(a.prev_db_partial, (int)gridDim.x, kCout, i, lane);
+          if (lane == 0) a.prev_db_out[i] = sdb;
+        }
+    }
     float dbacc[kCout];
 #pragma unroll
     for (int c = 0; c < kCout; ++c) dbacc[c] = 0.f;
@@ -1237,7 +1269,9 @@ extern "C" int igm_conv3x3_wgrad(int batch, int height, int width, int cin, cons
 
 extern "C" int igm_conv3x3_backward(int batch, int height, int width, const void* g, const void* wpack_bwd,
                                     const void* x, void* g_prev, float* db_partials, float* w_partials, int n_parts,
-                                    float alpha, int* err, void* stream) {
+                                    float alpha, int* err, const float* prev_w_partials,
+                                    const float* prev_db_partials, float* prev_w_out, float* prev_db_out,
+                                    void* stream) {
   using G = BwdGeom;
   IGM_CHECK_ARG(batch >= 1 && height >= 1 && width >= 1 && batch <= 65535, IGM_ERR_BAD_SHAPE,
                 "igm_conv3x3_backward: bad shape %dx%dx%d", batch, height, width);
@@ -1245,6 +1279,12 @@ extern "C" int igm_conv3x3_backward(int batch, int height, int width, const void
                 "igm_conv3x3_backward: NULL argument");
   IGM_CHECK_ARG(((uintptr_t)g & 15) == 0 && ((uintptr_t)x & 15) == 0 && ((uintptr_t)g_prev & 15) == 0,
                 IGM_ERR_BAD_ARGUMENT, "igm_conv3x3_backward: activations must be 16-byte aligned");
+  const bool prev = prev_w_partials != nullptr;
+  IGM_CHECK_ARG(prev == (prev_db_partials != nullptr) && prev == (prev_w_out != nullptr) &&
+                    prev == (prev_db_out != nullptr),
+                IGM_ERR_BAD_ARGUMENT, "igm_conv3x3_backward: the four prev_* pointers are all set or all NULL");
+  IGM_CHECK_ARG(!prev || (prev_w_partials != w_partials && prev_db_partials != db_partials), IGM_ERR_BAD_ARGUMENT,
+                "igm_conv3x3_backward: the previous partials must not be this call's partial buffers");
   static bool configured = false;
   int rc = set_smem(conv3x3_bwd_kernel, G::SMEM, &configured);
   if (rc) return rc;
@@ -1261,6 +1301,10 @@ extern "C" int igm_conv3x3_backward(int batch, int height, int width, const void
   a.w_partial = w_partials;
   a.alpha = alpha;
   a.err = err;
+  a.prev_w_partial = prev_w_partials;
+  a.prev_db_partial = prev_db_partials;
+  a.prev_w_out = prev_w_out;
+  a.prev_db_out = prev_db_out;
   launch_pdl(conv3x3_bwd_kernel, dim3(n_parts), dim3(kConvFwdThreads), G::SMEM, as_stream(stream), a);
   return launch_status("conv3x3_bwd_kernel");
 }

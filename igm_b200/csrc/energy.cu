@@ -218,9 +218,14 @@ struct StencilSmem {
 };
 
 // Thread rows per CTA (each thread row = one warp = two cell rows).
-template <typename T> struct ThreadRows { static constexpr int value = 8; };
+#ifndef IGM_STENCIL_ROWS_F32
+#define IGM_STENCIL_ROWS_F32 8
+#endif
+template <typename T> struct ThreadRows { static constexpr int value = IGM_STENCIL_ROWS_F32; };
 template <> struct ThreadRows<double> { static constexpr int value = 4; };
-template <typename T, int MODE> struct MinBlocks { static constexpr int value = MODE == kEnergyOnly ? 3 : 2; };
+template <typename T, int MODE> struct MinBlocks {
+  static constexpr int value = (MODE == kEnergyOnly ? 3 : 2) * 8 / IGM_STENCIL_ROWS_F32;
+};
 template <int MODE> struct MinBlocks<double, MODE> { static constexpr int value = 2; };
 
 struct TileGeo {

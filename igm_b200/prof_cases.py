@@ -91,7 +91,8 @@ def main():
     L.check(lib.igm_conv3x3_wgrad(B, H, W, 32, x.data_ptr(), y.data_ptr(), part.data_ptr(), 148, err.data_ptr(), s),
             "conv wgrad")
     L.check(lib.igm_conv3x3_backward(B, H, W, y.data_ptr(), wp.data_ptr(), x.data_ptr(), y2.data_ptr(),
-                                     dbp.data_ptr(), part.data_ptr(), 148, 0.01, err.data_ptr(), s), "conv backward")
+                                     dbp.data_ptr(), part.data_ptr(), 148, 0.01, err.data_ptr(), None, None, None, None,
+                                     s), "conv backward")
     # the forward stack: 15 layers of batch 1 x 1000 x 1000, outputs alternating between two buffers
     import ctypes as C
     nl = 15

@@ -530,10 +530,16 @@ IGM_API size_t igm_conv3x3_stack_flags_len(int batch, int height, int width, int
  *   db_partials = per-CTA sums of g_prev over the pixels, [n_parts][32];
  *   w_partials  = the igm_conv3x3_wgrad(cin 32) partials of (x, g), [n_parts]
  *                 x igm_conv3x3_wgrad_partial_len(32) floats, for igm_cnn_wgrad_finish.
- * Every slot of both partial buffers is written.  err as for igm_conv3x3. */
+ * Every slot of both partial buffers is written.  err as for igm_conv3x3.
+ * With prev_w_partials, prev_db_partials (the partial buffers of the previous
+ * call, the layer above, n_parts parts each; not this call's buffers) the call
+ * also finishes them: prev_w_out = igm_cnn_wgrad_finish(prev_w_partials, cin 32)
+ * and prev_db_out = igm_reduce_partials(prev_db_partials, 32), bit for bit as
+ * those calls compute them.  All four prev_* NULL: nothing is finished. */
 IGM_API int igm_conv3x3_backward(int batch, int height, int width, const void* g, const void* wpack_bwd,
                                  const void* x, void* g_prev, float* db_partials, float* w_partials, int n_parts,
-                                 float alpha, int* err, void* stream);
+                                 float alpha, int* err, const float* prev_w_partials, const float* prev_db_partials,
+                                 float* prev_w_out, float* prev_db_out, void* stream);
 IGM_API int igm_conv_sm_count(void);
 
 IGM_API size_t igm_cnn_param_count(int nb_layers, int cin, int nout);

@@ -157,7 +157,8 @@ def test_conv_backward_fused(B, H, W, npart):
     db2 = torch.full((npart, 32), float("nan"), device="cuda")
     p2 = torch.full((npart, plen), float("nan"), device="cuda")
     L.check(lib.igm_conv3x3_backward(B, H, W, gd.data_ptr(), wd.data_ptr(), ad.data_ptr(), y2.data_ptr(),
-                                     db2.data_ptr(), p2.data_ptr(), npart, 0.01, err.data_ptr(), st))
+                                     db2.data_ptr(), p2.data_ptr(), npart, 0.01, err.data_ptr(), None, None, None, None,
+                                     st))
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     assert torch.equal(y1, y2)
@@ -212,3 +213,37 @@ def test_conv_stack(B, H, W, nl, pingpong):
         if not pingpong:
             for k in range(nl):
                 assert torch.equal(outs[k], ref[k]), k
+
+
+@pytest.mark.parametrize("B,H,W,npart", [(1, 8, 128, 148), (2, 37, 300, 23), (1, 1000, 1000, 148)])
+def test_conv_backward_finishes_the_previous_layer(B, H, W, npart):
+    """A fused backward call given the previous call's partial buffers also
+    finishes them: the kernel gradient bit for bit as igm_cnn_wgrad_finish, the
+    bias gradient as igm_reduce_partials; its own outputs are unchanged."""
+    g = torch.Generator().manual_seed(B + H + W)
+    lib, st = L.lib(), L.stream_ptr()
+    mk = lambda: to_rc(bf(torch.randn(B, 32, H, W, generator=g))).to(torch.bfloat16).cuda()  # noqa: E731
+    g1, x1, g2, x2 = mk(), mk(), mk(), mk()
+    w1 = pack_bwd(torch.randn(3, 3, 32, 32, generator=g) * (1.0 / np.sqrt(288))).cuda()
+    w2 = pack_bwd(torch.randn(3, 3, 32, 32, generator=g) * (1.0 / np.sqrt(288))).cuda()
+    plen = int(lib.igm_conv3x3_wgrad_partial_len(32))
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    y1, y2, y2b = (torch.empty_like(g1) for _ in range(3))
+    p1, p2, p2b = (torch.full((npart, plen), float("nan"), device="cuda") for _ in range(3))
+    d1, d2, d2b = (torch.full((npart, 32), float("nan"), device="cuda") for _ in range(3))
+    call = lambda gg, ww, xx, yy, dd, pp, *fin: L.check(lib.igm_conv3x3_backward(  # noqa: E731
+        B, H, W, gg.data_ptr(), ww.data_ptr(), xx.data_ptr(), yy.data_ptr(), dd.data_ptr(), pp.data_ptr(), npart,
+        0.01, err.data_ptr(), *fin, st))
+    call(g1, w1, x1, y1, d1, p1, None, None, None, None)
+    wout = torch.full((3, 3, 32, 32), float("nan"), device="cuda")
+    dbout = torch.full((32,), float("nan"), device="cuda")
+    call(g2, w2, x2, y2, d2, p2, p1.data_ptr(), d1.data_ptr(), wout.data_ptr(), dbout.data_ptr())
+    call(g2, w2, x2, y2b, d2b, p2b, None, None, None, None)
+    wref = torch.empty_like(wout)
+    dbref = torch.empty_like(dbout)
+    L.check(lib.igm_cnn_wgrad_finish(p1.data_ptr(), npart, 32, 32, wref.data_ptr(), st))
+    L.check(lib.igm_reduce_partials(d1.data_ptr(), npart, 32, 32, dbref.data_ptr(), 0, st))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert torch.equal(wout, wref) and torch.equal(dbout, dbref)
+    assert torch.equal(y2, y2b) and torch.equal(p2, p2b) and torch.equal(d2, d2b)
