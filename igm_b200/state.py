@@ -7,9 +7,11 @@ attribute bag.  The processes accept two residencies:
   processes rebind attributes to new tensors, as the reference rebinds TF
   tensors;
 * host-resident: ``state.thk`` is a numpy array.  Each process then copies
-  the fields it reads to the device (through pinned staging buffers) and
-  writes the fields it produces back into pinned numpy arrays on the state.
-  This is what a host-side caller of the plugin pays per step.
+  the fields it reads to the device and writes the fields it produces back
+  into pinned numpy arrays on the state; a host array the processes did not
+  produce is replaced, on its first use, by a pinned array of the same values,
+  so every copy is a DMA from pinned memory.  This is what a host-side caller
+  of the plugin pays per step.
 """
 
 from __future__ import annotations
@@ -62,8 +64,14 @@ def get(state, name, dtype=torch.float32):
         if t is not None and t.numpy() is not None and t.data_ptr() == arr.__array_interface__["data"][0]:
             src = t
         if src is None:
+            # a host array the processes did not produce: copy it once into a pinned buffer and bind that
+            # in its place (same values), so that every later step copies it to the device by DMA from
+            # pinned memory, without a host-side staging copy
             src = _pinned(state, "in:" + name, arr.shape, torch.from_numpy(np.empty(0, arr.dtype)).dtype)
             src.numpy()[...] = arr
+            view = src.numpy()
+            state.__dict__.setdefault("_igm_pinned_views", {})[id(view)] = src
+            setattr(state, name, view)
     return src.to(dev, non_blocking=True).to(dtype)
 
 
