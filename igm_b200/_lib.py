@@ -112,6 +112,7 @@ SIGNATURES = {
     "igm_cfl_dt": (I, [P, P, D, D, D, P]),
     "igm_conv3x3": (I, [I, I, I, I, I, P, P, P, P, P, P, I, C.c_float, P, P]),
     "igm_conv3x3_wgrad": (I, [I, I, I, I, P, P, P, I, P, P]),
+    "igm_conv1x1_wgrad": (I, [I, I, I, P, P, P, I, P, P]),
     "igm_conv3x3_backward": (I, [I, I, I, P, P, P, P, P, P, I, C.c_float, P, P, P, P, P, P]),
     "igm_conv3x3_stack": (I, [I, I, I, I, P, P, P, P, P, I, C.c_float, P, P]),
     "igm_conv3x3_stack_flags_len": (C.c_size_t, [I, I, I, I]),

@@ -236,9 +236,9 @@ class CNN:
                                             gp + 4 * self.offsets[2 * self.L + 1], 0, st), "reduce head bias")
             L.check(lib.igm_reduce_partials(buf["hpart"].data_ptr() + 4 * self.nout, npart2, F, stride,
                                             gp + 4 * self.offsets[2 * (self.L - 1) + 1], 0, st), "reduce db")
-            rc = lib.igm_conv3x3_wgrad(B, h, w, F, _p(acts[self.L - 1]), _p(buf["dyb"]), _p(buf["wpart"]), npart,
+            rc = lib.igm_conv1x1_wgrad(B, h, w, _p(acts[self.L - 1]), _p(buf["dyb"]), _p(buf["wpart"]), npart,
                                        _p(self.err), st)
-            L.check(rc, "igm_conv3x3_wgrad head")
+            L.check(rc, "igm_conv1x1_wgrad head")
             L.check(lib.igm_cnn_head_wgrad_finish(_p(buf["wpart"]), npart, self.nout, gp + 4 * self.offsets[2 * self.L],
                                                   st), "igm_cnn_head_wgrad_finish")
         elif self.nout > F:

@@ -628,6 +628,7 @@ struct WgradArgs {
   const __nv_bfloat16* g;  // gradient w.r.t. the pre-activation [B][H][4][W][8]
   float* partial;  // [gridDim.x][3][128][32]
   int* err;
+  int centre_only;  // only the kw = 1 accumulators (a 1x1 convolution's weight gradient)
 };
 
 // Output rows per work item of the weight-gradient kernel, and its input stages.
@@ -736,6 +737,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3x3_wgrad_kernel(const Wg
           const uint32_t acc0 = (it > 0 || q > 0) ? 1u : 0u;
 #pragma unroll
           for (int dx = 0; dx < 3; ++dx) {
+            if (a.centre_only && dx != 1) continue;
 #pragma unroll
             for (int ks = 0; ks < kTW / 16; ++ks) {
               const uint64_t ad = tc::desc_join(xq + ((dx * 16 + ks * 256) >> 4), x_hi);
@@ -1211,7 +1213,7 @@ static int conv_launch(int B, int H, int W, const void* x, const void* wpack, co
 
 template <int C8_IN>
 static int wgrad_launch(int B, int H, int W, const void* x, const void* g, float* partial, int n_parts, int* err,
-                        cudaStream_t st) {
+                        cudaStream_t st, int centre_only = 0) {
   using G = WgradGeom<C8_IN>;
   static bool configured = false;
   int rc = set_smem(conv3x3_wgrad_kernel<C8_IN>, G::SMEM, &configured);
@@ -1227,6 +1229,7 @@ static int wgrad_launch(int B, int H, int W, const void* x, const void* g, float
   a.g = (const __nv_bfloat16*)g;
   a.partial = partial;
   a.err = err;
+  a.centre_only = centre_only;
   launch_pdl(conv3x3_wgrad_kernel<C8_IN>, dim3(n_parts), dim3(kConvThreads), G::SMEM, st, a);
   return launch_status("conv3x3_wgrad_kernel");
 }
@@ -1362,6 +1365,13 @@ extern "C" int igm_conv3x3_stack(int batch, int height, int width, int nlayers, 
 
 extern "C" size_t igm_conv3x3_stack_flags_len(int batch, int height, int width, int nlayers) {
   return (size_t)nlayers * batch * ((width + kTW - 1) / kTW) * ((height + kRows - 1) / kRows);
+}
+
+extern "C" int igm_conv1x1_wgrad(int batch, int height, int width, const void* x, const void* g, float* partials,
+                                 int n_parts, int* err, void* stream) {
+  IGM_CHECK_ARG(batch >= 1 && height >= 1 && width >= 1, IGM_ERR_BAD_SHAPE, "igm_conv1x1_wgrad: bad shape");
+  IGM_CHECK_ARG(x && g && partials && n_parts >= 1, IGM_ERR_BAD_ARGUMENT, "igm_conv1x1_wgrad: bad argument");
+  return wgrad_launch<4>(batch, height, width, x, g, partials, n_parts, err, as_stream(stream), 1);
 }
 
 extern "C" size_t igm_conv3x3_wgrad_partial_len(int cin) {

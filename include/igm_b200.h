@@ -507,6 +507,12 @@ IGM_API int igm_conv3x3(int mode, int batch, int height, int width, int cin, con
 IGM_API int igm_conv3x3_wgrad(int batch, int height, int width, int cin, const void* x, const void* g,
                               float* partials, int n_parts, int* err, void* stream);
 IGM_API size_t igm_conv3x3_wgrad_partial_len(int cin);
+/* The centre tap alone of igm_conv3x3_wgrad (cin 32): the partials of kw = 1 bit
+ * for bit as igm_conv3x3_wgrad writes them (the weight gradient of the 1x1
+ * head, igm_cnn_head_wgrad_finish), a third of the MMAs; the kw = 0, 2 slots of
+ * the partial buffer hold no defined values. */
+IGM_API int igm_conv1x1_wgrad(int batch, int height, int width, const void* x, const void* g, float* partials,
+                              int n_parts, int* err, void* stream);
 /* nlayers (1..16) forward 3x3 convolutions of 32 -> 32 channels in one launch,
  * as nlayers calls of igm_conv3x3(IGM_CONV_FWD_LEAKY) would compute them: layer
  * k reads x (k = 0) or outs[k-1] and writes outs[k] = LeakyReLU(conv(., wpacks[k])

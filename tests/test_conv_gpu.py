@@ -247,3 +247,28 @@ def test_conv_backward_finishes_the_previous_layer(B, H, W, npart):
     assert int(err.item()) == 0
     assert torch.equal(wout, wref) and torch.equal(dbout, dbref)
     assert torch.equal(y2, y2b) and torch.equal(p2, p2b) and torch.equal(d2, d2b)
+
+
+@pytest.mark.parametrize("B,H,W", [(1, 8, 128), (2, 9, 150), (1, 1000, 1000)])
+def test_conv1x1_wgrad_is_the_centre_tap(B, H, W):
+    """igm_conv1x1_wgrad: the kw = 1 partials bit for bit as igm_conv3x3_wgrad's,
+    so the head's kernel gradient (igm_cnn_head_wgrad_finish) is unchanged."""
+    g = torch.Generator().manual_seed(B * 3 + H + W)
+    lib, st = L.lib(), L.stream_ptr()
+    x = to_rc(bf(torch.randn(B, 32, H, W, generator=g))).to(torch.bfloat16).cuda()
+    gd = to_rc(bf(torch.randn(B, 32, H, W, generator=g))).to(torch.bfloat16).cuda()
+    npart = 148
+    plen = int(lib.igm_conv3x3_wgrad_partial_len(32))
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    p3 = torch.empty((npart, 3, 128, plen // 384), device="cuda")
+    p1 = torch.empty_like(p3)
+    L.check(lib.igm_conv3x3_wgrad(B, H, W, 32, x.data_ptr(), gd.data_ptr(), p3.data_ptr(), npart, err.data_ptr(), st))
+    L.check(lib.igm_conv1x1_wgrad(B, H, W, x.data_ptr(), gd.data_ptr(), p1.data_ptr(), npart, err.data_ptr(), st))
+    o3 = torch.empty((32, 20), device="cuda")
+    o1 = torch.empty_like(o3)
+    L.check(lib.igm_cnn_head_wgrad_finish(p3.data_ptr(), npart, 20, o3.data_ptr(), st))
+    L.check(lib.igm_cnn_head_wgrad_finish(p1.data_ptr(), npart, 20, o1.data_ptr(), st))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert torch.equal(p1[:, 1], p3[:, 1])
+    assert torch.equal(o1, o3)
