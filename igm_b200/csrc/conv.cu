@@ -421,6 +421,12 @@ __global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_stack_kernel(const
   volatile int* abort_epi = reinterpret_cast<volatile int*>(smem + OFF_BAR + 132);  // an epilogue wait gave up
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int per = a.n_tiles;
+  // Layer k's tiles t = first(k) + j * gridDim.x: the CTAs that take the layer's last, partial round
+  // of tiles move on by (per mod gridDim.x) each layer, so over the stack every CTA takes about the
+  // same number of tiles (a fixed assignment would let the same CTAs take one tile more in every
+  // layer, and the others wait for them)
+  const int ncta = (int)gridDim.x, rem = per % ncta;
+  auto first = [&](int k) { return ((int)blockIdx.x + ncta - (int)(((long long)k * rem) % ncta)) % ncta; };
 
   if (threadIdx.x == 0) {
     *abort_epi = 0;
@@ -450,7 +456,7 @@ __global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_stack_kernel(const
     bool ok = true;
     for (int k = 0; k < a.nlayers && ok; ++k) {
       const __nv_bfloat16* src = k == 0 ? a.in : a.out[k - 1];
-      for (int t = blockIdx.x; t < per; t += gridDim.x, ++it) {
+      for (int t = first(k); t < per; t += gridDim.x, ++it) {
         const int s = it % NST, use = it / NST;
         if (!tc::mbar_wait(&empty[s], (use & 1) ^ 1)) {
           if (lane == 0) set_err(a.err, 31);
@@ -484,7 +490,7 @@ __global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_stack_kernel(const
           tc::fence_proxy_async_global();  // the acquired data is read next by the bulk-copy (async) proxy
         }
         unsigned char* st = smem + s * G::STAGE;
-        if (t == (int)blockIdx.x && lane == 0) {
+        if (t == first(k) && lane == 0) {
           // this layer's weights, on the barrier of its first tile (their buffer's last reader, layer
           // k - 2, completed: the commit that released this stage covers every earlier MMA)
           tc::mbar_expect_tx_only(&full[s], G::WBYTES);
@@ -502,7 +508,7 @@ __global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_stack_kernel(const
       bool ok = true;
       for (int k = 0; k < a.nlayers && ok; ++k) {
         const uint32_t w_lo = tc::desc_lo(sbase + G::OFF_W + (k & 1) * G::WBYTES, kWRowsN * 16);
-        for (int t = blockIdx.x; t < per; t += gridDim.x, ++it) {
+        for (int t = first(k); t < per; t += gridDim.x, ++it) {
           const int s = it % NST, use = it / NST, acc = it % NACC, ause = it / NACC;
           if (!tc::mbar_wait(&tempty[acc], (ause & 1) ^ 1) || !tc::mbar_wait(&full[s], use & 1)) {
             set_err(a.err, 33);
@@ -556,7 +562,7 @@ __global__ void __launch_bounds__(kConvFwdThreads, 1) conv3x3_stack_kernel(const
 #pragma unroll
       for (int c = 0; c < kCout; ++c) bias[c] = __ldg(a.bias[k] + c);
       uint4* o = reinterpret_cast<uint4*>(a.out[k]);
-      for (int t = blockIdx.x; t < per; t += gridDim.x, ++it) {
+      for (int t = first(k); t < per; t += gridDim.x, ++it) {
         const int use = it / NACC, acc = it % NACC;
         const int txi = t % a.tiles_w, rest = t / a.tiles_w;
         const int tyi = rest % a.tiles_h, b = rest / a.tiles_h;
