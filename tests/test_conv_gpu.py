@@ -272,3 +272,33 @@ def test_conv1x1_wgrad_is_the_centre_tap(B, H, W):
     assert int(err.item()) == 0
     assert torch.equal(p1[:, 1], p3[:, 1])
     assert torch.equal(o1, o3)
+
+
+@pytest.mark.parametrize("B,H,W,nz,mask", [(1, 4, 128, 10, False), (2, 9, 173, 10, True), (1, 1000, 1000, 10, True),
+                                           (3, 5, 41, 16, True), (1, 7, 301, 5, False), (1, 1, 1, 1, True)])
+def test_head_forward(B, H, W, nz, mask):
+    """igm_cnn_head_forward (the 1x1 head) against a float64 evaluation of the
+    same sum: FP32 fma chains over the 32 channels, so within 1e-5 of the
+    output's scale; zero where thk_mask <= 0."""
+    g = torch.Generator().manual_seed(B + H + W + nz)
+    lib, st = L.lib(), L.stream_ptr()
+    nout = 2 * nz
+    a32 = bf(torch.randn(B, 32, H, W, generator=g))
+    act = to_rc(a32).to(torch.bfloat16).cuda()
+    wh = torch.randn(32, nout, generator=g) * 0.3
+    bh = torch.randn(nout, generator=g) * 0.1
+    thk = torch.rand(B, H, W, generator=g) - 0.3
+    U = torch.full((B, nz, H, W), float("nan"), device="cuda")
+    V = torch.full_like(U, float("nan"))
+    thk_d, wh_d, bh_d = thk.cuda(), wh.cuda(), bh.cuda()  # device copies held for the call
+    L.check(lib.igm_cnn_head_forward(B, H, W, nz, act.data_ptr(), wh_d.data_ptr(), bh_d.data_ptr(), 2.5,
+                                     U.data_ptr(), V.data_ptr(), thk_d.data_ptr() if mask else None, st))
+    torch.cuda.synchronize()
+    y = (torch.einsum("bchw,cj->bjhw", a32.double(), wh.double()) + bh.double()[None, :, None, None]) * 2.5
+    if mask:
+        y = torch.where((thk > 0)[:, None], y, torch.zeros_like(y))
+    got = torch.cat([U, V], 1).cpu().double()
+    assert bool(torch.isfinite(got).all())
+    assert float((got - y).abs().max()) <= 1e-5 * float(y.abs().max()) + 1e-6
+    if mask:
+        assert bool((got[(thk <= 0)[:, None].expand_as(got)] == 0).all())
