@@ -365,3 +365,35 @@ def test_force_max_velbar_in_the_process(method):
     ub, _ = O.get_velbar(cpu(st.U), cpu(st.V), w)
     assert rel_l2(cpu(st.ubar).numpy(), ub.numpy()) < 1e-6
     assert torch.equal(st.uvelsurf, st.U[-1]) and torch.equal(st.uvelbase, st.U[0])
+
+
+def test_host_resident_state_matches_device_resident():
+    """The same three solved time steps with the state in host numpy arrays
+    and on the device: identical fields; the caller's input arrays are
+    replaced by pinned arrays of the same values (so each step's copies are
+    DMAs), and the outputs come back as pinned numpy arrays."""
+    cfg = make_cfg("solved", nbitmax=10)
+    dev_st, host_st = make_state(seed=5), make_state(seed=5)
+    orig = {}
+    for k in ("topg", "thk", "arrhenius", "slidingco"):
+        orig[k] = getattr(host_st, k).cpu().numpy().copy()
+        setattr(host_st, k, orig[k].copy())
+    host_st.device = "cuda"
+    runs = []
+    for st in (dev_st, host_st):
+        mods = init(cfg, st)
+        for _ in range(3):
+            for m in mods:
+                m.update(cfg, st)
+            st.it += 1
+        runs.append(st)
+    for k in ("thk", "usurf", "ubar", "vbar", "smb"):
+        h = getattr(host_st, k)
+        assert isinstance(h, np.ndarray), k
+        assert torch.from_numpy(h).is_pinned(), k
+        np.testing.assert_array_equal(h, cpu(getattr(dev_st, k)).numpy(), err_msg=k)
+    for k in ("arrhenius", "slidingco", "topg"):
+        h = getattr(host_st, k)
+        assert isinstance(h, np.ndarray) and torch.from_numpy(h).is_pinned(), k
+        np.testing.assert_array_equal(h, orig[k], err_msg=k)
+    assert float(host_st.t) == float(dev_st.t)
