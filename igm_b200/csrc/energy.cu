@@ -143,8 +143,14 @@ enum StencilMode { kEnergyOnly = 0, kGradient = 1, kAdamStep = 2 };
 // (their Adam moments and old velocities are read when they are finished).
 // The solver mode stages six tiles per level, so it looks two levels less
 // ahead to keep two CTAs per SM.
+// Energy-only mode: levels in flight and CTAs per SM (build-time constants; 3 ahead with 4 CTAs per
+// SM measured best: 115 -> 104 us at 1500^2, the gradient modes keep 4 ahead / 2 CTAs per SM, whose
+// registers a third CTA would spill)
+#ifndef IGM_STENCIL_AHEAD_E
+#define IGM_STENCIL_AHEAD_E 3
+#endif
 template <int MODE> struct Ring {
-  static constexpr int ahead = MODE == kAdamStep ? 2 : 4;
+  static constexpr int ahead = MODE == kAdamStep ? 2 : (MODE == kEnergyOnly ? IGM_STENCIL_AHEAD_E : 4);
   static constexpr int stages = ahead + 3;
 };
 
@@ -223,8 +229,14 @@ struct StencilSmem {
 #endif
 template <typename T> struct ThreadRows { static constexpr int value = IGM_STENCIL_ROWS_F32; };
 template <> struct ThreadRows<double> { static constexpr int value = 4; };
+#ifndef IGM_STENCIL_MINB_E
+#define IGM_STENCIL_MINB_E 4
+#endif
+#ifndef IGM_STENCIL_MINB_G
+#define IGM_STENCIL_MINB_G 2
+#endif
 template <typename T, int MODE> struct MinBlocks {
-  static constexpr int value = (MODE == kEnergyOnly ? 3 : 2) * 8 / IGM_STENCIL_ROWS_F32;
+  static constexpr int value = (MODE == kEnergyOnly ? IGM_STENCIL_MINB_E : IGM_STENCIL_MINB_G) * 8 / IGM_STENCIL_ROWS_F32;
 };
 template <int MODE> struct MinBlocks<double, MODE> { static constexpr int value = 2; };
 
