@@ -567,20 +567,21 @@ def run_ours(args, rank, world, dist):
     # ---- e2e: host-resident state through the process API ----------------------
     e2e = None
     if not args.no_e2e:
+        from igm_b200.state import reset_transfer_counts, transfer_counts
         st = make_state(args, host=True)
         mods = init_run(cfg_e, st)
         run_cycles(cfg_e, st, mods, W)
         t_start = float(st.t)
-        nbytes = args.size * args.size * 4
+        reset_transfer_counts(st)
         el_h, _ = timed(lambda k: run_cycles(cfg_e, st, mods, k), K, sync)
+        h2d, d2h = transfer_counts(st)  # the bytes the timed steps copied, counted by the state
         el_h = max_over_ranks(el_h)
         yrs = float(st.t) - t_start
-        # per time step: smb reads usurf; iceflow reads thk, usurf, arrhenius, slidingco; time reads nothing
-        # new (fused max); thk reads ubar, vbar, thk, topg, smb.  Writes: smb; ubar, vbar, velbase x2,
-        # velsurf x2; thk, lsurf, usurf, divflux.
+        # per time step: smb reads usurf; iceflow reads thk, usurf, arrhenius, slidingco (once per update,
+        # also at retrainings and checks); time reads nothing new (fused max); thk reads ubar, vbar, thk,
+        # topg, smb.  Writes: smb; ubar, vbar, velbase x2, velsurf x2; thk, lsurf, usurf, divflux.
         e2e = {"value": world * yrs / el_h, "unit": "model years/s",
-               "h2d_bytes_per_step": 10 * nbytes * TIME_STEPS_PER_STEP,
-               "d2h_bytes_per_step": 11 * nbytes * TIME_STEPS_PER_STEP}
+               "h2d_bytes_per_step": round(h2d / K), "d2h_bytes_per_step": round(d2h / K)}
         del st, mods
         torch.cuda.empty_cache()
     return res, det, conv_ms, clocks, launches, e2e

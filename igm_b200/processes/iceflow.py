@@ -155,6 +155,11 @@ def initialize(cfg, state):
 
 
 def update(cfg, state):
+    with S.update_scope(state):  # a host field is copied to the device once per update
+        _update(cfg, state)
+
+
+def _update(cfg, state):
     if hasattr(state, "logger"):
         state.logger.info("Update ICEFLOW at iteration : " + str(state.it))
     ic = cfg.processes.iceflow

@@ -27,6 +27,11 @@ def initialize(cfg, state):
 
 
 def update(cfg, state):
+    with S.update_scope(state):  # a host field is copied to the device once per update
+        _update(cfg, state)
+
+
+def _update(cfg, state):
     c = cfg.processes.smb_simple
     t = float(state.t)
     if (t - float(state.tlast_mb)) >= c.update_freq:

@@ -31,6 +31,11 @@ def initialize(cfg, state):
 
 
 def update(cfg, state):
+    with S.update_scope(state):  # a host field is copied to the device once per update
+        _update(cfg, state)
+
+
+def _update(cfg, state):
     if state.it >= 0:
         if hasattr(state, "logger"):
             state.logger.info("Ice thickness equation at time : " + str(float(state.t)))

@@ -31,6 +31,11 @@ def velomax(state) -> np.float32:
 
 
 def update(cfg, state):
+    with S.update_scope(state):  # a host field is copied to the device once per update
+        _update(cfg, state)
+
+
+def _update(cfg, state):
     c = cfg.processes.time
     if hasattr(state, "logger"):
         state.logger.info("Update DT at time : " + str(float(state.t)))

@@ -22,6 +22,11 @@ def initialize(cfg, state):
 
 
 def update(cfg, state):
+    with S.update_scope(state):  # a host field is copied to the device once per update
+        _update(cfg, state)
+
+
+def _update(cfg, state):
     vert_basis = cfg.processes.iceflow.numerics.vert_basis
     vf = cfg.processes.vert_flow
     if vert_basis not in ("Lagrange", "Legendre", "SIA"):

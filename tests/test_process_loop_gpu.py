@@ -379,14 +379,19 @@ def test_host_resident_state_matches_device_resident():
         orig[k] = getattr(host_st, k).cpu().numpy().copy()
         setattr(host_st, k, orig[k].copy())
     host_st.device = "cuda"
-    runs = []
+    from igm_b200.state import reset_transfer_counts, transfer_counts
     for st in (dev_st, host_st):
         mods = init(cfg, st)
+        reset_transfer_counts(st)
         for _ in range(3):
             for m in mods:
                 m.update(cfg, st)
             st.it += 1
-        runs.append(st)
+    # each process copies a field to the device at most once per update: smb 1, iceflow 4, thk 5
+    h2d, d2h = transfer_counts(host_st)
+    field = orig["thk"].nbytes
+    assert 0 < h2d <= 3 * 10 * field and h2d % field == 0, (h2d, field)
+    assert d2h > 0 and transfer_counts(dev_st) == (0, 0)
     for k in ("thk", "usurf", "ubar", "vbar", "smb"):
         h = getattr(host_st, k)
         assert isinstance(h, np.ndarray), k
