@@ -16,8 +16,11 @@ steps: --steps K times K cycles after --warmup W untimed cycles.
 
 value       emulator-driven model years/s, inputs resident in HBM.
 e2e         the same run through the process API with a host-resident state:
-            every time step copies its 2-D inputs host->device and its 2-D
-            results device->host (pinned buffers).
+            each step the caller hands its 2-D input fields in from pinned
+            host arrays (thk, usurf, topg, arrhenius, slidingco: one copy
+            each) and reads the step's result back (sync_host); every time
+            step's 2-D results go device->host into pinned arrays on a side
+            stream, overlapping the processes that follow.
 plain       the plain solver (the reference's Adam at lr 1) on the same
             workload, warm-started at the converged velocities of the initial
             state: with the reference's early stopping (its default) and with
@@ -567,19 +570,27 @@ def run_ours(args, rank, world, dist):
     # ---- e2e: host-resident state through the process API ----------------------
     e2e = None
     if not args.no_e2e:
-        from igm_b200.state import reset_transfer_counts, transfer_counts
+        from igm_b200.state import invalidate, reset_transfer_counts, sync_host, transfer_counts
         st = make_state(args, host=True)
         mods = init_run(cfg_e, st)
-        run_cycles(cfg_e, st, mods, W)
+        inputs = ("thk", "usurf", "topg", "arrhenius", "slidingco")
+
+        def e2e_steps(k):
+            for _ in range(k):
+                invalidate(st, *inputs)  # the caller hands the step's input fields in from its host arrays
+                run_cycles(cfg_e, st, mods, 1)
+                sync_host(st)  # and reads the step's result back
+            return k
+
+        e2e_steps(W)
         t_start = float(st.t)
         reset_transfer_counts(st)
-        el_h, _ = timed(lambda k: run_cycles(cfg_e, st, mods, k), K, sync)
+        el_h, _ = timed(e2e_steps, K, sync)
         h2d, d2h = transfer_counts(st)  # the bytes the timed steps copied, counted by the state
         el_h = max_over_ranks(el_h)
         yrs = float(st.t) - t_start
-        # per time step: smb reads usurf; iceflow reads thk, usurf, arrhenius, slidingco (once per update,
-        # also at retrainings and checks); time reads nothing new (fused max); thk reads ubar, vbar, thk,
-        # topg, smb.  Writes: smb; ubar, vbar, velbase x2, velsurf x2; thk, lsurf, usurf, divflux.
+        # per step: the five input fields in; per time step out: smb; ubar, vbar, velbase x2, velsurf x2;
+        # thk, lsurf, usurf, divflux
         e2e = {"value": world * yrs / el_h, "unit": "model years/s",
                "h2d_bytes_per_step": round(h2d / K), "d2h_bytes_per_step": round(d2h / K)}
         del st, mods

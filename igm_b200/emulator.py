@@ -113,7 +113,6 @@ def update_iceflow_emulated(cfg, state):
     if cfg.processes.iceflow.force_max_velbar > 0:  # emulate.py:147-148
         K.force_max_velbar(state.U, state.V, cfg.processes.iceflow.force_max_velbar)
     P.set_derived_velocities(cfg, state, mask=False)
-    S.sync_host(state)
 
 
 def train_step(model: CNN, fields_full, dx, windows, h, w, dzeta, phys, lr, opt: EmulatorOptimizer):
@@ -256,7 +255,6 @@ def update_iceflow_fallback(cfg, state):
     if fallback:
         state.U, state.V = U, V
         P.set_derived_velocities(cfg, state, mask=False)
-        S.sync_host(state)
 
 
 def update_iceflow_takeover(cfg, state):
@@ -297,7 +295,6 @@ def update_iceflow_takeover(cfg, state):
         if fallback:
             state.U, state.V = U, V
             P.set_derived_velocities(cfg, state, mask=False)
-            S.sync_host(state)
         return
     if state.__dict__.get("_igm_fallback_active", False):
         U, V, _ = state.iceflow_solver.solve(solved[0], solved[1], *f, dx, state.dzeta, nbitmax=int(fb.nbitmax),
@@ -305,7 +302,6 @@ def update_iceflow_takeover(cfg, state):
         state._igm_solved = (U, V)
         state.U, state.V = U, V
         P.set_derived_velocities(cfg, state, mask=False)
-        S.sync_host(state)
     else:
         update_iceflow_emulated(cfg, state)
 

@@ -24,6 +24,8 @@ import os
 
 import numpy as np
 
+from .state import sync_host
+
 VAR_INFO = {
     "topg": ["Basal Topography", "m"],
     "usurf": ["Surface Topography", "m"],
@@ -114,6 +116,7 @@ def update_netcdf_ex(cfg, state):
     float32 record per listed field present on the state."""
     from scipy.io import netcdf_file
     path = _opt(cfg, "output_file")
+    sync_host(state)  # a host-resident state: the processes' result copies have landed
     t = float(getattr(state, "t", 0.0))
     fields = {v: _host(getattr(state, v)) for v in _opt(cfg, "vars_to_save") if hasattr(state, v)}
     info = getattr(state, "var_info_ncdf_ex", VAR_INFO)
@@ -159,6 +162,7 @@ def update_netcdf_ts(cfg, state):
     area (thk > 1 m) dx^2 / 1e6 km^2 per save time."""
     from scipy.io import netcdf_file
     path = _opt(cfg, "output_ts_file")
+    sync_host(state)
     thk = _host(state.thk).astype(np.float64)
     dx = float(state.dx)
     vol = float(thk.sum() * dx * dx / 1e9)

@@ -276,7 +276,7 @@ def optimize_update(cfg, state, cost, i):
     lib, st = L.lib(), L.stream_ptr()
     x = {}
     for k, c in enumerate(a.controls):
-        x[c] = S.get(state, c).contiguous()
+        x[c] = S.get(state, c, writable=True).contiguous()  # rewritten in place by the control update below
         K.assim_control(0, x[c], a.scale[c], variable=a.block(a.var, k), m=a.block(a.m, k), v=a.block(a.v, k),
                         **a.control_kw(c))
         S.put(state, c, x[c])
@@ -331,7 +331,7 @@ def optimize_update(cfg, state, cost, i):
         S.put(state, c, x[c])
     if a.reproject and "icemask" in a.cost_list and "thk" not in a.controls:
         # update.py:84-88: thk is masked by the reprojection even when it is not a control
-        thk = S.get(state, "thk").contiguous()
+        thk = S.get(state, "thk", writable=True).contiguous()
         K.assim_control(3, thk, 1.0, icemaskobs=a.icemaskobs)
         S.put(state, "thk", thk)
     thk = S.get(state, "thk").contiguous()
@@ -404,6 +404,7 @@ def _snapshot_fields(cfg, state):
     if "sliding_ratio" in want:
         vs = state.velsurf_mag
         state.sliding_ratio = torch.where(vs > 10, state.velbase_mag / vs, torch.full_like(vs, float("nan")))
+    S.sync_host(state)  # a host-resident state: the result copies have landed
     out = {}
     for v in want:
         if hasattr(state, v):

@@ -125,7 +125,6 @@ def update_iceflow_solved(cfg, state):
                    + "-" + str(state.it) + ".dat", np.array(costs), fmt="%5.10f")
     state.COST_Glen = float(costs[-1]) if len(costs) else float("nan")
     set_derived_velocities(cfg, state, mask=False)
-    S.sync_host(state)
 
 
 def initialize(cfg, state):

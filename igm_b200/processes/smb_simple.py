@@ -46,7 +46,6 @@ def _update(cfg, state):
         icemask = S.get(state, "icemask") if hasattr(state, "icemask") else None
         smb = K.smb_simple(usurf, gradabl, gradacc, ela, maxacc, icemask=icemask)
         S.put(state, "smb", smb)
-        S.sync_host(state)
         state.tlast_mb = t
 
 

@@ -50,7 +50,6 @@ def _update(cfg, state):
         S.put(state, "thk", thk_new)
         S.put(state, "lsurf", lsurf)
         S.put(state, "usurf", usurf)
-        S.sync_host(state)
 
 
 def finalize(cfg, state):

@@ -45,7 +45,6 @@ def _update(cfg, state):
     S.put(state, "W", W)
     S.put(state, "wvelbase", W[0])
     S.put(state, "wvelsurf", W[-1])
-    S.sync_host(state)
 
 
 def finalize(cfg, state):

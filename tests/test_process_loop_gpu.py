@@ -32,6 +32,7 @@ from igm_b200 import emulator as E
 from igm_b200.config import default_cfg
 from igm_b200.processes import iceflow, smb_simple, thk
 from igm_b200.processes import time as tproc
+from igm_b200 import state as S
 from igm_b200.state import State
 from oracle import iceflow_oracle as O
 from tests.gpu_util import rel_l2
@@ -367,38 +368,85 @@ def test_force_max_velbar_in_the_process(method):
     assert torch.equal(st.uvelsurf, st.U[-1]) and torch.equal(st.uvelbase, st.U[0])
 
 
-def test_host_resident_state_matches_device_resident():
-    """The same three solved time steps with the state in host numpy arrays
-    and on the device: identical fields; the caller's input arrays are
-    replaced by pinned arrays of the same values (so each step's copies are
-    DMAs), and the outputs come back as pinned numpy arrays."""
-    cfg = make_cfg("solved", nbitmax=10)
+def _host_and_device_states(cfg):
+    """The same glacier as a device-resident state and as a host-resident
+    one whose input fields are the caller's numpy arrays."""
     dev_st, host_st = make_state(seed=5), make_state(seed=5)
     orig = {}
     for k in ("topg", "thk", "arrhenius", "slidingco"):
         orig[k] = getattr(host_st, k).cpu().numpy().copy()
         setattr(host_st, k, orig[k].copy())
     host_st.device = "cuda"
-    from igm_b200.state import reset_transfer_counts, transfer_counts
-    for st in (dev_st, host_st):
-        mods = init(cfg, st)
-        reset_transfer_counts(st)
-        for _ in range(3):
-            for m in mods:
+    return dev_st, host_st, orig
+
+
+def _steps(cfg, states, mods, n):
+    for st, ms in zip(states, mods):
+        for _ in range(n):
+            for m in ms:
                 m.update(cfg, st)
             st.it += 1
-    # each process copies a field to the device at most once per update: smb 1, iceflow 4, thk 5
-    h2d, d2h = transfer_counts(host_st)
-    field = orig["thk"].nbytes
-    assert 0 < h2d <= 3 * 10 * field and h2d % field == 0, (h2d, field)
-    assert d2h > 0 and transfer_counts(dev_st) == (0, 0)
-    for k in ("thk", "usurf", "ubar", "vbar", "smb"):
+
+
+def _assert_same(dev_st, host_st, keys=("thk", "usurf", "ubar", "vbar", "smb")):
+    S.sync_host(host_st)
+    for k in keys:
         h = getattr(host_st, k)
         assert isinstance(h, np.ndarray), k
         assert torch.from_numpy(h).is_pinned(), k
         np.testing.assert_array_equal(h, cpu(getattr(dev_st, k)).numpy(), err_msg=k)
+    assert float(host_st.t) == float(dev_st.t)
+
+
+def test_host_resident_state_matches_device_resident():
+    """The same three solved time steps with the state in host numpy arrays
+    and on the device: identical fields once sync_host returned; the
+    caller's input arrays are replaced by pinned arrays of the same values
+    (so each copy is a DMA), the outputs come back as pinned numpy arrays,
+    and a field the state holds on the device is not copied again."""
+    cfg = make_cfg("solved", nbitmax=10)
+    dev_st, host_st, orig = _host_and_device_states(cfg)
+    mods = [init(cfg, st) for st in (dev_st, host_st)]
+    for st in (dev_st, host_st):
+        S.reset_transfer_counts(st)
+    _steps(cfg, (dev_st, host_st), mods, 3)
+    # each of the caller's four input fields goes to the device at most once over the run
+    h2d, d2h = S.transfer_counts(host_st)
+    field = orig["thk"].nbytes
+    assert h2d <= 4 * field and h2d % field == 0, (h2d, field)
+    assert d2h >= 3 * 10 * field and S.transfer_counts(dev_st) == (0, 0), d2h
+    _assert_same(dev_st, host_st)
     for k in ("arrhenius", "slidingco", "topg"):
         h = getattr(host_st, k)
         assert isinstance(h, np.ndarray) and torch.from_numpy(h).is_pinned(), k
         np.testing.assert_array_equal(h, orig[k], err_msg=k)
-    assert float(host_st.t) == float(dev_st.t)
+
+
+def test_host_resident_state_sees_rebound_and_invalidated_fields():
+    """A host field the caller rebinds to another array, or changes in place
+    and declares with invalidate(), reaches the device on the next update
+    (one copy each); results stay identical to a device-resident state given
+    the same changes."""
+    cfg = make_cfg("solved", nbitmax=10)
+    dev_st, host_st, _ = _host_and_device_states(cfg)
+    mods = [init(cfg, st) for st in (dev_st, host_st)]
+    _steps(cfg, (dev_st, host_st), mods, 2)
+    _assert_same(dev_st, host_st)
+    field = np.asarray(host_st.thk).nbytes
+    # rebinding: a new array
+    host_st.slidingco = np.asarray(host_st.slidingco) * np.float32(1.5)
+    dev_st.slidingco = dev_st.slidingco * 1.5
+    S.reset_transfer_counts(host_st)
+    _steps(cfg, (dev_st, host_st), mods, 1)
+    assert S.transfer_counts(host_st)[0] == field
+    _assert_same(dev_st, host_st)
+    # in place: the state's own (pinned) arrays, declared changed
+    host_st.thk[...] = np.maximum(host_st.thk - np.float32(5.0), np.float32(0.0))
+    host_st.topg += np.float32(1.0)
+    S.invalidate(host_st, "thk", "topg")
+    dev_st.thk = torch.clamp(dev_st.thk - 5.0, min=0.0)
+    dev_st.topg = dev_st.topg + 1.0
+    S.reset_transfer_counts(host_st)
+    _steps(cfg, (dev_st, host_st), mods, 1)
+    assert S.transfer_counts(host_st)[0] == 2 * field
+    _assert_same(dev_st, host_st)

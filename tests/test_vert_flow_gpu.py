@@ -10,7 +10,7 @@ import torch
 from igm_b200 import kernels as K
 from igm_b200.config import default_cfg
 from igm_b200.processes import vert_flow
-from igm_b200.state import State
+from igm_b200.state import State, sync_host
 from oracle import iceflow_oracle as O
 from tests.gpu_util import dev
 
@@ -94,6 +94,7 @@ def test_process_api(host, method):
     vert_flow.initialize(cfg, st)
     vert_flow.update(cfg, st)
     vert_flow.finalize(cfg, st)
+    sync_host(st)  # a host-resident state holds the results once the copies have landed
     fn = O.vertical_velocity_kinematic if method == "kinematic" else O.vertical_velocity_incompressibility
     ref = fn(*(torch.as_tensor(a) for a in (U, V, topg, thk)), lv, w, 50.0).numpy()
     W = st.W if host else st.W.cpu().numpy()
