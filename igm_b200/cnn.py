@@ -142,7 +142,6 @@ class CNN:
                 b["npart2"] = 2 * npart     # head / first-layer reductions: two CTAs per SM
                 wlen = max(int(L.lib().igm_conv3x3_wgrad_partial_len(F)), int(L.lib().igm_conv3x3_wgrad_partial_len(16)))
                 b["wpart"] = torch.empty(npart * wlen, dtype=torch.float32, device=d)
-                b["dbpart"] = torch.zeros((npart, F), dtype=torch.float32, device=d)
                 # the hidden layers' fused backward alternates between two partial buffers: each call
                 # finishes the previous call's partials while it writes its own
                 plen = int(L.lib().igm_conv3x3_wgrad_partial_len(F))
@@ -278,13 +277,7 @@ class CNN:
                 L.check(lib.igm_reduce_partials(_p(buf["dbpart2"][prev % 2]), npart, F, F,
                                                 gp + 4 * self.offsets[2 * (prev - 1) + 1], 0, st), "reduce db")
                 prev = None
-            if l > 0 and param_grads:
-                rc = lib.igm_conv3x3_wgrad(B, h, w, F, _p(acts[l - 1]), _p(gl), _p(buf["wpart"]), npart,
-                                           _p(self.err), st)
-                L.check(rc, f"igm_conv3x3_wgrad layer {l}")
-                rc = lib.igm_cnn_wgrad_finish(_p(buf["wpart"]), npart, F, F, gp + 4 * self.offsets[2 * l], st)
-                L.check(rc, "igm_cnn_wgrad_finish")
-            elif l == 0:
+            if l == 0:
                 if field_grad is not None:
                     ng = int(field_grad.shape[1])
                     if field_grad.shape != (B, ng, h, w) or not field_grad.is_contiguous() or ng > self.cin:
@@ -301,13 +294,11 @@ class CNN:
                                                         st)
                     L.check(rc, "igm_cnn_wgrad_finish_split")
             if l > 0:
+                # the data gradient alone (no parameter gradients wanted)
                 nxt = g[1 - cur]
-                rc = lib.igm_conv3x3(1, B, h, w, F, _p(gl), self._wb(l), None, _p(acts[l - 1]), _p(nxt),
-                                     _p(buf["dbpart"]) if param_grads else None, npart, self.alpha, _p(self.err), st)
+                rc = lib.igm_conv3x3(1, B, h, w, F, _p(gl), self._wb(l), None, _p(acts[l - 1]), _p(nxt), None, npart,
+                                     self.alpha, _p(self.err), st)
                 L.check(rc, f"igm_conv3x3 dgrad layer {l}")
-                if param_grads:
-                    L.check(lib.igm_reduce_partials(_p(buf["dbpart"]), npart, F, F,
-                                                    gp + 4 * self.offsets[2 * (l - 1) + 1], 0, st), "reduce db")
                 cur = 1 - cur
 
     def adam_step(self, lr, beta_1=0.9, beta_2=0.999, epsilon=1e-7, clipnorm=1.0):
