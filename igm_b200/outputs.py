@@ -95,6 +95,7 @@ def run(cfg, state):
     file and the time-series file."""
     if not getattr(state, "saveresult", False):
         return
+    sync_host(state)  # a host-resident state: the processes' result copies have landed
     fmts = list(_opt(cfg, "file_format_list"))
     if any(f not in ("netcdf",) for f in fmts):
         raise NotImplementedError(f"output formats {fmts}: only 'netcdf' is written")
