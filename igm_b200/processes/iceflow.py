@@ -154,7 +154,7 @@ def initialize(cfg, state):
 
 
 def update(cfg, state):
-    with S.update_scope(state):  # a host field is copied to the device once per update
+    with S.update_scope(state):  # host-resident state: the results go back in one batch at the end
         _update(cfg, state)
 
 
