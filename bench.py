@@ -34,12 +34,12 @@ accuracy    velocity error (relative L2 of the staggered velocities over ice
             independent minimisation of the same energy), the fallback log
             of the timed window, and the emulator's initial-state field
             polished by k = 10 .. 1000 plain-solver iterations (untimed).
-config1     the 100 x 100 plain-solver run (100 iterations per time step, ELA
+plain 100   the 100 x 100 plain-solver run (100 iterations per time step, ELA
             transport) against the oracle on the same first time steps.
-config3     the emulator training recipe alone: a fresh He-initialised network,
+recipe      the emulator training recipe alone: a fresh He-initialised network,
             2000 Adam steps at lr 1e-4 on batches of 8 windows of 64 x 64
             cells, its whole-domain velocity error against the judge.
-config5     4096 x 4096 x Nz 16 (ridge bed, plain spin-up): emulator vs plain.
+4096        4096 x 4096 x Nz 16 (ridge bed, plain spin-up): emulator vs plain.
 --impl reference   the oracle's restatement of the same emulated run
             (torch-CPU FP32, all host threads, the same network weights) on a
             band of columns at the valley's upstream end, where the fastest ice
@@ -87,9 +87,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-da", action="store_true")
-    ap.add_argument("--no-config1", action="store_true")
-    ap.add_argument("--no-config3", action="store_true")
-    ap.add_argument("--no-config5", action="store_true")
+    ap.add_argument("--no-plain-100", action="store_true")
+    ap.add_argument("--no-recipe", action="store_true")
+    ap.add_argument("--no-4096", action="store_true")
     ap.add_argument("--no-kernels", action="store_true")
     ap.add_argument("--write-emulator", default="", help="pretrain the bench's emulator, write it to this "
                     "directory (model.npz, fieldin.dat, vert_grid.dat) and exit")
@@ -508,8 +508,8 @@ def run_ours(args, rank, world, dist):
     # untimed: the emulator polished by k plain-solver iterations, against the same judge
     det["polished"] = polished_errors(cfg_e, st, Uj, Vj)
     res["polished_vel_rel_l2_vs_fp64"] = {str(r["iterations"]): r["vel_rel_l2_vs_fp64"] for r in det["polished"]}
-    if rank == 0 and not args.no_config3:
-        det["config3"] = emulator_recipe(args, cfg_e, st, Uj, Vj)
+    if rank == 0 and not args.no_recipe:
+        det["emulator_recipe"] = emulator_recipe(args, cfg_e, st, Uj, Vj)
     U_init, V_init = Uj.float(), Vj.float()
     run_cycles(cfg_e, st, mods, W)
     conv_ev = []
@@ -834,7 +834,7 @@ def roofline_conv(conv_ms, size, peaks, layers=15):
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback"}
 
 
-def config1(args, cpu_steps=2, gpu_max_steps=3000, gpu_max_s=40.0):
+def plain_run_100x100(args, cpu_steps=2, gpu_max_steps=3000, gpu_max_s=40.0):
     """The 100 x 100 valley glacier at dx 100 m, Nz 10 (A 78, c 0.045): the
     plain solver at 100 Adam iterations per time step (early stopping off),
     then the ELA transport (ELA 2900 m, gradient 0.009 /a, cap 2 m/a), CFL
@@ -886,12 +886,12 @@ def config1(args, cpu_steps=2, gpu_max_steps=3000, gpu_max_s=40.0):
                                   "years_per_s": first[1] / first[0]}
     del st, mods
     if not args.no_cpu:
-        out["cpu"] = config1_cpu(cpu_steps)
+        out["cpu"] = plain_run_100x100_cpu(cpu_steps)
     return out
 
 
-def config1_cpu(nsteps):
-    """The oracle on the first nsteps time steps of config1 (all host threads)."""
+def plain_run_100x100_cpu(nsteps):
+    """The oracle on the first nsteps time steps of the 100 x 100 plain run (all host threads)."""
     import torch
     from oracle import iceflow_oracle as O
     from igm_b200.synthetic import valley_glacier
@@ -918,7 +918,7 @@ def config1_cpu(nsteps):
             "cores": os.cpu_count() or 1, "kind": "port"}
 
 
-def config5(args, spinup_years=50.0, pretrain_steps=3000, K5=10, nz=16, n=4096):
+def run_4096x4096(args, spinup_years=50.0, pretrain_steps=3000, K5=10, nz=16, n=4096):
     """4096 x 4096 at dx 25 m, Nz 16: the ridge bed (a 0.05 plane + 12 seeded
     Gaussian ridges), thk from a plain-solver spin-up of spinup_years under
     ELA 2800 m (untimed), an emulator with 2 x 16 = 32 outputs pretrained
@@ -1276,10 +1276,10 @@ def main():
             det["plain_kernels"] = plain_kernels(args, peaks)
         if not args.no_da:
             det["data_assimilation"] = assimilation_bench(args, peaks)
-        if not args.no_config1:
-            det["config1"] = config1(args)
-        if not args.no_config5:
-            det["config5"] = config5(args)
+        if not args.no_plain_100:
+            det["plain_100x100"] = plain_run_100x100(args)
+        if not args.no_4096:
+            det["run_4096x4096xNz16"] = run_4096x4096(args)
     line = {"metric": METRIC, "value": value, "unit": "model years/s", "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": 1e3 * em["seconds"] / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16 conv / f32 energy", "data": "synthetic",
@@ -1301,17 +1301,17 @@ def main():
             "roofline": roofline_conv(conv_ms, args.size, peaks, layers=15),
             "clocks": clocks, "gpu_launches": int(launches), "e2e": e2e}
     if rank == 0:
-        if "config1" in det:
-            c1 = det["config1"]
-            line["config1_years_per_s"] = c1["gpu"]["years_per_s"]
+        if "plain_100x100" in det:
+            c1 = det["plain_100x100"]
+            line["plain_100x100_years_per_s"] = c1["gpu"]["years_per_s"]
             if "cpu" in c1 and "gpu_first_steps" in c1:
-                line["config1_first_steps_gpu_vs_cpu"] = (c1["gpu_first_steps"]["years_per_s"]
+                line["plain_100x100_first_steps_gpu_vs_cpu"] = (c1["gpu_first_steps"]["years_per_s"]
                                                           / c1["cpu"]["years_per_s"])
-        if "config3" in det:
-            line["config3_recipe_vel_rel_l2_vs_fp64"] = det["config3"]["vel_rel_l2_vs_fp64"]
-        if "config5" in det:
-            line["config5_speedup_vs_plain"] = det["config5"]["speedup_vs_plain"]
-            line["config5_emulated_years_per_s"] = det["config5"]["emulated"]["years_per_s"]
+        if "emulator_recipe" in det:
+            line["recipe_64x64_windows_vel_rel_l2_vs_fp64"] = det["emulator_recipe"]["vel_rel_l2_vs_fp64"]
+        if "run_4096x4096xNz16" in det:
+            line["emulated_4096x4096_speedup_vs_plain"] = det["run_4096x4096xNz16"]["speedup_vs_plain"]
+            line["emulated_4096x4096_years_per_s"] = det["run_4096x4096xNz16"]["emulated"]["years_per_s"]
         if world == 1 and not args.no_cpu:
             try:
                 v, cb = cpu_emulated_band(args, min(K, 3), 1)

@@ -62,7 +62,7 @@ def test_adjoint_central_differences_1000x1000():
     assert np.median(errs) < 1e-6 and np.max(errs) < 1e-3, (np.median(errs), np.max(errs))
 
 
-def _config5_state(n=4096, dx=25.0, nz=16):
+def _ridge_state(n=4096, dx=25.0, nz=16):
     st = ridge_glacier(n, dx, seed=0)
     x = np.arange(n) * dx
     X, Y = np.meshgrid(x, x)
@@ -73,7 +73,7 @@ def _config5_state(n=4096, dx=25.0, nz=16):
 
 def test_fp32_matches_fp64_4096x4096_nz16():
     n, nz, dx = 4096, 16, 25.0
-    thk, usurf, A, c = _config5_state(n, dx, nz)
+    thk, usurf, A, c = _ridge_state(n, dx, nz)
     dz = _dzeta(nz)
     g = torch.Generator("cuda").manual_seed(5)
     U64 = torch.randn((nz, n, n), dtype=torch.float64, device="cuda", generator=g) * 40 + 30
@@ -95,7 +95,7 @@ def test_fp32_matches_fp64_4096x4096_nz16():
 def test_transport_bit_exact_4096x4096():
     n, dx = 4096, 25.0
     rng = np.random.default_rng(9)
-    thk, usurf, _, _ = _config5_state(n, dx)
+    thk, usurf, _, _ = _ridge_state(n, dx)
     topg = (usurf - thk).astype(np.float32)
     u = rng.normal(0, 80, (n, n)).astype(np.float32)
     v = rng.normal(0, 80, (n, n)).astype(np.float32)
