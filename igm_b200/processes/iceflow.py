@@ -18,8 +18,6 @@ default energy components, no sliding_law, dim_arrhenius 2, architecture
 
 from __future__ import annotations
 
-import os
-
 import numpy as np
 import torch
 
