@@ -9,7 +9,6 @@ pinnbp_10_4_cnn_16_32_2_1_a/model.h5."""
 
 import os
 
-import numpy as np
 import pytest
 import torch
 
