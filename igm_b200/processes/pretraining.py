@@ -23,8 +23,10 @@ scipy's netCDF reader, so ``ex.nc`` must be netCDF-3 (the format the output
 writer ``igm_b200.outputs`` produces; a netCDF-4 file raises
 NotImplementedError naming the conversion); the draws use a seeded numpy
 generator (``pretraining.seed``) where the reference draws unseeded; the
-models are written as ``model-<epoch>.npz`` / ``model.npz`` (the emulator's
-save format) instead of Keras ``.h5``; the misfit plots are not drawn
+models are written as the reference's Keras ``model-<epoch>.h5`` /
+``model.h5`` and, beside them, as ``.npz`` (the exact parameters with their
+scales and the Adam state, which this package's loader reads); the misfit
+plots are not drawn
 (no matplotlib).  Every computation on the fields -- the solves, the
 network's forward and backward passes, the energy and its adjoint, Adam --
 runs in the device kernels; the host prepares the inputs (slicing,
@@ -189,10 +191,19 @@ def misfits(cfg, state, thk, U, V, Up, Vp):
     return n1, n2, l1bar, l1bar
 
 
-def _save(net, path):
+def _save(net, path, init="glorot_uniform"):
+    """The network at ``path`` (``.npz``: the exact parameters with their
+    input and output scales and the Adam state, which this package's loader
+    reads) and beside it, under the same name with ``.h5``, the Keras model
+    file the reference writes (pretraining.py:350-351, 491-492): the network
+    on raw fields, which the reference's emulator loads."""
+    from ..emulator import keras_variables
+    from ..keras_h5 import write_keras_cnn
     np.savez(path, params=net.params.cpu().numpy(), adam_m=net.m.cpu().numpy(), adam_v=net.v.cpu().numpy(),
              iterations=np.array(net.opt_iterations), nb_layers=np.array(net.L), nout=np.array(net.nout),
              cin=np.array(net.cin), scales=net.scales, out_scale=np.array(net.out_scale))
+    write_keras_cnn(os.path.splitext(path)[0] + ".h5", keras_variables(net), net.L, net.cin, net.nout,
+                    alpha=net.alpha, init=init)
 
 
 def train_iceflow_emulator(cfg, state, trainingset, augmentation=True):
@@ -201,6 +212,7 @@ def train_iceflow_emulator(cfg, state, trainingset, augmentation=True):
     pt = cfg.processes.pretraining
     e = ic.emulator
     nz = int(ic.numerics.Nz)
+    init = str(e.network.weight_initialization)
     dev = torch.device("cuda", torch.cuda.current_device())
     rng = np.random.default_rng(int(pt.get("seed", 0)))
     net = CNN(nb_layers=int(e.network.nb_layers), cin=len(e.fieldin), nout=2 * nz,
@@ -244,7 +256,7 @@ def train_iceflow_emulator(cfg, state, trainingset, augmentation=True):
             train_step(net, f, float((x[1] - x[0]) * co), [(0, 0)], ny, nx, state.dzeta, phys, lr, opt)
         lr = learning_rate(cfg, epoch)
         if epoch % save_every == 0:
-            _save(net, os.path.join(state.direct_name, f"model-{epoch}.npz"))
+            _save(net, os.path.join(state.direct_name, f"model-{epoch}.npz"), init)
         if epoch % int(pt.freq_test) == 0:
             mis, mis_co = [], []
             for par, (fx, (U, V)), cost0 in zip(state.PAR, state.solutions, state.solutions_cost):
@@ -269,7 +281,7 @@ def train_iceflow_emulator(cfg, state, trainingset, augmentation=True):
     net.check_errors()
     state.MISFIT = np.stack(state.MISFIT) if state.MISFIT else np.zeros((0, len(state.PAR)))
     state.MISFIT_CO = np.stack(state.MISFIT_CO) if state.MISFIT_CO else np.zeros((0, len(state.PAR)))
-    _save(net, os.path.join(state.direct_name, "model.npz"))
+    _save(net, os.path.join(state.direct_name, "model.npz"), init)
     state.iceflow_model = net
 
 

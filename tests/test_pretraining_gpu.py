@@ -65,8 +65,8 @@ def test_pretraining_process(tmp_path, monkeypatch):
         assert (case / "costs-stokes.dat").exists()
         rows = np.loadtxt(case / "misfit-pinn.dat", ndmin=2)
         assert rows.shape == (3, 6) and list(rows[:, 0]) == [0, 4, 8]
-    for f in ("model.npz", "model-0.npz", "model-2.npz", "model-10.npz"):
-        assert (d / f).exists(), f
+    for f in ("model", "model-0", "model-2", "model-10"):
+        assert (d / (f + ".npz")).exists() and (d / (f + ".h5")).exists(), f
     assert st.MISFIT.shape == (3, 6) and st.MISFIT_CO.shape == (3, 6)
     # the energy gap of the emulator to the solved test cases shrinks with training
     gap = st.MISFIT_CO.mean(1)
