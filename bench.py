@@ -1306,7 +1306,7 @@ def main():
             line["plain_100x100_years_per_s"] = c1["gpu"]["years_per_s"]
             if "cpu" in c1 and "gpu_first_steps" in c1:
                 line["plain_100x100_first_steps_gpu_vs_cpu"] = (c1["gpu_first_steps"]["years_per_s"]
-                                                          / c1["cpu"]["years_per_s"])
+                                                                / c1["cpu"]["years_per_s"])
         if "emulator_recipe" in det:
             line["recipe_64x64_windows_vel_rel_l2_vs_fp64"] = det["emulator_recipe"]["vel_rel_l2_vs_fp64"]
         if "run_4096x4096xNz16" in det:
